@@ -1,0 +1,104 @@
+/*
+ * pf_oracle.h -- CPU restatement of the adaptive-pf-flip sparse 3D two-phase
+ * solver step (P2G, marker/boundary passes, beta=1/rho PCG projection, G2P,
+ * RK2/RK3 advection).
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is the checker that the GPU path is
+ * compared against; it is never linked into, loaded by, or called from the
+ * product library (libpfgpu).  Only tests, the smoke check and the CPU-baseline
+ * leg of bench.py use it.
+ *
+ * Every function states the reference file:line it restates (paths relative to
+ * the adaptive-pf-flip source tree).  The floating-point operation order of the
+ * reference is kept wherever the result is compared bit-for-bit (activation
+ * tests, per-node accumulation order, PCG reductions in ascending cell order),
+ * so the oracle reproduces the reference's own outputs exactly on the same
+ * inputs; the parity tests check that against the compiled reference.
+ *
+ * Grid representation: every field is a dense float array over its own node
+ * lattice (u: (nx+1,ny,nz), v: (nx,ny+1,nz), w: (nx,ny,nz+1), mu/mv/mw alike,
+ * p and the marker: (nx,ny,nz)), index i + X*(j + Y*k), plus a byte per 4^3
+ * block (bid = bx + nbx*(by + nby*bz)) recording whether the reference's
+ * SparseBlockGrid3D<4> would hold that block active.  Values inside inactive
+ * blocks are kept at zero, which is what SparseBlockGrid3D::get returns for
+ * them (src/grid/sparse_block_grid3d.h:50-55).
+ */
+#ifndef PF_ORACLE_H
+#define PF_ORACLE_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { PFO_U = 0, PFO_V, PFO_W, PFO_MU, PFO_MV, PFO_MW, PFO_P, PFO_MK, PFO_NFIELDS };
+
+typedef struct pfo_grid pfo_grid;
+
+typedef struct {
+  double rho_l, rho_g, alpha_phi, rho_tilde_0; /* PhaseParams, src/physics/phasefield.h:4-9 */
+} pfo_phase;
+
+typedef struct {
+  int max_iter;     /* cg_iters */
+  double abs_tol;   /* reference cg_tol: stop when max|r| < tol */
+  double rel_tol;   /* 0 = reference behaviour; else tol = max(abs, rel*max|r0|) */
+  double c_div;     /* divergenceCorrection */
+} pfo_solve_cfg;
+
+typedef struct {
+  int iterations;
+  int n_cells;
+  long long pin_cell; /* linear cell index or -1 */
+  double res0, res_final, tol_effective;
+  int converged;
+  int breakdown;
+} pfo_solve_stats;
+
+typedef struct {
+  int clamped_liquid, clamped_gas;
+  int x_lo, x_hi, y_lo, y_hi, z_lo, z_hi;
+} pfo_clamp_stats;
+
+typedef struct {
+  double dt, gravity, Vp, alpha_l, alpha_g;
+  int cg_iters;
+  double cg_tol, cg_rel_tol, c_div;
+  int advect_order;
+} pfo_step_cfg;
+
+pfo_grid* pfo_grid_create(int nx, int ny, int nz, double dx, double ox, double oy, double oz);
+void pfo_grid_destroy(pfo_grid* g);
+int pfo_grid_copy(pfo_grid* dst, const pfo_grid* src);
+int pfo_field_dims(const pfo_grid* g, int f, int* dims3, int* bdims3);
+int pfo_get_field(const pfo_grid* g, int f, float* dense, unsigned char* act);
+int pfo_set_field(pfo_grid* g, int f, const float* dense, const unsigned char* act);
+int pfo_clear_field(pfo_grid* g, int f);
+int pfo_clear_all(pfo_grid* g);
+
+double pfo_phi_from_raw(double raw, const pfo_phase* pp);
+double pfo_beta_from_raw(double raw, const pfo_phase* pp);
+double pfo_calibrate_rho_tilde0(const pfo_phase* pp, double Vp);
+
+int pfo_mark_cells(pfo_grid* g, size_t n, const double* pos);
+int pfo_p2g(pfo_grid* g, size_t n, const double* pos, const double* vel,
+            const unsigned char* type, const double* vol, const pfo_phase* pp, double Vp);
+int pfo_apply_gravity(pfo_grid* g, double dt, double gravity);
+int pfo_apply_wall_boundary(pfo_grid* g);
+int pfo_project(pfo_grid* g, const pfo_phase* pp, double dt, const pfo_solve_cfg* cfg,
+                pfo_solve_stats* st);
+int pfo_g2p(const pfo_grid* g, const pfo_grid* saved, size_t n, const double* pos, double* vel,
+            const unsigned char* type, double aL, double aG);
+int pfo_advect(const pfo_grid* g, size_t n, double* pos, const unsigned char* type,
+               const double* vel, const double* vol, double dt, int order,
+               pfo_clamp_stats* st, double* escape_out, size_t* n_escape);
+int pfo_collect_cells(const pfo_grid* g, int marker, int* out, size_t* n);
+int pfo_step(pfo_grid* g, pfo_grid* saved, size_t n, double* pos, double* vel,
+             const unsigned char* type, const double* vol, const pfo_phase* pp,
+             const pfo_step_cfg* cfg, pfo_solve_stats* sst, pfo_clamp_stats* cst);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,210 @@
+// ref_capi.cpp -- TEST INFRASTRUCTURE ONLY.
+//
+// A thin extern "C" wrapper that drives the UNMODIFIED adaptive-pf-flip
+// reference (its sparse 3D two-phase sources compiled where they lie, see
+// oracle/Makefile) so Python tests can feed it the same seeded inputs as the
+// GPU path and the C restatement.  Nothing here reimplements reference
+// arithmetic: every operation calls the reference's own public API
+//   spP2G3D_tp / spProjectStepVC3D / spG2P3D_tp / spAdvect3D_tp
+//     (src/driver/sparse_ops3d_tp.h:8-15)
+//   SparseSim3DTP::step()   (src/driver/sparse_sim3d_tp.cpp:854-884)
+//   calibrateRhoTilde0      (src/transfer/transfer3d_tp.cpp:29-36)
+//   phiFromRawDensity / betaFromPhi (src/physics/phasefield.h:10-18)
+// and converts between its SparseMacGrid3D<4> block pool and dense arrays
+// plus one activity byte per 4^3 block.
+#include "driver/sparse_ops3d_tp.h"
+#include "driver/sparse_sim3d_tp.h"
+#include "grid/sparse_mac_grid3d.h"
+#include "particles/particles3d_tp.h"
+#include "physics/phasefield.h"
+#include "transfer/transfer3d_tp.h"
+
+#include <cstddef>
+#include <cstring>
+#include <new>
+
+namespace {
+
+struct Handle {
+  SparseSim3DTP sim;
+  Handle(int nx, int ny, int nz, double dx) : sim(nx, ny, nz, dx) {}
+};
+
+SparseBlockGrid3D<4>* fieldOf(SparseMacGrid3D<4>& g, int f) {
+  switch (f) {
+    case 0: return &g.uf;
+    case 1: return &g.vf;
+    case 2: return &g.wf;
+    case 3: return &g.muf;
+    case 4: return &g.mvf;
+    case 5: return &g.mwf;
+    case 6: return &g.pf;
+    case 7: return &g.mkf;
+    default: return nullptr;
+  }
+}
+
+PhaseParams phaseOf(const double* ph) {
+  PhaseParams pp;
+  pp.rho_l = ph[0];
+  pp.rho_g = ph[1];
+  pp.alpha_phi = ph[2];
+  pp.rho_tilde_0 = ph[3];
+  return pp;
+}
+
+}  // namespace
+
+extern "C" {
+
+void* pfr_create(int nx, int ny, int nz, double dx, double ox, double oy, double oz) {
+  Handle* h = new (std::nothrow) Handle(nx, ny, nz, dx);
+  if (!h) return nullptr;
+  h->sim.grid.ox = ox;
+  h->sim.grid.oy = oy;
+  h->sim.grid.oz = oz;
+  return h;
+}
+
+void pfr_destroy(void* hp) { delete static_cast<Handle*>(hp); }
+
+int pfr_copy_grid(void* dst, const void* src) {
+  static_cast<Handle*>(dst)->sim.grid = static_cast<const Handle*>(src)->sim.grid;
+  return 0;
+}
+
+int pfr_get_field(void* hp, int f, float* dense, unsigned char* act) {
+  SparseBlockGrid3D<4>* fld = fieldOf(static_cast<Handle*>(hp)->sim.grid, f);
+  if (!fld) return -1;
+  const size_t nb = fld->totalBlocks();
+  for (size_t b = 0; b < nb; ++b) act[b] = fld->blockmap[b] >= 0 ? 1 : 0;
+  for (int k = 0; k < fld->nz; ++k)
+    for (int j = 0; j < fld->ny; ++j)
+      for (int i = 0; i < fld->nx; ++i)
+        dense[(size_t)i + (size_t)fld->nx * ((size_t)j + (size_t)fld->ny * k)] = fld->get(i, j, k);
+  return 0;
+}
+
+int pfr_set_field(void* hp, int f, const float* dense, const unsigned char* act) {
+  SparseBlockGrid3D<4>* fld = fieldOf(static_cast<Handle*>(hp)->sim.grid, f);
+  if (!fld) return -1;
+  fld->clear();
+  for (int bz = 0; bz < fld->nbz; ++bz)
+    for (int by = 0; by < fld->nby; ++by)
+      for (int bx = 0; bx < fld->nbx; ++bx)
+        if (act[fld->bid(bx, by, bz)]) fld->activateBlock(bx, by, bz);
+  for (int k = 0; k < fld->nz; ++k)
+    for (int j = 0; j < fld->ny; ++j)
+      for (int i = 0; i < fld->nx; ++i)
+        if (fld->blockActive(i / 4, j / 4, k / 4))
+          fld->ref(i, j, k) = dense[(size_t)i + (size_t)fld->nx * ((size_t)j + (size_t)fld->ny * k)];
+  return 0;
+}
+
+// Active block ids in the reference's allocation order.
+int pfr_active_block_ids(void* hp, int f, int* out, size_t* n) {
+  SparseBlockGrid3D<4>* fld = fieldOf(static_cast<Handle*>(hp)->sim.grid, f);
+  if (!fld) return -1;
+  const auto& ids = fld->activeBlockIds();
+  if (out) std::memcpy(out, ids.data(), ids.size() * sizeof(int));
+  *n = ids.size();
+  return 0;
+}
+
+int pfr_set_particles(void* hp, size_t n, const double* pos, const double* vel,
+                      const unsigned char* type, const double* vol) {
+  Particles3DTP& ps = static_cast<Handle*>(hp)->sim.particles;
+  ps = Particles3DTP();
+  for (size_t p = 0; p < n; ++p)
+    ps.add({pos[3 * p], pos[3 * p + 1], pos[3 * p + 2]},
+           {vel[3 * p], vel[3 * p + 1], vel[3 * p + 2]}, type[p], vol[p]);
+  return 0;
+}
+
+size_t pfr_num_particles(void* hp) { return static_cast<Handle*>(hp)->sim.particles.size(); }
+
+int pfr_get_particles(void* hp, double* pos, double* vel, unsigned char* type, double* vol) {
+  const Particles3DTP& ps = static_cast<Handle*>(hp)->sim.particles;
+  for (size_t p = 0; p < ps.size(); ++p) {
+    if (pos) { pos[3 * p] = ps.pos[p].x; pos[3 * p + 1] = ps.pos[p].y; pos[3 * p + 2] = ps.pos[p].z; }
+    if (vel) { vel[3 * p] = ps.vel[p].x; vel[3 * p + 1] = ps.vel[p].y; vel[3 * p + 2] = ps.vel[p].z; }
+    if (type) type[p] = ps.type[p];
+    if (vol) vol[p] = ps.volume[p];
+  }
+  return 0;
+}
+
+int pfr_p2g(void* hp, const double* phase, double Vp) {
+  Handle* h = static_cast<Handle*>(hp);
+  spP2G3D_tp(h->sim.grid, h->sim.particles, phaseOf(phase), Vp);
+  return 0;
+}
+
+int pfr_project(void* hp, const double* phase, double dt, int iters, double tol, double cdiv) {
+  Handle* h = static_cast<Handle*>(hp);
+  spProjectStepVC3D(h->sim.grid, phaseOf(phase), dt, iters, tol, cdiv);
+  return 0;
+}
+
+int pfr_g2p(void* hp, const void* savedp, double aL, double aG) {
+  Handle* h = static_cast<Handle*>(hp);
+  const Handle* s = static_cast<const Handle*>(savedp);
+  spG2P3D_tp(h->sim.grid, h->sim.particles, s->sim.grid, aL, aG);
+  return 0;
+}
+
+// stats8: clamped_liquid, clamped_gas, x_lo, x_hi, y_lo, y_hi, z_lo, z_hi
+int pfr_advect(void* hp, double dt, int order, int* stats8, double* escape_out, size_t* n_escape) {
+  Handle* h = static_cast<Handle*>(hp);
+  ParticleEscapeStats3D st;
+  ParticleEscapeBuffer3D buf;
+  spAdvect3D_tp(h->sim.particles, h->sim.grid, dt, &st, order, escape_out ? &buf : nullptr);
+  if (stats8) {
+    stats8[0] = st.clamped_liquid; stats8[1] = st.clamped_gas;
+    stats8[2] = st.clamped_x_lo; stats8[3] = st.clamped_x_hi;
+    stats8[4] = st.clamped_y_lo; stats8[5] = st.clamped_y_hi;
+    stats8[6] = st.clamped_z_lo; stats8[7] = st.clamped_z_hi;
+  }
+  if (escape_out) {
+    for (size_t r = 0; r < buf.records.size(); ++r) {
+      const EscapedParticleRecord3D& e = buf.records[r];
+      double* o = escape_out + 8 * r;
+      o[0] = e.type; o[1] = e.pos.x; o[2] = e.pos.y; o[3] = e.pos.z;
+      o[4] = e.vel.x; o[5] = e.vel.y; o[6] = e.vel.z; o[7] = e.volume;
+    }
+    if (n_escape) *n_escape = buf.records.size();
+  }
+  return 0;
+}
+
+// cfg: dt, gravity, Vp, alpha_l, alpha_g, cg_iters, cg_tol, advect_order
+int pfr_step(void* hp, const double* phase, const double* cfg) {
+  Handle* h = static_cast<Handle*>(hp);
+  SparseSim3DTP& s = h->sim;
+  s.phase = phaseOf(phase);
+  s.dt = cfg[0];
+  s.gravity = cfg[1];
+  s.Vp = cfg[2];
+  s.alpha_liquid = cfg[3];
+  s.alpha_gas = cfg[4];
+  s.cg_iters = (int)cfg[5];
+  s.cg_tol = cfg[6];
+  s.advection_order = (int)cfg[7];
+  s.step();
+  return 0;
+}
+
+double pfr_calibrate_rho_tilde0(const double* phase, double Vp) {
+  return calibrateRhoTilde0(phaseOf(phase), Vp);
+}
+
+double pfr_phi_from_raw(double raw, const double* phase) {
+  return phiFromRawDensity(raw, phaseOf(phase));
+}
+
+double pfr_beta_from_raw(double raw, const double* phase) {
+  PhaseParams pp = phaseOf(phase);
+  return betaFromPhi(phiFromRawDensity(raw, pp), pp);
+}
+
+}  // extern "C"
