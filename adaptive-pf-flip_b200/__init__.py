@@ -1,0 +1,35 @@
+"""B200 (sm_100a) solver-step backend for the sparse 3D two-phase Phase-Field-FLIP
+step of adaptive-pf-flip.
+
+The Python side mirrors the reference's C++ interface for this path, with the
+same names, argument meanings and order:
+
+    spP2G3D_tp(grid, particles, phase, Vp)                  src/driver/sparse_ops3d_tp.h:9
+    spProjectStepVC3D(grid, phase, dt, cg_iters, cg_tol, divergenceCorrection=0.0)
+                                                            src/driver/sparse_ops3d_tp.h:10
+    spG2P3D_tp(grid, particles, saved, aL, aG)              src/driver/sparse_ops3d_tp.h:12
+    spAdvect3D_tp(particles, grid, dt, stats=None, advectionOrder=2, escapeBuffer=None)
+                                                            src/driver/sparse_ops3d_tp.h:13
+    SparseSim3DTP(nx, ny, nz, dx).step()                    src/driver/sparse_sim3d_tp.cpp:854-884
+    SparseMacGrid3D, Particles3DTP, PhaseParams             src/grid/sparse_mac_grid3d.h,
+                                                            src/particles/particles3d_tp.h,
+                                                            src/physics/phasefield.h
+
+Every compute call goes through libpfgpu.so (include/pfgpu.h); nothing here
+computes on the CPU except scalar phase-field helpers used on results.
+"""
+from ._lib import (PF_MK, PF_MU, PF_MV, PF_MW, PF_P, PF_SOLVER_LEARNED, PF_SOLVER_MIXED, PF_SOLVER_PLAIN, PF_U,
+                   PF_V, PF_W, PfError, load)
+from .sparse import (ParticleEscapeBuffer3D, ParticleEscapeStats3D, Particles3DTP, PhaseParams, SolverConfig,
+                     SparseMacGrid3D, SparseSim3DTP, betaFromPhi, calibrateRhoTilde0, densityFromPhi, etaPhi,
+                     phiFromRawDensity, spAdvect3D_tp, spG2P3D_tp, spP2G3D_tp, spProjectStepVC3D)
+from . import scenes
+
+__all__ = [
+    "PF_U", "PF_V", "PF_W", "PF_MU", "PF_MV", "PF_MW", "PF_P", "PF_MK",
+    "PF_SOLVER_PLAIN", "PF_SOLVER_MIXED", "PF_SOLVER_LEARNED", "PfError", "load",
+    "PhaseParams", "Particles3DTP", "SparseMacGrid3D", "SparseSim3DTP", "SolverConfig",
+    "ParticleEscapeStats3D", "ParticleEscapeBuffer3D",
+    "spP2G3D_tp", "spProjectStepVC3D", "spG2P3D_tp", "spAdvect3D_tp", "calibrateRhoTilde0",
+    "etaPhi", "phiFromRawDensity", "densityFromPhi", "betaFromPhi", "scenes",
+]

@@ -1,0 +1,158 @@
+"""ctypes binding of libpfgpu.so (the C ABI declared in include/pfgpu.h).
+
+The library is the only compute path: if it is missing, or no sm_100 GPU is
+usable, calls raise -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "lib", "libpfgpu.so")
+
+PF_OK = 0
+PF_ERR_INVALID = -1
+PF_ERR_CUDA = -2
+PF_ERR_CAPACITY = -3
+PF_ERR_NONFINITE = -4
+PF_ERR_NO_DEVICE = -5
+ERR_NAMES = {PF_ERR_INVALID: "PF_ERR_INVALID", PF_ERR_CUDA: "PF_ERR_CUDA", PF_ERR_CAPACITY: "PF_ERR_CAPACITY",
+             PF_ERR_NONFINITE: "PF_ERR_NONFINITE", PF_ERR_NO_DEVICE: "PF_ERR_NO_DEVICE"}
+
+PF_U, PF_V, PF_W, PF_MU, PF_MV, PF_MW, PF_P, PF_MK = range(8)
+PF_SOLVER_PLAIN, PF_SOLVER_MIXED, PF_SOLVER_LEARNED = 0, 1, 2
+
+# every entry point include/pfgpu.h declares
+EXPORTS = (
+    "pf_create", "pf_destroy", "pf_last_error", "pf_sync", "pf_stream",
+    "pf_upload_particles", "pf_download_particles", "pf_upload_particles_f64", "pf_download_particles_f64",
+    "pf_num_particles", "pf_grid_set_field", "pf_grid_get_field", "pf_grid_clear_field", "pf_grid_clear_all",
+    "pf_grid_copy", "pf_active_blocks4", "pf_active_cells", "pf_active_tiles", "pf_mark_cells", "pf_p2g",
+    "pf_save_velocity", "pf_apply_gravity", "pf_apply_wall_boundary", "pf_project", "pf_g2p", "pf_advect",
+    "pf_step", "pf_calibrate_rho_tilde0", "pf_set_timing", "pf_get_timing", "pf_launch_count",
+)
+
+STAGES = ("bin", "sort", "splat", "normalize", "mark", "boundary", "project", "pcg", "g2p")
+
+
+class GridDesc(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("dx", C.c_double), ("ox", C.c_double),
+                ("oy", C.c_double), ("oz", C.c_double), ("max_particles", C.c_size_t), ("device", C.c_int)]
+
+
+class Phase(C.Structure):
+    _fields_ = [("rho_l", C.c_double), ("rho_g", C.c_double), ("alpha_phi", C.c_double),
+                ("rho_tilde_0", C.c_double)]
+
+
+class SolveCfg(C.Structure):
+    _fields_ = [("mode", C.c_int), ("max_iter", C.c_int), ("abs_tol", C.c_double), ("rel_tol", C.c_double),
+                ("c_div", C.c_double), ("bf16_storage", C.c_int), ("check_every", C.c_int),
+                ("max_refine", C.c_int), ("inner_rel_tol", C.c_double)]
+
+
+class SolveStats(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("refinements", C.c_int), ("n_cells", C.c_int), ("converged", C.c_int),
+                ("breakdown", C.c_int), ("pin_cell", C.c_longlong), ("res0", C.c_double),
+                ("res_final", C.c_double), ("tol_effective", C.c_double), ("precond_applied", C.c_int),
+                ("precond_rejected", C.c_int), ("solve_ms", C.c_double)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+class ClampStats(C.Structure):
+    _fields_ = [("clamped_liquid", C.c_int), ("clamped_gas", C.c_int), ("x_lo", C.c_int), ("x_hi", C.c_int),
+                ("y_lo", C.c_int), ("y_hi", C.c_int), ("z_lo", C.c_int), ("z_hi", C.c_int)]
+
+    def as_tuple(self):
+        return tuple(getattr(self, n) for n, _ in self._fields_)
+
+
+class StepCfg(C.Structure):
+    _fields_ = [("dt", C.c_double), ("gravity", C.c_double), ("Vp", C.c_double), ("alpha_l", C.c_double),
+                ("alpha_g", C.c_double), ("phase", Phase), ("solve", SolveCfg), ("advect_order", C.c_int)]
+
+
+class StepStats(C.Structure):
+    _fields_ = [("solve", SolveStats), ("clamp", ClampStats), ("active_tiles", C.c_int)]
+
+
+class Timing(C.Structure):
+    _fields_ = [("ms", C.c_double * 9), ("count", C.c_longlong * 9)]
+
+    def as_dict(self):
+        return {name: (self.ms[i], self.count[i]) for i, name in enumerate(STAGES)}
+
+
+class PfError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{ERR_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+_LIB = None
+
+
+def load(path: str = LIB_PATH) -> C.CDLL:
+    """Load libpfgpu.so and declare its signatures (no GPU needed)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(path):
+        raise FileNotFoundError(
+            f"libpfgpu.so not built at {path}: run `python adaptive-pf-flip_b200/build.py` "
+            "(there is no CPU fallback)")
+    lib = C.CDLL(path)
+    vp, sz, i, d = C.c_void_p, C.c_size_t, C.c_int, C.c_double
+    P = C.POINTER
+    sig = {
+        "pf_create": (i, [P(GridDesc), P(vp)]),
+        "pf_destroy": (i, [vp]),
+        "pf_last_error": (C.c_char_p, [vp]),
+        "pf_sync": (i, [vp]),
+        "pf_stream": (vp, [vp]),
+        "pf_upload_particles": (i, [vp, sz, vp, vp, vp, vp]),
+        "pf_download_particles": (i, [vp, vp, vp, vp, vp]),
+        "pf_upload_particles_f64": (i, [vp, sz, vp, vp, vp, vp]),
+        "pf_download_particles_f64": (i, [vp, vp, vp, vp, vp]),
+        "pf_num_particles": (sz, [vp]),
+        "pf_grid_set_field": (i, [vp, i, vp, vp]),
+        "pf_grid_get_field": (i, [vp, i, vp, vp]),
+        "pf_grid_clear_field": (i, [vp, i]),
+        "pf_grid_clear_all": (i, [vp]),
+        "pf_grid_copy": (i, [vp, vp]),
+        "pf_active_blocks4": (i, [vp, i, vp, P(sz)]),
+        "pf_active_cells": (i, [vp, vp, P(sz)]),
+        "pf_active_tiles": (i, [vp]),
+        "pf_mark_cells": (i, [vp]),
+        "pf_p2g": (i, [vp, P(Phase), d]),
+        "pf_save_velocity": (i, [vp]),
+        "pf_apply_gravity": (i, [vp, d, d]),
+        "pf_apply_wall_boundary": (i, [vp]),
+        "pf_project": (i, [vp, P(Phase), d, P(SolveCfg), P(SolveStats)]),
+        "pf_g2p": (i, [vp, vp, d, d]),
+        "pf_advect": (i, [vp, d, i, P(ClampStats), vp, P(sz)]),
+        "pf_step": (i, [vp, P(StepCfg), P(StepStats)]),
+        "pf_calibrate_rho_tilde0": (i, [vp, P(Phase), d, P(d)]),
+        "pf_set_timing": (i, [vp, i]),
+        "pf_get_timing": (i, [vp, P(Timing), i]),
+        "pf_launch_count": (C.c_longlong, [vp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _LIB = lib
+    return lib
+
+
+def check(rc: int, ctx=None, what: str = ""):
+    if rc != PF_OK:
+        msg = what
+        if ctx:
+            m = load().pf_last_error(ctx)
+            if m:
+                msg = f"{what}: {m.decode(errors='replace')}"
+        raise PfError(rc, msg)

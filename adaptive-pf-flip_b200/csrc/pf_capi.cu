@@ -1,0 +1,473 @@
+// pf_capi.cu -- the extern "C" entry points of libpfgpu (include/pfgpu.h):
+// context set-up, particle exchange, grid access and the solver-step calls.
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+#include "pf_ctx.h"
+
+using namespace pf;
+
+namespace {
+
+// AoS (n x 3) -> SoA, FP32 or FP64 input
+template <typename T>
+__global__ void k_unpack3(const T* aos, float* a, float* b, float* c, size_t n) {
+  const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  a[p] = (float)aos[3 * p + 0];
+  b[p] = (float)aos[3 * p + 1];
+  c[p] = (float)aos[3 * p + 2];
+}
+
+template <typename T>
+__global__ void k_pack3(const float* a, const float* b, const float* c, T* aos, size_t n) {
+  const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  aos[3 * p + 0] = (T)a[p];
+  aos[3 * p + 1] = (T)b[p];
+  aos[3 * p + 2] = (T)c[p];
+}
+
+template <typename T>
+__global__ void k_convert(const T* in, float* out, size_t n) {
+  const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < n) out[p] = (float)in[p];
+}
+
+template <typename T>
+__global__ void k_convert_back(const float* in, T* out, size_t n) {
+  const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < n) out[p] = (T)in[p];
+}
+
+void free_all(pf_ctx* c) {
+  auto F = [](void* p) { if (p) cudaFree(p); };
+  F(c->tile_slot); F(c->slot_tile); F(c->d_nslots); F(c->tile_need); F(c->tile_new); F(c->tile_rank);
+  for (int f = 0; f < PF_NFIELDS; ++f) { F(c->fld[f]); F(c->act4[f]); }
+  for (int a = 0; a < PF_NSAVED; ++a) F(c->saved[a]);
+  F(c->d_wall_tiles);
+  F(c->px); F(c->py); F(c->pz); F(c->vx); F(c->vy); F(c->vz); F(c->vol); F(c->type); F(c->staging);
+  F(c->tile_count); F(c->tile_start); F(c->pkey); F(c->prank); F(c->perm);
+  for (int* p : c->scan_levels) F(p);
+  F(c->d_scalar);
+  F(c->x); F(c->r); F(c->p); F(c->Ap); F(c->diag); F(c->cx); F(c->cy); F(c->cz); F(c->kind);
+  F(c->partials); F(c->ctl);
+  F(c->xf); F(c->rf); F(c->pf32); F(c->Apf); F(c->diagf); F(c->cxf); F(c->cyf); F(c->czf); F(c->pbf); F(c->cbf);
+  F(c->b64);
+  F(c->d_clamp); F(c->d_flags); F(c->cell_flags); F(c->esc_buf);
+  for (const auto& t : c->timed) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }
+  for (int s = 0; s < PF_NSTAGES; ++s) if (c->open_ev[s]) cudaEventDestroy(c->open_ev[s]);
+  if (c->h_ctl) cudaFreeHost(c->h_ctl);
+  if (c->h_pinned_ints) cudaFreeHost(c->h_pinned_ints);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->stream) cudaStreamDestroy(c->stream);
+}
+
+int create_impl(pf_ctx* ctx, const pf_grid_desc* d) {
+  PF_CUDA_TRY(cudaSetDevice(d->device));
+  cudaDeviceProp prop;
+  PF_CUDA_TRY(cudaGetDeviceProperties(&prop, d->device));
+  if (prop.major < 10) return set_error(ctx, PF_ERR_NO_DEVICE, "libpfgpu needs an sm_100 device");
+  ctx->device = d->device;
+  ctx->num_sms = prop.multiProcessorCount;
+  PF_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+  PF_CUDA_TRY(cudaEventCreate(&ctx->ev0));
+  PF_CUDA_TRY(cudaEventCreate(&ctx->ev1));
+
+  Geom& g = ctx->g;
+  g.nx = d->nx; g.ny = d->ny; g.nz = d->nz;
+  g.dx = d->dx; g.ox = d->ox; g.oy = d->oy; g.oz = d->oz;
+  g.TX = (d->nx + 1 + 7) / 8; g.TY = (d->ny + 1 + 7) / 8; g.TZ = (d->nz + 1 + 7) / 8;
+  g.ntiles = g.TX * g.TY * g.TZ;
+  const int dims[PF_NFIELDS][3] = {{g.nx + 1, g.ny, g.nz}, {g.nx, g.ny + 1, g.nz}, {g.nx, g.ny, g.nz + 1},
+                                   {g.nx + 1, g.ny, g.nz}, {g.nx, g.ny + 1, g.nz}, {g.nx, g.ny, g.nz + 1},
+                                   {g.nx, g.ny, g.nz},     {g.nx, g.ny, g.nz}};
+  size_t max_field_nodes = 0;
+  for (int f = 0; f < PF_NFIELDS; ++f) {
+    for (int a = 0; a < 3; ++a) {
+      g.fdim[f][a] = dims[f][a];
+      g.bdim[f][a] = (dims[f][a] + 3) / 4;
+    }
+    const size_t nn = (size_t)dims[f][0] * dims[f][1] * dims[f][2];
+    if (nn > max_field_nodes) max_field_nodes = nn;
+    ctx->act4_n[f] = (size_t)g.bdim[f][0] * g.bdim[f][1] * g.bdim[f][2];
+  }
+  const size_t nt = (size_t)g.ntiles;
+  const size_t cells = nt * PF_TV;  // pool capacity = every tile
+  ctx->cells_cap = cells;
+
+  PF_CUDA_TRY(cudaMalloc(&ctx->tile_slot, nt * sizeof(int)));
+  PF_CUDA_TRY(cudaMemset(ctx->tile_slot, 0xff, nt * sizeof(int)));
+  PF_CUDA_TRY(cudaMalloc(&ctx->slot_tile, nt * sizeof(int)));
+  PF_CUDA_TRY(cudaMalloc(&ctx->d_nslots, sizeof(int)));
+  PF_CUDA_TRY(cudaMemset(ctx->d_nslots, 0, sizeof(int)));
+  PF_CUDA_TRY(cudaMalloc(&ctx->tile_need, nt));
+  PF_CUDA_TRY(cudaMemset(ctx->tile_need, 0, nt));
+  PF_CUDA_TRY(cudaMalloc(&ctx->tile_new, nt * sizeof(int)));
+  PF_CUDA_TRY(cudaMalloc(&ctx->tile_rank, nt * sizeof(int)));
+  for (int f = 0; f < PF_NFIELDS; ++f) {
+    PF_CUDA_TRY(cudaMalloc(&ctx->fld[f], cells * sizeof(float)));
+    PF_CUDA_TRY(cudaMemset(ctx->fld[f], 0, cells * sizeof(float)));
+    PF_CUDA_TRY(cudaMalloc(&ctx->act4[f], ctx->act4_n[f]));
+    PF_CUDA_TRY(cudaMemset(ctx->act4[f], 0, ctx->act4_n[f]));
+  }
+  for (int a = 0; a < PF_NSAVED; ++a) {
+    PF_CUDA_TRY(cudaMalloc(&ctx->saved[a], cells * sizeof(float)));
+    PF_CUDA_TRY(cudaMemset(ctx->saved[a], 0, cells * sizeof(float)));
+  }
+  // tiles touched by markCells walls and applyWallBoundary: every tile with
+  // a node at index 0, 1, n-1 or n along some axis
+  {
+    std::vector<int>& wt = ctx->wall_tiles;
+    auto on_wall = [](int t, int n) {
+      const int lo = t * 8, hi = t * 8 + 7;
+      const int cand[4] = {0, 1, n - 1, n};
+      for (int q = 0; q < 4; ++q)
+        if (cand[q] >= lo && cand[q] <= hi && cand[q] >= 0) return true;
+      return false;
+    };
+    for (int tz = 0; tz < g.TZ; ++tz)
+      for (int ty = 0; ty < g.TY; ++ty)
+        for (int tx = 0; tx < g.TX; ++tx)
+          if (on_wall(tx, g.nx) || on_wall(ty, g.ny) || on_wall(tz, g.nz)) wt.push_back(tile_id(g, tx, ty, tz));
+    PF_CUDA_TRY(cudaMalloc(&ctx->d_wall_tiles, (wt.size() + 1) * sizeof(int)));
+    if (!wt.empty())
+      PF_CUDA_TRY(cudaMemcpy(ctx->d_wall_tiles, wt.data(), wt.size() * sizeof(int), cudaMemcpyHostToDevice));
+  }
+
+  // particles
+  const size_t cap = d->max_particles > 0 ? d->max_particles : 1;
+  ctx->cap = cap;
+  float** pa[7] = {&ctx->px, &ctx->py, &ctx->pz, &ctx->vx, &ctx->vy, &ctx->vz, &ctx->vol};
+  for (float** q : pa) PF_CUDA_TRY(cudaMalloc(q, cap * sizeof(float)));
+  PF_CUDA_TRY(cudaMalloc(&ctx->type, cap));
+  const long long ncell = (long long)g.nx * g.ny * g.nz;
+  size_t stg = cap * 3 * sizeof(double);
+  const size_t fld_bytes = max_field_nodes * sizeof(float) + ctx->act4_n[0] + 64;
+  if (fld_bytes > stg) stg = fld_bytes;
+  if ((size_t)ncell * sizeof(int32_t) > stg) stg = (size_t)ncell * sizeof(int32_t);
+  if ((size_t)(4096 + 16) * sizeof(double) > stg) stg = (4096 + 16) * sizeof(double);
+  ctx->staging_bytes = stg;
+  PF_CUDA_TRY(cudaMalloc(&ctx->staging, stg));
+
+  PF_CUDA_TRY(cudaMalloc(&ctx->tile_count, (nt + 1) * sizeof(int)));
+  PF_CUDA_TRY(cudaMalloc(&ctx->tile_start, (nt + 2) * sizeof(int)));
+  PF_CUDA_TRY(cudaMalloc(&ctx->pkey, cap * sizeof(int)));
+  PF_CUDA_TRY(cudaMalloc(&ctx->prank, cap * sizeof(int)));
+  PF_CUDA_TRY(cudaMalloc(&ctx->perm, cap * sizeof(int)));
+  size_t scan_max = nt + 1;
+  if ((size_t)ncell > scan_max) scan_max = (size_t)ncell;
+  if (cap > scan_max) scan_max = cap;
+  int rc = scan_alloc(ctx, scan_max);
+  if (rc) return rc;
+  PF_CUDA_TRY(cudaMalloc(&ctx->d_scalar, 16 * sizeof(int)));
+
+  double** dv[8] = {&ctx->x, &ctx->r, &ctx->p, &ctx->Ap, &ctx->diag, &ctx->cx, &ctx->cy, &ctx->cz};
+  for (double** q : dv) {
+    PF_CUDA_TRY(cudaMalloc(q, cells * sizeof(double)));
+    PF_CUDA_TRY(cudaMemset(*q, 0, cells * sizeof(double)));
+  }
+  PF_CUDA_TRY(cudaMalloc(&ctx->kind, cells));
+  PF_CUDA_TRY(cudaMemset(ctx->kind, 0, cells));
+  PF_CUDA_TRY(cudaMalloc(&ctx->partials, (size_t)kMaxRedBlocks * 3 * sizeof(double)));
+  PF_CUDA_TRY(cudaMalloc(&ctx->ctl, sizeof(SolveCtl)));
+  PF_CUDA_TRY(cudaMemset(ctx->ctl, 0, sizeof(SolveCtl)));
+  PF_CUDA_TRY(cudaMallocHost(&ctx->h_ctl, sizeof(SolveCtl)));
+  PF_CUDA_TRY(cudaMallocHost(&ctx->h_pinned_ints, 64 * sizeof(int)));
+  PF_CUDA_TRY(cudaMalloc(&ctx->d_clamp, 8 * sizeof(int)));
+  PF_CUDA_TRY(cudaMalloc(&ctx->d_flags, 2 * cap * sizeof(int)));
+  size_t cf = 2 * (size_t)ncell + 2;
+  for (int f = 0; f < PF_NFIELDS; ++f)
+    if (2 * ctx->act4_n[f] + 2 > cf) cf = 2 * ctx->act4_n[f] + 2;
+  PF_CUDA_TRY(cudaMalloc(&ctx->cell_flags, cf * sizeof(int32_t)));
+  PF_CUDA_TRY(cudaDeviceSynchronize());
+  return PF_OK;
+}
+
+bool valid_field(int f) { return f >= 0 && f < PF_NFIELDS; }
+
+}  // namespace
+
+extern "C" {
+
+int pf_create(const pf_grid_desc* desc, pf_ctx** out) {
+  if (!desc || !out) return PF_ERR_INVALID;
+  *out = nullptr;
+  if (desc->nx <= 0 || desc->ny <= 0 || desc->nz <= 0 || !(desc->dx > 0.0)) return PF_ERR_INVALID;
+  if ((long long)desc->nx * desc->ny * desc->nz > (1LL << 31) - 1) return PF_ERR_INVALID;
+  if (desc->max_particles > (size_t)0x7fffffff) return PF_ERR_INVALID;
+  pf_ctx* ctx = new (std::nothrow) pf_ctx();
+  if (!ctx) return PF_ERR_INVALID;
+  const int rc = create_impl(ctx, desc);
+  if (rc) {
+    fprintf(stderr, "pf_create: %s\n", ctx->err.c_str());
+    free_all(ctx);
+    delete ctx;
+    return rc;
+  }
+  *out = ctx;
+  return PF_OK;
+}
+
+int pf_destroy(pf_ctx* ctx) {
+  if (!ctx) return PF_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  free_all(ctx);
+  delete ctx;
+  return PF_OK;
+}
+
+const char* pf_last_error(const pf_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int pf_sync(pf_ctx* ctx) {
+  if (!ctx) return PF_ERR_INVALID;
+  PF_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return PF_OK;
+}
+
+void* pf_stream(pf_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+size_t pf_num_particles(const pf_ctx* ctx) { return ctx ? ctx->np : 0; }
+
+int pf_active_tiles(const pf_ctx* ctx) { return ctx ? ctx->nslots : -1; }
+
+static int upload_impl(pf_ctx* ctx, size_t n, const void* pos, const void* vel, const uint8_t* type,
+                       const void* vol, bool f64) {
+  if (!ctx || (n && (!pos || !vel || !type || !vol))) return PF_ERR_INVALID;
+  if (n > ctx->cap) return set_error(ctx, PF_ERR_CAPACITY, "more particles than max_particles");
+  cudaSetDevice(ctx->device);
+  ctx->np = n;
+  if (n == 0) return PF_OK;
+  const size_t es = f64 ? sizeof(double) : sizeof(float);
+  const int nb = nblocks(n, 256);
+  PF_CUDA_TRY(cudaMemcpyAsync(ctx->staging, pos, 3 * n * es, cudaMemcpyDefault, ctx->stream));
+  if (f64) (++ctx->launches), k_unpack3<double><<<nb, 256, 0, ctx->stream>>>((const double*)ctx->staging, ctx->px, ctx->py, ctx->pz, n);
+  else (++ctx->launches), k_unpack3<float><<<nb, 256, 0, ctx->stream>>>((const float*)ctx->staging, ctx->px, ctx->py, ctx->pz, n);
+  PF_CUDA_TRY(cudaMemcpyAsync(ctx->staging, vel, 3 * n * es, cudaMemcpyDefault, ctx->stream));
+  if (f64) (++ctx->launches), k_unpack3<double><<<nb, 256, 0, ctx->stream>>>((const double*)ctx->staging, ctx->vx, ctx->vy, ctx->vz, n);
+  else (++ctx->launches), k_unpack3<float><<<nb, 256, 0, ctx->stream>>>((const float*)ctx->staging, ctx->vx, ctx->vy, ctx->vz, n);
+  PF_CUDA_TRY(cudaMemcpyAsync(ctx->type, type, n, cudaMemcpyDefault, ctx->stream));
+  if (f64) {
+    PF_CUDA_TRY(cudaMemcpyAsync(ctx->staging, vol, n * es, cudaMemcpyDefault, ctx->stream));
+    (++ctx->launches), k_convert<double><<<nb, 256, 0, ctx->stream>>>((const double*)ctx->staging, ctx->vol, n);
+  } else {
+    PF_CUDA_TRY(cudaMemcpyAsync(ctx->vol, vol, n * es, cudaMemcpyDefault, ctx->stream));
+  }
+  PF_CUDA_TRY(cudaGetLastError());
+  return PF_OK;
+}
+
+static int download_impl(pf_ctx* ctx, void* pos, void* vel, uint8_t* type, void* vol, bool f64) {
+  if (!ctx) return PF_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  const size_t n = ctx->np;
+  if (n == 0) return PF_OK;
+  const size_t es = f64 ? sizeof(double) : sizeof(float);
+  const int nb = nblocks(n, 256);
+  if (pos) {
+    if (f64) (++ctx->launches), k_pack3<double><<<nb, 256, 0, ctx->stream>>>(ctx->px, ctx->py, ctx->pz, (double*)ctx->staging, n);
+    else (++ctx->launches), k_pack3<float><<<nb, 256, 0, ctx->stream>>>(ctx->px, ctx->py, ctx->pz, (float*)ctx->staging, n);
+    PF_CUDA_TRY(cudaMemcpyAsync(pos, ctx->staging, 3 * n * es, cudaMemcpyDefault, ctx->stream));
+  }
+  if (vel) {
+    if (f64) (++ctx->launches), k_pack3<double><<<nb, 256, 0, ctx->stream>>>(ctx->vx, ctx->vy, ctx->vz, (double*)ctx->staging, n);
+    else (++ctx->launches), k_pack3<float><<<nb, 256, 0, ctx->stream>>>(ctx->vx, ctx->vy, ctx->vz, (float*)ctx->staging, n);
+    PF_CUDA_TRY(cudaMemcpyAsync(vel, ctx->staging, 3 * n * es, cudaMemcpyDefault, ctx->stream));
+  }
+  if (type) PF_CUDA_TRY(cudaMemcpyAsync(type, ctx->type, n, cudaMemcpyDefault, ctx->stream));
+  if (vol) {
+    if (f64) {
+      (++ctx->launches), k_convert_back<double><<<nb, 256, 0, ctx->stream>>>(ctx->vol, (double*)ctx->staging, n);
+      PF_CUDA_TRY(cudaMemcpyAsync(vol, ctx->staging, n * es, cudaMemcpyDefault, ctx->stream));
+    } else {
+      PF_CUDA_TRY(cudaMemcpyAsync(vol, ctx->vol, n * es, cudaMemcpyDefault, ctx->stream));
+    }
+  }
+  PF_CUDA_TRY(cudaGetLastError());
+  PF_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return PF_OK;
+}
+
+int pf_upload_particles(pf_ctx* ctx, size_t n, const float* pos, const float* vel, const uint8_t* type,
+                        const float* volume) {
+  return upload_impl(ctx, n, pos, vel, type, volume, false);
+}
+int pf_download_particles(pf_ctx* ctx, float* pos, float* vel, uint8_t* type, float* volume) {
+  return download_impl(ctx, pos, vel, type, volume, false);
+}
+int pf_upload_particles_f64(pf_ctx* ctx, size_t n, const double* pos, const double* vel, const uint8_t* type,
+                            const double* volume) {
+  return upload_impl(ctx, n, pos, vel, type, volume, true);
+}
+int pf_download_particles_f64(pf_ctx* ctx, double* pos, double* vel, uint8_t* type, double* volume) {
+  return download_impl(ctx, pos, vel, type, volume, true);
+}
+
+int pf_grid_set_field(pf_ctx* ctx, int field, const float* dense, const uint8_t* act4) {
+  if (!ctx || !valid_field(field) || !dense || !act4) return PF_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  return pf::grid_set_field(ctx, field, dense, act4);
+}
+
+int pf_grid_get_field(pf_ctx* ctx, int field, float* dense, uint8_t* act4) {
+  if (!ctx || !valid_field(field)) return PF_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  return pf::grid_get_field(ctx, field, dense, act4);
+}
+
+int pf_grid_clear_field(pf_ctx* ctx, int field) {
+  if (!ctx || !valid_field(field)) return PF_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  return field_clear(ctx, field);
+}
+
+int pf_grid_clear_all(pf_ctx* ctx) {
+  if (!ctx) return PF_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  return pool_reset(ctx);
+}
+
+int pf_grid_copy(pf_ctx* dst, const pf_ctx* src) {
+  if (!dst || !src) return PF_ERR_INVALID;
+  const Geom &a = dst->g, &b = src->g;
+  if (a.nx != b.nx || a.ny != b.ny || a.nz != b.nz) return set_error(dst, PF_ERR_INVALID, "grid shapes differ");
+  if (dst->device != src->device) return set_error(dst, PF_ERR_INVALID, "contexts on different devices");
+  pf_ctx* ctx = dst;
+  cudaSetDevice(ctx->device);
+  PF_CUDA_TRY(cudaStreamSynchronize(src->stream));
+  int rc = pool_reset(dst);
+  if (rc) return rc;
+  const size_t nt = (size_t)a.ntiles;
+  const size_t cells = (size_t)src->nslots * PF_TV;
+  PF_CUDA_TRY(cudaMemcpyAsync(dst->tile_slot, src->tile_slot, nt * sizeof(int), cudaMemcpyDeviceToDevice, dst->stream));
+  PF_CUDA_TRY(cudaMemcpyAsync(dst->slot_tile, src->slot_tile, nt * sizeof(int), cudaMemcpyDeviceToDevice, dst->stream));
+  PF_CUDA_TRY(cudaMemcpyAsync(dst->d_nslots, src->d_nslots, sizeof(int), cudaMemcpyDeviceToDevice, dst->stream));
+  for (int f = 0; f < PF_NFIELDS; ++f) {
+    if (cells) PF_CUDA_TRY(cudaMemcpyAsync(dst->fld[f], src->fld[f], cells * sizeof(float), cudaMemcpyDeviceToDevice, dst->stream));
+    PF_CUDA_TRY(cudaMemcpyAsync(dst->act4[f], src->act4[f], dst->act4_n[f], cudaMemcpyDeviceToDevice, dst->stream));
+  }
+  for (int s = 0; s < PF_NSAVED; ++s)
+    if (cells) PF_CUDA_TRY(cudaMemcpyAsync(dst->saved[s], src->saved[s], cells * sizeof(float), cudaMemcpyDeviceToDevice, dst->stream));
+  dst->nslots = src->nslots;
+  dst->saved_valid = src->saved_valid;
+  PF_CUDA_TRY(cudaStreamSynchronize(dst->stream));
+  return PF_OK;
+}
+
+int pf_active_blocks4(pf_ctx* ctx, int field, int32_t* ids, size_t* n) {
+  if (!ctx || !valid_field(field) || !n) return PF_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  return pf::active_blocks4(ctx, field, ids, n);
+}
+
+int pf_active_cells(pf_ctx* ctx, int32_t* cells, size_t* n) {
+  if (!ctx || !n) return PF_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  return pf::active_cells(ctx, cells, n);
+}
+
+int pf_mark_cells(pf_ctx* ctx) {
+  if (!ctx) return PF_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  return pf::mark_cells(ctx);
+}
+
+int pf_p2g(pf_ctx* ctx, const pf_phase* phase, double Vp) {
+  if (!ctx || !phase) return PF_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  return pf::p2g(ctx, phase, Vp);
+}
+
+int pf_save_velocity(pf_ctx* ctx) {
+  if (!ctx) return PF_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  return pf::save_velocity(ctx);
+}
+
+int pf_apply_gravity(pf_ctx* ctx, double dt, double gravity) {
+  if (!ctx) return PF_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  return pf::apply_gravity(ctx, dt, gravity);
+}
+
+int pf_apply_wall_boundary(pf_ctx* ctx) {
+  if (!ctx) return PF_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  return pf::apply_walls(ctx);
+}
+
+static int check_solve_cfg(const pf_solve_cfg* cfg) {
+  if (!cfg) return PF_ERR_INVALID;
+  if (cfg->mode < PF_SOLVER_PLAIN || cfg->mode > PF_SOLVER_LEARNED) return PF_ERR_INVALID;
+  if (cfg->max_iter < 0 || !(cfg->abs_tol >= 0.0) || !(cfg->rel_tol >= 0.0)) return PF_ERR_INVALID;
+  return PF_OK;
+}
+
+int pf_project(pf_ctx* ctx, const pf_phase* phase, double dt, const pf_solve_cfg* cfg, pf_solve_stats* stats) {
+  if (!ctx || !phase || check_solve_cfg(cfg)) return PF_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  return pf::project(ctx, phase, dt, cfg, stats);
+}
+
+int pf_g2p(pf_ctx* ctx, const pf_ctx* saved, double alpha_l, double alpha_g) {
+  if (!ctx) return PF_ERR_INVALID;
+  if (saved && saved != ctx) {
+    const Geom &a = ctx->g, &b = saved->g;
+    if (a.nx != b.nx || a.ny != b.ny || a.nz != b.nz || saved->device != ctx->device)
+      return set_error(ctx, PF_ERR_INVALID, "saved grid differs in shape or device");
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(saved->stream);
+  }
+  cudaSetDevice(ctx->device);
+  return pf::g2p(ctx, saved, alpha_l, alpha_g);
+}
+
+int pf_advect(pf_ctx* ctx, double dt, int order, pf_clamp_stats* stats, double* escape, size_t* n_escape) {
+  if (!ctx || (order != 2 && order != 3)) return PF_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  return pf::advect(ctx, dt, order, stats, escape, n_escape);
+}
+
+// SparseSim3DTP::step() order (src/driver/sparse_sim3d_tp.cpp:854-884):
+// markCells, P2G, saved copy, gravity, walls, projection, G2P, advection.
+// The grid holds nothing across steps, so the pool is rebuilt from scratch.
+int pf_step(pf_ctx* ctx, const pf_step_cfg* cfg, pf_step_stats* stats) {
+  if (!ctx || !cfg || check_solve_cfg(&cfg->solve)) return PF_ERR_INVALID;
+  if (cfg->advect_order != 2 && cfg->advect_order != 3) return PF_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  int rc = pool_reset(ctx);
+  if (rc) return rc;
+  rc = pf::mark_cells(ctx);
+  if (rc) return rc;
+  rc = pf::p2g(ctx, &cfg->phase, cfg->Vp);  // normalisation without the fused extras
+  if (rc) return rc;
+  rc = pf::save_velocity(ctx);
+  if (rc) return rc;
+  rc = pf::apply_gravity(ctx, cfg->dt, cfg->gravity);
+  if (rc) return rc;
+  rc = pf::apply_walls(ctx);
+  if (rc) return rc;
+  pf_solve_stats sst{};
+  rc = pf::project(ctx, &cfg->phase, cfg->dt, &cfg->solve, &sst);
+  if (rc) return rc;
+  pf_clamp_stats cst{};
+  rc = pf::g2p_advect(ctx, cfg->alpha_l, cfg->alpha_g, cfg->dt, cfg->advect_order, &cst);
+  if (rc) return rc;
+  if (stats) {
+    stats->solve = sst;
+    stats->clamp = cst;
+    stats->active_tiles = ctx->nslots;
+  }
+  return PF_OK;
+}
+
+int pf_calibrate_rho_tilde0(pf_ctx* ctx, const pf_phase* phase, double Vp, double* out) {
+  if (!ctx || !phase || !out) return PF_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  return pf::calibrate(ctx, phase, Vp, out);
+}
+
+}  // extern "C"

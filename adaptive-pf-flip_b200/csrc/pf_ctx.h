@@ -1,0 +1,146 @@
+// pf_ctx.h -- host-side context of libpfgpu (one grid + one particle set on
+// one device).  Internal: the public ABI is include/pfgpu.h.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "pf_internal.cuh"
+
+struct pf_ctx {
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  pf::Geom g{};
+
+  // ---- tile pool ----
+  int* tile_slot = nullptr;   // [ntiles] dense block-pointer array
+  int* slot_tile = nullptr;   // [ntiles] slot -> tile
+  int nslots = 0;             // host copy of the pool size
+  int* d_nslots = nullptr;    // device copy
+  uint8_t* tile_need = nullptr;  // [ntiles] activation requests
+  int* tile_new = nullptr;       // [ntiles] scratch for slot assignment
+  int* tile_rank = nullptr;      // [ntiles] scratch for slot assignment
+  float* fld[PF_NFIELDS] = {};
+  float* saved[PF_NSAVED] = {};
+  uint8_t* act4[PF_NFIELDS] = {};
+  size_t act4_n[PF_NFIELDS] = {};
+  std::vector<int> wall_tiles;  // tiles written by markCells walls / applyWallBoundary
+  int* d_wall_tiles = nullptr;
+  bool saved_valid = false;
+
+  // ---- particles (SoA FP32) ----
+  size_t cap = 0, np = 0;
+  float *px = nullptr, *py = nullptr, *pz = nullptr;
+  float *vx = nullptr, *vy = nullptr, *vz = nullptr;
+  float* vol = nullptr;
+  uint8_t* type = nullptr;
+  void* staging = nullptr;  // upload/download staging (cap * 3 doubles)
+  size_t staging_bytes = 0;
+
+  // ---- binning ----
+  int* tile_count = nullptr;  // [ntiles+1]
+  int* tile_start = nullptr;  // [ntiles+1]
+  int* pkey = nullptr;        // [cap]
+  int* prank = nullptr;       // [cap]
+  int* perm = nullptr;        // [cap]
+
+  // ---- scan scratch ----
+  std::vector<int*> scan_levels;
+  int* d_scalar = nullptr;  // small device scratch (ints)
+
+  // ---- projection / PCG (pool layout, cap slots * 512) ----
+  size_t cells_cap = 0;
+  double *x = nullptr, *r = nullptr, *p = nullptr, *Ap = nullptr;
+  double *diag = nullptr, *cx = nullptr, *cy = nullptr, *cz = nullptr;
+  double* partials = nullptr;  // [kMaxRedBlocks * 4]
+  uint8_t* kind = nullptr;     // per cell: 0 not an unknown, 1 fluid, 2 pinned
+  pf::SolveCtl* ctl = nullptr;
+  pf::SolveCtl* h_ctl = nullptr;  // pinned mirror
+  // mixed precision
+  float *xf = nullptr, *rf = nullptr, *pf32 = nullptr, *Apf = nullptr;
+  float *diagf = nullptr, *cxf = nullptr, *cyf = nullptr, *czf = nullptr;
+  uint16_t *pbf = nullptr, *cbf = nullptr;  // bf16 direction / coefficients (3 per cell)
+  double* b64 = nullptr;  // right-hand side kept in FP64
+  // learned preconditioner state lives in its own module
+  void* learned = nullptr;
+
+  // ---- misc ----
+  int* d_clamp = nullptr;      // 8 counters
+  int* d_flags = nullptr;      // escape flags / scratch [cap]
+  void* esc_buf = nullptr;     // escape records, grown on demand
+  size_t esc_bytes = 0;
+  int* h_pinned_ints = nullptr;
+  int32_t* cell_flags = nullptr;  // dense nx*ny*nz scratch for compaction
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::string err;
+
+  long long launches = 0;  // kernels launched by this context
+
+  // ---- optional per-stage timing ----
+  bool timing_on = false;
+  cudaEvent_t open_ev[PF_NSTAGES] = {};  // start event of each open stage
+  struct TimedStage { int stage; cudaEvent_t a, b; };
+  std::vector<TimedStage> timed;
+  double acc_ms[PF_NSTAGES] = {};
+  long long acc_n[PF_NSTAGES] = {};
+};
+
+namespace pf {
+
+int set_cuda_error(pf_ctx* ctx, cudaError_t e, const char* what, const char* file, int line);
+int set_error(pf_ctx* ctx, int code, const std::string& msg);
+
+// launch helpers
+inline int nblocks(size_t n, int nt) { return (int)((n + (size_t)nt - 1) / (size_t)nt); }
+
+// scan.cu
+int scan_exclusive(pf_ctx* ctx, const int* in, int* out, int n, int* total_dev);
+int scan_alloc(pf_ctx* ctx, size_t max_n);
+
+// pool.cu
+int pool_reset(pf_ctx* ctx);
+int pool_commit(pf_ctx* ctx);  // give slots to requested tiles, read back nslots
+int field_clear(pf_ctx* ctx, int f);
+int request_wall_tiles(pf_ctx* ctx);
+DevGrid dev_grid(const pf_ctx* ctx);
+int grid_set_field(pf_ctx* ctx, int f, const float* dense, const uint8_t* act4);
+int grid_get_field(pf_ctx* ctx, int f, float* dense, uint8_t* act4);
+int active_blocks4(pf_ctx* ctx, int f, int32_t* ids, size_t* n);
+int active_cells(pf_ctx* ctx, int32_t* cells, size_t* n);
+
+// transfer.cu
+int mark_cells(pf_ctx* ctx);
+int p2g(pf_ctx* ctx, const pf_phase* ph, double Vp);
+int save_velocity(pf_ctx* ctx);
+int apply_gravity(pf_ctx* ctx, double dt, double gravity);
+int apply_walls(pf_ctx* ctx);
+int normalize_save_gravity(pf_ctx* ctx, bool save, bool gravity, double dt, double gval);
+int g2p(pf_ctx* ctx, const pf_ctx* saved, double aL, double aG);
+int advect(pf_ctx* ctx, double dt, int order, pf_clamp_stats* st, double* esc, size_t* nesc);
+int g2p_advect(pf_ctx* ctx, double aL, double aG, double dt, int order, pf_clamp_stats* st);
+int calibrate(pf_ctx* ctx, const pf_phase* ph, double Vp, double* out);
+
+// project.cu
+int project(pf_ctx* ctx, const pf_phase* ph, double dt, const pf_solve_cfg* cfg,
+            pf_solve_stats* st);
+
+constexpr int kMaxRedBlocks = 1184;  // 8 CTAs per SM on 148 SMs
+
+// pf_timing.cu
+using TimedStage = pf_ctx::TimedStage;
+void stage_begin(pf_ctx* ctx, int stage);
+void stage_end(pf_ctx* ctx, int stage);
+int get_timing(pf_ctx* ctx, pf_timing* out, int reset);
+
+struct StageScope {
+  pf_ctx* c;
+  int s;
+  StageScope(pf_ctx* ctx, int stage) : c(ctx), s(stage) { stage_begin(c, s); }
+  ~StageScope() { stage_end(c, s); }
+};
+
+}  // namespace pf

@@ -1,0 +1,194 @@
+// pf_solver.cuh -- building blocks of the pressure solvers: pool-layout
+// vectors, fixed-order two-level reductions that finish in the producing
+// kernel's last CTA, and the scalar recurrences of (flexible) PCG kept in
+// device memory.
+#pragma once
+
+#include <cmath>
+
+#include "pf_ctx.h"
+
+namespace pf {
+
+template <typename V>
+struct PcgVec {
+  V *x, *r, *p, *Ap, *diag, *cx, *cy, *cz;
+  __device__ __forceinline__ void store_p(size_t o, double v) const { p[o] = (V)v; }
+};
+
+struct SolveResult {
+  int iterations = 0, refinements = 0, converged = 0, breakdown = 0, nonfinite = 0;
+  int precond_applied = 0, precond_rejected = 0;
+  double res0 = 0.0, res_final = 0.0, tol = 0.0;
+};
+
+// reduction stages finished by the last CTA
+enum RedStage {
+  kStageInit = 0,    // after assembly: rz, max|r0| -> tolerance, early exit
+  kStagePAp = 1,     // after SpMV: p.Ap -> alpha (breakdown check)
+  kStageUpdate = 2,  // after x/r update: r.z, max|r| -> convergence, beta
+  kStageResid = 3,   // outer refinement: max|b - A x| (FP64)
+  kStageFlex = 4,    // flexible PCG: r.z, r.(z - z_prev)
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Sum of a and max of b over the block, in a fixed order (result in thread 0).
+__device__ __forceinline__ void block_sum_max(double& a, double& b) {
+  __shared__ double sa[32], sb[32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  a = warp_sum(a);
+  b = warp_max(b);
+  __syncthreads();
+  if (lane == 0) { sa[wid] = a; sb[wid] = b; }
+  __syncthreads();
+  if (wid == 0) {
+    a = lane < nw ? sa[lane] : 0.0;
+    b = lane < nw ? sb[lane] : 0.0;
+    a = warp_sum(a);
+    b = warp_max(b);
+  }
+}
+
+__device__ __forceinline__ void finalize_stage(SolveCtl* ctl, int stage, double S, double M, double S2) {
+  switch (stage) {
+    case kStageInit: {
+      ctl->rz = S;
+      ctl->res0 = M;
+      ctl->res = M;
+      double tol = ctl->tol_abs;
+      if (ctl->tol_rel > 0.0 && ctl->tol_rel * M > tol) tol = ctl->tol_rel * M;
+      ctl->tol = tol;
+      ctl->it = 0;
+      if (!isfinite(S) || !isfinite(M)) ctl->done = 4;
+      else if (!(M >= tol)) ctl->done = 1;
+      else ctl->done = 0;
+      break;
+    }
+    case kStagePAp: {
+      ctl->pAp = S;
+      if (!isfinite(S)) ctl->done = 4;
+      else if (fabs(S) < 1e-30) ctl->done = 2;
+      else ctl->alpha = ctl->rz / S;
+      break;
+    }
+    case kStageUpdate: {
+      ctl->it += 1;
+      ctl->res = M;
+      if (!isfinite(M) || !isfinite(S)) ctl->done = 4;
+      else if (M < ctl->tol) ctl->done = 1;
+      else if (ctl->it >= ctl->max_iter) ctl->done = 3;
+      else {
+        ctl->beta = S / ctl->rz;
+        ctl->rz = S;
+      }
+      break;
+    }
+    case kStageResid: {
+      ctl->res = M;
+      if (!isfinite(M)) ctl->done = 4;
+      break;
+    }
+    case kStageFlex: {
+      ctl->it += 1;
+      ctl->res = M;
+      if (!isfinite(M) || !isfinite(S) || !isfinite(S2)) ctl->done = 4;
+      else if (M < ctl->tol) ctl->done = 1;
+      else if (ctl->it >= ctl->max_iter) ctl->done = 3;
+      else {
+        double b = ctl->rz != 0.0 ? S2 / ctl->rz : 0.0;  // Polak-Ribiere
+        if (!isfinite(b) || b < 0.0) b = 0.0;
+        ctl->beta = b;
+        ctl->rz = S;
+      }
+      break;
+    }
+  }
+}
+
+// Per-CTA partial (sum a, max b, sum c) -> partials; the last CTA reduces all
+// partials in index order and finishes the stage.  Every CTA of the grid must
+// call this exactly once.
+__device__ __forceinline__ void block_reduce_3(double a, double b, double c, double* partials, SolveCtl* ctl,
+                                               int stage) {
+  __shared__ bool am_last;
+  double c2 = c, z0 = 0.0;
+  block_sum_max(a, b);
+  block_sum_max(c2, z0);
+  if (threadIdx.x == 0) {
+    partials[3 * blockIdx.x + 0] = a;
+    partials[3 * blockIdx.x + 1] = b;
+    partials[3 * blockIdx.x + 2] = c2;
+    __threadfence();
+    const unsigned t = atomicAdd(&ctl->counter, 1u);
+    am_last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!am_last) return;
+  __threadfence();
+  double S = 0.0, M = 0.0, S2 = 0.0;
+  for (int q = threadIdx.x; q < (int)gridDim.x; q += blockDim.x) {
+    S += __ldcg(&partials[3 * q + 0]);
+    M = fmax(M, __ldcg(&partials[3 * q + 1]));
+    S2 += __ldcg(&partials[3 * q + 2]);
+  }
+  block_sum_max(S, M);
+  double z1 = 0.0;
+  block_sum_max(S2, z1);
+  if (threadIdx.x == 0) {
+    finalize_stage(ctl, stage, S, M, S2);
+    ctl->counter = 0;
+  }
+}
+
+__device__ __forceinline__ void block_reduce_2(double a, double b, double* partials, SolveCtl* ctl, int stage,
+                                               double /*unused*/ = 0.0) {
+  block_reduce_3(a, b, 0.0, partials, ctl, stage);
+}
+
+// Neighbour slots of the tile of slot s, order +x -x +y -y +z -z (-1 if none).
+__device__ __forceinline__ void neighbor_slots(const DevGrid& G, int s, int* nbs) {
+  if (threadIdx.x < 6) {
+    const int t = G.slot_tile[s];
+    int tx = t % G.g.TX, q = t / G.g.TX, ty = q % G.g.TY, tz = q / G.g.TY;
+    const int d = threadIdx.x;
+    tx += d == 0 ? 1 : d == 1 ? -1 : 0;
+    ty += d == 2 ? 1 : d == 3 ? -1 : 0;
+    tz += d == 4 ? 1 : d == 5 ? -1 : 0;
+    int v = -1;
+    if (tx >= 0 && ty >= 0 && tz >= 0 && tx < G.g.TX && ty < G.g.TY && tz < G.g.TZ)
+      v = G.tile_slot[tile_id(G.g, tx, ty, tz)];
+    nbs[d] = v;
+  }
+}
+
+// Offsets of the six neighbours of local cell l within slot s: element index
+// into a pool-layout array, or -1 when the neighbour tile is not pooled.
+__device__ __forceinline__ void neighbor_offsets(int s, int l, const int* nbs, long long* off) {
+  const int lx = l & 7, ly = (l >> 3) & 7, lz = l >> 6;
+  const long long base = (long long)s * PF_TV;
+  off[0] = lx < 7 ? base + l + 1 : (nbs[0] >= 0 ? (long long)nbs[0] * PF_TV + (l & ~7) : -1);
+  off[1] = lx > 0 ? base + l - 1 : (nbs[1] >= 0 ? (long long)nbs[1] * PF_TV + (l | 7) : -1);
+  off[2] = ly < 7 ? base + l + 8 : (nbs[2] >= 0 ? (long long)nbs[2] * PF_TV + (l & ~56) : -1);
+  off[3] = ly > 0 ? base + l - 8 : (nbs[3] >= 0 ? (long long)nbs[3] * PF_TV + (l | 56) : -1);
+  off[4] = lz < 7 ? base + l + 64 : (nbs[4] >= 0 ? (long long)nbs[4] * PF_TV + (l & ~448) : -1);
+  off[5] = lz > 0 ? base + l - 64 : (nbs[5] >= 0 ? (long long)nbs[5] * PF_TV + (l | 448) : -1);
+}
+
+// solver drivers (pf_pcg.cu)
+int pcg_plain(pf_ctx* ctx, int nslots, int nred, const uint8_t* kind, PcgVec<double> vec, double scale,
+              const pf_solve_cfg* cfg, SolveResult* res);
+int solve_mixed(pf_ctx* ctx, int nslots, int nred, const uint8_t* kind, double scale, const pf_solve_cfg* cfg,
+                const void* phase_consts, SolveResult* res);
+int ensure_solver_buffers(pf_ctx* ctx, int mode);
+
+}  // namespace pf

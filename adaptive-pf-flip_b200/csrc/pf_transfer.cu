@@ -1,0 +1,773 @@
+// pf_transfer.cu -- particle<->grid transfer kernels for sm_100a.
+//
+//   markCells        src/driver/sparse_sim3d_tp.cpp:22-50
+//   spP2G3D_tp       src/driver/sparse_ops3d_tp.cpp:23-75, 95-153
+//   applyGravity     src/driver/sparse_sim3d_tp.cpp:52-70
+//   applyWallBoundary src/driver/sparse_sim3d_tp.cpp:72-97
+//   spG2P3D_tp       src/driver/sparse_ops3d_tp.cpp:155-172 (+ sampleField,
+//                    src/driver/sparse_ops3d_common.h:30-63)
+//   spAdvect3D_tp    src/driver/sparse_ops3d_tp.cpp:176-232
+//   calibrateRhoTilde0 src/transfer/transfer3d_tp.cpp:29-36
+//
+// P2G design (replaces the reference's 8 colour threads that each rescan every
+// particle): particles are binned by the 8^3 tile of their cell with
+// warp-aggregated atomics; one CTA per tile splats its particles into a
+// shared-memory box of 12^3 nodes per face field (the tile plus the kernel's
+// -2..+3 halo), then adds the box into the pooled field once.  Block
+// activation is decided in FP64 with the reference's exact operation order,
+// so the active 4^3 set is bit-identical; weights and accumulation are FP32.
+#include <cmath>
+
+#include "pf_ctx.h"
+
+namespace pf {
+namespace {
+
+constexpr double kR2 = 2.25;  // KR*KR with KR = 1.5 (sparse_ops3d_tp.cpp:21)
+constexpr int kBox = 12;      // shared box edge: tile (8) + halo 2 below, 2 above
+constexpr int kBox3 = kBox * kBox * kBox;
+
+// grid coordinate (pos - o)/dx in the reference's double arithmetic
+__device__ __forceinline__ double grid_coord(float p, double o, double dx) {
+  return __ddiv_rn(__dsub_rn((double)p, o), dx);
+}
+
+// ---------------------------------------------------------------------------
+// exact FP64 activation of the 4^3 blocks a particle's kernel window touches
+// (preactivateKernel, sparse_ops3d_tp.cpp:23-40).  Along each axis only nodes
+// i0-1..i0+2 can have |d| < 1.5; per 4-node block the closest node gives the
+// smallest rounded d^2, and rounding is monotone, so testing the per-axis
+// minima decides "some node of this block has w > 0" exactly.
+// ---------------------------------------------------------------------------
+__device__ void activate_window(const DevGrid& G, int fv, double c0, double c1, double c2,
+                                uint8_t* need) {
+  const double c[3] = {c0, c1, c2};
+  int nb[3];
+  int blk[3][2];
+  double m2[3][2];
+#pragma unroll
+  for (int ax = 0; ax < 3; ++ax) {
+    const int dim = G.g.fdim[fv][ax];
+    const int i0 = (int)floor(c[ax]);
+    nb[ax] = 0;
+#pragma unroll
+    for (int o = -1; o <= 2; ++o) {
+      const int i = i0 + o;
+      if (i < 0 || i >= dim) continue;
+      const double d = __dsub_rn(c[ax], (double)i);
+      const double dd = __dmul_rn(d, d);
+      const int b = i >> 2;
+      if (nb[ax] > 0 && blk[ax][nb[ax] - 1] == b) {
+        if (dd < m2[ax][nb[ax] - 1]) m2[ax][nb[ax] - 1] = dd;
+      } else {
+        blk[ax][nb[ax]] = b;
+        m2[ax][nb[ax]] = dd;
+        ++nb[ax];
+      }
+    }
+  }
+  const int fm = fv + 3;
+  for (int z = 0; z < nb[2]; ++z)
+    for (int y = 0; y < nb[1]; ++y)
+      for (int x = 0; x < nb[0]; ++x) {
+        const double d2 = __dadd_rn(__dadd_rn(m2[0][x], m2[1][y]), m2[2][z]);
+        if (!(__ddiv_rn(d2, kR2) < 1.0)) continue;
+        const int bx = blk[0][x], by = blk[1][y], bz = blk[2][z];
+        const int bi = bx + G.g.bdim[fv][0] * (by + G.g.bdim[fv][1] * bz);
+        if (!G.act4[fv][bi]) G.act4[fv][bi] = 1;
+        if (!G.act4[fm][bi]) G.act4[fm][bi] = 1;
+        uint8_t* nd = &need[tile_id(G.g, bx >> 1, by >> 1, bz >> 1)];
+        if (!*nd) *nd = 1;
+      }
+}
+
+// One pass over the particles: tile key + warp-aggregated rank (binning),
+// the tile of the particle's cell (pooled for markCells), and the exact
+// activation of u/v/w and their mass fields.
+__global__ void __launch_bounds__(256) k_bin_activate(DevGrid G, const float* __restrict__ px,
+                                                      const float* __restrict__ py,
+                                                      const float* __restrict__ pz, int n,
+                                                      int* tile_count, int* pkey, int* prank,
+                                                      uint8_t* need, int do_bin, int do_act) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned active = __ballot_sync(0xffffffffu, p < n);
+  if (p >= n) return;
+  const double gx = grid_coord(px[p], G.g.ox, G.g.dx);
+  const double gy = grid_coord(py[p], G.g.oy, G.g.dx);
+  const double gz = grid_coord(pz[p], G.g.oz, G.g.dx);
+  int ci = (int)floor(gx), cj = (int)floor(gy), ck = (int)floor(gz);
+  ci = min(max(ci, 0), G.g.nx - 1);
+  cj = min(max(cj, 0), G.g.ny - 1);
+  ck = min(max(ck, 0), G.g.nz - 1);
+  const int t = tile_id(G.g, ci >> 3, cj >> 3, ck >> 3);
+  if (do_bin) {
+    const int r = warp_agg_inc(tile_count, t, active);
+    pkey[p] = t;
+    prank[p] = r;
+  }
+  if (!need[t]) need[t] = 1;
+  if (do_act) {
+    activate_window(G, PF_U, gx, __dsub_rn(gy, 0.5), __dsub_rn(gz, 0.5), need);
+    activate_window(G, PF_V, __dsub_rn(gx, 0.5), gy, __dsub_rn(gz, 0.5), need);
+    activate_window(G, PF_W, __dsub_rn(gx, 0.5), __dsub_rn(gy, 0.5), gz, need);
+  }
+}
+
+__global__ void k_bin_scatter(const int* __restrict__ pkey, const int* __restrict__ prank,
+                              const int* __restrict__ tile_start, int* perm, int n) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < n) perm[tile_start[pkey[p]] + prank[p]] = p;
+}
+
+// ---------------------------------------------------------------------------
+// markCells (sparse_sim3d_tp.cpp:22-50)
+// ---------------------------------------------------------------------------
+__global__ void k_mark_walls(DevGrid G) {
+  const int nx = G.g.nx, ny = G.g.ny, nz = G.g.nz;
+  const long long nxf = 2LL * ny * nz, nyf = 2LL * nx * nz, nzf = 2LL * nx * ny;
+  const long long total = nxf + nyf + nzf;
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < total;
+       q += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    if (q < nxf) {
+      const long long r = q >> 1;
+      j = (int)(r % ny); k = (int)(r / ny); i = (q & 1) ? nx - 1 : 0;
+    } else if (q < nxf + nyf) {
+      const long long s = q - nxf, r = s >> 1;
+      i = (int)(r % nx); k = (int)(r / nx); j = (s & 1) ? ny - 1 : 0;
+    } else {
+      const long long s = q - nxf - nyf, r = s >> 1;
+      i = (int)(r % nx); j = (int)(r / nx); k = (s & 1) ? nz - 1 : 0;
+    }
+    const int sl = slot_of(G, i, j, k);
+    if (sl < 0) continue;  // unreachable: wall tiles are pooled first
+    G.fld[PF_MK][(size_t)sl * PF_TV + local_id(i, j, k)] = 2.0f;
+    activate4(G, PF_MK, i, j, k);
+  }
+}
+
+__global__ void k_mark_particles(DevGrid G, const float* __restrict__ px, const float* __restrict__ py,
+                                 const float* __restrict__ pz, int n) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  // (int) truncation, as the reference's cast
+  const int i = __double2int_rz(grid_coord(px[p], G.g.ox, G.g.dx));
+  const int j = __double2int_rz(grid_coord(py[p], G.g.oy, G.g.dx));
+  const int k = __double2int_rz(grid_coord(pz[p], G.g.oz, G.g.dx));
+  if (!in_cells(G.g, i, j, k)) return;
+  const int sl = slot_of(G, i, j, k);
+  if (sl < 0) return;  // unreachable: particle cell tiles are pooled first
+  float* m = &G.fld[PF_MK][(size_t)sl * PF_TV + local_id(i, j, k)];
+  if ((int)(*m + 0.5f) != 2) {
+    *m = 1.0f;
+    activate4(G, PF_MK, i, j, k);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// P2G splat: one CTA per tile holding particles
+// ---------------------------------------------------------------------------
+struct AxisW {
+  int base;   // first candidate node
+  float a[3]; // d^2 / r^2 of the three candidates (>= 1 when out of the lattice)
+};
+
+__device__ __forceinline__ AxisW axis_weights(double c, int dim) {
+  AxisW w;
+  const int i0 = (int)floor(c);
+  const float fr = (float)(c - (double)i0);
+  w.base = fr < 0.5f ? i0 - 1 : i0;
+#pragma unroll
+  for (int m = 0; m < 3; ++m) {
+    const int i = w.base + m;
+    const float d = fr + (float)(i0 - i);
+    w.a[m] = (i >= 0 && i < dim) ? d * d * (1.0f / 2.25f) : 2.0f;
+  }
+  return w;
+}
+
+__device__ __forceinline__ float cubic(float s) {
+  const float t = 1.0f - s;
+  return t > 0.0f ? t * t * t : 0.0f;
+}
+
+__global__ void __launch_bounds__(256) k_splat(DevGrid G, const int* __restrict__ tile_start,
+                                               const int* __restrict__ perm,
+                                               const float* __restrict__ px, const float* __restrict__ py,
+                                               const float* __restrict__ pz, const float* __restrict__ vx,
+                                               const float* __restrict__ vy, const float* __restrict__ vz,
+                                               const uint8_t* __restrict__ type,
+                                               const float* __restrict__ vol, double rho_l, double rho_g,
+                                               double Vp) {
+  extern __shared__ float sm[];  // [3 axes][mom, mass][kBox3]
+  const int t = blockIdx.x;
+  const int beg = tile_start[t], end = tile_start[t + 1];
+  if (beg >= end) return;
+  for (int e = threadIdx.x; e < 6 * kBox3; e += blockDim.x) sm[e] = 0.0f;
+  __syncthreads();
+  const int tx = t % G.g.TX, tq = t / G.g.TX, ty = tq % G.g.TY, tz = tq / G.g.TY;
+  const int o0 = tx * 8 - 2, o1 = ty * 8 - 2, o2 = tz * 8 - 2;
+
+  for (int q = beg + threadIdx.x; q < end; q += blockDim.x) {
+    const int p = perm[q];
+    const double gx = grid_coord(px[p], G.g.ox, G.g.dx);
+    const double gy = grid_coord(py[p], G.g.oy, G.g.dx);
+    const double gz = grid_coord(pz[p], G.g.oz, G.g.dx);
+    const float mp = (float)((type[p] == 0 ? rho_l : rho_g) * Vp * (double)vol[p]);
+    const float vel[3] = {vx[p], vy[p], vz[p]};
+#pragma unroll 1
+    for (int a = 0; a < 3; ++a) {
+      const int fv = PF_U + a;
+      const AxisW wx = axis_weights(a == 0 ? gx : gx - 0.5, G.g.fdim[fv][0]);
+      const AxisW wy = axis_weights(a == 1 ? gy : gy - 0.5, G.g.fdim[fv][1]);
+      const AxisW wz = axis_weights(a == 2 ? gz : gz - 0.5, G.g.fdim[fv][2]);
+      float w[27];
+      float wsum = 0.0f;
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+#pragma unroll
+          for (int e = 0; e < 3; ++e) {
+            const float v = cubic(wx.a[e] + wy.a[b] + wz.a[c]);
+            w[(c * 3 + b) * 3 + e] = v;
+            wsum += v;
+          }
+      if (!(wsum > 0.0f)) continue;
+      const float inv = 1.0f / wsum;
+      const float mom = mp * vel[a];
+      float* smom = sm + (2 * a) * kBox3;
+      float* smas = sm + (2 * a + 1) * kBox3;
+      const int lx = wx.base - o0, ly = wy.base - o1, lz = wz.base - o2;
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+#pragma unroll
+          for (int e = 0; e < 3; ++e) {
+            const float wn = w[(c * 3 + b) * 3 + e] * inv;
+            if (wn > 0.0f) {
+              const int X = lx + e, Y = ly + b, Z = lz + c;
+              if ((unsigned)X < (unsigned)kBox && (unsigned)Y < (unsigned)kBox && (unsigned)Z < (unsigned)kBox) {
+                const int si = X + kBox * (Y + kBox * Z);
+                atomicAdd(&smom[si], wn * mom);
+                atomicAdd(&smas[si], wn * mp);
+              }
+            }
+          }
+    }
+  }
+  __syncthreads();
+  // add the box into the pooled fields (neighbouring tiles overlap in halos)
+  for (int e = threadIdx.x; e < 3 * kBox3; e += blockDim.x) {
+    const int a = e / kBox3, si = e - a * kBox3;
+    const float mom = sm[(2 * a) * kBox3 + si], mas = sm[(2 * a + 1) * kBox3 + si];
+    if (mom == 0.0f && mas == 0.0f) continue;
+    const int X = si % kBox, Y = (si / kBox) % kBox, Z = si / (kBox * kBox);
+    const int i = o0 + X, j = o1 + Y, k = o2 + Z;
+    if (!in_field(G.g, PF_U + a, i, j, k)) continue;
+    // FP32 weights may be (negligibly) nonzero where the exact FP64 test left
+    // the block inactive; such contributions are dropped so inactive blocks
+    // stay zero.
+    if (!G.act4[PF_MU + a][act4_index(G.g, PF_MU + a, i, j, k)]) continue;
+    const int sl = slot_of(G, i, j, k);
+    if (sl < 0) continue;
+    const size_t o = (size_t)sl * PF_TV + local_id(i, j, k);
+    atomicAdd(&G.fld[PF_U + a][o], mom);
+    atomicAdd(&G.fld[PF_MU + a][o], mas);
+  }
+}
+
+// normalisation u = P/m where m > 0 (sparse_ops3d_tp.cpp:126-152), with the
+// optional saved copy (step(): `saved = grid`) and gravity on v where mv > 0
+// (applyGravity) fused in.
+__global__ void k_normalize(DevGrid G, int nslots, int save, int gravity, float dv) {
+  for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
+    const size_t o = (size_t)s * PF_TV + threadIdx.x;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const float m = G.fld[PF_MU + a][o];
+      float u = G.fld[PF_U + a][o];
+      if (m > 0.0f) u = u / m;
+      if (save) G.saved[a][o] = u;
+      if (a == 1 && gravity && m > 0.0f) u = u + dv;
+      G.fld[PF_U + a][o] = u;
+    }
+  }
+}
+
+__global__ void k_save(DevGrid G, int nslots) {
+  for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
+    const size_t o = (size_t)s * PF_TV + threadIdx.x;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) G.saved[a][o] = G.fld[PF_U + a][o];
+  }
+}
+
+__global__ void k_gravity(DevGrid G, int nslots, float dv) {
+  for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
+    const size_t o = (size_t)s * PF_TV + threadIdx.x;
+    if (G.fld[PF_MV][o] > 0.0f) {
+      G.fld[PF_V][o] = G.fld[PF_V][o] + dv;
+      const int t = G.slot_tile[s];
+      const int tx = t % G.g.TX, q = t / G.g.TX, ty = q % G.g.TY, tz = q / G.g.TY;
+      const int l = threadIdx.x;
+      activate4(G, PF_V, tx * 8 + (l & 7), ty * 8 + ((l >> 3) & 7), tz * 8 + (l >> 6));
+    }
+  }
+}
+
+// applyWallBoundary: zero two face layers at every wall
+__global__ void k_walls(DevGrid G) {
+  const int nx = G.g.nx, ny = G.g.ny, nz = G.g.nz;
+  const long long nu = 4LL * ny * nz, nv = 4LL * nx * nz, nw = 4LL * nx * ny;
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < nu + nv + nw;
+       q += (long long)gridDim.x * blockDim.x) {
+    int f, i, j, k;
+    if (q < nu) {
+      const int s = (int)(q & 3); const long long r = q >> 2;
+      j = (int)(r % ny); k = (int)(r / ny);
+      i = s == 0 ? 0 : s == 1 ? 1 : s == 2 ? nx - 1 : nx;
+      f = PF_U;
+    } else if (q < nu + nv) {
+      const long long qq = q - nu; const int s = (int)(qq & 3); const long long r = qq >> 2;
+      i = (int)(r % nx); k = (int)(r / nx);
+      j = s == 0 ? 0 : s == 1 ? 1 : s == 2 ? ny - 1 : ny;
+      f = PF_V;
+    } else {
+      const long long qq = q - nu - nv; const int s = (int)(qq & 3); const long long r = qq >> 2;
+      i = (int)(r % nx); j = (int)(r / nx);
+      k = s == 0 ? 0 : s == 1 ? 1 : s == 2 ? nz - 1 : nz;
+      f = PF_W;
+    }
+    if (!in_field(G.g, f, i, j, k)) continue;
+    const int sl = slot_of(G, i, j, k);
+    if (sl < 0) continue;  // unreachable: wall tiles are pooled first
+    G.fld[f][(size_t)sl * PF_TV + local_id(i, j, k)] = 0.0f;
+    activate4(G, f, i, j, k);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// G2P / advection
+// ---------------------------------------------------------------------------
+
+// Clamped trilinear sample of face field `a` at grid coordinate (cx,cy,cz),
+// current and (optionally) saved values from the same nodes.
+template <bool kSaved>
+__device__ __forceinline__ void sample2(const DevGrid& G, int a, double cx, double cy, double cz,
+                                        float& cur, float& old) {
+  const int fv = PF_U + a;
+  const int X = G.g.fdim[fv][0], Y = G.g.fdim[fv][1], Z = G.g.fdim[fv][2];
+  const int i0 = (int)floor(cx), j0 = (int)floor(cy), k0 = (int)floor(cz);
+  const float fx = (float)(cx - i0), fy = (float)(cy - j0), fz = (float)(cz - k0);
+  const float wx[2] = {1.0f - fx, fx}, wy[2] = {1.0f - fy, fy}, wz[2] = {1.0f - fz, fz};
+  float s = 0.0f, so = 0.0f;
+#pragma unroll
+  for (int dk = 0; dk < 2; ++dk)
+#pragma unroll
+    for (int dj = 0; dj < 2; ++dj)
+#pragma unroll
+      for (int di = 0; di < 2; ++di) {
+        const int i = min(max(i0 + di, 0), X - 1);
+        const int j = min(max(j0 + dj, 0), Y - 1);
+        const int k = min(max(k0 + dk, 0), Z - 1);
+        const int sl = slot_of(G, i, j, k);
+        const float w = wx[di] * wy[dj] * wz[dk];
+        if (sl >= 0) {
+          const size_t o = (size_t)sl * PF_TV + local_id(i, j, k);
+          s += w * G.fld[fv][o];
+          if (kSaved) so += w * G.saved[a][o];
+        }
+      }
+  cur = s;
+  old = so;
+}
+
+__device__ __forceinline__ float sample1(const DevGrid& G, int a, double cx, double cy, double cz) {
+  float c, o;
+  sample2<false>(G, a, cx, cy, cz, c, o);
+  return c;
+}
+
+__device__ __forceinline__ void velocity_at(const DevGrid& G, double x, double y, double z, double out[3]) {
+  const double gx = __ddiv_rn(__dsub_rn(x, G.g.ox), G.g.dx);
+  const double gy = __ddiv_rn(__dsub_rn(y, G.g.oy), G.g.dx);
+  const double gz = __ddiv_rn(__dsub_rn(z, G.g.oz), G.g.dx);
+  out[0] = sample1(G, 0, gx, gy - 0.5, gz - 0.5);
+  out[1] = sample1(G, 1, gx - 0.5, gy, gz - 0.5);
+  out[2] = sample1(G, 2, gx - 0.5, gy - 0.5, gz);
+}
+
+struct ParticlePtrs {
+  float *px, *py, *pz, *vx, *vy, *vz, *vol;
+  const uint8_t* type;
+};
+
+// FLIP/PIC blend; saved grid either this pool's saved copy (S == nullptr
+// semantics via kExternal=false) or another context's u/v/w.
+template <bool kExternal>
+__global__ void __launch_bounds__(256) k_g2p(DevGrid G, DevGrid S, ParticlePtrs P, int n, double aL, double aG) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const double gx = grid_coord(P.px[p], G.g.ox, G.g.dx);
+  const double gy = grid_coord(P.py[p], G.g.oy, G.g.dx);
+  const double gz = grid_coord(P.pz[p], G.g.oz, G.g.dx);
+  const double c[3][3] = {{gx, gy - 0.5, gz - 0.5}, {gx - 0.5, gy, gz - 0.5}, {gx - 0.5, gy - 0.5, gz}};
+  const float a = P.type[p] == 0 ? (float)aL : (float)aG;
+  float* vp[3] = {P.vx, P.vy, P.vz};
+#pragma unroll
+  for (int ax = 0; ax < 3; ++ax) {
+    float cur, old;
+    if (kExternal) {
+      cur = sample1(G, ax, c[ax][0], c[ax][1], c[ax][2]);
+      old = sample1(S, ax, c[ax][0], c[ax][1], c[ax][2]);
+    } else {
+      sample2<true>(G, ax, c[ax][0], c[ax][1], c[ax][2], cur, old);
+    }
+    const float v = vp[ax][p];
+    vp[ax][p] = (v + (cur - old)) * a + cur * (1.0f - a);
+  }
+}
+
+__device__ __forceinline__ void warp_count(int* counters, int idx, bool flag) {
+  const unsigned m = __ballot_sync(__activemask(), flag);
+  if (m && (threadIdx.x & 31) == (__ffs(__activemask()) - 1)) atomicAdd(&counters[idx], __popc(m));
+}
+
+// RK2 (midpoint) or RK3 advection, boundary clamp, clamp statistics; with
+// fuse_g2p the FLIP/PIC update uses the first stage's samples.
+__global__ void __launch_bounds__(256) k_advect(DevGrid G, ParticlePtrs P, int n, double dt, int order,
+                                                int* counters, int* esc_flags, int fuse_g2p, double aL,
+                                                double aG) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = p < n;
+  bool low[3] = {false, false, false}, high[3] = {false, false, false};
+  int ty = -1;
+  if (live) {
+    const double x0[3] = {(double)P.px[p], (double)P.py[p], (double)P.pz[p]};
+    double k1[3], k2[3], nx[3];
+    if (fuse_g2p) {
+      const double gx = __ddiv_rn(__dsub_rn(x0[0], G.g.ox), G.g.dx);
+      const double gy = __ddiv_rn(__dsub_rn(x0[1], G.g.oy), G.g.dx);
+      const double gz = __ddiv_rn(__dsub_rn(x0[2], G.g.oz), G.g.dx);
+      const double c[3][3] = {{gx, gy - 0.5, gz - 0.5}, {gx - 0.5, gy, gz - 0.5}, {gx - 0.5, gy - 0.5, gz}};
+      const float a = P.type[p] == 0 ? (float)aL : (float)aG;
+      float* vp[3] = {P.vx, P.vy, P.vz};
+#pragma unroll
+      for (int ax = 0; ax < 3; ++ax) {
+        float cur, old;
+        sample2<true>(G, ax, c[ax][0], c[ax][1], c[ax][2], cur, old);
+        k1[ax] = cur;
+        const float v = vp[ax][p];
+        vp[ax][p] = (v + (cur - old)) * a + cur * (1.0f - a);
+      }
+    } else {
+      velocity_at(G, x0[0], x0[1], x0[2], k1);
+    }
+    if (order == 3) {
+      double m1[3], m2[3], k3[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) m1[c] = x0[c] + k1[c] * (0.5 * dt);
+      velocity_at(G, m1[0], m1[1], m1[2], k2);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) m2[c] = (x0[c] - k1[c] * dt) + k2[c] * (2.0 * dt);
+      velocity_at(G, m2[0], m2[1], m2[2], k3);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) nx[c] = x0[c] + ((k1[c] + k2[c] * 4.0) + k3[c]) * (dt / 6.0);
+    } else {
+      double mid[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) mid[c] = x0[c] + k1[c] * (0.5 * dt);
+      velocity_at(G, mid[0], mid[1], mid[2], k2);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) nx[c] = x0[c] + k2[c] * dt;
+    }
+    const double lo[3] = {G.g.ox + 0.5 * G.g.dx, G.g.oy + 0.5 * G.g.dx, G.g.oz + 0.5 * G.g.dx};
+    const double hi[3] = {G.g.ox + (G.g.nx - 0.5) * G.g.dx, G.g.oy + (G.g.ny - 0.5) * G.g.dx,
+                          G.g.oz + (G.g.nz - 0.5) * G.g.dx};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      low[c] = nx[c] < lo[c];
+      high[c] = nx[c] > hi[c];
+      nx[c] = fmax(lo[c], fmin(hi[c], nx[c]));
+    }
+    P.px[p] = (float)nx[0];
+    P.py[p] = (float)nx[1];
+    P.pz[p] = (float)nx[2];
+    ty = P.type[p];
+  }
+  const bool clamped = low[0] || high[0] || low[1] || high[1] || low[2] || high[2];
+  if (esc_flags && live) esc_flags[p] = clamped ? 1 : 0;
+  warp_count(counters, 0, clamped && ty == 0);
+  warp_count(counters, 1, clamped && ty == 1);
+  warp_count(counters, 2, low[0]);
+  warp_count(counters, 3, high[0]);
+  warp_count(counters, 4, low[1]);
+  warp_count(counters, 5, high[1]);
+  warp_count(counters, 6, low[2]);
+  warp_count(counters, 7, high[2]);
+}
+
+__global__ void k_escape_records(ParticlePtrs P, const int* flags, const int* pos, int n, double* out) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n || !flags[p]) return;
+  double* r = out + 8 * (size_t)pos[p];
+  r[0] = P.type[p];
+  r[1] = P.px[p]; r[2] = P.py[p]; r[3] = P.pz[p];
+  r[4] = P.vx[p]; r[5] = P.vy[p]; r[6] = P.vz[p];
+  r[7] = P.vol[p];
+}
+
+// calibrateRhoTilde0: each of the 4096 lattice particles computes its
+// normalised-weight contribution to u-face (4,4,4) in the reference's FP64
+// order; one thread then sums them in particle order.
+__device__ double cubic_d(double d2) {
+  const double q = __ddiv_rn(d2, kR2);
+  const double t = __dsub_rn(1.0, q);
+  return t > 0.0 ? __dmul_rn(__dmul_rn(t, t), t) : 0.0;
+}
+
+__global__ void k_calib_contrib(double mp, double* contrib) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= 4096) return;
+  const int s = q & 7, cell = q >> 3;
+  const int i = cell & 7, j = (cell >> 3) & 7, k = cell >> 6;
+  const double x = __dadd_rn(__dadd_rn((double)i, 0.25), __dmul_rn(0.5, (double)(s & 1)));
+  const double y = __dadd_rn(__dadd_rn((double)j, 0.25), __dmul_rn(0.5, (double)((s >> 1) & 1)));
+  const double z = __dadd_rn(__dadd_rn((double)k, 0.25), __dmul_rn(0.5, (double)((s >> 2) & 1)));
+  const double gx = x, gy = __dsub_rn(y, 0.5), gz = __dsub_rn(z, 0.5);
+  const int i0 = (int)floor(gx), j0 = (int)floor(gy), k0 = (int)floor(gz);
+  double wsum = 0.0, w444 = 0.0;
+  for (int dk = -2; dk <= 3; ++dk)
+    for (int dj = -2; dj <= 3; ++dj)
+      for (int di = -2; di <= 3; ++di) {
+        const int a = i0 + di, b = j0 + dj, c = k0 + dk;
+        if (a < 0 || a >= 9 || b < 0 || b >= 8 || c < 0 || c >= 8) continue;
+        const double ex = __dsub_rn(gx, (double)a), ey = __dsub_rn(gy, (double)b), ez = __dsub_rn(gz, (double)c);
+        const double wv = cubic_d(__dadd_rn(__dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey)), __dmul_rn(ez, ez)));
+        wsum = __dadd_rn(wsum, wv);
+        if (a == 4 && b == 4 && c == 4) w444 = wv;
+      }
+  double v = 0.0;
+  if (wsum > 0.0) {
+    const double w = __ddiv_rn(w444, wsum);
+    if (w > 0.0) v = __dmul_rn(w, mp);
+  }
+  contrib[q] = v;
+}
+
+__global__ void k_calib_sum(const double* contrib, double rho_l, double* out) {
+  double s = 0.0;
+  for (int q = 0; q < 4096; ++q) s = __dadd_rn(s, contrib[q]);
+  *out = s > 0.0 ? __ddiv_rn(s, rho_l) : 1.0;
+}
+
+ParticlePtrs particle_ptrs(pf_ctx* ctx) {
+  return ParticlePtrs{ctx->px, ctx->py, ctx->pz, ctx->vx, ctx->vy, ctx->vz, ctx->vol, ctx->type};
+}
+
+int slot_grid(const pf_ctx* ctx) {
+  const int cap = 16 * ctx->num_sms;
+  return ctx->nslots < cap ? ctx->nslots : cap;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// host orchestration
+// ---------------------------------------------------------------------------
+
+int mark_cells(pf_ctx* ctx) {
+  StageScope stage(ctx, PF_STAGE_MARK);
+  int rc = field_clear(ctx, PF_MK);
+  if (rc) return rc;
+  const int n = (int)ctx->np;
+  DevGrid G = dev_grid(ctx);
+  // request tiles: walls + particle cells
+  rc = request_wall_tiles(ctx);
+  if (rc) return rc;
+  if (n > 0)
+    (++ctx->launches), k_bin_activate<<<nblocks(n, 256), 256, 0, ctx->stream>>>(G, ctx->px, ctx->py, ctx->pz, n, nullptr,
+                                                             nullptr, nullptr, ctx->tile_need, 0, 0);
+  PF_CUDA_TRY(cudaGetLastError());
+  rc = pool_commit(ctx);
+  if (rc) return rc;
+  G = dev_grid(ctx);
+  (++ctx->launches), k_mark_walls<<<4 * ctx->num_sms, 256, 0, ctx->stream>>>(G);
+  if (n > 0) (++ctx->launches), k_mark_particles<<<nblocks(n, 256), 256, 0, ctx->stream>>>(G, ctx->px, ctx->py, ctx->pz, n);
+  PF_CUDA_TRY(cudaGetLastError());
+  return PF_OK;
+}
+
+static int p2g_core(pf_ctx* ctx, const pf_phase* ph, double Vp) {
+  const int n = (int)ctx->np;
+  const int nt = ctx->g.ntiles;
+  for (int f = PF_U; f <= PF_MW; ++f) {
+    int rc = field_clear(ctx, f);
+    if (rc) return rc;
+  }
+  int rc;
+  {
+    StageScope sc(ctx, PF_STAGE_BIN);
+    PF_CUDA_TRY(cudaMemsetAsync(ctx->tile_count, 0, (size_t)(nt + 1) * sizeof(int), ctx->stream));
+    DevGrid G = dev_grid(ctx);
+    if (n > 0)
+      (++ctx->launches), k_bin_activate<<<nblocks(n, 256), 256, 0, ctx->stream>>>(G, ctx->px, ctx->py, ctx->pz, n, ctx->tile_count,
+                                                               ctx->pkey, ctx->prank, ctx->tile_need, 1, 1);
+    PF_CUDA_TRY(cudaGetLastError());
+    rc = pool_commit(ctx);
+    if (rc) return rc;
+  }
+  if (n == 0) return PF_OK;
+  {
+    StageScope sc(ctx, PF_STAGE_SORT);
+    rc = scan_exclusive(ctx, ctx->tile_count, ctx->tile_start, nt + 1, nullptr);
+    if (rc) return rc;
+    (++ctx->launches), k_bin_scatter<<<nblocks(n, 256), 256, 0, ctx->stream>>>(ctx->pkey, ctx->prank, ctx->tile_start, ctx->perm, n);
+    PF_CUDA_TRY(cudaGetLastError());
+  }
+  {
+    StageScope sc(ctx, PF_STAGE_SPLAT);
+    const size_t smem = 6 * kBox3 * sizeof(float);
+    (++ctx->launches), k_splat<<<nt, 256, smem, ctx->stream>>>(dev_grid(ctx), ctx->tile_start, ctx->perm, ctx->px, ctx->py, ctx->pz,
+                                            ctx->vx, ctx->vy, ctx->vz, ctx->type, ctx->vol, ph->rho_l, ph->rho_g,
+                                            Vp);
+    PF_CUDA_TRY(cudaGetLastError());
+  }
+  return PF_OK;
+}
+
+int p2g(pf_ctx* ctx, const pf_phase* ph, double Vp) {
+  int rc = p2g_core(ctx, ph, Vp);
+  if (rc) return rc;
+  return normalize_save_gravity(ctx, false, false, 0.0, 0.0);
+}
+
+int normalize_save_gravity(pf_ctx* ctx, bool save, bool gravity, double dt, double gval) {
+  StageScope stage(ctx, PF_STAGE_NORMALIZE);
+  if (ctx->nslots > 0)
+    (++ctx->launches), k_normalize<<<slot_grid(ctx), PF_TV, 0, ctx->stream>>>(dev_grid(ctx), ctx->nslots, save ? 1 : 0,
+                                                           gravity ? 1 : 0, (float)(dt * gval));
+  PF_CUDA_TRY(cudaGetLastError());
+  if (save) ctx->saved_valid = true;
+  return PF_OK;
+}
+
+int save_velocity(pf_ctx* ctx) {
+  StageScope stage(ctx, PF_STAGE_BOUNDARY);
+  if (ctx->nslots > 0) (++ctx->launches), k_save<<<slot_grid(ctx), PF_TV, 0, ctx->stream>>>(dev_grid(ctx), ctx->nslots);
+  PF_CUDA_TRY(cudaGetLastError());
+  ctx->saved_valid = true;
+  return PF_OK;
+}
+
+int apply_gravity(pf_ctx* ctx, double dt, double gval) {
+  StageScope stage(ctx, PF_STAGE_BOUNDARY);
+  if (ctx->nslots > 0)
+    (++ctx->launches), k_gravity<<<slot_grid(ctx), PF_TV, 0, ctx->stream>>>(dev_grid(ctx), ctx->nslots, (float)(dt * gval));
+  PF_CUDA_TRY(cudaGetLastError());
+  return PF_OK;
+}
+
+int apply_walls(pf_ctx* ctx) {
+  StageScope stage(ctx, PF_STAGE_BOUNDARY);
+  int rc = request_wall_tiles(ctx);
+  if (rc) return rc;
+  rc = pool_commit(ctx);
+  if (rc) return rc;
+  (++ctx->launches), k_walls<<<4 * ctx->num_sms, 256, 0, ctx->stream>>>(dev_grid(ctx));
+  PF_CUDA_TRY(cudaGetLastError());
+  return PF_OK;
+}
+
+int g2p(pf_ctx* ctx, const pf_ctx* saved, double aL, double aG) {
+  StageScope stage(ctx, PF_STAGE_G2P);
+  const int n = (int)ctx->np;
+  if (n == 0) return PF_OK;
+  DevGrid G = dev_grid(ctx);
+  if (saved && saved != ctx) {
+    DevGrid S = dev_grid(saved);
+    (++ctx->launches), k_g2p<true><<<nblocks(n, 256), 256, 0, ctx->stream>>>(G, S, particle_ptrs(ctx), n, aL, aG);
+  } else {
+    if (!ctx->saved_valid) return set_error(ctx, PF_ERR_INVALID, "g2p: no saved velocity (call pf_save_velocity)");
+    (++ctx->launches), k_g2p<false><<<nblocks(n, 256), 256, 0, ctx->stream>>>(G, G, particle_ptrs(ctx), n, aL, aG);
+  }
+  PF_CUDA_TRY(cudaGetLastError());
+  return PF_OK;
+}
+
+static int read_clamp(pf_ctx* ctx, pf_clamp_stats* st) {
+  PF_CUDA_TRY(cudaMemcpyAsync(ctx->h_pinned_ints, ctx->d_clamp, 8 * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  PF_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  if (st) {
+    const int* c = ctx->h_pinned_ints;
+    st->clamped_liquid = c[0]; st->clamped_gas = c[1];
+    st->x_lo = c[2]; st->x_hi = c[3]; st->y_lo = c[4]; st->y_hi = c[5]; st->z_lo = c[6]; st->z_hi = c[7];
+  }
+  return PF_OK;
+}
+
+int advect(pf_ctx* ctx, double dt, int order, pf_clamp_stats* st, double* esc, size_t* nesc) {
+  StageScope stage(ctx, PF_STAGE_G2P);
+  const int n = (int)ctx->np;
+  PF_CUDA_TRY(cudaMemsetAsync(ctx->d_clamp, 0, 8 * sizeof(int), ctx->stream));
+  if (n > 0) {
+    (++ctx->launches), k_advect<<<nblocks(n, 256), 256, 0, ctx->stream>>>(dev_grid(ctx), particle_ptrs(ctx), n, dt, order,
+                                                        ctx->d_clamp, esc ? ctx->d_flags : nullptr, 0, 0.0, 0.0);
+    PF_CUDA_TRY(cudaGetLastError());
+  }
+  if (esc) {
+    int total = 0;
+    if (n > 0) {
+      int* pos = ctx->d_flags + ctx->cap;
+      int rc = scan_exclusive(ctx, ctx->d_flags, pos, n, ctx->d_scalar);
+      if (rc) return rc;
+      PF_CUDA_TRY(cudaMemcpyAsync(ctx->h_pinned_ints + 8, ctx->d_scalar, sizeof(int), cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+      PF_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+      total = ctx->h_pinned_ints[8];
+      const size_t need_bytes = (size_t)(total > 0 ? total : 1) * 8 * sizeof(double);
+      if (need_bytes > ctx->esc_bytes) {
+        if (ctx->esc_buf) PF_CUDA_TRY(cudaFree(ctx->esc_buf));
+        ctx->esc_buf = nullptr;
+        ctx->esc_bytes = 0;
+        PF_CUDA_TRY(cudaMalloc(&ctx->esc_buf, need_bytes));
+        ctx->esc_bytes = need_bytes;
+      }
+      double* out = (double*)ctx->esc_buf;
+      (++ctx->launches), k_escape_records<<<nblocks(n, 256), 256, 0, ctx->stream>>>(particle_ptrs(ctx), ctx->d_flags, pos, n, out);
+      PF_CUDA_TRY(cudaGetLastError());
+      if (total > 0)
+        PF_CUDA_TRY(cudaMemcpyAsync(esc, out, (size_t)total * 8 * sizeof(double), cudaMemcpyDefault, ctx->stream));
+    }
+    if (nesc) *nesc = (size_t)total;
+  }
+  return read_clamp(ctx, st);
+}
+
+int g2p_advect(pf_ctx* ctx, double aL, double aG, double dt, int order, pf_clamp_stats* st) {
+  StageScope stage(ctx, PF_STAGE_G2P);
+  const int n = (int)ctx->np;
+  PF_CUDA_TRY(cudaMemsetAsync(ctx->d_clamp, 0, 8 * sizeof(int), ctx->stream));
+  if (n > 0) {
+    (++ctx->launches), k_advect<<<nblocks(n, 256), 256, 0, ctx->stream>>>(dev_grid(ctx), particle_ptrs(ctx), n, dt, order,
+                                                        ctx->d_clamp, nullptr, 1, aL, aG);
+    PF_CUDA_TRY(cudaGetLastError());
+  }
+  if (st) return read_clamp(ctx, st);
+  return PF_OK;
+}
+
+int calibrate(pf_ctx* ctx, const pf_phase* ph, double Vp, double* out) {
+  double* contrib = (double*)ctx->staging;  // 4096 doubles + 1
+  const double mp = ph->rho_l * Vp;
+  (++ctx->launches), k_calib_contrib<<<16, 256, 0, ctx->stream>>>(mp, contrib);
+  (++ctx->launches), k_calib_sum<<<1, 1, 0, ctx->stream>>>(contrib, ph->rho_l, contrib + 4096);
+  PF_CUDA_TRY(cudaGetLastError());
+  PF_CUDA_TRY(cudaMemcpyAsync(out, contrib + 4096, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  PF_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return PF_OK;
+}
+
+}  // namespace pf

@@ -1,0 +1,410 @@
+"""Host-side mirror of the reference's sparse 3D two-phase interface over libpfgpu.
+
+Names, argument meaning and argument order follow the reference:
+  spP2G3D_tp / spProjectStepVC3D / spG2P3D_tp / spAdvect3D_tp
+    (src/driver/sparse_ops3d_tp.h:8-15), SparseMacGrid3D<4>
+    (src/grid/sparse_mac_grid3d.h:6-47), Particles3DTP
+    (src/particles/particles3d_tp.h:4-35), PhaseParams and the Eq. 7 helpers
+    (src/physics/phasefield.h:4-18), ParticleEscapeStats3D/Buffer3D
+    (src/driver/particle_escape3d.h), SparseSim3DTP::step
+    (src/driver/sparse_sim3d_tp.cpp:854-884).
+
+A SparseMacGrid3D owns one libpfgpu context (device-resident tile pool and a
+particle buffer).  The per-call functions move the caller's FP64 particle
+arrays in and out of that context around each call, as the reference's
+in-place mutation of Particles3DTP implies; SparseSim3DTP keeps the particles
+on the device across steps.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib as L
+
+FIELD_NAMES = ("u", "v", "w", "mu", "mv", "mw", "p", "mk")
+
+
+# ---------------------------------------------------------------------------
+# phase field (src/physics/phasefield.h)
+# ---------------------------------------------------------------------------
+
+@dataclass
+class PhaseParams:
+    """PhaseParams (src/physics/phasefield.h:4-9)."""
+    rho_l: float = 1.0
+    rho_g: float = 0.01
+    alpha_phi: float = 1.0
+    rho_tilde_0: float = 1.0
+
+    def _c(self):
+        return L.Phase(self.rho_l, self.rho_g, self.alpha_phi, self.rho_tilde_0)
+
+
+def etaPhi(pp: PhaseParams) -> float:
+    return math.log(pp.rho_l / pp.rho_g)
+
+
+def phiFromRawDensity(rt: float, pp: PhaseParams) -> float:
+    rmin = etaPhi(pp) * pp.rho_g * pp.rho_tilde_0
+    if rt < rmin:
+        return 0.0
+    v = math.sqrt(max(rt - rmin, 0.0) / (pp.alpha_phi * pp.rho_tilde_0 * pp.rho_l))
+    return min(v, 1.0)
+
+
+def densityFromPhi(phi: float, pp: PhaseParams) -> float:
+    return phi * pp.rho_l + (1.0 - phi) * pp.rho_g
+
+
+def betaFromPhi(phi: float, pp: PhaseParams) -> float:
+    return 1.0 / densityFromPhi(phi, pp)
+
+
+# ---------------------------------------------------------------------------
+# particles (src/particles/particles3d_tp.h)
+# ---------------------------------------------------------------------------
+
+class Particles3DTP:
+    """Particles3DTP: pos/vel (n,3) float64, type uint8 (0 liquid, 1 gas), volume float64."""
+
+    def __init__(self, pos=None, vel=None, type=None, volume=None):
+        n = 0 if pos is None else len(pos)
+        self.pos = np.ascontiguousarray(np.zeros((n, 3)) if pos is None else pos, np.float64).reshape(n, 3)
+        self.vel = np.ascontiguousarray(np.zeros((n, 3)) if vel is None else vel, np.float64).reshape(n, 3)
+        self.type = np.ascontiguousarray(np.zeros(n) if type is None else type, np.uint8).reshape(n)
+        self.volume = np.ascontiguousarray(np.ones(n) if volume is None else volume, np.float64).reshape(n)
+
+    def size(self):
+        return len(self.pos)
+
+    __len__ = size
+
+    def add(self, p, v, t, vol=1.0):
+        self.pos = np.vstack([self.pos, np.asarray(p, np.float64).reshape(1, 3)])
+        self.vel = np.vstack([self.vel, np.asarray(v, np.float64).reshape(1, 3)])
+        self.type = np.append(self.type, np.uint8(t)).astype(np.uint8)
+        self.volume = np.append(self.volume, float(vol))
+
+    def copy(self):
+        return Particles3DTP(self.pos.copy(), self.vel.copy(), self.type.copy(), self.volume.copy())
+
+
+@dataclass
+class ParticleEscapeStats3D:
+    """ParticleEscapeStats3D (src/driver/particle_escape3d.h:38-80)."""
+    clamped_liquid: int = 0
+    clamped_gas: int = 0
+    clamped_x_lo: int = 0
+    clamped_x_hi: int = 0
+    clamped_y_lo: int = 0
+    clamped_y_hi: int = 0
+    clamped_z_lo: int = 0
+    clamped_z_hi: int = 0
+
+    def clamped_total(self):
+        return self.clamped_liquid + self.clamped_gas
+
+    def droplet_candidates(self):
+        return self.clamped_liquid
+
+    def bubble_candidates(self):
+        return self.clamped_gas
+
+
+@dataclass
+class ParticleEscapeBuffer3D:
+    """ParticleEscapeBuffer3D: records (type, pos, vel, volume) of clamped particles in order."""
+    records: list = field(default_factory=list)
+
+    def droplet_count(self):
+        return sum(1 for r in self.records if r["type"] == 0)
+
+    def bubble_count(self):
+        return sum(1 for r in self.records if r["type"] == 1)
+
+
+@dataclass
+class SolverConfig:
+    """Pressure solver selection beyond the reference's (cg_iters, cg_tol)."""
+    mode: int = L.PF_SOLVER_PLAIN
+    rel_tol: float = 0.0
+    bf16_storage: bool = False
+    check_every: int = 0
+    max_refine: int = 0
+    inner_rel_tol: float = 0.0
+
+
+# ---------------------------------------------------------------------------
+# grid (src/grid/sparse_mac_grid3d.h)
+# ---------------------------------------------------------------------------
+
+def _field_dims(nx, ny, nz, f):
+    return [(nx + 1, ny, nz), (nx, ny + 1, nz), (nx, ny, nz + 1), (nx + 1, ny, nz), (nx, ny + 1, nz),
+            (nx, ny, nz + 1), (nx, ny, nz), (nx, ny, nz)][f]
+
+
+class SparseMacGrid3D:
+    """GPU-resident SparseMacGrid3D<4>: eight sparse fields in a pool of 8^3
+    tiles, reference-granular (4^3) activity per field."""
+
+    def __init__(self, nx, ny, nz, dx, origin=(0.0, 0.0, 0.0), max_particles=1 << 16, device=0):
+        self.lib = L.load()
+        self.nx, self.ny, self.nz, self.dx = int(nx), int(ny), int(nz), float(dx)
+        self.ox, self.oy, self.oz = (float(o) for o in origin)
+        self.device = int(device)
+        self.max_particles = int(max_particles)
+        d = L.GridDesc(self.nx, self.ny, self.nz, self.dx, self.ox, self.oy, self.oz, self.max_particles,
+                       self.device)
+        h = C.c_void_p()
+        rc = self.lib.pf_create(C.byref(d), C.byref(h))
+        L.check(rc, None, "pf_create")
+        self.ctx = h.value
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.lib.pf_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- shape helpers --
+    def dims(self, f):
+        return _field_dims(self.nx, self.ny, self.nz, f)
+
+    def bdims(self, f):
+        X, Y, Z = self.dims(f)
+        return ((X + 3) // 4, (Y + 3) // 4, (Z + 3) // 4)
+
+    def inBounds(self, i, j, k):
+        return 0 <= i < self.nx and 0 <= j < self.ny and 0 <= k < self.nz
+
+    # -- field exchange --
+    def get_field(self, f):
+        X, Y, Z = self.dims(f)
+        bx, by, bz = self.bdims(f)
+        dense = np.zeros((Z, Y, X), np.float32)
+        act = np.zeros((bz, by, bx), np.uint8)
+        rc = self.lib.pf_grid_get_field(self.ctx, f, dense.ctypes.data, act.ctypes.data)
+        L.check(rc, self.ctx, "pf_grid_get_field")
+        return dense, act
+
+    def set_field(self, f, dense, act):
+        X, Y, Z = self.dims(f)
+        dense = np.ascontiguousarray(dense, np.float32).reshape(Z, Y, X)
+        act = np.ascontiguousarray(act, np.uint8).reshape(self.bdims(f)[::-1])
+        rc = self.lib.pf_grid_set_field(self.ctx, f, dense.ctypes.data, act.ctypes.data)
+        L.check(rc, self.ctx, "pf_grid_set_field")
+
+    def set_values(self, f, values):
+        """Write a dense (Z,Y,X) array; nonzero nodes activate their 4^3 block
+        (the reference's ref() on every written node)."""
+        v = np.asarray(values, np.float32)
+        X, Y, Z = self.dims(f)
+        act = np.zeros(self.bdims(f)[::-1], np.uint8)
+        kk, jj, ii = np.nonzero(v)
+        act[kk // 4, jj // 4, ii // 4] = 1
+        self.set_field(f, v, act)
+
+    def set_cells(self, markers):
+        """Marker field from a dense (nz,ny,nx) int array (SparseMacGrid3D::setCell)."""
+        self.set_values(L.PF_MK, np.asarray(markers, np.float32))
+
+    def field(self, f):
+        return self.get_field(f)[0]
+
+    def clear_field(self, f):
+        L.check(self.lib.pf_grid_clear_field(self.ctx, f), self.ctx, "pf_grid_clear_field")
+
+    def clearAll(self):
+        L.check(self.lib.pf_grid_clear_all(self.ctx), self.ctx, "pf_grid_clear_all")
+
+    def copy(self):
+        g = SparseMacGrid3D(self.nx, self.ny, self.nz, self.dx, (self.ox, self.oy, self.oz),
+                            max_particles=1, device=self.device)
+        L.check(self.lib.pf_grid_copy(g.ctx, self.ctx), g.ctx, "pf_grid_copy")
+        return g
+
+    def active_blocks(self, f):
+        """Sorted ids (bx + nbx*(by + nby*bz)) of the active 4^3 blocks of field f."""
+        n = C.c_size_t()
+        L.check(self.lib.pf_active_blocks4(self.ctx, f, None, C.byref(n)), self.ctx, "pf_active_blocks4")
+        out = np.zeros(max(n.value, 1), np.int32)
+        L.check(self.lib.pf_active_blocks4(self.ctx, f, out.ctypes.data, C.byref(n)), self.ctx, "pf_active_blocks4")
+        return out[: n.value].astype(np.int64)
+
+    def activeBlockCount(self, f):
+        return len(self.active_blocks(f))
+
+    def activeCellBlocks(self):
+        return self.activeBlockCount(L.PF_P)
+
+    def fluid_cells(self):
+        """collectCellsWithMarker(g, 1): fluid cells ascending in i + nx*(j + ny*k)."""
+        n = C.c_size_t()
+        L.check(self.lib.pf_active_cells(self.ctx, None, C.byref(n)), self.ctx, "pf_active_cells")
+        out = np.zeros(max(n.value, 1), np.int32)
+        L.check(self.lib.pf_active_cells(self.ctx, out.ctypes.data, C.byref(n)), self.ctx, "pf_active_cells")
+        return out[: n.value].astype(np.int64)
+
+    def active_tiles(self):
+        return int(self.lib.pf_active_tiles(self.ctx))
+
+    def cell_markers(self):
+        return (self.field(L.PF_MK) + np.float32(0.5)).astype(np.int32)
+
+    # -- particle exchange --
+    def _ensure_capacity(self, n):
+        if n > self.max_particles:
+            raise L.PfError(L.PF_ERR_CAPACITY, f"{n} particles > max_particles={self.max_particles}")
+
+    def upload(self, ps):
+        n = len(ps.pos)
+        self._ensure_capacity(n)
+        pos = np.ascontiguousarray(ps.pos, np.float64)
+        vel = np.ascontiguousarray(ps.vel, np.float64)
+        typ = np.ascontiguousarray(ps.type, np.uint8)
+        vol = np.ascontiguousarray(ps.volume, np.float64)
+        rc = self.lib.pf_upload_particles_f64(self.ctx, n, pos.ctypes.data, vel.ctypes.data, typ.ctypes.data,
+                                              vol.ctypes.data)
+        L.check(rc, self.ctx, "pf_upload_particles_f64")
+
+    def download(self, ps, pos=True, vel=True):
+        n = len(ps.pos)
+        if n == 0:
+            return
+        P = np.empty((n, 3), np.float64) if pos else None
+        V = np.empty((n, 3), np.float64) if vel else None
+        rc = self.lib.pf_download_particles_f64(self.ctx, P.ctypes.data if pos else None,
+                                                V.ctypes.data if vel else None, None, None)
+        L.check(rc, self.ctx, "pf_download_particles_f64")
+        if pos:
+            ps.pos = P
+        if vel:
+            ps.vel = V
+
+
+# ---------------------------------------------------------------------------
+# per-call drop-ins (src/driver/sparse_ops3d_tp.h:8-15)
+# ---------------------------------------------------------------------------
+
+def calibrateRhoTilde0(pp: PhaseParams, Vp: float, grid: SparseMacGrid3D | None = None) -> float:
+    """calibrateRhoTilde0 (src/transfer/transfer3d_tp.cpp:29-36) on the GPU."""
+    g = grid or SparseMacGrid3D(8, 8, 8, 1.0, max_particles=1)
+    out = C.c_double()
+    L.check(g.lib.pf_calibrate_rho_tilde0(g.ctx, C.byref(pp._c()), float(Vp), C.byref(out)), g.ctx,
+            "pf_calibrate_rho_tilde0")
+    return out.value
+
+
+def spP2G3D_tp(g: SparseMacGrid3D, ps, pp: PhaseParams, Vp: float):
+    g.upload(ps)
+    L.check(g.lib.pf_p2g(g.ctx, C.byref(pp._c()), float(Vp)), g.ctx, "pf_p2g")
+
+
+def spProjectStepVC3D(g: SparseMacGrid3D, pp: PhaseParams, dt, cg_iters, cg_tol, divergenceCorrection=0.0,
+                      solver: SolverConfig | None = None) -> L.SolveStats:
+    s = solver or SolverConfig()
+    cfg = L.SolveCfg(int(s.mode), int(cg_iters), float(cg_tol), float(s.rel_tol), float(divergenceCorrection),
+                     int(bool(s.bf16_storage)), int(s.check_every), int(s.max_refine), float(s.inner_rel_tol))
+    st = L.SolveStats()
+    L.check(g.lib.pf_project(g.ctx, C.byref(pp._c()), float(dt), C.byref(cfg), C.byref(st)), g.ctx,
+            "pf_project")
+    return st
+
+
+def spG2P3D_tp(g: SparseMacGrid3D, ps, saved: SparseMacGrid3D, aL, aG):
+    g.upload(ps)
+    L.check(g.lib.pf_g2p(g.ctx, saved.ctx if saved is not None else None, float(aL), float(aG)), g.ctx,
+            "pf_g2p")
+    g.download(ps, pos=False, vel=True)
+
+
+def spAdvect3D_tp(ps, g: SparseMacGrid3D, dt, stats: ParticleEscapeStats3D | None = None, advectionOrder=2,
+                  escapeBuffer: ParticleEscapeBuffer3D | None = None):
+    g.upload(ps)
+    cs = L.ClampStats()
+    n = len(ps.pos)
+    esc = np.zeros((max(n, 1), 8), np.float64) if escapeBuffer is not None else None
+    nesc = C.c_size_t()
+    rc = g.lib.pf_advect(g.ctx, float(dt), int(advectionOrder), C.byref(cs),
+                         esc.ctypes.data if esc is not None else None, C.byref(nesc))
+    L.check(rc, g.ctx, "pf_advect")
+    g.download(ps, pos=True, vel=False)
+    if stats is not None:
+        (stats.clamped_liquid, stats.clamped_gas, stats.clamped_x_lo, stats.clamped_x_hi, stats.clamped_y_lo,
+         stats.clamped_y_hi, stats.clamped_z_lo, stats.clamped_z_hi) = cs.as_tuple()
+    if escapeBuffer is not None:
+        for r in esc[: nesc.value]:
+            escapeBuffer.records.append({"type": int(r[0]), "pos": r[1:4].copy(), "vel": r[4:7].copy(),
+                                         "volume": float(r[7])})
+    return cs
+
+
+# ---------------------------------------------------------------------------
+# device-resident step (SparseSim3DTP)
+# ---------------------------------------------------------------------------
+
+class SparseSim3DTP:
+    """SparseSim3DTP with particles resident on the GPU; step() runs
+    markCells, P2G, saved copy, gravity, walls, projection, G2P and
+    advection in the reference's order (src/driver/sparse_sim3d_tp.cpp:854-884).
+    Defaults follow src/driver/sparse_sim3d_tp.h:12-28."""
+
+    def __init__(self, nx, ny, nz, dx, max_particles=1 << 20, device=0):
+        self.grid = SparseMacGrid3D(nx, ny, nz, dx, max_particles=max_particles, device=device)
+        self.phase = PhaseParams()
+        self.dt, self.gravity, self.Vp = 0.02, -9.81, 1.0
+        self.alpha_liquid = self.alpha_gas = 0.95
+        self.advection_order = 2
+        self.cg_iters, self.cg_tol = 600, 1e-7
+        self.c_div_last = 0.0
+        self.solver = SolverConfig()
+        self.n = 0
+        self.last_stats = None
+
+    def set_particles(self, pos, vel, type, volume):
+        """Upload FP32 (n,3) pos/vel, uint8 type, FP32 volume (host or device pointers via numpy)."""
+        pos = np.ascontiguousarray(pos, np.float32)
+        vel = np.ascontiguousarray(vel, np.float32)
+        typ = np.ascontiguousarray(type, np.uint8)
+        vol = np.ascontiguousarray(volume, np.float32)
+        n = len(pos)
+        self.grid._ensure_capacity(n)
+        rc = self.grid.lib.pf_upload_particles(self.grid.ctx, n, pos.ctypes.data, vel.ctypes.data,
+                                               typ.ctypes.data, vol.ctypes.data)
+        L.check(rc, self.grid.ctx, "pf_upload_particles")
+        self.n = n
+
+    def get_particles(self):
+        n = self.n
+        pos = np.empty((n, 3), np.float32)
+        vel = np.empty((n, 3), np.float32)
+        typ = np.empty(n, np.uint8)
+        vol = np.empty(n, np.float32)
+        rc = self.grid.lib.pf_download_particles(self.grid.ctx, pos.ctypes.data, vel.ctypes.data, typ.ctypes.data,
+                                                 vol.ctypes.data)
+        L.check(rc, self.grid.ctx, "pf_download_particles")
+        return pos, vel, typ, vol
+
+    def step_cfg(self):
+        s = self.solver
+        solve = L.SolveCfg(int(s.mode), int(self.cg_iters), float(self.cg_tol), float(s.rel_tol),
+                           float(self.c_div_last), int(bool(s.bf16_storage)), int(s.check_every),
+                           int(s.max_refine), float(s.inner_rel_tol))
+        return L.StepCfg(self.dt, self.gravity, self.Vp, self.alpha_liquid, self.alpha_gas, self.phase._c(), solve,
+                         int(self.advection_order))
+
+    def step(self):
+        cfg = self.step_cfg()
+        st = L.StepStats()
+        L.check(self.grid.lib.pf_step(self.grid.ctx, C.byref(cfg), C.byref(st)), self.grid.ctx, "pf_step")
+        self.last_stats = st
+        return st

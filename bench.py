@@ -1,0 +1,385 @@
+#!/usr/bin/env python
+"""Solver-step benchmark for the B200 backend (one JSON line on rank 0).
+
+Default workload (transfer stress): bubble tank on a 128^3 grid, 8^3-cell
+tiles, water below y = 0.7 with an air bubble of radius 0.15 at
+(0.5, 0.3, 0.5), 8 jittered particles per cell (11,303,712 particles),
+velocities N(0, 0.1^2); one step = P2G (u, v, w and face raw mass, the phi
+input) + saved copy + G2P with FLIP ratio 0.97, device-resident.
+
+  value       step particles/s with inputs resident on the device, CUDA events
+              on the library's stream around K steps (max over ranks)
+  e2e         the same through the public C ABI from pinned host buffers:
+              every step uploads the particles (29 B each) and reads back the
+              updated velocities (12 B each)
+  roofline    the dominant kernel's algorithmic bytes per launch / its mean
+              device time (per-stage CUDA events), against the measured HBM
+              copy bandwidth
+  cpu_baseline the reference's own C++ P2G + G2P (compiled from its sources
+              into oracle/_ref) on a bounded slab of the same scene
+
+--impl reference times that reference CPU path alone (rank 0; other ranks
+exit).  Multi-GPU runs are independent replicas (weak scaling): the solver
+step is single-GPU by design.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.join(ROOT, "adaptive-pf-flip_b200")
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def load_pkg():
+    name = "adaptive_pf_flip_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(name, os.path.join(PKG_DIR, "__init__.py"),
+                                                  submodule_search_locations=[PKG_DIR])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+METRIC = "step particles/s (P2G + G2P transfer step, bubble tank 128^3)"
+UNIT = "particles/s"
+# algorithmic bytes (FP32 SoA particles: pos 12, vel 12, type 1, volume 4)
+P2G_BYTES_PER_PARTICLE = 29
+P2G_BYTES_PER_FACE = 8       # momentum->velocity + raw mass written once per active face node
+G2P_BYTES_PER_PARTICLE = 37  # read pos+vel+type, write vel
+G2P_BYTES_PER_FACE = 8       # current + saved face velocity read once
+
+
+def measured_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return rank, world, local, dist
+
+
+def reduce_max(dist, value, local):
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+
+class TransferStep:
+    """P2G + saved copy + G2P on one libpfgpu context."""
+
+    def __init__(self, pf, sc, device, alpha=0.97):
+        import torch
+        self.pf, self.L = pf, pf._lib
+        self.lib = pf.load()
+        self.n = len(sc["pos"])
+        nx = sc["nx"]
+        self.g = pf.SparseMacGrid3D(nx, sc["ny"], sc["nz"], sc["dx"], max_particles=self.n, device=device)
+        self.ctx = self.g.ctx
+        pp = pf.PhaseParams(sc["rho_l"], sc["rho_g"])
+        pp.rho_tilde_0 = pf.calibrateRhoTilde0(pp, 1.0, grid=self.g)
+        self.phase = pp._c()
+        self.alpha = alpha
+        # pinned host copies of the inputs (for the end-to-end leg)
+        self.h_pos = torch.from_numpy(np.ascontiguousarray(sc["pos"], np.float32)).pin_memory()
+        self.h_vel = torch.from_numpy(np.ascontiguousarray(sc["vel"], np.float32)).pin_memory()
+        self.h_type = torch.from_numpy(np.ascontiguousarray(sc["type"], np.uint8)).pin_memory()
+        self.h_vol = torch.from_numpy(np.ascontiguousarray(sc["volume"], np.float32)).pin_memory()
+        self.h_out = torch.empty((self.n, 3), dtype=torch.float32).pin_memory()
+        self.stream = torch.cuda.ExternalStream(self.lib.pf_stream(self.ctx), device=f"cuda:{device}")
+        self.upload()
+
+    def upload(self):
+        rc = self.lib.pf_upload_particles(self.ctx, self.n, self.h_pos.data_ptr(), self.h_vel.data_ptr(),
+                                          self.h_type.data_ptr(), self.h_vol.data_ptr())
+        self.L.check(rc, self.ctx, "pf_upload_particles")
+
+    def download_vel(self):
+        rc = self.lib.pf_download_particles(self.ctx, None, self.h_out.data_ptr(), None, None)
+        self.L.check(rc, self.ctx, "pf_download_particles")
+
+    def step(self):
+        L, lib, ctx = self.L, self.lib, self.ctx
+        L.check(lib.pf_p2g(ctx, C.byref(self.phase), 1.0), ctx, "pf_p2g")
+        L.check(lib.pf_save_velocity(ctx), ctx, "pf_save_velocity")
+        L.check(lib.pf_g2p(ctx, None, self.alpha, self.alpha), ctx, "pf_g2p")
+
+    def active_faces(self):
+        n = 0
+        for f in (self.pf.PF_MU, self.pf.PF_MV, self.pf.PF_MW):
+            m, _ = self.g.get_field(f)
+            n += int((m > 0).sum())
+        return n
+
+
+def time_steps(ts, steps, warmup, dist, local, e2e=False):
+    import torch
+    for _ in range(warmup):
+        if e2e:
+            ts.upload()
+        ts.step()
+        if e2e:
+            ts.download_vel()
+    torch.cuda.synchronize(local)
+    barrier(dist)
+    torch.cuda.synchronize(local)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = ts.lib.pf_launch_count(ts.ctx)
+    ev0.record(ts.stream)
+    for _ in range(steps):
+        if e2e:
+            ts.upload()
+        ts.step()
+        if e2e:
+            ts.download_vel()
+    ev1.record(ts.stream)
+    ev1.synchronize()
+    torch.cuda.synchronize(local)
+    launches = ts.lib.pf_launch_count(ts.ctx) - launches0
+    barrier(dist)
+    ms = ev0.elapsed_time(ev1)
+    return reduce_max(dist, ms, local), launches
+
+
+def cpu_reference_sample(sc, slab_cells, steps, warmup=0, alpha=0.97):
+    """Reference P2G + saved copy + G2P (oracle/_ref, the unmodified sources)
+    on the particles of the first `slab_cells` x-columns of the scene."""
+    import oracle as O
+    n = sc["nx"]
+    x = sc["pos"][:, 0].astype(np.float64)
+    sel = x < slab_cells * sc["dx"]
+    ps = O.Particles(sc["pos"][sel].astype(np.float64), sc["vel"][sel].astype(np.float64), sc["type"][sel],
+                     sc["volume"][sel].astype(np.float64))
+    ref = O.Reference()
+    pp = O.PhaseParams(sc["rho_l"], sc["rho_g"])
+    pp.rho_tilde_0 = ref.calibrate_rho_tilde0(pp, 1.0)
+    g = O.ReferenceGrid(n, n, n, sc["dx"])
+    saved = O.ReferenceGrid(n, n, n, sc["dx"])
+    lib = g.lib
+    g._put(ps)
+    arr = pp.as_array()
+    times = []
+    for it in range(warmup + steps):
+        t0 = time.perf_counter()
+        lib.pfr_p2g(g.h, arr, 1.0)
+        lib.pfr_copy_grid(saved.h, g.h)
+        lib.pfr_g2p(g.h, saved.h, alpha, alpha)
+        t1 = time.perf_counter()
+        if it >= warmup:
+            times.append(t1 - t0)
+    return len(ps), times
+
+
+def run_ours(args, rank, world, local, dist):
+    import torch
+    pf = load_pkg()
+    torch.cuda.set_device(local)
+    sc = pf.scenes.bubble_tank(128, seed=args.seed + rank)
+    ts = TransferStep(pf, sc, local)
+    n = ts.n
+    # device-resident timing with per-stage events
+    ts.lib.pf_set_timing(ts.ctx, 1)
+    tm = pf._lib.Timing()
+    ts.lib.pf_get_timing(ts.ctx, C.byref(tm), 1)
+    with ClockSampler(local) as clk:
+        ms, launches = time_steps(ts, args.steps, args.warmup, dist, local)
+    ts.lib.pf_get_timing(ts.ctx, C.byref(tm), 1)
+    stages = tm.as_dict()
+    ts.lib.pf_set_timing(ts.ctx, 0)
+    # end-to-end from pinned host buffers
+    ms_e2e, _ = time_steps(ts, args.steps, max(1, args.warmup // 2), dist, local, e2e=True)
+    n_faces = ts.active_faces()
+
+    value = n * args.steps * world / (ms / 1000.0)
+    e2e_value = n * args.steps * world / (ms_e2e / 1000.0)
+    peak, peak_kind = measured_hbm()
+    # dominant kernel of the step by device time
+    splat_ms = stages["splat"][0] / max(stages["splat"][1], 1)
+    g2p_ms = stages["g2p"][0] / max(stages["g2p"][1], 1)
+    if splat_ms >= g2p_ms:
+        kname, kms = "k_splat (P2G)", splat_ms
+        kbytes = P2G_BYTES_PER_PARTICLE * n + P2G_BYTES_PER_FACE * n_faces
+    else:
+        kname, kms = "k_g2p (G2P)", g2p_ms
+        kbytes = G2P_BYTES_PER_PARTICLE * n + G2P_BYTES_PER_FACE * n_faces
+    achieved = kbytes / (kms / 1000.0) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic_bubble128.json")
+    if os.path.exists(tpath):
+        try:
+            with open(tpath) as f:
+                traffic = json.load(f).get(kname.split()[0])
+        except Exception:
+            traffic = None
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded bubble tank scene)",
+        "config": {"workload": "bubble_tank_128 transfer stress: P2G(u,v,w,raw mass)+G2P, FLIP 0.97",
+                   "grid": [128, 128, 128], "tile": 8, "particles_per_gpu": n, "global_particles": n * world,
+                   "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (particle SoA %.0f MB per GPU)" % (n * 29 / 1e6)},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": n * 29, "d2h_bytes_per_step": n * 12},
+        "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_launch": kbytes, "mean_launch_ms": kms},
+        "stages_ms_per_step": {k: v[0] / max(args.steps, 1) for k, v in stages.items() if v[1]},
+        "gpu_launches": int(launches) * world,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        cores = 8
+        np_s, times = cpu_reference_sample(sc, slab_cells=args.cpu_slab, steps=1)
+        line["cpu_baseline"] = {"value": np_s / times[0], "unit": UNIT, "cores": cores, "kind": "reference",
+                                "sample": f"reference spP2G3D_tp + saved copy + spG2P3D_tp on the {np_s} particles "
+                                          f"of the first {args.cpu_slab} x-columns of the 128^3 scene, 1 step "
+                                          f"({times[0]:.1f} s); P2G uses the reference's 8 colour threads, G2P 1"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    pf = load_pkg()
+    sc = pf.scenes.bubble_tank(128, seed=args.seed)
+    np_s, times = cpu_reference_sample(sc, slab_cells=args.cpu_slab, steps=args.steps, warmup=args.warmup)
+    total = sum(times)
+    value = np_s * len(times) / total
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * total / len(times), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded bubble tank scene)", "impl": "reference",
+        "config": {"workload": "bubble_tank_128 transfer stress: P2G(u,v,w,raw mass)+G2P, FLIP 0.97",
+                   "grid": [128, 128, 128], "sample_particles": np_s},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 8, "kind": "reference",
+                         "sample": f"{np_s} particles (first {args.cpu_slab} x-columns) per step"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--cpu-slab", type=int, default=4, help="x-columns of the scene in the CPU sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    if args.impl == "reference":
+        rank = int(os.environ.get("RANK", "0"))
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        run_reference(args, rank, world)
+        return
+    rank, world, local, dist = dist_setup(args.gpus)
+    try:
+        run_ours(args, rank, world, local, dist)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,213 @@
+/*
+ * pfgpu.h -- C ABI of the B200 (sm_100a) solver-step library for the sparse
+ * 3D two-phase Phase-Field-FLIP step of adaptive-pf-flip.
+ *
+ * One context owns one sparse MAC grid (a pool of 8^3-cell tiles behind a
+ * dense tile->slot array, with 4^3-block activity kept per field exactly as
+ * the reference's SparseBlockGrid3D<4> tracks it) and one particle set, both
+ * resident in device memory.  Every entry point is stream-ordered on the
+ * context's own CUDA stream, returns 0 on success or a negative PF_ERR_* code,
+ * and is not thread-safe per context.  Entry points that return statistics
+ * synchronise the stream before returning.
+ *
+ * Reference interfaces replaced (paths relative to the adaptive-pf-flip tree):
+ *   spP2G3D_tp         src/driver/sparse_ops3d_tp.h:9   -> pf_p2g
+ *   spProjectStepVC3D  src/driver/sparse_ops3d_tp.h:10  -> pf_project
+ *   spG2P3D_tp         src/driver/sparse_ops3d_tp.h:12  -> pf_g2p
+ *   spAdvect3D_tp      src/driver/sparse_ops3d_tp.h:13  -> pf_advect
+ *   SparseSim3DTP::step (markCells, applyGravity, applyWallBoundary and the
+ *     call order of src/driver/sparse_sim3d_tp.cpp:22-97, 854-884)
+ *                                                       -> pf_mark_cells,
+ *        pf_apply_gravity, pf_apply_wall_boundary, pf_save_velocity, pf_step
+ *   SparseMacGrid3D<4> / SparseBlockGrid3D<4> storage
+ *     (src/grid/sparse_mac_grid3d.h:6-47, src/grid/sparse_block_grid3d.h:10-68)
+ *                                                       -> pf_grid_set_field,
+ *        pf_grid_get_field, pf_grid_clear_field, pf_active_blocks4
+ *   collectCellsWithMarker (src/driver/sparse_ops3d_common.h:65-85)
+ *                                                       -> pf_active_cells
+ *   Particles3DTP storage (src/particles/particles3d_tp.h:4-35)
+ *                                                       -> pf_upload_particles*,
+ *        pf_download_particles*
+ */
+#ifndef PFGPU_H
+#define PFGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PFGPU_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define PFGPU_API __attribute__((visibility("default")))
+#else
+#define PFGPU_API
+#endif
+
+/* status codes */
+#define PF_OK 0
+#define PF_ERR_INVALID (-1)   /* bad argument or size */
+#define PF_ERR_CUDA (-2)      /* CUDA runtime error (message via pf_last_error) */
+#define PF_ERR_CAPACITY (-3)  /* more particles than the context was created for */
+#define PF_ERR_NONFINITE (-4) /* NaN/Inf met in the solve */
+#define PF_ERR_NO_DEVICE (-5) /* no usable sm_100 device */
+
+/* field ids: the eight SparseMacGrid3D<4> fields */
+enum pf_field { PF_U = 0, PF_V, PF_W, PF_MU, PF_MV, PF_MW, PF_P, PF_MK, PF_NFIELDS };
+
+typedef struct pf_ctx pf_ctx;
+
+typedef struct {
+  int nx, ny, nz;        /* cells */
+  double dx;             /* cell size */
+  double ox, oy, oz;     /* origin */
+  size_t max_particles;  /* particle capacity */
+  int device;            /* CUDA device ordinal */
+} pf_grid_desc;
+
+/* PhaseParams (src/physics/phasefield.h:4-9) */
+typedef struct {
+  double rho_l, rho_g, alpha_phi, rho_tilde_0;
+} pf_phase;
+
+/* pressure solver modes */
+#define PF_SOLVER_PLAIN 0   /* FP64 Jacobi-PCG, the reference-equivalent drop-in */
+#define PF_SOLVER_MIXED 1   /* FP32 SpMV/preconditioner, FP64 dots, iterative refinement */
+#define PF_SOLVER_LEARNED 2 /* mixed + learned per-tile preconditioner in flexible PCG */
+
+typedef struct {
+  int mode;             /* PF_SOLVER_* */
+  int max_iter;         /* reference cg_iters */
+  double abs_tol;       /* reference cg_tol: stop when max|r| < tol */
+  double rel_tol;       /* 0: reference rule; else tol = max(abs_tol, rel_tol*max|r0|) */
+  double c_div;         /* divergenceCorrection */
+  int bf16_storage;     /* mixed/learned: store beta and search direction in BF16 */
+  int check_every;      /* host convergence poll interval in iterations (0 = default) */
+  int max_refine;       /* mixed/learned: outer refinement sweeps (0 = default) */
+  double inner_rel_tol; /* mixed/learned: inner solve relative reduction (0 = default) */
+} pf_solve_cfg;
+
+typedef struct {
+  int iterations;        /* total inner PCG iterations */
+  int refinements;       /* outer refinement sweeps (mixed/learned) */
+  int n_cells;           /* fluid cells (unknowns incl. the pin) */
+  int converged;
+  int breakdown;         /* |p.Ap| < 1e-30 or non-finite */
+  long long pin_cell;    /* linear index of the pinned cell or -1 */
+  double res0;           /* max|r0| */
+  double res_final;      /* max|r| at exit (FP64 residual) */
+  double tol_effective;
+  int precond_applied;   /* learned: network applications accepted */
+  int precond_rejected;  /* learned: applications that fell back to Jacobi */
+  double solve_ms;       /* device time of the solve */
+} pf_solve_stats;
+
+/* ParticleEscapeStats3D (src/driver/particle_escape3d.h:38-80) */
+typedef struct {
+  int clamped_liquid, clamped_gas;
+  int x_lo, x_hi, y_lo, y_hi, z_lo, z_hi;
+} pf_clamp_stats;
+
+typedef struct {
+  double dt, gravity, Vp, alpha_l, alpha_g;
+  pf_phase phase;
+  pf_solve_cfg solve;
+  int advect_order;      /* 2 (midpoint) or 3 */
+} pf_step_cfg;
+
+typedef struct {
+  pf_solve_stats solve;
+  pf_clamp_stats clamp;
+  int active_tiles;      /* pooled 8^3 tiles */
+} pf_step_stats;
+
+/* ---- context ---------------------------------------------------------- */
+PFGPU_API int pf_create(const pf_grid_desc* desc, pf_ctx** out);
+PFGPU_API int pf_destroy(pf_ctx* ctx);
+PFGPU_API const char* pf_last_error(const pf_ctx* ctx);
+PFGPU_API int pf_sync(pf_ctx* ctx);
+/* The context's stream as an opaque handle (a cudaStream_t). */
+PFGPU_API void* pf_stream(pf_ctx* ctx);
+
+/* ---- particles (pointers may be host or device memory) ---------------- */
+/* FP32: pos/vel are n x 3 interleaved xyz, type 0 liquid / 1 gas, volume. */
+PFGPU_API int pf_upload_particles(pf_ctx* ctx, size_t n, const float* pos, const float* vel,
+                        const uint8_t* type, const float* volume);
+PFGPU_API int pf_download_particles(pf_ctx* ctx, float* pos, float* vel, uint8_t* type, float* volume);
+/* FP64: the reference's Particles3DTP layout (std::vector<Vec3> = n x 3 doubles). */
+PFGPU_API int pf_upload_particles_f64(pf_ctx* ctx, size_t n, const double* pos, const double* vel,
+                            const uint8_t* type, const double* volume);
+PFGPU_API int pf_download_particles_f64(pf_ctx* ctx, double* pos, double* vel, uint8_t* type,
+                              double* volume);
+PFGPU_API size_t pf_num_particles(const pf_ctx* ctx);
+
+/* ---- grid access (dense host/device arrays over the field's own lattice:
+ *      u (nx+1,ny,nz), v (nx,ny+1,nz), w (nx,ny,nz+1), mu/mv/mw alike,
+ *      p and mk (nx,ny,nz); index i + X*(j + Y*k); act4 holds one byte per
+ *      4^3 block, bid = bx + nbx*(by + nby*bz), nbx = ceil(X/4)).  The
+ *      marker field mk is exchanged as float 0 air / 1 fluid / 2 solid. --- */
+PFGPU_API int pf_grid_set_field(pf_ctx* ctx, int field, const float* dense, const uint8_t* act4);
+PFGPU_API int pf_grid_get_field(pf_ctx* ctx, int field, float* dense, uint8_t* act4);
+PFGPU_API int pf_grid_clear_field(pf_ctx* ctx, int field);
+PFGPU_API int pf_grid_clear_all(pf_ctx* ctx);
+/* Copy every field (values and activity) of src into dst (same lattice). */
+PFGPU_API int pf_grid_copy(pf_ctx* dst, const pf_ctx* src);
+/* Sorted 4^3 block ids active in a field; ids may be NULL to query *n. */
+PFGPU_API int pf_active_blocks4(pf_ctx* ctx, int field, int32_t* ids, size_t* n);
+/* Cells with marker 1 as ascending linear indices i + nx*(j + ny*k). */
+PFGPU_API int pf_active_cells(pf_ctx* ctx, int32_t* cells, size_t* n);
+PFGPU_API int pf_active_tiles(const pf_ctx* ctx);
+
+/* ---- solver step pieces ------------------------------------------------ */
+PFGPU_API int pf_mark_cells(pf_ctx* ctx);
+PFGPU_API int pf_p2g(pf_ctx* ctx, const pf_phase* phase, double Vp);
+PFGPU_API int pf_save_velocity(pf_ctx* ctx);
+PFGPU_API int pf_apply_gravity(pf_ctx* ctx, double dt, double gravity);
+PFGPU_API int pf_apply_wall_boundary(pf_ctx* ctx);
+PFGPU_API int pf_project(pf_ctx* ctx, const pf_phase* phase, double dt, const pf_solve_cfg* cfg,
+               pf_solve_stats* stats);
+/* saved: context holding the pre-force grid, or NULL for the copy taken by
+ * pf_save_velocity on ctx itself. */
+PFGPU_API int pf_g2p(pf_ctx* ctx, const pf_ctx* saved, double alpha_l, double alpha_g);
+/* escape (optional, host or device, capacity n x 8 doubles): per clamped
+ * particle {type, x, y, z, vx, vy, vz, volume} in particle order. */
+PFGPU_API int pf_advect(pf_ctx* ctx, double dt, int order, pf_clamp_stats* stats, double* escape,
+              size_t* n_escape);
+/* One full step in the reference's step() order, device-resident. */
+PFGPU_API int pf_step(pf_ctx* ctx, const pf_step_cfg* cfg, pf_step_stats* stats);
+
+/* ---- per-stage device timing (CUDA events on the context stream) -------
+ * Off by default.  When on, every solver-step entry point brackets its
+ * stages with events; pf_get_timing synchronises and returns the summed
+ * device milliseconds and launch counts per stage since the last reset. */
+enum pf_stage {
+  PF_STAGE_BIN = 0,      /* particle binning + exact 4^3 activation + pool growth */
+  PF_STAGE_SORT,         /* tile offsets scan + particle permutation */
+  PF_STAGE_SPLAT,        /* P2G splat kernel */
+  PF_STAGE_NORMALIZE,    /* momentum / mass (+ saved copy, gravity) */
+  PF_STAGE_MARK,         /* markCells */
+  PF_STAGE_BOUNDARY,     /* gravity, walls, saved copy */
+  PF_STAGE_PROJECT,      /* whole projection */
+  PF_STAGE_PCG,          /* iterative solve only */
+  PF_STAGE_G2P,          /* G2P and/or advection */
+  PF_NSTAGES
+};
+typedef struct {
+  double ms[PF_NSTAGES];
+  long long count[PF_NSTAGES];
+} pf_timing;
+PFGPU_API int pf_set_timing(pf_ctx* ctx, int enable);
+/* Number of kernels this context has launched since it was created. */
+PFGPU_API long long pf_launch_count(const pf_ctx* ctx);
+PFGPU_API int pf_get_timing(pf_ctx* ctx, pf_timing* out, int reset);
+
+/* calibrateRhoTilde0 (src/transfer/transfer3d_tp.cpp:29-36), on the device. */
+PFGPU_API int pf_calibrate_rho_tilde0(pf_ctx* ctx, const pf_phase* phase, double Vp, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PFGPU_H */

@@ -1,0 +1,157 @@
+"""GPU projection and full-step parity against the CPU oracle.
+
+Restates tests/test_sparse_vc3d.cpp (divergence removal, c_div target,
+pressure block count) on the GPU drop-in, then compares the GPU solve with the
+oracle on identical grids and the full step over 10 steps.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from gpu_helpers import compare_grids, phase_for, rel_err, scene_particles, to_oracle_phase
+
+pytestmark = pytest.mark.gpu
+
+
+def _box_grid(pf, with_u):
+    g = pf.SparseMacGrid3D(8, 8, 8, 1.0)
+    mk = np.zeros((8, 8, 8), np.float32)
+    mk[[0, -1], :, :] = 2
+    mk[:, [0, -1], :] = 2
+    mk[:, :, [0, -1]] = 2
+    mk[2:6, 2:6, 2:6] = 1
+    g.set_cells(mk)
+    mu = np.zeros((8, 8, 9), np.float32)
+    mu[2:6, 2:6, 2:7] = 1.0
+    mv = np.zeros((8, 9, 8), np.float32)
+    mv[2:6, 2:6, 2:6] = 1.0
+    mw = np.zeros((9, 8, 8), np.float32)
+    mw[2:6, 2:6, 2:6] = 1.0
+    mw[2:7, 2:6, 2:6] = 1.0
+    g.set_values(pf.PF_MU, mu)
+    g.set_values(pf.PF_MV, mv)
+    g.set_values(pf.PF_MW, mw)
+    if with_u:
+        u = np.zeros((8, 8, 9), np.float32)
+        for i in range(2, 7):
+            u[2:6, 2:6, i] = float(i)
+        g.set_values(pf.PF_U, u)
+    return g
+
+
+def _div(g, pf):
+    u, _ = g.get_field(pf.PF_U)
+    v, _ = g.get_field(pf.PF_V)
+    w, _ = g.get_field(pf.PF_W)
+    u, v, w = (a.astype(np.float64) for a in (u, v, w))
+    d = (u[2:6, 2:6, 3:7] - u[2:6, 2:6, 2:6]) + (v[2:6, 3:7, 2:6] - v[2:6, 2:6, 2:6]) + \
+        (w[3:7, 2:6, 2:6] - w[2:6, 2:6, 2:6])
+    return d
+
+
+@pytest.mark.parametrize("mode", ["plain", "mixed", "mixed_bf16"])
+def test_vc_projection_removes_divergence(pf, mode):
+    # tests/test_sparse_vc3d.cpp:8-54
+    g = _box_grid(pf, True)
+    pp = pf.PhaseParams()
+    solver = pf.SolverConfig(mode=pf.PF_SOLVER_PLAIN if mode == "plain" else pf.PF_SOLVER_MIXED,
+                             bf16_storage=(mode == "mixed_bf16"))
+    st = pf.spProjectStepVC3D(g, pp, 1.0, 1000, 1e-9, solver=solver)
+    assert st.converged
+    assert np.max(np.abs(_div(g, pf))) < 1e-4
+    assert g.activeCellBlocks() == 8
+
+
+def test_vc_projection_preserves_target_cdiv(pf):
+    # tests/test_sparse_vc3d.cpp:56-100
+    g = _box_grid(pf, False)
+    pf.spProjectStepVC3D(g, pf.PhaseParams(), 1.0, 1000, 1e-9, 0.125)
+    assert _div(g, pf).mean() == pytest.approx(0.125, rel=1e-4)
+
+
+def _stepped_grid(pf, n, seed):
+    """RT scene after markCells + P2G + gravity + walls, on both sides."""
+    sc = pf.scenes.rayleigh_taylor(n, seed=seed)
+    rng = np.random.default_rng(seed)
+    sc["vel"] = rng.normal(0, 0.3, sc["pos"].shape).astype(np.float32)
+    pp = phase_for(sc, pf)
+    ps = scene_particles(sc)
+    o = O.Oracle()
+    go = O.OracleGrid(n, n, n, 1.0 / n)
+    o.mark_cells(go, ps)
+    o.p2g(go, ps, to_oracle_phase(pp), 1.0)
+    o.apply_gravity(go, 1 / 240, -9.81)
+    o.apply_wall_boundary(go)
+    g = pf.SparseMacGrid3D(n, n, n, 1.0 / n)
+    for f in range(8):
+        g.set_field(f, *go.get_field(f))
+    return g, go, pp
+
+
+@pytest.mark.parametrize("n", [16, 24])
+def test_projection_matches_oracle(pf, n):
+    g, go, pp = _stepped_grid(pf, n, seed=n)
+    dt = 1 / 240
+    st = pf.spProjectStepVC3D(g, pp, dt, 2000, 0.0, solver=pf.SolverConfig(rel_tol=1e-10))
+    sto = O.Oracle().project(go, to_oracle_phase(pp), dt, 2000, 0.0, rel_tol=1e-10)
+    assert st.converged and sto.converged
+    assert st.pin_cell == sto.pin_cell
+    assert st.n_cells == sto.n_cells
+    assert abs(st.iterations - sto.iterations) <= max(3, sto.iterations // 20)
+    res = compare_grids(g, go, (0, 1, 2, 6))
+    for name, (err, nact) in res.items():
+        assert nact == 0, f"{name}: activity differs"
+        assert err < 1e-5, f"{name}: {err}"
+
+
+def test_projection_reference_tolerance_rule(pf):
+    """Absolute max-norm stop (cg_tol) with the reference's default 1e-7."""
+    g, go, pp = _stepped_grid(pf, 16, seed=4)
+    st = pf.spProjectStepVC3D(g, pp, 1 / 240, 600, 1e-7)
+    sto = O.Oracle().project(go, to_oracle_phase(pp), 1 / 240, 600, 1e-7)
+    assert st.converged == sto.converged
+    assert st.res_final < 1e-7
+    assert abs(st.iterations - sto.iterations) <= 3
+
+
+@pytest.mark.parametrize("mode,bf16", [(1, False), (1, True)])
+def test_mixed_solver_matches_fp64_oracle(pf, mode, bf16):
+    n = 24
+    g, go, pp = _stepped_grid(pf, n, seed=9)
+    dt = 1 / 240
+    st = pf.spProjectStepVC3D(g, pp, dt, 4000, 0.0,
+                              solver=pf.SolverConfig(mode=mode, rel_tol=1e-6, bf16_storage=bf16))
+    sto = O.Oracle().project(go, to_oracle_phase(pp), dt, 4000, 0.0, rel_tol=1e-12)
+    assert st.converged
+    assert st.res_final <= 1e-6 * st.res0
+    pg, _ = g.get_field(pf.PF_P)
+    po, _ = go.get_field(O.P)
+    assert rel_err(pg, po) < 2e-5
+
+
+def test_full_step_ten_steps_match_oracle(pf):
+    n = 16
+    sc = pf.scenes.rayleigh_taylor(n, seed=1)
+    pp = phase_for(sc, pf)
+    ps = scene_particles(sc)
+    sim = pf.SparseSim3DTP(n, n, n, 1.0 / n, max_particles=len(ps))
+    sim.phase = pp
+    sim.dt = 1 / 240
+    sim.alpha_liquid = sim.alpha_gas = 0.95
+    sim.cg_iters, sim.cg_tol = 2000, 0.0
+    sim.solver = pf.SolverConfig(rel_tol=1e-8)
+    sim.set_particles(sc["pos"], sc["vel"], sc["type"], sc["volume"])
+    o = O.Oracle()
+    go, so = O.OracleGrid(n, n, n, 1.0 / n), O.OracleGrid(n, n, n, 1.0 / n)
+    cfg = dict(dt=1 / 240, gravity=-9.81, Vp=1.0, alpha_l=0.95, alpha_g=0.95, cg_iters=2000, cg_tol=0.0,
+               cg_rel_tol=1e-8)
+    for step in range(10):
+        sim.step()
+        o.step(go, so, ps, to_oracle_phase(pp), cfg)
+        pos, vel, _, _ = sim.get_particles()
+        assert np.max(np.abs(pos - ps.pos)) < 1e-5 / n, f"step {step}"
+        assert rel_err(vel, ps.vel) < 1e-4, f"step {step}"
+        res = compare_grids(sim.grid, go, range(8))
+        for name, (err, nact) in res.items():
+            assert err < 1e-4, f"step {step} {name}: {err}"
+            assert nact == 0, f"step {step} {name}: {nact} activity flags differ"

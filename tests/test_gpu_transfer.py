@@ -1,0 +1,185 @@
+"""GPU transfer parity: libpfgpu through the C ABI versus the CPU oracle.
+
+The first group restates the reference's own transfer tests
+(tests/test_sparse_transfer3d_tp.cpp, tests/test_transfer3d_tp.cpp) against
+the GPU drop-ins; the second compares whole fields and activity sets on seeded
+scenes.  Tolerances: field values within 1e-5 of the field's scale (FP32
+weights/accumulation against the reference's FP64 weights), active 4^3 block
+sets and marker/cell lists bit-exact.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from gpu_helpers import compare_grids, phase_for, rel_err, scene_particles, to_oracle_phase
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+
+
+def test_p2g_conserves_normalized_cubic_momentum(pf):
+    # tests/test_sparse_transfer3d_tp.cpp:11-29
+    g = pf.SparseMacGrid3D(8, 8, 8, 1.0)
+    pp = pf.PhaseParams()
+    ps = pf.Particles3DTP()
+    ps.add((3.0, 2.5, 2.5), (4.0, 3.0, 2.0), 0)
+    pf.spP2G3D_tp(g, ps, pp, 1.0)
+    u, _ = g.get_field(pf.PF_U)
+    mu, _ = g.get_field(pf.PF_MU)
+    mom = float((u.astype(np.float64) * mu.astype(np.float64)).sum())
+    assert mom == pytest.approx(4.0, rel=1e-6)
+    n_act = g.activeBlockCount(pf.PF_MU)
+    assert 0 < n_act < 3 * 2 * 2  # total u-field blocks of an 8^3 grid: ceil(9/4)*2*2
+
+
+def test_p2g_separates_liquid_and_gas(pf):
+    # tests/test_sparse_transfer3d_tp.cpp:31-58
+    g = pf.SparseMacGrid3D(8, 8, 8, 1.0, max_particles=4096)
+    pp = pf.PhaseParams()
+    ps = pf.Particles3DTP()
+    pos, typ = [], []
+    for k in range(1, 7):
+        for j in range(1, 7):
+            for i in range(1, 7):
+                for s in range(8):
+                    pos.append((i + 0.25 + 0.5 * (s & 1), j + 0.25 + 0.5 * ((s >> 1) & 1), k + 0.25 + 0.5 * ((s >> 2) & 1)))
+                    typ.append(0 if j < 4 else 1)
+    ps = pf.Particles3DTP(np.array(pos), np.zeros((len(pos), 3)), np.array(typ), np.ones(len(pos)))
+    pp.rho_tilde_0 = pf.calibrateRhoTilde0(pp, 1.0)
+    pf.spP2G3D_tp(g, ps, pp, 1.0)
+    mu, _ = g.get_field(pf.PF_MU)
+    assert pf.phiFromRawDensity(float(mu[3, 2, 4]), pp) > 0.8
+    assert pf.phiFromRawDensity(float(mu[3, 5, 4]), pp) < 0.2
+
+
+def test_g2p_uses_phase_specific_flip_alpha(pf):
+    # tests/test_sparse_transfer3d_tp.cpp:60-78
+    g = pf.SparseMacGrid3D(8, 8, 8, 1.0)
+    saved = pf.SparseMacGrid3D(8, 8, 8, 1.0)
+    ug = np.zeros((8, 8, 9), np.float32)
+    us = np.zeros((8, 8, 9), np.float32)
+    ug[1:3, 1:3, 2:4] = 5.0
+    us[1:3, 1:3, 2:4] = 2.0
+    g.set_values(pf.PF_U, ug)
+    saved.set_values(pf.PF_U, us)
+    ps = pf.Particles3DTP()
+    ps.add((2.0, 2.0, 2.0), (10.0, 0.0, 0.0), 0)
+    ps.add((2.0, 2.0, 2.0), (10.0, 0.0, 0.0), 1)
+    pf.spG2P3D_tp(g, ps, saved, 1.0, 0.0)
+    assert ps.vel[0, 0] == pytest.approx(13.0, rel=1e-6)
+    assert ps.vel[1, 0] == pytest.approx(5.0, rel=1e-6)
+
+
+def test_advect_reports_phase_boundary_clamps(pf):
+    # tests/test_sparse_transfer3d_tp.cpp:123-161
+    g = pf.SparseMacGrid3D(8, 8, 8, 1.0)
+    g.set_values(pf.PF_U, np.full((8, 8, 9), 10.0, np.float32))
+    g.set_values(pf.PF_V, np.full((8, 9, 8), -10.0, np.float32))
+    ps = pf.Particles3DTP()
+    ps.add((7.45, 4.0, 4.0), (0.0, 0.0, 0.0), 0)
+    ps.add((4.0, 0.55, 4.0), (0.0, 0.0, 0.0), 1)
+    stats = pf.ParticleEscapeStats3D()
+    buf = pf.ParticleEscapeBuffer3D()
+    pf.spAdvect3D_tp(ps, g, 0.1, stats, 2, buf)
+    assert ps.pos[0, 0] == pytest.approx(7.5, rel=1e-7)
+    assert ps.pos[1, 1] == pytest.approx(0.5, rel=1e-7)
+    assert (stats.clamped_liquid, stats.clamped_gas) == (1, 1)
+    assert stats.clamped_x_hi == 1 and stats.clamped_y_lo == 1
+    assert stats.clamped_total() == 2
+    assert stats.droplet_candidates() == 1 and stats.bubble_candidates() == 1
+    assert len(buf.records) == 2
+    assert buf.droplet_count() == 1 and buf.bubble_count() == 1
+    assert buf.records[0]["type"] == 0 and buf.records[0]["pos"][0] == pytest.approx(7.5, rel=1e-7)
+    assert buf.records[0]["volume"] == pytest.approx(1.0)
+    assert buf.records[1]["type"] == 1 and buf.records[1]["pos"][1] == pytest.approx(0.5, rel=1e-7)
+
+
+def test_advect_rk3_follows_linear_field(pf):
+    # tests/test_sparse_transfer3d_tp.cpp:163-180
+    g = pf.SparseMacGrid3D(8, 8, 8, 1.0)
+    u = np.broadcast_to(np.arange(9, dtype=np.float32), (8, 8, 9)).copy()
+    g.set_values(pf.PF_U, u)
+    g.set_field(pf.PF_U, u, np.ones(g.bdims(pf.PF_U)[::-1], np.uint8))
+    ps = pf.Particles3DTP()
+    ps.add((2.0, 4.0, 4.0), (0.0, 0.0, 0.0), 0)
+    pf.spAdvect3D_tp(ps, g, 0.1, None, 3)
+    expected = 2.0 + 0.1 / 6.0 * (2.0 + 4.0 * 2.1 + 2.22)
+    assert ps.pos[0, 0] == pytest.approx(expected, rel=1e-6)
+    assert ps.pos[0, 1] == pytest.approx(4.0, rel=1e-7)
+    assert ps.pos[0, 2] == pytest.approx(4.0, rel=1e-7)
+
+
+def test_calibrate_rho_tilde0_bit_exact(pf):
+    o = O.Oracle()
+    for rl, rg in ((1.0, 0.01), (1000.0, 1.0)):
+        pp = pf.PhaseParams(rl, rg)
+        assert pf.calibrateRhoTilde0(pp, 1.0) == o.calibrate_rho_tilde0(O.PhaseParams(rl, rg), 1.0)
+
+
+@pytest.mark.parametrize("scene,n", [("rt", 16), ("rt", 24), ("bubble", 16)])
+def test_p2g_fields_and_active_sets_match_oracle(pf, scene, n):
+    sc = pf.scenes.rayleigh_taylor(n, seed=3) if scene == "rt" else pf.scenes.bubble_tank(n, seed=5)
+    if scene == "rt":
+        rng = np.random.default_rng(7)
+        sc["vel"] = rng.normal(0, 0.2, sc["pos"].shape).astype(np.float32)
+    pp = phase_for(sc, pf)
+    ps = scene_particles(sc)
+    g = pf.SparseMacGrid3D(n, n, n, 1.0 / n, max_particles=len(ps))
+    pf.spP2G3D_tp(g, ps, pp, 1.0)
+    o = O.Oracle()
+    go = O.OracleGrid(n, n, n, 1.0 / n)
+    o.p2g(go, ps, to_oracle_phase(pp), 1.0)
+    res = compare_grids(g, go, range(6))
+    for name, (err, nact) in res.items():
+        assert nact == 0, f"{name}: {nact} 4^3 activity flags differ"
+        assert err < TOL, f"{name}: relative error {err}"
+
+
+def test_mark_cells_matches_oracle(pf):
+    n = 16
+    sc = pf.scenes.bubble_tank(n, seed=2)
+    ps = scene_particles(sc)
+    sim = pf.SparseSim3DTP(n, n, n, 1.0 / n, max_particles=len(ps))
+    sim.set_particles(sc["pos"], sc["vel"], sc["type"], sc["volume"])
+    from adaptive_pf_flip_b200 import _lib as L
+    L.check(sim.grid.lib.pf_mark_cells(sim.grid.ctx), sim.grid.ctx, "pf_mark_cells")
+    o = O.Oracle()
+    go = O.OracleGrid(n, n, n, 1.0 / n)
+    o.mark_cells(go, ps)
+    dg, ag = sim.grid.get_field(pf.PF_MK)
+    dc, ac = go.get_field(O.MK)
+    assert np.array_equal(dg, dc)
+    assert np.array_equal(ag, ac)
+    assert np.array_equal(sim.grid.fluid_cells(), go.fluid_cells())
+
+
+def test_g2p_and_advect_match_oracle(pf):
+    n = 16
+    sc = pf.scenes.bubble_tank(n, seed=11)
+    pp = phase_for(sc, pf)
+    ps = scene_particles(sc)
+    g = pf.SparseMacGrid3D(n, n, n, 1.0 / n, max_particles=len(ps))
+    pf.spP2G3D_tp(g, ps, pp, 1.0)
+    saved = g.copy()
+    # perturb the live grid so FLIP and PIC differ
+    for f in (pf.PF_U, pf.PF_V, pf.PF_W):
+        d, a = g.get_field(f)
+        rng = np.random.default_rng(f)
+        d = (d + rng.normal(0, 0.05, d.shape).astype(np.float32) * (d != 0)).astype(np.float32)
+        g.set_field(f, d, a)
+    o = O.Oracle()
+    go = O.OracleGrid(n, n, n, 1.0 / n)
+    so = O.OracleGrid(n, n, n, 1.0 / n)
+    for f in range(8):
+        go.set_field(f, *g.get_field(f))
+        so.set_field(f, *saved.get_field(f))
+    ps_g, ps_o = ps.copy(), ps.copy()
+    pf.spG2P3D_tp(g, ps_g, saved, 0.97, 0.9)
+    o.g2p(go, ps_o, so, 0.97, 0.9)
+    assert rel_err(ps_g.vel, ps_o.vel) < TOL
+    st_g = pf.ParticleEscapeStats3D()
+    pf.spAdvect3D_tp(ps_g, g, 1.0 / 60.0, st_g, 2)
+    st_o = o.advect(ps_o, go, 1.0 / 60.0, 2)
+    assert np.max(np.abs(ps_g.pos - ps_o.pos)) < 1e-5 / n
+    assert (st_g.clamped_liquid, st_g.clamped_gas) == (st_o.clamped_liquid, st_o.clamped_gas)
