@@ -79,6 +79,7 @@ int create_impl(pf_ctx* ctx, const pf_grid_desc* d) {
   Geom& g = ctx->g;
   g.nx = d->nx; g.ny = d->ny; g.nz = d->nz;
   g.dx = d->dx; g.ox = d->ox; g.oy = d->oy; g.oz = d->oz;
+  g.inv_dx = 1.0 / d->dx;
   g.TX = (d->nx + 1 + 7) / 8; g.TY = (d->ny + 1 + 7) / 8; g.TZ = (d->nz + 1 + 7) / 8;
   g.ntiles = g.TX * g.TY * g.TZ;
   const int dims[PF_NFIELDS][3] = {{g.nx + 1, g.ny, g.nz}, {g.nx, g.ny + 1, g.nz}, {g.nx, g.ny, g.nz + 1},

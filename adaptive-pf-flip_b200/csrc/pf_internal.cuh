@@ -31,6 +31,7 @@ struct Geom {
   int TX, TY, TZ;  // tile lattice
   int ntiles;
   double dx, ox, oy, oz;
+  double inv_dx;            // 1/dx, for coordinates that need not round as the reference's
   int fdim[PF_NFIELDS][3];  // node lattice per field
   int bdim[PF_NFIELDS][3];  // 4^3 block lattice per field
 };

@@ -39,46 +39,61 @@ __device__ __forceinline__ double grid_coord(float p, double o, double dx) {
 // smallest rounded d^2, and rounding is monotone, so testing the per-axis
 // minima decides "some node of this block has w > 0" exactly.
 // ---------------------------------------------------------------------------
-__device__ void activate_window(const DevGrid& G, int fv, double c0, double c1, double c2,
-                                uint8_t* need) {
-  const double c[3] = {c0, c1, c2};
-  int nb[3];
-  int blk[3][2];
-  double m2[3][2];
+// Per axis: the (at most two) 4-node blocks holding the in-lattice candidates
+// i0-1..i0+2 and, for each, the smallest rounded d^2 = fl((c - i)^2).
+struct AxisBlocks {
+  int b0, nb;
+  double m0, m1;
+};
+
+__device__ __forceinline__ AxisBlocks axis_blocks(double c, int dim) {
+  const int i0 = (int)floor(c);
+  const int lo = max(i0 - 1, 0), hi = min(i0 + 2, dim - 1);
+  AxisBlocks r;
+  r.b0 = lo >> 2;
+  r.nb = lo > hi ? 0 : (hi >> 2) - (lo >> 2) + 1;
+  r.m0 = r.m1 = 1e300;
 #pragma unroll
-  for (int ax = 0; ax < 3; ++ax) {
-    const int dim = G.g.fdim[fv][ax];
-    const int i0 = (int)floor(c[ax]);
-    nb[ax] = 0;
-#pragma unroll
-    for (int o = -1; o <= 2; ++o) {
-      const int i = i0 + o;
-      if (i < 0 || i >= dim) continue;
-      const double d = __dsub_rn(c[ax], (double)i);
-      const double dd = __dmul_rn(d, d);
-      const int b = i >> 2;
-      if (nb[ax] > 0 && blk[ax][nb[ax] - 1] == b) {
-        if (dd < m2[ax][nb[ax] - 1]) m2[ax][nb[ax] - 1] = dd;
-      } else {
-        blk[ax][nb[ax]] = b;
-        m2[ax][nb[ax]] = dd;
-        ++nb[ax];
-      }
+  for (int o = 0; o < 4; ++o) {
+    const int i = i0 - 1 + o;
+    const double d = __dsub_rn(c, (double)i);
+    const double dd = __dmul_rn(d, d);
+    if (i >= lo && i <= hi) {
+      if ((i >> 2) == r.b0) r.m0 = fmin(r.m0, dd);
+      else r.m1 = fmin(r.m1, dd);
     }
   }
+  return r;
+}
+
+__device__ __forceinline__ void activate_window(const DevGrid& G, int fv, double c0, double c1, double c2,
+                                                uint8_t* need) {
+  const AxisBlocks ax = axis_blocks(c0, G.g.fdim[fv][0]);
+  const AxisBlocks ay = axis_blocks(c1, G.g.fdim[fv][1]);
+  const AxisBlocks az = axis_blocks(c2, G.g.fdim[fv][2]);
   const int fm = fv + 3;
-  for (int z = 0; z < nb[2]; ++z)
-    for (int y = 0; y < nb[1]; ++y)
-      for (int x = 0; x < nb[0]; ++x) {
-        const double d2 = __dadd_rn(__dadd_rn(m2[0][x], m2[1][y]), m2[2][z]);
-        if (!(__ddiv_rn(d2, kR2) < 1.0)) continue;
-        const int bx = blk[0][x], by = blk[1][y], bz = blk[2][z];
+#pragma unroll
+  for (int z = 0; z < 2; ++z) {
+    if (z >= az.nb) continue;
+#pragma unroll
+    for (int y = 0; y < 2; ++y) {
+      if (y >= ay.nb) continue;
+#pragma unroll
+      for (int x = 0; x < 2; ++x) {
+        if (x >= ax.nb) continue;
+        // kern(d2) > 0  <=>  fl(d2 / 2.25) < 1  <=>  d2 < 2.25 (the quotient of
+        // the largest double below 2.25 still rounds below 1)
+        const double d2 = __dadd_rn(__dadd_rn(x ? ax.m1 : ax.m0, y ? ay.m1 : ay.m0), z ? az.m1 : az.m0);
+        if (!(d2 < kR2)) continue;
+        const int bx = ax.b0 + x, by = ay.b0 + y, bz = az.b0 + z;
         const int bi = bx + G.g.bdim[fv][0] * (by + G.g.bdim[fv][1] * bz);
         if (!G.act4[fv][bi]) G.act4[fv][bi] = 1;
         if (!G.act4[fm][bi]) G.act4[fm][bi] = 1;
         uint8_t* nd = &need[tile_id(G.g, bx >> 1, by >> 1, bz >> 1)];
         if (!*nd) *nd = 1;
       }
+    }
+  }
 }
 
 // One pass over the particles: tile key + warp-aggregated rank (binning),
@@ -167,21 +182,25 @@ __global__ void k_mark_particles(DevGrid G, const float* __restrict__ px, const 
 // ---------------------------------------------------------------------------
 // P2G splat: one CTA per tile holding particles
 // ---------------------------------------------------------------------------
+// Per axis of one face field: the first of the three candidate nodes (box-
+// local index) and d^2/r^2 for each (>= 1 when the node is off the lattice,
+// which removes it from the weight sum as the reference's bounds test does).
 struct AxisW {
-  int base;   // first candidate node
-  float a[3]; // d^2 / r^2 of the three candidates (>= 1 when out of the lattice)
+  int base;
+  float a[3];
 };
 
-__device__ __forceinline__ AxisW axis_weights(double c, int dim) {
+__device__ __forceinline__ AxisW axis_weights(float x, int lo, int hi) {
   AxisW w;
-  const int i0 = (int)floor(c);
-  const float fr = (float)(c - (double)i0);
+  const float f0 = floorf(x);
+  const int i0 = (int)f0;
+  const float fr = x - f0;
   w.base = fr < 0.5f ? i0 - 1 : i0;
 #pragma unroll
   for (int m = 0; m < 3; ++m) {
     const int i = w.base + m;
     const float d = fr + (float)(i0 - i);
-    w.a[m] = (i >= 0 && i < dim) ? d * d * (1.0f / 2.25f) : 2.0f;
+    w.a[m] = (i >= lo && i < hi) ? d * d * (1.0f / 2.25f) : 2.0f;
   }
   return w;
 }
@@ -191,75 +210,96 @@ __device__ __forceinline__ float cubic(float s) {
   return t > 0.0f ? t * t * t : 0.0f;
 }
 
-__global__ void __launch_bounds__(256) k_splat(DevGrid G, const int* __restrict__ tile_start,
-                                               const int* __restrict__ perm,
-                                               const float* __restrict__ px, const float* __restrict__ py,
-                                               const float* __restrict__ pz, const float* __restrict__ vx,
-                                               const float* __restrict__ vy, const float* __restrict__ vz,
-                                               const uint8_t* __restrict__ type,
-                                               const float* __restrict__ vol, double rho_l, double rho_g,
-                                               double Vp) {
-  extern __shared__ float sm[];  // [3 axes][mom, mass][kBox3]
+constexpr int kSplatThreads = 256;
+// Particles are staged in shared memory in batches of 256 and lane L of the
+// batch takes staged particle (L*33) mod 256: with particles grouped by cell,
+// the lanes of a warp then splat into disjoint node windows instead of
+// serialising on the same shared-memory addresses.
+constexpr int kSplatStride = 33;
+constexpr int kStageFields = 7;  // box-local x, y, z, mass, vx, vy, vz
+
+__global__ void __launch_bounds__(kSplatThreads) k_splat(DevGrid G, const int* __restrict__ tile_start,
+                                                         const int* __restrict__ perm,
+                                                         const float* __restrict__ px,
+                                                         const float* __restrict__ py,
+                                                         const float* __restrict__ pz,
+                                                         const float* __restrict__ vx,
+                                                         const float* __restrict__ vy,
+                                                         const float* __restrict__ vz,
+                                                         const uint8_t* __restrict__ type,
+                                                         const float* __restrict__ vol, float m_l, float m_g) {
+  extern __shared__ float sm[];  // [3 axes][mom, mass][kBox3], then the particle stage
+  float* stage = sm + 6 * kBox3;
   const int t = blockIdx.x;
   const int beg = tile_start[t], end = tile_start[t + 1];
   if (beg >= end) return;
-  for (int e = threadIdx.x; e < 6 * kBox3; e += blockDim.x) sm[e] = 0.0f;
-  __syncthreads();
+  for (int e = threadIdx.x; e < 6 * kBox3; e += kSplatThreads) sm[e] = 0.0f;
   const int tx = t % G.g.TX, tq = t / G.g.TX, ty = tq % G.g.TY, tz = tq / G.g.TY;
   const int o0 = tx * 8 - 2, o1 = ty * 8 - 2, o2 = tz * 8 - 2;
+  const double inv_dx = G.g.inv_dx;
 
-  for (int q = beg + threadIdx.x; q < end; q += blockDim.x) {
-    const int p = perm[q];
-    const double gx = grid_coord(px[p], G.g.ox, G.g.dx);
-    const double gy = grid_coord(py[p], G.g.oy, G.g.dx);
-    const double gz = grid_coord(pz[p], G.g.oz, G.g.dx);
-    const float mp = (float)((type[p] == 0 ? rho_l : rho_g) * Vp * (double)vol[p]);
-    const float vel[3] = {vx[p], vy[p], vz[p]};
+  for (int b0 = beg; b0 < end; b0 += kSplatThreads) {
+    const int q = b0 + threadIdx.x;
+    if (q < end) {
+      const int p = perm[q];
+      stage[0 * kSplatThreads + threadIdx.x] = (float)(((double)px[p] - G.g.ox) * inv_dx - o0);
+      stage[1 * kSplatThreads + threadIdx.x] = (float)(((double)py[p] - G.g.oy) * inv_dx - o1);
+      stage[2 * kSplatThreads + threadIdx.x] = (float)(((double)pz[p] - G.g.oz) * inv_dx - o2);
+      stage[3 * kSplatThreads + threadIdx.x] = (type[p] == 0 ? m_l : m_g) * vol[p];
+      stage[4 * kSplatThreads + threadIdx.x] = vx[p];
+      stage[5 * kSplatThreads + threadIdx.x] = vy[p];
+      stage[6 * kSplatThreads + threadIdx.x] = vz[p];
+    }
+    __syncthreads();
+    const int e = (threadIdx.x * kSplatStride) & (kSplatThreads - 1);
+    if (b0 + e < end) {
+      const float lx = stage[e], ly = stage[kSplatThreads + e], lz = stage[2 * kSplatThreads + e];
+      const float mp = stage[3 * kSplatThreads + e];
 #pragma unroll 1
-    for (int a = 0; a < 3; ++a) {
-      const int fv = PF_U + a;
-      const AxisW wx = axis_weights(a == 0 ? gx : gx - 0.5, G.g.fdim[fv][0]);
-      const AxisW wy = axis_weights(a == 1 ? gy : gy - 0.5, G.g.fdim[fv][1]);
-      const AxisW wz = axis_weights(a == 2 ? gz : gz - 0.5, G.g.fdim[fv][2]);
-      float w[27];
-      float wsum = 0.0f;
+      for (int a = 0; a < 3; ++a) {
+        const int fv = PF_U + a;
+        const AxisW wx = axis_weights(a == 0 ? lx : lx - 0.5f, -o0, G.g.fdim[fv][0] - o0);
+        const AxisW wy = axis_weights(a == 1 ? ly : ly - 0.5f, -o1, G.g.fdim[fv][1] - o1);
+        const AxisW wz = axis_weights(a == 2 ? lz : lz - 0.5f, -o2, G.g.fdim[fv][2] - o2);
+        float w[27];
+        float wsum = 0.0f;
 #pragma unroll
-      for (int c = 0; c < 3; ++c)
+        for (int c = 0; c < 3; ++c)
 #pragma unroll
-        for (int b = 0; b < 3; ++b)
+          for (int b = 0; b < 3; ++b)
 #pragma unroll
-          for (int e = 0; e < 3; ++e) {
-            const float v = cubic(wx.a[e] + wy.a[b] + wz.a[c]);
-            w[(c * 3 + b) * 3 + e] = v;
-            wsum += v;
-          }
-      if (!(wsum > 0.0f)) continue;
-      const float inv = 1.0f / wsum;
-      const float mom = mp * vel[a];
-      float* smom = sm + (2 * a) * kBox3;
-      float* smas = sm + (2 * a + 1) * kBox3;
-      const int lx = wx.base - o0, ly = wy.base - o1, lz = wz.base - o2;
+            for (int d = 0; d < 3; ++d) {
+              const float v = cubic(wx.a[d] + wy.a[b] + wz.a[c]);
+              w[(c * 3 + b) * 3 + d] = v;
+              wsum += v;
+            }
+        if (!(wsum > 0.0f)) continue;
+        const float inv = 1.0f / wsum;
+        const float mom = mp * stage[(4 + a) * kSplatThreads + e];
+        float* smom = sm + (2 * a) * kBox3;
+        float* smas = sm + (2 * a + 1) * kBox3;
 #pragma unroll
-      for (int c = 0; c < 3; ++c)
+        for (int c = 0; c < 3; ++c)
 #pragma unroll
-        for (int b = 0; b < 3; ++b)
+          for (int b = 0; b < 3; ++b)
 #pragma unroll
-          for (int e = 0; e < 3; ++e) {
-            const float wn = w[(c * 3 + b) * 3 + e] * inv;
-            if (wn > 0.0f) {
-              const int X = lx + e, Y = ly + b, Z = lz + c;
-              if ((unsigned)X < (unsigned)kBox && (unsigned)Y < (unsigned)kBox && (unsigned)Z < (unsigned)kBox) {
-                const int si = X + kBox * (Y + kBox * Z);
-                atomicAdd(&smom[si], wn * mom);
-                atomicAdd(&smas[si], wn * mp);
+            for (int d = 0; d < 3; ++d) {
+              const float wn = w[(c * 3 + b) * 3 + d] * inv;
+              if (wn > 0.0f) {
+                const int X = wx.base + d, Y = wy.base + b, Z = wz.base + c;
+                if ((unsigned)X < (unsigned)kBox && (unsigned)Y < (unsigned)kBox && (unsigned)Z < (unsigned)kBox) {
+                  const int si = X + kBox * (Y + kBox * Z);
+                  atomicAdd(&smom[si], wn * mom);
+                  atomicAdd(&smas[si], wn * mp);
+                }
               }
             }
-          }
+      }
     }
+    __syncthreads();
   }
-  __syncthreads();
   // add the box into the pooled fields (neighbouring tiles overlap in halos)
-  for (int e = threadIdx.x; e < 3 * kBox3; e += blockDim.x) {
+  for (int e = threadIdx.x; e < 3 * kBox3; e += kSplatThreads) {
     const int a = e / kBox3, si = e - a * kBox3;
     const float mom = sm[(2 * a) * kBox3 + si], mas = sm[(2 * a + 1) * kBox3 + si];
     if (mom == 0.0f && mas == 0.0f) continue;
@@ -363,6 +403,32 @@ __device__ __forceinline__ void sample2(const DevGrid& G, int a, double cx, doub
   const float fx = (float)(cx - i0), fy = (float)(cy - j0), fz = (float)(cz - k0);
   const float wx[2] = {1.0f - fx, fx}, wy[2] = {1.0f - fy, fy}, wz[2] = {1.0f - fz, fz};
   float s = 0.0f, so = 0.0f;
+  // common case: all eight nodes inside the lattice and inside one tile
+  if (i0 >= 0 && j0 >= 0 && k0 >= 0 && i0 + 1 < X && j0 + 1 < Y && k0 + 1 < Z && (i0 & 7) != 7 &&
+      (j0 & 7) != 7 && (k0 & 7) != 7) {
+    const int sl = slot_of(G, i0, j0, k0);
+    if (sl < 0) {
+      cur = 0.0f;
+      old = 0.0f;
+      return;
+    }
+    const float* f = G.fld[fv] + (size_t)sl * PF_TV + local_id(i0, j0, k0);
+    const float* h = G.saved[a] + (size_t)sl * PF_TV + local_id(i0, j0, k0);
+#pragma unroll
+    for (int dk = 0; dk < 2; ++dk)
+#pragma unroll
+      for (int dj = 0; dj < 2; ++dj)
+#pragma unroll
+        for (int di = 0; di < 2; ++di) {
+          const int off = di + 8 * dj + 64 * dk;
+          const float w = wx[di] * wy[dj] * wz[dk];
+          s += w * __ldg(f + off);
+          if (kSaved) so += w * __ldg(h + off);
+        }
+    cur = s;
+    old = so;
+    return;
+  }
 #pragma unroll
   for (int dk = 0; dk < 2; ++dk)
 #pragma unroll
@@ -390,10 +456,15 @@ __device__ __forceinline__ float sample1(const DevGrid& G, int a, double cx, dou
   return c;
 }
 
+// (pos - o) / dx as a product with the reciprocal: G2P and advection only need
+// it to within rounding, unlike the activation test.
+__device__ __forceinline__ double to_grid(double p, double o, double inv_dx) { return (p - o) * inv_dx; }
+
 __device__ __forceinline__ void velocity_at(const DevGrid& G, double x, double y, double z, double out[3]) {
-  const double gx = __ddiv_rn(__dsub_rn(x, G.g.ox), G.g.dx);
-  const double gy = __ddiv_rn(__dsub_rn(y, G.g.oy), G.g.dx);
-  const double gz = __ddiv_rn(__dsub_rn(z, G.g.oz), G.g.dx);
+  const double inv_dx = G.g.inv_dx;
+  const double gx = to_grid(x, G.g.ox, inv_dx);
+  const double gy = to_grid(y, G.g.oy, inv_dx);
+  const double gz = to_grid(z, G.g.oz, inv_dx);
   out[0] = sample1(G, 0, gx, gy - 0.5, gz - 0.5);
   out[1] = sample1(G, 1, gx - 0.5, gy, gz - 0.5);
   out[2] = sample1(G, 2, gx - 0.5, gy - 0.5, gz);
@@ -410,9 +481,9 @@ template <bool kExternal>
 __global__ void __launch_bounds__(256) k_g2p(DevGrid G, DevGrid S, ParticlePtrs P, int n, double aL, double aG) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
-  const double gx = grid_coord(P.px[p], G.g.ox, G.g.dx);
-  const double gy = grid_coord(P.py[p], G.g.oy, G.g.dx);
-  const double gz = grid_coord(P.pz[p], G.g.oz, G.g.dx);
+  const double gx = to_grid((double)P.px[p], G.g.ox, G.g.inv_dx);
+  const double gy = to_grid((double)P.py[p], G.g.oy, G.g.inv_dx);
+  const double gz = to_grid((double)P.pz[p], G.g.oz, G.g.inv_dx);
   const double c[3][3] = {{gx, gy - 0.5, gz - 0.5}, {gx - 0.5, gy, gz - 0.5}, {gx - 0.5, gy - 0.5, gz}};
   const float a = P.type[p] == 0 ? (float)aL : (float)aG;
   float* vp[3] = {P.vx, P.vy, P.vz};
@@ -448,9 +519,9 @@ __global__ void __launch_bounds__(256) k_advect(DevGrid G, ParticlePtrs P, int n
     const double x0[3] = {(double)P.px[p], (double)P.py[p], (double)P.pz[p]};
     double k1[3], k2[3], nx[3];
     if (fuse_g2p) {
-      const double gx = __ddiv_rn(__dsub_rn(x0[0], G.g.ox), G.g.dx);
-      const double gy = __ddiv_rn(__dsub_rn(x0[1], G.g.oy), G.g.dx);
-      const double gz = __ddiv_rn(__dsub_rn(x0[2], G.g.oz), G.g.dx);
+      const double gx = to_grid(x0[0], G.g.ox, G.g.inv_dx);
+      const double gy = to_grid(x0[1], G.g.oy, G.g.inv_dx);
+      const double gz = to_grid(x0[2], G.g.oz, G.g.inv_dx);
       const double c[3][3] = {{gx, gy - 0.5, gz - 0.5}, {gx - 0.5, gy, gz - 0.5}, {gx - 0.5, gy - 0.5, gz}};
       const float a = P.type[p] == 0 ? (float)aL : (float)aG;
       float* vp[3] = {P.vx, P.vy, P.vz};
@@ -629,10 +700,10 @@ static int p2g_core(pf_ctx* ctx, const pf_phase* ph, double Vp) {
   }
   {
     StageScope sc(ctx, PF_STAGE_SPLAT);
-    const size_t smem = 6 * kBox3 * sizeof(float);
-    (++ctx->launches), k_splat<<<nt, 256, smem, ctx->stream>>>(dev_grid(ctx), ctx->tile_start, ctx->perm, ctx->px, ctx->py, ctx->pz,
-                                            ctx->vx, ctx->vy, ctx->vz, ctx->type, ctx->vol, ph->rho_l, ph->rho_g,
-                                            Vp);
+    const size_t smem = (6 * kBox3 + kStageFields * kSplatThreads) * sizeof(float);
+    (++ctx->launches), k_splat<<<nt, kSplatThreads, smem, ctx->stream>>>(
+        dev_grid(ctx), ctx->tile_start, ctx->perm, ctx->px, ctx->py, ctx->pz, ctx->vx, ctx->vy, ctx->vz, ctx->type,
+        ctx->vol, (float)(ph->rho_l * Vp), (float)(ph->rho_g * Vp));
     PF_CUDA_TRY(cudaGetLastError());
   }
   return PF_OK;

@@ -275,16 +275,19 @@ def run_ours(args, rank, world, local, dist):
     ts = TransferStep(pf, sc, local)
     n = ts.n
     # device-resident timing with per-stage events
+    for _ in range(args.warmup):
+        ts.step()
+    torch.cuda.synchronize(local)
     ts.lib.pf_set_timing(ts.ctx, 1)
     tm = pf._lib.Timing()
     ts.lib.pf_get_timing(ts.ctx, C.byref(tm), 1)
     with ClockSampler(local) as clk:
-        ms, launches = time_steps(ts, args.steps, args.warmup, dist, local)
-    ts.lib.pf_get_timing(ts.ctx, C.byref(tm), 1)
-    stages = tm.as_dict()
-    ts.lib.pf_set_timing(ts.ctx, 0)
-    # end-to-end from pinned host buffers
-    ms_e2e, _ = time_steps(ts, args.steps, max(1, args.warmup // 2), dist, local, e2e=True)
+        ms, launches = time_steps(ts, args.steps, 0, dist, local)
+        ts.lib.pf_get_timing(ts.ctx, C.byref(tm), 1)
+        stages = tm.as_dict()
+        ts.lib.pf_set_timing(ts.ctx, 0)
+        # end-to-end from pinned host buffers
+        ms_e2e, _ = time_steps(ts, args.steps, max(1, args.warmup // 2), dist, local, e2e=True)
     n_faces = ts.active_faces()
 
     value = n * args.steps * world / (ms / 1000.0)
@@ -359,7 +362,7 @@ def run_reference(args, rank, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--seed", type=int, default=0)
