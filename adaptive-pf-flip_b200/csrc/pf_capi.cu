@@ -153,12 +153,13 @@ int create_impl(pf_ctx* ctx, const pf_grid_desc* d) {
   ctx->staging_bytes = stg;
   PF_CUDA_TRY(cudaMalloc(&ctx->staging, stg));
 
-  PF_CUDA_TRY(cudaMalloc(&ctx->tile_count, (nt + 1) * sizeof(int)));
-  PF_CUDA_TRY(cudaMalloc(&ctx->tile_start, (nt + 2) * sizeof(int)));
+  // particle bins: one per pooled cell slot (tile * 512 + local cell)
+  PF_CUDA_TRY(cudaMalloc(&ctx->tile_count, (cells + 1) * sizeof(int)));
+  PF_CUDA_TRY(cudaMalloc(&ctx->tile_start, (cells + 2) * sizeof(int)));
   PF_CUDA_TRY(cudaMalloc(&ctx->pkey, cap * sizeof(int)));
   PF_CUDA_TRY(cudaMalloc(&ctx->prank, cap * sizeof(int)));
   PF_CUDA_TRY(cudaMalloc(&ctx->perm, cap * sizeof(int)));
-  size_t scan_max = nt + 1;
+  size_t scan_max = cells + 1;
   if ((size_t)ncell > scan_max) scan_max = (size_t)ncell;
   if (cap > scan_max) scan_max = cap;
   int rc = scan_alloc(ctx, scan_max);

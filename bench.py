@@ -271,7 +271,7 @@ def run_ours(args, rank, world, local, dist):
     import torch
     pf = load_pkg()
     torch.cuda.set_device(local)
-    sc = pf.scenes.bubble_tank(128, seed=args.seed + rank)
+    sc = pf.scenes.bubble_tank(args.n, seed=args.seed + rank)
     ts = TransferStep(pf, sc, local)
     n = ts.n
     # device-resident timing with per-stage events
@@ -315,8 +315,8 @@ def run_ours(args, rank, world, local, dist):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded bubble tank scene)",
-        "config": {"workload": "bubble_tank_128 transfer stress: P2G(u,v,w,raw mass)+G2P, FLIP 0.97",
-                   "grid": [128, 128, 128], "tile": 8, "particles_per_gpu": n, "global_particles": n * world,
+        "config": {"workload": f"bubble_tank_{args.n} transfer stress: P2G(u,v,w,raw mass)+G2P, FLIP 0.97",
+                   "grid": [args.n] * 3, "tile": 8, "particles_per_gpu": n, "global_particles": n * world,
                    "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (particle SoA %.0f MB per GPU)" % (n * 29 / 1e6)},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": n * 29, "d2h_bytes_per_step": n * 12},
@@ -342,7 +342,7 @@ def run_reference(args, rank, world):
     if rank != 0:
         return
     pf = load_pkg()
-    sc = pf.scenes.bubble_tank(128, seed=args.seed)
+    sc = pf.scenes.bubble_tank(args.n, seed=args.seed)
     np_s, times = cpu_reference_sample(sc, slab_cells=args.cpu_slab, steps=args.steps, warmup=args.warmup)
     total = sum(times)
     value = np_s * len(times) / total
@@ -350,8 +350,8 @@ def run_reference(args, rank, world):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000.0 * total / len(times), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded bubble tank scene)", "impl": "reference",
-        "config": {"workload": "bubble_tank_128 transfer stress: P2G(u,v,w,raw mass)+G2P, FLIP 0.97",
-                   "grid": [128, 128, 128], "sample_particles": np_s},
+        "config": {"workload": f"bubble_tank_{args.n} transfer stress: P2G(u,v,w,raw mass)+G2P, FLIP 0.97",
+                   "grid": [args.n] * 3, "sample_particles": np_s},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": 8, "kind": "reference",
                          "sample": f"{np_s} particles (first {args.cpu_slab} x-columns) per step"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -366,6 +366,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--n", type=int, default=128, help="grid cells per axis (128 is the benchmarked workload)")
     ap.add_argument("--cpu-slab", type=int, default=4, help="x-columns of the scene in the CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

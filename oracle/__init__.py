@@ -440,3 +440,14 @@ def build(quiet=True):
         raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
     if not quiet:
         print(out.stdout)
+
+
+def build_reference_tests(quiet=True):
+    """Build the reference's doctest cases against the GPU drop-in
+    (make -C oracle ref_tests; needs libpfgpu.so built first)."""
+    import subprocess
+    out = subprocess.run(["make", "-C", HERE, "ref_tests"], capture_output=True, text=True)
+    if out.returncode != 0:
+        raise RuntimeError("reference test build failed:\n" + out.stdout + out.stderr)
+    if not quiet:
+        print(out.stdout)
