@@ -31,6 +31,7 @@ EXPORTS = (
     "pf_grid_copy", "pf_active_blocks4", "pf_active_cells", "pf_active_tiles", "pf_mark_cells", "pf_p2g",
     "pf_save_velocity", "pf_apply_gravity", "pf_apply_wall_boundary", "pf_project", "pf_g2p", "pf_advect",
     "pf_step", "pf_calibrate_rho_tilde0", "pf_set_timing", "pf_get_timing", "pf_launch_count",
+    "pf_project_noalloc",
 )
 
 STAGES = ("bin", "sort", "splat", "normalize", "mark", "boundary", "project", "pcg", "g2p")
@@ -139,6 +140,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "pf_set_timing": (i, [vp, i]),
         "pf_get_timing": (i, [vp, P(Timing), i]),
         "pf_launch_count": (C.c_longlong, [vp]),
+        "pf_project_noalloc": (i, [i, i, i, d, vp, vp, vp, vp, vp, vp, vp, vp, P(Phase), d, i, d, d, d,
+                                   P(SolveStats), vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

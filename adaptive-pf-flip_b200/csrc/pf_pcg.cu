@@ -461,3 +461,16 @@ int solve_mixed(pf_ctx* ctx, int nslots, int nred, const uint8_t* kind, double s
 }
 
 }  // namespace pf
+
+namespace pf {
+
+// One PLAIN Jacobi-PCG iteration (the three kernels pcg_plain launches), for
+// the allocation-free projection (pf_noalloc.cu).
+void launch_pcg_plain_iteration(const DevGrid& G, int nslots, int nred, SolveCtl* ctl, const uint8_t* kind,
+                                PcgVec<double> v, double scale, double* partials, cudaStream_t s) {
+  k_spmv_plain<<<nred, PF_TV, 0, s>>>(G, nslots, ctl, kind, v, scale, partials);
+  k_update_plain<<<nred, PF_TV, 0, s>>>(nslots, ctl, kind, v, scale, partials);
+  k_direction_plain<<<nred, PF_TV, 0, s>>>(nslots, ctl, kind, v, scale);
+}
+
+}  // namespace pf

@@ -301,3 +301,23 @@ int project(pf_ctx* ctx, const pf_phase* ph, double dt, const pf_solve_cfg* cfg,
 }
 
 }  // namespace pf
+
+namespace pf {
+
+// Launchers for the allocation-free projection (pf_noalloc.cu): the kernels of
+// project() above, on caller-provided buffers and stream.
+void launch_project_setup(const DevGrid& G, int nslots, int nred, SolveCtl* ctl, uint8_t* kind,
+                          PcgVec<double> vec, double scale, double cdiv, const pf_phase* ph, double* partials,
+                          cudaStream_t s) {
+  k_classify<<<nred, PF_TV, 0, s>>>(G, nslots, ctl, kind);
+  k_pick_pin<<<1, 1, 0, s>>>(ctl);
+  k_assemble<double><<<nred, PF_TV, 0, s>>>(G, nslots, ctl, kind, vec, scale, cdiv, phase_consts(ph), partials);
+}
+
+void launch_project_finish(const DevGrid& G, int nslots, int nred, const uint8_t* kind, const double* x,
+                           double dt_over_dx, const pf_phase* ph, cudaStream_t s) {
+  k_write_pressure<double><<<nred, PF_TV, 0, s>>>(G, nslots, kind, x);
+  k_velocity_update<<<nred, PF_TV, 0, s>>>(G, nslots, dt_over_dx, phase_consts(ph));
+}
+
+}  // namespace pf

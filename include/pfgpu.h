@@ -204,6 +204,37 @@ PFGPU_API int pf_set_timing(pf_ctx* ctx, int enable);
 PFGPU_API long long pf_launch_count(const pf_ctx* ctx);
 PFGPU_API int pf_get_timing(pf_ctx* ctx, pf_timing* out, int reset);
 
+/* ---- allocation-free projection ----------------------------------------
+ * No counterpart in the reference.  For callers that may not allocate device
+ * memory: hosts that reserve the whole device budget themselves and hand out
+ * buffers from their own allocator (and plug-ins running inside such hosts),
+ * or fixed-rate loops that must never wait on the driver's allocator.  It
+ * does what pf_project does in PLAIN mode (same kernels, same results to
+ * rounding of the inner products) on dense device arrays the caller owns:
+ * mk (nx,ny,nz) markers 0/1/2, face raw masses mu/mv/mw and face velocities
+ * u/v/w on the field lattices of pf_grid_set_field (index i + X*(j + Y*k)),
+ * all treated as fully active.  u, v, w are updated in place and p
+ * (nx,ny,nz) receives the pressure (0 outside fluid cells).
+ *
+ * All working memory sits in one fixed __device__ array inside the library
+ * (about 6.3 MB on every GPU that loads it, held until the process exits);
+ * the call makes no cudaMalloc/cudaFree or other allocating call.  Limit:
+ * ceil((nx+1)/8)*ceil((ny+1)/8)*ceil((nz+1)/8) <= PF_NOALLOC_MAX_TILES, e.g.
+ * grids up to 39^3 cells; larger grids return PF_ERR_INVALID without running.
+ * The first call on a device looks the array's device address up
+ * (cudaGetSymbolAddress, with that device current); make that first call
+ * before any stream capture.  Every call uses the same array and leaves its
+ * contents behind (each call re-initialises what it reads), so calls whose
+ * work overlaps on the GPU -- on different streams, or from different host
+ * threads -- race and must be serialised by the caller.  `stream` is a
+ * cudaStream_t (NULL: the default stream); the call returns after its work on
+ * that stream has finished. */
+#define PF_NOALLOC_MAX_TILES 125
+PFGPU_API int pf_project_noalloc(int nx, int ny, int nz, double dx, const float* mk, const float* mu,
+                                 const float* mv, const float* mw, float* u, float* v, float* w, float* p,
+                                 const pf_phase* phase, double dt, int max_iter, double abs_tol,
+                                 double rel_tol, double c_div, pf_solve_stats* stats, void* stream);
+
 /* calibrateRhoTilde0 (src/transfer/transfer3d_tp.cpp:29-36), on the device. */
 PFGPU_API int pf_calibrate_rho_tilde0(pf_ctx* ctx, const pf_phase* phase, double Vp, double* out);
 
