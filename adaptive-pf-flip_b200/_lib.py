@@ -22,6 +22,7 @@ ERR_NAMES = {PF_ERR_INVALID: "PF_ERR_INVALID", PF_ERR_CUDA: "PF_ERR_CUDA", PF_ER
 
 PF_U, PF_V, PF_W, PF_MU, PF_MV, PF_MW, PF_P, PF_MK = range(8)
 PF_SOLVER_PLAIN, PF_SOLVER_MIXED, PF_SOLVER_LEARNED = 0, 1, 2
+PF_PRECOND_NETWORK, PF_PRECOND_EXACT_COARSE, PF_PRECOND_JACOBI = 0, 1, 2
 
 # every entry point include/pfgpu.h declares
 EXPORTS = (
@@ -31,7 +32,9 @@ EXPORTS = (
     "pf_grid_copy", "pf_active_blocks4", "pf_active_cells", "pf_active_tiles", "pf_mark_cells", "pf_p2g",
     "pf_save_velocity", "pf_apply_gravity", "pf_apply_wall_boundary", "pf_project", "pf_g2p", "pf_advect",
     "pf_step", "pf_calibrate_rho_tilde0", "pf_set_timing", "pf_get_timing", "pf_launch_count",
-    "pf_project_noalloc",
+    "pf_project_noalloc", "pf_learned_num_params", "pf_learned_init", "pf_learned_load", "pf_learned_params",
+    "pf_learned_harvest", "pf_learned_dataset", "pf_learned_clear_dataset", "pf_learned_train",
+    "pf_learned_eval", "pf_learned_adam",
 )
 
 STAGES = ("bin", "sort", "splat", "normalize", "mark", "boundary", "project", "pcg", "g2p")
@@ -50,7 +53,8 @@ class Phase(C.Structure):
 class SolveCfg(C.Structure):
     _fields_ = [("mode", C.c_int), ("max_iter", C.c_int), ("abs_tol", C.c_double), ("rel_tol", C.c_double),
                 ("c_div", C.c_double), ("bf16_storage", C.c_int), ("check_every", C.c_int),
-                ("max_refine", C.c_int), ("inner_rel_tol", C.c_double)]
+                ("max_refine", C.c_int), ("inner_rel_tol", C.c_double), ("precond", C.c_int),
+                ("accept_min_gain", C.c_double), ("inner_fp32", C.c_int)]
 
 
 class SolveStats(C.Structure):
@@ -142,6 +146,16 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "pf_launch_count": (C.c_longlong, [vp]),
         "pf_project_noalloc": (i, [i, i, i, d, vp, vp, vp, vp, vp, vp, vp, vp, P(Phase), d, i, d, d, d,
                                    P(SolveStats), vp]),
+        "pf_learned_num_params": (sz, []),
+        "pf_learned_init": (i, [vp, C.c_ulonglong]),
+        "pf_learned_load": (i, [vp, vp, sz]),
+        "pf_learned_params": (i, [vp, vp, sz]),
+        "pf_learned_harvest": (i, [vp, i, i, i, sz]),
+        "pf_learned_dataset": (i, [vp, P(i), P(i)]),
+        "pf_learned_clear_dataset": (i, [vp]),
+        "pf_learned_train": (i, [vp, i, i, d, C.c_ulonglong, vp]),
+        "pf_learned_eval": (i, [vp, i, i, i, vp, vp, vp, i, vp, P(d), vp]),
+        "pf_learned_adam": (i, [vp, vp, sz, d]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -4,6 +4,7 @@
 #include <cstring>
 #include <new>
 
+#include "pf_coarse.cuh"
 #include "pf_ctx.h"
 
 using namespace pf;
@@ -43,6 +44,7 @@ __global__ void k_convert_back(const float* in, T* out, size_t n) {
 
 void free_all(pf_ctx* c) {
   auto F = [](void* p) { if (p) cudaFree(p); };
+  pf::coarse_release(c);
   F(c->tile_slot); F(c->slot_tile); F(c->d_nslots); F(c->tile_need); F(c->tile_new); F(c->tile_rank);
   for (int f = 0; f < PF_NFIELDS; ++f) { F(c->fld[f]); F(c->act4[f]); }
   for (int a = 0; a < PF_NSAVED; ++a) F(c->saved[a]);
@@ -173,7 +175,8 @@ int create_impl(pf_ctx* ctx, const pf_grid_desc* d) {
   }
   PF_CUDA_TRY(cudaMalloc(&ctx->kind, cells));
   PF_CUDA_TRY(cudaMemset(ctx->kind, 0, cells));
-  PF_CUDA_TRY(cudaMalloc(&ctx->partials, (size_t)kMaxRedBlocks * 3 * sizeof(double)));
+  // per-CTA partials: up to kRedSlots doubles per reduction CTA
+  PF_CUDA_TRY(cudaMalloc(&ctx->partials, (size_t)kMaxRedBlocks * kRedSlots * sizeof(double)));
   PF_CUDA_TRY(cudaMalloc(&ctx->ctl, sizeof(SolveCtl)));
   PF_CUDA_TRY(cudaMemset(ctx->ctl, 0, sizeof(SolveCtl)));
   PF_CUDA_TRY(cudaMallocHost(&ctx->h_ctl, sizeof(SolveCtl)));

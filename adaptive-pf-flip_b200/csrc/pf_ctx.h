@@ -129,6 +129,7 @@ int project(pf_ctx* ctx, const pf_phase* ph, double dt, const pf_solve_cfg* cfg,
             pf_solve_stats* st);
 
 constexpr int kMaxRedBlocks = 1184;  // 8 CTAs per SM on 148 SMs
+constexpr int kRedSlots = 4;         // partial values one reduction CTA may write
 
 // pf_timing.cu
 using TimedStage = pf_ctx::TimedStage;

@@ -1,0 +1,677 @@
+// pf_learned_kernels.cuh -- device kernels of the learned coarse solve
+// (included by pf_learned.cu only).
+//
+// Every convolution is a 3x3x3 implicit GEMM on the tensor cores
+// (mma.sync m16n8k16, BF16 operands, FP32 accumulation): M = positions,
+// N = output channels, K = 27 taps x input channels.  Activations are FP32 in
+// HBM, channels-last with the channel stride padded to 16; the operands are
+// rounded to BF16 when the fragments are built.  Weights keep an FP32 master
+// copy (Adam) and are repacked into BF16 fragment order after every update.
+#pragma once
+
+#include <cuda_bf16.h>
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "pf_coarse.cuh"
+#include "pf_solver.cuh"
+
+namespace pf {
+
+namespace {
+
+struct LayerSpec {
+  int cin, cout, relu, bias;
+};
+// gate U-Net (layers 0-11), then the linear operator G (layers 12-15, no bias)
+constexpr int kNumLayers = 16;
+constexpr LayerSpec kLayers[kNumLayers] = {
+    {32, 16, 1, 1}, {16, 16, 1, 1}, {16, 32, 1, 1}, {32, 32, 1, 1}, {32, 64, 1, 1}, {64, 64, 1, 1},
+    {64, 64, 1, 1}, {64, 64, 1, 1}, {128, 64, 1, 1}, {96, 32, 1, 1}, {48, 16, 1, 1}, {16, 8, 0, 1},
+    {2, 8, 0, 0},   {8, 8, 0, 0},   {8, 8, 0, 0},   {8, 8, 0, 0}};
+enum { L_E0A, L_E0B, L_E1A, L_E1B, L_E2A, L_E2B, L_E3A, L_E3B, L_D2, L_D1, L_D0, L_OUT, L_G0, L_G1, L_G2, L_G3 };
+constexpr int kInCh = 32;
+constexpr int kGS = 16;  // channel stride of every tensor of the G path (8 channels used)
+
+__host__ __device__ constexpr int pad16(int c) { return (c + 15) & ~15; }
+__host__ __device__ constexpr int pad8(int c) { return (c + 7) & ~7; }
+
+struct Dims {
+  int X, Y, Z, n;
+};
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+  __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<uint32_t*>(&v);
+}
+
+__device__ __forceinline__ void mma_bf16(float* c, uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
+                                         uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// tap k = (dz+1)*9 + (dy+1)*3 + (dx+1)
+__device__ __forceinline__ int tap_dx(int k) { return k % 3 - 1; }
+__device__ __forceinline__ int tap_dy(int k) { return (k / 3) % 3 - 1; }
+__device__ __forceinline__ int tap_dz(int k) { return k / 9 - 1; }
+
+// Position p + tap within the same sample, or -1 outside the lattice.
+__device__ __forceinline__ int neighbor(const Dims& d, int b, int x, int y, int z, int k) {
+  const int xx = x + tap_dx(k), yy = y + tap_dy(k), zz = z + tap_dz(k);
+  if (xx < 0 || yy < 0 || zz < 0 || xx >= d.X || yy >= d.Y || zz >= d.Z) return -1;
+  return b * d.n + xx + d.X * (yy + d.Y * zz);
+}
+
+// ---------------------------------------------------------------------------
+// weight packing: FP32 master W[27][cin][cout] -> BF16 B fragments
+//   fwd: (tap, kc, nt, lane) -> {W[tap][kc*16+2t(+1)][nt*8+g], W[tap][kc*16+2t+8(+9)][nt*8+g]}
+//   bwd: the same for W'[tap][co][ci] = W[26 - tap][ci][co] (transposed, flipped)
+
+__global__ void k_pack(const float* W, int cin, int cout, int transpose, uint2* out) {
+  const int ci_n = transpose ? cout : cin;   // GEMM K extent (input channels of this conv)
+  const int co_n = transpose ? cin : cout;   // GEMM N extent
+  const int KC = pad16(ci_n) / 16, NT = pad8(co_n) / 8;
+  const int total = 27 * KC * NT * 32;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < total; q += gridDim.x * blockDim.x) {
+    const int lane = q & 31;
+    int r = q >> 5;
+    const int nt = r % NT;
+    r /= NT;
+    const int kc = r % KC;
+    const int tap = r / KC;
+    const int g = lane >> 2, t = lane & 3;
+    const int n = nt * 8 + g;
+    float v[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int k = kc * 16 + 2 * t + (e & 1) + (e >> 1) * 8;
+      float w = 0.0f;
+      if (k < ci_n && n < co_n) {
+        w = transpose ? W[((size_t)(26 - tap) * cin + n) * cout + k] : W[((size_t)tap * cin + k) * cout + n];
+      }
+      v[e] = w;
+    }
+    out[q] = make_uint2(pack_bf16(v[0], v[1]), pack_bf16(v[2], v[3]));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// convolution: y[p][co] = act(bias[co] + sum_tap sum_ci x[p+tap][ci] w[tap][ci][co])
+// One warp computes 16 positions x all NT*8 output channels; 4 warps per CTA.
+
+struct ConvArgs {
+  const float* x;
+  const float* gate;  // optional: x counts only where gate > 0 (ReLU backward)
+  int xs;             // channel stride of x and gate (multiple of 16) = 16 * KC
+  const uint2* wf;
+  const float* bias;  // optional
+  int cout, relu;
+  float* y;
+  int ys;             // channel stride of y (multiple of 16, >= NT*8)
+  Dims d;
+  int P;              // positions (batch * d.n)
+  const SolveCtl* skip;
+};
+
+template <int NT>
+__global__ void __launch_bounds__(128) k_conv(ConvArgs a) {
+  if (a.skip && a.skip->done) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, t = lane & 3;
+  const int base = (blockIdx.x * 4 + warp) * 16;
+  if (base >= a.P) return;
+  const int KC = a.xs / 16;
+  int rb[2], rx[2], ry[2], rz[2];
+  bool rv[2];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int p = base + g + 8 * h;
+    rv[h] = p < a.P;
+    const int pp = rv[h] ? p : 0;
+    rb[h] = pp / a.d.n;
+    const int tt = pp - rb[h] * a.d.n;
+    rx[h] = tt % a.d.X;
+    ry[h] = (tt / a.d.X) % a.d.Y;
+    rz[h] = tt / (a.d.X * a.d.Y);
+  }
+  float acc[NT][4];
+#pragma unroll
+  for (int j = 0; j < NT; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0f;
+  for (int k = 0; k < 27; ++k) {
+    int q[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) q[h] = rv[h] ? neighbor(a.d, rb[h], rx[h], ry[h], rz[h], k) : -1;
+    for (int kc = 0; kc < KC; ++kc) {
+      float2 v[2][2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        if (q[h] >= 0) {
+          const float* src = a.x + (size_t)q[h] * a.xs + kc * 16 + 2 * t;
+          v[h][0] = *reinterpret_cast<const float2*>(src);
+          v[h][1] = *reinterpret_cast<const float2*>(src + 8);
+          if (a.gate) {
+            const float* gs = a.gate + (size_t)q[h] * a.xs + kc * 16 + 2 * t;
+            const float2 g0 = *reinterpret_cast<const float2*>(gs);
+            const float2 g1 = *reinterpret_cast<const float2*>(gs + 8);
+            if (!(g0.x > 0.0f)) v[h][0].x = 0.0f;
+            if (!(g0.y > 0.0f)) v[h][0].y = 0.0f;
+            if (!(g1.x > 0.0f)) v[h][1].x = 0.0f;
+            if (!(g1.y > 0.0f)) v[h][1].y = 0.0f;
+          }
+        } else {
+          v[h][0] = make_float2(0.0f, 0.0f);
+          v[h][1] = make_float2(0.0f, 0.0f);
+        }
+      }
+      const uint32_t a0 = pack_bf16(v[0][0].x, v[0][0].y);
+      const uint32_t a1 = pack_bf16(v[1][0].x, v[1][0].y);
+      const uint32_t a2 = pack_bf16(v[0][1].x, v[0][1].y);
+      const uint32_t a3 = pack_bf16(v[1][1].x, v[1][1].y);
+      const uint2* wb = a.wf + ((size_t)(k * KC + kc) * NT) * 32 + lane;
+#pragma unroll
+      for (int j = 0; j < NT; ++j) {
+        const uint2 b = __ldg(wb + j * 32);
+        mma_bf16(acc[j], a0, a1, a2, a3, b.x, b.y);
+      }
+    }
+  }
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    if (!rv[h]) continue;
+    float* yr = a.y + (size_t)(base + g + 8 * h) * a.ys;
+#pragma unroll
+    for (int j = 0; j < NT; ++j) {
+      const int c0 = j * 8 + 2 * t;
+      float o0 = acc[j][2 * h], o1 = acc[j][2 * h + 1];
+      if (c0 < a.cout) {
+        if (a.bias) o0 += a.bias[c0];
+        if (a.relu) o0 = fmaxf(o0, 0.0f);
+      } else {
+        o0 = 0.0f;
+      }
+      if (c0 + 1 < a.cout) {
+        if (a.bias) o1 += a.bias[c0 + 1];
+        if (a.relu) o1 = fmaxf(o1, 0.0f);
+      } else {
+        o1 = 0.0f;
+      }
+      *reinterpret_cast<float2*>(yr + c0) = make_float2(o0, o1);
+    }
+    for (int c = NT * 8 + 2 * t; c < a.ys; c += 8) *reinterpret_cast<float2*>(yr + c) = make_float2(0.0f, 0.0f);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// weight gradient: part[cta][tap][ci][co] = sum_{p in the CTA's chunks} x[p+tap][ci] dz[p][co]
+// with dz = dy (gated by y > 0 for ReLU layers).  Grid (nctas, 27), 8 warps;
+// each chunk of 64 positions is staged transposed in shared memory as BF16.
+
+constexpr int kWChunk = 64;
+constexpr int kWPitch = kWChunk + 8;  // BF16 elements per staged row (bank-conflict-free fragments)
+
+struct WgradArgs {
+  const float* x;
+  int xs, cin;
+  const float* dy;
+  const float* gate;
+  int ds, cout;
+  float* part;
+  Dims d;
+  int P;
+};
+
+__global__ void __launch_bounds__(256) k_wgrad(WgradArgs a) {
+  __shared__ __align__(16) __nv_bfloat16 XT[128][kWPitch];
+  __shared__ __align__(16) __nv_bfloat16 DT[64][kWPitch];
+  const int tap = blockIdx.y;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, t = lane & 3;
+  const int MT = pad16(a.cin) / 16, NTt = pad8(a.cout) / 8;
+  const int cin16 = MT * 16, cout8 = NTt * 8;
+  const int tiles = MT * NTt;
+  float acc[8][4];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0f;
+  const int nchunks = (a.P + kWChunk - 1) / kWChunk;
+  for (int c = blockIdx.x; c < nchunks; c += gridDim.x) {
+    __syncthreads();
+    for (int e = threadIdx.x; e < kWChunk * cin16; e += blockDim.x) {
+      const int pl = e / cin16, ci = e - pl * cin16;
+      const int p = c * kWChunk + pl;
+      float v = 0.0f;
+      if (p < a.P && ci < a.cin) {
+        const int b = p / a.d.n, tt = p - b * a.d.n;
+        const int q = neighbor(a.d, b, tt % a.d.X, (tt / a.d.X) % a.d.Y, tt / (a.d.X * a.d.Y), tap);
+        if (q >= 0) v = a.x[(size_t)q * a.xs + ci];
+      }
+      XT[ci][pl] = __float2bfloat16_rn(v);
+    }
+    for (int e = threadIdx.x; e < kWChunk * cout8; e += blockDim.x) {
+      const int pl = e / cout8, co = e - pl * cout8;
+      const int p = c * kWChunk + pl;
+      float v = 0.0f;
+      if (p < a.P && co < a.cout) {
+        v = a.dy[(size_t)p * a.ds + co];
+        if (a.gate && !(a.gate[(size_t)p * a.ds + co] > 0.0f)) v = 0.0f;
+      }
+      DT[co][pl] = __float2bfloat16_rn(v);
+    }
+    __syncthreads();
+    for (int j = 0; j < 8; ++j) {
+      const int tile = warp + 8 * j;
+      if (tile >= tiles) break;
+      const int mt = tile / NTt, nt = tile - mt * NTt;
+#pragma unroll
+      for (int ks = 0; ks < kWChunk / 16; ++ks) {
+        const int kk = ks * 16 + 2 * t;
+        const uint32_t a0 = *reinterpret_cast<const uint32_t*>(&XT[mt * 16 + g][kk]);
+        const uint32_t a1 = *reinterpret_cast<const uint32_t*>(&XT[mt * 16 + g + 8][kk]);
+        const uint32_t a2 = *reinterpret_cast<const uint32_t*>(&XT[mt * 16 + g][kk + 8]);
+        const uint32_t a3 = *reinterpret_cast<const uint32_t*>(&XT[mt * 16 + g + 8][kk + 8]);
+        const uint32_t b0 = *reinterpret_cast<const uint32_t*>(&DT[nt * 8 + g][kk]);
+        const uint32_t b1 = *reinterpret_cast<const uint32_t*>(&DT[nt * 8 + g][kk + 8]);
+        mma_bf16(acc[j], a0, a1, a2, a3, b0, b1);
+      }
+    }
+  }
+  float* out = a.part + ((size_t)blockIdx.x * 27 + tap) * a.cin * a.cout;
+  for (int j = 0; j < 8; ++j) {
+    const int tile = warp + 8 * j;
+    if (tile >= tiles) break;
+    const int mt = tile / NTt, nt = tile - mt * NTt;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int ci = mt * 16 + g + 8 * (e >> 1), co = nt * 8 + 2 * t + (e & 1);
+      if (ci < a.cin && co < a.cout) out[(size_t)ci * a.cout + co] = acc[j][e];
+    }
+  }
+}
+
+// dW += sum over CTA partials (fixed order)
+__global__ void k_wgrad_reduce(const float* part, int nparts, int count, float* dW) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < count; q += gridDim.x * blockDim.x) {
+    float s = 0.0f;
+    for (int c = 0; c < nparts; ++c) s += part[(size_t)c * count + q];
+    dW[q] += s;
+  }
+}
+
+// db[co] += sum_p dz[p][co], one CTA per output channel, FP64 fixed-order sums
+__global__ void __launch_bounds__(256) k_bias_grad(const float* dy, const float* gate, int ds, int P, float* db) {
+  const int co = blockIdx.x;
+  double s = 0.0;
+  for (int p = threadIdx.x; p < P; p += blockDim.x) {
+    float v = dy[(size_t)p * ds + co];
+    if (gate && !(gate[(size_t)p * ds + co] > 0.0f)) v = 0.0f;
+    s += v;
+  }
+  __shared__ double sh[8];
+  s = warp_sum(s);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double tot = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += sh[w];
+    db[co] += (float)tot;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// pooling, upsampling + concatenation, and their adjoints (B samples)
+
+__global__ void k_pool(const float* x, int cs, Dims f, Dims c, int B, float* y, const SolveCtl* skip) {
+  if (skip && skip->done) return;
+  const size_t total = (size_t)B * c.n * cs;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
+    const int ch = (int)(q % cs);
+    const size_t pc = q / cs;
+    const int b = (int)(pc / c.n), tc = (int)(pc % c.n);
+    const int X = tc % c.X, Y = (tc / c.X) % c.Y, Z = tc / (c.X * c.Y);
+    float s = 0.0f;
+    for (int dz = 0; dz < 2; ++dz)
+      for (int dy = 0; dy < 2; ++dy)
+        for (int dx = 0; dx < 2; ++dx) {
+          const int xx = 2 * X + dx, yy = 2 * Y + dy, zz = 2 * Z + dz;
+          if (xx < f.X && yy < f.Y && zz < f.Z) s += x[((size_t)b * f.n + xx + f.X * (yy + f.Y * zz)) * cs + ch];
+        }
+    y[q] = s * 0.125f;
+  }
+}
+
+// dx[child] += dy[parent] / 8
+__global__ void k_pool_bwd(const float* dy, int cs, Dims f, Dims c, int B, float* dx) {
+  const size_t total = (size_t)B * f.n * cs;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
+    const int ch = (int)(q % cs);
+    const size_t pf = q / cs;
+    const int b = (int)(pf / f.n), tf = (int)(pf % f.n);
+    const int x = tf % f.X, y = (tf / f.X) % f.Y, z = tf / (f.X * f.Y);
+    const size_t pc = (size_t)b * c.n + (x >> 1) + c.X * ((y >> 1) + c.Y * (z >> 1));
+    dx[q] += dy[pc * cs + ch] * 0.125f;
+  }
+}
+
+// out[p] = [coarse[parent(p)][0:cu], skip[p][0:csk]] with stride cu + csk
+__global__ void k_up_concat(const float* coarse, int cu, Dims c, const float* skipt, int csk, Dims f, int B,
+                            float* out, const SolveCtl* skip) {
+  if (skip && skip->done) return;
+  const int cs = cu + csk;
+  const size_t total = (size_t)B * f.n * cs;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
+    const int ch = (int)(q % cs);
+    const size_t pf = q / cs;
+    float v;
+    if (ch < cu) {
+      const int b = (int)(pf / f.n), tf = (int)(pf % f.n);
+      const int x = tf % f.X, y = (tf / f.X) % f.Y, z = tf / (f.X * f.Y);
+      const size_t pc = (size_t)b * c.n + (x >> 1) + c.X * ((y >> 1) + c.Y * (z >> 1));
+      v = coarse[pc * cu + ch];
+    } else {
+      v = skipt[pf * csk + (ch - cu)];
+    }
+    out[q] = v;
+  }
+}
+
+// d_coarse[parent][ch] = sum over children of dout[child][ch] (ch < cu);
+// d_skip[p][ch] = dout[p][cu + ch]
+__global__ void k_up_concat_bwd(const float* dout, int cu, int csk, Dims c, Dims f, int B, float* dcoarse,
+                                float* dskip) {
+  const int cs = cu + csk;
+  const size_t tc_total = (size_t)B * c.n * cu;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < tc_total; q += (size_t)gridDim.x * blockDim.x) {
+    const int ch = (int)(q % cu);
+    const size_t pc = q / cu;
+    const int b = (int)(pc / c.n), tc = (int)(pc % c.n);
+    const int X = tc % c.X, Y = (tc / c.X) % c.Y, Z = tc / (c.X * c.Y);
+    float s = 0.0f;
+    for (int dz = 0; dz < 2; ++dz)
+      for (int dy = 0; dy < 2; ++dy)
+        for (int dx = 0; dx < 2; ++dx) {
+          const int xx = 2 * X + dx, yy = 2 * Y + dy, zz = 2 * Z + dz;
+          if (xx < f.X && yy < f.Y && zz < f.Z) s += dout[((size_t)b * f.n + xx + f.X * (yy + f.Y * zz)) * cs + ch];
+        }
+    dcoarse[q] = s;
+  }
+  const size_t ts_total = (size_t)B * f.n * csk;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < ts_total; q += (size_t)gridDim.x * blockDim.x) {
+    const size_t pf = q / csk;
+    const int ch = (int)(q % csk);
+    dskip[q] = dout[pf * cs + cu + ch];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// features, scales, output mapping, loss
+
+__device__ __forceinline__ bool live(const float* cop, int t, int c) {
+  return cop[(size_t)t * kCopStride + kCopN + c] > 0.0f && cop[(size_t)t * kCopStride + kCopD + c] > 0.0f;
+}
+
+// sc[b] = max over live unknowns |rc_b| (b < B); sc[B] = d_ref
+__global__ void __launch_bounds__(256) k_scales(const float* cop, const float* rc, int nt, int B, float* sc,
+                                                const SolveCtl* skip) {
+  if (skip && skip->done) return;
+  const int b = blockIdx.x;
+  float m = 0.0f, m1 = 0.0f;
+  for (int t = threadIdx.x; t < nt; t += blockDim.x) {
+    for (int c = 0; c < 2; ++c) {
+      if (!live(cop, t, c)) continue;
+      if (b < B) {
+        if (rc) m = fmaxf(m, fabsf(rc[((size_t)b * nt + t) * 2 + c]));
+      } else {
+        const float d = cop[(size_t)t * kCopStride + kCopD + c];
+        if (c == 0) m = fmaxf(m, d);
+        else m1 = fmaxf(m1, d);
+      }
+    }
+  }
+  __shared__ float sh[2][8];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    m = fmaxf(m, __shfl_down_sync(0xffffffffu, m, o));
+    m1 = fmaxf(m1, __shfl_down_sync(0xffffffffu, m1, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    sh[0][threadIdx.x >> 5] = m;
+    sh[1][threadIdx.x >> 5] = m1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float a = 0.0f, a1 = 0.0f;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      a = fmaxf(a, sh[0][w]);
+      a1 = fmaxf(a1, sh[1][w]);
+    }
+    sc[b] = (b < B || a > 0.0f) ? a : a1;
+  }
+}
+
+__global__ void k_features(const float* cop, const float* rc, Dims d, int B, const float* sc, float* F,
+                           const SolveCtl* skip) {
+  if (skip && skip->done) return;
+  const size_t total = (size_t)B * d.n;
+  const float inv_log = 1.0f / logf(1e4f);
+  const float dref = sc[B];
+  for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < total; p += (size_t)gridDim.x * blockDim.x) {
+    const int b = (int)(p / d.n), t = (int)(p % d.n);
+    const float s = sc[b];
+    const float inv_s = s > 0.0f ? 1.0f / s : 0.0f;
+    float f[kInCh];
+#pragma unroll
+    for (int c = 0; c < kInCh; ++c) f[c] = 0.0f;
+    const float* R = cop + (size_t)t * kCopStride;
+    const bool l0 = live(cop, t, 0), l1 = live(cop, t, 1);
+    const bool lv[2] = {l0, l1};
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      if (!lv[c]) continue;
+      f[c] = rc ? rc[((size_t)b * d.n + t) * 2 + c] * inv_s : 0.0f;
+      f[2 + c] = 1.0f;
+      f[4 + c] = dref > 0.0f ? logf(R[kCopD + c] / dref) * inv_log : 0.0f;
+    }
+    if (l0 && l1) f[6] = R[kCopE] / sqrtf(R[kCopD] * R[kCopD + 1]);
+    const int x = t % d.X, y = (t / d.X) % d.Y, z = t / (d.X * d.Y);
+    const int has[3] = {x > 0, y > 0, z > 0};
+    const int step[3] = {1, d.X, d.X * d.Y};
+    const int base[3] = {kCopX, kCopY, kCopZ};
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      if (!has[q]) continue;
+      const int u = t - step[q];
+      const float* Ru = cop + (size_t)u * kCopStride;
+#pragma unroll
+      for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int bb = 0; bb < 2; ++bb)
+          if (lv[a] && live(cop, u, bb))
+            f[7 + 4 * q + 2 * a + bb] = R[base[q] + 2 * a + bb] / sqrtf(R[kCopD + a] * Ru[kCopD + bb]);
+    }
+    float4* out = reinterpret_cast<float4*>(F + p * kInCh);
+#pragma unroll
+    for (int c = 0; c < kInCh / 4; ++c) out[c] = make_float4(f[4 * c], f[4 * c + 1], f[4 * c + 2], f[4 * c + 3]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// the G path: e = S G^T G S rc, S = diag(d_c^-1/2) on live unknowns
+
+__device__ __forceinline__ float inv_sqrt_diag(const float* cop, int t, int c) {
+  return live(cop, t, c) ? rsqrtf(cop[(size_t)t * kCopStride + kCopD + c]) : 0.0f;
+}
+
+// out[p][0:2] = S * in[p][0:2] (in: [B][nt][2] packed, or stride-16 when in_stride16), channels 2..15 = 0
+__global__ void k_scale_in(const float* in, int in_stride16, const float* cop, int nt, int B, float* out,
+                           const SolveCtl* skip) {
+  if (skip && skip->done) return;
+  const size_t total = (size_t)B * nt * kGS;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
+    const int c = (int)(q % kGS);
+    const size_t p = q / kGS;
+    float v = 0.0f;
+    if (c < 2) {
+      const int t = (int)(p % nt);
+      v = inv_sqrt_diag(cop, t, c) * (in_stride16 ? in[p * kGS + c] : in[p * 2 + c]);
+    }
+    out[q] = v;
+  }
+}
+
+// e[p][c] = S * w[p][c] for c < 2 (w has stride 16)
+__global__ void k_scale_out(const float* w, const float* cop, int nt, int B, float* e, const SolveCtl* skip) {
+  if (skip && skip->done) return;
+  const size_t total = (size_t)B * nt * 2;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
+    const int c = (int)(q & 1);
+    const size_t p = q >> 1;
+    e[q] = inv_sqrt_diag(cop, (int)(p % nt), c) * w[p * kGS + c];
+  }
+}
+
+// out = g * a, g shared by the B samples ([n][16])
+__global__ void k_gmul(float* out, const float* g, const float* a, int n, int B, const SolveCtl* skip) {
+  if (skip && skip->done) return;
+  const size_t total = (size_t)B * n * kGS;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x)
+    out[q] = g[q % ((size_t)n * kGS)] * a[q];
+}
+
+// b = h + P^T v (v on the coarser level: each child gets v[parent] / 8); t = g * b
+__global__ void k_up_add_gate(const float* h, const float* v, const float* g, Dims f, Dims c, int B, float* b,
+                              float* t, const SolveCtl* skip) {
+  if (skip && skip->done) return;
+  const size_t total = (size_t)B * f.n * kGS;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
+    const int ch = (int)(q % kGS);
+    const size_t pf = q / kGS;
+    const int bb = (int)(pf / f.n), tf = (int)(pf % f.n);
+    const int x = tf % f.X, y = (tf / f.X) % f.Y, z = tf / (f.X * f.Y);
+    const size_t pc = (size_t)bb * c.n + (x >> 1) + c.X * ((y >> 1) + c.Y * (z >> 1));
+    const float bv = h[q] + v[pc * kGS + ch] * 0.125f;
+    if (b) b[q] = bv;
+    t[q] = g[(size_t)tf * kGS + ch] * bv;
+  }
+}
+
+// dg[i] += sum_b u[b][i] v[b][i]  (i over n * 16)
+__global__ void k_gate_grad(float* dg, const float* u, const float* v, int n, int B) {
+  const size_t m = (size_t)n * kGS;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < m; i += (size_t)gridDim.x * blockDim.x) {
+    float s = 0.0f;
+    for (int b = 0; b < B; ++b) s += u[(size_t)b * m + i] * v[(size_t)b * m + i];
+    dg[i] += s;
+  }
+}
+
+// out += in (B samples, stride 16)
+__global__ void k_add(float* out, const float* in, size_t total) {
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x)
+    out[q] += in[q];
+}
+
+template <typename T>
+__device__ __forceinline__ double capply(const float* cop, const Dims& d, const T* x, int t, int c) {
+  const int tx = t % d.X, q = t / d.X, ty = q % d.Y, tz = q / d.Y;
+  const float* R = cop + (size_t)t * kCopStride;
+  double y = (double)R[kCopD + c] * (double)x[2 * t + c] - (double)R[kCopE] * (double)x[2 * t + 1 - c];
+  const int step[3] = {1, d.X, d.X * d.Y};
+  const int has_lo[3] = {tx > 0, ty > 0, tz > 0};
+  const int has_hi[3] = {tx + 1 < d.X, ty + 1 < d.Y, tz + 1 < d.Z};
+  const int base[3] = {kCopX, kCopY, kCopZ};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    if (has_lo[a]) {
+      const int u = t - step[a];
+      y -= (double)R[base[a] + 2 * c] * (double)x[2 * u] + (double)R[base[a] + 2 * c + 1] * (double)x[2 * u + 1];
+    }
+    if (has_hi[a]) {
+      const int u = t + step[a];
+      const float* Ru = cop + (size_t)u * kCopStride;
+      y -= (double)Ru[base[a] + c] * (double)x[2 * u] + (double)Ru[base[a] + 2 + c] * (double)x[2 * u + 1];
+    }
+  }
+  return y;
+}
+
+// v = e - target (live), per-sample den = target . rc (live)
+__global__ void __launch_bounds__(256) k_loss_prep(const float* e, const float* tgt, const float* rc,
+                                                   const float* cop, int nt, double* v, double* den) {
+  const int b = blockIdx.x;
+  double s = 0.0;
+  for (int q = threadIdx.x; q < 2 * nt; q += blockDim.x) {
+    const int t = q >> 1, c = q & 1;
+    const size_t o = (size_t)b * 2 * nt + q;
+    if (live(cop, t, c)) {
+      v[o] = (double)e[o] - (double)tgt[o];
+      s += (double)tgt[o] * (double)rc[o];
+    } else {
+      v[o] = 0.0;
+    }
+  }
+  __shared__ double sh[8];
+  s = warp_sum(s);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double tot = 0.0;
+    for (int w = 0; w < 8; ++w) tot += sh[w];
+    den[b] = tot;
+  }
+}
+
+// per sample: loss_b = v.Av / den_b; de = live ? 2 Av / den_b / B : 0 (stride 16)
+__global__ void __launch_bounds__(256) k_loss_grad(const double* v, const double* den, const float* cop, Dims d,
+                                                   int B, float* dout, double* loss) {
+  const int b = blockIdx.x;
+  const int nt = d.n;
+  const double dn = den[b];
+  const double scale = 1.0;
+  const bool ok = dn > 0.0;
+  double s = 0.0;
+  for (int q = threadIdx.x; q < 2 * nt; q += blockDim.x) {
+    const int t = q >> 1, c = q & 1;
+    const size_t o = (size_t)b * 2 * nt + q;
+    double g = 0.0;
+    if (live(cop, t, c)) {
+      const double av = capply(cop, d, v + (size_t)b * 2 * nt, t, c);
+      s += v[o] * av;
+      if (ok) g = 2.0 * av / dn / B * scale;
+    }
+    dout[((size_t)b * nt + t) * 16 + c] = (float)g;
+  }
+  __shared__ double sh[8];
+  s = warp_sum(s);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double tot = 0.0;
+    for (int w = 0; w < 8; ++w) tot += sh[w];
+    loss[b] = ok ? tot / dn : 0.0;
+  }
+}
+
+__global__ void k_adam(float* p, const float* g, float* m, float* v, size_t n, float lr, float b1, float b2,
+                       float c1, float c2, float eps) {
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+    const float gq = g[q];
+    const float mq = b1 * m[q] + (1.0f - b1) * gq;
+    const float vq = b2 * v[q] + (1.0f - b2) * gq * gq;
+    m[q] = mq;
+    v[q] = vq;
+    p[q] -= lr * (mq / c1) / (sqrtf(vq / c2) + eps);
+  }
+}
+
+__global__ void k_zero_f(float* p, size_t n) {
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x)
+    p[q] = 0.0f;
+}
+
+}  // namespace
+}  // namespace pf

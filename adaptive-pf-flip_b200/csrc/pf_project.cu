@@ -269,6 +269,10 @@ int project(pf_ctx* ctx, const pf_phase* ph, double dt, const pf_solve_cfg* cfg,
     rc = pcg_plain(ctx, nslots, nred, kind, vec, scale, cfg, &res);
     if (rc) return rc;
     (++ctx->launches), k_write_pressure<double><<<nred, PF_TV, 0, ctx->stream>>>(G, nslots, kind, ctx->x);
+  } else if (cfg->mode == PF_SOLVER_LEARNED) {
+    rc = solve_learned(ctx, nslots, nred, kind, scale, cfg, &res);
+    if (rc) return rc;
+    (++ctx->launches), k_write_pressure<double><<<nred, PF_TV, 0, ctx->stream>>>(G, nslots, kind, ctx->x);
   } else {
     rc = solve_mixed(ctx, nslots, nred, kind, scale, cfg, (const void*)&phk, &res);
     if (rc) return rc;

@@ -28,7 +28,7 @@ enum RedStage {
   kStagePAp = 1,     // after SpMV: p.Ap -> alpha (breakdown check)
   kStageUpdate = 2,  // after x/r update: r.z, max|r| -> convergence, beta
   kStageResid = 3,   // outer refinement: max|b - A x| (FP64)
-  kStageFlex = 4,    // flexible PCG: r.z, r.(z - z_prev)
+  kStageFlex = 4,    // flexible PCG x/r update: max|r| -> convergence (beta comes from the preconditioner step)
 };
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -77,7 +77,7 @@ __device__ __forceinline__ void finalize_stage(SolveCtl* ctl, int stage, double 
     case kStagePAp: {
       ctl->pAp = S;
       if (!isfinite(S)) ctl->done = 4;
-      else if (fabs(S) < 1e-30) ctl->done = 2;
+      else if (fabs(S) < 1e-30 || !isfinite(ctl->rz / S)) ctl->done = 2;
       else ctl->alpha = ctl->rz / S;
       break;
     }
@@ -101,15 +101,9 @@ __device__ __forceinline__ void finalize_stage(SolveCtl* ctl, int stage, double 
     case kStageFlex: {
       ctl->it += 1;
       ctl->res = M;
-      if (!isfinite(M) || !isfinite(S) || !isfinite(S2)) ctl->done = 4;
+      if (!isfinite(M)) ctl->done = 4;
       else if (M < ctl->tol) ctl->done = 1;
       else if (ctl->it >= ctl->max_iter) ctl->done = 3;
-      else {
-        double b = ctl->rz != 0.0 ? S2 / ctl->rz : 0.0;  // Polak-Ribiere
-        if (!isfinite(b) || b < 0.0) b = 0.0;
-        ctl->beta = b;
-        ctl->rz = S;
-      }
       break;
     }
   }
@@ -190,5 +184,7 @@ int pcg_plain(pf_ctx* ctx, int nslots, int nred, const uint8_t* kind, PcgVec<dou
 int solve_mixed(pf_ctx* ctx, int nslots, int nred, const uint8_t* kind, double scale, const pf_solve_cfg* cfg,
                 const void* phase_consts, SolveResult* res);
 int ensure_solver_buffers(pf_ctx* ctx, int mode);
+int solve_learned(pf_ctx* ctx, int nslots, int nred, const uint8_t* kind, double scale, const pf_solve_cfg* cfg,
+                  SolveResult* res);
 
 }  // namespace pf

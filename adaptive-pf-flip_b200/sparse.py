@@ -136,6 +136,15 @@ class SolverConfig:
     check_every: int = 0
     max_refine: int = 0
     inner_rel_tol: float = 0.0
+    precond: int = L.PF_PRECOND_NETWORK
+    accept_min_gain: float = 0.0
+    inner_fp32: bool = False
+
+    def _c(self, cg_iters, cg_tol, c_div) -> L.SolveCfg:
+        return L.SolveCfg(int(self.mode), int(cg_iters), float(cg_tol), float(self.rel_tol), float(c_div),
+                          int(bool(self.bf16_storage)), int(self.check_every), int(self.max_refine),
+                          float(self.inner_rel_tol), int(self.precond), float(self.accept_min_gain),
+                          int(bool(self.inner_fp32)))
 
 
 # ---------------------------------------------------------------------------
@@ -312,8 +321,7 @@ def spP2G3D_tp(g: SparseMacGrid3D, ps, pp: PhaseParams, Vp: float):
 def spProjectStepVC3D(g: SparseMacGrid3D, pp: PhaseParams, dt, cg_iters, cg_tol, divergenceCorrection=0.0,
                       solver: SolverConfig | None = None) -> L.SolveStats:
     s = solver or SolverConfig()
-    cfg = L.SolveCfg(int(s.mode), int(cg_iters), float(cg_tol), float(s.rel_tol), float(divergenceCorrection),
-                     int(bool(s.bf16_storage)), int(s.check_every), int(s.max_refine), float(s.inner_rel_tol))
+    cfg = s._c(cg_iters, cg_tol, divergenceCorrection)
     st = L.SolveStats()
     L.check(g.lib.pf_project(g.ctx, C.byref(pp._c()), float(dt), C.byref(cfg), C.byref(st)), g.ctx,
             "pf_project")
@@ -395,10 +403,7 @@ class SparseSim3DTP:
         return pos, vel, typ, vol
 
     def step_cfg(self):
-        s = self.solver
-        solve = L.SolveCfg(int(s.mode), int(self.cg_iters), float(self.cg_tol), float(s.rel_tol),
-                           float(self.c_div_last), int(bool(s.bf16_storage)), int(s.check_every),
-                           int(s.max_refine), float(s.inner_rel_tol))
+        solve = self.solver._c(self.cg_iters, self.cg_tol, self.c_div_last)
         return L.StepCfg(self.dt, self.gravity, self.Vp, self.alpha_liquid, self.alpha_gas, self.phase._c(), solve,
                          int(self.advection_order))
 

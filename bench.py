@@ -267,6 +267,69 @@ def cpu_reference_sample(sc, slab_cells, steps, warmup=0, alpha=0.97):
     return len(ps), times
 
 
+def run_pcg(pf, n, modes, max_iter=20000, seed=0):
+    """Pressure-only system (n^3, every interior cell fluid, 64 air ellipsoids
+    in water at 1000:1, band-limited RHS): device time to a 1e-6 relative
+    FP64 residual per solver mode, and each mode's pressure against the
+    PLAIN FP64 solve."""
+    sc = pf.scenes.ellipsoid_pressure(n, seed=seed)
+    pp = pf.PhaseParams(sc["rho_l"], sc["rho_g"])
+    g = pf.SparseMacGrid3D(n, n, n, sc["dx"], max_particles=1)
+    pp.rho_tilde_0 = pf.calibrateRhoTilde0(pp, 1.0, grid=g)
+    f = pf.scenes.pressure_grid_fields(sc, pp.rho_tilde_0)
+    full = {k: np.ones(g.bdims(i)[::-1], np.uint8) for i, k in enumerate(("u", "v", "w", "mu", "mv", "mw", "p", "mk"))}
+    for k in ("mu", "mv", "mw", "mk"):
+        g.set_field(("u", "v", "w", "mu", "mv", "mw", "p", "mk").index(k), f[k], full[k])
+    out, p_plain = {}, None
+    for name, mode, bf16 in modes:
+        for k in ("u", "v", "w"):
+            g.set_field(("u", "v", "w").index(k), f[k], full[k])
+        st = pf.spProjectStepVC3D(g, pp, 1.0 / 240.0, max_iter, 0.0,
+                                  solver=pf.SolverConfig(mode=mode, rel_tol=1e-6, bf16_storage=bf16))
+        p, _ = g.get_field(pf.PF_P)
+        rec = {"ms_to_1e-6": st.solve_ms, "iterations": st.iterations, "refinements": st.refinements,
+               "converged": bool(st.converged), "rel_residual": st.res_final / max(st.res0, 1e-300)}
+        if p_plain is None:
+            p_plain = p.astype(np.float64)
+        else:
+            rec["p_rel_diff_vs_plain"] = float(np.abs(p - p_plain).max() / max(np.abs(p_plain).max(), 1e-300))
+        out[name] = rec
+    base = out[modes[0][0]]["ms_to_1e-6"]
+    for name in out:
+        out[name]["speedup_vs_plain"] = base / max(out[name]["ms_to_1e-6"], 1e-9)
+    return {"workload": f"ellipsoid_pressure_{n}: {(n - 2) ** 3} unknowns, 64 air ellipsoids, 1000:1, "
+                        "band-limited RHS |k|<=8", "modes": out}
+
+
+def run_full_step(pf, n=48, steps=20, seed=0):
+    """Whole solver step (markCells .. advection) on the Rayleigh-Taylor scene
+    at 1000:1, PLAIN PCG to 1e-6 relative; device-timed particles/s."""
+    import torch
+    sc = pf.scenes.rayleigh_taylor(n, seed=seed)
+    sim = pf.SparseSim3DTP(n, n, n, sc["dx"], max_particles=len(sc["pos"]))
+    sim.phase = pf.PhaseParams(sc["rho_l"], sc["rho_g"])
+    sim.phase.rho_tilde_0 = pf.calibrateRhoTilde0(sim.phase, 1.0, grid=sim.grid)
+    sim.dt = 1.0 / 240.0
+    sim.cg_iters, sim.cg_tol = 4000, 0.0
+    sim.solver = pf.SolverConfig(rel_tol=1e-6)
+    sim.set_particles(sc["pos"], sc["vel"], sc["type"], sc["volume"])
+    stream = torch.cuda.ExternalStream(pf.load().pf_stream(sim.grid.ctx))
+    for _ in range(3):
+        sim.step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    iters = 0
+    e0.record(stream)
+    for _ in range(steps):
+        iters += sim.step().solve.iterations
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    return {"workload": f"rayleigh_taylor_{n}: {len(sc['pos'])} particles, 1000:1, dt 1/240, plain PCG to 1e-6",
+            "particles_per_s": len(sc["pos"]) * steps / (ms / 1000.0), "ms_per_step": ms / steps,
+            "pcg_iterations_per_step": iters / steps}
+
+
 def run_ours(args, rank, world, local, dist):
     import torch
     pf = load_pkg()
@@ -327,6 +390,11 @@ def run_ours(args, rank, world, local, dist):
         "gpu_launches": int(launches) * world,
         "clocks": clk.summary(),
     }
+    if rank == 0 and not args.no_extras:
+        line["pcg"] = run_pcg(pf, args.pcg_n, [("plain_fp64", pf.PF_SOLVER_PLAIN, False),
+                                               ("mixed_fp32", pf.PF_SOLVER_MIXED, False),
+                                               ("mixed_bf16", pf.PF_SOLVER_MIXED, True)])
+        line["full_step"] = run_full_step(pf)
     if rank == 0 and not args.no_cpu_baseline:
         cores = 8
         np_s, times = cpu_reference_sample(sc, slab_cells=args.cpu_slab, steps=1)
@@ -369,6 +437,8 @@ def main():
     ap.add_argument("--n", type=int, default=128, help="grid cells per axis (128 is the benchmarked workload)")
     ap.add_argument("--cpu-slab", type=int, default=4, help="x-columns of the scene in the CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the PCG and full-step blocks")
+    ap.add_argument("--pcg-n", type=int, default=256, help="grid of the pressure-only block")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

@@ -76,7 +76,7 @@ typedef struct {
 /* pressure solver modes */
 #define PF_SOLVER_PLAIN 0   /* FP64 Jacobi-PCG, the reference-equivalent drop-in */
 #define PF_SOLVER_MIXED 1   /* FP32 SpMV/preconditioner, FP64 dots, iterative refinement */
-#define PF_SOLVER_LEARNED 2 /* mixed + learned per-tile preconditioner in flexible PCG */
+#define PF_SOLVER_LEARNED 2 /* flexible PCG, Jacobi + learned two-level coarse correction */
 
 typedef struct {
   int mode;             /* PF_SOLVER_* */
@@ -88,7 +88,15 @@ typedef struct {
   int check_every;      /* host convergence poll interval in iterations (0 = default) */
   int max_refine;       /* mixed/learned: outer refinement sweeps (0 = default) */
   double inner_rel_tol; /* mixed/learned: inner solve relative reduction (0 = default) */
+  int precond;          /* learned: PF_PRECOND_* */
+  double accept_min_gain; /* learned: keep the coarse term only if r.z >= (1+gain) r.D^-1 r */
+  int inner_fp32;       /* learned: 0 FP64 vectors; 1 FP32 vectors inside FP64 iterative refinement */
 } pf_solve_cfg;
+
+/* preconditioner of the LEARNED mode's flexible PCG */
+#define PF_PRECOND_NETWORK 0      /* Jacobi + learned coarse correction (the default) */
+#define PF_PRECOND_EXACT_COARSE 1 /* Jacobi + exact Galerkin coarse solve (training target, ablation) */
+#define PF_PRECOND_JACOBI 2       /* Jacobi alone: the same solver without the network */
 
 typedef struct {
   int iterations;        /* total inner PCG iterations */
@@ -237,6 +245,37 @@ PFGPU_API int pf_project_noalloc(int nx, int ny, int nz, double dx, const float*
 
 /* calibrateRhoTilde0 (src/transfer/transfer3d_tp.cpp:29-36), on the device. */
 PFGPU_API int pf_calibrate_rho_tilde0(pf_ctx* ctx, const pf_phase* phase, double Vp, double* out);
+
+/* ---- learned coarse solve (PF_SOLVER_LEARNED with PF_PRECOND_NETWORK) ----
+ * New in this library (the reference's sparse path has no learned solver; its
+ * flexible-PCG / guarded-preconditioner pattern is
+ * src/pressure/multires_pressure3d.cpp:1301-1447).  The network maps the
+ * tile-lattice coarse residual and operator to the coarse correction; its
+ * parameters are one flat FP32 vector of pf_learned_num_params() floats
+ * (per layer: weights [27][C_in][C_out], then biases [C_out]). */
+PFGPU_API size_t pf_learned_num_params(void);
+/* Fresh He-normal weights from a seed; resets the optimiser. */
+PFGPU_API int pf_learned_init(pf_ctx* ctx, unsigned long long seed);
+/* Load / read the parameter vector (n must equal pf_learned_num_params()). */
+PFGPU_API int pf_learned_load(pf_ctx* ctx, const float* params, size_t n);
+PFGPU_API int pf_learned_params(pf_ctx* ctx, float* out, size_t n);
+/* Training data: while enabled, every EXACT_COARSE solve stores its coarse
+ * operator and up to max_per_system (r_c, A_c^-1 r_c) pairs, one every
+ * `stride` coarse solves, into a device pool of capacity_floats floats. */
+PFGPU_API int pf_learned_harvest(pf_ctx* ctx, int enable, int stride, int max_per_system, size_t capacity_floats);
+PFGPU_API int pf_learned_dataset(pf_ctx* ctx, int* systems, int* pairs);
+PFGPU_API int pf_learned_clear_dataset(pf_ctx* ctx);
+/* `steps` Adam steps on batches of `batch` pairs of one system each; losses
+ * (optional, [steps]) receives each step's mean energy-norm error. */
+PFGPU_API int pf_learned_train(pf_ctx* ctx, int steps, int batch, double lr, unsigned long long seed,
+                               double* losses);
+/* The network on a caller-given coarse system: cop [X*Y*Z][17], rc and
+ * target [B][X*Y*Z][2] (target may be NULL), e_out [B][X*Y*Z][2]; with a
+ * target also the mean loss and the parameter gradient (grad_out may be NULL). */
+PFGPU_API int pf_learned_eval(pf_ctx* ctx, int X, int Y, int Z, const float* cop, const float* rc,
+                              const float* target, int B, float* e_out, double* loss_out, float* grad_out);
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8) with a caller-given gradient. */
+PFGPU_API int pf_learned_adam(pf_ctx* ctx, const float* grad, size_t n, double lr);
 
 #ifdef __cplusplus
 }
