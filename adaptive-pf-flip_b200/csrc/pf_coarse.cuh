@@ -43,8 +43,9 @@ struct CoarseCtx {
   CoarseOp op{};
   LearnedState* net = nullptr;
   size_t cls_cap = 0;
-  double* z64 = nullptr;  // stored M^-1 r of the FP64 flexible PCG
-  size_t z64_cap = 0;
+  int* nbr = nullptr;       // neighbour-slot table of the pool (6 per slot)
+  float* rc_part = nullptr; // per-warp restriction partials (16 warps x 2 classes per slot)
+  size_t nbr_cap = 0;       // slots
 };
 
 int coarse_ensure(pf_ctx* ctx);

@@ -4,14 +4,25 @@
 // targets, the exact Galerkin coarse solve; or nothing, plain Jacobi).
 //
 // Polak-Ribiere beta r.(z - z_prev)/rz as the reference's flexible option
-// (src/pressure/multires_pressure3d.cpp:1425-1434).  Each iteration forms
-// both candidates z_j = D^-1 r and z_c = z_j + P c; z_c is accepted only when
+// (src/pressure/multires_pressure3d.cpp:1425-1434).  Each iteration has both
+// candidates z_j = D^-1 r and z_c = z_j + P c; z_c is accepted only when
 // r.z_c >= r.z_j (1 + min_gain) (the rz-gain guard of
 // src/pressure/multires_pressure3d.cpp:1322-1334), and after kDisableAfter
 // consecutive rejections the solve continues with Jacobi alone (the
 // auto-disable of :1172).  Whatever the coarse term does, convergence is
 // judged on the residual of the exact FP64 operator: directly in the FP64
 // variant, through FP64 iterative refinement in the FP32 variant.
+//
+// Three fine-grid passes per iteration:
+//   spmv    Ap, p.Ap -> alpha
+//   update  x += alpha p, r -= alpha Ap, max|r|, r.D^-1 r, r.z_prev and the
+//           per-warp partial sums of the restriction rc = P^T r (z_prev is
+//           recomputed from the old r, so z is never stored)
+//   [coarse solve on the tile lattice: rc from the partials, ec = c(rc)]
+//   guard   r.P ec = rc.ec on the coarse lattice, so r.z_c = r.D^-1 r + rc.ec
+//           without another fine pass; accept or reject, beta
+//   dir     p = z + beta p
+// The iteration body can be captured once into a CUDA graph and replayed.
 #include <algorithm>
 #include <cmath>
 
@@ -25,9 +36,9 @@ constexpr int kDisableAfter = 8;
 
 template <typename V>
 struct FlexVec {
-  V *e, *r, *Ap, *z, *p;  // solution (correction), residual, A p, stored M^-1 r, direction
-  V *d, *cx, *cy, *cz;    // operator: diagonal and low-face couplings, times scale
-  const uint8_t* cls;     // coarse class of each unknown (255: none)
+  V *e, *r, *Ap, *p;    // solution (correction), residual, A p, direction
+  V *d, *cx, *cy, *cz;  // operator: diagonal and low-face couplings, times scale
+  const uint8_t* cls;   // coarse class of each unknown (255: none)
   V scale;
 };
 
@@ -38,6 +49,7 @@ __global__ void k_fx_set(SolveCtl* ctl, double tol_abs, double tol_rel, int max_
   ctl->done = 0;
   ctl->it = 0;
   ctl->counter = 0;
+  ctl->aux[0] = 0.0;
   ctl->aux[2] = offered;
   if (reset) {
     ctl->aux[1] = 0.0;
@@ -64,100 +76,182 @@ __global__ void __launch_bounds__(PF_TV) k_fx_setup32(int nslots, const uint8_t*
 }
 
 template <typename V>
-__global__ void __launch_bounds__(PF_TV) k_fx_start(int nslots, SolveCtl* ctl, const uint8_t* kind, const double* r64,
-                                                    FlexVec<V> m, double* partials) {
-  double rmax = 0.0;
-  for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
-    const size_t o = (size_t)s * PF_TV + threadIdx.x;
-    const V r = kind[o] ? (V)r64[o] : (V)0;
-    m.r[o] = r;
-    m.e[o] = (V)0;
-    m.z[o] = (V)0;
-    m.p[o] = (V)0;
-    rmax = fmax(rmax, fabs((double)r));
-  }
-  block_reduce_2(0.0, rmax, partials, ctl, kStageInit);  // sets res0, tol, done
+__device__ __forceinline__ double inv_diag(const FlexVec<V>& m, uint8_t kd, size_t o) {
+  const double d = kd == 1 ? (double)m.scale * (double)m.d[o] : 0.0;
+  return d > 0.0 ? 1.0 / d : 0.0;
 }
 
 template <typename V>
-__device__ __forceinline__ V jacobi(const FlexVec<V>& m, uint8_t kd, size_t o) {
-  const V d = kd == 1 ? m.scale * m.d[o] : (V)0;
-  return d > (V)0 ? m.r[o] / d : (V)0;
-}
-
-template <typename V>
-__device__ __forceinline__ V coarse_term(const FlexVec<V>& m, const int* slot_tile, int s, size_t o,
-                                         const float* ec) {
+__device__ __forceinline__ double coarse_term(const FlexVec<V>& m, const int* slot_tile, int s, size_t o,
+                                              const float* ec) {
   const uint8_t c = m.cls[o];
-  return c != 255 ? (V)ec[coarse_index(slot_tile[s], c)] : (V)0;
+  return c != 255 ? (double)ec[coarse_index(slot_tile[s], c)] : 0.0;
 }
 
-// Dots of both candidates: r.zc, r.zj, r.(zc - z_prev), r.(zj - z_prev); the
-// last CTA applies the guard, picks the preconditioner and the flexible beta.
+constexpr int kWarpsPerSlot = PF_TV / 32;
+
+// Per-warp class sums of r (32 cells of slot s) into part[(s * 16 + warp) * 2 + class];
+// k_rc_reduce folds them into rc.  No block synchronisation.
+__device__ __forceinline__ void restrict_warp(const uint8_t* cls, size_t o, double r, int s, float* part) {
+  const uint8_t c = cls[o];
+  double a0 = c == 0 ? r : 0.0, a1 = c == 1 ? r : 0.0;
+  a0 = warp_sum(a0);
+  a1 = warp_sum(a1);
+  if ((threadIdx.x & 31) == 0) {
+    float* q = part + ((size_t)s * kWarpsPerSlot + (threadIdx.x >> 5)) * 2;
+    q[0] = (float)a0;
+    q[1] = (float)a1;
+  }
+}
+
+// rc[2 tile + c] = sum of the 16 warp partials of the tile's slot, in order
+__global__ void k_rc_reduce(const float* part, const int* slot_tile, int nslots, float* rc, const SolveCtl* skip) {
+  if (skip && skip->done) return;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < 2 * nslots; q += gridDim.x * blockDim.x) {
+    const int s = q >> 1, c = q & 1;
+    double t = 0.0;
+    for (int w = 0; w < kWarpsPerSlot; ++w) t += (double)part[((size_t)s * kWarpsPerSlot + w) * 2 + c];
+    rc[coarse_index(slot_tile[s], (uint8_t)c)] = (float)t;
+  }
+}
+
+// r = r_init (on unknowns), x = p = 0; max|r| -> res0 / tolerance; r.D^-1 r;
+// rc = P^T r when rc != nullptr
 template <typename V>
-__global__ void __launch_bounds__(PF_TV) k_fx_precond(const int* slot_tile, int nslots, SolveCtl* ctl,
-                                                      const uint8_t* kind, FlexVec<V> m, const float* ec, int first,
-                                                      double min_gain, double* partials) {
-  if (ctl->done) return;
-  const bool offered = ctl->aux[2] != 0.0 && ctl->aux[1] == 0.0;
-  double a[4] = {0.0, 0.0, 0.0, 0.0};
+__global__ void __launch_bounds__(PF_TV) k_fx_start(int nslots, SolveCtl* ctl, const uint8_t* kind, const double* r64,
+                                                    FlexVec<V> m, float* rc_part, double* partials) {
+  double rmax = 0.0, rzj = 0.0;
   for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
     const size_t o = (size_t)s * PF_TV + threadIdx.x;
     const uint8_t kd = kind[o];
-    if (!kd) continue;
-    const double r = (double)m.r[o];
-    const double zj = (double)jacobi(m, kd, o);
-    const double zc = offered ? zj + (double)coarse_term(m, slot_tile, s, o, ec) : zj;
-    const double zp = (double)m.z[o];
-    a[0] += r * zc;
-    a[1] += r * zj;
-    a[2] += r * (zc - zp);
-    a[3] += r * (zj - zp);
+    const V r = kd ? (V)r64[o] : (V)0;
+    m.r[o] = r;
+    m.e[o] = (V)0;
+    m.p[o] = (V)0;
+    rmax = fmax(rmax, fabs((double)r));
+    rzj += (double)r * (double)r * inv_diag(m, kd, o);
+    if (rc_part) restrict_warp(m.cls, o, (double)r, s, rc_part);
   }
-  __shared__ double sh[4][32];
+  block_reduce_3(rzj, rmax, 0.0, partials, ctl, kStageInit);  // res0, tol, done; flex = {r.D^-1 r, 0}
+}
+
+__global__ void k_build_nbr(DevGrid G, int nslots, int* nbr) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < 6 * nslots; q += gridDim.x * blockDim.x) {
+    const int s = q / 6, d = q - 6 * s;
+    const int t = G.slot_tile[s];
+    int tx = t % G.g.TX, r = t / G.g.TX, ty = r % G.g.TY, tz = r / G.g.TY;
+    tx += d == 0 ? 1 : d == 1 ? -1 : 0;
+    ty += d == 2 ? 1 : d == 3 ? -1 : 0;
+    tz += d == 4 ? 1 : d == 5 ? -1 : 0;
+    int v = -1;
+    if (tx >= 0 && ty >= 0 && tz >= 0 && tx < G.g.TX && ty < G.g.TY && tz < G.g.TZ)
+      v = G.tile_slot[tile_id(G.g, tx, ty, tz)];
+    nbr[q] = v;
+  }
+}
+
+template <typename V>
+__global__ void __launch_bounds__(PF_TV) k_fx_spmv(const int* __restrict__ nbr, int nslots, SolveCtl* ctl,
+                                                   const uint8_t* kind, FlexVec<V> m, double* partials) {
+  if (ctl->done) return;
+  double acc = 0.0;
+  for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
+    const int l = threadIdx.x;
+    const size_t o = (size_t)s * PF_TV + l;
+    const uint8_t kd = kind[o];
+    if (!kd) continue;
+    const V p0 = m.p[o];
+    V ap;
+    if (kd == 2) {
+      ap = p0;
+    } else {
+      long long no[6];
+      neighbor_offsets_tab(nbr, s, l, no);
+      V off = (V)0;
+      if (no[0] >= 0) off += m.cx[no[0]] * m.p[no[0]];
+      if (no[1] >= 0) off += m.cx[o] * m.p[no[1]];
+      if (no[2] >= 0) off += m.cy[no[2]] * m.p[no[2]];
+      if (no[3] >= 0) off += m.cy[o] * m.p[no[3]];
+      if (no[4] >= 0) off += m.cz[no[4]] * m.p[no[4]];
+      if (no[5] >= 0) off += m.cz[o] * m.p[no[5]];
+      ap = m.scale * (m.d[o] * p0 - off);
+    }
+    m.Ap[o] = ap;
+    acc += (double)p0 * (double)ap;
+  }
+  block_reduce_2(acc, 0.0, partials, ctl, kStagePAp);
+}
+
+// x/r update with max|r| (convergence), r.D^-1 r and r.z_prev of the new r,
+// where z_prev = D^-1 r_old (+ P ec_old if the last direction used it); and
+// the warp partials of rc = P^T r_new when rc_part != nullptr
+template <typename V>
+__global__ void __launch_bounds__(PF_TV) k_fx_update(int nslots, SolveCtl* ctl, const uint8_t* kind, FlexVec<V> m,
+                                                     const int* slot_tile, const float* ec, float* rc_part,
+                                                     double* partials) {
+  if (ctl->done) return;
+  const V alpha = (V)ctl->alpha;
+  const bool used_c = ctl->aux[0] != 0.0;
+  double rmax = 0.0, rzj = 0.0, rzp = 0.0;
+  for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
+    const size_t o = (size_t)s * PF_TV + threadIdx.x;
+    const uint8_t kd = kind[o];
+    double rn = 0.0;
+    if (kd) {
+      m.e[o] += alpha * m.p[o];
+      const V r_old = m.r[o];
+      const V r = r_old - alpha * m.Ap[o];
+      m.r[o] = r;
+      rn = (double)r;
+      const double di = inv_diag(m, kd, o);
+      double zp = (double)r_old * di;
+      if (used_c) zp += coarse_term(m, slot_tile, s, o, ec);
+      rmax = fmax(rmax, fabs(rn));
+      rzj += rn * rn * di;
+      rzp += rn * zp;
+    }
+    if (rc_part) restrict_warp(m.cls, o, rn, s, rc_part);
+  }
+  block_reduce_3(rzj, rmax, rzp, partials, ctl, kStageFlex);
+}
+
+// rc.ec over the coarse unknowns (grid-stride partials; the last CTA sums
+// them in order), then the guard and beta:
+//   r.z_j = flex[0], r.z_prev = flex[1], r.z_c = r.z_j + rc.ec
+constexpr int kGuardThreads = 256;
+
+__global__ void __launch_bounds__(kGuardThreads) k_fx_guard(SolveCtl* ctl, const float* rc, const float* ec, int nu,
+                                                            int first, double min_gain, double* partials) {
+  if (ctl->done) return;
+  const bool offered = ctl->aux[2] != 0.0 && ctl->aux[1] == 0.0;
+  double d = 0.0;
+  if (offered)
+    for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < nu; u += gridDim.x * blockDim.x)
+      d += (double)rc[u] * (double)ec[u];
+  __shared__ double sh[kGuardThreads / 32];
   __shared__ bool am_last;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const double v = warp_sum(a[q]);
-    if (lane == 0) sh[q][wid] = v;
-  }
+  d = warp_sum(d);
+  if (lane == 0) sh[wid] = d;
   __syncthreads();
   if (threadIdx.x == 0) {
-    for (int q = 0; q < 4; ++q) {
-      double v = 0.0;
-      for (int w = 0; w < nw; ++w) v += sh[q][w];
-      partials[kRedSlots * blockIdx.x + q] = v;
-    }
+    double v = 0.0;
+    for (int w = 0; w < nw; ++w) v += sh[w];
+    partials[kRedSlots * blockIdx.x] = v;
     __threadfence();
     am_last = atomicAdd(&ctl->counter, 1u) == gridDim.x - 1;
   }
   __syncthreads();
-  if (!am_last) return;
+  if (!am_last || threadIdx.x != 0) return;
   __threadfence();
-  // the last CTA sums the partials with all its threads, in a fixed order
-  double S[4] = {0.0, 0.0, 0.0, 0.0};
-  for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
-#pragma unroll
-    for (int q = 0; q < 4; ++q) S[q] += __ldcg(&partials[kRedSlots * b + q]);
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const double v = warp_sum(S[q]);
-    __syncthreads();
-    if (lane == 0) sh[q][wid] = v;
-  }
-  __syncthreads();
-  if (threadIdx.x != 0) return;
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    double v = 0.0;
-    for (int w = 0; w < nw; ++w) v += sh[q][w];
-    S[q] = v;
-  }
+  double D = 0.0;
+  for (int b = 0; b < (int)gridDim.x; ++b) D += __ldcg(&partials[kRedSlots * b]);
   ctl->counter = 0;
+  const double S1 = ctl->flex[0], Q = ctl->flex[1];
+  const double S0 = S1 + D;
   bool use_c = false;
   if (offered) {
-    use_c = isfinite(S[0]) && S[0] > 0.0 && S[0] >= S[1] * (1.0 + min_gain);
+    use_c = isfinite(S0) && S0 > 0.0 && S0 >= S1 * (1.0 + min_gain);
     if (use_c) {
       ctl->accepted += 1;
       ctl->aux[3] = 0.0;
@@ -168,14 +262,14 @@ __global__ void __launch_bounds__(PF_TV) k_fx_precond(const int* slot_tile, int 
     }
   }
   ctl->aux[0] = use_c ? 1.0 : 0.0;
-  const double rzn = use_c ? S[0] : S[1];
+  const double rzn = use_c ? S0 : S1;
   if (!isfinite(rzn)) {
     ctl->done = 4;
     return;
   }
   double b = 0.0;
   if (!first && ctl->rz != 0.0) {
-    b = (use_c ? S[2] : S[3]) / ctl->rz;
+    b = (rzn - Q) / ctl->rz;  // Polak-Ribiere: r.(z - z_prev) / r_prev.z_prev
     if (!isfinite(b) || b < 0.0) b = 0.0;
   }
   ctl->beta = b;
@@ -192,64 +286,10 @@ __global__ void __launch_bounds__(PF_TV) k_fx_dir(const int* slot_tile, int nslo
     const size_t o = (size_t)s * PF_TV + threadIdx.x;
     const uint8_t kd = kind[o];
     if (!kd) continue;
-    V z = jacobi(m, kd, o);
+    double z = (double)m.r[o] * inv_diag(m, kd, o);
     if (use_c) z += coarse_term(m, slot_tile, s, o, ec);
-    m.z[o] = z;
-    m.p[o] = z + beta * m.p[o];
+    m.p[o] = (V)z + beta * m.p[o];
   }
-}
-
-template <typename V>
-__global__ void __launch_bounds__(PF_TV) k_fx_spmv(DevGrid G, int nslots, SolveCtl* ctl, const uint8_t* kind,
-                                                   FlexVec<V> m, double* partials) {
-  if (ctl->done) return;
-  __shared__ int nbs[6];
-  double acc = 0.0;
-  for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
-    __syncthreads();
-    neighbor_slots(G, s, nbs);
-    __syncthreads();
-    const int l = threadIdx.x;
-    const size_t o = (size_t)s * PF_TV + l;
-    const uint8_t kd = kind[o];
-    if (!kd) continue;
-    const V p0 = m.p[o];
-    V ap;
-    if (kd == 2) {
-      ap = p0;
-    } else {
-      long long no[6];
-      neighbor_offsets(s, l, nbs, no);
-      V off = (V)0;
-      if (no[0] >= 0) off += m.cx[no[0]] * m.p[no[0]];
-      if (no[1] >= 0) off += m.cx[o] * m.p[no[1]];
-      if (no[2] >= 0) off += m.cy[no[2]] * m.p[no[2]];
-      if (no[3] >= 0) off += m.cy[o] * m.p[no[3]];
-      if (no[4] >= 0) off += m.cz[no[4]] * m.p[no[4]];
-      if (no[5] >= 0) off += m.cz[o] * m.p[no[5]];
-      ap = m.scale * (m.d[o] * p0 - off);
-    }
-    m.Ap[o] = ap;
-    acc += (double)p0 * (double)ap;
-  }
-  block_reduce_2(acc, 0.0, partials, ctl, kStagePAp);
-}
-
-template <typename V>
-__global__ void __launch_bounds__(PF_TV) k_fx_update(int nslots, SolveCtl* ctl, const uint8_t* kind, FlexVec<V> m,
-                                                     double* partials) {
-  if (ctl->done) return;
-  const V alpha = (V)ctl->alpha;
-  double rmax = 0.0;
-  for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
-    const size_t o = (size_t)s * PF_TV + threadIdx.x;
-    if (!kind[o]) continue;
-    m.e[o] += alpha * m.p[o];
-    const V r = m.r[o] - alpha * m.Ap[o];
-    m.r[o] = r;
-    rmax = fmax(rmax, fabs((double)r));
-  }
-  block_reduce_2(0.0, rmax, partials, ctl, kStageFlex);
 }
 
 __global__ void k_fx_add(int nslots, const uint8_t* kind, double* x, const float* e) {
@@ -260,16 +300,12 @@ __global__ void k_fx_add(int nslots, const uint8_t* kind, double* x, const float
 }
 
 // r = b - A x with the exact FP64 operator; max|r| -> ctl->res
-__global__ void __launch_bounds__(PF_TV) k_fx_residual(DevGrid G, int nslots, SolveCtl* ctl, const uint8_t* kind,
-                                                       const double* x, const double* diag, const double* cx,
-                                                       const double* cy, const double* cz, const double* b,
-                                                       double scale, double* r, double* partials) {
-  __shared__ int nbs[6];
+__global__ void __launch_bounds__(PF_TV) k_fx_residual(const int* __restrict__ nbr, int nslots, SolveCtl* ctl,
+                                                       const uint8_t* kind, const double* x, const double* diag,
+                                                       const double* cx, const double* cy, const double* cz,
+                                                       const double* b, double scale, double* r, double* partials) {
   double rmax = 0.0;
   for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
-    __syncthreads();
-    neighbor_slots(G, s, nbs);
-    __syncthreads();
     const int l = threadIdx.x;
     const size_t o = (size_t)s * PF_TV + l;
     const uint8_t kd = kind[o];
@@ -279,7 +315,7 @@ __global__ void __launch_bounds__(PF_TV) k_fx_residual(DevGrid G, int nslots, So
       ax = x[o];
     } else {
       long long no[6];
-      neighbor_offsets(s, l, nbs, no);
+      neighbor_offsets_tab(nbr, s, l, no);
       double off = 0.0;
       if (no[0] >= 0) off += cx[no[0]] * x[no[0]];
       if (no[1] >= 0) off += cx[o] * x[no[1]];
@@ -303,12 +339,102 @@ int poll_ctl(pf_ctx* ctx, SolveCtl* out) {
   return PF_OK;
 }
 
-template <typename V>
-int apply_coarse(pf_ctx* ctx, int nslots, const uint8_t* kind, const V* r, int precond) {
-  int rc = coarse_restrict(ctx, nslots, kind, r, ctx->ctl);
-  if (rc) return rc;
+}  // namespace
+
+int build_neighbor_table(pf_ctx* ctx, int nslots, int** nbr) {
+  CoarseCtx* c = (CoarseCtx*)ctx->learned;
+  const size_t cap = ctx->cells_cap / PF_TV;
+  if (c->nbr_cap < cap) {
+    if (c->nbr) cudaFree(c->nbr);
+    if (c->rc_part) cudaFree(c->rc_part);
+    c->nbr = nullptr;
+    c->rc_part = nullptr;
+    PF_CUDA_TRY(cudaMalloc(&c->nbr, 6 * cap * sizeof(int)));
+    PF_CUDA_TRY(cudaMalloc(&c->rc_part, cap * kWarpsPerSlot * 2 * sizeof(float)));
+    c->nbr_cap = cap;
+  }
+  if (nslots > 0) {
+    const int blocks = std::min((6 * nslots + 255) / 256, 148 * 16);
+    (++ctx->launches), k_build_nbr<<<blocks, 256, 0, ctx->stream>>>(dev_grid(ctx), nslots, c->nbr);
+    PF_CUDA_TRY(cudaGetLastError());
+  }
+  *nbr = c->nbr;
+  return PF_OK;
+}
+
+namespace {
+
+// rc from the warp partials, then the coarse correction ec
+int coarse_solve(pf_ctx* ctx, int nslots, int precond) {
+  CoarseCtx* c = (CoarseCtx*)ctx->learned;
+  const int blocks = std::max(1, std::min((2 * nslots + 255) / 256, 148 * 8));
+  (++ctx->launches), k_rc_reduce<<<blocks, 256, 0, ctx->stream>>>(c->rc_part, ctx->slot_tile, nslots, c->op.rc,
+                                                                  ctx->ctl);
+  PF_CUDA_TRY(cudaGetLastError());
   if (precond == PF_PRECOND_EXACT_COARSE) return coarse_solve_exact(ctx, 400, 1e-6, ctx->ctl);
   return coarse_solve_net(ctx, ctx->ctl);
+}
+
+int launch_guard(pf_ctx* ctx, bool coarse, int first, double min_gain) {
+  CoarseOp& A = ((CoarseCtx*)ctx->learned)->op;
+  const int nu = coarse ? 2 * A.nt : 0;
+  const int blocks = std::max(1, std::min((nu + kGuardThreads - 1) / kGuardThreads, 64));
+  (++ctx->launches), k_fx_guard<<<blocks, kGuardThreads, 0, ctx->stream>>>(ctx->ctl, A.rc, A.ec, nu, first, min_gain,
+                                                                          ctx->partials);
+  PF_CUDA_TRY(cudaGetLastError());
+  return PF_OK;
+}
+
+// spmv, update, [coarse solve], guard, dir
+template <typename V>
+int launch_iteration(pf_ctx* ctx, int nslots, int nred, const uint8_t* kind, const FlexVec<V>& m, int precond,
+                     double min_gain) {
+  CoarseOp& A = ((CoarseCtx*)ctx->learned)->op;
+  const bool coarse = precond != PF_PRECOND_JACOBI;
+  const int* nbr = ((CoarseCtx*)ctx->learned)->nbr;
+  (++ctx->launches), k_fx_spmv<V><<<nred, PF_TV, 0, ctx->stream>>>(nbr, nslots, ctx->ctl, kind, m, ctx->partials);
+  float* rc_part = coarse ? ((CoarseCtx*)ctx->learned)->rc_part : nullptr;
+  (++ctx->launches), k_fx_update<V><<<nred, PF_TV, 0, ctx->stream>>>(nslots, ctx->ctl, kind, m, ctx->slot_tile, A.ec,
+                                                                     rc_part, ctx->partials);
+  if (coarse) {
+    int rc = coarse_solve(ctx, nslots, precond);
+    if (rc) return rc;
+  }
+  int rcg = launch_guard(ctx, coarse, 0, min_gain);
+  if (rcg) return rcg;
+  (++ctx->launches), k_fx_dir<V><<<nred, PF_TV, 0, ctx->stream>>>(ctx->slot_tile, nslots, ctx->ctl, kind, m, A.ec);
+  PF_CUDA_TRY(cudaGetLastError());
+  return PF_OK;
+}
+
+// The iteration body captured once; replays are launched like one kernel.
+struct IterGraph {
+  cudaGraphExec_t exec = nullptr;
+  long long launches = 0;  // kernels per replay
+  ~IterGraph() {
+    if (exec) cudaGraphExecDestroy(exec);
+  }
+};
+
+template <typename V>
+int capture_iteration(pf_ctx* ctx, int nslots, int nred, const uint8_t* kind, const FlexVec<V>& m, int precond,
+                      double min_gain, IterGraph* g) {
+  const long long before = ctx->launches;
+  PF_CUDA_TRY(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  const int rc = launch_iteration<V>(ctx, nslots, nred, kind, m, precond, min_gain);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+  if (rc) {
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+  }
+  PF_CUDA_TRY(e);
+  const cudaError_t ei = cudaGraphInstantiate(&g->exec, graph, 0);
+  cudaGraphDestroy(graph);
+  PF_CUDA_TRY(ei);
+  g->launches = ctx->launches - before;
+  ctx->launches = before;
+  return PF_OK;
 }
 
 // Flexible PCG from x = 0 on r_init until max|r| < max(tol_abs, tol_rel max|r0|).
@@ -316,19 +442,27 @@ template <typename V>
 int flex_solve(pf_ctx* ctx, int nslots, int nred, const uint8_t* kind, FlexVec<V> m, const double* r_init,
                double tol_abs, double tol_rel, int max_iter, int check_every, int precond, double min_gain,
                int reset_guard, SolveCtl* out) {
-  DevGrid G = dev_grid(ctx);
-  const float* ec = ((CoarseCtx*)ctx->learned)->op.ec;
+  CoarseOp& A = ((CoarseCtx*)ctx->learned)->op;
   const bool coarse = precond != PF_PRECOND_JACOBI;
   (++ctx->launches), k_fx_set<<<1, 1, 0, ctx->stream>>>(ctx->ctl, tol_abs, tol_rel, max_iter, coarse ? 1.0 : 0.0,
                                                         reset_guard);
-  (++ctx->launches), k_fx_start<V><<<nred, PF_TV, 0, ctx->stream>>>(nslots, ctx->ctl, kind, r_init, m, ctx->partials);
+  float* rc_part = coarse ? ((CoarseCtx*)ctx->learned)->rc_part : nullptr;
+  (++ctx->launches), k_fx_start<V><<<nred, PF_TV, 0, ctx->stream>>>(nslots, ctx->ctl, kind, r_init, m, rc_part,
+                                                                    ctx->partials);
   int rc = PF_OK;
-  if (coarse) rc = apply_coarse<V>(ctx, nslots, kind, m.r, precond);
+  if (coarse) rc = coarse_solve(ctx, nslots, precond);
   if (rc) return rc;
-  (++ctx->launches), k_fx_precond<V><<<nred, PF_TV, 0, ctx->stream>>>(ctx->slot_tile, nslots, ctx->ctl, kind, m, ec, 1,
-                                                                      min_gain, ctx->partials);
-  (++ctx->launches), k_fx_dir<V><<<nred, PF_TV, 0, ctx->stream>>>(ctx->slot_tile, nslots, ctx->ctl, kind, m, ec);
+  rc = launch_guard(ctx, coarse, 1, min_gain);
+  if (rc) return rc;
+  (++ctx->launches), k_fx_dir<V><<<nred, PF_TV, 0, ctx->stream>>>(ctx->slot_tile, nslots, ctx->ctl, kind, m, A.ec);
   PF_CUDA_TRY(cudaGetLastError());
+  // the exact coarse solve records training pairs on the host side, so it is
+  // launched directly; the other bodies are replayed from a graph
+  IterGraph graph;
+  if (precond != PF_PRECOND_EXACT_COARSE) {
+    rc = capture_iteration<V>(ctx, nslots, nred, kind, m, precond, min_gain, &graph);
+    if (rc) return rc;
+  }
   SolveCtl c{};
   rc = poll_ctl(ctx, &c);
   if (rc) return rc;
@@ -337,35 +471,20 @@ int flex_solve(pf_ctx* ctx, int nslots, int nred, const uint8_t* kind, FlexVec<V
   while (!c.done && launched < max_iter) {
     const int nb = std::min(batch, max_iter - launched);
     for (int q = 0; q < nb; ++q) {
-      (++ctx->launches), k_fx_spmv<V><<<nred, PF_TV, 0, ctx->stream>>>(G, nslots, ctx->ctl, kind, m, ctx->partials);
-      (++ctx->launches), k_fx_update<V><<<nred, PF_TV, 0, ctx->stream>>>(nslots, ctx->ctl, kind, m, ctx->partials);
-      if (coarse) {
-        rc = apply_coarse<V>(ctx, nslots, kind, m.r, precond);
+      if (graph.exec) {
+        PF_CUDA_TRY(cudaGraphLaunch(graph.exec, ctx->stream));
+        ctx->launches += graph.launches;
+      } else {
+        rc = launch_iteration<V>(ctx, nslots, nred, kind, m, precond, min_gain);
         if (rc) return rc;
       }
-      (++ctx->launches), k_fx_precond<V><<<nred, PF_TV, 0, ctx->stream>>>(ctx->slot_tile, nslots, ctx->ctl, kind, m,
-                                                                          ec, 0, min_gain, ctx->partials);
-      (++ctx->launches), k_fx_dir<V><<<nred, PF_TV, 0, ctx->stream>>>(ctx->slot_tile, nslots, ctx->ctl, kind, m, ec);
     }
-    PF_CUDA_TRY(cudaGetLastError());
     launched += nb;
     rc = poll_ctl(ctx, &c);
     if (rc) return rc;
     if (check_every <= 0) batch = std::min(batch * 2, 64);
   }
   *out = c;
-  return PF_OK;
-}
-
-int ensure_z64(pf_ctx* ctx, double** z) {
-  CoarseCtx* cc = (CoarseCtx*)ctx->learned;
-  if (cc->z64_cap < ctx->cells_cap) {
-    if (cc->z64) cudaFree(cc->z64);
-    cc->z64 = nullptr;
-    PF_CUDA_TRY(cudaMalloc(&cc->z64, ctx->cells_cap * sizeof(double)));
-    cc->z64_cap = ctx->cells_cap;
-  }
-  *z = cc->z64;
   return PF_OK;
 }
 
@@ -400,14 +519,13 @@ int solve_learned(pf_ctx* ctx, int nslots, int nred, const uint8_t* kind, double
     res->res_final = c.res0;
     return PF_OK;
   }
-  DevGrid G = dev_grid(ctx);
+  int* nbr = nullptr;
+  rc = build_neighbor_table(ctx, nslots, &nbr);
+  if (rc) return rc;
 
   if (!cfg->inner_fp32) {
     // FP64 flexible PCG on the exact operator
-    double* z64 = nullptr;
-    rc = ensure_z64(ctx, &z64);
-    if (rc) return rc;
-    FlexVec<double> m{ctx->x, ctx->r, ctx->Ap, z64, ctx->p, ctx->diag, ctx->cx, ctx->cy, ctx->cz, cls, scale};
+    FlexVec<double> m{ctx->x, ctx->r, ctx->Ap, ctx->p, ctx->diag, ctx->cx, ctx->cy, ctx->cz, cls, scale};
     SolveCtl o{};
     rc = flex_solve<double>(ctx, nslots, nred, kind, m, ctx->r, cfg->abs_tol, cfg->rel_tol, cfg->max_iter,
                             cfg->check_every, precond, cfg->accept_min_gain, 1, &o);
@@ -430,9 +548,7 @@ int solve_learned(pf_ctx* ctx, int nslots, int nred, const uint8_t* kind, double
                                                                     ctx->r, scale, ctx->diagf, ctx->cxf, ctx->cyf,
                                                                     ctx->czf, ctx->b64);
   PF_CUDA_TRY(cudaGetLastError());
-  // z needs its own FP32 array: the BF16 coupling buffer (6 bytes per cell) is unused here
-  FlexVec<float> m{ctx->xf, ctx->rf, ctx->Apf, (float*)ctx->cbf, ctx->pf32, ctx->diagf,
-                   ctx->cxf, ctx->cyf, ctx->czf, cls, 1.0f};
+  FlexVec<float> m{ctx->xf, ctx->rf, ctx->Apf, ctx->pf32, ctx->diagf, ctx->cxf, ctx->cyf, ctx->czf, cls, 1.0f};
   const double tol = c.tol;
   double resid = c.res0;
   int iters = 0, sweeps = 0;
@@ -449,7 +565,7 @@ int solve_learned(pf_ctx* ctx, int nslots, int nred, const uint8_t* kind, double
     res->precond_applied = ic.accepted;
     res->precond_rejected = ic.rejected;
     (++ctx->launches), k_fx_add<<<nred, PF_TV, 0, ctx->stream>>>(nslots, kind, ctx->x, m.e);
-    (++ctx->launches), k_fx_residual<<<nred, PF_TV, 0, ctx->stream>>>(G, nslots, ctx->ctl, kind, ctx->x, ctx->diag,
+    (++ctx->launches), k_fx_residual<<<nred, PF_TV, 0, ctx->stream>>>(nbr, nslots, ctx->ctl, kind, ctx->x, ctx->diag,
                                                                       ctx->cx, ctx->cy, ctx->cz, ctx->b64, scale,
                                                                       ctx->r, ctx->partials);
     PF_CUDA_TRY(cudaGetLastError());

@@ -130,6 +130,7 @@ struct SolveCtl {
   int touches_air;
   int min_fluid;
   int accepted, rejected;  // learned preconditioner outcomes
+  double flex[2];          // flexible PCG: r.D^-1 r and r.z_prev of the current residual
 };
 
 }  // namespace pf

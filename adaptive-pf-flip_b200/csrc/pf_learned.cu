@@ -4,11 +4,13 @@
 // operator applied to the restricted residual:
 //
 //   e = S G^T G S r_c,    S = diag(d_c)^-1/2 over live coarse unknowns,
-//   G r = (h_0, h_1, h_2, h_3),  h_0 = g_0 * C_0 r,  h_l = g_l * C_l P h_{l-1},
+//   G r = (h_0, ..., h_{L-1}),  h_0 = g_0 * C_0 r,  h_l = g_l * C_min(l,3) P h_{l-1},
 //
 // where C_l are 3x3x3 convolutions (2->8, then 8->8 channels) on the tile
-// lattice and its three 2x coarser levels, P is 2x2x2 average pooling and the
-// g_l are per-position, per-channel gates.  The gates depend on the coarse
+// lattice and its 2x coarser levels down to 2 tiles per axis (L = 4..8, the
+// last convolution shared by the levels below the fourth), P is 2x2x2
+// average pooling and the g_l are per-position, per-channel gates -- a
+// learned multilevel (BPX-like) additive operator.  The gates depend on the coarse
 // operator only: a 4-level U-Net (3x3x3 convolutions with bias and ReLU,
 // 16-64 channels, skip concatenations) maps scale-free features of A_c to
 // g_0 once per solve, and g_{l+1} = P g_l.  Because e is linear and
@@ -26,15 +28,33 @@ namespace pf {
 
 namespace {
 
+constexpr int kMaxLevels = 8;
+
 Dims make_dims(int X, int Y, int Z) { return Dims{X, Y, Z, X * Y * Z}; }
+
+Dims halve(const Dims& d) { return make_dims((d.X + 1) / 2, (d.Y + 1) / 2, (d.Z + 1) / 2); }
+
+// levels of G: halve until every extent is <= 2 (at least 4, at most kMaxLevels)
+int g_levels(Dims d) {
+  int n = 1;
+  while (std::max(d.X, std::max(d.Y, d.Z)) > 2 && n < kMaxLevels) {
+    d = halve(d);
+    ++n;
+  }
+  return std::max(4, n);
+}
+
+// G layer of level l: the last one is shared by every deeper level
+int g_layer(int l) { return L_G0 + std::min(l, 3); }
 
 // Device buffers for one batch size and lattice: the gate U-Net (one sample)
 // and the G path (B samples).  Every G-path tensor has channel stride kGS.
 struct Work {
   int B = 0, Balloc = 0;
   bool bwd = false;
-  Dims D[4]{};
-  size_t cap[4] = {0, 0, 0, 0};
+  int NL = 0;  // levels of G (the U-Net uses the first four)
+  Dims D[kMaxLevels]{};
+  size_t cap[kMaxLevels] = {};
   // U-Net forward (one sample)
   float *F = nullptr, *a0 = nullptr, *s0 = nullptr, *q1 = nullptr, *a1 = nullptr, *s1 = nullptr, *q2 = nullptr,
         *a2 = nullptr, *s2 = nullptr, *q3 = nullptr, *a3 = nullptr, *b3 = nullptr, *c2 = nullptr, *u2 = nullptr,
@@ -43,10 +63,12 @@ struct Work {
   float *g0a = nullptr, *g0b = nullptr, *g0c = nullptr, *g1a = nullptr, *g1b = nullptr, *g1c = nullptr,
         *g2a = nullptr, *g2b = nullptr, *g2c = nullptr, *g3a = nullptr, *g3b = nullptr;
   // gates (one sample) and their gradients
-  float *gam[4] = {}, *dgam[4] = {};
-  // G path (B samples)
-  float *x0 = nullptr, *a[4] = {}, *h[4] = {}, *q[4] = {}, *b[4] = {}, *t[4] = {}, *v[4] = {}, *e = nullptr;
-  float *de = nullptr, *dxe = nullptr, *dt[4] = {}, *dh[4] = {}, *dv[4] = {}, *da[4] = {}, *dq[4] = {};
+  float *gam[kMaxLevels] = {}, *dgam[kMaxLevels] = {};
+  // G path (B samples); q[0] is the scaled input S rc
+  float *a[kMaxLevels] = {}, *h[kMaxLevels] = {}, *q[kMaxLevels] = {}, *b[kMaxLevels] = {}, *t[kMaxLevels] = {},
+        *v[kMaxLevels] = {}, *e = nullptr;
+  float *de = nullptr, *dt[kMaxLevels] = {}, *dh[kMaxLevels] = {}, *dv[kMaxLevels] = {}, *da[kMaxLevels] = {},
+        *dq[kMaxLevels] = {};
   double *v64 = nullptr, *den = nullptr, *loss = nullptr;
   std::vector<void*> owned;
 };
@@ -96,6 +118,8 @@ int grid_for(size_t n, int threads = 256) {
 
 size_t frag_count(int cin, int cout) { return (size_t)27 * (pad16(cin) / 16) * (pad8(cout) / 8) * 32; }
 
+int allow_brick_smem(pf_ctx* ctx);
+
 int state_init(pf_ctx* ctx, LearnedState* L) {
   size_t o = 0;
   for (int l = 0; l < kNumLayers; ++l) {
@@ -116,7 +140,7 @@ int state_init(pf_ctx* ctx, LearnedState* L) {
     PF_CUDA_TRY(cudaMalloc(&L->wt[l], frag_count(co, ci) * sizeof(uint2)));
   }
   PF_CUDA_TRY(cudaMalloc(&L->wpart, (size_t)kWgradCtas * 27 * 128 * 64 * sizeof(float)));
-  return PF_OK;
+  return allow_brick_smem(ctx);
 }
 
 LearnedState* get_state(pf_ctx* ctx, int* rc) {
@@ -150,25 +174,28 @@ void work_free(Work& W) {
 }
 
 int work_ensure(pf_ctx* ctx, Work& W, Dims d0, int B, bool bwd) {
-  Dims D[4];
+  const int NL = g_levels(d0);
+  Dims D[kMaxLevels];
   D[0] = d0;
-  for (int l = 1; l < 4; ++l) D[l] = make_dims((D[l - 1].X + 1) / 2, (D[l - 1].Y + 1) / 2, (D[l - 1].Z + 1) / 2);
+  for (int l = 1; l < NL; ++l) D[l] = halve(D[l - 1]);
   // buffers hold Balloc samples of up to cap[l] positions per level
   bool fits = W.Balloc >= B && (W.bwd || !bwd);
-  for (int l = 0; l < 4 && fits; ++l) fits = (size_t)D[l].n <= W.cap[l];
+  for (int l = 0; l < NL && fits; ++l) fits = (size_t)D[l].n <= W.cap[l];
   if (fits) {
     W.B = B;
-    for (int l = 0; l < 4; ++l) W.D[l] = D[l];
+    W.NL = NL;
+    for (int l = 0; l < NL; ++l) W.D[l] = D[l];
     return PF_OK;
   }
   work_free(W);
-  size_t n[4], P[4];
-  for (int l = 0; l < 4; ++l) {
+  size_t n[kMaxLevels], P[kMaxLevels];
+  for (int l = 0; l < NL; ++l) {
     n[l] = (size_t)D[l].n;
     P[l] = (size_t)B * n[l];
     W.cap[l] = n[l];
     W.D[l] = D[l];
   }
+  W.NL = NL;
   W.B = B;
   W.Balloc = B;
   W.bwd = bwd;
@@ -202,15 +229,14 @@ int work_ensure(pf_ctx* ctx, Work& W, Dims d0, int B, bool bwd) {
   alloc(&W.o, n[0] * 16);
   alloc(&W.sc, 2);
   W.gam[0] = W.o;
-  for (int l = 1; l < 4; ++l) alloc(&W.gam[l], n[l] * kGS);
-  alloc(&W.x0, P[0] * kGS);
-  for (int l = 0; l < 4; ++l) {
+  for (int l = 1; l < NL; ++l) alloc(&W.gam[l], n[l] * kGS);
+  for (int l = 0; l < NL; ++l) {
     alloc(&W.a[l], P[l] * kGS);
     alloc(&W.h[l], P[l] * kGS);
     alloc(&W.t[l], P[l] * kGS);
     alloc(&W.v[l], P[l] * kGS);
-    if (l > 0) alloc(&W.q[l], P[l] * kGS);
-    if (bwd && l < 3) alloc(&W.b[l], P[l] * kGS);
+    alloc(&W.q[l], P[l] * kGS);
+    if (bwd && l < NL - 1) alloc(&W.b[l], P[l] * kGS);
   }
   alloc(&W.e, P[0] * 2);
   if (bwd) {
@@ -226,8 +252,7 @@ int work_ensure(pf_ctx* ctx, Work& W, Dims d0, int B, bool bwd) {
     alloc(&W.g3a, n[3] * 64);
     alloc(&W.g3b, n[3] * 64);
     alloc(&W.de, P[0] * kGS);
-    alloc(&W.dxe, P[0] * kGS);
-    for (int l = 0; l < 4; ++l) {
+    for (int l = 0; l < NL; ++l) {
       alloc(&W.dgam[l], n[l] * kGS);
       alloc(&W.dt[l], P[l] * kGS);
       alloc(&W.dh[l], P[l] * kGS);
@@ -252,7 +277,7 @@ int work_ensure(pf_ctx* ctx, Work& W, Dims d0, int B, bool bwd) {
 // layers
 
 int conv(pf_ctx* ctx, LearnedState* L, int layer, const float* x, int xs, const float* gate, bool transpose,
-         float* y, int ys, Dims d, int B, const SolveCtl* skip) {
+         float* y, int ys, Dims d, int B, const SolveCtl* skip, const float* gmul = nullptr) {
   const LayerSpec& s = kLayers[layer];
   ConvArgs a;
   a.x = x;
@@ -267,22 +292,40 @@ int conv(pf_ctx* ctx, LearnedState* L, int layer, const float* x, int xs, const 
   a.d = d;
   a.P = B * d.n;
   a.skip = skip;
-  if (xs != pad16(transpose ? s.cout : s.cin) || ys < pad8(a.cout))
+  a.gmul = gmul;
+  if (xs != pad16(transpose ? s.cout : s.cin) || ys < pad8(a.cout) || (gmul && (a.bias || a.relu)))
     return set_error(ctx, PF_ERR_INVALID, "learned: channel stride mismatch");
   const int NT = pad8(a.cout) / 8;
-  const int blocks = (a.P + 63) / 64;
+  const int bx = (d.X + kBrick - 1) / kBrick, by = (d.Y + kBrick - 1) / kBrick, bz = (d.Z + kBrick - 1) / kBrick;
+  const int blocks = B * bx * by * bz;
+  const int KC = xs / 16;
+  a.stage_w = brick_smem_w(KC, NT) <= kStageWeightsMax ? 1 : 0;
+  const size_t smem = (size_t)brick_smem_halo(KC) + (a.stage_w ? brick_smem_w(KC, NT) : 0);
   ++ctx->launches;
   switch (NT) {
-    case 1: k_conv<1><<<blocks, 128, 0, ctx->stream>>>(a); break;
-    case 2: k_conv<2><<<blocks, 128, 0, ctx->stream>>>(a); break;
-    case 4: k_conv<4><<<blocks, 128, 0, ctx->stream>>>(a); break;
-    case 6: k_conv<6><<<blocks, 128, 0, ctx->stream>>>(a); break;
-    case 8: k_conv<8><<<blocks, 128, 0, ctx->stream>>>(a); break;
-    case 12: k_conv<12><<<blocks, 128, 0, ctx->stream>>>(a); break;
-    case 16: k_conv<16><<<blocks, 128, 0, ctx->stream>>>(a); break;
+    case 1: k_conv_brick<1><<<blocks, 128, smem, ctx->stream>>>(a, bx, by, bz); break;
+    case 2: k_conv_brick<2><<<blocks, 128, smem, ctx->stream>>>(a, bx, by, bz); break;
+    case 4: k_conv_brick<4><<<blocks, 128, smem, ctx->stream>>>(a, bx, by, bz); break;
+    case 6: k_conv_brick<6><<<blocks, 128, smem, ctx->stream>>>(a, bx, by, bz); break;
+    case 8: k_conv_brick<8><<<blocks, 128, smem, ctx->stream>>>(a, bx, by, bz); break;
+    case 12: k_conv_brick<12><<<blocks, 128, smem, ctx->stream>>>(a, bx, by, bz); break;
+    case 16: k_conv_brick<16><<<blocks, 128, smem, ctx->stream>>>(a, bx, by, bz); break;
     default: return set_error(ctx, PF_ERR_INVALID, "learned: unsupported channel count");
   }
   PF_CUDA_TRY(cudaGetLastError());
+  return PF_OK;
+}
+
+// the widest input (128 channels) stages 58.75 KB, more than the default 48 KB
+int allow_brick_smem(pf_ctx* ctx) {
+  const int bytes = brick_smem_halo(8) + kStageWeightsMax;
+  PF_CUDA_TRY(cudaFuncSetAttribute(k_conv_brick<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  PF_CUDA_TRY(cudaFuncSetAttribute(k_conv_brick<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  PF_CUDA_TRY(cudaFuncSetAttribute(k_conv_brick<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  PF_CUDA_TRY(cudaFuncSetAttribute(k_conv_brick<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  PF_CUDA_TRY(cudaFuncSetAttribute(k_conv_brick<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  PF_CUDA_TRY(cudaFuncSetAttribute(k_conv_brick<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  PF_CUDA_TRY(cudaFuncSetAttribute(k_conv_brick<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
   return PF_OK;
 }
 
@@ -355,7 +398,7 @@ int unet_forward(pf_ctx* ctx, LearnedState* L, Work& W, const float* cop, const 
   rc = rc ? rc : conv(ctx, L, L_D0, W.c0, 48, nullptr, false, W.u0, 16, D[0], 1, skip);
   rc = rc ? rc : conv(ctx, L, L_OUT, W.u0, 16, nullptr, false, W.o, 16, D[0], 1, skip);
   if (rc) return rc;
-  for (int l = 0; l < 3; ++l) pool_to(W.gam[l], kGS, l, W.gam[l + 1]);
+  for (int l = 0; l + 1 < W.NL; ++l) pool_to(W.gam[l], kGS, l, W.gam[l + 1]);
   PF_CUDA_TRY(cudaGetLastError());
   return PF_OK;
 }
@@ -400,28 +443,31 @@ int unet_backward(pf_ctx* ctx, LearnedState* L, Work& W) {
 
 int gtg_forward(pf_ctx* ctx, LearnedState* L, Work& W, const float* cop, const float* rc_in, float* e_out,
                 const SolveCtl* skip) {
-  const int B = W.B;
+  const int B = W.B, NL = W.NL;
   const Dims* D = W.D;
   int rc = 0;
   auto n16 = [&](int l) { return (size_t)B * D[l].n * kGS; };
   ++ctx->launches;
-  k_scale_in<<<grid_for(n16(0)), 256, 0, ctx->stream>>>(rc_in, 0, cop, D[0].n, B, W.x0, skip);
-  const int layer[4] = {L_G0, L_G1, L_G2, L_G3};
-  for (int l = 0; l < 4 && !rc; ++l) {
-    const float* in = l == 0 ? W.x0 : W.q[l];
+  k_scale_in<<<grid_for(n16(0)), 256, 0, ctx->stream>>>(rc_in, 0, cop, D[0].n, B, W.q[0], skip);
+  for (int l = 0; l < NL && !rc; ++l) {
     if (l > 0) {
       ++ctx->launches;
       k_pool<<<grid_for(n16(l)), 256, 0, ctx->stream>>>(W.h[l - 1], kGS, D[l - 1], D[l], B, W.q[l], skip);
     }
-    rc = conv(ctx, L, layer[l], in, kGS, nullptr, false, W.a[l], kGS, D[l], B, skip);
-    ++ctx->launches;
-    k_gmul<<<grid_for(n16(l)), 256, 0, ctx->stream>>>(W.h[l], W.gam[l], W.a[l], D[l].n, B, skip);
+    if (W.bwd) {  // training keeps the ungated a_l for the gate gradient
+      rc = conv(ctx, L, g_layer(l), W.q[l], kGS, nullptr, false, W.a[l], kGS, D[l], B, skip);
+      ++ctx->launches;
+      k_gmul<<<grid_for(n16(l)), 256, 0, ctx->stream>>>(W.h[l], W.gam[l], W.a[l], D[l].n, B, skip);
+    } else {
+      rc = conv(ctx, L, g_layer(l), W.q[l], kGS, nullptr, false, W.h[l], kGS, D[l], B, skip, W.gam[l]);
+    }
   }
   if (rc) return rc;
   ++ctx->launches;
-  k_gmul<<<grid_for(n16(3)), 256, 0, ctx->stream>>>(W.t[3], W.gam[3], W.h[3], D[3].n, B, skip);
-  for (int l = 3; l >= 1 && !rc; --l) {
-    rc = conv(ctx, L, layer[l], W.t[l], kGS, nullptr, true, W.v[l], kGS, D[l], B, skip);
+  k_gmul<<<grid_for(n16(NL - 1)), 256, 0, ctx->stream>>>(W.t[NL - 1], W.gam[NL - 1], W.h[NL - 1], D[NL - 1].n, B,
+                                                         skip);
+  for (int l = NL - 1; l >= 1 && !rc; --l) {
+    rc = conv(ctx, L, g_layer(l), W.t[l], kGS, nullptr, true, W.v[l], kGS, D[l], B, skip);
     ++ctx->launches;
     k_up_add_gate<<<grid_for(n16(l - 1)), 256, 0, ctx->stream>>>(W.h[l - 1], W.v[l], W.gam[l - 1], D[l - 1], D[l], B,
                                                                   W.b[l - 1], W.t[l - 1], skip);
@@ -437,52 +483,46 @@ int gtg_forward(pf_ctx* ctx, LearnedState* L, Work& W, const float* cop, const f
 
 // gradients of <de, e> into the G weights (accumulated) and dgam[0] (gates folded to level 0)
 int gtg_backward(pf_ctx* ctx, LearnedState* L, Work& W, const float* cop) {
-  const int B = W.B;
+  const int B = W.B, NL = W.NL;
   const Dims* D = W.D;
   auto n16 = [&](int l) { return (size_t)B * D[l].n * kGS; };
   auto g16 = [&](int l) { return (size_t)D[l].n * kGS; };
-  const int layer[4] = {L_G0, L_G1, L_G2, L_G3};
   int rc = 0;
-  for (int l = 0; l < 4; ++l) {
+  for (int l = 0; l < NL; ++l) {
     ++ctx->launches;
     k_zero_f<<<grid_for(g16(l)), 256, 0, ctx->stream>>>(W.dgam[l], g16(l));
   }
-  // transposed half, fine to coarse
-  ++ctx->launches;
-  k_scale_in<<<grid_for(n16(0)), 256, 0, ctx->stream>>>(W.de, 1, cop, D[0].n, B, W.dxe, nullptr);
-  rc = rc ? rc : conv(ctx, L, L_G0, W.dxe, kGS, nullptr, false, W.dt[0], kGS, D[0], B, nullptr);
-  rc = rc ? rc : wgrad_acc(ctx, L, L_G0, W.dxe, kGS, W.t[0], nullptr, kGS, D[0], B);
-  for (int l = 0; l < 3 && !rc; ++l) {
+  // transposed half, fine to coarse: dv_l = (l ? P dh_{l-1} : S de), dt_l = C_l dv_l
+  for (int l = 0; l < NL && !rc; ++l) {
     ++ctx->launches;
-    k_gate_grad<<<grid_for(g16(l)), 256, 0, ctx->stream>>>(W.dgam[l], W.dt[l], W.b[l], D[l].n, B);
+    if (l == 0)
+      k_scale_in<<<grid_for(n16(0)), 256, 0, ctx->stream>>>(W.de, 1, cop, D[0].n, B, W.dv[0], nullptr);
+    else
+      k_pool<<<grid_for(n16(l)), 256, 0, ctx->stream>>>(W.dh[l - 1], kGS, D[l - 1], D[l], B, W.dv[l], nullptr);
+    rc = conv(ctx, L, g_layer(l), W.dv[l], kGS, nullptr, false, W.dt[l], kGS, D[l], B, nullptr);
+    rc = rc ? rc : wgrad_acc(ctx, L, g_layer(l), W.dv[l], kGS, W.t[l], nullptr, kGS, D[l], B);
+    ++ctx->launches;
+    k_gate_grad<<<grid_for(g16(l)), 256, 0, ctx->stream>>>(W.dgam[l], W.dt[l], l < NL - 1 ? W.b[l] : W.h[l], D[l].n,
+                                                          B);
     ++ctx->launches;
     k_gmul<<<grid_for(n16(l)), 256, 0, ctx->stream>>>(W.dh[l], W.gam[l], W.dt[l], D[l].n, B, nullptr);
-    ++ctx->launches;
-    k_pool<<<grid_for(n16(l + 1)), 256, 0, ctx->stream>>>(W.dh[l], kGS, D[l], D[l + 1], B, W.dv[l + 1], nullptr);
-    rc = conv(ctx, L, layer[l + 1], W.dv[l + 1], kGS, nullptr, false, W.dt[l + 1], kGS, D[l + 1], B, nullptr);
-    rc = rc ? rc : wgrad_acc(ctx, L, layer[l + 1], W.dv[l + 1], kGS, W.t[l + 1], nullptr, kGS, D[l + 1], B);
   }
-  if (rc) return rc;
-  ++ctx->launches;
-  k_gate_grad<<<grid_for(g16(3)), 256, 0, ctx->stream>>>(W.dgam[3], W.dt[3], W.h[3], D[3].n, B);
-  ++ctx->launches;
-  k_gmul<<<grid_for(n16(3)), 256, 0, ctx->stream>>>(W.dh[3], W.gam[3], W.dt[3], D[3].n, B, nullptr);
   // forward half, coarse to fine
-  for (int l = 3; l >= 0 && !rc; --l) {
+  for (int l = NL - 1; l >= 0 && !rc; --l) {
     ++ctx->launches;
     k_gmul<<<grid_for(n16(l)), 256, 0, ctx->stream>>>(W.da[l], W.gam[l], W.dh[l], D[l].n, B, nullptr);
     ++ctx->launches;
     k_gate_grad<<<grid_for(g16(l)), 256, 0, ctx->stream>>>(W.dgam[l], W.a[l], W.dh[l], D[l].n, B);
-    rc = wgrad_acc(ctx, L, layer[l], l == 0 ? W.x0 : W.q[l], kGS, W.da[l], nullptr, kGS, D[l], B);
+    rc = wgrad_acc(ctx, L, g_layer(l), W.q[l], kGS, W.da[l], nullptr, kGS, D[l], B);
     if (l > 0 && !rc) {
-      rc = conv(ctx, L, layer[l], W.da[l], kGS, nullptr, true, W.dq[l], kGS, D[l], B, nullptr);
+      rc = conv(ctx, L, g_layer(l), W.da[l], kGS, nullptr, true, W.dq[l], kGS, D[l], B, nullptr);
       ++ctx->launches;
       k_pool_bwd<<<grid_for(n16(l - 1)), 256, 0, ctx->stream>>>(W.dq[l], kGS, D[l - 1], D[l], B, W.dh[l - 1]);
     }
   }
   if (rc) return rc;
   // g_{l+1} = P g_l
-  for (int l = 2; l >= 0; --l) {
+  for (int l = NL - 2; l >= 0; --l) {
     ++ctx->launches;
     k_pool_bwd<<<grid_for(g16(l)), 256, 0, ctx->stream>>>(W.dgam[l + 1], kGS, D[l], D[l + 1], 1, W.dgam[l]);
   }

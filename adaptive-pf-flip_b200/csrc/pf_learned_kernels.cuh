@@ -103,7 +103,6 @@ __global__ void k_pack(const float* W, int cin, int cout, int transpose, uint2* 
 
 // ---------------------------------------------------------------------------
 // convolution: y[p][co] = act(bias[co] + sum_tap sum_ci x[p+tap][ci] w[tap][ci][co])
-// One warp computes 16 positions x all NT*8 output channels; 4 warps per CTA.
 
 struct ConvArgs {
   const float* x;
@@ -117,78 +116,103 @@ struct ConvArgs {
   Dims d;
   int P;              // positions (batch * d.n)
   const SolveCtl* skip;
+  const float* gmul;  // optional: y = gmul[p mod d.n] * acc (one sample, stride ys; layers without bias/ReLU)
+  int stage_w;        // brick kernel: copy the weight fragments to shared memory first
 };
 
+// ---------------------------------------------------------------------------
+// The input is staged once per CTA: a CTA owns a 4x4x4
+// brick of positions of one sample and loads the brick plus its one-position
+// halo (6x6x6 positions, every input channel, gated) into shared memory as
+// BF16; the 27 taps then read their A fragments from there.  Warp w computes
+// z-slice w of the brick (16 positions = the M rows of one mma tile).
+
+constexpr int kBrick = 4;
+constexpr int kHalo = kBrick + 2;
+constexpr int kHaloN = kHalo * kHalo * kHalo;
+
+__host__ __device__ constexpr int brick_pitch(int KC) { return KC * 16 + 8; }  // BF16 per halo position
+__host__ __device__ constexpr int brick_smem_halo(int KC) { return (kHaloN * brick_pitch(KC) * 2 + 15) & ~15; }
+// weight fragments of a layer with KC input and NT output chunks, in bytes
+__host__ __device__ constexpr int brick_smem_w(int KC, int NT) { return 27 * KC * NT * 32 * 8; }
+constexpr int kStageWeightsMax = 16 * 1024;  // stage weight fragments up to this size
+
 template <int NT>
-__global__ void __launch_bounds__(128) k_conv(ConvArgs a) {
+__global__ void __launch_bounds__(128) k_conv_brick(ConvArgs a, int bx, int by, int bz) {
   if (a.skip && a.skip->done) return;
+  extern __shared__ __align__(16) unsigned char conv_smem[];
+  __nv_bfloat16* S = reinterpret_cast<__nv_bfloat16*>(conv_smem);
+  const int KC = a.xs / 16;
+  const int pitch = brick_pitch(KC);
+  int brick = blockIdx.x;
+  const int per_sample = bx * by * bz;
+  const int b = brick / per_sample;
+  brick -= b * per_sample;
+  const int X0 = (brick % bx) * kBrick, Y0 = ((brick / bx) % by) * kBrick, Z0 = (brick / (bx * by)) * kBrick;
+  // small layers also stage their weight fragments (after the halo block)
+  const int nw = a.stage_w ? 27 * KC * NT * 32 : 0;
+  uint2* SW = reinterpret_cast<uint2*>(conv_smem + brick_smem_halo(KC));
+  for (int e = threadIdx.x; e < nw; e += blockDim.x) SW[e] = __ldg(a.wf + e);
+  // stage the halo block, two channels per item
+  const int half = a.xs / 2;
+#pragma unroll 4
+  for (int e = threadIdx.x; e < kHaloN * half; e += blockDim.x) {
+    const int hp = e / half, c2 = (e - hp * half) * 2;
+    const int x = X0 + hp % kHalo - 1, y = Y0 + (hp / kHalo) % kHalo - 1, z = Z0 + hp / (kHalo * kHalo) - 1;
+    float2 v = make_float2(0.0f, 0.0f);
+    if (x >= 0 && y >= 0 && z >= 0 && x < a.d.X && y < a.d.Y && z < a.d.Z) {
+      const size_t q = (size_t)b * a.d.n + x + (size_t)a.d.X * (y + (size_t)a.d.Y * z);
+      v = *reinterpret_cast<const float2*>(a.x + q * a.xs + c2);
+      if (a.gate) {
+        const float2 gv = *reinterpret_cast<const float2*>(a.gate + q * a.xs + c2);
+        if (!(gv.x > 0.0f)) v.x = 0.0f;
+        if (!(gv.y > 0.0f)) v.y = 0.0f;
+      }
+    }
+    *reinterpret_cast<uint32_t*>(S + (size_t)hp * pitch + c2) = pack_bf16(v.x, v.y);
+  }
+  __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g = lane >> 2, t = lane & 3;
-  const int base = (blockIdx.x * 4 + warp) * 16;
-  if (base >= a.P) return;
-  const int KC = a.xs / 16;
-  int rb[2], rx[2], ry[2], rz[2];
-  bool rv[2];
-#pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    const int p = base + g + 8 * h;
-    rv[h] = p < a.P;
-    const int pp = rv[h] ? p : 0;
-    rb[h] = pp / a.d.n;
-    const int tt = pp - rb[h] * a.d.n;
-    rx[h] = tt % a.d.X;
-    ry[h] = (tt / a.d.X) % a.d.Y;
-    rz[h] = tt / (a.d.X * a.d.Y);
-  }
+  // rows g and g + 8 of this warp's 16 positions: (x, y) = (g % 4, g / 4) and (g % 4, g / 4 + 2), z = warp
+  const int lx = g & 3, ly0 = g >> 2, ly1 = ly0 + 2, lz = warp;
   float acc[NT][4];
 #pragma unroll
   for (int j = 0; j < NT; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0f;
   for (int k = 0; k < 27; ++k) {
-    int q[2];
-#pragma unroll
-    for (int h = 0; h < 2; ++h) q[h] = rv[h] ? neighbor(a.d, rb[h], rx[h], ry[h], rz[h], k) : -1;
+    const int hx = lx + 1 + tap_dx(k), hz = lz + 1 + tap_dz(k);
+    const int hp0 = hx + kHalo * (ly0 + 1 + tap_dy(k) + kHalo * hz);
+    const int hp1 = hx + kHalo * (ly1 + 1 + tap_dy(k) + kHalo * hz);
+    const __nv_bfloat16* r0 = S + (size_t)hp0 * pitch + 2 * t;
+    const __nv_bfloat16* r1 = S + (size_t)hp1 * pitch + 2 * t;
     for (int kc = 0; kc < KC; ++kc) {
-      float2 v[2][2];
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        if (q[h] >= 0) {
-          const float* src = a.x + (size_t)q[h] * a.xs + kc * 16 + 2 * t;
-          v[h][0] = *reinterpret_cast<const float2*>(src);
-          v[h][1] = *reinterpret_cast<const float2*>(src + 8);
-          if (a.gate) {
-            const float* gs = a.gate + (size_t)q[h] * a.xs + kc * 16 + 2 * t;
-            const float2 g0 = *reinterpret_cast<const float2*>(gs);
-            const float2 g1 = *reinterpret_cast<const float2*>(gs + 8);
-            if (!(g0.x > 0.0f)) v[h][0].x = 0.0f;
-            if (!(g0.y > 0.0f)) v[h][0].y = 0.0f;
-            if (!(g1.x > 0.0f)) v[h][1].x = 0.0f;
-            if (!(g1.y > 0.0f)) v[h][1].y = 0.0f;
-          }
-        } else {
-          v[h][0] = make_float2(0.0f, 0.0f);
-          v[h][1] = make_float2(0.0f, 0.0f);
-        }
-      }
-      const uint32_t a0 = pack_bf16(v[0][0].x, v[0][0].y);
-      const uint32_t a1 = pack_bf16(v[1][0].x, v[1][0].y);
-      const uint32_t a2 = pack_bf16(v[0][1].x, v[0][1].y);
-      const uint32_t a3 = pack_bf16(v[1][1].x, v[1][1].y);
-      const uint2* wb = a.wf + ((size_t)(k * KC + kc) * NT) * 32 + lane;
+      const uint32_t a0 = *reinterpret_cast<const uint32_t*>(r0 + kc * 16);
+      const uint32_t a1 = *reinterpret_cast<const uint32_t*>(r1 + kc * 16);
+      const uint32_t a2 = *reinterpret_cast<const uint32_t*>(r0 + kc * 16 + 8);
+      const uint32_t a3 = *reinterpret_cast<const uint32_t*>(r1 + kc * 16 + 8);
+      const size_t wo = ((size_t)(k * KC + kc) * NT) * 32 + lane;
 #pragma unroll
       for (int j = 0; j < NT; ++j) {
-        const uint2 b = __ldg(wb + j * 32);
-        mma_bf16(acc[j], a0, a1, a2, a3, b.x, b.y);
+        const uint2 bw = nw ? SW[wo + j * 32] : __ldg(a.wf + wo + j * 32);
+        mma_bf16(acc[j], a0, a1, a2, a3, bw.x, bw.y);
       }
     }
   }
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
-    if (!rv[h]) continue;
-    float* yr = a.y + (size_t)(base + g + 8 * h) * a.ys;
+    const int x = X0 + lx, y = Y0 + (h ? ly1 : ly0), z = Z0 + lz;
+    if (x >= a.d.X || y >= a.d.Y || z >= a.d.Z) continue;
+    const int tpos = x + a.d.X * (y + a.d.Y * z);
+    float* yr = a.y + ((size_t)b * a.d.n + tpos) * a.ys;
+    const float* gr = a.gmul ? a.gmul + (size_t)tpos * a.ys : nullptr;
 #pragma unroll
     for (int j = 0; j < NT; ++j) {
       const int c0 = j * 8 + 2 * t;
       float o0 = acc[j][2 * h], o1 = acc[j][2 * h + 1];
+      if (gr) {
+        o0 *= gr[c0];
+        o1 *= gr[c0 + 1];
+      }
       if (c0 < a.cout) {
         if (a.bias) o0 += a.bias[c0];
         if (a.relu) o0 = fmaxf(o0, 0.0f);

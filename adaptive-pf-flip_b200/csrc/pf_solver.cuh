@@ -28,7 +28,7 @@ enum RedStage {
   kStagePAp = 1,     // after SpMV: p.Ap -> alpha (breakdown check)
   kStageUpdate = 2,  // after x/r update: r.z, max|r| -> convergence, beta
   kStageResid = 3,   // outer refinement: max|b - A x| (FP64)
-  kStageFlex = 4,    // flexible PCG x/r update: max|r| -> convergence (beta comes from the preconditioner step)
+  kStageFlex = 4,    // flexible PCG x/r update: max|r| -> convergence; r.D^-1 r, r.z_prev kept for the guard
 };
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -63,6 +63,8 @@ __device__ __forceinline__ void finalize_stage(SolveCtl* ctl, int stage, double 
   switch (stage) {
     case kStageInit: {
       ctl->rz = S;
+      ctl->flex[0] = S;
+      ctl->flex[1] = S2;
       ctl->res0 = M;
       ctl->res = M;
       double tol = ctl->tol_abs;
@@ -101,7 +103,9 @@ __device__ __forceinline__ void finalize_stage(SolveCtl* ctl, int stage, double 
     case kStageFlex: {
       ctl->it += 1;
       ctl->res = M;
-      if (!isfinite(M)) ctl->done = 4;
+      ctl->flex[0] = S;
+      ctl->flex[1] = S2;
+      if (!isfinite(M) || !isfinite(S) || !isfinite(S2)) ctl->done = 4;
       else if (M < ctl->tol) ctl->done = 1;
       else if (ctl->it >= ctl->max_iter) ctl->done = 3;
       break;
@@ -177,6 +181,25 @@ __device__ __forceinline__ void neighbor_offsets(int s, int l, const int* nbs, l
   off[4] = lz < 7 ? base + l + 64 : (nbs[4] >= 0 ? (long long)nbs[4] * PF_TV + (l & ~448) : -1);
   off[5] = lz > 0 ? base + l - 64 : (nbs[5] >= 0 ? (long long)nbs[5] * PF_TV + (l | 448) : -1);
 }
+
+// The same offsets from a neighbour-slot table nbr[6 s + d] (order as
+// neighbor_slots), read only by the threads on a tile face: the stencil then
+// needs no per-slot shared memory or synchronisation.
+__device__ __forceinline__ void neighbor_offsets_tab(const int* __restrict__ nbr, int s, int l, long long* off) {
+  const int lx = l & 7, ly = (l >> 3) & 7, lz = l >> 6;
+  const long long base = (long long)s * PF_TV;
+  const int* nb = nbr + 6 * (size_t)s;
+  int t;
+  off[0] = lx < 7 ? base + l + 1 : ((t = __ldg(nb + 0)) >= 0 ? (long long)t * PF_TV + (l & ~7) : -1);
+  off[1] = lx > 0 ? base + l - 1 : ((t = __ldg(nb + 1)) >= 0 ? (long long)t * PF_TV + (l | 7) : -1);
+  off[2] = ly < 7 ? base + l + 8 : ((t = __ldg(nb + 2)) >= 0 ? (long long)t * PF_TV + (l & ~56) : -1);
+  off[3] = ly > 0 ? base + l - 8 : ((t = __ldg(nb + 3)) >= 0 ? (long long)t * PF_TV + (l | 56) : -1);
+  off[4] = lz < 7 ? base + l + 64 : ((t = __ldg(nb + 4)) >= 0 ? (long long)t * PF_TV + (l & ~448) : -1);
+  off[5] = lz > 0 ? base + l - 64 : ((t = __ldg(nb + 5)) >= 0 ? (long long)t * PF_TV + (l | 448) : -1);
+}
+
+// nbr[6 s + d] for every pooled slot (pf_flex.cu)
+int build_neighbor_table(pf_ctx* ctx, int nslots, int** nbr);
 
 // solver drivers (pf_pcg.cu)
 int pcg_plain(pf_ctx* ctx, int nslots, int nred, const uint8_t* kind, PcgVec<double> vec, double scale,

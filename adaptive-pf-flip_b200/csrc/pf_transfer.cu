@@ -96,235 +96,6 @@ __device__ __forceinline__ void activate_window(const DevGrid& G, int fv, double
   }
 }
 
-// The same exact test, returned as a 27-bit mask of the touched blocks
-// relative to the 4^3 block (cb0, cb1, cb2) of the particle's cell: bit
-// (rz+1)*9 + (ry+1)*3 + (rx+1) for block cb + (rx, ry, rz).  A window spans
-// nodes c-2..c+2 at most, so offsets stay within -1..1 for particles inside
-// the lattice; `outside` reports the rare case that does not fit.
-__device__ __forceinline__ unsigned window_mask(const DevGrid& G, int fv, double c0, double c1, double c2, int cb0,
-                                                int cb1, int cb2, bool& outside) {
-  const AxisBlocks ax = axis_blocks(c0, G.g.fdim[fv][0]);
-  const AxisBlocks ay = axis_blocks(c1, G.g.fdim[fv][1]);
-  const AxisBlocks az = axis_blocks(c2, G.g.fdim[fv][2]);
-  unsigned mask = 0u;
-#pragma unroll
-  for (int z = 0; z < 2; ++z) {
-    if (z >= az.nb) continue;
-#pragma unroll
-    for (int y = 0; y < 2; ++y) {
-      if (y >= ay.nb) continue;
-#pragma unroll
-      for (int x = 0; x < 2; ++x) {
-        if (x >= ax.nb) continue;
-        const double d2 = __dadd_rn(__dadd_rn(x ? ax.m1 : ax.m0, y ? ay.m1 : ay.m0), z ? az.m1 : az.m0);
-        if (!(d2 < kR2)) continue;
-        const int rx = ax.b0 + x - cb0, ry = ay.b0 + y - cb1, rz = az.b0 + z - cb2;
-        if (rx < -1 || rx > 1 || ry < -1 || ry > 1 || rz < -1 || rz > 1) {
-          outside = true;
-          continue;
-        }
-        mask |= 1u << ((rz + 1) * 9 + (ry + 1) * 3 + (rx + 1));
-      }
-    }
-  }
-  return mask;
-}
-
-__device__ __forceinline__ void flush_mask(const DevGrid& G, int fv, unsigned mask, int cb0, int cb1, int cb2,
-                                           uint8_t* need) {
-  const int fm = fv + 3;
-  while (mask) {
-    const int b = __ffs(mask) - 1;
-    mask &= mask - 1u;
-    const int bx = cb0 + b % 3 - 1, by = cb1 + (b / 3) % 3 - 1, bz = cb2 + b / 9 - 1;
-    const int bi = bx + G.g.bdim[fv][0] * (by + G.g.bdim[fv][1] * bz);
-    if (!G.act4[fv][bi]) G.act4[fv][bi] = 1;
-    if (!G.act4[fm][bi]) G.act4[fm][bi] = 1;
-    uint8_t* nd = &need[tile_id(G.g, bx >> 1, by >> 1, bz >> 1)];
-    if (!*nd) *nd = 1;
-  }
-}
-
-// One pass over the particles: cell bin + warp-aggregated rank, the tile of
-// the particle's cell (pooled for markCells), and the exact activation of
-// u/v/w and their mass fields.  Lanes whose cells share a 4^3 block merge
-// their block masks first, so each activity byte is touched once per warp.
-__global__ void __launch_bounds__(256) k_bin_activate2(DevGrid G, const float* __restrict__ px,
-                                                       const float* __restrict__ py,
-                                                       const float* __restrict__ pz, int n, int* bin_count,
-                                                       int* pkey, int* prank, uint8_t* need, int do_bin,
-                                                       int do_act) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  const unsigned active = __ballot_sync(0xffffffffu, p < n);
-  if (p >= n) return;
-  const double gx = grid_coord(px[p], G.g.ox, G.g.dx);
-  const double gy = grid_coord(py[p], G.g.oy, G.g.dx);
-  const double gz = grid_coord(pz[p], G.g.oz, G.g.dx);
-  const int fi = (int)floor(gx), fj = (int)floor(gy), fk = (int)floor(gz);
-  const int ci = min(max(fi, 0), G.g.nx - 1);
-  const int cj = min(max(fj, 0), G.g.ny - 1);
-  const int ck = min(max(fk, 0), G.g.nz - 1);
-  const int t = tile_id(G.g, ci >> 3, cj >> 3, ck >> 3);
-  if (do_bin) {
-    const int key = t * PF_TV + local_id(ci, cj, ck);
-    const int r = warp_agg_inc(bin_count, key, active);
-    pkey[p] = key;
-    prank[p] = r;
-  }
-  if (!need[t]) need[t] = 1;
-  if (!do_act) return;
-  const int cb0 = fi >> 2, cb1 = fj >> 2, cb2 = fk >> 2;  // arithmetic shift: floor for negatives too
-  bool outside = false;
-  const unsigned mu = window_mask(G, PF_U, gx, __dsub_rn(gy, 0.5), __dsub_rn(gz, 0.5), cb0, cb1, cb2, outside);
-  const unsigned mv = window_mask(G, PF_V, __dsub_rn(gx, 0.5), gy, __dsub_rn(gz, 0.5), cb0, cb1, cb2, outside);
-  const unsigned mw = window_mask(G, PF_W, __dsub_rn(gx, 0.5), __dsub_rn(gy, 0.5), gz, cb0, cb1, cb2, outside);
-  const unsigned long long key = ((unsigned long long)(unsigned)(cb2 + 1048576) << 42) |
-                                 ((unsigned long long)(unsigned)(cb1 + 1048576) << 21) |
-                                 (unsigned long long)(unsigned)(cb0 + 1048576);
-  const unsigned peers = __match_any_sync(active, key);
-  const unsigned au = __reduce_or_sync(peers, mu);
-  const unsigned av = __reduce_or_sync(peers, mv);
-  const unsigned aw = __reduce_or_sync(peers, mw);
-  if ((threadIdx.x & 31) == __ffs(peers) - 1) {
-    flush_mask(G, PF_U, au, cb0, cb1, cb2, need);
-    flush_mask(G, PF_V, av, cb0, cb1, cb2, need);
-    flush_mask(G, PF_W, aw, cb0, cb1, cb2, need);
-  }
-  if (outside) {  // a particle off the lattice: activate its blocks directly
-    activate_window(G, PF_U, gx, __dsub_rn(gy, 0.5), __dsub_rn(gz, 0.5), need);
-    activate_window(G, PF_V, __dsub_rn(gx, 0.5), gy, __dsub_rn(gz, 0.5), need);
-    activate_window(G, PF_W, __dsub_rn(gx, 0.5), __dsub_rn(gy, 0.5), gz, need);
-  }
-}
-
-// Activation with an FP32 fast path.  Per axis the candidate distances come
-// from the cell-local fraction (so the error is ~1e-7 whatever the grid
-// size); a block whose FP32 minimum d^2 is clear of 2.25 by kMargin is decided
-// there, and only blocks inside the band are decided by the exact FP64 test.
-constexpr float kMargin = 1e-5f;
-
-struct AxisBlocksF {
-  int b0, nb;
-  float m0, m1;
-};
-
-__device__ __forceinline__ AxisBlocksF axis_blocks_f(double g, int dim) {
-  const double fl = floor(g);
-  const int i0 = (int)fl;
-  const float fr = (float)(g - fl);
-  const int lo = max(i0 - 1, 0), hi = min(i0 + 2, dim - 1);
-  AxisBlocksF r;
-  r.b0 = lo >> 2;
-  r.nb = lo > hi ? 0 : (hi >> 2) - (lo >> 2) + 1;
-  r.m0 = r.m1 = 1e30f;
-#pragma unroll
-  for (int o = 0; o < 4; ++o) {
-    const int i = i0 - 1 + o;
-    const float d = fr + (float)(1 - o);  // g - i
-    const float dd = d * d;
-    if (i >= lo && i <= hi) {
-      if ((i >> 2) == r.b0) r.m0 = fminf(r.m0, dd);
-      else r.m1 = fminf(r.m1, dd);
-    }
-  }
-  return r;
-}
-
-// Blocks of field fv touched by a particle at grid coordinate g (from the
-// product with 1/dx) and, for the exact fallback, ge (the reference's
-// (pos-o)/dx); offsets c0..c2 are 0 or -0.5 per axis.  Returns the 27-bit
-// mask relative to the cell block (cb0, cb1, cb2); `outside` flags blocks
-// beyond +-1.
-__device__ __forceinline__ unsigned window_mask_fast(const DevGrid& G, int fv, const double* g, const double* ge,
-                                                     const double* sh, int cb0, int cb1, int cb2, bool& outside) {
-  const AxisBlocksF ax = axis_blocks_f(g[0] + sh[0], G.g.fdim[fv][0]);
-  const AxisBlocksF ay = axis_blocks_f(g[1] + sh[1], G.g.fdim[fv][1]);
-  const AxisBlocksF az = axis_blocks_f(g[2] + sh[2], G.g.fdim[fv][2]);
-  unsigned mask = 0u;
-  bool exact_needed = false;
-#pragma unroll
-  for (int z = 0; z < 2; ++z) {
-    if (z >= az.nb) continue;
-#pragma unroll
-    for (int y = 0; y < 2; ++y) {
-      if (y >= ay.nb) continue;
-#pragma unroll
-      for (int x = 0; x < 2; ++x) {
-        if (x >= ax.nb) continue;
-        const float d2 = ((x ? ax.m1 : ax.m0) + (y ? ay.m1 : ay.m0)) + (z ? az.m1 : az.m0);
-        if (d2 > 2.25f + kMargin) continue;
-        if (d2 >= 2.25f - kMargin) {
-          exact_needed = true;
-          continue;
-        }
-        const int rx = ax.b0 + x - cb0, ry = ay.b0 + y - cb1, rz = az.b0 + z - cb2;
-        if (rx < -1 || rx > 1 || ry < -1 || ry > 1 || rz < -1 || rz > 1) {
-          outside = true;
-          continue;
-        }
-        mask |= 1u << ((rz + 1) * 9 + (ry + 1) * 3 + (rx + 1));
-      }
-    }
-  }
-  if (exact_needed) {  // rare: redo this field with the reference's exact FP64 test
-    bool out2 = false;
-    const unsigned m = window_mask(G, fv, sh[0] == 0.0 ? ge[0] : __dsub_rn(ge[0], 0.5),
-                                   sh[1] == 0.0 ? ge[1] : __dsub_rn(ge[1], 0.5),
-                                   sh[2] == 0.0 ? ge[2] : __dsub_rn(ge[2], 0.5), cb0, cb1, cb2, out2);
-    outside = outside || out2;
-    mask = m;
-  }
-  return mask;
-}
-
-// Binning + activation, fast version (see above).  The bin cell uses the
-// same coordinate formula as the splat, (pos - o) * (1/dx) in FP64.
-__global__ void __launch_bounds__(256) k_bin_activate3(DevGrid G, const float* __restrict__ px,
-                                                       const float* __restrict__ py,
-                                                       const float* __restrict__ pz, int n, int* bin_count,
-                                                       int* pkey, int* prank, uint8_t* need) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  const unsigned active = __ballot_sync(0xffffffffu, p < n);
-  if (p >= n) return;
-  const float X = px[p], Y = py[p], Z = pz[p];
-  const double g[3] = {((double)X - G.g.ox) * G.g.inv_dx, ((double)Y - G.g.oy) * G.g.inv_dx,
-                       ((double)Z - G.g.oz) * G.g.inv_dx};
-  const int fi = (int)floor(g[0]), fj = (int)floor(g[1]), fk = (int)floor(g[2]);
-  const int ci = min(max(fi, 0), G.g.nx - 1);
-  const int cj = min(max(fj, 0), G.g.ny - 1);
-  const int ck = min(max(fk, 0), G.g.nz - 1);
-  const int t = tile_id(G.g, ci >> 3, cj >> 3, ck >> 3);
-  const int key = t * PF_TV + local_id(ci, cj, ck);
-  const int r = warp_agg_inc(bin_count, key, active);
-  pkey[p] = key;
-  prank[p] = r;
-  if (!need[t]) need[t] = 1;
-  // exact coordinates for the rare band cases (the reference's division)
-  const double ge[3] = {grid_coord(X, G.g.ox, G.g.dx), grid_coord(Y, G.g.oy, G.g.dx),
-                        grid_coord(Z, G.g.oz, G.g.dx)};
-  const int cb0 = fi >> 2, cb1 = fj >> 2, cb2 = fk >> 2;
-  bool outside = false;
-  const double su[3] = {0.0, -0.5, -0.5}, sv[3] = {-0.5, 0.0, -0.5}, sw[3] = {-0.5, -0.5, 0.0};
-  const unsigned mu = window_mask_fast(G, PF_U, g, ge, su, cb0, cb1, cb2, outside);
-  const unsigned mv = window_mask_fast(G, PF_V, g, ge, sv, cb0, cb1, cb2, outside);
-  const unsigned mw = window_mask_fast(G, PF_W, g, ge, sw, cb0, cb1, cb2, outside);
-  const unsigned bkey = ((unsigned)(cb2 + 512) << 20) | ((unsigned)(cb1 + 512) << 10) | (unsigned)(cb0 + 512);
-  const unsigned peers = __match_any_sync(active, bkey);
-  const unsigned au = __reduce_or_sync(peers, mu);
-  const unsigned av = __reduce_or_sync(peers, mv);
-  const unsigned aw = __reduce_or_sync(peers, mw);
-  if ((threadIdx.x & 31) == __ffs(peers) - 1) {
-    flush_mask(G, PF_U, au, cb0, cb1, cb2, need);
-    flush_mask(G, PF_V, av, cb0, cb1, cb2, need);
-    flush_mask(G, PF_W, aw, cb0, cb1, cb2, need);
-  }
-  if (outside) {
-    activate_window(G, PF_U, ge[0], __dsub_rn(ge[1], 0.5), __dsub_rn(ge[2], 0.5), need);
-    activate_window(G, PF_V, __dsub_rn(ge[0], 0.5), ge[1], __dsub_rn(ge[2], 0.5), need);
-    activate_window(G, PF_W, __dsub_rn(ge[0], 0.5), __dsub_rn(ge[1], 0.5), ge[2], need);
-  }
-}
-
 // One pass over the particles: tile key + warp-aggregated rank (binning),
 // the tile of the particle's cell (pooled for markCells), and the exact
 // activation of u/v/w and their mass fields.
@@ -922,8 +693,8 @@ static int p2g_core(pf_ctx* ctx, const pf_phase* ph, double Vp) {
     PF_CUDA_TRY(cudaMemsetAsync(ctx->tile_count, 0, (size_t)(nt * PF_TV + 1) * sizeof(int), ctx->stream));
     DevGrid G = dev_grid(ctx);
     if (n > 0)
-      (++ctx->launches), k_bin_activate3<<<nblocks(n, 256), 256, 0, ctx->stream>>>(
-          G, ctx->px, ctx->py, ctx->pz, n, ctx->tile_count, ctx->pkey, ctx->prank, ctx->tile_need);
+      (++ctx->launches), k_bin_activate<<<nblocks(n, 256), 256, 0, ctx->stream>>>(
+          G, ctx->px, ctx->py, ctx->pz, n, ctx->tile_count, ctx->pkey, ctx->prank, ctx->tile_need, 1, 1);
     PF_CUDA_TRY(cudaGetLastError());
     rc = pool_commit(ctx);
     if (rc) return rc;

@@ -20,12 +20,14 @@ network on caller-given coarse systems for tests.
 from __future__ import annotations
 
 import ctypes as C
+import os
 
 import numpy as np
 
 from . import _lib as L
 
 COP_STRIDE = 17
+DEFAULT_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights", "coarse_net.npy")
 
 
 def num_params() -> int:
@@ -61,6 +63,14 @@ class LearnedCoarseSolver:
 
     def load_file(self, path):
         self.load(np.load(path))
+
+    def load_default(self) -> str:
+        """Load the weights shipped with the package (written by
+        train_coarse_net.py); returns their path."""
+        if not os.path.exists(DEFAULT_WEIGHTS):
+            raise FileNotFoundError(f"no trained weights at {DEFAULT_WEIGHTS}: run train_coarse_net.py")
+        self.load_file(DEFAULT_WEIGHTS)
+        return os.path.relpath(DEFAULT_WEIGHTS, os.path.dirname(os.path.dirname(DEFAULT_WEIGHTS)))
 
     def harvest(self, enable: bool, stride: int = 1, max_per_system: int = 64, capacity_floats: int = 1 << 26):
         self._check(self.lib.pf_learned_harvest(self.ctx, int(bool(enable)), int(stride), int(max_per_system),

@@ -1,0 +1,107 @@
+"""Train the learned coarse solve of the LEARNED pressure mode and save its
+parameter vector (the file the package loads by default).
+
+Training pairs (r_c, A_c^-1 r_c) are harvested on the GPU from exact
+two-level solves (PF_PRECOND_EXACT_COARSE) of seeded pressure systems:
+64 air ellipsoids in water at 1000:1 with a band-limited divergence
+(scenes.ellipsoid_pressure), at 64^3 and 128^3.  Each grid size has its own
+context, so training alternates between them and carries the weights over.
+
+    python adaptive-pf-flip_b200/train_coarse_net.py [--out PATH] [--steps N]
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+DEFAULT_OUT = os.path.join(HERE, "weights", "coarse_net.npy")
+NAMES = ("u", "v", "w", "mu", "mv", "mw", "p", "mk")
+
+
+def _package():
+    name = "adaptive_pf_flip_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(name, os.path.join(HERE, "__init__.py"),
+                                                  submodule_search_locations=[HERE])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def pressure_system(pf, n, seed, grid=None):
+    """Load the seeded ellipsoid pressure system into `grid` (new n^3 grid if
+    None); returns (grid, solve) where solve(cfg, max_iter) resets u/v/w and
+    projects."""
+    sc = pf.scenes.ellipsoid_pressure(n, seed=seed)
+    pp = pf.PhaseParams(sc["rho_l"], sc["rho_g"])
+    g = grid or pf.SparseMacGrid3D(n, n, n, sc["dx"], max_particles=1)
+    pp.rho_tilde_0 = pf.calibrateRhoTilde0(pp, 1.0, grid=g)
+    f = pf.scenes.pressure_grid_fields(sc, pp.rho_tilde_0)
+    full = {k: np.ones(g.bdims(i)[::-1], np.uint8) for i, k in enumerate(NAMES)}
+    for k in ("mu", "mv", "mw", "mk"):
+        g.set_field(NAMES.index(k), f[k], full[k])
+
+    def solve(cfg, max_iter=20000):
+        for k in ("u", "v", "w"):
+            g.set_field(NAMES.index(k), f[k], full[k])
+        st = pf.spProjectStepVC3D(g, pp, 1.0 / 240.0, max_iter, 0.0, solver=cfg)
+        p, _ = g.get_field(pf.PF_P)
+        return st, p.astype(np.float64)
+
+    return g, solve
+
+
+def train(plan=((64, 1), (64, 2), (64, 3), (128, 1), (128, 2)), steps=1800, batch=8, seed=11, log=print):
+    pf = _package()
+    nets, grids, params = {}, {}, None
+    t0 = time.time()
+    for n, s in plan:
+        g, solve = pressure_system(pf, n, s, grids.get(n))
+        grids[n] = g
+        if n not in nets:
+            nets[n] = pf.LearnedCoarseSolver(g)
+            if params is None:
+                nets[n].init(seed)
+                params = nets[n].params()
+            else:
+                nets[n].load(params)
+            nets[n].harvest(True, stride=2, max_per_system=200, capacity_floats=1 << 27)
+        st, _ = solve(pf.SolverConfig(mode=pf.PF_SOLVER_LEARNED, rel_tol=1e-6, precond=pf.PF_PRECOND_EXACT_COARSE))
+        log(f"harvest n={n} seed={s}: {st.iterations} exact two-level iterations, {time.time() - t0:.1f} s")
+    for net in nets.values():
+        net.harvest(False)
+    rounds = 6
+    per = max(1, steps // (rounds * len(nets)))
+    for r in range(rounds):
+        lr = 1e-3 if r < rounds - 2 else 3e-4
+        for n in sorted(nets):
+            nets[n].load(params)
+            losses = nets[n].train(steps=per, batch=batch, lr=lr, seed=1000 * r + n)
+            params = nets[n].params()
+            log(f"round {r} n={n}: loss {losses[:10].mean():.4f} -> {losses[-10:].mean():.4f}")
+    for g in grids.values():
+        g.close()
+    return params
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=DEFAULT_OUT)
+    ap.add_argument("--steps", type=int, default=1800)
+    args = ap.parse_args()
+    params = train(steps=args.steps)
+    os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
+    np.save(args.out, params.astype(np.float32))
+    print(f"saved {params.size} parameters to {args.out}")
+
+
+if __name__ == "__main__":
+    main()

@@ -267,11 +267,25 @@ def cpu_reference_sample(sc, slab_cells, steps, warmup=0, alpha=0.97):
     return len(ps), times
 
 
+def pcg_modes(pf, names):
+    """Solver configurations of the pressure-only block, by name."""
+    L = pf.PF_SOLVER_LEARNED
+    table = {
+        "plain_fp64": pf.SolverConfig(mode=pf.PF_SOLVER_PLAIN, rel_tol=1e-6),
+        "mixed_fp32": pf.SolverConfig(mode=pf.PF_SOLVER_MIXED, rel_tol=1e-6),
+        "mixed_bf16": pf.SolverConfig(mode=pf.PF_SOLVER_MIXED, rel_tol=1e-6, bf16_storage=True),
+        # the learned two-level preconditioner and its net-free ablation
+        "learned": pf.SolverConfig(mode=L, rel_tol=1e-6, precond=pf.PF_PRECOND_NETWORK),
+        "flex_jacobi": pf.SolverConfig(mode=L, rel_tol=1e-6, precond=pf.PF_PRECOND_JACOBI),
+    }
+    return [(name, table[name]) for name in names]
+
+
 def run_pcg(pf, n, modes, max_iter=20000, seed=0):
     """Pressure-only system (n^3, every interior cell fluid, 64 air ellipsoids
     in water at 1000:1, band-limited RHS): device time to a 1e-6 relative
     FP64 residual per solver mode, and each mode's pressure against the
-    PLAIN FP64 solve."""
+    PLAIN FP64 solve (the first mode)."""
     sc = pf.scenes.ellipsoid_pressure(n, seed=seed)
     pp = pf.PhaseParams(sc["rho_l"], sc["rho_g"])
     g = pf.SparseMacGrid3D(n, n, n, sc["dx"], max_particles=1)
@@ -280,15 +294,23 @@ def run_pcg(pf, n, modes, max_iter=20000, seed=0):
     full = {k: np.ones(g.bdims(i)[::-1], np.uint8) for i, k in enumerate(("u", "v", "w", "mu", "mv", "mw", "p", "mk"))}
     for k in ("mu", "mv", "mw", "mk"):
         g.set_field(("u", "v", "w", "mu", "mv", "mw", "p", "mk").index(k), f[k], full[k])
+    weights = None
+    if any(cfg.mode == pf.PF_SOLVER_LEARNED and cfg.precond == pf.PF_PRECOND_NETWORK for _, cfg in modes):
+        net = pf.LearnedCoarseSolver(g)
+        weights = net.load_default()
     out, p_plain = {}, None
-    for name, mode, bf16 in modes:
+    for name, cfg in modes:
         for k in ("u", "v", "w"):
             g.set_field(("u", "v", "w").index(k), f[k], full[k])
-        st = pf.spProjectStepVC3D(g, pp, 1.0 / 240.0, max_iter, 0.0,
-                                  solver=pf.SolverConfig(mode=mode, rel_tol=1e-6, bf16_storage=bf16))
+        st = pf.spProjectStepVC3D(g, pp, 1.0 / 240.0, max_iter, 0.0, solver=cfg)
         p, _ = g.get_field(pf.PF_P)
         rec = {"ms_to_1e-6": st.solve_ms, "iterations": st.iterations, "refinements": st.refinements,
                "converged": bool(st.converged), "rel_residual": st.res_final / max(st.res0, 1e-300)}
+        if cfg.mode == pf.PF_SOLVER_LEARNED:
+            rec["coarse_accepted"] = st.precond_applied
+            rec["coarse_rejected"] = st.precond_rejected
+            if cfg.precond == pf.PF_PRECOND_NETWORK:
+                rec["weights"] = weights
         if p_plain is None:
             p_plain = p.astype(np.float64)
         else:
@@ -391,9 +413,7 @@ def run_ours(args, rank, world, local, dist):
         "clocks": clk.summary(),
     }
     if rank == 0 and not args.no_extras:
-        line["pcg"] = run_pcg(pf, args.pcg_n, [("plain_fp64", pf.PF_SOLVER_PLAIN, False),
-                                               ("mixed_fp32", pf.PF_SOLVER_MIXED, False),
-                                               ("mixed_bf16", pf.PF_SOLVER_MIXED, True)])
+        line["pcg"] = run_pcg(pf, args.pcg_n, pcg_modes(pf, args.pcg_modes.split(",")))
         line["full_step"] = run_full_step(pf)
     if rank == 0 and not args.no_cpu_baseline:
         cores = 8
@@ -439,6 +459,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the PCG and full-step blocks")
     ap.add_argument("--pcg-n", type=int, default=256, help="grid of the pressure-only block")
+    ap.add_argument("--pcg-modes", default="plain_fp64,learned,flex_jacobi",
+                    help="solvers of the pressure-only block (plain_fp64 first): plain_fp64, learned, "
+                         "flex_jacobi, mixed_fp32, mixed_bf16")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

@@ -158,11 +158,23 @@ def features(cop, dims, rc):
     return F, s, dref
 
 
-def level_dims(dims):
+def level_dims(dims, count=4):
     out = [tuple(dims)]
-    for _ in range(3):
+    for _ in range(count - 1):
         out.append(tuple((d + 1) // 2 for d in out[-1]))
     return out
+
+
+MAX_LEVELS = 8
+
+
+def g_levels(dims):
+    """Levels of G: halve until every extent is <= 2 (at least 4, at most 8)."""
+    n, d = 1, tuple(dims)
+    while max(d) > 2 and n < MAX_LEVELS:
+        d = tuple((v + 1) // 2 for v in d)
+        n += 1
+    return max(4, n)
 
 
 TAPS = [(dx, dy, dz) for dz in (-1, 0, 1) for dy in (-1, 0, 1) for dx in (-1, 0, 1)]
@@ -364,12 +376,12 @@ def inv_sqrt_diag(cop):
 
 
 def gates(params, cop, dims, round_bf16=False, keep=False):
-    """Per-level gates gamma_0..3 (1, n_l, 8) from the operator alone."""
+    """Per-level gates gamma_l (1, n_l, 8) of every G level, from the operator alone."""
     F, _, _ = features(cop, dims, np.zeros((1, int(np.prod(dims)), 2)))
-    D = level_dims(dims)
+    D = level_dims(dims, g_levels(dims))
     g0, tape = forward(params, F, dims, round_bf16, keep=True)
     gs = [g0]
-    for l in range(3):
+    for l in range(len(D) - 1):
         gs.append(pool(gs[-1], D[l]))
     return (gs, tape) if keep else gs
 
@@ -380,69 +392,61 @@ def _gW(params):
 
 
 def apply_gtg(params, gs, cop, dims, rc, round_bf16=False, keep=False):
-    """e = S G^T G S rc with G = (gamma_l * C_l P)... (levels 0..3)."""
-    D = level_dims(dims)
-    Wa, Wb, Wc, Wd = _gW(params)
+    """e = S G^T G S rc, G r = (h_0 .. h_{L-1}), h_0 = gamma_0 C_0 S r,
+    h_l = gamma_l C_min(l,3) P h_{l-1}; L = g_levels(dims)."""
+    NL = g_levels(dims)
+    D = level_dims(dims, NL)
+    Wg = _gW(params)
+    W = [Wg[min(l, 3)] for l in range(NL)]
     S = inv_sqrt_diag(cop)[None]
-    rc = np.asarray(rc, np.float64)
-    x0 = S * rc
-    a0 = conv(x0, D[0], Wa, 0.0, False, round_bf16)
-    h0 = gs[0] * a0
-    q1 = pool(h0, D[0])
-    a1 = conv(q1, D[1], Wb, 0.0, False, round_bf16)
-    h1 = gs[1] * a1
-    q2 = pool(h1, D[1])
-    a2 = conv(q2, D[2], Wc, 0.0, False, round_bf16)
-    h2 = gs[2] * a2
-    q3 = pool(h2, D[2])
-    a3 = conv(q3, D[3], Wd, 0.0, False, round_bf16)
-    h3 = gs[3] * a3
-    t3 = gs[3] * h3
-    b2 = h2 + pool_backward(convT(t3, D[3], Wd, round_bf16), D[2])
-    t2 = gs[2] * b2
-    b1 = h1 + pool_backward(convT(t2, D[2], Wc, round_bf16), D[1])
-    t1 = gs[1] * b1
-    b0 = h0 + pool_backward(convT(t1, D[1], Wb, round_bf16), D[0])
-    t0 = gs[0] * b0
-    e = S * convT(t0, D[0], Wa, round_bf16)
+    x0 = S * np.asarray(rc, np.float64)
+    a, h, q, b, t = [None] * NL, [None] * NL, [None] * NL, [None] * NL, [None] * NL
+    for l in range(NL):
+        xin = x0 if l == 0 else pool(h[l - 1], D[l - 1])
+        q[l] = xin
+        a[l] = conv(xin, D[l], W[l], 0.0, False, round_bf16)
+        h[l] = gs[l] * a[l]
+    b[NL - 1] = h[NL - 1]
+    t[NL - 1] = gs[NL - 1] * h[NL - 1]
+    for l in range(NL - 1, 0, -1):
+        b[l - 1] = h[l - 1] + pool_backward(convT(t[l], D[l], W[l], round_bf16), D[l - 1])
+        t[l - 1] = gs[l - 1] * b[l - 1]
+    e = S * convT(t[0], D[0], W[0], round_bf16)
     if not keep:
         return e
-    return e, dict(S=S, x0=x0, a=[a0, a1, a2, a3], h=[h0, h1, h2, h3], q=[None, q1, q2, q3], b=[b0, b1, b2, h3],
-                   t=[t0, t1, t2, t3])
+    return e, dict(S=S, a=a, h=h, q=q, b=b, t=t)
 
 
 def apply_gtg_backward(params, gs, dims, tape, de, round_bf16=False):
-    """Gradients of <de, e> w.r.t. the four G weights and the gates gamma_0..3."""
-    D = level_dims(dims)
-    W = _gW(params)
+    """Gradients of <de, e> w.r.t. the four G weights (the last shared by the
+    deeper levels) and the gate gamma_0 (deeper gates are its poolings)."""
+    NL = g_levels(dims)
+    D = level_dims(dims, NL)
+    Wg = _gW(params)
+    W = [Wg[min(l, 3)] for l in range(NL)]
     S = tape["S"]
     a, h, q, b, t = tape["a"], tape["h"], tape["q"], tape["b"], tape["t"]
-    gW = [np.zeros_like(w) for w in W]
+    gW = [np.zeros_like(w) for w in Wg]
     dg = [np.zeros_like(g) for g in gs]
-    dh = [None] * 4
+    dh = [None] * NL
     # transposed half, fine to coarse
-    dxe = S * de
-    dt = conv(dxe, D[0], W[0], 0.0, False, round_bf16)
-    gW[0] += wgrad(dxe, D[0], t[0], round_bf16)
-    for l in range(3):
+    dv = S * de
+    for l in range(NL):
+        if l > 0:
+            dv = pool(dh[l - 1], D[l - 1])
+        dt = conv(dv, D[l], W[l], 0.0, False, round_bf16)
+        gW[min(l, 3)] += wgrad(dv, D[l], t[l], round_bf16)
         dg[l] += (dt * b[l]).sum(axis=0, keepdims=True)
-        db = gs[l] * dt
-        dh[l] = db.copy()
-        dv = pool(db, D[l])
-        dt = conv(dv, D[l + 1], W[l + 1], 0.0, False, round_bf16)
-        gW[l + 1] += wgrad(dv, D[l + 1], t[l + 1], round_bf16)
-    dg[3] += (dt * h[3]).sum(axis=0, keepdims=True)
-    dh[3] = gs[3] * dt
+        dh[l] = gs[l] * dt
     # forward half, coarse to fine
-    for l in (3, 2, 1, 0):
+    for l in range(NL - 1, -1, -1):
         da = gs[l] * dh[l]
         dg[l] += (a[l] * dh[l]).sum(axis=0, keepdims=True)
-        xin = tape["x0"] if l == 0 else q[l]
-        gW[l] += wgrad(xin, D[l], da, round_bf16)
+        gW[min(l, 3)] += wgrad(q[l], D[l], da, round_bf16)
         if l > 0:
             dh[l - 1] += pool_backward(convT(da, D[l], W[l], round_bf16), D[l - 1])
     # gamma_{l+1} = P gamma_l
-    for l in (2, 1, 0):
+    for l in range(NL - 2, -1, -1):
         dg[l] += pool_backward(dg[l + 1], D[l])
     return gW, dg[0]
 

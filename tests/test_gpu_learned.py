@@ -38,12 +38,12 @@ def small(pf):
 DIMS = (7, 5, 6)  # odd sizes exercise the ragged pooling / upsampling edges
 
 
-def _system(seed, B=3):
-    cop = cn.random_system(DIMS, seed=seed, contrast=1000.0)
+def _system(seed, B=3, dims=DIMS):
+    cop = cn.random_system(dims, seed=seed, contrast=1000.0)
     rng = np.random.default_rng(seed + 100)
-    nt = int(np.prod(DIMS))
+    nt = int(np.prod(dims))
     rc = (rng.normal(0, 1, (B, nt, 2)) * cn.live_mask(cop)[None]).astype(np.float32)
-    tgt = cn.exact_correction(cop, DIMS, rc).astype(np.float32)
+    tgt = cn.exact_correction(cop, dims, rc).astype(np.float32)
     return cop, rc, tgt
 
 
@@ -60,21 +60,23 @@ def test_forward_matches_cpu(small):
     assert np.all(e_gpu[:, ~live] == 0.0)
 
 
-def test_loss_and_gradient_match_cpu(small):
+@pytest.mark.parametrize("dims", [DIMS, (17, 3, 3)])  # 4 and 5 levels of G (the last weight shared)
+def test_loss_and_gradient_match_cpu(small, dims):
     _, net = small
-    cop, rc, tgt = _system(2)
+    cop, rc, tgt = _system(2, dims=dims)
     params = cn.unflatten(net.params())
-    e_gpu, loss_gpu, grad_gpu = net.eval(DIMS, cop, rc, tgt)
-    loss_cpu, grads_cpu, e_cpu = cn.loss_and_grad(params, cop, DIMS, rc, tgt, round_bf16=True)
+    e_gpu, loss_gpu, grad_gpu = net.eval(dims, cop, rc, tgt)
+    loss_cpu, grads_cpu, e_cpu = cn.loss_and_grad(params, cop, dims, rc, tgt, round_bf16=True)
     assert abs(loss_gpu - loss_cpu) <= 2e-3 * abs(loss_cpu)
     assert rel_l2(e_gpu, e_cpu) < 2e-3
     g_cpu = cn.flatten(grads_cpu)
     # per tensor: weights and biases of every layer
+    names = [layer[0] for layer in cn.LAYERS] + [layer[0] for layer in cn.G_LAYERS]
     o = 0
     for q, s in enumerate(cn.param_shapes()):
         n = int(np.prod(s))
         err = rel_l2(grad_gpu[o:o + n], g_cpu[o:o + n])
-        assert err < 2e-2, (cn.LAYERS[q // 2][0], "W" if q % 2 == 0 else "b", err)
+        assert err < 2e-2, (names[q // 2], "W" if q % 2 == 0 else "b", err)
         o += n
 
 

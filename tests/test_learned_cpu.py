@@ -2,6 +2,7 @@
 (oracle/coarse_net.py): its hand-written backward pass against central
 finite differences, and the structure of its seeded coarse systems."""
 import numpy as np
+import pytest
 
 from oracle import coarse_net as cn
 
@@ -15,8 +16,8 @@ def test_coarse_operator_is_symmetric_positive_definite():
     assert np.linalg.eigvalsh(A).min() > 0
 
 
-def test_backward_matches_finite_differences():
-    dims = (5, 4, 3)
+@pytest.mark.parametrize("dims", [(5, 4, 3), (17, 3, 3)])  # 4 G levels; 5 (the last G weight shared)
+def test_backward_matches_finite_differences(dims):
     cop = cn.random_system(dims, seed=1, contrast=30.0)
     rng = np.random.default_rng(2)
     params = [rng.normal(0, np.sqrt(2 / (27 * s[1])), s) if len(s) == 3 else rng.normal(0, 0.1, s)
