@@ -33,7 +33,8 @@ EXPORTS = (
     "pf_save_velocity", "pf_apply_gravity", "pf_apply_wall_boundary", "pf_project", "pf_g2p", "pf_advect",
     "pf_step", "pf_calibrate_rho_tilde0", "pf_set_timing", "pf_get_timing", "pf_launch_count",
     "pf_project_noalloc", "pf_learned_num_params", "pf_learned_init", "pf_learned_load", "pf_learned_params",
-    "pf_learned_harvest", "pf_learned_dataset", "pf_learned_clear_dataset", "pf_learned_train",
+    "pf_learned_harvest", "pf_learned_dataset", "pf_learned_clear_dataset", "pf_learned_merge_dataset",
+    "pf_learned_train",
     "pf_learned_eval", "pf_learned_adam",
 )
 
@@ -153,6 +154,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "pf_learned_harvest": (i, [vp, i, i, i, sz]),
         "pf_learned_dataset": (i, [vp, P(i), P(i)]),
         "pf_learned_clear_dataset": (i, [vp]),
+        "pf_learned_merge_dataset": (i, [vp, vp]),
         "pf_learned_train": (i, [vp, i, i, d, C.c_ulonglong, vp]),
         "pf_learned_eval": (i, [vp, i, i, i, vp, vp, vp, i, vp, P(d), vp]),
         "pf_learned_adam": (i, [vp, vp, sz, d]),

@@ -6,7 +6,7 @@
 //   e = S G^T G S r_c,    S = diag(d_c)^-1/2 over live coarse unknowns,
 //   G r = (h_0, ..., h_{L-1}),  h_0 = g_0 * C_0 r,  h_l = g_l * C_min(l,3) P h_{l-1},
 //
-// where C_l are 3x3x3 convolutions (2->8, then 8->8 channels) on the tile
+// where C_l are 3x3x3 convolutions (2->16, then 16->16 channels) on the tile
 // lattice and its 2x coarser levels down to 2 tiles per axis (L = 4..8, the
 // last convolution shared by the levels below the fourth), P is 2x2x2
 // average pooling and the g_l are per-position, per-channel gates -- a
@@ -361,7 +361,7 @@ int layer_backward(pf_ctx* ctx, LearnedState* L, int layer, const float* x, int 
 }
 
 // ---------------------------------------------------------------------------
-// the gate U-Net (one sample): features of A_c -> g_0 (8 channels), g_1..3 by pooling
+// the gate U-Net (one sample): features of A_c -> g_0 (16 channels), deeper gates by pooling
 
 int unet_forward(pf_ctx* ctx, LearnedState* L, Work& W, const float* cop, const SolveCtl* skip) {
   const Dims* D = W.D;
@@ -757,6 +757,46 @@ int pf_learned_dataset(pf_ctx* ctx, int* systems, int* pairs) {
   }
   if (systems) *systems = ns;
   if (pairs) *pairs = np;
+  return PF_OK;
+}
+
+// Append src's training set (systems and pairs) to dst's; both contexts must
+// live on the same device.  Lets one optimiser train on grids of several sizes.
+int pf_learned_merge_dataset(pf_ctx* dst, pf_ctx* src) {
+  if (!dst || !src || dst == src) return PF_ERR_INVALID;
+  pf_ctx* ctx = dst;  // errors are reported on the destination
+  if (dst->device != src->device) return set_error(ctx, PF_ERR_INVALID, "merge: contexts on different devices");
+  const CoarseCtx* cs = (const CoarseCtx*)src->learned;
+  if (!cs || !cs->net || cs->net->systems.empty()) return PF_OK;
+  cudaSetDevice(dst->device);
+  int rc = 0;
+  LearnedState* D = get_state(dst, &rc);
+  if (!D) return rc;
+  const LearnedState* S = cs->net;
+  PF_CUDA_TRY(cudaStreamSynchronize(src->stream));
+  PF_CUDA_TRY(cudaStreamSynchronize(dst->stream));
+  const size_t need = D->pool_used + S->pool_used;
+  if (need > D->pool_cap) {
+    float* np = nullptr;
+    PF_CUDA_TRY(cudaMalloc(&np, need * sizeof(float)));
+    if (D->pool_used) PF_CUDA_TRY(cudaMemcpy(np, D->pool, D->pool_used * sizeof(float), cudaMemcpyDeviceToDevice));
+    if (D->pool) cudaFree(D->pool);
+    D->pool = np;
+    D->pool_cap = need;
+  }
+  if (S->pool_used)
+    PF_CUDA_TRY(cudaMemcpy(D->pool + D->pool_used, S->pool, S->pool_used * sizeof(float), cudaMemcpyDeviceToDevice));
+  for (const auto& s : S->systems) {
+    if (s.pairs.empty()) continue;
+    LearnedState::System t;
+    t.d = s.d;
+    const size_t bytes = (size_t)s.d.n * kCopStride * sizeof(float);
+    PF_CUDA_TRY(cudaMalloc(&t.cop, bytes));
+    PF_CUDA_TRY(cudaMemcpy(t.cop, s.cop, bytes, cudaMemcpyDeviceToDevice));
+    for (size_t off : s.pairs) t.pairs.push_back(off + D->pool_used);
+    D->systems.push_back(t);
+  }
+  D->pool_used = need;
   return PF_OK;
 }
 

@@ -29,11 +29,11 @@ struct LayerSpec {
 constexpr int kNumLayers = 16;
 constexpr LayerSpec kLayers[kNumLayers] = {
     {32, 16, 1, 1}, {16, 16, 1, 1}, {16, 32, 1, 1}, {32, 32, 1, 1}, {32, 64, 1, 1}, {64, 64, 1, 1},
-    {64, 64, 1, 1}, {64, 64, 1, 1}, {128, 64, 1, 1}, {96, 32, 1, 1}, {48, 16, 1, 1}, {16, 8, 0, 1},
-    {2, 8, 0, 0},   {8, 8, 0, 0},   {8, 8, 0, 0},   {8, 8, 0, 0}};
+    {64, 64, 1, 1}, {64, 64, 1, 1}, {128, 64, 1, 1}, {96, 32, 1, 1}, {48, 16, 1, 1}, {16, 16, 0, 1},
+    {2, 16, 0, 0},  {16, 16, 0, 0}, {16, 16, 0, 0}, {16, 16, 0, 0}};
 enum { L_E0A, L_E0B, L_E1A, L_E1B, L_E2A, L_E2B, L_E3A, L_E3B, L_D2, L_D1, L_D0, L_OUT, L_G0, L_G1, L_G2, L_G3 };
 constexpr int kInCh = 32;
-constexpr int kGS = 16;  // channel stride of every tensor of the G path (8 channels used)
+constexpr int kGS = 16;  // channels (and channel stride) of every tensor of the G path
 
 __host__ __device__ constexpr int pad16(int c) { return (c + 15) & ~15; }
 __host__ __device__ constexpr int pad8(int c) { return (c + 7) & ~7; }

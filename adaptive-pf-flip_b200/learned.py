@@ -84,6 +84,10 @@ class LearnedCoarseSolver:
     def clear_dataset(self):
         self._check(self.lib.pf_learned_clear_dataset(self.ctx), "pf_learned_clear_dataset")
 
+    def merge_dataset(self, other: "LearnedCoarseSolver"):
+        """Append the training pairs harvested on another grid (same device)."""
+        self._check(self.lib.pf_learned_merge_dataset(self.ctx, other.ctx), "pf_learned_merge_dataset")
+
     def train(self, steps: int, batch: int = 8, lr: float = 1e-3, seed: int = 0) -> np.ndarray:
         losses = np.zeros(max(int(steps), 1), np.float64)
         self._check(self.lib.pf_learned_train(self.ctx, int(steps), int(batch), float(lr), C.c_ulonglong(seed),

@@ -4,8 +4,9 @@ parameter vector (the file the package loads by default).
 Training pairs (r_c, A_c^-1 r_c) are harvested on the GPU from exact
 two-level solves (PF_PRECOND_EXACT_COARSE) of seeded pressure systems:
 64 air ellipsoids in water at 1000:1 with a band-limited divergence
-(scenes.ellipsoid_pressure), at 64^3 and 128^3.  Each grid size has its own
-context, so training alternates between them and carries the weights over.
+(scenes.ellipsoid_pressure), at 64^3, 128^3 and 256^3 (seeds 1-3, 1-2, 1;
+seed 0 is left for evaluation).  Each grid size harvests on its own context;
+the pairs are then merged into one context and trained with one optimiser.
 
     python adaptive-pf-flip_b200/train_coarse_net.py [--out PATH] [--steps N]
 """
@@ -59,7 +60,10 @@ def pressure_system(pf, n, seed, grid=None):
     return g, solve
 
 
-def train(plan=((64, 1), (64, 2), (64, 3), (128, 1), (128, 2)), steps=1800, batch=8, seed=11, log=print):
+PLAN = ((64, 1), (64, 2), (64, 3), (128, 1), (128, 2), (256, 1))
+
+
+def train(plan=PLAN, steps=3600, batch=8, seed=11, log=print):
     pf = _package()
     nets, grids, params = {}, {}, None
     t0 = time.time()
@@ -78,15 +82,19 @@ def train(plan=((64, 1), (64, 2), (64, 3), (128, 1), (128, 2)), steps=1800, batc
         log(f"harvest n={n} seed={s}: {st.iterations} exact two-level iterations, {time.time() - t0:.1f} s")
     for net in nets.values():
         net.harvest(False)
-    rounds = 6
-    per = max(1, steps // (rounds * len(nets)))
-    for r in range(rounds):
-        lr = 1e-3 if r < rounds - 2 else 3e-4
-        for n in sorted(nets):
-            nets[n].load(params)
-            losses = nets[n].train(steps=per, batch=batch, lr=lr, seed=1000 * r + n)
-            params = nets[n].params()
-            log(f"round {r} n={n}: loss {losses[:10].mean():.4f} -> {losses[-10:].mean():.4f}")
+    # one optimiser over every grid size: gather the pairs in the largest grid's context
+    trainer = nets[max(nets)]
+    for n, net in nets.items():
+        if net is not trainer:
+            trainer.merge_dataset(net)
+    systems, pairs = trainer.dataset()
+    log(f"training set: {systems} systems, {pairs} pairs")
+    phases = ((int(steps * 0.7), 1e-3), (steps - int(steps * 0.7), 3e-4))
+    for q, (k, lr) in enumerate(phases):
+        losses = trainer.train(steps=k, batch=batch, lr=lr, seed=seed + q)
+        for a in range(0, k, max(1, k // 6)):
+            log(f"steps {a}-{a + max(1, k // 6)} at lr {lr:g}: loss {losses[a:a + max(1, k // 6)].mean():.4f}")
+    params = trainer.params()
     for g in grids.values():
         g.close()
     return params
@@ -95,7 +103,7 @@ def train(plan=((64, 1), (64, 2), (64, 3), (128, 1), (128, 2)), steps=1800, batc
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=DEFAULT_OUT)
-    ap.add_argument("--steps", type=int, default=1800)
+    ap.add_argument("--steps", type=int, default=3600)
     args = ap.parse_args()
     params = train(steps=args.steps)
     os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)

@@ -388,13 +388,17 @@ def run_ours(args, rank, world, local, dist):
         kname, kms = "k_g2p (G2P)", g2p_ms
         kbytes = G2P_BYTES_PER_PARTICLE * n + G2P_BYTES_PER_FACE * n_faces
     achieved = kbytes / (kms / 1000.0) / 1e9
+    # DRAM bytes per launch of the roofline kernel from an ncu capture
+    # (profiles/traffic.json), valid for the 128^3 workload it was scaled to
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "traffic_bubble128.json")
-    if os.path.exists(tpath):
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath) and args.n == 128:
         try:
             with open(tpath) as f:
-                traffic = json.load(f).get(kname.split()[0])
-        except Exception:
+                rec = json.load(f)
+            if rec.get("kernel") == kname.split()[0] and rec.get("scaled_to_particles") == n:
+                traffic = rec["bytes_per_launch"]
+        except (OSError, ValueError, KeyError):
             traffic = None
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -459,6 +463,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the PCG and full-step blocks")
     ap.add_argument("--pcg-n", type=int, default=256, help="grid of the pressure-only block")
+    ap.add_argument("--pcg-only", action="store_true", help="run only the pressure-only block")
+    ap.add_argument("--pcg-max-iter", type=int, default=20000, help="iteration cap of the pressure-only block")
     ap.add_argument("--pcg-modes", default="plain_fp64,learned,flex_jacobi",
                     help="solvers of the pressure-only block (plain_fp64 first): plain_fp64, learned, "
                          "flex_jacobi, mixed_fp32, mixed_bf16")
@@ -469,6 +475,11 @@ def main():
         rank = int(os.environ.get("RANK", "0"))
         world = int(os.environ.get("WORLD_SIZE", "1"))
         run_reference(args, rank, world)
+        return
+    if args.pcg_only:  # the pressure-only block alone (profiling)
+        pf = load_pkg()
+        print(json.dumps(run_pcg(pf, args.pcg_n, pcg_modes(pf, args.pcg_modes.split(",")),
+                                 max_iter=args.pcg_max_iter)), flush=True)
         return
     rank, world, local, dist = dist_setup(args.gpus)
     try:

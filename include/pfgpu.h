@@ -265,6 +265,9 @@ PFGPU_API int pf_learned_params(pf_ctx* ctx, float* out, size_t n);
 PFGPU_API int pf_learned_harvest(pf_ctx* ctx, int enable, int stride, int max_per_system, size_t capacity_floats);
 PFGPU_API int pf_learned_dataset(pf_ctx* ctx, int* systems, int* pairs);
 PFGPU_API int pf_learned_clear_dataset(pf_ctx* ctx);
+/* Append src's training set to dst's (same device): one optimiser can then
+ * train on pairs harvested on grids of several sizes. */
+PFGPU_API int pf_learned_merge_dataset(pf_ctx* dst, pf_ctx* src);
 /* `steps` Adam steps on batches of `batch` pairs of one system each; losses
  * (optional, [steps]) receives each step's mean energy-norm error. */
 PFGPU_API int pf_learned_train(pf_ctx* ctx, int steps, int batch, double lr, unsigned long long seed,

@@ -8,9 +8,10 @@ GPU forward pass, its gradients and its Adam step:
 * the two-class coarse operator on the tile lattice (17 floats per tile:
   diagonals d0 d1, in-tile coupling e, the 2x2 couplings to the -x, -y, -z
   neighbour tile, the aggregate sizes n0 n1) and its product A_c x;
-* the input features, the 4-level U-Net (3x3x3 convolutions, ReLU, 2x2x2
-  average pooling, nearest upsampling with skip concatenation) and the output
-  scaling e = (s / d_ref) o;
+* the input features of A_c and the 4-level gate U-Net (3x3x3 convolutions,
+  ReLU, 2x2x2 average pooling, nearest upsampling with skip concatenation);
+* the learned coarse correction e = S G^T G S r_c: S = diag(d_c)^-1/2, G the
+  gated multilevel operator h_0 = g_0 C_0 S r, h_l = g_l C_min(l,3) P h_{l-1};
 * the energy-norm loss (e - e*)^T A_c (e - e*) / (e*^T r_c) and its gradient
   by reverse-mode differentiation written out by hand;
 * Adam.
@@ -35,11 +36,11 @@ LAYERS = [
     ("enc2a", 32, 64, True), ("enc2b", 64, 64, True),
     ("enc3a", 64, 64, True), ("enc3b", 64, 64, True),
     ("dec2", 128, 64, True), ("dec1", 96, 32, True), ("dec0", 48, 16, True),
-    ("out", 16, 8, False),
+    ("out", 16, 16, False),
 ]
 # the linear operator G: (name, C_in, C_out), one per level, no bias (the
 # bias slots exist in the parameter vector and stay zero)
-G_LAYERS = [("g0", 2, 8), ("g1", 8, 8), ("g2", 8, 8), ("g3", 8, 8)]
+G_LAYERS = [("g0", 2, 16), ("g1", 16, 16), ("g2", 16, 16), ("g3", 16, 16)]
 
 
 def param_shapes():
@@ -376,7 +377,7 @@ def inv_sqrt_diag(cop):
 
 
 def gates(params, cop, dims, round_bf16=False, keep=False):
-    """Per-level gates gamma_l (1, n_l, 8) of every G level, from the operator alone."""
+    """Per-level gates gamma_l (1, n_l, 16) of every G level, from the operator alone."""
     F, _, _ = features(cop, dims, np.zeros((1, int(np.prod(dims)), 2)))
     D = level_dims(dims, g_levels(dims))
     g0, tape = forward(params, F, dims, round_bf16, keep=True)

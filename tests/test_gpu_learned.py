@@ -248,3 +248,29 @@ def test_network_mode_without_weights_is_an_error(pf):
             solve(pf.SolverConfig(mode=pf.PF_SOLVER_LEARNED, rel_tol=1e-6, precond=pf.PF_PRECOND_NETWORK))
     finally:
         g.close()
+
+
+def test_merge_dataset_across_grid_sizes(pf):
+    """Pairs harvested on two grids of different size train in one context."""
+    L = pf.PF_SOLVER_LEARNED
+    g1, solve1 = _pressure_system(pf, 32, seed=6)
+    g2, solve2 = _pressure_system(pf, 48, seed=7)
+    try:
+        n1, n2 = pf.LearnedCoarseSolver(g1), pf.LearnedCoarseSolver(g2)
+        n1.init(seed=1)
+        n2.load(n1.params())
+        for net, solve in ((n1, solve1), (n2, solve2)):
+            net.harvest(True, stride=1, max_per_system=20, capacity_floats=1 << 22)
+            st, _ = solve(pf.SolverConfig(mode=L, rel_tol=1e-6, precond=pf.PF_PRECOND_EXACT_COARSE))
+            assert st.converged
+            net.harvest(False)
+        s1, p1 = n1.dataset()
+        s2, p2 = n2.dataset()
+        assert s1 == 1 and s2 == 1 and p1 > 0 and p2 > 0
+        n1.merge_dataset(n2)
+        assert n1.dataset() == (s1 + s2, p1 + p2)
+        losses = n1.train(steps=20, batch=4, lr=1e-3, seed=3)
+        assert np.all(np.isfinite(losses))
+    finally:
+        g1.close()
+        g2.close()
