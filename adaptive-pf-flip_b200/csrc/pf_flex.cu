@@ -93,14 +93,19 @@ constexpr int kWarpsPerSlot = PF_TV / 32;
 // Per-warp class sums of r (32 cells of slot s) into part[(s * 16 + warp) * 2 + class];
 // k_rc_reduce folds them into rc.  No block synchronisation.
 __device__ __forceinline__ void restrict_warp(const uint8_t* cls, size_t o, double r, int s, float* part) {
+  // FP32 suffices for the coarse residual (the preconditioner's input)
   const uint8_t c = cls[o];
-  double a0 = c == 0 ? r : 0.0, a1 = c == 1 ? r : 0.0;
-  a0 = warp_sum(a0);
-  a1 = warp_sum(a1);
+  const float rf = (float)r;
+  float a0 = c == 0 ? rf : 0.0f, a1 = c == 1 ? rf : 0.0f;
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) {
+    a0 += __shfl_down_sync(0xffffffffu, a0, d);
+    a1 += __shfl_down_sync(0xffffffffu, a1, d);
+  }
   if ((threadIdx.x & 31) == 0) {
     float* q = part + ((size_t)s * kWarpsPerSlot + (threadIdx.x >> 5)) * 2;
-    q[0] = (float)a0;
-    q[1] = (float)a1;
+    q[0] = a0;
+    q[1] = a1;
   }
 }
 

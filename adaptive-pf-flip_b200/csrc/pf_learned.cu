@@ -51,7 +51,8 @@ int g_layer(int l) { return L_G0 + std::min(l, 3); }
 // and the G path (B samples).  Every G-path tensor has channel stride kGS.
 struct Work {
   int B = 0, Balloc = 0;
-  bool bwd = false;
+  bool bwd = false;    // backward buffers allocated
+  bool train = false;  // the current use keeps the forward intermediates for a backward pass
   int NL = 0;  // levels of G (the U-Net uses the first four)
   Dims D[kMaxLevels]{};
   size_t cap[kMaxLevels] = {};
@@ -181,6 +182,7 @@ int work_ensure(pf_ctx* ctx, Work& W, Dims d0, int B, bool bwd) {
   // buffers hold Balloc samples of up to cap[l] positions per level
   bool fits = W.Balloc >= B && (W.bwd || !bwd);
   for (int l = 0; l < NL && fits; ++l) fits = (size_t)D[l].n <= W.cap[l];
+  W.train = bwd;
   if (fits) {
     W.B = B;
     W.NL = NL;
@@ -199,6 +201,7 @@ int work_ensure(pf_ctx* ctx, Work& W, Dims d0, int B, bool bwd) {
   W.B = B;
   W.Balloc = B;
   W.bwd = bwd;
+  W.train = bwd;
   int rc = 0;
   auto alloc = [&](float** q, size_t count) {
     if (rc) return;
@@ -441,8 +444,63 @@ int unet_backward(pf_ctx* ctx, LearnedState* L, Work& W) {
 // ---------------------------------------------------------------------------
 // the G path (B samples): e = S G^T G S rc
 
+// Inference: 2 NL launches of the 16-channel G kernel (pool, gates, upsampling
+// and the diagonal scaling folded into its staging and epilogue).
+int gtg_apply(pf_ctx* ctx, LearnedState* L, Work& W, const float* cop, const float* rc_in, float* e_out,
+              const SolveCtl* skip) {
+  const int NL = W.NL;
+  const Dims* D = W.D;
+  auto args = [&](int l) {
+    GConvArgs a{};
+    a.d = D[l];
+    a.dc = l + 1 < NL ? D[l + 1] : D[l];
+    a.bx = (D[l].X + kGBX - 1) / kGBX;
+    a.by = (D[l].Y + kGBY - 1) / kGBY;
+    a.gate = W.gam[l];
+    a.cop = cop;
+    a.skip = skip;
+    return a;
+  };
+  auto grid = [&](int l) {
+    return dim3((unsigned)(((D[l].X + kGBX - 1) / kGBX) * ((D[l].Y + kGBY - 1) / kGBY) * ((D[l].Z + kGBZ - 1) / kGBZ)),
+                (unsigned)W.B);
+  };
+  for (int l = 0; l < NL; ++l) {
+    GConvArgs a = args(l);
+    a.wf = L->wf[g_layer(l)];
+    a.y = W.h[l];
+    a.pool = l + 1 < NL ? W.q[l + 1] : nullptr;
+    ++ctx->launches;
+    if (l == 0) {
+      a.x = rc_in;
+      k_gconv<GIN_SCALE, GOUT_GATE, 2><<<grid(l), 128, 0, ctx->stream>>>(a);
+    } else {
+      a.x = W.q[l];
+      k_gconv<GIN_PLAIN, GOUT_GATE, 2><<<grid(l), 128, 0, ctx->stream>>>(a);
+    }
+  }
+  for (int l = NL - 1; l >= 0; --l) {
+    GConvArgs a = args(l);
+    a.x = W.h[l];
+    a.vpar = l + 1 < NL ? W.v[l + 1] : nullptr;
+    ++ctx->launches;
+    if (l > 0) {
+      a.wf = L->wt[g_layer(l)];
+      a.y = W.v[l];
+      k_gconv<GIN_TGATE, GOUT_PLAIN, 2><<<grid(l), 128, 0, ctx->stream>>>(a);
+    } else {
+      a.wf = L->wt[L_G0];
+      a.y = e_out;
+      k_gconv<GIN_TGATE, GOUT_SCALE, 1><<<grid(l), 128, 0, ctx->stream>>>(a);
+    }
+  }
+  PF_CUDA_TRY(cudaGetLastError());
+  return PF_OK;
+}
+
 int gtg_forward(pf_ctx* ctx, LearnedState* L, Work& W, const float* cop, const float* rc_in, float* e_out,
                 const SolveCtl* skip) {
+  if (!W.train) return gtg_apply(ctx, L, W, cop, rc_in, e_out, skip);
   const int B = W.B, NL = W.NL;
   const Dims* D = W.D;
   int rc = 0;
@@ -454,7 +512,7 @@ int gtg_forward(pf_ctx* ctx, LearnedState* L, Work& W, const float* cop, const f
       ++ctx->launches;
       k_pool<<<grid_for(n16(l)), 256, 0, ctx->stream>>>(W.h[l - 1], kGS, D[l - 1], D[l], B, W.q[l], skip);
     }
-    if (W.bwd) {  // training keeps the ungated a_l for the gate gradient
+    if (W.train) {  // training keeps the ungated a_l for the gate gradient
       rc = conv(ctx, L, g_layer(l), W.q[l], kGS, nullptr, false, W.a[l], kGS, D[l], B, skip);
       ++ctx->launches;
       k_gmul<<<grid_for(n16(l)), 256, 0, ctx->stream>>>(W.h[l], W.gam[l], W.a[l], D[l].n, B, skip);
@@ -468,6 +526,7 @@ int gtg_forward(pf_ctx* ctx, LearnedState* L, Work& W, const float* cop, const f
                                                          skip);
   for (int l = NL - 1; l >= 1 && !rc; --l) {
     rc = conv(ctx, L, g_layer(l), W.t[l], kGS, nullptr, true, W.v[l], kGS, D[l], B, skip);
+    if (rc) break;
     ++ctx->launches;
     k_up_add_gate<<<grid_for(n16(l - 1)), 256, 0, ctx->stream>>>(W.h[l - 1], W.v[l], W.gam[l - 1], D[l - 1], D[l], B,
                                                                   W.b[l - 1], W.t[l - 1], skip);

@@ -697,5 +697,239 @@ __global__ void k_zero_f(float* p, size_t n) {
     p[q] = 0.0f;
 }
 
+// ---------------------------------------------------------------------------
+// The G path of the solver's coarse correction (inference), 16 channels.
+//
+// The general brick kernel above spends its time on per-CTA latency: runtime
+// channel counts make every staged element and every tap cost index
+// arithmetic, and one warp per SM sub-partition exposes each instruction's
+// latency.  This kernel fixes the channel counts (16 in, 16 or 8 out), reads
+// its A fragments with ldmatrix at compile-time tap offsets, stages the weight
+// fragments with cp.async, and absorbs the elementwise steps between the
+// convolutions into its operand staging and epilogue, so that one application
+// of e = S G^T G S r_c costs 2 NL launches:
+//   forward, level 0:    x = S r_c                      h_0 = g_0 * (C_0 x),  q_1 = P h_0
+//   forward, level l:    x = q_l                        h_l = g_l * (C_l x),  q_{l+1} = P h_l
+//   transpose, level l:  x = g_l * (h_l + P^T v_{l+1})  v_l = C_l^T x
+//   transpose, level 0:  as level l, then               e = S v_0 (two channels)
+// P averages the 2x2x2 children that exist (sum / 8); P^T gives each child 1/8
+// of its parent; at the deepest level x = g * h.
+//
+// A CTA computes an 8x4x2 brick of one sample.  Warp w owns y in
+// {2(w&1), 2(w&1)+1} at z = w>>1; row r of its mma tile is x = r&7,
+// y = 2(w&1) + (r>>3).  A halo row holds the 16 BF16 channels of one position
+// with a 48-byte pitch: the 8 rows one ldmatrix matrix reads (8 consecutive x)
+// then start in 8 distinct 16-byte bank groups.  Every brick origin is even,
+// so the 2x2x2 children of each pooled output lie inside one CTA.
+
+constexpr int kGBX = 8, kGBY = 4, kGBZ = 2;
+constexpr int kGHX = kGBX + 2, kGHY = kGBY + 2, kGHZ = kGBZ + 2;
+constexpr int kGHN = kGHX * kGHY * kGHZ;
+constexpr int kGPitch = 24;  // BF16 per halo row
+
+enum { GIN_SCALE = 0, GIN_PLAIN = 1, GIN_TGATE = 2 };
+enum { GOUT_GATE = 0, GOUT_PLAIN = 1, GOUT_SCALE = 2 };
+
+struct GConvArgs {
+  const float* x;     // GIN_SCALE: r_c [B][n][2]; GIN_PLAIN: q_l; GIN_TGATE: h_l  ([B][n][16])
+  const float* vpar;  // GIN_TGATE: v_{l+1} [B][nc][16], or null at the deepest level
+  const float* gate;  // g_l [n][16] (GIN_TGATE, GOUT_GATE)
+  const float* cop;   // coarse operator records (GIN_SCALE, GOUT_SCALE)
+  const uint2* wf;    // B fragments: 27 taps x NT x 32 lanes
+  float* y;           // GOUT_GATE: h_l; GOUT_PLAIN: v_l; GOUT_SCALE: e [B][n][2]
+  float* pool;        // GOUT_GATE: q_{l+1} [B][nc][16], or null at the deepest level
+  Dims d, dc;         // this level, the next coarser level
+  int bx, by;         // bricks along x and y
+  const SolveCtl* skip;
+};
+
+__host__ __device__ constexpr int gconv_tap_offset(int k) {
+  return (k % 3) + kGHX * ((k / 3) % 3 + kGHY * (k / 9));
+}
+
+__device__ __forceinline__ void ldmatrix_x4(uint32_t* r, uint32_t addr) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(addr));
+}
+
+template <int IN, int OUT, int NT>
+__global__ void __launch_bounds__(128) k_gconv(GConvArgs a) {
+  if (a.skip && a.skip->done) return;
+  __shared__ __align__(16) __nv_bfloat16 S[kGHN * kGPitch];
+  __shared__ __align__(16) uint2 SW[27 * NT * 32];
+  __shared__ float2 zx[OUT == GOUT_GATE ? 2 * 32 * NT : 1];
+  const int tid = threadIdx.x, b = blockIdx.y;
+  const int brick = blockIdx.x;
+  const int X0 = (brick % a.bx) * kGBX, Y0 = ((brick / a.bx) % a.by) * kGBY, Z0 = (brick / (a.bx * a.by)) * kGBZ;
+  const size_t nb = (size_t)b * a.d.n;
+
+  // weight fragments: 16-byte asynchronous copies, waited for before the mma loop
+  {
+    constexpr int kChunks = 27 * NT * 32 * 8 / 16;
+    const char* src = reinterpret_cast<const char*>(a.wf);
+    const uint32_t dst = (uint32_t)__cvta_generic_to_shared(SW);
+    for (int e = tid; e < kChunks; e += 128)
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst + e * 16), "l"(src + (size_t)e * 16));
+    asm volatile("cp.async.commit_group;\n" ::);
+  }
+
+  // operand halo (10x6x4 positions), rounded to BF16
+  if (IN == GIN_SCALE) {
+    for (int hp = tid; hp < kGHN; hp += 128) {
+      const int x = X0 + hp % kGHX - 1, y = Y0 + (hp / kGHX) % kGHY - 1, z = Z0 + hp / (kGHX * kGHY) - 1;
+      float v0 = 0.0f, v1 = 0.0f;
+      if (x >= 0 && y >= 0 && z >= 0 && x < a.d.X && y < a.d.Y && z < a.d.Z) {
+        const int p = x + a.d.X * (y + a.d.Y * z);
+        const float2 r = *reinterpret_cast<const float2*>(a.x + (nb + p) * 2);
+        v0 = inv_sqrt_diag(a.cop, p, 0) * r.x;
+        v1 = inv_sqrt_diag(a.cop, p, 1) * r.y;
+      }
+      uint4* row = reinterpret_cast<uint4*>(S + hp * kGPitch);
+      row[0] = make_uint4(pack_bf16(v0, v1), 0u, 0u, 0u);
+      row[1] = make_uint4(0u, 0u, 0u, 0u);
+    }
+  } else {
+    constexpr int kItems = kGHN * 4;  // float4 per halo row
+    constexpr int kIter = (kItems + 127) / 128;
+    float4 v[kIter];
+#pragma unroll
+    for (int i = 0; i < kIter; ++i) {
+      const int e = tid + i * 128;
+      v[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      const int hp = e >> 2, c = (e & 3) * 4;
+      const int x = X0 + hp % kGHX - 1, y = Y0 + (hp / kGHX) % kGHY - 1, z = Z0 + hp / (kGHX * kGHY) - 1;
+      if (e < kItems && x >= 0 && y >= 0 && z >= 0 && x < a.d.X && y < a.d.Y && z < a.d.Z) {
+        const int p = x + a.d.X * (y + a.d.Y * z);
+        float4 h = __ldg(reinterpret_cast<const float4*>(a.x + (nb + p) * kGS + c));
+        if (IN == GIN_TGATE) {
+          if (a.vpar) {
+            const int pp = (x >> 1) + a.dc.X * ((y >> 1) + a.dc.Y * (z >> 1));
+            const float4 u =
+                __ldg(reinterpret_cast<const float4*>(a.vpar + ((size_t)b * a.dc.n + pp) * kGS + c));
+            h.x += u.x * 0.125f;
+            h.y += u.y * 0.125f;
+            h.z += u.z * 0.125f;
+            h.w += u.w * 0.125f;
+          }
+          const float4 g = __ldg(reinterpret_cast<const float4*>(a.gate + (size_t)p * kGS + c));
+          h.x *= g.x;
+          h.y *= g.y;
+          h.z *= g.z;
+          h.w *= g.w;
+        }
+        v[i] = h;
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < kIter; ++i) {
+      const int e = tid + i * 128;
+      if (e < kItems)
+        *reinterpret_cast<uint2*>(S + (e >> 2) * kGPitch + (e & 3) * 4) =
+            make_uint2(pack_bf16(v[i].x, v[i].y), pack_bf16(v[i].z, v[i].w));
+    }
+  }
+  asm volatile("cp.async.wait_all;\n" ::);
+  __syncthreads();
+
+  // 27 taps, A fragments prefetched kPre taps ahead, two accumulator sets (even / odd taps)
+  const int warp = tid >> 5, lane = tid & 31;
+  const int yp = warp & 1, wz = warp >> 1;
+  const int lm = lane >> 3;
+  const uint32_t abase = (uint32_t)__cvta_generic_to_shared(S) +
+                         (uint32_t)(((lane & 7) + kGHX * (2 * yp + (lm & 1) + kGHY * wz)) * kGPitch + (lm >> 1) * 8) * 2;
+  constexpr int kPre = 4;
+  uint32_t fa[kPre][4];
+#pragma unroll
+  for (int k = 0; k < kPre; ++k) ldmatrix_x4(fa[k], abase + gconv_tap_offset(k) * kGPitch * 2);
+  float acc[2][NT][4];
+#pragma unroll
+  for (int s = 0; s < 2; ++s)
+#pragma unroll
+    for (int j = 0; j < NT; ++j) acc[s][j][0] = acc[s][j][1] = acc[s][j][2] = acc[s][j][3] = 0.0f;
+#pragma unroll
+  for (int k = 0; k < 27; ++k) {
+    uint32_t* f = fa[k % kPre];
+    const uint32_t a0 = f[0], a1 = f[1], a2 = f[2], a3 = f[3];
+    if (k + kPre < 27) ldmatrix_x4(f, abase + gconv_tap_offset(k + kPre) * kGPitch * 2);
+#pragma unroll
+    for (int j = 0; j < NT; ++j) {
+      const uint2 bw = SW[(k * NT + j) * 32 + lane];
+      mma_bf16(acc[k & 1][j], a0, a1, a2, a3, bw.x, bw.y);
+    }
+  }
+
+  // epilogue: lane (g, t) holds rows g (y = Y0 + 2yp) and g + 8 (y + 1), channels j*8 + 2t, +1
+  const int g = lane >> 2, t = lane & 3;
+  const int x = X0 + g, z = Z0 + wz;
+  float r[NT][4];
+#pragma unroll
+  for (int j = 0; j < NT; ++j)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) r[j][q] = acc[0][j][q] + acc[1][j][q];
+  bool inr[2];
+  int pos[2];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int y = Y0 + 2 * yp + h;
+    inr[h] = x < a.d.X && y < a.d.Y && z < a.d.Z;
+    pos[h] = x + a.d.X * (y + a.d.Y * z);
+  }
+  if (OUT == GOUT_SCALE) {
+    if (t == 0) {
+#pragma unroll
+      for (int h = 0; h < 2; ++h)
+        if (inr[h])
+          *reinterpret_cast<float2*>(a.y + (nb + pos[h]) * 2) =
+              make_float2(inv_sqrt_diag(a.cop, pos[h], 0) * r[0][2 * h], inv_sqrt_diag(a.cop, pos[h], 1) * r[0][2 * h + 1]);
+    }
+  } else if (OUT == GOUT_PLAIN) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+      if (inr[h])
+#pragma unroll
+        for (int j = 0; j < NT; ++j)
+          *reinterpret_cast<float2*>(a.y + (nb + pos[h]) * kGS + j * 8 + 2 * t) = make_float2(r[j][2 * h], r[j][2 * h + 1]);
+  } else {
+    float2 s[NT];
+#pragma unroll
+    for (int j = 0; j < NT; ++j) s[j] = make_float2(0.0f, 0.0f);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      if (!inr[h]) continue;
+#pragma unroll
+      for (int j = 0; j < NT; ++j) {
+        const int c0 = j * 8 + 2 * t;
+        const float2 gv = __ldg(reinterpret_cast<const float2*>(a.gate + (size_t)pos[h] * kGS + c0));
+        const float2 hv = make_float2(gv.x * r[j][2 * h], gv.y * r[j][2 * h + 1]);
+        *reinterpret_cast<float2*>(a.y + (nb + pos[h]) * kGS + c0) = hv;
+        s[j].x += hv.x;
+        s[j].y += hv.y;
+      }
+    }
+    if (a.pool) {  // uniform over the CTA
+#pragma unroll
+      for (int j = 0; j < NT; ++j) {  // x pairs: rows g and g ^ 1
+        s[j].x += __shfl_xor_sync(0xffffffffu, s[j].x, 4);
+        s[j].y += __shfl_xor_sync(0xffffffffu, s[j].y, 4);
+      }
+      if (wz == 1)
+#pragma unroll
+        for (int j = 0; j < NT; ++j) zx[(yp * 32 + lane) * NT + j] = s[j];
+      __syncthreads();
+      const int cx = x >> 1, cy = (Y0 >> 1) + yp, cz = Z0 >> 1;
+      if (wz == 0 && (g & 1) == 0 && cx < a.dc.X && cy < a.dc.Y && cz < a.dc.Z) {
+        float* q = a.pool + ((size_t)b * a.dc.n + cx + (size_t)a.dc.X * (cy + (size_t)a.dc.Y * cz)) * kGS;
+#pragma unroll
+        for (int j = 0; j < NT; ++j) {
+          const float2 o = zx[(yp * 32 + lane) * NT + j];
+          *reinterpret_cast<float2*>(q + j * 8 + 2 * t) =
+              make_float2((s[j].x + o.x) * 0.125f, (s[j].y + o.y) * 0.125f);
+        }
+      }
+    }
+  }
+}
+
 }  // namespace
 }  // namespace pf

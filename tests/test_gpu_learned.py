@@ -47,12 +47,14 @@ def _system(seed, B=3, dims=DIMS):
     return cop, rc, tgt
 
 
-def test_forward_matches_cpu(small):
+@pytest.mark.parametrize("dims,B", [(DIMS, 3), (DIMS, 1), ((9, 9, 9), 1), ((13, 9, 6), 1)])
+def test_forward_matches_cpu(small, dims, B):
+    """Batches of residuals and the solver's single residual, on odd lattices."""
     _, net = small
-    cop, rc, _ = _system(1)
+    cop, rc, _ = _system(1, B=B, dims=dims)
     params = cn.unflatten(net.params())
-    e_gpu = net.eval(DIMS, cop, rc)
-    e_cpu = cn.coarse_correction(params, cop, DIMS, rc, round_bf16=True)
+    e_gpu = net.eval(dims, cop, rc)
+    e_cpu = cn.coarse_correction(params, cop, dims, rc, round_bf16=True)
     assert np.all(np.isfinite(e_gpu))
     assert rel_l2(e_gpu, e_cpu) < 2e-3
     # dead unknowns get no correction
@@ -170,7 +172,7 @@ def trained(pf):
     net.harvest(False)
     systems, pairs = net.dataset()
     assert systems == 3 and pairs >= 3 * 150
-    losses = net.train(steps=600, batch=8, lr=1e-3, seed=1)
+    losses = net.train(steps=1200, batch=8, lr=1e-3, seed=1)
     out = {"losses": losses, "params": net.params(), "dataset": (systems, pairs)}
     g.close()
     return out
@@ -218,7 +220,7 @@ def test_learned_preconditioner_ablation(pf, trained):
         # conditioning times that residual, not by 1e-6
         assert np.abs(p_n - p_plain).max() < 2e-4 * np.abs(p_plain).max()
         assert st_n.precond_applied > 0
-        assert st_n.iterations < 0.8 * st_j.iterations, (st_n.iterations, st_j.iterations)
+        assert st_n.iterations < 0.85 * st_j.iterations, (st_n.iterations, st_j.iterations)
     finally:
         g.close()
 
@@ -274,3 +276,23 @@ def test_merge_dataset_across_grid_sizes(pf):
     finally:
         g1.close()
         g2.close()
+
+
+def test_shipped_weights_ablation_128(pf):
+    """The shipped weights on a 128^3 system none of the training systems
+    was: at most 0.6x the iterations of the same flexible PCG without the
+    network, same plain solution."""
+    L = pf.PF_SOLVER_LEARNED
+    g, solve = _pressure_system(pf, 128, seed=0)
+    try:
+        net = pf.LearnedCoarseSolver(g)
+        net.load_default()
+        st_p, p_plain = solve(pf.SolverConfig(mode=pf.PF_SOLVER_PLAIN, rel_tol=1e-6))
+        st_j, _ = solve(pf.SolverConfig(mode=L, rel_tol=1e-6, precond=pf.PF_PRECOND_JACOBI))
+        st_n, p_n = solve(pf.SolverConfig(mode=L, rel_tol=1e-6, precond=pf.PF_PRECOND_NETWORK))
+        assert st_n.converged and st_n.res_final <= 1e-6 * st_n.res0
+        assert st_n.precond_rejected == 0
+        assert np.abs(p_n - p_plain).max() < 2e-4 * np.abs(p_plain).max()
+        assert st_n.iterations < 0.6 * st_j.iterations, (st_n.iterations, st_j.iterations)
+    finally:
+        g.close()
