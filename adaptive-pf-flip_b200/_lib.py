@@ -38,7 +38,7 @@ EXPORTS = (
     "pf_learned_eval", "pf_learned_adam",
 )
 
-STAGES = ("bin", "sort", "splat", "normalize", "mark", "boundary", "project", "pcg", "g2p")
+STAGES = ("bin", "sort", "splat", "normalize", "mark", "boundary", "project", "pcg", "g2p", "precond_setup")
 
 
 class GridDesc(C.Structure):
@@ -86,7 +86,7 @@ class StepStats(C.Structure):
 
 
 class Timing(C.Structure):
-    _fields_ = [("ms", C.c_double * 9), ("count", C.c_longlong * 9)]
+    _fields_ = [("ms", C.c_double * len(STAGES)), ("count", C.c_longlong * len(STAGES))]
 
     def as_dict(self):
         return {name: (self.ms[i], self.count[i]) for i, name in enumerate(STAGES)}

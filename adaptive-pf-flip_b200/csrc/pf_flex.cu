@@ -498,6 +498,7 @@ int flex_solve(pf_ctx* ctx, int nslots, int nred, const uint8_t* kind, FlexVec<V
 int solve_learned(pf_ctx* ctx, int nslots, int nred, const uint8_t* kind, double scale, const pf_solve_cfg* cfg,
                   SolveResult* res) {
   StageScope stage(ctx, PF_STAGE_PCG);
+  StageScope setup_stage(ctx, PF_STAGE_PRECOND_SETUP);
   int rc = coarse_ensure(ctx);
   if (rc) return rc;
   const int precond = cfg->precond;
@@ -527,6 +528,7 @@ int solve_learned(pf_ctx* ctx, int nslots, int nred, const uint8_t* kind, double
   int* nbr = nullptr;
   rc = build_neighbor_table(ctx, nslots, &nbr);
   if (rc) return rc;
+  stage_end(ctx, PF_STAGE_PRECOND_SETUP);
 
   if (!cfg->inner_fp32) {
     // FP64 flexible PCG on the exact operator

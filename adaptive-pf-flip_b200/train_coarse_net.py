@@ -2,11 +2,17 @@
 parameter vector (the file the package loads by default).
 
 Training pairs (r_c, A_c^-1 r_c) are harvested on the GPU from exact
-two-level solves (PF_PRECOND_EXACT_COARSE) of seeded pressure systems:
-64 air ellipsoids in water at 1000:1 with a band-limited divergence
-(scenes.ellipsoid_pressure), at 64^3, 128^3 and 256^3 (seeds 1-3, 1-2, 1;
-seed 0 is left for evaluation).  Each grid size harvests on its own context;
-the pairs are then merged into one context and trained with one optimiser.
+two-level solves (PF_PRECOND_EXACT_COARSE) of seeded pressure systems
+(seed 0 of every scene is left for evaluation):
+
+* 64 air ellipsoids in water at 1000:1 with a band-limited divergence
+  (scenes.ellipsoid_pressure) at 64^3, 128^3 and 256^3;
+* the pressure systems of whole solver steps: Rayleigh-Taylor at 48^3 and
+  128^3 (heavy over light, walls only) and the bubble tank at 128^3 (air
+  bubble in water under an open headspace), several consecutive steps each.
+
+Each grid harvests on its own context; the pairs are then merged into one
+context and trained with one optimiser.
 
     python adaptive-pf-flip_b200/train_coarse_net.py [--out PATH] [--steps N]
 """
@@ -60,31 +66,70 @@ def pressure_system(pf, n, seed, grid=None):
     return g, solve
 
 
-PLAN = ((64, 1), (64, 2), (64, 3), (128, 1), (128, 2), (256, 1))
+def step_systems(pf, scene, n, seed, steps, solve_cfg, harvest_on):
+    """Run `steps` whole solver steps of a seeded scene with the given solver
+    (the harvest is switched on by `harvest_on(grid)` after the first, plain,
+    step so that every harvested system has a developed velocity field);
+    returns (sim, iterations per harvested step)."""
+    sc = pf.scenes.rayleigh_taylor(n, seed=seed) if scene == "rt" else pf.scenes.bubble_tank(n, seed=seed)
+    sim = pf.SparseSim3DTP(n, n, n, sc["dx"], max_particles=len(sc["pos"]))
+    sim.phase = pf.PhaseParams(sc["rho_l"], sc["rho_g"])
+    sim.phase.rho_tilde_0 = pf.calibrateRhoTilde0(sim.phase, 1.0, grid=sim.grid)
+    sim.dt = 1.0 / 240.0
+    if scene == "bubble":
+        sim.alpha_liquid = sim.alpha_gas = 0.97
+    sim.cg_iters, sim.cg_tol = 20000, 0.0
+    sim.solver = pf.SolverConfig(rel_tol=1e-6)
+    sim.set_particles(sc["pos"], sc["vel"], sc["type"], sc["volume"])
+    del sc
+    sim.step()
+    harvest_on(sim.grid)
+    sim.solver = solve_cfg
+    return sim, [sim.step().solve.iterations for _ in range(steps)]
+
+
+# (scene, n, seed, steps): ellipsoid systems are solved once; step scenes
+# harvest from `steps` consecutive steps
+PLAN = (("ellipsoid", 64, 1, 1), ("ellipsoid", 64, 2, 1), ("ellipsoid", 64, 3, 1), ("ellipsoid", 128, 1, 1),
+        ("ellipsoid", 128, 2, 1), ("ellipsoid", 256, 1, 1), ("rt", 48, 1, 6), ("rt", 128, 1, 3),
+        ("bubble", 128, 1, 3), ("bubble", 128, 2, 2))
 
 
 def train(plan=PLAN, steps=3600, batch=8, seed=11, log=print):
     pf = _package()
     nets, grids, params = {}, {}, None
+    exact = pf.SolverConfig(mode=pf.PF_SOLVER_LEARNED, rel_tol=1e-6, precond=pf.PF_PRECOND_EXACT_COARSE)
     t0 = time.time()
-    for n, s in plan:
-        g, solve = pressure_system(pf, n, s, grids.get(n))
-        grids[n] = g
-        if n not in nets:
-            nets[n] = pf.LearnedCoarseSolver(g)
-            if params is None:
-                nets[n].init(seed)
-                params = nets[n].params()
-            else:
-                nets[n].load(params)
-            nets[n].harvest(True, stride=2, max_per_system=200, capacity_floats=1 << 27)
-        st, _ = solve(pf.SolverConfig(mode=pf.PF_SOLVER_LEARNED, rel_tol=1e-6, precond=pf.PF_PRECOND_EXACT_COARSE))
-        log(f"harvest n={n} seed={s}: {st.iterations} exact two-level iterations, {time.time() - t0:.1f} s")
+
+    def start(key, g):
+        nonlocal params
+        net = pf.LearnedCoarseSolver(g)
+        if params is None:
+            net.init(seed)
+            params = net.params()
+        else:
+            net.load(params)
+        net.harvest(True, stride=2, max_per_system=200, capacity_floats=1 << 27)
+        nets[key] = net
+
+    for scene, n, s, k in plan:
+        if scene == "ellipsoid":
+            g, solve = pressure_system(pf, n, s, grids.get(("ellipsoid", n)))
+            if ("ellipsoid", n) not in nets:
+                grids[("ellipsoid", n)] = g
+                start(("ellipsoid", n), g)
+            st, _ = solve(exact)
+            its = [st.iterations]
+        else:
+            key = (scene, n, s)
+            sim, its = step_systems(pf, scene, n, s, k, exact, lambda g: start(key, g))
+            grids[key] = sim.grid
+        log(f"harvest {scene} n={n} seed={s}: exact two-level iterations {its}, {time.time() - t0:.1f} s")
     for net in nets.values():
         net.harvest(False)
-    # one optimiser over every grid size: gather the pairs in the largest grid's context
-    trainer = nets[max(nets)]
-    for n, net in nets.items():
+    # one optimiser over every system: gather the pairs in the context of the largest lattice
+    trainer = nets[("ellipsoid", max(n for sc_, n, _, _ in plan if sc_ == "ellipsoid"))]
+    for key, net in nets.items():
         if net is not trainer:
             trainer.merge_dataset(net)
     systems, pairs = trainer.dataset()

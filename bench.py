@@ -277,11 +277,23 @@ def pcg_modes(pf, names):
         # the learned two-level preconditioner and its net-free ablation
         "learned": pf.SolverConfig(mode=L, rel_tol=1e-6, precond=pf.PF_PRECOND_NETWORK),
         "flex_jacobi": pf.SolverConfig(mode=L, rel_tol=1e-6, precond=pf.PF_PRECOND_JACOBI),
+        # the same two-level solver with an exact coarse solve: the bound a perfect network reaches
+        "exact_coarse": pf.SolverConfig(mode=L, rel_tol=1e-6, precond=pf.PF_PRECOND_EXACT_COARSE),
     }
-    return [(name, table[name]) for name in names]
+    # "name#k" repeats a mode (a second solve on the same context: allocations done)
+    return [(name, table[name.split("#")[0]]) for name in names]
 
 
-def run_pcg(pf, n, modes, max_iter=20000, seed=0):
+def load_weights(pf, grid, path=None):
+    """Load the shipped network weights (or the file at `path`) into a grid's context."""
+    net = pf.LearnedCoarseSolver(grid)
+    if path:
+        net.load_file(path)
+        return os.path.relpath(os.path.abspath(path), ROOT)
+    return net.load_default()
+
+
+def run_pcg(pf, n, modes, max_iter=20000, seed=0, weights_path=None):
     """Pressure-only system (n^3, every interior cell fluid, 64 air ellipsoids
     in water at 1000:1, band-limited RHS): device time to a 1e-6 relative
     FP64 residual per solver mode, and each mode's pressure against the
@@ -296,16 +308,21 @@ def run_pcg(pf, n, modes, max_iter=20000, seed=0):
         g.set_field(("u", "v", "w", "mu", "mv", "mw", "p", "mk").index(k), f[k], full[k])
     weights = None
     if any(cfg.mode == pf.PF_SOLVER_LEARNED and cfg.precond == pf.PF_PRECOND_NETWORK for _, cfg in modes):
-        net = pf.LearnedCoarseSolver(g)
-        weights = net.load_default()
+        weights = load_weights(pf, g, weights_path)
     out, p_plain = {}, None
+    lib = pf.load()
     for name, cfg in modes:
         for k in ("u", "v", "w"):
             g.set_field(("u", "v", "w").index(k), f[k], full[k])
+        lib.pf_set_timing(g.ctx, 1)
         st = pf.spProjectStepVC3D(g, pp, 1.0 / 240.0, max_iter, 0.0, solver=cfg)
+        tm = pf._lib.Timing()
+        lib.pf_get_timing(g.ctx, C.byref(tm), 1)
+        lib.pf_set_timing(g.ctx, 0)
         p, _ = g.get_field(pf.PF_P)
         rec = {"ms_to_1e-6": st.solve_ms, "iterations": st.iterations, "refinements": st.refinements,
-               "converged": bool(st.converged), "rel_residual": st.res_final / max(st.res0, 1e-300)}
+               "converged": bool(st.converged), "rel_residual": st.res_final / max(st.res0, 1e-300),
+               "setup_ms": tm.as_dict()["precond_setup"][0]}
         if cfg.mode == pf.PF_SOLVER_LEARNED:
             rec["coarse_accepted"] = st.precond_applied
             rec["coarse_rejected"] = st.precond_rejected
@@ -321,6 +338,75 @@ def run_pcg(pf, n, modes, max_iter=20000, seed=0):
         out[name]["speedup_vs_plain"] = base / max(out[name]["ms_to_1e-6"], 1e-9)
     return {"workload": f"ellipsoid_pressure_{n}: {(n - 2) ** 3} unknowns, 64 air ellipsoids, 1000:1, "
                         "band-limited RHS |k|<=8", "modes": out}
+
+
+def step_scene(pf, name, n, seed=0):
+    """Scene of a whole-step pressure system: Rayleigh-Taylor (heavy over
+    light, 1000:1, walls only) or the bubble tank (air bubble in water, open
+    headspace)."""
+    if name == "rt":
+        return pf.scenes.rayleigh_taylor(n, seed=seed)
+    if name == "bubble":
+        return pf.scenes.bubble_tank(n, seed=seed)
+    raise ValueError(f"unknown step scene {name!r} (rt, bubble)")
+
+
+def run_step_pcg(pf, name, n, modes, pre_steps=1, max_iter=20000, seed=0, weights_path=None):
+    """Pressure systems of real solver steps: the scene runs `pre_steps` plain
+    steps, then every solver mode runs one whole step (markCells .. advect)
+    from that same particle snapshot.  Reports each solve's device time to a
+    1e-6 relative FP64 residual, iterations, the coarse-correction fallback
+    rate and the pressure against the PLAIN solve (the first mode)."""
+    sc = step_scene(pf, name, n, seed)
+    np_ = len(sc["pos"])
+    sim = pf.SparseSim3DTP(n, n, n, sc["dx"], max_particles=np_)
+    sim.phase = pf.PhaseParams(sc["rho_l"], sc["rho_g"])
+    sim.phase.rho_tilde_0 = pf.calibrateRhoTilde0(sim.phase, 1.0, grid=sim.grid)
+    sim.dt = 1.0 / 240.0
+    if name == "bubble":
+        sim.alpha_liquid = sim.alpha_gas = 0.97
+    sim.cg_iters, sim.cg_tol = max_iter, 0.0
+    sim.solver = pf.SolverConfig(rel_tol=1e-6)
+    sim.set_particles(sc["pos"], sc["vel"], sc["type"], sc["volume"])
+    del sc
+    for _ in range(pre_steps):
+        sim.step()
+    snap = sim.get_particles()
+    weights = None
+    if any(cfg.mode == pf.PF_SOLVER_LEARNED and cfg.precond == pf.PF_PRECOND_NETWORK for _, cfg in modes):
+        weights = load_weights(pf, sim.grid, weights_path)
+    out, p_plain = {}, None
+    lib = pf.load()
+    for mname, cfg in modes:
+        sim.set_particles(*snap)
+        sim.solver = cfg
+        lib.pf_set_timing(sim.grid.ctx, 1)
+        st = sim.step().solve
+        tm = pf._lib.Timing()
+        lib.pf_get_timing(sim.grid.ctx, C.byref(tm), 1)
+        lib.pf_set_timing(sim.grid.ctx, 0)
+        p, _ = sim.grid.get_field(pf.PF_P)
+        stages = tm.as_dict()
+        rec = {"ms_to_1e-6": st.solve_ms, "iterations": st.iterations, "refinements": st.refinements,
+               "converged": bool(st.converged), "rel_residual": st.res_final / max(st.res0, 1e-300),
+               "setup_ms": stages["precond_setup"][0]}
+        if cfg.mode == pf.PF_SOLVER_LEARNED:
+            tot = st.precond_applied + st.precond_rejected
+            rec["coarse_accepted"] = st.precond_applied
+            rec["coarse_rejected"] = st.precond_rejected
+            rec["fallback_rate"] = st.precond_rejected / tot if tot else 0.0
+            if cfg.precond == pf.PF_PRECOND_NETWORK:
+                rec["weights"] = weights
+        if p_plain is None:
+            p_plain = p.astype(np.float64)
+        else:
+            rec["p_rel_diff_vs_plain"] = float(np.abs(p - p_plain).max() / max(np.abs(p_plain).max(), 1e-300))
+        out[mname] = rec
+    base = out[modes[0][0]]["ms_to_1e-6"]
+    for mname in out:
+        out[mname]["speedup_vs_plain"] = base / max(out[mname]["ms_to_1e-6"], 1e-9)
+    return {"workload": f"{name}_{n} step pressure system after {pre_steps} plain step(s): {np_} particles, "
+                        f"1000:1, dt 1/240", "unknowns": int(st.n_cells), "modes": out}
 
 
 def run_full_step(pf, n=48, steps=20, seed=0):
@@ -468,6 +554,10 @@ def main():
     ap.add_argument("--pcg-modes", default="plain_fp64,learned,flex_jacobi",
                     help="solvers of the pressure-only block (plain_fp64 first): plain_fp64, learned, "
                          "flex_jacobi, mixed_fp32, mixed_bf16")
+    ap.add_argument("--step-pcg", default="",
+                    help="run only whole-step pressure systems, e.g. rt:256,bubble:128 (modes from --pcg-modes)")
+    ap.add_argument("--step-pcg-pre", type=int, default=1, help="plain steps before the step-pressure snapshot")
+    ap.add_argument("--weights", default="", help="network weights for the learned mode (default: shipped)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
@@ -476,10 +566,19 @@ def main():
         world = int(os.environ.get("WORLD_SIZE", "1"))
         run_reference(args, rank, world)
         return
+    if args.step_pcg:  # whole-step pressure systems alone
+        pf = load_pkg()
+        modes = pcg_modes(pf, args.pcg_modes.split(","))
+        for item in args.step_pcg.split(","):
+            name, n = item.split(":")
+            print(json.dumps(run_step_pcg(pf, name, int(n), modes, pre_steps=args.step_pcg_pre,
+                                          max_iter=args.pcg_max_iter, weights_path=args.weights or None)),
+                  flush=True)
+        return
     if args.pcg_only:  # the pressure-only block alone (profiling)
         pf = load_pkg()
         print(json.dumps(run_pcg(pf, args.pcg_n, pcg_modes(pf, args.pcg_modes.split(",")),
-                                 max_iter=args.pcg_max_iter)), flush=True)
+                                 max_iter=args.pcg_max_iter, weights_path=args.weights or None)), flush=True)
         return
     rank, world, local, dist = dist_setup(args.gpus)
     try:

@@ -201,6 +201,7 @@ enum pf_stage {
   PF_STAGE_PROJECT,      /* whole projection */
   PF_STAGE_PCG,          /* iterative solve only */
   PF_STAGE_G2P,          /* G2P and/or advection */
+  PF_STAGE_PRECOND_SETUP, /* LEARNED solves: coarse operator, gate network, neighbour table */
   PF_NSTAGES
 };
 typedef struct {
