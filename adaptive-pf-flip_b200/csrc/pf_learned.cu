@@ -84,6 +84,7 @@ struct LearnedState {
   uint2 *wf[kNumLayers] = {}, *wt[kNumLayers] = {};
   int adam_step = 0;
   float* wpart = nullptr;
+  double* gstat = nullptr;  // gradient clipping state (k_grad_clip)
   Work inf, train, eval;
   // training set: systems (coarse operators) and (rc, e*) pairs
   struct System {
@@ -141,6 +142,8 @@ int state_init(pf_ctx* ctx, LearnedState* L) {
     PF_CUDA_TRY(cudaMalloc(&L->wt[l], frag_count(co, ci) * sizeof(uint2)));
   }
   PF_CUDA_TRY(cudaMalloc(&L->wpart, (size_t)kWgradCtas * 27 * 128 * 64 * sizeof(float)));
+  PF_CUDA_TRY(cudaMalloc(&L->gstat, 4 * sizeof(double)));
+  PF_CUDA_TRY(cudaMemset(L->gstat, 0, 4 * sizeof(double)));
   return allow_brick_smem(ctx);
 }
 
@@ -611,13 +614,21 @@ int loss_backward(pf_ctx* ctx, LearnedState* L, Work& W, const float* cop, const
   return unet_backward(ctx, L, W);
 }
 
-int adam_step(pf_ctx* ctx, LearnedState* L, double lr) {
+// One Adam step on L->grads; `clip` applies the training loop's gradient-norm
+// clipping first (the step counter still advances on a skipped step).
+int adam_step(pf_ctx* ctx, LearnedState* L, double lr, bool clip) {
   L->adam_step += 1;
   const double b1 = 0.9, b2 = 0.999;
   const double c1 = 1.0 - std::pow(b1, L->adam_step), c2 = 1.0 - std::pow(b2, L->adam_step);
+  if (clip) {
+    ctx->launches += 2;
+    k_grad_sumsq<<<grid_for(L->nparams), 256, 0, ctx->stream>>>(L->grads, L->nparams, L->gstat);
+    k_grad_clip<<<1, 1, 0, ctx->stream>>>(L->gstat);
+  }
   ++ctx->launches;
   k_adam<<<grid_for(L->nparams), 256, 0, ctx->stream>>>(L->params, L->grads, L->adam_m, L->adam_v, L->nparams,
-                                                       (float)lr, (float)b1, (float)b2, (float)c1, (float)c2, 1e-8f);
+                                                       (float)lr, (float)b1, (float)b2, (float)c1, (float)c2, 1e-8f,
+                                                       clip ? L->gstat + 1 : nullptr);
   PF_CUDA_TRY(cudaGetLastError());
   return repack(ctx, L);
 }
@@ -690,6 +701,7 @@ void learned_release(CoarseCtx* c) {
   float* fl[] = {L->params, L->grads, L->adam_m, L->adam_v, L->wpart, L->pool, L->batch_rc, L->batch_tgt};
   for (float* q : fl)
     if (q) cudaFree(q);
+  if (L->gstat) cudaFree(L->gstat);
   for (int l = 0; l < kNumLayers; ++l) {
     if (L->wf[l]) cudaFree(L->wf[l]);
     if (L->wt[l]) cudaFree(L->wt[l]);
@@ -743,6 +755,7 @@ int pf_learned_init(pf_ctx* ctx, unsigned long long seed) {
   PF_CUDA_TRY(cudaMemcpyAsync(L->params, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
   PF_CUDA_TRY(cudaMemsetAsync(L->adam_m, 0, L->nparams * sizeof(float), ctx->stream));
   PF_CUDA_TRY(cudaMemsetAsync(L->adam_v, 0, L->nparams * sizeof(float), ctx->stream));
+  PF_CUDA_TRY(cudaMemsetAsync(L->gstat, 0, 4 * sizeof(double), ctx->stream));
   L->adam_step = 0;
   rc = repack(ctx, L);
   if (rc) return rc;
@@ -763,6 +776,7 @@ int pf_learned_load(pf_ctx* ctx, const float* params, size_t n) {
   PF_CUDA_TRY(cudaMemcpyAsync(L->params, params, n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
   PF_CUDA_TRY(cudaMemsetAsync(L->adam_m, 0, n * sizeof(float), ctx->stream));
   PF_CUDA_TRY(cudaMemsetAsync(L->adam_v, 0, n * sizeof(float), ctx->stream));
+  PF_CUDA_TRY(cudaMemsetAsync(L->gstat, 0, 4 * sizeof(double), ctx->stream));
   L->adam_step = 0;
   rc = repack(ctx, L);
   if (rc) return rc;
@@ -911,7 +925,7 @@ int pf_learned_train(pf_ctx* ctx, int steps, int batch, double lr, unsigned long
     if (rc) return rc;
     rc = loss_backward(ctx, L, L->train, sys.cop, L->batch_rc, L->batch_tgt);
     if (rc) return rc;
-    rc = adam_step(ctx, L, lr);
+    rc = adam_step(ctx, L, lr, true);
     if (rc) return rc;
     if (losses) {
       PF_CUDA_TRY(cudaMemcpyAsync(hl.data(), L->train.loss, batch * sizeof(double), cudaMemcpyDeviceToHost,
@@ -982,7 +996,7 @@ int pf_learned_adam(pf_ctx* ctx, const float* grad, size_t n, double lr) {
   cudaSetDevice(ctx->device);
   LearnedState* L = ((CoarseCtx*)ctx->learned)->net;
   PF_CUDA_TRY(cudaMemcpyAsync(L->grads, grad, n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
-  int r = adam_step(ctx, L, lr);
+  int r = adam_step(ctx, L, lr, false);
   if (r) return r;
   PF_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   return PF_OK;

@@ -680,10 +680,53 @@ __global__ void __launch_bounds__(256) k_loss_grad(const double* v, const double
   }
 }
 
-__global__ void k_adam(float* p, const float* g, float* m, float* v, size_t n, float lr, float b1, float b2,
-                       float c1, float c2, float eps) {
+// Global gradient-norm clipping of the training loop.  gs[0] = sum of g^2
+// (accumulated by k_grad_sumsq), gs[1] = the step's gradient scale, gs[2] =
+// running average of the clipped norm, gs[3] = steps seen.  A non-finite
+// gradient skips the step (scale 0); a norm above twice the running average
+// is scaled down to it, so that one outlier batch neither moves the weights
+// far nor inflates Adam's second moment for thousands of steps.
+__global__ void __launch_bounds__(256) k_grad_sumsq(const float* g, size_t n, double* gs) {
+  double a = 0.0;
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
-    const float gq = g[q];
+    const double v = g[q];
+    a += v * v;
+  }
+  a = warp_sum(a);
+  __shared__ double sh[8];
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = a;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < 8; ++w) t += sh[w];
+    atomicAdd(gs, t);
+  }
+}
+
+__global__ void k_grad_clip(double* gs) {
+  const double norm = sqrt(gs[0]);
+  double scale = 1.0;
+  if (!isfinite(norm)) {
+    scale = 0.0;
+  } else {
+    const double thr = gs[3] > 0.0 ? 2.0 * gs[2] : norm;
+    if (norm > thr && norm > 0.0) scale = thr / norm;
+    const double clipped = norm * scale;
+    gs[2] = gs[3] > 0.0 ? 0.95 * gs[2] + 0.05 * clipped : clipped;
+    gs[3] += 1.0;
+  }
+  gs[1] = scale;
+  gs[0] = 0.0;
+}
+
+// Adam; `gscale` (optional) multiplies the gradient, and a zero scale leaves
+// the parameters and moments unchanged.
+__global__ void k_adam(float* p, const float* g, float* m, float* v, size_t n, float lr, float b1, float b2,
+                       float c1, float c2, float eps, const double* gscale) {
+  const float sc = gscale ? (float)*gscale : 1.0f;
+  if (sc == 0.0f) return;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+    const float gq = g[q] * sc;
     const float mq = b1 * m[q] + (1.0f - b1) * gq;
     const float vq = b2 * v[q] + (1.0f - b2) * gq * gq;
     m[q] = mq;

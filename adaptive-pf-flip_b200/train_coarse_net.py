@@ -7,12 +7,14 @@ two-level solves (PF_PRECOND_EXACT_COARSE) of seeded pressure systems
 
 * 64 air ellipsoids in water at 1000:1 with a band-limited divergence
   (scenes.ellipsoid_pressure) at 64^3, 128^3 and 256^3;
-* the pressure systems of whole solver steps: Rayleigh-Taylor at 48^3 and
-  128^3 (heavy over light, walls only) and the bubble tank at 128^3 (air
-  bubble in water under an open headspace), several consecutive steps each.
+* the pressure systems of whole solver steps: Rayleigh-Taylor at 48^3,
+  128^3 and 256^3 (heavy over light, walls only) and the bubble tank at
+  128^3 (air bubble in water under an open headspace), one to six
+  consecutive steps each.
 
 Each grid harvests on its own context; the pairs are then merged into one
-context and trained with one optimiser.
+context and trained with one optimiser (Adam with gradient-norm clipping,
+8000 steps of batch 8).
 
     python adaptive-pf-flip_b200/train_coarse_net.py [--out PATH] [--steps N]
 """
@@ -92,10 +94,10 @@ def step_systems(pf, scene, n, seed, steps, solve_cfg, harvest_on):
 # harvest from `steps` consecutive steps
 PLAN = (("ellipsoid", 64, 1, 1), ("ellipsoid", 64, 2, 1), ("ellipsoid", 64, 3, 1), ("ellipsoid", 128, 1, 1),
         ("ellipsoid", 128, 2, 1), ("ellipsoid", 256, 1, 1), ("rt", 48, 1, 6), ("rt", 128, 1, 3),
-        ("bubble", 128, 1, 3), ("bubble", 128, 2, 2))
+        ("bubble", 128, 1, 3), ("bubble", 128, 2, 2), ("rt", 256, 1, 1), ("rt", 128, 2, 3))
 
 
-def train(plan=PLAN, steps=3600, batch=8, seed=11, log=print):
+def train(plan=PLAN, steps=8000, batch=8, seed=11, log=print):
     pf = _package()
     nets, grids, params = {}, {}, None
     exact = pf.SolverConfig(mode=pf.PF_SOLVER_LEARNED, rel_tol=1e-6, precond=pf.PF_PRECOND_EXACT_COARSE)
@@ -148,7 +150,7 @@ def train(plan=PLAN, steps=3600, batch=8, seed=11, log=print):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=DEFAULT_OUT)
-    ap.add_argument("--steps", type=int, default=3600)
+    ap.add_argument("--steps", type=int, default=8000)
     args = ap.parse_args()
     params = train(steps=args.steps)
     os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
