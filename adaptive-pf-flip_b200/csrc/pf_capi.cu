@@ -1,5 +1,6 @@
 // pf_capi.cu -- the extern "C" entry points of libpfgpu (include/pfgpu.h):
 // context set-up, particle exchange, grid access and the solver-step calls.
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -82,6 +83,10 @@ int create_impl(pf_ctx* ctx, const pf_grid_desc* d) {
   g.nx = d->nx; g.ny = d->ny; g.nz = d->nz;
   g.dx = d->dx; g.ox = d->ox; g.oy = d->oy; g.oz = d->oz;
   g.inv_dx = 1.0 / d->dx;
+  {
+    int e = 0;
+    g.dx_pow2 = std::frexp(d->dx, &e) == 0.5 ? 1 : 0;
+  }
   g.TX = (d->nx + 1 + 7) / 8; g.TY = (d->ny + 1 + 7) / 8; g.TZ = (d->nz + 1 + 7) / 8;
   g.ntiles = g.TX * g.TY * g.TZ;
   const int dims[PF_NFIELDS][3] = {{g.nx + 1, g.ny, g.nz}, {g.nx, g.ny + 1, g.nz}, {g.nx, g.ny, g.nz + 1},
@@ -245,6 +250,7 @@ static int upload_impl(pf_ctx* ctx, size_t n, const void* pos, const void* vel, 
   if (n > ctx->cap) return set_error(ctx, PF_ERR_CAPACITY, "more particles than max_particles");
   cudaSetDevice(ctx->device);
   ctx->np = n;
+  ctx->bins_valid = false;
   if (n == 0) return PF_OK;
   const size_t es = f64 ? sizeof(double) : sizeof(float);
   const int nb = nblocks(n, 256);

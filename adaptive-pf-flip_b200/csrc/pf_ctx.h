@@ -31,6 +31,7 @@ struct pf_ctx {
   std::vector<int> wall_tiles;  // tiles written by markCells walls / applyWallBoundary
   int* d_wall_tiles = nullptr;
   bool saved_valid = false;
+  bool bins_valid = false;  // tile_start/perm bin the current particle positions (set by P2G)
 
   // ---- particles (SoA FP32) ----
   size_t cap = 0, np = 0;

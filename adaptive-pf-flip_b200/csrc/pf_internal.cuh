@@ -32,6 +32,7 @@ struct Geom {
   int ntiles;
   double dx, ox, oy, oz;
   double inv_dx;            // 1/dx, for coordinates that need not round as the reference's
+  int dx_pow2;              // dx is a power of two: (p - o) / dx == (p - o) * inv_dx exactly
   int fdim[PF_NFIELDS][3];  // node lattice per field
   int bdim[PF_NFIELDS][3];  // 4^3 block lattice per field
 };

@@ -13,6 +13,7 @@
 //
 // It runs the same kernels as pf_project in PLAIN mode (the launchers in
 // pf_project.cu and pf_pcg.cu), on a pool in which every tile is active.
+#include <cmath>
 #include <cstring>
 #include <mutex>
 
@@ -78,6 +79,10 @@ Geom make_geom(int nx, int ny, int nz, double dx) {
   Geom g{};
   g.nx = nx; g.ny = ny; g.nz = nz;
   g.dx = dx; g.inv_dx = 1.0 / dx;
+  {
+    int e = 0;
+    g.dx_pow2 = std::frexp(dx, &e) == 0.5 ? 1 : 0;
+  }
   g.TX = (nx + 1 + 7) / 8; g.TY = (ny + 1 + 7) / 8; g.TZ = (nz + 1 + 7) / 8;
   g.ntiles = g.TX * g.TY * g.TZ;
   const int dims[PF_NFIELDS][3] = {{nx + 1, ny, nz}, {nx, ny + 1, nz}, {nx, ny, nz + 1}, {nx + 1, ny, nz},

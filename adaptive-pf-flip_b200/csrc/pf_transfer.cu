@@ -510,6 +510,79 @@ __global__ void __launch_bounds__(256) k_g2p(DevGrid G, DevGrid S, ParticlePtrs 
   }
 }
 
+// G2P over the P2G bins (particles have not moved since the binning): one
+// CTA per tile with particles stages the current and saved u, v, w of the
+// tile's nodes and a one-node halo -- 10^3 nodes per field, node indices
+// clamped to the field lattice exactly as sample2 clamps them -- in shared
+// memory, then samples its particles from there.  A particle whose stencil
+// leaves the box (a position outside the domain) takes sample2.
+constexpr int kG2PBox = 10;
+constexpr int kG2PBox3 = kG2PBox * kG2PBox * kG2PBox;
+
+__global__ void __launch_bounds__(256) k_g2p_tiles(DevGrid G, const int* __restrict__ cell_start,
+                                                   const int* __restrict__ perm, ParticlePtrs P, double aL,
+                                                   double aG) {
+  __shared__ float2 box[3][kG2PBox3];  // (current, saved)
+  const int t = blockIdx.x;
+  const int beg = cell_start[(size_t)t * PF_TV], end = cell_start[(size_t)(t + 1) * PF_TV];
+  if (beg >= end) return;
+  const int tx = t % G.g.TX, tq = t / G.g.TX, ty = tq % G.g.TY, tz = tq / G.g.TY;
+  const int b0 = tx * 8 - 1, b1 = ty * 8 - 1, b2 = tz * 8 - 1;
+  for (int e = threadIdx.x; e < 3 * kG2PBox3; e += blockDim.x) {
+    const int a = e / kG2PBox3, s = e - a * kG2PBox3;
+    const int fv = PF_U + a;
+    const int i = min(max(b0 + s % kG2PBox, 0), G.g.fdim[fv][0] - 1);
+    const int j = min(max(b1 + (s / kG2PBox) % kG2PBox, 0), G.g.fdim[fv][1] - 1);
+    const int k = min(max(b2 + s / (kG2PBox * kG2PBox), 0), G.g.fdim[fv][2] - 1);
+    const int sl = slot_of(G, i, j, k);
+    float2 v = make_float2(0.0f, 0.0f);
+    if (sl >= 0) {
+      const size_t o = (size_t)sl * PF_TV + local_id(i, j, k);
+      v = make_float2(G.fld[fv][o], G.saved[a][o]);
+    }
+    box[a][s] = v;
+  }
+  __syncthreads();
+  float* vp[3] = {P.vx, P.vy, P.vz};
+  for (int q = beg + threadIdx.x; q < end; q += blockDim.x) {
+    const int p = perm[q];
+    const double gx = to_grid((double)P.px[p], G.g.ox, G.g.inv_dx);
+    const double gy = to_grid((double)P.py[p], G.g.oy, G.g.inv_dx);
+    const double gz = to_grid((double)P.pz[p], G.g.oz, G.g.inv_dx);
+    const double c[3][3] = {{gx, gy - 0.5, gz - 0.5}, {gx - 0.5, gy, gz - 0.5}, {gx - 0.5, gy - 0.5, gz}};
+    const float al = P.type[p] == 0 ? (float)aL : (float)aG;
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+      const int i0 = (int)floor(c[ax][0]), j0 = (int)floor(c[ax][1]), k0 = (int)floor(c[ax][2]);
+      const int li = i0 - b0, lj = j0 - b1, lk = k0 - b2;
+      float cur, old;
+      if (li >= 0 && lj >= 0 && lk >= 0 && li < kG2PBox - 1 && lj < kG2PBox - 1 && lk < kG2PBox - 1) {
+        const float fx = (float)(c[ax][0] - i0), fy = (float)(c[ax][1] - j0), fz = (float)(c[ax][2] - k0);
+        const float wx[2] = {1.0f - fx, fx}, wy[2] = {1.0f - fy, fy}, wz[2] = {1.0f - fz, fz};
+        const float2* bp = &box[ax][li + kG2PBox * (lj + kG2PBox * lk)];
+        float s = 0.0f, so = 0.0f;
+#pragma unroll
+        for (int dk = 0; dk < 2; ++dk)
+#pragma unroll
+          for (int dj = 0; dj < 2; ++dj)
+#pragma unroll
+            for (int di = 0; di < 2; ++di) {
+              const float w = wx[di] * wy[dj] * wz[dk];
+              const float2 v = bp[di + kG2PBox * (dj + kG2PBox * dk)];
+              s += w * v.x;
+              so += w * v.y;
+            }
+        cur = s;
+        old = so;
+      } else {
+        sample2<true>(G, ax, c[ax][0], c[ax][1], c[ax][2], cur, old);
+      }
+      const float v = vp[ax][p];
+      vp[ax][p] = (v + (cur - old)) * al + cur * (1.0f - al);
+    }
+  }
+}
+
 __device__ __forceinline__ void warp_count(int* counters, int idx, bool flag) {
   const unsigned m = __ballot_sync(__activemask(), flag);
   if (m && (threadIdx.x & 31) == (__ffs(__activemask()) - 1)) atomicAdd(&counters[idx], __popc(m));
@@ -683,6 +756,7 @@ int mark_cells(pf_ctx* ctx) {
 static int p2g_core(pf_ctx* ctx, const pf_phase* ph, double Vp) {
   const int n = (int)ctx->np;
   const int nt = ctx->g.ntiles;
+  ctx->bins_valid = false;
   for (int f = PF_U; f <= PF_MW; ++f) {
     int rc = field_clear(ctx, f);
     if (rc) return rc;
@@ -706,6 +780,7 @@ static int p2g_core(pf_ctx* ctx, const pf_phase* ph, double Vp) {
     if (rc) return rc;
     (++ctx->launches), k_bin_scatter<<<nblocks(n, 256), 256, 0, ctx->stream>>>(ctx->pkey, ctx->prank, ctx->tile_start, ctx->perm, n);
     PF_CUDA_TRY(cudaGetLastError());
+    ctx->bins_valid = true;
   }
   {
     StageScope sc(ctx, PF_STAGE_SPLAT);
@@ -771,7 +846,11 @@ int g2p(pf_ctx* ctx, const pf_ctx* saved, double aL, double aG) {
     (++ctx->launches), k_g2p<true><<<nblocks(n, 256), 256, 0, ctx->stream>>>(G, S, particle_ptrs(ctx), n, aL, aG);
   } else {
     if (!ctx->saved_valid) return set_error(ctx, PF_ERR_INVALID, "g2p: no saved velocity (call pf_save_velocity)");
-    (++ctx->launches), k_g2p<false><<<nblocks(n, 256), 256, 0, ctx->stream>>>(G, G, particle_ptrs(ctx), n, aL, aG);
+    if (ctx->bins_valid)
+      (++ctx->launches), k_g2p_tiles<<<ctx->g.ntiles, 256, 0, ctx->stream>>>(G, ctx->tile_start, ctx->perm,
+                                                                               particle_ptrs(ctx), aL, aG);
+    else
+      (++ctx->launches), k_g2p<false><<<nblocks(n, 256), 256, 0, ctx->stream>>>(G, G, particle_ptrs(ctx), n, aL, aG);
   }
   PF_CUDA_TRY(cudaGetLastError());
   return PF_OK;
@@ -791,6 +870,7 @@ static int read_clamp(pf_ctx* ctx, pf_clamp_stats* st) {
 int advect(pf_ctx* ctx, double dt, int order, pf_clamp_stats* st, double* esc, size_t* nesc) {
   StageScope stage(ctx, PF_STAGE_G2P);
   const int n = (int)ctx->np;
+  ctx->bins_valid = false;  // particles move
   PF_CUDA_TRY(cudaMemsetAsync(ctx->d_clamp, 0, 8 * sizeof(int), ctx->stream));
   if (n > 0) {
     (++ctx->launches), k_advect<<<nblocks(n, 256), 256, 0, ctx->stream>>>(dev_grid(ctx), particle_ptrs(ctx), n, dt, order,
@@ -829,6 +909,7 @@ int advect(pf_ctx* ctx, double dt, int order, pf_clamp_stats* st, double* esc, s
 int g2p_advect(pf_ctx* ctx, double aL, double aG, double dt, int order, pf_clamp_stats* st) {
   StageScope stage(ctx, PF_STAGE_G2P);
   const int n = (int)ctx->np;
+  ctx->bins_valid = false;  // particles move
   PF_CUDA_TRY(cudaMemsetAsync(ctx->d_clamp, 0, 8 * sizeof(int), ctx->stream));
   if (n > 0) {
     (++ctx->launches), k_advect<<<nblocks(n, 256), 256, 0, ctx->stream>>>(dev_grid(ctx), particle_ptrs(ctx), n, dt, order,

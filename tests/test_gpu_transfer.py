@@ -154,6 +154,51 @@ def test_mark_cells_matches_oracle(pf):
     assert np.array_equal(sim.grid.fluid_cells(), go.fluid_cells())
 
 
+@pytest.mark.parametrize("n", [16, 24])
+def test_g2p_over_p2g_bins_matches_oracle(pf, n):
+    """G2P right after P2G on one context (the transfer step: pf_p2g,
+    pf_save_velocity, pf_g2p) samples shared-memory tiles over the P2G bins.
+    It must match the oracle, and the per-particle kernel (taken once an
+    upload invalidates the bins) bit for bit.  Particles in the boundary
+    cells exercise the clamped nodes, one outside the domain the fallback."""
+    import ctypes as C
+    sc = pf.scenes.bubble_tank(n, seed=5)
+    pp = phase_for(sc, pf)
+    ps = scene_particles(sc)
+    dx = 1.0 / n
+    for pos in ((0.3 * dx, 0.3 * dx, 0.5), (0.5, 0.2 * dx, 1.0 - 0.3 * dx), (1.0 - 0.1 * dx, 0.4, 0.6),
+                (-1.6 * dx, 0.3, 0.4)):
+        ps.add(pos, (0.1, -0.2, 0.3), 0)
+    lib = pf.load()
+    g = pf.SparseMacGrid3D(n, n, n, dx, max_particles=len(ps))
+    g.upload(ps)
+    ph = pp._c()
+    pf._lib.check(lib.pf_p2g(g.ctx, C.byref(ph), 1.0), g.ctx, "pf_p2g")
+    pf._lib.check(lib.pf_save_velocity(g.ctx), g.ctx, "pf_save_velocity")
+    o = O.Oracle()
+    go = O.OracleGrid(n, n, n, dx)
+    so = O.OracleGrid(n, n, n, dx)
+    for f in range(8):
+        so.set_field(f, *g.get_field(f))
+    for f in (pf.PF_U, pf.PF_V, pf.PF_W):  # perturb the live grid so FLIP and PIC differ
+        d, a = g.get_field(f)
+        rng = np.random.default_rng(f + 7)
+        g.set_field(f, (d + rng.normal(0, 0.05, d.shape).astype(np.float32) * (d != 0)).astype(np.float32), a)
+    for f in range(8):
+        go.set_field(f, *g.get_field(f))
+    pf._lib.check(lib.pf_g2p(g.ctx, None, 0.97, 0.9), g.ctx, "pf_g2p")
+    ps_tiles = ps.copy()
+    g.download(ps_tiles, pos=False, vel=True)
+    g.upload(ps)  # invalidates the bins: the per-particle kernel
+    pf._lib.check(lib.pf_g2p(g.ctx, None, 0.97, 0.9), g.ctx, "pf_g2p")
+    ps_flat = ps.copy()
+    g.download(ps_flat, pos=False, vel=True)
+    ps_o = ps.copy()
+    o.g2p(go, ps_o, so, 0.97, 0.9)
+    assert np.array_equal(ps_tiles.vel, ps_flat.vel)
+    assert rel_err(ps_tiles.vel, ps_o.vel) < TOL
+
+
 def test_g2p_and_advect_match_oracle(pf):
     n = 16
     sc = pf.scenes.bubble_tank(n, seed=11)
