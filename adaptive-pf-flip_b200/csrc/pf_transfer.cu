@@ -226,11 +226,25 @@ __device__ __forceinline__ void splat_cell(const DevGrid& G, float* sm, int cl, 
   float am[NW], ap[NW];
 #pragma unroll
   for (int k = 0; k < NW; ++k) { am[k] = 0.0f; ap[k] = 0.0f; }
+  // the next particle's attributes are loaded while this one is splatted
+  int pn = perm[beg];
+  float xn = px[pn], yn = py[pn], zn = pz[pn], vn = vA[pn], voln = vol[pn];
+  uint8_t tn = type[pn];
   for (int q = beg; q < end; ++q) {
-    const int p = perm[q];
-    float gx = (float)(((double)px[p] - G.g.ox) * inv_dx - o0);
-    float gy = (float)(((double)py[p] - G.g.oy) * inv_dx - o1);
-    float gz = (float)(((double)pz[p] - G.g.oz) * inv_dx - o2);
+    const float X = xn, Y = yn, Z = zn, VA = vn, VOL = voln;
+    const uint8_t TY = tn;
+    if (q + 1 < end) {
+      pn = perm[q + 1];
+      xn = px[pn];
+      yn = py[pn];
+      zn = pz[pn];
+      vn = vA[pn];
+      voln = vol[pn];
+      tn = type[pn];
+    }
+    float gx = (float)(((double)X - G.g.ox) * inv_dx - o0);
+    float gy = (float)(((double)Y - G.g.oy) * inv_dx - o1);
+    float gz = (float)(((double)Z - G.g.oz) * inv_dx - o2);
     if (A != 0) gx -= 0.5f;
     if (A != 1) gy -= 0.5f;
     if (A != 2) gz -= 0.5f;
@@ -254,9 +268,9 @@ __device__ __forceinline__ void splat_cell(const DevGrid& G, float* sm, int cl, 
           wsum += v;
         }
     if (!(wsum > 0.0f)) continue;
-    const float mp = (type[p] == 0 ? m_l : m_g) * vol[p];
+    const float mp = (TY == 0 ? m_l : m_g) * VOL;
     const float sm_ = mp / wsum;
-    const float sp_ = sm_ * vA[p];
+    const float sp_ = sm_ * VA;
 #pragma unroll
     for (int e = 0; e < NW; ++e) {
       am[e] = fmaf(w[e], sm_, am[e]);

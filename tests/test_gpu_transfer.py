@@ -136,6 +136,39 @@ def test_p2g_fields_and_active_sets_match_oracle(pf, scene, n):
         assert err < TOL, f"{name}: relative error {err}"
 
 
+@pytest.mark.parametrize("n", [16, 24])
+def test_activation_on_threshold_particles_matches_oracle(pf, n):
+    """Particles on half- and quarter-integer grid coordinates put window
+    nodes at |d| = 1.5 and block minima at d^2 sums of exactly 2.25, where
+    the FP32 block test hands over to the reference's FP64 test.  The 4^3
+    activity sets must still be the reference's bit for bit, for a
+    power-of-two dx (16) and one that is not (24).  Field values: the masses
+    to the usual tolerance; velocities u = P/m where m is not vanishing -- a
+    node reached only at |d| = 1.5 +- 1e-7 gets m ~ 1e-21 from FP32 weights
+    and 0 from FP64 ones, and P/m there is a 0/0 limit."""
+    rng = np.random.default_rng(n)
+    k = rng.integers(2, 4 * n - 2, size=(600, 3))  # quarter-cell lattice
+    pos = (k.astype(np.float64) / (4 * n)).astype(np.float32).astype(np.float64)
+    ps = O.Particles(pos, rng.normal(0, 0.1, pos.shape), (rng.random(len(pos)) < 0.3).astype(np.uint8),
+                     np.ones(len(pos)))
+    pp = pf.PhaseParams(1000.0, 1.0, 1.0, 1.0)
+    pp.rho_tilde_0 = pf.calibrateRhoTilde0(pp, 1.0)
+    g = pf.SparseMacGrid3D(n, n, n, 1.0 / n, max_particles=len(ps))
+    pf.spP2G3D_tp(g, ps, pp, 1.0)
+    o = O.Oracle()
+    go = O.OracleGrid(n, n, n, 1.0 / n)
+    o.p2g(go, ps, to_oracle_phase(pp), 1.0)
+    res = compare_grids(g, go, range(6))
+    for name, (err, nact) in res.items():
+        assert nact == 0, f"{name}: {nact} 4^3 activity flags differ"
+    for f in (pf.PF_MU, pf.PF_MV, pf.PF_MW):
+        assert rel_err(g.get_field(f)[0], go.get_field(f)[0]) < TOL
+    for f, fm in ((pf.PF_U, pf.PF_MU), (pf.PF_V, pf.PF_MV), (pf.PF_W, pf.PF_MW)):
+        m = go.get_field(fm)[0]
+        sel = m > 1e-6 * m.max()
+        assert rel_err(g.get_field(f)[0][sel], go.get_field(f)[0][sel]) < TOL
+
+
 def test_mark_cells_matches_oracle(pf):
     n = 16
     sc = pf.scenes.bubble_tank(n, seed=2)
