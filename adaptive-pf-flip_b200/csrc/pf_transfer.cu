@@ -32,102 +32,62 @@ __device__ __forceinline__ double grid_coord(float p, double o, double dx) {
   return __ddiv_rn(__dsub_rn((double)p, o), dx);
 }
 
-// ---------------------------------------------------------------------------
-// exact FP64 activation of the 4^3 blocks a particle's kernel window touches
-// (preactivateKernel, sparse_ops3d_tp.cpp:23-40).  Along each axis only nodes
-// i0-1..i0+2 can have |d| < 1.5; per 4-node block the closest node gives the
-// smallest rounded d^2, and rounding is monotone, so testing the per-axis
-// minima decides "some node of this block has w > 0" exactly.
-// ---------------------------------------------------------------------------
-// Per axis: the (at most two) 4-node blocks holding the in-lattice candidates
-// i0-1..i0+2 and, for each, the smallest rounded d^2 = fl((c - i)^2).
-struct AxisBlocks {
-  int b0, nb;
-  double m0, m1;
-};
-
-__device__ __forceinline__ AxisBlocks axis_blocks(double c, int dim) {
-  const int i0 = (int)floor(c);
-  const int lo = max(i0 - 1, 0), hi = min(i0 + 2, dim - 1);
-  AxisBlocks r;
-  r.b0 = lo >> 2;
-  r.nb = lo > hi ? 0 : (hi >> 2) - (lo >> 2) + 1;
-  r.m0 = r.m1 = 1e300;
-#pragma unroll
-  for (int o = 0; o < 4; ++o) {
-    const int i = i0 - 1 + o;
-    const double d = __dsub_rn(c, (double)i);
-    const double dd = __dmul_rn(d, d);
-    if (i >= lo && i <= hi) {
-      if ((i >> 2) == r.b0) r.m0 = fmin(r.m0, dd);
-      else r.m1 = fmin(r.m1, dd);
-    }
-  }
-  return r;
+// The same double; for a power-of-two dx the product with 1/dx is exact.
+__device__ __forceinline__ double grid_coord_g(const Geom& g, float p, double o) {
+  const double d = __dsub_rn((double)p, o);
+  return g.dx_pow2 ? __dmul_rn(d, g.inv_dx) : __ddiv_rn(d, g.dx);
 }
 
-__device__ __forceinline__ void activate_window(const DevGrid& G, int fv, double c0, double c1, double c2,
-                                                uint8_t* need) {
-  const AxisBlocks ax = axis_blocks(c0, G.g.fdim[fv][0]);
-  const AxisBlocks ay = axis_blocks(c1, G.g.fdim[fv][1]);
-  const AxisBlocks az = axis_blocks(c2, G.g.fdim[fv][2]);
-  const int fm = fv + 3;
-#pragma unroll
-  for (int z = 0; z < 2; ++z) {
-    if (z >= az.nb) continue;
-#pragma unroll
-    for (int y = 0; y < 2; ++y) {
-      if (y >= ay.nb) continue;
-#pragma unroll
-      for (int x = 0; x < 2; ++x) {
-        if (x >= ax.nb) continue;
-        // kern(d2) > 0  <=>  fl(d2 / 2.25) < 1  <=>  d2 < 2.25 (the quotient of
-        // the largest double below 2.25 still rounds below 1)
-        const double d2 = __dadd_rn(__dadd_rn(x ? ax.m1 : ax.m0, y ? ay.m1 : ay.m0), z ? az.m1 : az.m0);
-        if (!(d2 < kR2)) continue;
-        const int bx = ax.b0 + x, by = ay.b0 + y, bz = az.b0 + z;
-        const int bi = bx + G.g.bdim[fv][0] * (by + G.g.bdim[fv][1] * bz);
-        if (!G.act4[fv][bi]) G.act4[fv][bi] = 1;
-        if (!G.act4[fm][bi]) G.act4[fm][bi] = 1;
-        uint8_t* nd = &need[tile_id(G.g, bx >> 1, by >> 1, bz >> 1)];
-        if (!*nd) *nd = 1;
-      }
-    }
-  }
-}
-
-// One pass over the particles: tile key + warp-aggregated rank (binning),
-// the tile of the particle's cell (pooled for markCells), and the exact
-// activation of u/v/w and their mass fields.
-__global__ void __launch_bounds__(256) k_bin_activate(DevGrid G, const float* __restrict__ px,
-                                                      const float* __restrict__ py,
-                                                      const float* __restrict__ pz, int n,
-                                                      int* tile_count, int* pkey, int* prank,
-                                                      uint8_t* need, int do_bin, int do_act) {
+// ---------------------------------------------------------------------------
+// Binning.  One pass over the particles: the particle's cell (the reference's
+// FP64 (pos - o) / dx, floored and clamped) as a bin key tile * 512 + local
+// cell with a warp-aggregated rank, and a request for the tile of the cell.
+// The 4^3 activation is decided later, in the splat (reach bits below); the
+// pool takes the one-tile dilation of the requested tiles, which holds every
+// node a particle's window can reach (within two nodes of its cell).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_bin(DevGrid G, const float* __restrict__ px, const float* __restrict__ py,
+                                             const float* __restrict__ pz, int n, int* tile_count, int* pkey,
+                                             int* prank, uint8_t* need, int do_bin) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   const unsigned active = __ballot_sync(0xffffffffu, p < n);
   if (p >= n) return;
-  const double gx = grid_coord(px[p], G.g.ox, G.g.dx);
-  const double gy = grid_coord(py[p], G.g.oy, G.g.dx);
-  const double gz = grid_coord(pz[p], G.g.oz, G.g.dx);
-  int ci = (int)floor(gx), cj = (int)floor(gy), ck = (int)floor(gz);
-  ci = min(max(ci, 0), G.g.nx - 1);
-  cj = min(max(cj, 0), G.g.ny - 1);
-  ck = min(max(ck, 0), G.g.nz - 1);
+  const int ci = min(max((int)floor(grid_coord_g(G.g, px[p], G.g.ox)), 0), G.g.nx - 1);
+  const int cj = min(max((int)floor(grid_coord_g(G.g, py[p], G.g.oy)), 0), G.g.ny - 1);
+  const int ck = min(max((int)floor(grid_coord_g(G.g, pz[p], G.g.oz)), 0), G.g.nz - 1);
   const int t = tile_id(G.g, ci >> 3, cj >> 3, ck >> 3);
+  // the lanes of one cell share one counter increment and one tile request
+  const int key = t * PF_TV + local_id(ci, cj, ck);
+  const unsigned peers = __match_any_sync(active, key);
+  const int lane = threadIdx.x & 31, leader = __ffs(peers) - 1;
   if (do_bin) {
-    // bin = the particle's cell in tile-major order (tile * 512 + local cell)
-    const int key = t * PF_TV + local_id(ci, cj, ck);
-    const int r = warp_agg_inc(tile_count, key, active);
+    int base = 0;
+    if (lane == leader) base = atomicAdd(&tile_count[key], __popc(peers));
+    base = __shfl_sync(peers, base, leader);
     pkey[p] = key;
-    prank[p] = r;
+    prank[p] = base + __popc(peers & ((1u << lane) - 1u));
   }
-  if (!need[t]) need[t] = 1;
-  if (do_act) {
-    activate_window(G, PF_U, gx, __dsub_rn(gy, 0.5), __dsub_rn(gz, 0.5), need);
-    activate_window(G, PF_V, __dsub_rn(gx, 0.5), gy, __dsub_rn(gz, 0.5), need);
-    activate_window(G, PF_W, __dsub_rn(gx, 0.5), __dsub_rn(gy, 0.5), gz, need);
-  }
+  if (lane == leader && !need[t]) need[t] = 1;
+}
+
+// need <- the one-tile dilation of need (through the int scratch `tmp`)
+__global__ void k_need_snapshot(const uint8_t* need, int* tmp, int n) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) tmp[t] = need[t];
+}
+
+__global__ void k_need_dilate(Geom g, const int* tmp, uint8_t* need) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.ntiles) return;
+  const int tx = t % g.TX, q = t / g.TX, ty = q % g.TY, tz = q / g.TY;
+  int any = 0;
+  for (int dz = -1; dz <= 1; ++dz)
+    for (int dy = -1; dy <= 1; ++dy)
+      for (int dx = -1; dx <= 1; ++dx) {
+        const int x = tx + dx, y = ty + dy, z = tz + dz;
+        if (x >= 0 && y >= 0 && z >= 0 && x < g.TX && y < g.TY && z < g.TZ) any |= tmp[tile_id(g, x, y, z)];
+      }
+  if (any) need[t] = 1;
 }
 
 __global__ void k_bin_scatter(const int* __restrict__ pkey, const int* __restrict__ prank,
@@ -193,7 +153,18 @@ __global__ void k_mark_particles(DevGrid G, const float* __restrict__ px, const 
 // receive weight 0 -- and adds the window into the tile's shared box once:
 // 72 shared atomics per cell and field instead of 54 per particle, and in each
 // atomic instruction the lanes (neighbouring cells) address distinct nodes.
+//
+// The same pass decides the 4^3 activation (preactivateKernel,
+// sparse_ops3d_tp.cpp:23-40: the block of every node with w > 0, i.e.
+// fl(fl(dx^2 + dy^2) + dz^2) < 2.25 in FP64).  A window spans at most two
+// blocks per axis; a block is reached iff the sum of the per-axis minima of
+// d^2 over its window nodes is below 2.25.  The FP32 minima (the weights'
+// d^2/r^2, absolute error below 1e-5) decide every block clear of the
+// threshold by kReachEps; a particle with a block inside the band redoes the
+// field's blocks in the reference's FP64 arithmetic.  Reached blocks are
+// OR-ed per cell, then per tile, and each tile CTA writes its blocks' bytes.
 constexpr int kSplatThreads = 256;
+constexpr float kReachEps = 2e-5f;
 
 __device__ __forceinline__ float cubic(float s) {
   const float t = 1.0f - s;
@@ -201,14 +172,51 @@ __device__ __forceinline__ float cubic(float s) {
 }
 
 // d^2/r^2 of node `node` for coordinate g (both box-local), 2 (weight 0, out
-// of the weight sum) when the node is off the field's lattice [lo, hi).
+// of the weight sum, never reached) when the node is off the field's lattice
+// [lo, hi).
 __device__ __forceinline__ float node_a(float g, int node, int lo, int hi) {
   const float d = g - (float)node;
   return (node >= lo && node < hi) ? d * d * (1.0f / 2.25f) : 2.0f;
 }
 
+// The FP64 decision for one particle and field: bit x + 2y + 4z for window
+// block (x, y, z), where window block 0 along an axis holds the window nodes
+// before the split s of that axis.  n[] are the global first window nodes.
 template <int A>
-__device__ __forceinline__ void splat_cell(const DevGrid& G, float* sm, int cl, int beg, int end,
+__device__ unsigned exact_reach(const DevGrid& G, float ppx, float ppy, float ppz, const int* n, const int* sp) {
+  constexpr int NX = A == 0 ? 4 : 3, NY = A == 1 ? 4 : 3, NZ = A == 2 ? 4 : 3;
+  const int cnt[3] = {NX, NY, NZ};
+  const int fv = PF_U + A;
+  const double g[3] = {grid_coord(ppx, G.g.ox, G.g.dx), grid_coord(ppy, G.g.oy, G.g.dx),
+                       grid_coord(ppz, G.g.oz, G.g.dx)};
+  double m[3][2];
+#pragma unroll
+  for (int ax = 0; ax < 3; ++ax) {
+    const double c = ax == A ? g[ax] : __dsub_rn(g[ax], 0.5);
+    m[ax][0] = m[ax][1] = 1e300;
+    for (int i = 0; i < cnt[ax]; ++i) {
+      const int node = n[ax] + i;
+      if (node < 0 || node >= G.g.fdim[fv][ax]) continue;
+      const double d = __dsub_rn(c, (double)node);
+      const double dd = __dmul_rn(d, d);
+      if (i < sp[ax]) m[ax][0] = fmin(m[ax][0], dd);
+      else m[ax][1] = fmin(m[ax][1], dd);
+    }
+  }
+  unsigned r = 0u;
+#pragma unroll
+  for (int z = 0; z < 2; ++z)
+#pragma unroll
+    for (int y = 0; y < 2; ++y)
+#pragma unroll
+      for (int x = 0; x < 2; ++x)
+        if (__dadd_rn(__dadd_rn(m[0][x], m[1][y]), m[2][z]) < kR2) r |= 1u << (x + 2 * y + 4 * z);
+  return r;
+}
+
+// Returns the cell's reached blocks as bits of the tile's 4x4x4 block box.
+template <int A>
+__device__ __forceinline__ unsigned long long splat_cell(const DevGrid& G, float* sm, int cl, int beg, int end,
                                            const int* __restrict__ perm, const float* __restrict__ px,
                                            const float* __restrict__ py, const float* __restrict__ pz,
                                            const float* __restrict__ vA, const uint8_t* __restrict__ type,
@@ -223,9 +231,13 @@ __device__ __forceinline__ void splat_cell(const DevGrid& G, float* sm, int cl, 
   const int lox = -o0, hix = G.g.fdim[fv][0] - o0;
   const int loy = -o1, hiy = G.g.fdim[fv][1] - o1;
   const int loz = -o2, hiz = G.g.fdim[fv][2] - o2;
+  // global first window node per axis and the split between its two blocks
+  const int n[3] = {o0 + bx, o1 + by, o2 + bz};
+  const int sp[3] = {min(4 - (n[0] & 3), NX), min(4 - (n[1] & 3), NY), min(4 - (n[2] & 3), NZ)};
   float am[NW], ap[NW];
 #pragma unroll
   for (int k = 0; k < NW; ++k) { am[k] = 0.0f; ap[k] = 0.0f; }
+  unsigned reach = 0u;
   // the next particle's attributes are loaded while this one is splatted
   int pn = perm[beg];
   float xn = px[pn], yn = py[pn], zn = pz[pn], vn = vA[pn], voln = vol[pn];
@@ -255,6 +267,36 @@ __device__ __forceinline__ void splat_cell(const DevGrid& G, float* sm, int cl, 
     for (int j = 0; j < NY; ++j) ay[j] = node_a(gy, by + j, loy, hiy);
 #pragma unroll
     for (int k = 0; k < NZ; ++k) az[k] = node_a(gz, bz + k, loz, hiz);
+    // activation: per-axis minima over each window block
+    float mx0 = 4.0f, mx1 = 4.0f, my0 = 4.0f, my1 = 4.0f, mz0 = 4.0f, mz1 = 4.0f;
+#pragma unroll
+    for (int i = 0; i < NX; ++i) {
+      if (i < sp[0]) mx0 = fminf(mx0, ax[i]);
+      else mx1 = fminf(mx1, ax[i]);
+    }
+#pragma unroll
+    for (int j = 0; j < NY; ++j) {
+      if (j < sp[1]) my0 = fminf(my0, ay[j]);
+      else my1 = fminf(my1, ay[j]);
+    }
+#pragma unroll
+    for (int k = 0; k < NZ; ++k) {
+      if (k < sp[2]) mz0 = fminf(mz0, az[k]);
+      else mz1 = fminf(mz1, az[k]);
+    }
+    bool band = false;
+#pragma unroll
+    for (int z = 0; z < 2; ++z)
+#pragma unroll
+      for (int y = 0; y < 2; ++y)
+#pragma unroll
+        for (int x = 0; x < 2; ++x) {
+          const float sa = ((x ? mx1 : mx0) + (y ? my1 : my0)) + (z ? mz1 : mz0);
+          if (sa < 1.0f - kReachEps) reach |= 1u << (x + 2 * y + 4 * z);
+          band = band || fabsf(sa - 1.0f) <= kReachEps;
+        }
+    if (band) reach |= exact_reach<A>(G, X, Y, Z, n, sp);
+    // weights
     float w[NW];
     float wsum = 0.0f;
 #pragma unroll
@@ -292,6 +334,13 @@ __device__ __forceinline__ void splat_cell(const DevGrid& G, float* sm, int cl, 
           atomicAdd(&smas[si], am[e]);
         }
       }
+  // reached window blocks -> the tile's 4x4x4 block box (block of node o -> (o >> 2) - (o0 >> 2))
+  const int w0 = (n[0] >> 2) - (o0 >> 2), w1 = (n[1] >> 2) - (o1 >> 2), w2 = (n[2] >> 2) - (o2 >> 2);
+  unsigned long long box = 0ull;
+#pragma unroll
+  for (int b = 0; b < 8; ++b)
+    if ((reach >> b) & 1u) box |= 1ull << ((w0 + (b & 1)) + 4 * ((w1 + ((b >> 1) & 1)) + 4 * (w2 + (b >> 2))));
+  return box;
 }
 
 __global__ void __launch_bounds__(kSplatThreads, 2) k_splat(DevGrid G, const int* __restrict__ cell_start,
@@ -305,23 +354,48 @@ __global__ void __launch_bounds__(kSplatThreads, 2) k_splat(DevGrid G, const int
                                                          const uint8_t* __restrict__ type,
                                                          const float* __restrict__ vol, float m_l, float m_g) {
   extern __shared__ float sm[];  // [3 axes][mom, mass][kBox3]
+  __shared__ unsigned sblk[6];   // [3 axes][64 reached blocks of the box]
   const int t = blockIdx.x;
   const int* cs = cell_start + (size_t)t * PF_TV;
   if (cs[0] >= cs[PF_TV]) return;
   for (int e = threadIdx.x; e < 6 * kBox3; e += kSplatThreads) sm[e] = 0.0f;
+  if (threadIdx.x < 6) sblk[threadIdx.x] = 0u;
   __syncthreads();
   const int tx = t % G.g.TX, tq = t / G.g.TX, ty = tq % G.g.TY, tz = tq / G.g.TY;
   const int o0 = tx * 8 - 2, o1 = ty * 8 - 2, o2 = tz * 8 - 2;
   const double inv_dx = G.g.inv_dx;
+  unsigned long long box[3] = {0ull, 0ull, 0ull};  // reached blocks of this thread's cells
   for (int cl = threadIdx.x; cl < PF_TV; cl += kSplatThreads) {
     const int beg = cs[cl], end = cs[cl + 1];
     if (beg >= end) continue;
-    splat_cell<0>(G, sm, cl, beg, end, perm, px, py, pz, vx, type, vol, m_l, m_g, o0, o1, o2, inv_dx);
-    splat_cell<1>(G, sm, cl, beg, end, perm, px, py, pz, vy, type, vol, m_l, m_g, o0, o1, o2, inv_dx);
-    splat_cell<2>(G, sm, cl, beg, end, perm, px, py, pz, vz, type, vol, m_l, m_g, o0, o1, o2, inv_dx);
+    box[0] |= splat_cell<0>(G, sm, cl, beg, end, perm, px, py, pz, vx, type, vol, m_l, m_g, o0, o1, o2, inv_dx);
+    box[1] |= splat_cell<1>(G, sm, cl, beg, end, perm, px, py, pz, vy, type, vol, m_l, m_g, o0, o1, o2, inv_dx);
+    box[2] |= splat_cell<2>(G, sm, cl, beg, end, perm, px, py, pz, vz, type, vol, m_l, m_g, o0, o1, o2, inv_dx);
+  }
+  // one shared OR per warp and word
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const unsigned lo = __reduce_or_sync(0xffffffffu, (unsigned)box[a]);
+    const unsigned hi = __reduce_or_sync(0xffffffffu, (unsigned)(box[a] >> 32));
+    if ((threadIdx.x & 31) == 0) {
+      if (lo) atomicOr(&sblk[2 * a], lo);
+      if (hi) atomicOr(&sblk[2 * a + 1], hi);
+    }
   }
   __syncthreads();
-  // add the box into the pooled fields (neighbouring tiles overlap in halos)
+  // activity bytes of the reached blocks (a byte is stored only when it reads 0)
+  if (threadIdx.x < 3 * 64) {
+    const int a = threadIdx.x >> 6, idx = threadIdx.x & 63;
+    if ((sblk[2 * a + (idx >> 5)] >> (idx & 31)) & 1u) {
+      const int fv = PF_U + a;
+      const int gbx = (o0 >> 2) + (idx & 3), gby = (o1 >> 2) + ((idx >> 2) & 3), gbz = (o2 >> 2) + (idx >> 4);
+      const int bi = gbx + G.g.bdim[fv][0] * (gby + G.g.bdim[fv][1] * gbz);
+      if (!G.act4[fv][bi]) G.act4[fv][bi] = 1;
+      if (!G.act4[fv + 3][bi]) G.act4[fv + 3][bi] = 1;
+    }
+  }
+  // add the box into the pooled fields (neighbouring tiles overlap in halos);
+  // contributions in blocks that end up inactive are cleared by k_normalize
   for (int e = threadIdx.x; e < 3 * kBox3; e += kSplatThreads) {
     const int a = e / kBox3, si = e - a * kBox3;
     const float mom = sm[(2 * a) * kBox3 + si], mas = sm[(2 * a + 1) * kBox3 + si];
@@ -329,10 +403,6 @@ __global__ void __launch_bounds__(kSplatThreads, 2) k_splat(DevGrid G, const int
     const int X = si % kBox, Y = (si / kBox) % kBox, Z = si / (kBox * kBox);
     const int i = o0 + X, j = o1 + Y, k = o2 + Z;
     if (!in_field(G.g, PF_U + a, i, j, k)) continue;
-    // FP32 weights may be (negligibly) nonzero where the exact FP64 test left
-    // the block inactive; such contributions are dropped so inactive blocks
-    // stay zero.
-    if (!G.act4[PF_MU + a][act4_index(G.g, PF_MU + a, i, j, k)]) continue;
     const int sl = slot_of(G, i, j, k);
     if (sl < 0) continue;
     const size_t o = (size_t)sl * PF_TV + local_id(i, j, k);
@@ -344,13 +414,22 @@ __global__ void __launch_bounds__(kSplatThreads, 2) k_splat(DevGrid G, const int
 // normalisation u = P/m where m > 0 (sparse_ops3d_tp.cpp:126-152), with the
 // optional saved copy (step(): `saved = grid`) and gravity on v where mv > 0
 // (applyGravity) fused in.
+// Nodes of blocks the exact activation left inactive are cleared first: the
+// splat's FP32 weights may put a negligible contribution where the reference's
+// FP64 weight is zero, and inactive blocks stay zero.
 __global__ void k_normalize(DevGrid G, int nslots, int save, int gravity, float dv) {
   for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
     const size_t o = (size_t)s * PF_TV + threadIdx.x;
+    const int t = G.slot_tile[s];
+    const int tx = t % G.g.TX, tq = t / G.g.TX, ty = tq % G.g.TY, tz = tq / G.g.TY;
+    const int i = tx * 8 + (threadIdx.x & 7), j = ty * 8 + ((threadIdx.x >> 3) & 7), k = tz * 8 + (threadIdx.x >> 6);
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      const float m = G.fld[PF_MU + a][o];
-      float u = G.fld[PF_U + a][o];
+      const int f = PF_MU + a;
+      const bool act = in_field(G.g, f, i, j, k) && G.act4[f][act4_index(G.g, f, i, j, k)];
+      float m = act ? G.fld[f][o] : 0.0f;
+      float u = act ? G.fld[PF_U + a][o] : 0.0f;
+      if (!act) G.fld[f][o] = 0.0f;
       if (m > 0.0f) u = u / m;
       if (save) G.saved[a][o] = u;
       if (a == 1 && gravity && m > 0.0f) u = u + dv;
@@ -755,8 +834,8 @@ int mark_cells(pf_ctx* ctx) {
   rc = request_wall_tiles(ctx);
   if (rc) return rc;
   if (n > 0)
-    (++ctx->launches), k_bin_activate<<<nblocks(n, 256), 256, 0, ctx->stream>>>(G, ctx->px, ctx->py, ctx->pz, n, nullptr,
-                                                             nullptr, nullptr, ctx->tile_need, 0, 0);
+    (++ctx->launches), k_bin<<<nblocks(n, 256), 256, 0, ctx->stream>>>(G, ctx->px, ctx->py, ctx->pz, n, nullptr,
+                                                                        nullptr, nullptr, ctx->tile_need, 0);
   PF_CUDA_TRY(cudaGetLastError());
   rc = pool_commit(ctx);
   if (rc) return rc;
@@ -780,9 +859,15 @@ static int p2g_core(pf_ctx* ctx, const pf_phase* ph, double Vp) {
     StageScope sc(ctx, PF_STAGE_BIN);
     PF_CUDA_TRY(cudaMemsetAsync(ctx->tile_count, 0, (size_t)(nt * PF_TV + 1) * sizeof(int), ctx->stream));
     DevGrid G = dev_grid(ctx);
-    if (n > 0)
-      (++ctx->launches), k_bin_activate<<<nblocks(n, 256), 256, 0, ctx->stream>>>(
-          G, ctx->px, ctx->py, ctx->pz, n, ctx->tile_count, ctx->pkey, ctx->prank, ctx->tile_need, 1, 1);
+    if (n > 0) {
+      (++ctx->launches), k_bin<<<nblocks(n, 256), 256, 0, ctx->stream>>>(
+          G, ctx->px, ctx->py, ctx->pz, n, ctx->tile_count, ctx->pkey, ctx->prank, ctx->tile_need, 1);
+      // the tiles a particle's window can reach: the requested ones and their neighbours
+      const int nt0 = ctx->g.ntiles;
+      (++ctx->launches), k_need_snapshot<<<nblocks(nt0, 256), 256, 0, ctx->stream>>>(ctx->tile_need, ctx->tile_new, nt0);
+      (++ctx->launches), k_need_dilate<<<nblocks(nt0, 256), 256, 0, ctx->stream>>>(ctx->g, ctx->tile_new,
+                                                                                   ctx->tile_need);
+    }
     PF_CUDA_TRY(cudaGetLastError());
     rc = pool_commit(ctx);
     if (rc) return rc;
