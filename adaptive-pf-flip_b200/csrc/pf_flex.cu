@@ -297,10 +297,11 @@ __global__ void __launch_bounds__(PF_TV) k_fx_dir(const int* slot_tile, int nslo
   }
 }
 
-__global__ void k_fx_add(int nslots, const uint8_t* kind, double* x, const float* e) {
+// x += sign * e
+__global__ void k_fx_add(int nslots, const uint8_t* kind, double* x, const float* e, double sign) {
   for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
     const size_t o = (size_t)s * PF_TV + threadIdx.x;
-    if (kind[o]) x[o] += (double)e[o];
+    if (kind[o]) x[o] += sign * (double)e[o];
   }
 }
 
@@ -559,25 +560,42 @@ int solve_learned(pf_ctx* ctx, int nslots, int nred, const uint8_t* kind, double
   const double tol = c.tol;
   double resid = c.res0;
   int iters = 0, sweeps = 0;
-  const int max_sweeps = cfg->max_refine > 0 ? cfg->max_refine : 8;
-  const double inner_rel = cfg->inner_rel_tol > 0.0 ? cfg->inner_rel_tol : 1e-5;
+  // Short sweeps: FP32 recurrences stagnate (and can overflow) long before a
+  // deep inner reduction at 1000:1, so each sweep stops after a modest
+  // reduction or kSweepIters iterations and the FP64 residual restarts it.
+  constexpr int kSweepIters = 1000;
+  const int max_sweeps = cfg->max_refine > 0 ? cfg->max_refine : 64;
+  const double inner_rel = cfg->inner_rel_tol > 0.0 ? cfg->inner_rel_tol : 1e-3;
   bool converged = false, nonfinite = false;
   while (!converged && sweeps < max_sweeps && iters < cfg->max_iter) {
     SolveCtl ic{};
-    rc = flex_solve<float>(ctx, nslots, nred, kind, m, ctx->r, 0.0, inner_rel, cfg->max_iter - iters,
-                           cfg->check_every, precond, cfg->accept_min_gain, sweeps == 0, &ic);
+    rc = flex_solve<float>(ctx, nslots, nred, kind, m, ctx->r, 0.0, inner_rel,
+                           std::min(kSweepIters, cfg->max_iter - iters), cfg->check_every, precond,
+                           cfg->accept_min_gain, sweeps == 0, &ic);
     if (rc) return rc;
     ++sweeps;
     iters += ic.it;
     res->precond_applied = ic.accepted;
     res->precond_rejected = ic.rejected;
-    (++ctx->launches), k_fx_add<<<nred, PF_TV, 0, ctx->stream>>>(nslots, kind, ctx->x, m.e);
+    (++ctx->launches), k_fx_add<<<nred, PF_TV, 0, ctx->stream>>>(nslots, kind, ctx->x, m.e, 1.0);
     (++ctx->launches), k_fx_residual<<<nred, PF_TV, 0, ctx->stream>>>(nbr, nslots, ctx->ctl, kind, ctx->x, ctx->diag,
                                                                       ctx->cx, ctx->cy, ctx->cz, ctx->b64, scale,
                                                                       ctx->r, ctx->partials);
     PF_CUDA_TRY(cudaGetLastError());
     rc = poll_ctl(ctx, &c);
     if (rc) return rc;
+    if (!(c.res < resid) && ic.done != 4) {
+      // the sweep made the FP64 residual worse: take it back and stop with the best solution so far
+      (++ctx->launches), k_fx_add<<<nred, PF_TV, 0, ctx->stream>>>(nslots, kind, ctx->x, m.e, -1.0);
+      (++ctx->launches), k_fx_residual<<<nred, PF_TV, 0, ctx->stream>>>(nbr, nslots, ctx->ctl, kind, ctx->x,
+                                                                        ctx->diag, ctx->cx, ctx->cy, ctx->cz,
+                                                                        ctx->b64, scale, ctx->r, ctx->partials);
+      PF_CUDA_TRY(cudaGetLastError());
+      rc = poll_ctl(ctx, &c);
+      if (rc) return rc;
+      resid = c.res;
+      break;
+    }
     resid = c.res;
     if (!std::isfinite(resid) || ic.done == 4) {
       nonfinite = true;

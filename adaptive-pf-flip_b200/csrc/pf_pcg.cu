@@ -286,10 +286,11 @@ __global__ void __launch_bounds__(PF_TV) k_refine_residual(DevGrid G, int nslots
   block_reduce_2(0.0, rmax, partials, ctl, kStageResid);
 }
 
-__global__ void k_add_correction(int nslots, const uint8_t* kind, double* x, const float* e) {
+// x += sign * e
+__global__ void k_add_correction(int nslots, const uint8_t* kind, double* x, const float* e, double sign) {
   for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
     const size_t o = (size_t)s * PF_TV + threadIdx.x;
-    if (kind[o]) x[o] += (double)e[o];
+    if (kind[o]) x[o] += sign * (double)e[o];
   }
 }
 
@@ -425,12 +426,24 @@ static int solve_mixed_t(pf_ctx* ctx, int nslots, int nred, const uint8_t* kind,
                         &iters, &ic);
     if (rc) return rc;
     ++sweeps;
-    (++ctx->launches), k_add_correction<<<nred, PF_TV, 0, ctx->stream>>>(nslots, kind, ctx->x, m.e);
+    (++ctx->launches), k_add_correction<<<nred, PF_TV, 0, ctx->stream>>>(nslots, kind, ctx->x, m.e, 1.0);
     (++ctx->launches), k_refine_residual<C><<<nred, PF_TV, 0, ctx->stream>>>(G, nslots, ctx->ctl, kind, v, ctx->b64, m.e, scale,
                                                           ctx->partials, 0);
     PF_CUDA_TRY(cudaGetLastError());
     rc = poll(ctx, &c);
     if (rc) return rc;
+    if (!(c.res < resid) && ic.done != 4) {
+      // the sweep made the FP64 residual worse (FP32 recurrences past their
+      // accuracy): take it back and stop with the best solution so far
+      (++ctx->launches), k_add_correction<<<nred, PF_TV, 0, ctx->stream>>>(nslots, kind, ctx->x, m.e, -1.0);
+      (++ctx->launches), k_refine_residual<C><<<nred, PF_TV, 0, ctx->stream>>>(G, nslots, ctx->ctl, kind, v, ctx->b64,
+                                                                               m.e, scale, ctx->partials, 0);
+      PF_CUDA_TRY(cudaGetLastError());
+      rc = poll(ctx, &c);
+      if (rc) return rc;
+      resid = c.res;
+      break;
+    }
     resid = c.res;
     if (!std::isfinite(resid) || ic.done == 4) { nonfinite = true; break; }
     converged = resid < tol;

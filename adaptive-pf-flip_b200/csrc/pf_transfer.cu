@@ -637,13 +637,30 @@ __global__ void __launch_bounds__(256) k_g2p_tiles(DevGrid G, const int* __restr
   }
   __syncthreads();
   float* vp[3] = {P.vx, P.vy, P.vz};
-  for (int q = beg + threadIdx.x; q < end; q += blockDim.x) {
-    const int p = perm[q];
-    const double gx = to_grid((double)P.px[p], G.g.ox, G.g.inv_dx);
-    const double gy = to_grid((double)P.py[p], G.g.oy, G.g.inv_dx);
-    const double gz = to_grid((double)P.pz[p], G.g.oz, G.g.inv_dx);
+  // the next particle's attributes are loaded while this one is sampled
+  int q = beg + threadIdx.x;
+  int pn = 0;
+  float xn = 0.0f, yn = 0.0f, zn = 0.0f, vn[3] = {0.0f, 0.0f, 0.0f};
+  uint8_t tn = 0;
+  if (q < end) {
+    pn = perm[q];
+    xn = P.px[pn]; yn = P.py[pn]; zn = P.pz[pn]; tn = P.type[pn];
+    vn[0] = P.vx[pn]; vn[1] = P.vy[pn]; vn[2] = P.vz[pn];
+  }
+  for (; q < end; q += blockDim.x) {
+    const int p = pn;
+    const float X = xn, Y = yn, Z = zn, v0[3] = {vn[0], vn[1], vn[2]};
+    const uint8_t ty = tn;
+    if (q + (int)blockDim.x < end) {
+      pn = perm[q + blockDim.x];
+      xn = P.px[pn]; yn = P.py[pn]; zn = P.pz[pn]; tn = P.type[pn];
+      vn[0] = P.vx[pn]; vn[1] = P.vy[pn]; vn[2] = P.vz[pn];
+    }
+    const double gx = to_grid((double)X, G.g.ox, G.g.inv_dx);
+    const double gy = to_grid((double)Y, G.g.oy, G.g.inv_dx);
+    const double gz = to_grid((double)Z, G.g.oz, G.g.inv_dx);
     const double c[3][3] = {{gx, gy - 0.5, gz - 0.5}, {gx - 0.5, gy, gz - 0.5}, {gx - 0.5, gy - 0.5, gz}};
-    const float al = P.type[p] == 0 ? (float)aL : (float)aG;
+    const float al = ty == 0 ? (float)aL : (float)aG;
 #pragma unroll
     for (int ax = 0; ax < 3; ++ax) {
       const int i0 = (int)floor(c[ax][0]), j0 = (int)floor(c[ax][1]), k0 = (int)floor(c[ax][2]);
@@ -670,8 +687,7 @@ __global__ void __launch_bounds__(256) k_g2p_tiles(DevGrid G, const int* __restr
       } else {
         sample2<true>(G, ax, c[ax][0], c[ax][1], c[ax][2], cur, old);
       }
-      const float v = vp[ax][p];
-      vp[ax][p] = (v + (cur - old)) * al + cur * (1.0f - al);
+      vp[ax][p] = (v0[ax] + (cur - old)) * al + cur * (1.0f - al);
     }
   }
 }

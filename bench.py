@@ -277,6 +277,8 @@ def pcg_modes(pf, names):
         # the learned two-level preconditioner and its net-free ablation
         "learned": pf.SolverConfig(mode=L, rel_tol=1e-6, precond=pf.PF_PRECOND_NETWORK),
         "flex_jacobi": pf.SolverConfig(mode=L, rel_tol=1e-6, precond=pf.PF_PRECOND_JACOBI),
+        # the learned solver with FP32 inner flexible PCG inside FP64 refinement
+        "learned_fp32": pf.SolverConfig(mode=L, rel_tol=1e-6, precond=pf.PF_PRECOND_NETWORK, inner_fp32=True),
         # the same two-level solver with an exact coarse solve: the bound a perfect network reaches
         "exact_coarse": pf.SolverConfig(mode=L, rel_tol=1e-6, precond=pf.PF_PRECOND_EXACT_COARSE),
     }
