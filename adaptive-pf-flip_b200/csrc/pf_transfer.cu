@@ -166,6 +166,39 @@ __global__ void k_mark_particles(DevGrid G, const float* __restrict__ px, const 
 constexpr int kSplatThreads = 256;
 constexpr float kReachEps = 2e-5f;
 
+// Two FP32 values in one 64-bit register, for the packed .f32x2 arithmetic
+// of sm_100 (one instruction for both lanes of add, sub, mul and fma).
+typedef unsigned long long f32x2;
+
+__device__ __forceinline__ f32x2 f2_pack(float lo, float hi) {
+  f32x2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void f2_unpack(f32x2 v, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f32x2 f2_add(f32x2 a, f32x2 b) {
+  f32x2 d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f32x2 f2_sub(f32x2 a, f32x2 b) {
+  f32x2 d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f32x2 f2_mul(f32x2 a, f32x2 b) {
+  f32x2 d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f32x2 f2_fma(f32x2 a, f32x2 b, f32x2 c) {
+  f32x2 d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+
 __device__ __forceinline__ float cubic(float s) {
   const float t = 1.0f - s;
   return t > 0.0f ? t * t * t : 0.0f;
@@ -234,9 +267,11 @@ __device__ __forceinline__ unsigned long long splat_cell(const DevGrid& G, float
   // global first window node per axis and the split between its two blocks
   const int n[3] = {o0 + bx, o1 + by, o2 + bz};
   const int sp[3] = {min(4 - (n[0] & 3), NX), min(4 - (n[1] & 3), NY), min(4 - (n[2] & 3), NZ)};
-  float am[NW], ap[NW];
+  // window accumulators, two nodes per register pair (node e = (k*NY + j)*NX + i)
+  constexpr int NP = NW / 2;
+  f32x2 am[NP], ap[NP];
 #pragma unroll
-  for (int k = 0; k < NW; ++k) { am[k] = 0.0f; ap[k] = 0.0f; }
+  for (int q = 0; q < NP; ++q) { am[q] = 0ull; ap[q] = 0ull; }
   unsigned reach = 0u;
   // the next particle's attributes are loaded while this one is splatted
   int pn = perm[beg];
@@ -296,44 +331,56 @@ __device__ __forceinline__ unsigned long long splat_cell(const DevGrid& G, float
           band = band || fabsf(sa - 1.0f) <= kReachEps;
         }
     if (band) reach |= exact_reach<A>(G, X, Y, Z, n, sp);
-    // weights
-    float w[NW];
-    float wsum = 0.0f;
+    // weights w = max(1 - (ax + (ay + az)), 0)^3, two nodes per packed instruction
+    float ayz[NY * NZ];
 #pragma unroll
     for (int k = 0; k < NZ; ++k)
 #pragma unroll
-      for (int j = 0; j < NY; ++j)
+      for (int j = 0; j < NY; ++j) ayz[k * NY + j] = ay[j] + az[k];
+    const f32x2 one2 = f2_pack(1.0f, 1.0f);
+    f32x2 w[NP];
+    f32x2 wsum2 = 0ull;
 #pragma unroll
-        for (int i = 0; i < NX; ++i) {
-          const float v = cubic(ax[i] + ay[j] + az[k]);
-          w[(k * NY + j) * NX + i] = v;
-          wsum += v;
-        }
+    for (int q = 0; q < NP; ++q) {
+      const int e0 = 2 * q, e1 = 2 * q + 1;
+      const f32x2 sa = f2_add(f2_pack(ax[e0 % NX], ax[e1 % NX]), f2_pack(ayz[e0 / NX], ayz[e1 / NX]));
+      float t0, t1;
+      f2_unpack(f2_sub(one2, sa), t0, t1);
+      const f32x2 t = f2_pack(fmaxf(t0, 0.0f), fmaxf(t1, 0.0f));
+      w[q] = f2_mul(f2_mul(t, t), t);
+      wsum2 = f2_add(wsum2, w[q]);
+    }
+    float ws0, ws1;
+    f2_unpack(wsum2, ws0, ws1);
+    const float wsum = ws0 + ws1;
     if (!(wsum > 0.0f)) continue;
     const float mp = (TY == 0 ? m_l : m_g) * VOL;
     const float sm_ = mp / wsum;
     const float sp_ = sm_ * VA;
+    const f32x2 sm2 = f2_pack(sm_, sm_), sp2 = f2_pack(sp_, sp_);
 #pragma unroll
-    for (int e = 0; e < NW; ++e) {
-      am[e] = fmaf(w[e], sm_, am[e]);
-      ap[e] = fmaf(w[e], sp_, ap[e]);
+    for (int q = 0; q < NP; ++q) {
+      am[q] = f2_fma(w[q], sm2, am[q]);
+      ap[q] = f2_fma(w[q], sp2, ap[q]);
     }
   }
   float* smom = sm + (2 * A) * kBox3;
   float* smas = sm + (2 * A + 1) * kBox3;
 #pragma unroll
-  for (int k = 0; k < NZ; ++k)
+  for (int q = 0; q < NP; ++q) {
+    float m2[2], p2[2];
+    f2_unpack(am[q], m2[0], m2[1]);
+    f2_unpack(ap[q], p2[0], p2[1]);
 #pragma unroll
-    for (int j = 0; j < NY; ++j)
-#pragma unroll
-      for (int i = 0; i < NX; ++i) {
-        const int e = (k * NY + j) * NX + i;
-        if (am[e] != 0.0f || ap[e] != 0.0f) {
-          const int si = (bx + i) + kBox * ((by + j) + kBox * (bz + k));
-          atomicAdd(&smom[si], ap[e]);
-          atomicAdd(&smas[si], am[e]);
-        }
+    for (int h = 0; h < 2; ++h) {
+      const int e = 2 * q + h, i = e % NX, j = (e / NX) % NY, k = e / (NX * NY);
+      if (m2[h] != 0.0f || p2[h] != 0.0f) {
+        const int si = (bx + i) + kBox * ((by + j) + kBox * (bz + k));
+        atomicAdd(&smom[si], p2[h]);
+        atomicAdd(&smas[si], m2[h]);
       }
+    }
+  }
   // reached window blocks -> the tile's 4x4x4 block box (block of node o -> (o >> 2) - (o0 >> 2))
   const int w0 = (n[0] >> 2) - (o0 >> 2), w1 = (n[1] >> 2) - (o1 >> 2), w2 = (n[2] >> 2) - (o2 >> 2);
   unsigned long long box = 0ull;
