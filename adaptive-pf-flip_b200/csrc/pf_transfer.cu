@@ -183,6 +183,12 @@ __device__ __forceinline__ f32x2 f2_add(f32x2 a, f32x2 b) {
   asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
   return d;
 }
+// the same add, never merged with an identical earlier one (forces a recomputation)
+__device__ __forceinline__ f32x2 f2_add_again(f32x2 a, f32x2 b) {
+  f32x2 d;
+  asm volatile("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
 __device__ __forceinline__ f32x2 f2_sub(f32x2 a, f32x2 b) {
   f32x2 d;
   asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
@@ -337,19 +343,21 @@ __device__ __forceinline__ unsigned long long splat_cell(const DevGrid& G, float
     for (int k = 0; k < NZ; ++k)
 #pragma unroll
       for (int j = 0; j < NY; ++j) ayz[k * NY + j] = ay[j] + az[k];
+    // two passes over the window: the weight sum, then the accumulation with
+    // the weights recomputed (cheaper than holding 36 of them in registers)
     const f32x2 one2 = f2_pack(1.0f, 1.0f);
-    f32x2 w[NP];
-    f32x2 wsum2 = 0ull;
-#pragma unroll
-    for (int q = 0; q < NP; ++q) {
+    auto weight = [&](int q, bool again) {
       const int e0 = 2 * q, e1 = 2 * q + 1;
-      const f32x2 sa = f2_add(f2_pack(ax[e0 % NX], ax[e1 % NX]), f2_pack(ayz[e0 / NX], ayz[e1 / NX]));
+      const f32x2 a2 = f2_pack(ax[e0 % NX], ax[e1 % NX]), b2 = f2_pack(ayz[e0 / NX], ayz[e1 / NX]);
+      const f32x2 sa = again ? f2_add_again(a2, b2) : f2_add(a2, b2);
       float t0, t1;
       f2_unpack(f2_sub(one2, sa), t0, t1);
       const f32x2 t = f2_pack(fmaxf(t0, 0.0f), fmaxf(t1, 0.0f));
-      w[q] = f2_mul(f2_mul(t, t), t);
-      wsum2 = f2_add(wsum2, w[q]);
-    }
+      return f2_mul(f2_mul(t, t), t);
+    };
+    f32x2 wsum2 = 0ull;
+#pragma unroll
+    for (int q = 0; q < NP; ++q) wsum2 = f2_add(wsum2, weight(q, false));
     float ws0, ws1;
     f2_unpack(wsum2, ws0, ws1);
     const float wsum = ws0 + ws1;
@@ -360,8 +368,9 @@ __device__ __forceinline__ unsigned long long splat_cell(const DevGrid& G, float
     const f32x2 sm2 = f2_pack(sm_, sm_), sp2 = f2_pack(sp_, sp_);
 #pragma unroll
     for (int q = 0; q < NP; ++q) {
-      am[q] = f2_fma(w[q], sm2, am[q]);
-      ap[q] = f2_fma(w[q], sp2, ap[q]);
+      const f32x2 wq = weight(q, true);
+      am[q] = f2_fma(wq, sm2, am[q]);
+      ap[q] = f2_fma(wq, sp2, ap[q]);
     }
   }
   float* smom = sm + (2 * A) * kBox3;
