@@ -411,33 +411,51 @@ def run_step_pcg(pf, name, n, modes, pre_steps=1, max_iter=20000, seed=0, weight
                         f"1000:1, dt 1/240", "unknowns": int(st.n_cells), "modes": out}
 
 
-def run_full_step(pf, n=48, steps=20, seed=0):
+def run_full_step(pf, n=48, steps=20, seed=0, solvers=("plain",), warmup=3):
     """Whole solver step (markCells .. advection) on the Rayleigh-Taylor scene
-    at 1000:1, PLAIN PCG to 1e-6 relative; device-timed particles/s."""
+    at 1000:1, pressure to 1e-6 relative; device-timed particles/s for each
+    pressure solver ("plain": PLAIN PCG, "learned": the learned two-level
+    preconditioner with the shipped weights), every solver from the same
+    initial particles."""
     import torch
     sc = pf.scenes.rayleigh_taylor(n, seed=seed)
-    sim = pf.SparseSim3DTP(n, n, n, sc["dx"], max_particles=len(sc["pos"]))
-    sim.phase = pf.PhaseParams(sc["rho_l"], sc["rho_g"])
-    sim.phase.rho_tilde_0 = pf.calibrateRhoTilde0(sim.phase, 1.0, grid=sim.grid)
-    sim.dt = 1.0 / 240.0
-    sim.cg_iters, sim.cg_tol = 4000, 0.0
-    sim.solver = pf.SolverConfig(rel_tol=1e-6)
-    sim.set_particles(sc["pos"], sc["vel"], sc["type"], sc["volume"])
-    stream = torch.cuda.ExternalStream(pf.load().pf_stream(sim.grid.ctx))
-    for _ in range(3):
-        sim.step()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    iters = 0
-    e0.record(stream)
-    for _ in range(steps):
-        iters += sim.step().solve.iterations
-    e1.record(stream)
-    e1.synchronize()
-    ms = e0.elapsed_time(e1)
-    return {"workload": f"rayleigh_taylor_{n}: {len(sc['pos'])} particles, 1000:1, dt 1/240, plain PCG to 1e-6",
-            "particles_per_s": len(sc["pos"]) * steps / (ms / 1000.0), "ms_per_step": ms / steps,
-            "pcg_iterations_per_step": iters / steps}
+    out = {"workload": f"rayleigh_taylor_{n}: {len(sc['pos'])} particles, 1000:1, dt 1/240, "
+                       f"pressure to 1e-6, {warmup} warm-up + {steps} timed steps"}
+    for solver in solvers:
+        sim = pf.SparseSim3DTP(n, n, n, sc["dx"], max_particles=len(sc["pos"]))
+        sim.phase = pf.PhaseParams(sc["rho_l"], sc["rho_g"])
+        sim.phase.rho_tilde_0 = pf.calibrateRhoTilde0(sim.phase, 1.0, grid=sim.grid)
+        sim.dt = 1.0 / 240.0
+        sim.cg_iters, sim.cg_tol = 20000, 0.0
+        if solver == "learned":
+            pf.LearnedCoarseSolver(sim.grid).load_default()
+            sim.solver = pf.SolverConfig(mode=pf.PF_SOLVER_LEARNED, rel_tol=1e-6, precond=pf.PF_PRECOND_NETWORK)
+        else:
+            sim.solver = pf.SolverConfig(rel_tol=1e-6)
+        sim.set_particles(sc["pos"], sc["vel"], sc["type"], sc["volume"])
+        stream = torch.cuda.ExternalStream(pf.load().pf_stream(sim.grid.ctx))
+        for _ in range(warmup):
+            sim.step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        iters, rejected = 0, 0
+        e0.record(stream)
+        for _ in range(steps):
+            st = sim.step().solve
+            iters += st.iterations
+            rejected += st.precond_rejected
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        rec = {"particles_per_s": len(sc["pos"]) * steps / (ms / 1000.0), "ms_per_step": ms / steps,
+               "pcg_iterations_per_step": iters / steps}
+        if solver == "learned":
+            rec["coarse_rejected"] = rejected
+        out[solver] = rec
+        sim.grid.close()
+    if "plain" in out and "learned" in out:
+        out["learned_speedup"] = out["plain"]["ms_per_step"] / out["learned"]["ms_per_step"]
+    return out
 
 
 def run_ours(args, rank, world, local, dist):
@@ -506,7 +524,8 @@ def run_ours(args, rank, world, local, dist):
     }
     if rank == 0 and not args.no_extras:
         line["pcg"] = run_pcg(pf, args.pcg_n, pcg_modes(pf, args.pcg_modes.split(",")))
-        line["full_step"] = run_full_step(pf)
+        line["full_step"] = run_full_step(pf, n=args.full_step_n, steps=args.full_step_steps,
+                                          solvers=("plain", "learned"))
     if rank == 0 and not args.no_cpu_baseline:
         cores = 8
         np_s, times = cpu_reference_sample(sc, slab_cells=args.cpu_slab, steps=1)
@@ -560,6 +579,9 @@ def main():
                     help="run only whole-step pressure systems, e.g. rt:256,bubble:128 (modes from --pcg-modes)")
     ap.add_argument("--step-pcg-pre", type=int, default=1, help="plain steps before the step-pressure snapshot")
     ap.add_argument("--weights", default="", help="network weights for the learned mode (default: shipped)")
+    ap.add_argument("--full-step-n", type=int, default=128, help="grid of the full-step block (Rayleigh-Taylor)")
+    ap.add_argument("--full-step-steps", type=int, default=5, help="timed steps of the full-step block")
+    ap.add_argument("--full-step-only", action="store_true", help="run only the full-step block")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
@@ -567,6 +589,11 @@ def main():
         rank = int(os.environ.get("RANK", "0"))
         world = int(os.environ.get("WORLD_SIZE", "1"))
         run_reference(args, rank, world)
+        return
+    if args.full_step_only:  # the full-step block alone
+        pf = load_pkg()
+        print(json.dumps(run_full_step(pf, n=args.full_step_n, steps=args.full_step_steps,
+                                       solvers=("plain", "learned"))), flush=True)
         return
     if args.step_pcg:  # whole-step pressure systems alone
         pf = load_pkg()
