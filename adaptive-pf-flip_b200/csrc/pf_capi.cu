@@ -59,6 +59,13 @@ void free_all(pf_ctx* c) {
   F(c->xf); F(c->rf); F(c->pf32); F(c->Apf); F(c->diagf); F(c->cxf); F(c->cyf); F(c->czf); F(c->pbf); F(c->cbf);
   F(c->b64);
   F(c->d_clamp); F(c->d_flags); F(c->cell_flags); F(c->esc_buf);
+  if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
+  for (int q = 0; q < 2; ++q) {
+    F(c->dl_staging[q]);
+    if (c->dl_packed[q]) cudaEventDestroy(c->dl_packed[q]);
+    if (c->dl_copied[q]) cudaEventDestroy(c->dl_copied[q]);
+  }
+  if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
   for (const auto& t : c->timed) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }
   for (int s = 0; s < PF_NSTAGES; ++s) if (c->open_ev[s]) cudaEventDestroy(c->open_ev[s]);
   if (c->h_ctl) cudaFreeHost(c->h_ctl);
@@ -235,6 +242,7 @@ const char* pf_last_error(const pf_ctx* ctx) { return ctx ? ctx->err.c_str() : "
 int pf_sync(pf_ctx* ctx) {
   if (!ctx) return PF_ERR_INVALID;
   PF_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  if (ctx->copy_stream) PF_CUDA_TRY(cudaStreamSynchronize(ctx->copy_stream));
   return PF_OK;
 }
 
@@ -309,6 +317,73 @@ int pf_upload_particles(pf_ctx* ctx, size_t n, const float* pos, const float* ve
 int pf_download_particles(pf_ctx* ctx, float* pos, float* vel, uint8_t* type, float* volume) {
   return download_impl(ctx, pos, vel, type, volume, false);
 }
+// Asynchronous FP32 download: the arrays are packed into one of two device
+// staging slots on the context stream, and the host copies run on a second
+// stream, so they overlap the calls that follow (the next step's upload runs
+// against the other direction of the link).  A slot is reused only after its
+// previous host copy finished.
+int pf_download_particles_async(pf_ctx* ctx, float* pos, float* vel, uint8_t* type, float* volume) {
+  if (!ctx) return PF_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  const size_t n = ctx->np;
+  if (n == 0 || (!pos && !vel && !type && !volume)) return PF_OK;
+  auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
+  const size_t b3 = up(3 * n * sizeof(float)), b1 = up(n * sizeof(float)), bt = up(n);
+  const size_t need = 2 * b3 + b1 + bt;  // room for every array
+  if (!ctx->copy_stream) {
+    PF_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+    for (int q = 0; q < 2; ++q) {
+      PF_CUDA_TRY(cudaEventCreateWithFlags(&ctx->dl_packed[q], cudaEventDisableTiming));
+      PF_CUDA_TRY(cudaEventCreateWithFlags(&ctx->dl_copied[q], cudaEventDisableTiming));
+    }
+  }
+  if (ctx->dl_bytes < need) {
+    PF_CUDA_TRY(cudaStreamSynchronize(ctx->copy_stream));
+    PF_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    for (int q = 0; q < 2; ++q) {
+      if (ctx->dl_staging[q]) PF_CUDA_TRY(cudaFree(ctx->dl_staging[q]));
+      ctx->dl_staging[q] = nullptr;
+      ctx->dl_recorded[q] = false;
+    }
+    ctx->dl_bytes = 0;
+    for (int q = 0; q < 2; ++q) PF_CUDA_TRY(cudaMalloc(&ctx->dl_staging[q], need));
+    ctx->dl_bytes = need;
+  }
+  const int slot = ctx->dl_slot;
+  ctx->dl_slot ^= 1;
+  if (ctx->dl_recorded[slot]) PF_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, ctx->dl_copied[slot], 0));
+  char* st = (char*)ctx->dl_staging[slot];
+  float* s_pos = (float*)st;
+  float* s_vel = (float*)(st + b3);
+  float* s_vol = (float*)(st + 2 * b3);
+  uint8_t* s_type = (uint8_t*)(st + 2 * b3 + b1);
+  const int nb = nblocks(n, 256);
+  if (pos) (++ctx->launches), k_pack3<float><<<nb, 256, 0, ctx->stream>>>(ctx->px, ctx->py, ctx->pz, s_pos, n);
+  if (vel) (++ctx->launches), k_pack3<float><<<nb, 256, 0, ctx->stream>>>(ctx->vx, ctx->vy, ctx->vz, s_vel, n);
+  if (type) PF_CUDA_TRY(cudaMemcpyAsync(s_type, ctx->type, n, cudaMemcpyDeviceToDevice, ctx->stream));
+  if (volume) PF_CUDA_TRY(cudaMemcpyAsync(s_vol, ctx->vol, n * sizeof(float), cudaMemcpyDeviceToDevice, ctx->stream));
+  PF_CUDA_TRY(cudaGetLastError());
+  PF_CUDA_TRY(cudaEventRecord(ctx->dl_packed[slot], ctx->stream));
+  PF_CUDA_TRY(cudaStreamWaitEvent(ctx->copy_stream, ctx->dl_packed[slot], 0));
+  if (pos) PF_CUDA_TRY(cudaMemcpyAsync(pos, s_pos, 3 * n * sizeof(float), cudaMemcpyDefault, ctx->copy_stream));
+  if (vel) PF_CUDA_TRY(cudaMemcpyAsync(vel, s_vel, 3 * n * sizeof(float), cudaMemcpyDefault, ctx->copy_stream));
+  if (type) PF_CUDA_TRY(cudaMemcpyAsync(type, s_type, n, cudaMemcpyDefault, ctx->copy_stream));
+  if (volume) PF_CUDA_TRY(cudaMemcpyAsync(volume, s_vol, n * sizeof(float), cudaMemcpyDefault, ctx->copy_stream));
+  PF_CUDA_TRY(cudaEventRecord(ctx->dl_copied[slot], ctx->copy_stream));
+  ctx->dl_recorded[slot] = true;
+  ctx->dl_last = slot;
+  return PF_OK;
+}
+
+// The context stream waits (on the device) for every asynchronous download so
+// far: work or events queued on it afterwards follow those host copies.
+int pf_join_downloads(pf_ctx* ctx) {
+  if (!ctx) return PF_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  if (ctx->dl_last >= 0) PF_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, ctx->dl_copied[ctx->dl_last], 0));
+  return PF_OK;
+}
+
 int pf_upload_particles_f64(pf_ctx* ctx, size_t n, const double* pos, const double* vel, const uint8_t* type,
                             const double* volume) {
   return upload_impl(ctx, n, pos, vel, type, volume, true);

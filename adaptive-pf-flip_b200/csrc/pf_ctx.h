@@ -41,6 +41,14 @@ struct pf_ctx {
   uint8_t* type = nullptr;
   void* staging = nullptr;  // upload/download staging (cap * 3 doubles)
   size_t staging_bytes = 0;
+  // asynchronous downloads: two device staging slots, copied to the host on copy_stream
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t dl_packed[2] = {}, dl_copied[2] = {};
+  bool dl_recorded[2] = {};
+  void* dl_staging[2] = {};
+  size_t dl_bytes = 0;
+  int dl_slot = 0;
+  int dl_last = -1;  // slot of the most recent asynchronous download
 
   // ---- binning ----
   int* tile_count = nullptr;  // [ntiles+1]

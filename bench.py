@@ -192,8 +192,13 @@ class TransferStep:
         self.L.check(rc, self.ctx, "pf_upload_particles")
 
     def download_vel(self):
-        rc = self.lib.pf_download_particles(self.ctx, None, self.h_out.data_ptr(), None, None)
-        self.L.check(rc, self.ctx, "pf_download_particles")
+        """The step's result to pinned host memory; the copy overlaps the next
+        step's upload (the timed region joins it before its end event)."""
+        rc = self.lib.pf_download_particles_async(self.ctx, None, self.h_out.data_ptr(), None, None)
+        self.L.check(rc, self.ctx, "pf_download_particles_async")
+
+    def join_downloads(self):
+        self.L.check(self.lib.pf_join_downloads(self.ctx), self.ctx, "pf_join_downloads")
 
     def step(self):
         L, lib, ctx = self.L, self.lib, self.ctx
@@ -217,6 +222,8 @@ def time_steps(ts, steps, warmup, dist, local, e2e=False):
         ts.step()
         if e2e:
             ts.download_vel()
+    if e2e:
+        ts.lib.pf_sync(ts.ctx)
     torch.cuda.synchronize(local)
     barrier(dist)
     torch.cuda.synchronize(local)
@@ -229,6 +236,8 @@ def time_steps(ts, steps, warmup, dist, local, e2e=False):
         ts.step()
         if e2e:
             ts.download_vel()
+    if e2e:
+        ts.join_downloads()
     ev1.record(ts.stream)
     ev1.synchronize()
     torch.cuda.synchronize(local)

@@ -136,6 +136,7 @@ typedef struct {
 PFGPU_API int pf_create(const pf_grid_desc* desc, pf_ctx** out);
 PFGPU_API int pf_destroy(pf_ctx* ctx);
 PFGPU_API const char* pf_last_error(const pf_ctx* ctx);
+/* Wait for the context's stream and its asynchronous downloads. */
 PFGPU_API int pf_sync(pf_ctx* ctx);
 /* The context's stream as an opaque handle (a cudaStream_t). */
 PFGPU_API void* pf_stream(pf_ctx* ctx);
@@ -145,6 +146,14 @@ PFGPU_API void* pf_stream(pf_ctx* ctx);
 PFGPU_API int pf_upload_particles(pf_ctx* ctx, size_t n, const float* pos, const float* vel,
                         const uint8_t* type, const float* volume);
 PFGPU_API int pf_download_particles(pf_ctx* ctx, float* pos, float* vel, uint8_t* type, float* volume);
+/* The same copy without waiting for it: the arrays are staged on the device
+ * in stream order and copied to the host on a second stream, overlapping the
+ * calls that follow (e.g. the next step's upload).  Host buffers should be
+ * pinned (a pageable buffer makes the copy synchronous).  The host may read
+ * them after pf_sync; pf_join_downloads makes the context stream wait for
+ * them on the device (for events recorded after it). */
+PFGPU_API int pf_download_particles_async(pf_ctx* ctx, float* pos, float* vel, uint8_t* type, float* volume);
+PFGPU_API int pf_join_downloads(pf_ctx* ctx);
 /* FP64: the reference's Particles3DTP layout (std::vector<Vec3> = n x 3 doubles). */
 PFGPU_API int pf_upload_particles_f64(pf_ctx* ctx, size_t n, const double* pos, const double* vel,
                             const uint8_t* type, const double* volume);

@@ -261,3 +261,37 @@ def test_g2p_and_advect_match_oracle(pf):
     st_o = o.advect(ps_o, go, 1.0 / 60.0, 2)
     assert np.max(np.abs(ps_g.pos - ps_o.pos)) < 1e-5 / n
     assert (st_g.clamped_liquid, st_g.clamped_gas) == (st_o.clamped_liquid, st_o.clamped_gas)
+
+
+def test_async_download_matches_blocking_download(pf):
+    """pf_download_particles_async stages on the device and copies on a second
+    stream; after pf_sync the pinned host arrays equal a blocking download,
+    also when three downloads cycle through the two staging slots between
+    uploads that change the particles."""
+    import ctypes as C
+
+    import torch
+    n = 16
+    sc = pf.scenes.bubble_tank(n, seed=3)
+    lib = pf.load()
+    g = pf.SparseMacGrid3D(n, n, n, 1.0 / n, max_particles=len(sc["pos"]))
+    np_ = len(sc["pos"])
+    outs = []
+    for k in range(3):
+        vel = (sc["vel"] * (k + 1)).astype(np.float32)
+        lib.pf_upload_particles(g.ctx, np_, sc["pos"].ctypes.data, vel.ctypes.data, sc["type"].ctypes.data,
+                                sc["volume"].ctypes.data)
+        hp = torch.empty((np_, 3), dtype=torch.float32).pin_memory()
+        hv = torch.empty((np_, 3), dtype=torch.float32).pin_memory()
+        ht = torch.empty((np_,), dtype=torch.uint8).pin_memory()
+        hw = torch.empty((np_,), dtype=torch.float32).pin_memory()
+        pf._lib.check(lib.pf_download_particles_async(g.ctx, hp.data_ptr(), hv.data_ptr(), ht.data_ptr(),
+                                                      hw.data_ptr()), g.ctx, "pf_download_particles_async")
+        outs.append((vel, hp, hv, ht, hw))
+    pf._lib.check(lib.pf_sync(g.ctx), g.ctx, "pf_sync")
+    for vel, hp, hv, ht, hw in outs:
+        assert np.array_equal(hp.numpy(), sc["pos"].astype(np.float32))
+        assert np.array_equal(hv.numpy(), vel)
+        assert np.array_equal(ht.numpy(), sc["type"])
+        assert np.array_equal(hw.numpy(), sc["volume"].astype(np.float32))
+    g.close()
