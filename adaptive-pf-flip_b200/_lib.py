@@ -28,7 +28,7 @@ PF_PRECOND_NETWORK, PF_PRECOND_EXACT_COARSE, PF_PRECOND_JACOBI = 0, 1, 2
 EXPORTS = (
     "pf_create", "pf_destroy", "pf_last_error", "pf_sync", "pf_stream",
     "pf_upload_particles", "pf_download_particles", "pf_upload_particles_f64", "pf_download_particles_f64",
-    "pf_download_particles_async", "pf_join_downloads",
+    "pf_download_particles_async", "pf_join_downloads", "pf_upload_particles_async",
     "pf_num_particles", "pf_grid_set_field", "pf_grid_get_field", "pf_grid_clear_field", "pf_grid_clear_all",
     "pf_grid_copy", "pf_active_blocks4", "pf_active_cells", "pf_active_tiles", "pf_mark_cells", "pf_p2g",
     "pf_save_velocity", "pf_apply_gravity", "pf_apply_wall_boundary", "pf_project", "pf_g2p", "pf_advect",
@@ -124,6 +124,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "pf_download_particles": (i, [vp, vp, vp, vp, vp]),
         "pf_download_particles_async": (i, [vp, vp, vp, vp, vp]),
         "pf_join_downloads": (i, [vp]),
+        "pf_upload_particles_async": (i, [vp, C.c_size_t, vp, vp, vp, vp]),
         "pf_upload_particles_f64": (i, [vp, sz, vp, vp, vp, vp]),
         "pf_download_particles_f64": (i, [vp, vp, vp, vp, vp]),
         "pf_num_particles": (sz, [vp]),

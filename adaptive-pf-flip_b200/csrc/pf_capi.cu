@@ -4,6 +4,7 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <utility>
 
 #include "pf_coarse.cuh"
 #include "pf_ctx.h"
@@ -59,6 +60,11 @@ void free_all(pf_ctx* c) {
   F(c->xf); F(c->rf); F(c->pf32); F(c->Apf); F(c->diagf); F(c->cxf); F(c->cyf); F(c->czf); F(c->pbf); F(c->cbf);
   F(c->b64);
   F(c->d_clamp); F(c->d_flags); F(c->cell_flags); F(c->esc_buf);
+  if (c->up_stream) cudaStreamSynchronize(c->up_stream);
+  F(c->bpx); F(c->bpy); F(c->bpz); F(c->bvx); F(c->bvy); F(c->bvz); F(c->bvol); F(c->btype); F(c->up_staging);
+  if (c->up_done) cudaEventDestroy(c->up_done);
+  if (c->back_free) cudaEventDestroy(c->back_free);
+  if (c->up_stream) cudaStreamDestroy(c->up_stream);
   if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
   for (int q = 0; q < 2; ++q) {
     F(c->dl_staging[q]);
@@ -243,20 +249,45 @@ int pf_sync(pf_ctx* ctx) {
   if (!ctx) return PF_ERR_INVALID;
   PF_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   if (ctx->copy_stream) PF_CUDA_TRY(cudaStreamSynchronize(ctx->copy_stream));
+  if (ctx->up_stream) PF_CUDA_TRY(cudaStreamSynchronize(ctx->up_stream));
   return PF_OK;
 }
 
 void* pf_stream(pf_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 
-size_t pf_num_particles(const pf_ctx* ctx) { return ctx ? ctx->np : 0; }
+size_t pf_num_particles(const pf_ctx* ctx) { return ctx ? (ctx->up_pending ? ctx->np_next : ctx->np) : 0; }
 
 int pf_active_tiles(const pf_ctx* ctx) { return ctx ? ctx->nslots : -1; }
+
+// Swap in the particle set of a pending asynchronous upload: the context
+// stream waits for it, and the set it replaces becomes free for the next
+// upload once the work queued so far (which still reads it) is done.
+static int take_upload(pf_ctx* ctx) {
+  if (!ctx->up_pending) return PF_OK;
+  PF_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, ctx->up_done, 0));
+  std::swap(ctx->px, ctx->bpx);
+  std::swap(ctx->py, ctx->bpy);
+  std::swap(ctx->pz, ctx->bpz);
+  std::swap(ctx->vx, ctx->bvx);
+  std::swap(ctx->vy, ctx->bvy);
+  std::swap(ctx->vz, ctx->bvz);
+  std::swap(ctx->vol, ctx->bvol);
+  std::swap(ctx->type, ctx->btype);
+  ctx->np = ctx->np_next;
+  ctx->bins_valid = false;
+  PF_CUDA_TRY(cudaEventRecord(ctx->back_free, ctx->stream));
+  ctx->back_free_recorded = true;
+  ctx->up_pending = false;
+  return PF_OK;
+}
 
 static int upload_impl(pf_ctx* ctx, size_t n, const void* pos, const void* vel, const uint8_t* type,
                        const void* vol, bool f64) {
   if (!ctx || (n && (!pos || !vel || !type || !vol))) return PF_ERR_INVALID;
   if (n > ctx->cap) return set_error(ctx, PF_ERR_CAPACITY, "more particles than max_particles");
   cudaSetDevice(ctx->device);
+  int rc = take_upload(ctx);
+  if (rc) return rc;
   ctx->np = n;
   ctx->bins_valid = false;
   if (n == 0) return PF_OK;
@@ -282,6 +313,8 @@ static int upload_impl(pf_ctx* ctx, size_t n, const void* pos, const void* vel, 
 static int download_impl(pf_ctx* ctx, void* pos, void* vel, uint8_t* type, void* vol, bool f64) {
   if (!ctx) return PF_ERR_INVALID;
   cudaSetDevice(ctx->device);
+  int rc = take_upload(ctx);
+  if (rc) return rc;
   const size_t n = ctx->np;
   if (n == 0) return PF_OK;
   const size_t es = f64 ? sizeof(double) : sizeof(float);
@@ -325,6 +358,10 @@ int pf_download_particles(pf_ctx* ctx, float* pos, float* vel, uint8_t* type, fl
 int pf_download_particles_async(pf_ctx* ctx, float* pos, float* vel, uint8_t* type, float* volume) {
   if (!ctx) return PF_ERR_INVALID;
   cudaSetDevice(ctx->device);
+  {
+    const int rc = take_upload(ctx);
+    if (rc) return rc;
+  }
   const size_t n = ctx->np;
   if (n == 0 || (!pos && !vel && !type && !volume)) return PF_OK;
   auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
@@ -381,6 +418,46 @@ int pf_join_downloads(pf_ctx* ctx) {
   if (!ctx) return PF_ERR_INVALID;
   cudaSetDevice(ctx->device);
   if (ctx->dl_last >= 0) PF_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, ctx->dl_copied[ctx->dl_last], 0));
+  return PF_OK;
+}
+
+// Asynchronous FP32 upload into the second particle set: the host copies
+// and the unpacking run on their own stream, overlapping the work already
+// queued (the current step), and the next call that uses the particles swaps
+// the set in.  A later upload before that call replaces this one.
+int pf_upload_particles_async(pf_ctx* ctx, size_t n, const float* pos, const float* vel, const uint8_t* type,
+                              const float* volume) {
+  if (!ctx || (n && (!pos || !vel || !type || !volume))) return PF_ERR_INVALID;
+  if (n > ctx->cap) return set_error(ctx, PF_ERR_CAPACITY, "more particles than max_particles");
+  cudaSetDevice(ctx->device);
+  const size_t cap = ctx->cap;
+  if (!ctx->up_stream) {
+    PF_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->up_stream, cudaStreamNonBlocking));
+    PF_CUDA_TRY(cudaEventCreateWithFlags(&ctx->up_done, cudaEventDisableTiming));
+    PF_CUDA_TRY(cudaEventCreateWithFlags(&ctx->back_free, cudaEventDisableTiming));
+    float** pa[7] = {&ctx->bpx, &ctx->bpy, &ctx->bpz, &ctx->bvx, &ctx->bvy, &ctx->bvz, &ctx->bvol};
+    for (float** q : pa) PF_CUDA_TRY(cudaMalloc(q, cap * sizeof(float)));
+    PF_CUDA_TRY(cudaMalloc(&ctx->btype, cap));
+    PF_CUDA_TRY(cudaMalloc(&ctx->up_staging, 6 * cap * sizeof(float)));
+  }
+  if (ctx->up_pending) PF_CUDA_TRY(cudaEventSynchronize(ctx->up_done));  // superseded; its copies must land first
+  // the second set was the particles of earlier work: wait until that work is done
+  if (ctx->back_free_recorded) PF_CUDA_TRY(cudaStreamWaitEvent(ctx->up_stream, ctx->back_free, 0));
+  if (n > 0) {
+    const int nb = nblocks(n, 256);
+    float* sp = ctx->up_staging;
+    float* sv = ctx->up_staging + 3 * cap;
+    PF_CUDA_TRY(cudaMemcpyAsync(sp, pos, 3 * n * sizeof(float), cudaMemcpyDefault, ctx->up_stream));
+    PF_CUDA_TRY(cudaMemcpyAsync(sv, vel, 3 * n * sizeof(float), cudaMemcpyDefault, ctx->up_stream));
+    PF_CUDA_TRY(cudaMemcpyAsync(ctx->btype, type, n, cudaMemcpyDefault, ctx->up_stream));
+    PF_CUDA_TRY(cudaMemcpyAsync(ctx->bvol, volume, n * sizeof(float), cudaMemcpyDefault, ctx->up_stream));
+    (++ctx->launches), k_unpack3<float><<<nb, 256, 0, ctx->up_stream>>>(sp, ctx->bpx, ctx->bpy, ctx->bpz, n);
+    (++ctx->launches), k_unpack3<float><<<nb, 256, 0, ctx->up_stream>>>(sv, ctx->bvx, ctx->bvy, ctx->bvz, n);
+    PF_CUDA_TRY(cudaGetLastError());
+  }
+  PF_CUDA_TRY(cudaEventRecord(ctx->up_done, ctx->up_stream));
+  ctx->np_next = n;
+  ctx->up_pending = true;
   return PF_OK;
 }
 
@@ -458,12 +535,20 @@ int pf_active_cells(pf_ctx* ctx, int32_t* cells, size_t* n) {
 int pf_mark_cells(pf_ctx* ctx) {
   if (!ctx) return PF_ERR_INVALID;
   cudaSetDevice(ctx->device);
+  {
+    const int rc = take_upload(ctx);
+    if (rc) return rc;
+  }
   return pf::mark_cells(ctx);
 }
 
 int pf_p2g(pf_ctx* ctx, const pf_phase* phase, double Vp) {
   if (!ctx || !phase) return PF_ERR_INVALID;
   cudaSetDevice(ctx->device);
+  {
+    const int rc = take_upload(ctx);
+    if (rc) return rc;
+  }
   return pf::p2g(ctx, phase, Vp);
 }
 
@@ -508,12 +593,18 @@ int pf_g2p(pf_ctx* ctx, const pf_ctx* saved, double alpha_l, double alpha_g) {
     cudaStreamSynchronize(saved->stream);
   }
   cudaSetDevice(ctx->device);
+  const int rc = take_upload(ctx);
+  if (rc) return rc;
   return pf::g2p(ctx, saved, alpha_l, alpha_g);
 }
 
 int pf_advect(pf_ctx* ctx, double dt, int order, pf_clamp_stats* stats, double* escape, size_t* n_escape) {
   if (!ctx || (order != 2 && order != 3)) return PF_ERR_INVALID;
   cudaSetDevice(ctx->device);
+  {
+    const int rc = take_upload(ctx);
+    if (rc) return rc;
+  }
   return pf::advect(ctx, dt, order, stats, escape, n_escape);
 }
 
@@ -524,7 +615,9 @@ int pf_step(pf_ctx* ctx, const pf_step_cfg* cfg, pf_step_stats* stats) {
   if (!ctx || !cfg || check_solve_cfg(&cfg->solve)) return PF_ERR_INVALID;
   if (cfg->advect_order != 2 && cfg->advect_order != 3) return PF_ERR_INVALID;
   cudaSetDevice(ctx->device);
-  int rc = pool_reset(ctx);
+  int rc = take_upload(ctx);
+  if (rc) return rc;
+  rc = pool_reset(ctx);
   if (rc) return rc;
   rc = pf::mark_cells(ctx);
   if (rc) return rc;

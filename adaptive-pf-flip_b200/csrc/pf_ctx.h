@@ -49,6 +49,16 @@ struct pf_ctx {
   size_t dl_bytes = 0;
   int dl_slot = 0;
   int dl_last = -1;  // slot of the most recent asynchronous download
+  // asynchronous uploads: a second particle set filled on up_stream and swapped
+  // in by the next call that uses the particles (take_upload)
+  cudaStream_t up_stream = nullptr;
+  cudaEvent_t up_done = nullptr, back_free = nullptr;
+  bool back_free_recorded = false, up_pending = false;
+  float *bpx = nullptr, *bpy = nullptr, *bpz = nullptr, *bvx = nullptr, *bvy = nullptr, *bvz = nullptr;
+  float* bvol = nullptr;
+  uint8_t* btype = nullptr;
+  float* up_staging = nullptr;  // pos and vel, n x 3 each, as uploaded
+  size_t np_next = 0;
 
   // ---- binning ----
   int* tile_count = nullptr;  // [ntiles+1]

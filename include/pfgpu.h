@@ -136,7 +136,7 @@ typedef struct {
 PFGPU_API int pf_create(const pf_grid_desc* desc, pf_ctx** out);
 PFGPU_API int pf_destroy(pf_ctx* ctx);
 PFGPU_API const char* pf_last_error(const pf_ctx* ctx);
-/* Wait for the context's stream and its asynchronous downloads. */
+/* Wait for the context's stream and its asynchronous uploads and downloads. */
 PFGPU_API int pf_sync(pf_ctx* ctx);
 /* The context's stream as an opaque handle (a cudaStream_t). */
 PFGPU_API void* pf_stream(pf_ctx* ctx);
@@ -146,6 +146,13 @@ PFGPU_API void* pf_stream(pf_ctx* ctx);
 PFGPU_API int pf_upload_particles(pf_ctx* ctx, size_t n, const float* pos, const float* vel,
                         const uint8_t* type, const float* volume);
 PFGPU_API int pf_download_particles(pf_ctx* ctx, float* pos, float* vel, uint8_t* type, float* volume);
+/* The same upload without waiting: the copies (host buffers should be pinned
+ * and stay unchanged until pf_sync) and the unpacking run on a second stream
+ * into a second particle set, overlapping the work already queued, e.g. the
+ * current step.  The next call that uses the particles (P2G, markCells, G2P,
+ * advection, a step, a download, another upload) swaps the set in. */
+PFGPU_API int pf_upload_particles_async(pf_ctx* ctx, size_t n, const float* pos, const float* vel,
+                                        const uint8_t* type, const float* volume);
 /* The same copy without waiting for it: the arrays are staged on the device
  * in stream order and copied to the host on a second stream, overlapping the
  * calls that follow (e.g. the next step's upload).  Host buffers should be

@@ -295,3 +295,44 @@ def test_async_download_matches_blocking_download(pf):
         assert np.array_equal(ht.numpy(), sc["type"])
         assert np.array_equal(hw.numpy(), sc["volume"].astype(np.float32))
     g.close()
+
+
+def test_async_upload_swaps_in_before_use(pf):
+    """pf_upload_particles_async fills the second particle set on its own
+    stream; the next call that uses the particles swaps it in.  A transfer
+    step after an async upload equals the same step after a blocking upload,
+    across repeated uploads that alternate the two sets."""
+    import ctypes as C
+
+    import torch
+    n = 16
+    sc = pf.scenes.bubble_tank(n, seed=4)
+    lib = pf.load()
+    np_ = len(sc["pos"])
+    pp = phase_for(sc, pf)
+    ph = pp._c()
+
+    def run(async_upload, k):
+        g = pf.SparseMacGrid3D(n, n, n, 1.0 / n, max_particles=np_)
+        out = None
+        for q in range(k):
+            vel = torch.from_numpy((sc["vel"] * (q + 1)).astype(np.float32)).pin_memory()
+            pos = torch.from_numpy(sc["pos"].astype(np.float32)).pin_memory()
+            typ = torch.from_numpy(sc["type"].astype(np.uint8)).pin_memory()
+            vol = torch.from_numpy(sc["volume"].astype(np.float32)).pin_memory()
+            up = lib.pf_upload_particles_async if async_upload else lib.pf_upload_particles
+            pf._lib.check(up(g.ctx, np_, pos.data_ptr(), vel.data_ptr(), typ.data_ptr(), vol.data_ptr()), g.ctx, "up")
+            pf._lib.check(lib.pf_p2g(g.ctx, C.byref(ph), 1.0), g.ctx, "pf_p2g")
+            pf._lib.check(lib.pf_save_velocity(g.ctx), g.ctx, "pf_save_velocity")
+            pf._lib.check(lib.pf_g2p(g.ctx, None, 0.97, 0.97), g.ctx, "pf_g2p")
+            hv = torch.empty((np_, 3), dtype=torch.float32).pin_memory()
+            pf._lib.check(lib.pf_download_particles_async(g.ctx, None, hv.data_ptr(), None, None), g.ctx, "dl")
+            pf._lib.check(lib.pf_sync(g.ctx), g.ctx, "pf_sync")
+            out = hv.numpy().copy()
+            assert lib.pf_num_particles(g.ctx) == np_
+        g.close()
+        return out
+
+    a, b = run(True, 3), run(False, 3)
+    # the splat's atomics may add in another order: equal to FP32 rounding
+    assert rel_err(a, b) < 1e-6
