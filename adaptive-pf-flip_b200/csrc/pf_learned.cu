@@ -121,6 +121,7 @@ int grid_for(size_t n, int threads = 256) {
 size_t frag_count(int cin, int cout) { return (size_t)27 * (pad16(cin) / 16) * (pad8(cout) / 8) * 32; }
 
 int allow_brick_smem(pf_ctx* ctx);
+int work_ensure(pf_ctx* ctx, Work& W, Dims d0, int B, bool bwd);
 
 int state_init(pf_ctx* ctx, LearnedState* L) {
   size_t o = 0;
@@ -144,7 +145,15 @@ int state_init(pf_ctx* ctx, LearnedState* L) {
   PF_CUDA_TRY(cudaMalloc(&L->wpart, (size_t)kWgradCtas * 27 * 128 * 64 * sizeof(float)));
   PF_CUDA_TRY(cudaMalloc(&L->gstat, 4 * sizeof(double)));
   PF_CUDA_TRY(cudaMemset(L->gstat, 0, 4 * sizeof(double)));
-  return allow_brick_smem(ctx);
+  int rc = allow_brick_smem(ctx);
+  if (rc) return rc;
+  // the solver's working memory for this context's tile lattice, so that no
+  // solve allocates: the gate network and G path, the neighbour-slot table
+  CoarseCtx* c = (CoarseCtx*)ctx->learned;
+  rc = work_ensure(ctx, L->inf, make_dims(c->op.TX, c->op.TY, c->op.TZ), 1, false);
+  if (rc) return rc;
+  int* nbr = nullptr;
+  return build_neighbor_table(ctx, 0, &nbr);
 }
 
 LearnedState* get_state(pf_ctx* ctx, int* rc) {
