@@ -14,7 +14,7 @@ two-level solves (PF_PRECOND_EXACT_COARSE) of seeded pressure systems
 
 Each grid harvests on its own context; the pairs are then merged into one
 context and trained with one optimiser (Adam with gradient-norm clipping,
-16000 steps of batch 8).
+32000 steps of batch 8).
 
     python adaptive-pf-flip_b200/train_coarse_net.py [--out PATH] [--steps N]
 """
@@ -97,7 +97,7 @@ PLAN = (("ellipsoid", 64, 1, 1), ("ellipsoid", 64, 2, 1), ("ellipsoid", 64, 3, 1
         ("bubble", 128, 1, 3), ("bubble", 128, 2, 2), ("rt", 256, 1, 1), ("rt", 128, 2, 3))
 
 
-def train(plan=PLAN, steps=16000, batch=8, seed=11, log=print):
+def train(plan=PLAN, steps=32000, batch=8, seed=11, log=print):
     pf = _package()
     nets, grids, params = {}, {}, None
     exact = pf.SolverConfig(mode=pf.PF_SOLVER_LEARNED, rel_tol=1e-6, precond=pf.PF_PRECOND_EXACT_COARSE)
@@ -150,7 +150,7 @@ def train(plan=PLAN, steps=16000, batch=8, seed=11, log=print):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=DEFAULT_OUT)
-    ap.add_argument("--steps", type=int, default=16000)
+    ap.add_argument("--steps", type=int, default=32000)
     args = ap.parse_args()
     params = train(steps=args.steps)
     os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
