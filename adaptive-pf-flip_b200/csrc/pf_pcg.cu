@@ -244,16 +244,14 @@ __global__ void __launch_bounds__(PF_TV) k_mixed_direction(int nslots, const Sol
   }
 }
 
-// x += e; r64 = b - A x with the exact FP64 operator; max|r64|
-template <typename C>
+// r64 = b - A x with the exact FP64 operator; max|r64|.  x already holds
+// the sweep's correction (k_add_correction, a separate launch: folding it in
+// here would race with the neighbour reads of x).
 __global__ void __launch_bounds__(PF_TV) k_refine_residual(DevGrid G, int nslots, SolveCtl* ctl, const uint8_t* kind,
-                                                           PcgVec<double> v, const double* b, const float* e,
-                                                           double scale, double* partials, int add_e) {
+                                                           PcgVec<double> v, const double* b, double scale,
+                                                           double* partials) {
   __shared__ int nbs[6];
   double rmax = 0.0;
-  // first pass folded into the same sweep would race with neighbour reads, so
-  // x is updated by the caller's previous launch (add_e==1 handled in a
-  // separate kernel); here x is final for this sweep.
   for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
     __syncthreads();
     neighbor_slots(G, s, nbs);
@@ -281,8 +279,6 @@ __global__ void __launch_bounds__(PF_TV) k_refine_residual(DevGrid G, int nslots
     v.r[o] = r;
     rmax = fmax(rmax, fabs(r));
   }
-  (void)e;
-  (void)add_e;
   block_reduce_2(0.0, rmax, partials, ctl, kStageResid);
 }
 
@@ -427,8 +423,8 @@ static int solve_mixed_t(pf_ctx* ctx, int nslots, int nred, const uint8_t* kind,
     if (rc) return rc;
     ++sweeps;
     (++ctx->launches), k_add_correction<<<nred, PF_TV, 0, ctx->stream>>>(nslots, kind, ctx->x, m.e, 1.0);
-    (++ctx->launches), k_refine_residual<C><<<nred, PF_TV, 0, ctx->stream>>>(G, nslots, ctx->ctl, kind, v, ctx->b64, m.e, scale,
-                                                          ctx->partials, 0);
+    (++ctx->launches), k_refine_residual<<<nred, PF_TV, 0, ctx->stream>>>(G, nslots, ctx->ctl, kind, v, ctx->b64, scale,
+                                                                          ctx->partials);
     PF_CUDA_TRY(cudaGetLastError());
     rc = poll(ctx, &c);
     if (rc) return rc;
@@ -436,8 +432,8 @@ static int solve_mixed_t(pf_ctx* ctx, int nslots, int nred, const uint8_t* kind,
       // the sweep made the FP64 residual worse (FP32 recurrences past their
       // accuracy): take it back and stop with the best solution so far
       (++ctx->launches), k_add_correction<<<nred, PF_TV, 0, ctx->stream>>>(nslots, kind, ctx->x, m.e, -1.0);
-      (++ctx->launches), k_refine_residual<C><<<nred, PF_TV, 0, ctx->stream>>>(G, nslots, ctx->ctl, kind, v, ctx->b64,
-                                                                               m.e, scale, ctx->partials, 0);
+      (++ctx->launches), k_refine_residual<<<nred, PF_TV, 0, ctx->stream>>>(G, nslots, ctx->ctl, kind, v, ctx->b64,
+                                                                            scale, ctx->partials);
       PF_CUDA_TRY(cudaGetLastError());
       rc = poll(ctx, &c);
       if (rc) return rc;

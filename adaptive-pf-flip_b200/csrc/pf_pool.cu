@@ -231,8 +231,7 @@ int field_clear(pf_ctx* ctx, int f) {
   if (ctx->nslots > 0)
     PF_CUDA_TRY(cudaMemsetAsync(ctx->fld[f], 0, (size_t)ctx->nslots * PF_TV * sizeof(float), ctx->stream));
   PF_CUDA_TRY(cudaMemsetAsync(ctx->act4[f], 0, ctx->act4_n[f], ctx->stream));
-  if (f <= PF_W) ctx->saved_valid = ctx->saved_valid;  // saved copy is independent
-  return PF_OK;
+  return PF_OK;  // the saved copy is separate storage and stays valid
 }
 
 }  // namespace pf

@@ -41,33 +41,51 @@ __device__ __forceinline__ double grid_coord_g(const Geom& g, float p, double o)
 // ---------------------------------------------------------------------------
 // Binning.  One pass over the particles: the particle's cell (the reference's
 // FP64 (pos - o) / dx, floored and clamped) as a bin key tile * 512 + local
-// cell with a warp-aggregated rank, and a request for the tile of the cell.
+// cell with a rank within the cell, and a request for the tile of the cell.
 // The 4^3 activation is decided later, in the splat (reach bits below); the
 // pool takes the one-tile dilation of the requested tiles, which holds every
 // node a particle's window can reach (within two nodes of its cell).
 // ---------------------------------------------------------------------------
+
+// floor((p - o) / dx) clamped to [0, n): with a power-of-two dx and a zero
+// origin the FP32 product with 1/dx is exact, so its floor is the FP64 one
+__device__ __forceinline__ int bin_cell(const Geom& g, float p, double o, bool fast, float inv_dx_f, int n) {
+  const int c = fast ? (int)floorf(p * inv_dx_f) : (int)floor(grid_coord_g(g, p, o));
+  return min(max(c, 0), n - 1);
+}
+
+// Ranks are aggregated over runs of equal keys in consecutive lanes (the
+// caller's particle order is largely spatial, so a warp's particles fall into
+// a few cells): the run's first lane takes one counter increment for the run.
 __global__ void __launch_bounds__(256) k_bin(DevGrid G, const float* __restrict__ px, const float* __restrict__ py,
                                              const float* __restrict__ pz, int n, int* tile_count, int* pkey,
                                              int* prank, uint8_t* need, int do_bin) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   const unsigned active = __ballot_sync(0xffffffffu, p < n);
   if (p >= n) return;
-  const int ci = min(max((int)floor(grid_coord_g(G.g, px[p], G.g.ox)), 0), G.g.nx - 1);
-  const int cj = min(max((int)floor(grid_coord_g(G.g, py[p], G.g.oy)), 0), G.g.ny - 1);
-  const int ck = min(max((int)floor(grid_coord_g(G.g, pz[p], G.g.oz)), 0), G.g.nz - 1);
+  const bool fast = G.g.dx_pow2 && G.g.ox == 0.0 && G.g.oy == 0.0 && G.g.oz == 0.0;
+  const float inv_dx_f = (float)G.g.inv_dx;
+  const int ci = bin_cell(G.g, px[p], G.g.ox, fast, inv_dx_f, G.g.nx);
+  const int cj = bin_cell(G.g, py[p], G.g.oy, fast, inv_dx_f, G.g.ny);
+  const int ck = bin_cell(G.g, pz[p], G.g.oz, fast, inv_dx_f, G.g.nz);
   const int t = tile_id(G.g, ci >> 3, cj >> 3, ck >> 3);
-  // the lanes of one cell share one counter increment and one tile request
   const int key = t * PF_TV + local_id(ci, cj, ck);
-  const unsigned peers = __match_any_sync(active, key);
-  const int lane = threadIdx.x & 31, leader = __ffs(peers) - 1;
+  // active lanes are a prefix of the warp; a run starts where the key changes
+  const int lane = threadIdx.x & 31;
+  const int prev = __shfl_up_sync(active, key, 1);
+  const unsigned heads = __ballot_sync(active, lane == 0 || prev != key);
+  const unsigned upto = 0xffffffffu >> (31 - lane);  // lanes 0..lane
+  const int start = 31 - __clz(heads & upto);
+  const unsigned after = heads & ~upto & active;     // heads past this lane
+  const int stop = after ? __ffs(after) - 1 : 32 - __clz(active);
   if (do_bin) {
     int base = 0;
-    if (lane == leader) base = atomicAdd(&tile_count[key], __popc(peers));
-    base = __shfl_sync(peers, base, leader);
+    if (lane == start) base = atomicAdd(&tile_count[key], stop - start);
+    base = __shfl_sync(active, base, start);
     pkey[p] = key;
-    prank[p] = base + __popc(peers & ((1u << lane) - 1u));
+    prank[p] = base + (lane - start);
   }
-  if (lane == leader && !need[t]) need[t] = 1;
+  if (lane == start && !need[t]) need[t] = 1;
 }
 
 // need <- the one-tile dilation of need (through the int scratch `tmp`)
@@ -178,17 +196,6 @@ __device__ __forceinline__ f32x2 f2_pack(float lo, float hi) {
 __device__ __forceinline__ void f2_unpack(f32x2 v, float& lo, float& hi) {
   asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
 }
-__device__ __forceinline__ f32x2 f2_add(f32x2 a, f32x2 b) {
-  f32x2 d;
-  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-  return d;
-}
-// the same add, never merged with an identical earlier one (forces a recomputation)
-__device__ __forceinline__ f32x2 f2_add_again(f32x2 a, f32x2 b) {
-  f32x2 d;
-  asm volatile("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-  return d;
-}
 __device__ __forceinline__ f32x2 f2_sub(f32x2 a, f32x2 b) {
   f32x2 d;
   asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
@@ -205,19 +212,12 @@ __device__ __forceinline__ f32x2 f2_fma(f32x2 a, f32x2 b, f32x2 c) {
   return d;
 }
 
-__device__ __forceinline__ float cubic(float s) {
-  const float t = 1.0f - s;
-  return t > 0.0f ? t * t * t : 0.0f;
+// t = min(max(a - b, 0), 1): one saturating subtract
+__device__ __forceinline__ float sub_sat(float a, float b) {
+  float d;
+  asm("sub.rn.sat.f32 %0, %1, %2;" : "=f"(d) : "f"(a), "f"(b));
+  return d;
 }
-
-// d^2/r^2 of node `node` for coordinate g (both box-local), 2 (weight 0, out
-// of the weight sum, never reached) when the node is off the field's lattice
-// [lo, hi).
-__device__ __forceinline__ float node_a(float g, int node, int lo, int hi) {
-  const float d = g - (float)node;
-  return (node >= lo && node < hi) ? d * d * (1.0f / 2.25f) : 2.0f;
-}
-
 // The FP64 decision for one particle and field: bit x + 2y + 4z for window
 // block (x, y, z), where window block 0 along an axis holds the window nodes
 // before the split s of that axis.  n[] are the global first window nodes.
@@ -253,32 +253,127 @@ __device__ unsigned exact_reach(const DevGrid& G, float ppx, float ppy, float pp
   return r;
 }
 
-// Returns the cell's reached blocks as bits of the tile's 4x4x4 block box.
+// Window geometry of one cell for face field A.  The window is 4 nodes along
+// the field's normal axis L = A and 3 along the transverse axes S1 < S2.
+template <int A>
+struct SplatWindow {
+  static constexpr int S1 = A == 0 ? 1 : 0, S2 = A == 2 ? 1 : 2;
+  int b[3];      // box-local first window node (the cell minus one) per axis
+  int n[3];      // global first window node per axis
+  int sp[3];     // window nodes before the 4^3 block boundary per axis
+  unsigned off;  // bit 4*axis + i: node i off the field's lattice
+
+  __device__ __forceinline__ SplatWindow(const DevGrid& G, int cl, int o0, int o1, int o2, bool edge) {
+    const int o[3] = {o0, o1, o2};
+    b[0] = (cl & 7) + 1;
+    b[1] = ((cl >> 3) & 7) + 1;
+    b[2] = (cl >> 6) + 1;
+    off = 0u;
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+      n[ax] = o[ax] + b[ax];
+      sp[ax] = min(4 - (n[ax] & 3), ax == A ? 4 : 3);
+      // only tiles at the domain's faces have window nodes off the lattice
+      if (edge)
+#pragma unroll
+        for (int i = 0; i < (ax == A ? 4 : 3); ++i)
+          if (n[ax] + i < 0 || n[ax] + i >= G.g.fdim[PF_U + A][ax]) off |= 1u << (4 * ax + i);
+    }
+  }
+
+  // Coordinates g relative to the first window node (transverse ones shifted
+  // by -1/2 onto the node lattice) and a = d^2/r^2 for window node i, d = g - i.
+  // With a power-of-two dx and a zero origin the product with 1/dx is exact
+  // and the FMA rounds X/dx - n once: the FP64 value rounded to float.  Nodes
+  // off the lattice get a = 2 (weight 0, never reached).
+  __device__ __forceinline__ void coords(const DevGrid& G, float X, float Y, float Z, bool fast, float inv_dx_f,
+                                         double inv_dx, bool edge, float (&g)[3], float (&a)[3][4]) const {
+    if (fast) {
+      g[0] = fmaf(X, inv_dx_f, (float)-n[0]);
+      g[1] = fmaf(Y, inv_dx_f, (float)-n[1]);
+      g[2] = fmaf(Z, inv_dx_f, (float)-n[2]);
+    } else {
+      g[0] = (float)(((double)X - G.g.ox) * inv_dx - n[0]);
+      g[1] = (float)(((double)Y - G.g.oy) * inv_dx - n[1]);
+      g[2] = (float)(((double)Z - G.g.oz) * inv_dx - n[2]);
+    }
+    const f32x2 k2 = f2_pack(1.0f / 2.25f, 1.0f / 2.25f);
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+      if (ax != A) g[ax] -= 0.5f;
+      const f32x2 gg = f2_pack(g[ax], g[ax]);
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const f32x2 d = f2_sub(gg, f2_pack((float)(2 * h), (float)(2 * h + 1)));
+        f2_unpack(f2_mul(f2_mul(d, d), k2), a[ax][2 * h], a[ax][2 * h + 1]);
+      }
+    }
+    if (edge) {
+#pragma unroll
+      for (int ax = 0; ax < 3; ++ax)
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          if ((off >> (4 * ax + i)) & 1u) a[ax][i] = 2.0f;
+    }
+  }
+
+  // FP32 activation from the per-axis minima of a over each window block: sets
+  // the bits of the blocks reached clear of the threshold, returns whether a
+  // block lies within kReachEps of it (decided in FP64 afterwards).
+  __device__ __forceinline__ bool reach32(const float (&a)[3][4], unsigned& reach) const {
+    float mn[3][2];
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+      mn[ax][0] = mn[ax][1] = 4.0f;
+#pragma unroll
+      for (int i = 0; i < (ax == A ? 4 : 3); ++i) {
+        if (i < sp[ax]) mn[ax][0] = fminf(mn[ax][0], a[ax][i]);
+        else mn[ax][1] = fminf(mn[ax][1], a[ax][i]);
+      }
+    }
+    bool band = false;
+#pragma unroll
+    for (int z = 0; z < 2; ++z)
+#pragma unroll
+      for (int y = 0; y < 2; ++y)
+#pragma unroll
+        for (int x = 0; x < 2; ++x) {
+          const float sa = (mn[0][x] + mn[1][y]) + mn[2][z];
+          if (sa < 1.0f - kReachEps) reach |= 1u << (x + 2 * y + 4 * z);
+          band = band || fabsf(sa - 1.0f) <= kReachEps;
+        }
+    return band;
+  }
+};
+
+// Splat of one cell's particles into face field A; returns the cell's reached
+// blocks as bits of the tile's 4x4x4 block box.
+//
+// Nodes are held in pairs along L, so one packed f32x2 instruction serves two
+// nodes: node pair h of transverse node (s1, s2) is accumulator
+// q = 2*(3*s2 + s1) + h, L nodes 2h and 2h + 1.  Per node and particle the
+// weight is w = t^3 with t = sat((1 - a_L) - (a_S1 + a_S2)), i.e.
+// 1 - d^2/r^2 clamped at 0 (t <= 1 holds by itself).  The weight sum is one
+// pass over the window, the accumulation a second one that recomputes the
+// weights, which is cheaper than holding 36 of them in registers.  Particles
+// near a block's threshold are decided in FP64 after the cell's window has
+// been added to the shared box, outside the register-heavy loop.
 template <int A>
 __device__ __forceinline__ unsigned long long splat_cell(const DevGrid& G, float* sm, int cl, int beg, int end,
                                            const int* __restrict__ perm, const float* __restrict__ px,
                                            const float* __restrict__ py, const float* __restrict__ pz,
                                            const float* __restrict__ vA, const uint8_t* __restrict__ type,
                                            const float* __restrict__ vol, float m_l, float m_g, int o0, int o1,
-                                           int o2, double inv_dx) {
-  constexpr int NX = A == 0 ? 4 : 3, NY = A == 1 ? 4 : 3, NZ = A == 2 ? 4 : 3;
-  constexpr int NW = NX * NY * NZ;  // 36
-  // box-local cell coordinates and the window's first node
-  const int cx = (cl & 7) + 2, cy = ((cl >> 3) & 7) + 2, cz = (cl >> 6) + 2;
-  const int bx = cx - 1, by = cy - 1, bz = cz - 1;
-  const int fv = PF_U + A;
-  const int lox = -o0, hix = G.g.fdim[fv][0] - o0;
-  const int loy = -o1, hiy = G.g.fdim[fv][1] - o1;
-  const int loz = -o2, hiz = G.g.fdim[fv][2] - o2;
-  // global first window node per axis and the split between its two blocks
-  const int n[3] = {o0 + bx, o1 + by, o2 + bz};
-  const int sp[3] = {min(4 - (n[0] & 3), NX), min(4 - (n[1] & 3), NY), min(4 - (n[2] & 3), NZ)};
-  // window accumulators, two nodes per register pair (node e = (k*NY + j)*NX + i)
-  constexpr int NP = NW / 2;
+                                           int o2, double inv_dx, float inv_dx_f, bool fast, bool edge) {
+  using W = SplatWindow<A>;
+  constexpr int NP = 18;  // node pairs: 9 transverse nodes x 2 pairs along L
+  const W win(G, cl, o0, o1, o2, edge);
   f32x2 am[NP], ap[NP];
 #pragma unroll
   for (int q = 0; q < NP; ++q) { am[q] = 0ull; ap[q] = 0ull; }
   unsigned reach = 0u;
+  bool banded = false;
+  const f32x2 one2 = f2_pack(1.0f, 1.0f);
   // the next particle's attributes are loaded while this one is splatted
   int pn = perm[beg];
   float xn = px[pn], yn = py[pn], zn = pz[pn], vn = vA[pn], voln = vol[pn];
@@ -295,83 +390,52 @@ __device__ __forceinline__ unsigned long long splat_cell(const DevGrid& G, float
       voln = vol[pn];
       tn = type[pn];
     }
-    float gx = (float)(((double)X - G.g.ox) * inv_dx - o0);
-    float gy = (float)(((double)Y - G.g.oy) * inv_dx - o1);
-    float gz = (float)(((double)Z - G.g.oz) * inv_dx - o2);
-    if (A != 0) gx -= 0.5f;
-    if (A != 1) gy -= 0.5f;
-    if (A != 2) gz -= 0.5f;
-    float ax[NX], ay[NY], az[NZ];
+    float g[3], a[3][4];
+    win.coords(G, X, Y, Z, fast, inv_dx_f, inv_dx, edge, g, a);
+    banded |= win.reach32(a, reach);
+    // 1 - a along L, and a_S1 + a_S2 per transverse node
+    f32x2 om2[2];
 #pragma unroll
-    for (int i = 0; i < NX; ++i) ax[i] = node_a(gx, bx + i, lox, hix);
+    for (int h = 0; h < 2; ++h) om2[h] = f2_sub(one2, f2_pack(a[A][2 * h], a[A][2 * h + 1]));
+    float om[4];
+    f2_unpack(om2[0], om[0], om[1]);
+    f2_unpack(om2[1], om[2], om[3]);
+    float at[9];
 #pragma unroll
-    for (int j = 0; j < NY; ++j) ay[j] = node_a(gy, by + j, loy, hiy);
+    for (int s2 = 0; s2 < 3; ++s2)
 #pragma unroll
-    for (int k = 0; k < NZ; ++k) az[k] = node_a(gz, bz + k, loz, hiz);
-    // activation: per-axis minima over each window block
-    float mx0 = 4.0f, mx1 = 4.0f, my0 = 4.0f, my1 = 4.0f, mz0 = 4.0f, mz1 = 4.0f;
+      for (int s1 = 0; s1 < 3; ++s1) at[3 * s2 + s1] = a[W::S1][s1] + a[W::S2][s2];
+    // pass 1: the weight sum.  Along L the particle sits in [1, 2) from the
+    // first window node, so node 0 (d = g) and node 3 (d = 3 - g) are never
+    // both inside r = 1.5: three L nodes per row carry all the weight.
+    const float oe = g[A] < 1.5f ? om[0] : om[3];
+    float ws0 = 0.0f, ws1 = 0.0f, ws2 = 0.0f;
 #pragma unroll
-    for (int i = 0; i < NX; ++i) {
-      if (i < sp[0]) mx0 = fminf(mx0, ax[i]);
-      else mx1 = fminf(mx1, ax[i]);
+    for (int r = 0; r < 9; ++r) {
+      const float t0 = sub_sat(oe, at[r]), t1 = sub_sat(om[1], at[r]), t2 = sub_sat(om[2], at[r]);
+      ws0 = fmaf(t0 * t0, t0, ws0);
+      ws1 = fmaf(t1 * t1, t1, ws1);
+      ws2 = fmaf(t2 * t2, t2, ws2);
     }
-#pragma unroll
-    for (int j = 0; j < NY; ++j) {
-      if (j < sp[1]) my0 = fminf(my0, ay[j]);
-      else my1 = fminf(my1, ay[j]);
-    }
-#pragma unroll
-    for (int k = 0; k < NZ; ++k) {
-      if (k < sp[2]) mz0 = fminf(mz0, az[k]);
-      else mz1 = fminf(mz1, az[k]);
-    }
-    bool band = false;
-#pragma unroll
-    for (int z = 0; z < 2; ++z)
-#pragma unroll
-      for (int y = 0; y < 2; ++y)
-#pragma unroll
-        for (int x = 0; x < 2; ++x) {
-          const float sa = ((x ? mx1 : mx0) + (y ? my1 : my0)) + (z ? mz1 : mz0);
-          if (sa < 1.0f - kReachEps) reach |= 1u << (x + 2 * y + 4 * z);
-          band = band || fabsf(sa - 1.0f) <= kReachEps;
-        }
-    if (band) reach |= exact_reach<A>(G, X, Y, Z, n, sp);
-    // weights w = max(1 - (ax + (ay + az)), 0)^3, two nodes per packed instruction
-    float ayz[NY * NZ];
-#pragma unroll
-    for (int k = 0; k < NZ; ++k)
-#pragma unroll
-      for (int j = 0; j < NY; ++j) ayz[k * NY + j] = ay[j] + az[k];
-    // two passes over the window: the weight sum, then the accumulation with
-    // the weights recomputed (cheaper than holding 36 of them in registers)
-    const f32x2 one2 = f2_pack(1.0f, 1.0f);
-    auto weight = [&](int q, bool again) {
-      const int e0 = 2 * q, e1 = 2 * q + 1;
-      const f32x2 a2 = f2_pack(ax[e0 % NX], ax[e1 % NX]), b2 = f2_pack(ayz[e0 / NX], ayz[e1 / NX]);
-      const f32x2 sa = again ? f2_add_again(a2, b2) : f2_add(a2, b2);
-      float t0, t1;
-      f2_unpack(f2_sub(one2, sa), t0, t1);
-      const f32x2 t = f2_pack(fmaxf(t0, 0.0f), fmaxf(t1, 0.0f));
-      return f2_mul(f2_mul(t, t), t);
-    };
-    f32x2 wsum2 = 0ull;
-#pragma unroll
-    for (int q = 0; q < NP; ++q) wsum2 = f2_add(wsum2, weight(q, false));
-    float ws0, ws1;
-    f2_unpack(wsum2, ws0, ws1);
-    const float wsum = ws0 + ws1;
+    const float wsum = (ws0 + ws1) + ws2;
     if (!(wsum > 0.0f)) continue;
     const float mp = (TY == 0 ? m_l : m_g) * VOL;
-    const float sm_ = mp / wsum;
-    const float sp_ = sm_ * VA;
-    const f32x2 sm2 = f2_pack(sm_, sm_), sp2 = f2_pack(sp_, sp_);
+    const float s_m = __fdividef(mp, wsum);
+    const float s_p = s_m * VA;
+    const f32x2 sm2 = f2_pack(s_m, s_m), sp2 = f2_pack(s_p, s_p);
+    // pass 2: the accumulation over the whole window, two L nodes per packed
+    // instruction (t clamped at 0 lane by lane; t <= 1 already)
 #pragma unroll
-    for (int q = 0; q < NP; ++q) {
-      const f32x2 wq = weight(q, true);
-      am[q] = f2_fma(wq, sm2, am[q]);
-      ap[q] = f2_fma(wq, sp2, ap[q]);
-    }
+    for (int r = 0; r < 9; ++r)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        float s0, s1;
+        f2_unpack(f2_sub(om2[h], f2_pack(at[r], at[r])), s0, s1);
+        const f32x2 t = f2_pack(fmaxf(s0, 0.0f), fmaxf(s1, 0.0f));
+        const f32x2 w = f2_mul(f2_mul(t, t), t);
+        am[2 * r + h] = f2_fma(w, sm2, am[2 * r + h]);
+        ap[2 * r + h] = f2_fma(w, sp2, ap[2 * r + h]);
+      }
   }
   float* smom = sm + (2 * A) * kBox3;
   float* smas = sm + (2 * A + 1) * kBox3;
@@ -381,21 +445,34 @@ __device__ __forceinline__ unsigned long long splat_cell(const DevGrid& G, float
     f2_unpack(am[q], m2[0], m2[1]);
     f2_unpack(ap[q], p2[0], p2[1]);
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int e = 2 * q + h, i = e % NX, j = (e / NX) % NY, k = e / (NX * NY);
-      if (m2[h] != 0.0f || p2[h] != 0.0f) {
-        const int si = (bx + i) + kBox * ((by + j) + kBox * (bz + k));
-        atomicAdd(&smom[si], p2[h]);
-        atomicAdd(&smas[si], m2[h]);
+    for (int e = 0; e < 2; ++e) {
+      if (m2[e] != 0.0f || p2[e] != 0.0f) {
+        int idx[3];
+        idx[A] = 2 * (q & 1) + e;
+        idx[W::S1] = (q >> 1) % 3;
+        idx[W::S2] = (q >> 1) / 3;
+        const int si = (win.b[0] + idx[0]) + kBox * ((win.b[1] + idx[1]) + kBox * (win.b[2] + idx[2]));
+        atomicAdd(&smom[si], p2[e]);
+        atomicAdd(&smas[si], m2[e]);
       }
     }
   }
+  // particles with a block inside the FP32 band: the reference's FP64 decision
+  if (banded) {
+    for (int q = beg; q < end; ++q) {
+      const int p = perm[q];
+      float g[3], a[3][4];
+      unsigned dummy = 0u;
+      win.coords(G, px[p], py[p], pz[p], fast, inv_dx_f, inv_dx, edge, g, a);
+      if (win.reach32(a, dummy)) reach |= exact_reach<A>(G, px[p], py[p], pz[p], win.n, win.sp);
+    }
+  }
   // reached window blocks -> the tile's 4x4x4 block box (block of node o -> (o >> 2) - (o0 >> 2))
-  const int w0 = (n[0] >> 2) - (o0 >> 2), w1 = (n[1] >> 2) - (o1 >> 2), w2 = (n[2] >> 2) - (o2 >> 2);
+  const int w0 = (win.n[0] >> 2) - (o0 >> 2), w1 = (win.n[1] >> 2) - (o1 >> 2), w2 = (win.n[2] >> 2) - (o2 >> 2);
   unsigned long long box = 0ull;
 #pragma unroll
-  for (int b = 0; b < 8; ++b)
-    if ((reach >> b) & 1u) box |= 1ull << ((w0 + (b & 1)) + 4 * ((w1 + ((b >> 1) & 1)) + 4 * (w2 + (b >> 2))));
+  for (int bb = 0; bb < 8; ++bb)
+    if ((reach >> bb) & 1u) box |= 1ull << ((w0 + (bb & 1)) + 4 * ((w1 + ((bb >> 1) & 1)) + 4 * (w2 + (bb >> 2))));
   return box;
 }
 
@@ -420,13 +497,21 @@ __global__ void __launch_bounds__(kSplatThreads, 2) k_splat(DevGrid G, const int
   const int tx = t % G.g.TX, tq = t / G.g.TX, ty = tq % G.g.TY, tz = tq / G.g.TY;
   const int o0 = tx * 8 - 2, o1 = ty * 8 - 2, o2 = tz * 8 - 2;
   const double inv_dx = G.g.inv_dx;
+  const float inv_dx_f = (float)inv_dx;
+  const bool fast = G.g.dx_pow2 && G.g.ox == 0.0 && G.g.oy == 0.0 && G.g.oz == 0.0;
+  // window nodes of this tile's cells span global nodes 8t - 1 .. 8t + 9 per axis
+  const bool edge = tx == 0 || ty == 0 || tz == 0 || tx * 8 + 10 > G.g.nx || ty * 8 + 10 > G.g.ny ||
+                    tz * 8 + 10 > G.g.nz;
   unsigned long long box[3] = {0ull, 0ull, 0ull};  // reached blocks of this thread's cells
   for (int cl = threadIdx.x; cl < PF_TV; cl += kSplatThreads) {
     const int beg = cs[cl], end = cs[cl + 1];
     if (beg >= end) continue;
-    box[0] |= splat_cell<0>(G, sm, cl, beg, end, perm, px, py, pz, vx, type, vol, m_l, m_g, o0, o1, o2, inv_dx);
-    box[1] |= splat_cell<1>(G, sm, cl, beg, end, perm, px, py, pz, vy, type, vol, m_l, m_g, o0, o1, o2, inv_dx);
-    box[2] |= splat_cell<2>(G, sm, cl, beg, end, perm, px, py, pz, vz, type, vol, m_l, m_g, o0, o1, o2, inv_dx);
+    box[0] |= splat_cell<0>(G, sm, cl, beg, end, perm, px, py, pz, vx, type, vol, m_l, m_g, o0, o1, o2, inv_dx,
+                             inv_dx_f, fast, edge);
+    box[1] |= splat_cell<1>(G, sm, cl, beg, end, perm, px, py, pz, vy, type, vol, m_l, m_g, o0, o1, o2, inv_dx,
+                             inv_dx_f, fast, edge);
+    box[2] |= splat_cell<2>(G, sm, cl, beg, end, perm, px, py, pz, vz, type, vol, m_l, m_g, o0, o1, o2, inv_dx,
+                             inv_dx_f, fast, edge);
   }
   // one shared OR per warp and word
 #pragma unroll

@@ -1,13 +1,15 @@
 """GPU projection and full-step parity against the CPU oracle.
 
 Restates tests/test_sparse_vc3d.cpp (divergence removal, c_div target,
-pressure block count) on the GPU drop-in, then compares the GPU solve with the
-oracle on identical grids and the full step over 10 steps.
+pressure block count) and tests/test_pressure3d_vc.cpp (beta = 1 box,
+hydrostatic two-phase column) on the GPU drop-in, then compares the GPU solve
+with the oracle on identical grids and the full step over 10 steps.
 """
 import numpy as np
 import pytest
 
 import oracle as O
+import vc_cases
 from gpu_helpers import compare_grids, phase_for, rel_err, scene_particles, to_oracle_phase
 
 pytestmark = pytest.mark.gpu
@@ -184,3 +186,29 @@ def test_full_step_ten_steps_match_oracle(pf):
             assert nact == 0, f"step {step} {name}: {nact} activity flags differ"
             assert err <= max(1e-5, 10 * e_self) and err < 2e-3, f"step {step} {name}: {err} (self {e_self})"
     print("worst relative field error over 10 steps:", {k: f"{v:.2e}" for k, v in worst.items()})
+
+
+@pytest.mark.parametrize("case,shape,iters", [("beta_one_box", (8, 8, 8), 1000),
+                                              ("hydrostatic_two_phase", (6, 16, 6), 2000)])
+def test_vc_reference_cases_match_oracle(pf, case, shape, iters):
+    # tests/test_pressure3d_vc.cpp:5-32 on both grids, GPU against the oracle
+    g, go = pf.SparseMacGrid3D(*shape, 1.0), O.OracleGrid(*shape, 1.0)
+    dt = getattr(vc_cases, case)(g)
+    getattr(vc_cases, case)(go)
+    st = pf.spProjectStepVC3D(g, pf.PhaseParams(*vc_cases.PHASE), dt, iters, 1e-10)
+    sto = O.Oracle().project(go, O.PhaseParams(*vc_cases.PHASE), dt, iters, 1e-10)
+    assert st.converged and sto.converged
+    assert st.pin_cell == sto.pin_cell
+    assert vc_cases.fluid_divergence(g) < 1e-4
+    if case == "hydrostatic_two_phase":
+        assert vc_cases.interior_max_v(g) < 0.6
+    for name, (_, nact) in compare_grids(g, go, (0, 1, 2, 6)).items():
+        assert nact == 0, f"{name}: activity differs"
+    # velocities against their common scale (u and w stay at rounding noise
+    # in the hydrostatic column), pressure against its own
+    vel = [(g.get_field(f)[0].astype(np.float64), go.get_field(f)[0].astype(np.float64)) for f in (0, 1, 2)]
+    vscale = max(float(np.max(np.abs(b))) for _, b in vel)
+    for f, (a, b) in zip("uvw", vel):
+        assert np.max(np.abs(a - b)) <= 1e-5 * vscale, f
+    assert rel_err(g.get_field(pf.PF_P)[0], go.get_field(O.P)[0]) < 1e-5
+    g.close()

@@ -6,7 +6,7 @@
    scenes, when that library is present: bit-for-bit for P2G, projection,
    G2P, advection with escape records, and whole steps.
 3. The reference's own inline known-answer tests, restated on the oracle
-   (tests/test_sparse_transfer3d_tp.cpp, test_sparse_vc3d.cpp,
+   (tests/test_sparse_transfer3d_tp.cpp, test_sparse_vc3d.cpp, test_pressure3d_vc.cpp,
    test_phasefield.cpp, test_block_color.cpp).
 """
 import json
@@ -17,6 +17,7 @@ import numpy as np
 import pytest
 
 import oracle as O
+import vc_cases
 from conftest import ROOT
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
@@ -304,6 +305,24 @@ def test_vc_projection_target_cdiv():
     g = _box(False)
     O.Oracle().project(g, O.PhaseParams(), 1.0, 1000, 1e-9, c_div=0.125)
     assert _divergence(g).mean() == pytest.approx(0.125, rel=1e-4)
+
+
+def test_vc_beta_one_box_removes_divergence():
+    # tests/test_pressure3d_vc.cpp:5-16
+    g = O.OracleGrid(8, 8, 8, 1.0)
+    dt = vc_cases.beta_one_box(g)
+    st = O.Oracle().project(g, O.PhaseParams(*vc_cases.PHASE), dt, 1000, 1e-10)
+    assert st.converged
+    assert vc_cases.fluid_divergence(g) < 1e-5
+
+
+def test_vc_hydrostatic_two_phase_bounded():
+    # tests/test_pressure3d_vc.cpp:17-32
+    g = O.OracleGrid(6, 16, 6, 1.0)
+    dt = vc_cases.hydrostatic_two_phase(g)
+    st = O.Oracle().project(g, O.PhaseParams(*vc_cases.PHASE), dt, 2000, 1e-10)
+    assert st.converged and st.pin_cell >= 0
+    assert vc_cases.interior_max_v(g) < 0.6
 
 
 def test_relative_tolerance_rule_and_stats():
