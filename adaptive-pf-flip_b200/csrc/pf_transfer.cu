@@ -26,6 +26,14 @@ namespace {
 constexpr double kR2 = 2.25;  // KR*KR with KR = 1.5 (sparse_ops3d_tp.cpp:21)
 constexpr int kBox = 12;      // shared box edge: tile (8) + halo 2 below, 2 above
 constexpr int kBox3 = kBox * kBox * kBox;
+// Shared box of one face field: each x row holds the 12 momentum nodes and
+// then the 12 mass nodes, so a row is 24 floats.  The splat's flush adds, per
+// instruction, one window offset for a warp's 32 cells (8 along x, 4 rows
+// along y): with a row pitch of 24 words those land in 32 distinct banks, for
+// momentum (x + 24y) and for mass (x + 12 + 24y) alike.
+constexpr int kRow = 2 * kBox;
+constexpr int kFieldBox = kRow * kBox * kBox;  // floats per face field
+__device__ __forceinline__ int box_mom(int X, int Y, int Z) { return X + kRow * (Y + kBox * Z); }
 
 // grid coordinate (pos - o)/dx in the reference's double arithmetic
 __device__ __forceinline__ double grid_coord(float p, double o, double dx) {
@@ -57,41 +65,90 @@ __device__ __forceinline__ int bin_cell(const Geom& g, float p, double o, bool f
 // Ranks are aggregated over runs of equal keys in consecutive lanes (the
 // caller's particle order is largely spatial, so a warp's particles fall into
 // a few cells): the run's first lane takes one counter increment for the run.
+// A warp bins kBinPer consecutive 32-particle groups and issues all their
+// loads, then all their counter increments, before it waits: the kernel is
+// bound by the latency of those round trips, not by bandwidth.  With DO_BIN
+// the tiles to pool are read off the counts afterwards (k_need_from_counts);
+// without it (cell marking) the run leaders request their cells' tiles.
+constexpr int kBinPer = 4;
+
+template <bool DO_BIN>
 __global__ void __launch_bounds__(256) k_bin(DevGrid G, const float* __restrict__ px, const float* __restrict__ py,
                                              const float* __restrict__ pz, int n, int* tile_count, int* pkey,
-                                             int* prank, uint8_t* need, int do_bin) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  const unsigned active = __ballot_sync(0xffffffffu, p < n);
-  if (p >= n) return;
+                                             int* prank, uint8_t* need) {
+  const int lane = threadIdx.x & 31;
+  const long long first = ((long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31)) * kBinPer;
   const bool fast = G.g.dx_pow2 && G.g.ox == 0.0 && G.g.oy == 0.0 && G.g.oz == 0.0;
   const float inv_dx_f = (float)G.g.inv_dx;
-  const int ci = bin_cell(G.g, px[p], G.g.ox, fast, inv_dx_f, G.g.nx);
-  const int cj = bin_cell(G.g, py[p], G.g.oy, fast, inv_dx_f, G.g.ny);
-  const int ck = bin_cell(G.g, pz[p], G.g.oz, fast, inv_dx_f, G.g.nz);
-  const int t = tile_id(G.g, ci >> 3, cj >> 3, ck >> 3);
-  const int key = t * PF_TV + local_id(ci, cj, ck);
-  // active lanes are a prefix of the warp; a run starts where the key changes
-  const int lane = threadIdx.x & 31;
-  const int prev = __shfl_up_sync(active, key, 1);
-  const unsigned heads = __ballot_sync(active, lane == 0 || prev != key);
-  const unsigned upto = 0xffffffffu >> (31 - lane);  // lanes 0..lane
-  const int start = 31 - __clz(heads & upto);
-  const unsigned after = heads & ~upto & active;     // heads past this lane
-  const int stop = after ? __ffs(after) - 1 : 32 - __clz(active);
-  if (do_bin) {
-    int base = 0;
-    if (lane == start) base = atomicAdd(&tile_count[key], stop - start);
-    base = __shfl_sync(active, base, start);
-    pkey[p] = key;
-    prank[p] = base + (lane - start);
+  float x[kBinPer], y[kBinPer], z[kBinPer];
+#pragma unroll
+  for (int u = 0; u < kBinPer; ++u) {
+    const long long p = first + 32 * u + lane;
+    x[u] = y[u] = z[u] = 0.0f;
+    if (p < n) {
+      x[u] = px[p];
+      y[u] = py[p];
+      z[u] = pz[p];
+    }
   }
-  if (lane == start && !need[t]) need[t] = 1;
+  int key[kBinPer], start[kBinPer], base[kBinPer], tile[kBinPer];
+  bool lead[kBinPer];
+#pragma unroll
+  for (int u = 0; u < kBinPer; ++u) {
+    const long long p = first + 32 * u + lane;
+    const int ci = bin_cell(G.g, x[u], G.g.ox, fast, inv_dx_f, G.g.nx);
+    const int cj = bin_cell(G.g, y[u], G.g.oy, fast, inv_dx_f, G.g.ny);
+    const int ck = bin_cell(G.g, z[u], G.g.oz, fast, inv_dx_f, G.g.nz);
+    tile[u] = tile_id(G.g, ci >> 3, cj >> 3, ck >> 3);
+    key[u] = tile[u] * PF_TV + local_id(ci, cj, ck);
+    // the particles of this group are a prefix of the warp; a run starts where the key changes
+    const unsigned valid = __ballot_sync(0xffffffffu, p < n);
+    const int prev = __shfl_up_sync(0xffffffffu, key[u], 1);
+    const unsigned heads = __ballot_sync(0xffffffffu, p < n && (lane == 0 || prev != key[u]));
+    const unsigned upto = 0xffffffffu >> (31 - lane);  // lanes 0..lane
+    start[u] = 31 - __clz(heads & upto | 1u);
+    const unsigned after = heads & ~upto;              // heads past this lane
+    const int stop = after ? __ffs(after) - 1 : 32 - __clz(valid);
+    base[u] = 0;
+    lead[u] = p < n && lane == start[u];
+    if (DO_BIN && lead[u]) base[u] = atomicAdd(&tile_count[key[u]], stop - start[u]);
+  }
+  if constexpr (DO_BIN) {
+#pragma unroll
+    for (int u = 0; u < kBinPer; ++u) {
+      const long long p = first + 32 * u + lane;
+      const int b = __shfl_sync(0xffffffffu, base[u], start[u]);
+      if (p < n) {
+        pkey[p] = key[u];
+        prank[p] = b + (lane - start[u]);
+      }
+    }
+  } else {
+    // a byte is stored only when it reads 0 (stores to hot bytes queue in L2)
+    uint8_t seen[kBinPer];
+#pragma unroll
+    for (int u = 0; u < kBinPer; ++u) seen[u] = lead[u] ? need[tile[u]] : 1;
+#pragma unroll
+    for (int u = 0; u < kBinPer; ++u)
+      if (!seen[u]) need[tile[u]] = 1;
+  }
 }
 
-// need <- the one-tile dilation of need (through the int scratch `tmp`)
-__global__ void k_need_snapshot(const uint8_t* need, int* tmp, int n) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < n) tmp[t] = need[t];
+// need <- the one-tile dilation of the tiles holding particles: tmp[t] =
+// need[t] or any particle binned into tile t (one warp per tile over its 512
+// cell counts), then k_need_dilate
+__global__ void k_need_from_counts(const int* __restrict__ tile_count, const uint8_t* need, int* tmp, int ntiles) {
+  const int t = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (t >= ntiles) return;
+  const int4* c = reinterpret_cast<const int4*>(tile_count + (size_t)t * PF_TV);
+  int any = 0;
+#pragma unroll
+  for (int q = 0; q < PF_TV / 128; ++q) {
+    const int4 v = c[q * 32 + lane];
+    any |= v.x | v.y | v.z | v.w;
+  }
+  any = __any_sync(0xffffffffu, any != 0);
+  if (lane == 0) tmp[t] = any || need[t];
 }
 
 __global__ void k_need_dilate(Geom g, const int* tmp, uint8_t* need) {
@@ -108,10 +165,25 @@ __global__ void k_need_dilate(Geom g, const int* tmp, uint8_t* need) {
   if (any) need[t] = 1;
 }
 
+// perm[start of the particle's cell + its rank] = particle, kBinPer per thread
+// with all gathers issued before the scatters
 __global__ void k_bin_scatter(const int* __restrict__ pkey, const int* __restrict__ prank,
                               const int* __restrict__ tile_start, int* perm, int n) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p < n) perm[tile_start[pkey[p]] + prank[p]] = p;
+  const long long first = (long long)blockIdx.x * blockDim.x * kBinPer + threadIdx.x;
+  int key[kBinPer], rank[kBinPer], at[kBinPer];
+#pragma unroll
+  for (int u = 0; u < kBinPer; ++u) {
+    const long long p = first + (long long)u * blockDim.x;
+    key[u] = p < n ? pkey[p] : 0;
+    rank[u] = p < n ? prank[p] : 0;
+  }
+#pragma unroll
+  for (int u = 0; u < kBinPer; ++u) at[u] = first + (long long)u * blockDim.x < n ? tile_start[key[u]] : 0;
+#pragma unroll
+  for (int u = 0; u < kBinPer; ++u) {
+    const long long p = first + (long long)u * blockDim.x;
+    if (p < n) perm[at[u] + rank[u]] = (int)p;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -437,8 +509,7 @@ __device__ __forceinline__ unsigned long long splat_cell(const DevGrid& G, float
         ap[2 * r + h] = f2_fma(w, sp2, ap[2 * r + h]);
       }
   }
-  float* smom = sm + (2 * A) * kBox3;
-  float* smas = sm + (2 * A + 1) * kBox3;
+  float* sbox = sm + A * kFieldBox;
 #pragma unroll
   for (int q = 0; q < NP; ++q) {
     float m2[2], p2[2];
@@ -451,9 +522,9 @@ __device__ __forceinline__ unsigned long long splat_cell(const DevGrid& G, float
         idx[A] = 2 * (q & 1) + e;
         idx[W::S1] = (q >> 1) % 3;
         idx[W::S2] = (q >> 1) / 3;
-        const int si = (win.b[0] + idx[0]) + kBox * ((win.b[1] + idx[1]) + kBox * (win.b[2] + idx[2]));
-        atomicAdd(&smom[si], p2[e]);
-        atomicAdd(&smas[si], m2[e]);
+        const int si = box_mom(win.b[0] + idx[0], win.b[1] + idx[1], win.b[2] + idx[2]);
+        atomicAdd(&sbox[si], p2[e]);
+        atomicAdd(&sbox[si + kBox], m2[e]);
       }
     }
   }
@@ -486,12 +557,12 @@ __global__ void __launch_bounds__(kSplatThreads, 2) k_splat(DevGrid G, const int
                                                          const float* __restrict__ vz,
                                                          const uint8_t* __restrict__ type,
                                                          const float* __restrict__ vol, float m_l, float m_g) {
-  extern __shared__ float sm[];  // [3 axes][mom, mass][kBox3]
+  extern __shared__ float sm[];  // [3 axes][kFieldBox]: rows of 12 momentum, 12 mass nodes
   __shared__ unsigned sblk[6];   // [3 axes][64 reached blocks of the box]
   const int t = blockIdx.x;
   const int* cs = cell_start + (size_t)t * PF_TV;
   if (cs[0] >= cs[PF_TV]) return;
-  for (int e = threadIdx.x; e < 6 * kBox3; e += kSplatThreads) sm[e] = 0.0f;
+  for (int e = threadIdx.x; e < 3 * kFieldBox; e += kSplatThreads) sm[e] = 0.0f;
   if (threadIdx.x < 6) sblk[threadIdx.x] = 0u;
   __syncthreads();
   const int tx = t % G.g.TX, tq = t / G.g.TX, ty = tq % G.g.TY, tz = tq / G.g.TY;
@@ -539,9 +610,10 @@ __global__ void __launch_bounds__(kSplatThreads, 2) k_splat(DevGrid G, const int
   // contributions in blocks that end up inactive are cleared by k_normalize
   for (int e = threadIdx.x; e < 3 * kBox3; e += kSplatThreads) {
     const int a = e / kBox3, si = e - a * kBox3;
-    const float mom = sm[(2 * a) * kBox3 + si], mas = sm[(2 * a + 1) * kBox3 + si];
-    if (mom == 0.0f && mas == 0.0f) continue;
     const int X = si % kBox, Y = (si / kBox) % kBox, Z = si / (kBox * kBox);
+    const float* sb = sm + a * kFieldBox + box_mom(X, Y, Z);
+    const float mom = sb[0], mas = sb[kBox];
+    if (mom == 0.0f && mas == 0.0f) continue;
     const int i = o0 + X, j = o1 + Y, k = o2 + Z;
     if (!in_field(G.g, PF_U + a, i, j, k)) continue;
     const int sl = slot_of(G, i, j, k);
@@ -778,6 +850,8 @@ __global__ void __launch_bounds__(256) k_g2p_tiles(DevGrid G, const int* __restr
   }
   __syncthreads();
   float* vp[3] = {P.vx, P.vy, P.vz};
+  const bool fast = G.g.dx_pow2 && G.g.ox == 0.0 && G.g.oy == 0.0 && G.g.oz == 0.0;
+  const float inv_dx_f = (float)G.g.inv_dx;
   // the next particle's attributes are loaded while this one is sampled
   int q = beg + threadIdx.x;
   int pn = 0;
@@ -797,18 +871,41 @@ __global__ void __launch_bounds__(256) k_g2p_tiles(DevGrid G, const int* __restr
       xn = P.px[pn]; yn = P.py[pn]; zn = P.pz[pn]; tn = P.type[pn];
       vn[0] = P.vx[pn]; vn[1] = P.vy[pn]; vn[2] = P.vz[pn];
     }
-    const double gx = to_grid((double)X, G.g.ox, G.g.inv_dx);
-    const double gy = to_grid((double)Y, G.g.oy, G.g.inv_dx);
-    const double gz = to_grid((double)Z, G.g.oz, G.g.inv_dx);
-    const double c[3][3] = {{gx, gy - 0.5, gz - 0.5}, {gx - 0.5, gy, gz - 0.5}, {gx - 0.5, gy - 0.5, gz}};
+    // grid coordinates; with a power-of-two dx and a zero origin the FP32
+    // product with 1/dx, its half-shifts, floors and fractions are exact and
+    // equal the FP64 ones
+    float gf[3];
+    double gd[3];
+    if (fast) {
+      gf[0] = X * inv_dx_f;
+      gf[1] = Y * inv_dx_f;
+      gf[2] = Z * inv_dx_f;
+    } else {
+      gd[0] = to_grid((double)X, G.g.ox, G.g.inv_dx);
+      gd[1] = to_grid((double)Y, G.g.oy, G.g.inv_dx);
+      gd[2] = to_grid((double)Z, G.g.oz, G.g.inv_dx);
+    }
     const float al = ty == 0 ? (float)aL : (float)aG;
 #pragma unroll
     for (int ax = 0; ax < 3; ++ax) {
-      const int i0 = (int)floor(c[ax][0]), j0 = (int)floor(c[ax][1]), k0 = (int)floor(c[ax][2]);
-      const int li = i0 - b0, lj = j0 - b1, lk = k0 - b2;
+      int n0[3];
+      float fr[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        if (fast) {
+          const float c = d == ax ? gf[d] : gf[d] - 0.5f;
+          n0[d] = (int)floorf(c);
+          fr[d] = c - (float)n0[d];
+        } else {
+          const double c = d == ax ? gd[d] : gd[d] - 0.5;
+          n0[d] = (int)floor(c);
+          fr[d] = (float)(c - n0[d]);
+        }
+      }
+      const int li = n0[0] - b0, lj = n0[1] - b1, lk = n0[2] - b2;
       float cur, old;
       if (li >= 0 && lj >= 0 && lk >= 0 && li < kG2PBox - 1 && lj < kG2PBox - 1 && lk < kG2PBox - 1) {
-        const float fx = (float)(c[ax][0] - i0), fy = (float)(c[ax][1] - j0), fz = (float)(c[ax][2] - k0);
+        const float fx = fr[0], fy = fr[1], fz = fr[2];
         const float wx[2] = {1.0f - fx, fx}, wy[2] = {1.0f - fy, fy}, wz[2] = {1.0f - fz, fz};
         const float2* bp = &box[ax][li + kG2PBox * (lj + kG2PBox * lk)];
         float s = 0.0f, so = 0.0f;
@@ -826,7 +923,13 @@ __global__ void __launch_bounds__(256) k_g2p_tiles(DevGrid G, const int* __restr
         cur = s;
         old = so;
       } else {
-        sample2<true>(G, ax, c[ax][0], c[ax][1], c[ax][2], cur, old);
+        double c[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          const double g = fast ? (double)gf[d] : gd[d];
+          c[d] = d == ax ? g : g - 0.5;
+        }
+        sample2<true>(G, ax, c[0], c[1], c[2], cur, old);
       }
       vp[ax][p] = (v0[ax] + (cur - old)) * al + cur * (1.0f - al);
     }
@@ -991,8 +1094,8 @@ int mark_cells(pf_ctx* ctx) {
   rc = request_wall_tiles(ctx);
   if (rc) return rc;
   if (n > 0)
-    (++ctx->launches), k_bin<<<nblocks(n, 256), 256, 0, ctx->stream>>>(G, ctx->px, ctx->py, ctx->pz, n, nullptr,
-                                                                        nullptr, nullptr, ctx->tile_need, 0);
+    (++ctx->launches), k_bin<false><<<nblocks(n, 256 * kBinPer), 256, 0, ctx->stream>>>(
+        G, ctx->px, ctx->py, ctx->pz, n, nullptr, nullptr, nullptr, ctx->tile_need);
   PF_CUDA_TRY(cudaGetLastError());
   rc = pool_commit(ctx);
   if (rc) return rc;
@@ -1017,11 +1120,13 @@ static int p2g_core(pf_ctx* ctx, const pf_phase* ph, double Vp) {
     PF_CUDA_TRY(cudaMemsetAsync(ctx->tile_count, 0, (size_t)(nt * PF_TV + 1) * sizeof(int), ctx->stream));
     DevGrid G = dev_grid(ctx);
     if (n > 0) {
-      (++ctx->launches), k_bin<<<nblocks(n, 256), 256, 0, ctx->stream>>>(
-          G, ctx->px, ctx->py, ctx->pz, n, ctx->tile_count, ctx->pkey, ctx->prank, ctx->tile_need, 1);
-      // the tiles a particle's window can reach: the requested ones and their neighbours
+      (++ctx->launches), k_bin<true><<<nblocks(n, 256 * kBinPer), 256, 0, ctx->stream>>>(
+          G, ctx->px, ctx->py, ctx->pz, n, ctx->tile_count, ctx->pkey, ctx->prank, ctx->tile_need);
+      // the tiles a particle's window can reach: the tiles holding particles
+      // (and any requested before) and their neighbours
       const int nt0 = ctx->g.ntiles;
-      (++ctx->launches), k_need_snapshot<<<nblocks(nt0, 256), 256, 0, ctx->stream>>>(ctx->tile_need, ctx->tile_new, nt0);
+      (++ctx->launches), k_need_from_counts<<<nblocks((size_t)nt0 * 32, 256), 256, 0, ctx->stream>>>(
+          ctx->tile_count, ctx->tile_need, ctx->tile_new, nt0);
       (++ctx->launches), k_need_dilate<<<nblocks(nt0, 256), 256, 0, ctx->stream>>>(ctx->g, ctx->tile_new,
                                                                                    ctx->tile_need);
     }
@@ -1034,13 +1139,13 @@ static int p2g_core(pf_ctx* ctx, const pf_phase* ph, double Vp) {
     StageScope sc(ctx, PF_STAGE_SORT);
     rc = scan_exclusive(ctx, ctx->tile_count, ctx->tile_start, nt * PF_TV + 1, nullptr);
     if (rc) return rc;
-    (++ctx->launches), k_bin_scatter<<<nblocks(n, 256), 256, 0, ctx->stream>>>(ctx->pkey, ctx->prank, ctx->tile_start, ctx->perm, n);
+    (++ctx->launches), k_bin_scatter<<<nblocks(n, 256 * kBinPer), 256, 0, ctx->stream>>>(ctx->pkey, ctx->prank, ctx->tile_start, ctx->perm, n);
     PF_CUDA_TRY(cudaGetLastError());
     ctx->bins_valid = true;
   }
   {
     StageScope sc(ctx, PF_STAGE_SPLAT);
-    const size_t smem = 6 * kBox3 * sizeof(float);
+    const size_t smem = 3 * kFieldBox * sizeof(float);
     (++ctx->launches), k_splat<<<nt, kSplatThreads, smem, ctx->stream>>>(
         dev_grid(ctx), ctx->tile_start, ctx->perm, ctx->px, ctx->py, ctx->pz, ctx->vx, ctx->vy, ctx->vz, ctx->type,
         ctx->vol, (float)(ph->rho_l * Vp), (float)(ph->rho_g * Vp));
