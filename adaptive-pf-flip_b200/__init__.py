@@ -11,6 +11,12 @@ same names, argument meanings and order:
     spAdvect3D_tp(particles, grid, dt, stats=None, advectionOrder=2, escapeBuffer=None)
                                                             src/driver/sparse_ops3d_tp.h:13
     SparseSim3DTP(nx, ny, nz, dx).step()                    src/driver/sparse_sim3d_tp.cpp:854-884
+    applyNarrowBandAir(particles, grid, enabled, radius)    src/driver/particle_adaptivity3d.h:111
+    applyTypedParticleCoarsening(particles, grid, enabled, particleType, target, seed)
+                                                            src/driver/particle_adaptivity3d.h:168
+    applyLiquidParticleRefill(particles, grid, enabled, target, seed, interfaceOnly,
+                              interfaceRadius, maxAddedPerStep)
+                                                            src/driver/particle_adaptivity3d.h:264
     SparseMacGrid3D, Particles3DTP, PhaseParams             src/grid/sparse_mac_grid3d.h,
                                                             src/particles/particles3d_tp.h,
                                                             src/physics/phasefield.h
@@ -23,8 +29,10 @@ from ._lib import (PF_MK, PF_MU, PF_MV, PF_MW, PF_P, PF_PRECOND_EXACT_COARSE, PF
                    load)
 from .learned import LearnedCoarseSolver
 from .sparse import (ParticleEscapeBuffer3D, ParticleEscapeStats3D, Particles3DTP, PhaseParams, SolverConfig,
-                     SparseMacGrid3D, SparseSim3DTP, betaFromPhi, calibrateRhoTilde0, densityFromPhi, etaPhi,
-                     phiFromRawDensity, spAdvect3D_tp, spG2P3D_tp, spP2G3D_tp, spProjectStepVC3D)
+                     SparseMacGrid3D, SparseSim3DTP, applyGasParticleCoarsening, applyLiquidParticleRefill,
+                     applyNarrowBandAir, applyTypedParticleCoarsening, betaFromPhi, calibrateRhoTilde0,
+                     densityFromPhi, etaPhi, phiFromRawDensity, spAdvect3D_tp, spG2P3D_tp, spP2G3D_tp,
+                     spProjectStepVC3D)
 from . import scenes
 
 __all__ = [
@@ -35,4 +43,5 @@ __all__ = [
     "ParticleEscapeStats3D", "ParticleEscapeBuffer3D",
     "spP2G3D_tp", "spProjectStepVC3D", "spG2P3D_tp", "spAdvect3D_tp", "calibrateRhoTilde0",
     "etaPhi", "phiFromRawDensity", "densityFromPhi", "betaFromPhi", "scenes",
+    "applyNarrowBandAir", "applyTypedParticleCoarsening", "applyGasParticleCoarsening", "applyLiquidParticleRefill",
 ]

@@ -37,9 +37,11 @@ EXPORTS = (
     "pf_learned_harvest", "pf_learned_dataset", "pf_learned_clear_dataset", "pf_learned_merge_dataset",
     "pf_learned_train",
     "pf_learned_eval", "pf_learned_adam",
+    "pf_narrow_band_air", "pf_coarsen_particles", "pf_refill_liquid", "pf_set_adaptivity", "pf_get_adaptivity_stats",
 )
 
-STAGES = ("bin", "sort", "splat", "normalize", "mark", "boundary", "project", "pcg", "g2p", "precond_setup")
+STAGES = ("bin", "sort", "splat", "normalize", "mark", "boundary", "project", "pcg", "g2p", "precond_setup",
+          "adapt")
 
 
 class GridDesc(C.Structure):
@@ -84,6 +86,49 @@ class StepCfg(C.Structure):
 
 class StepStats(C.Structure):
     _fields_ = [("solve", SolveStats), ("clamp", ClampStats), ("active_tiles", C.c_int)]
+
+
+class _Stats(C.Structure):
+    def as_tuple(self):
+        return tuple(getattr(self, n) for n, _ in self._fields_)
+
+
+class BandStats(_Stats):
+    """pf_band_stats: NarrowBandAirResult3D (src/driver/particle_adaptivity3d.h:49-54)"""
+    _fields_ = [("removed", C.c_int), ("liquid_cells", C.c_int), ("gas_before", C.c_int), ("gas_after", C.c_int)]
+
+
+class CoarsenStats(_Stats):
+    """pf_coarsen_stats: GasParticleCoarseningResult3D (src/driver/particle_adaptivity3d.h:56-62)"""
+    _fields_ = [("removed", C.c_int), ("cells", C.c_int), ("overfull_cells", C.c_int), ("before", C.c_int),
+                ("after", C.c_int)]
+
+
+class RefillStats(_Stats):
+    """pf_refill_stats: LiquidParticleRefillResult3D (src/driver/particle_adaptivity3d.h:64-72)"""
+    _fields_ = [("added", C.c_int), ("cells", C.c_int), ("interface_cells", C.c_int), ("underfull_cells", C.c_int),
+                ("budget_limited", C.c_int), ("before", C.c_int), ("after", C.c_int)]
+
+
+class AdaptCfg(C.Structure):
+    """pf_adapt_cfg: SparseSim3DTP's adaptivity switches (src/driver/sparse_sim3d_tp.h:29-66), with its defaults."""
+    _fields_ = [("narrow_band_air", C.c_int), ("narrow_band_radius", C.c_int),
+                ("gas_coarsening", C.c_int), ("gas_per_cell_target", C.c_int), ("gas_seed", C.c_uint),
+                ("liquid_coarsening", C.c_int), ("liquid_per_cell_target", C.c_int), ("liquid_seed", C.c_uint),
+                ("liquid_refill", C.c_int), ("refill_per_cell_target", C.c_int), ("refill_seed", C.c_uint),
+                ("refill_interface_only", C.c_int), ("refill_interface_radius", C.c_int),
+                ("refill_max_added", C.c_int)]
+
+    def __init__(self, **kw):
+        d = dict(narrow_band_radius=2, gas_per_cell_target=4, gas_seed=0x9e3779b9, liquid_per_cell_target=4,
+                 liquid_seed=0x7f4a7c15, refill_per_cell_target=4, refill_seed=0x6a09e667,
+                 refill_interface_radius=1)
+        d.update(kw)
+        super().__init__(**d)
+
+
+class AdaptStats(C.Structure):
+    _fields_ = [("band", BandStats), ("gas", CoarsenStats), ("liquid", CoarsenStats), ("refill", RefillStats)]
 
 
 class Timing(C.Structure):
@@ -162,6 +207,11 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "pf_learned_train": (i, [vp, i, i, d, C.c_ulonglong, vp]),
         "pf_learned_eval": (i, [vp, i, i, i, vp, vp, vp, i, vp, P(d), vp]),
         "pf_learned_adam": (i, [vp, vp, sz, d]),
+        "pf_narrow_band_air": (i, [vp, i, P(BandStats)]),
+        "pf_coarsen_particles": (i, [vp, i, i, C.c_uint, P(CoarsenStats)]),
+        "pf_refill_liquid": (i, [vp, i, C.c_uint, i, i, i, P(RefillStats)]),
+        "pf_set_adaptivity": (i, [vp, P(AdaptCfg)]),
+        "pf_get_adaptivity_stats": (i, [vp, P(AdaptStats)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

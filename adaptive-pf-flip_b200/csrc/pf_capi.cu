@@ -47,6 +47,7 @@ __global__ void k_convert_back(const float* in, T* out, size_t n) {
 void free_all(pf_ctx* c) {
   auto F = [](void* p) { if (p) cudaFree(p); };
   pf::coarse_release(c);
+  pf::adapt_free(c);
   F(c->tile_slot); F(c->slot_tile); F(c->d_nslots); F(c->tile_need); F(c->tile_new); F(c->tile_rank);
   for (int f = 0; f < PF_NFIELDS; ++f) { F(c->fld[f]); F(c->act4[f]); }
   for (int a = 0; a < PF_NSAVED; ++a) F(c->saved[a]);
@@ -212,6 +213,23 @@ int create_impl(pf_ctx* ctx, const pf_grid_desc* d) {
 bool valid_field(int f) { return f >= 0 && f < PF_NFIELDS; }
 
 }  // namespace
+
+namespace pf {
+// The second particle set: filled by asynchronous uploads and by compaction,
+// then swapped in.  Allocated on first use.
+int ensure_back_set(pf_ctx* ctx) {
+  if (ctx->up_stream) return PF_OK;
+  const size_t cap = ctx->cap;
+  PF_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->up_stream, cudaStreamNonBlocking));
+  PF_CUDA_TRY(cudaEventCreateWithFlags(&ctx->up_done, cudaEventDisableTiming));
+  PF_CUDA_TRY(cudaEventCreateWithFlags(&ctx->back_free, cudaEventDisableTiming));
+  float** pa[7] = {&ctx->bpx, &ctx->bpy, &ctx->bpz, &ctx->bvx, &ctx->bvy, &ctx->bvz, &ctx->bvol};
+  for (float** q : pa) PF_CUDA_TRY(cudaMalloc(q, cap * sizeof(float)));
+  PF_CUDA_TRY(cudaMalloc(&ctx->btype, cap));
+  PF_CUDA_TRY(cudaMalloc(&ctx->up_staging, 6 * cap * sizeof(float)));
+  return PF_OK;
+}
+}  // namespace pf
 
 extern "C" {
 
@@ -431,14 +449,9 @@ int pf_upload_particles_async(pf_ctx* ctx, size_t n, const float* pos, const flo
   if (n > ctx->cap) return set_error(ctx, PF_ERR_CAPACITY, "more particles than max_particles");
   cudaSetDevice(ctx->device);
   const size_t cap = ctx->cap;
-  if (!ctx->up_stream) {
-    PF_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->up_stream, cudaStreamNonBlocking));
-    PF_CUDA_TRY(cudaEventCreateWithFlags(&ctx->up_done, cudaEventDisableTiming));
-    PF_CUDA_TRY(cudaEventCreateWithFlags(&ctx->back_free, cudaEventDisableTiming));
-    float** pa[7] = {&ctx->bpx, &ctx->bpy, &ctx->bpz, &ctx->bvx, &ctx->bvy, &ctx->bvz, &ctx->bvol};
-    for (float** q : pa) PF_CUDA_TRY(cudaMalloc(q, cap * sizeof(float)));
-    PF_CUDA_TRY(cudaMalloc(&ctx->btype, cap));
-    PF_CUDA_TRY(cudaMalloc(&ctx->up_staging, 6 * cap * sizeof(float)));
+  {
+    const int rc = pf::ensure_back_set(ctx);
+    if (rc) return rc;
   }
   if (ctx->up_pending) PF_CUDA_TRY(cudaEventSynchronize(ctx->up_done));  // superseded; its copies must land first
   // the second set was the particles of earlier work: wait until that work is done
@@ -617,6 +630,11 @@ int pf_step(pf_ctx* ctx, const pf_step_cfg* cfg, pf_step_stats* stats) {
   cudaSetDevice(ctx->device);
   int rc = take_upload(ctx);
   if (rc) return rc;
+  // applyParticleAdaptivity comes first in SparseSim3DTP::step()
+  if (ctx->adapt_on) {
+    rc = pf::apply_adaptivity(ctx, ctx->adapt_cfg, &ctx->adapt_last);
+    if (rc) return rc;
+  }
   rc = pool_reset(ctx);
   if (rc) return rc;
   rc = pf::mark_cells(ctx);
@@ -647,6 +665,47 @@ int pf_calibrate_rho_tilde0(pf_ctx* ctx, const pf_phase* phase, double Vp, doubl
   if (!ctx || !phase || !out) return PF_ERR_INVALID;
   cudaSetDevice(ctx->device);
   return pf::calibrate(ctx, phase, Vp, out);
+}
+
+// ---- particle adaptivity --------------------------------------------------
+
+int pf_narrow_band_air(pf_ctx* ctx, int radius, pf_band_stats* stats) {
+  if (!ctx) return PF_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  const int rc = take_upload(ctx);
+  if (rc) return rc;
+  return pf::narrow_band_air(ctx, radius, stats);
+}
+
+int pf_coarsen_particles(pf_ctx* ctx, int type, int per_cell_target, unsigned seed, pf_coarsen_stats* stats) {
+  if (!ctx || type < 0 || type > 255) return PF_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  const int rc = take_upload(ctx);
+  if (rc) return rc;
+  return pf::coarsen_particles(ctx, type, per_cell_target, seed, stats);
+}
+
+int pf_refill_liquid(pf_ctx* ctx, int per_cell_target, unsigned seed, int interface_only, int interface_radius,
+                     int max_added, pf_refill_stats* stats) {
+  if (!ctx) return PF_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  const int rc = take_upload(ctx);
+  if (rc) return rc;
+  return pf::refill_liquid(ctx, per_cell_target, seed, interface_only, interface_radius, max_added, stats);
+}
+
+int pf_set_adaptivity(pf_ctx* ctx, const pf_adapt_cfg* cfg) {
+  if (!ctx) return PF_ERR_INVALID;
+  ctx->adapt_on = cfg != nullptr;
+  if (cfg) ctx->adapt_cfg = *cfg;
+  ctx->adapt_last = pf_adapt_stats{};
+  return PF_OK;
+}
+
+int pf_get_adaptivity_stats(const pf_ctx* ctx, pf_adapt_stats* out) {
+  if (!ctx || !out) return PF_ERR_INVALID;
+  *out = ctx->adapt_last;
+  return PF_OK;
 }
 
 }  // extern "C"

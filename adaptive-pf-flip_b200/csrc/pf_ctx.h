@@ -86,6 +86,11 @@ struct pf_ctx {
   double* b64 = nullptr;  // right-hand side kept in FP64
   // learned preconditioner state lives in its own module
   void* learned = nullptr;
+  // particle adaptivity: scratch (its own module) and the step's settings
+  void* adapt = nullptr;
+  bool adapt_on = false;
+  pf_adapt_cfg adapt_cfg{};
+  pf_adapt_stats adapt_last{};
 
   // ---- misc ----
   int* d_clamp = nullptr;      // 8 counters
@@ -146,6 +151,17 @@ int calibrate(pf_ctx* ctx, const pf_phase* ph, double Vp, double* out);
 // project.cu
 int project(pf_ctx* ctx, const pf_phase* ph, double dt, const pf_solve_cfg* cfg,
             pf_solve_stats* st);
+
+// adapt.cu
+int narrow_band_air(pf_ctx* ctx, int radius, pf_band_stats* st);
+int coarsen_particles(pf_ctx* ctx, int ptype, int target, unsigned seed, pf_coarsen_stats* st);
+int refill_liquid(pf_ctx* ctx, int target, unsigned seed, int interface_only, int interface_radius, int max_added,
+                  pf_refill_stats* st);
+int apply_adaptivity(pf_ctx* ctx, const pf_adapt_cfg& cfg, pf_adapt_stats* st);
+void adapt_free(pf_ctx* ctx);
+
+// capi.cu: the second particle set (asynchronous uploads, compaction target)
+int ensure_back_set(pf_ctx* ctx);
 
 constexpr int kMaxRedBlocks = 1184;  // 8 CTAs per SM on 148 SMs
 constexpr int kRedSlots = 4;         // partial values one reduction CTA may write

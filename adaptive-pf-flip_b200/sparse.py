@@ -285,6 +285,17 @@ class SparseMacGrid3D:
                                               vol.ctypes.data)
         L.check(rc, self.ctx, "pf_upload_particles_f64")
 
+    def take_particles(self, ps):
+        """Download the whole device particle set into ps (its count may have changed)."""
+        n = int(self.lib.pf_num_particles(self.ctx))
+        P, V = np.empty((n, 3), np.float64), np.empty((n, 3), np.float64)
+        T, W = np.empty(n, np.uint8), np.empty(n, np.float64)
+        if n:
+            rc = self.lib.pf_download_particles_f64(self.ctx, P.ctypes.data, V.ctypes.data, T.ctypes.data,
+                                                    W.ctypes.data)
+            L.check(rc, self.ctx, "pf_download_particles_f64")
+        ps.pos, ps.vel, ps.type, ps.volume = P, V, T, W
+
     def download(self, ps, pos=True, vel=True):
         n = len(ps.pos)
         if n == 0:
@@ -360,6 +371,60 @@ def spAdvect3D_tp(ps, g: SparseMacGrid3D, dt, stats: ParticleEscapeStats3D | Non
 # device-resident step (SparseSim3DTP)
 # ---------------------------------------------------------------------------
 
+# ---------------------------------------------------------------------------
+# particle adaptivity (src/driver/particle_adaptivity3d.h), on the device; the
+# grid supplies the cell domain (ParticleCellDomain3D) and holds the particles
+# for the call
+# ---------------------------------------------------------------------------
+
+def applyNarrowBandAir(particles, grid: SparseMacGrid3D, enabled=True, radius=2) -> L.BandStats:
+    """pa3d::applyNarrowBandAir (src/driver/particle_adaptivity3d.h:111-166)."""
+    st = L.BandStats()
+    if not enabled:
+        return st
+    grid.upload(particles)
+    L.check(grid.lib.pf_narrow_band_air(grid.ctx, int(radius), C.byref(st)), grid.ctx, "pf_narrow_band_air")
+    grid.take_particles(particles)
+    return st
+
+
+def applyTypedParticleCoarsening(particles, grid: SparseMacGrid3D, enabled=True, particleType=1,
+                                 particlesPerCellTarget=4, seed=0x9e3779b9) -> L.CoarsenStats:
+    """pa3d::applyTypedParticleCoarsening (src/driver/particle_adaptivity3d.h:168-248)."""
+    st = L.CoarsenStats()
+    if not enabled:
+        return st
+    grid.upload(particles)
+    rc = grid.lib.pf_coarsen_particles(grid.ctx, int(particleType), int(particlesPerCellTarget),
+                                       int(seed) & 0xffffffff, C.byref(st))
+    L.check(rc, grid.ctx, "pf_coarsen_particles")
+    grid.take_particles(particles)
+    return st
+
+
+def applyGasParticleCoarsening(particles, grid: SparseMacGrid3D, enabled=True, particlesPerCellTarget=4,
+                               seed=0x9e3779b9) -> L.CoarsenStats:
+    """pa3d::applyGasParticleCoarsening (src/driver/particle_adaptivity3d.h:250-262)."""
+    return applyTypedParticleCoarsening(particles, grid, enabled, 1, particlesPerCellTarget, seed)
+
+
+def applyLiquidParticleRefill(particles, grid: SparseMacGrid3D, enabled=True, particlesPerCellTarget=4,
+                              seed=0x6a09e667, interfaceOnly=False, interfaceRadius=1,
+                              maxAddedPerStep=0) -> L.RefillStats:
+    """pa3d::applyLiquidParticleRefill (src/driver/particle_adaptivity3d.h:264-374).  The grid's
+    max_particles must hold the particles after the refill (PfError PF_ERR_CAPACITY otherwise)."""
+    st = L.RefillStats()
+    if not enabled:
+        return st
+    grid.upload(particles)
+    rc = grid.lib.pf_refill_liquid(grid.ctx, int(particlesPerCellTarget), int(seed) & 0xffffffff,
+                                   int(bool(interfaceOnly)), int(interfaceRadius), int(maxAddedPerStep),
+                                   C.byref(st))
+    L.check(rc, grid.ctx, "pf_refill_liquid")
+    grid.take_particles(particles)
+    return st
+
+
 class SparseSim3DTP:
     """SparseSim3DTP with particles resident on the GPU; step() runs
     markCells, P2G, saved copy, gravity, walls, projection, G2P and
@@ -377,6 +442,18 @@ class SparseSim3DTP:
         self.solver = SolverConfig()
         self.n = 0
         self.last_stats = None
+        # particle adaptivity switches (src/driver/sparse_sim3d_tp.h:29-66), all off by default
+        self.narrow_band_air, self.narrow_band_air_radius = False, 2
+        self.gas_particle_coarsening, self.gas_particles_per_cell_target = False, 4
+        self.gas_particle_coarsening_seed = 0x9e3779b9
+        self.liquid_particle_coarsening, self.liquid_particles_per_cell_target = False, 4
+        self.liquid_particle_coarsening_seed = 0x7f4a7c15
+        self.liquid_particle_refill, self.liquid_refill_particles_per_cell_target = False, 4
+        self.liquid_particle_refill_seed = 0x6a09e667
+        self.liquid_particle_refill_interface_only = False
+        self.liquid_particle_refill_interface_radius = 1
+        self.liquid_particle_refill_max_added_per_step = 0
+        self.adaptivity_last = L.AdaptStats()
 
     def set_particles(self, pos, vel, type, volume):
         """Upload FP32 (n,3) pos/vel, uint8 type, FP32 volume (host or device pointers via numpy)."""
@@ -402,6 +479,47 @@ class SparseSim3DTP:
         L.check(rc, self.grid.ctx, "pf_download_particles")
         return pos, vel, typ, vol
 
+    def adapt_cfg(self):
+        return L.AdaptCfg(
+            narrow_band_air=int(self.narrow_band_air), narrow_band_radius=int(self.narrow_band_air_radius),
+            gas_coarsening=int(self.gas_particle_coarsening),
+            gas_per_cell_target=int(self.gas_particles_per_cell_target),
+            gas_seed=int(self.gas_particle_coarsening_seed) & 0xffffffff,
+            liquid_coarsening=int(self.liquid_particle_coarsening),
+            liquid_per_cell_target=int(self.liquid_particles_per_cell_target),
+            liquid_seed=int(self.liquid_particle_coarsening_seed) & 0xffffffff,
+            liquid_refill=int(self.liquid_particle_refill),
+            refill_per_cell_target=int(self.liquid_refill_particles_per_cell_target),
+            refill_seed=int(self.liquid_particle_refill_seed) & 0xffffffff,
+            refill_interface_only=int(self.liquid_particle_refill_interface_only),
+            refill_interface_radius=int(self.liquid_particle_refill_interface_radius),
+            refill_max_added=int(self.liquid_particle_refill_max_added_per_step))
+
+    def _adaptivity_on(self):
+        return (self.narrow_band_air or self.gas_particle_coarsening or self.liquid_particle_coarsening
+                or self.liquid_particle_refill)
+
+    def applyParticleAdaptivity(self):
+        """SparseSim3DTP::applyParticleAdaptivity (src/driver/sparse_sim3d_tp.cpp:843-848) on the resident
+        particles: narrow band, gas coarsening, liquid coarsening, liquid refill, each when switched on."""
+        a, out = self.adapt_cfg(), L.AdaptStats()
+        ctx, lib = self.grid.ctx, self.grid.lib
+        if a.narrow_band_air:
+            L.check(lib.pf_narrow_band_air(ctx, a.narrow_band_radius, C.byref(out.band)), ctx, "pf_narrow_band_air")
+        if a.gas_coarsening:
+            L.check(lib.pf_coarsen_particles(ctx, 1, a.gas_per_cell_target, a.gas_seed, C.byref(out.gas)), ctx,
+                    "pf_coarsen_particles")
+        if a.liquid_coarsening:
+            L.check(lib.pf_coarsen_particles(ctx, 0, a.liquid_per_cell_target, a.liquid_seed, C.byref(out.liquid)),
+                    ctx, "pf_coarsen_particles")
+        if a.liquid_refill:
+            L.check(lib.pf_refill_liquid(ctx, a.refill_per_cell_target, a.refill_seed, a.refill_interface_only,
+                                         a.refill_interface_radius, a.refill_max_added, C.byref(out.refill)), ctx,
+                    "pf_refill_liquid")
+        self.adaptivity_last = out
+        self.n = int(lib.pf_num_particles(ctx))
+        return out
+
     def step_cfg(self):
         solve = self.solver._c(self.cg_iters, self.cg_tol, self.c_div_last)
         return L.StepCfg(self.dt, self.gravity, self.Vp, self.alpha_liquid, self.alpha_gas, self.phase._c(), solve,
@@ -410,6 +528,16 @@ class SparseSim3DTP:
     def step(self):
         cfg = self.step_cfg()
         st = L.StepStats()
-        L.check(self.grid.lib.pf_step(self.grid.ctx, C.byref(cfg), C.byref(st)), self.grid.ctx, "pf_step")
+        ctx, lib = self.grid.ctx, self.grid.lib
+        # the step starts with applyParticleAdaptivity (src/driver/sparse_sim3d_tp.cpp:854-856)
+        if self._adaptivity_on():
+            ac = self.adapt_cfg()
+            L.check(lib.pf_set_adaptivity(ctx, C.byref(ac)), ctx, "pf_set_adaptivity")
+        else:
+            L.check(lib.pf_set_adaptivity(ctx, None), ctx, "pf_set_adaptivity")
+        L.check(lib.pf_step(ctx, C.byref(cfg), C.byref(st)), ctx, "pf_step")
+        if self._adaptivity_on():
+            L.check(lib.pf_get_adaptivity_stats(ctx, C.byref(self.adaptivity_last)), ctx, "pf_get_adaptivity_stats")
+        self.n = int(lib.pf_num_particles(ctx))
         self.last_stats = st
         return st

@@ -132,6 +132,35 @@ typedef struct {
   int active_tiles;      /* pooled 8^3 tiles */
 } pf_step_stats;
 
+/* Particle adaptivity results (src/driver/particle_adaptivity3d.h:49-72:
+ * NarrowBandAirResult3D, GasParticleCoarseningResult3D,
+ * LiquidParticleRefillResult3D). */
+typedef struct { int removed, liquid_cells, gas_before, gas_after; } pf_band_stats;
+typedef struct { int removed, cells, overfull_cells, before, after; } pf_coarsen_stats;
+typedef struct { int added, cells, interface_cells, underfull_cells, budget_limited, before, after; } pf_refill_stats;
+
+/* The adaptivity switches of SparseSim3DTP (src/driver/sparse_sim3d_tp.h:29-66),
+ * applied at the start of every pf_step in the order of
+ * SparseSim3DTP::applyParticleAdaptivity (src/driver/sparse_sim3d_tp.cpp:843-848).
+ * The reference's defaults: all off; radius 2; targets 4; seeds 0x9e3779b9
+ * (gas), 0x7f4a7c15 (liquid coarsening), 0x6a09e667 (refill); refill
+ * interface radius 1, budget 0 (none). */
+typedef struct {
+  int narrow_band_air, narrow_band_radius;
+  int gas_coarsening, gas_per_cell_target;
+  unsigned gas_seed;
+  int liquid_coarsening, liquid_per_cell_target;
+  unsigned liquid_seed;
+  int liquid_refill, refill_per_cell_target;
+  unsigned refill_seed;
+  int refill_interface_only, refill_interface_radius, refill_max_added;
+} pf_adapt_cfg;
+typedef struct {
+  pf_band_stats band;
+  pf_coarsen_stats gas, liquid;
+  pf_refill_stats refill;
+} pf_adapt_stats;
+
 /* ---- context ---------------------------------------------------------- */
 PFGPU_API int pf_create(const pf_grid_desc* desc, pf_ctx** out);
 PFGPU_API int pf_destroy(pf_ctx* ctx);
@@ -203,6 +232,29 @@ PFGPU_API int pf_advect(pf_ctx* ctx, double dt, int order, pf_clamp_stats* stats
 /* One full step in the reference's step() order, device-resident. */
 PFGPU_API int pf_step(pf_ctx* ctx, const pf_step_cfg* cfg, pf_step_stats* stats);
 
+/* ---- particle adaptivity (src/driver/particle_adaptivity3d.h) ----------
+ * Each call rewrites the context's particle set on the device; erasures keep
+ * the survivors' order, refill appends after the last particle.  Particle
+ * order, positions, types, velocities and volumes equal the reference's
+ * (FP64 results rounded to the FP32 storage). */
+/* pa3d::applyNarrowBandAir (:111-166): gas particles farther than `radius`
+ * cells (Chebyshev) from every cell holding liquid are erased. */
+PFGPU_API int pf_narrow_band_air(pf_ctx* ctx, int radius, pf_band_stats* stats);
+/* pa3d::applyTypedParticleCoarsening (:168-248): per cell, the
+ * per_cell_target particles of `type` with the lowest hash score stay and
+ * share the cell's volume (type 1 is applyGasParticleCoarsening). */
+PFGPU_API int pf_coarsen_particles(pf_ctx* ctx, int type, int per_cell_target, unsigned seed,
+                                   pf_coarsen_stats* stats);
+/* pa3d::applyLiquidParticleRefill (:250-374): underfull liquid cells get new
+ * particles at sub-cell centres.  PF_ERR_CAPACITY, with nothing changed, when
+ * the result would exceed max_particles. */
+PFGPU_API int pf_refill_liquid(pf_ctx* ctx, int per_cell_target, unsigned seed, int interface_only,
+                               int interface_radius, int max_added, pf_refill_stats* stats);
+/* Adaptivity run by pf_step (NULL: none, the default); the results of the
+ * last step's adaptivity. */
+PFGPU_API int pf_set_adaptivity(pf_ctx* ctx, const pf_adapt_cfg* cfg);
+PFGPU_API int pf_get_adaptivity_stats(const pf_ctx* ctx, pf_adapt_stats* out);
+
 /* ---- per-stage device timing (CUDA events on the context stream) -------
  * Off by default.  When on, every solver-step entry point brackets its
  * stages with events; pf_get_timing synchronises and returns the summed
@@ -218,6 +270,7 @@ enum pf_stage {
   PF_STAGE_PCG,          /* iterative solve only */
   PF_STAGE_G2P,          /* G2P and/or advection */
   PF_STAGE_PRECOND_SETUP, /* LEARNED solves: coarse operator, gate network, neighbour table */
+  PF_STAGE_ADAPT,        /* particle adaptivity: narrow band, coarsening, refill */
   PF_NSTAGES
 };
 typedef struct {

@@ -55,6 +55,32 @@ class SolveStats(C.Structure):
                 ("converged", C.c_int), ("breakdown", C.c_int)]
 
 
+class BandStats(C.Structure):
+    """NarrowBandAirResult3D (src/driver/particle_adaptivity3d.h:49-54)"""
+    _fields_ = [("removed", C.c_int), ("liquid_cells", C.c_int), ("gas_before", C.c_int), ("gas_after", C.c_int)]
+
+    def as_tuple(self):
+        return tuple(getattr(self, n) for n, _ in self._fields_)
+
+
+class CoarsenStats(C.Structure):
+    """GasParticleCoarseningResult3D (src/driver/particle_adaptivity3d.h:56-62)"""
+    _fields_ = [("removed", C.c_int), ("cells", C.c_int), ("overfull_cells", C.c_int), ("before", C.c_int),
+                ("after", C.c_int)]
+
+    def as_tuple(self):
+        return tuple(getattr(self, n) for n, _ in self._fields_)
+
+
+class RefillStats(C.Structure):
+    """LiquidParticleRefillResult3D (src/driver/particle_adaptivity3d.h:64-72)"""
+    _fields_ = [("added", C.c_int), ("cells", C.c_int), ("interface_cells", C.c_int), ("underfull_cells", C.c_int),
+                ("budget_limited", C.c_int), ("before", C.c_int), ("after", C.c_int)]
+
+    def as_tuple(self):
+        return tuple(getattr(self, n) for n, _ in self._fields_)
+
+
 class ClampStats(C.Structure):
     _fields_ = [("clamped_liquid", C.c_int), ("clamped_gas", C.c_int),
                 ("x_lo", C.c_int), ("x_hi", C.c_int), ("y_lo", C.c_int),
@@ -164,6 +190,16 @@ def oracle_lib():
     lib.pfo_collect_cells.argtypes = [vp, C.c_int, C.c_void_p, C.POINTER(C.c_size_t)]
     lib.pfo_step.argtypes = [vp, vp, C.c_size_t, _dp, _dp, _up, _dp, C.POINTER(_Phase),
                              C.POINTER(_StepCfg), C.POINTER(SolveStats), C.POINTER(ClampStats)]
+    sp = C.POINTER(C.c_size_t)
+    lib.pfo_particle_score.restype = C.c_uint
+    lib.pfo_particle_score.argtypes = [vp, _dp, C.c_int, C.c_int, C.c_int, C.c_uint]
+    lib.pfo_slot_score.restype = C.c_uint
+    lib.pfo_slot_score.argtypes = [C.c_size_t, C.c_int, C.c_uint]
+    lib.pfo_narrow_band_air.argtypes = [vp, sp, _dp, _dp, _up, _dp, C.c_int, C.POINTER(BandStats)]
+    lib.pfo_coarsen_particles.argtypes = [vp, sp, _dp, _dp, _up, _dp, C.c_int, C.c_int, C.c_uint,
+                                          C.POINTER(CoarsenStats)]
+    lib.pfo_refill_liquid.argtypes = [vp, sp, C.c_size_t, _dp, _dp, _up, _dp, C.c_int, C.c_uint, C.c_int, C.c_int,
+                                      C.c_int, C.POINTER(RefillStats)]
     lib._typed = True
     return lib
 
@@ -195,6 +231,9 @@ def ref_lib():
     lib.pfr_phi_from_raw.argtypes = [C.c_double, _dp]
     lib.pfr_beta_from_raw.restype = C.c_double
     lib.pfr_beta_from_raw.argtypes = [C.c_double, _dp]
+    lib.pfr_narrow_band_air.argtypes = [vp, C.c_int, _ip]
+    lib.pfr_coarsen_particles.argtypes = [vp, C.c_int, C.c_int, C.c_uint, _ip]
+    lib.pfr_refill_liquid.argtypes = [vp, C.c_int, C.c_uint, C.c_int, C.c_int, C.c_int, _ip]
     lib._typed = True
     return lib
 
@@ -316,6 +355,10 @@ class ReferenceGrid(_GridBase):
         self.lib.pfr_set_particles(self.h, len(ps), ps.pos, ps.vel, ps.type, ps.volume)
 
     def _take(self, ps: Particles):
+        n = int(self.lib.pfr_num_particles(self.h))
+        if n != len(ps):
+            ps.pos, ps.vel = np.zeros((n, 3)), np.zeros((n, 3))
+            ps.type, ps.volume = np.zeros(n, np.uint8), np.zeros(n)
         self.lib.pfr_get_particles(self.h, ps.pos, ps.vel, ps.type, ps.volume)
 
 
@@ -380,6 +423,48 @@ class Oracle:
         return sst, cst
 
 
+    # ---- particle adaptivity (src/driver/particle_adaptivity3d.h:111-374) ----
+    def narrow_band_air(self, g, ps: Particles, radius=2):
+        n = C.c_size_t(len(ps))
+        st = BandStats()
+        if self.lib.pfo_narrow_band_air(g.h, C.byref(n), ps.pos, ps.vel, ps.type, ps.volume, int(radius),
+                                        C.byref(st)):
+            raise MemoryError("pfo_narrow_band_air")
+        _truncate(ps, n.value)
+        return st
+
+    def coarsen_particles(self, g, ps: Particles, ptype, target, seed):
+        n = C.c_size_t(len(ps))
+        st = CoarsenStats()
+        if self.lib.pfo_coarsen_particles(g.h, C.byref(n), ps.pos, ps.vel, ps.type, ps.volume, int(ptype),
+                                          int(target), int(seed) & 0xffffffff, C.byref(st)):
+            raise MemoryError("pfo_coarsen_particles")
+        _truncate(ps, n.value)
+        return st
+
+    def refill_liquid(self, g, ps: Particles, target, seed, interface_only=False, interface_radius=1,
+                      max_added=0):
+        n0 = len(ps)
+        cap = n0 + int(np.count_nonzero(ps.type == 0)) * max(int(target), 1)
+        pos, vel = np.zeros((cap, 3)), np.zeros((cap, 3))
+        typ, vol = np.zeros(cap, np.uint8), np.zeros(cap)
+        pos[:n0], vel[:n0], typ[:n0], vol[:n0] = ps.pos, ps.vel, ps.type, ps.volume
+        n = C.c_size_t(n0)
+        st = RefillStats()
+        if self.lib.pfo_refill_liquid(g.h, C.byref(n), cap, pos, vel, typ, vol, int(target),
+                                      int(seed) & 0xffffffff, int(bool(interface_only)), int(interface_radius),
+                                      int(max_added), C.byref(st)):
+            raise MemoryError("pfo_refill_liquid")
+        m = n.value
+        ps.pos, ps.vel, ps.type, ps.volume = pos[:m].copy(), vel[:m].copy(), typ[:m].copy(), vol[:m].copy()
+        return st
+
+
+def _truncate(ps: Particles, n):
+    ps.pos, ps.vel = ps.pos[:n].copy(), ps.vel[:n].copy()
+    ps.type, ps.volume = ps.type[:n].copy(), ps.volume[:n].copy()
+
+
 class Reference:
     """Per-call API of the compiled, unmodified reference."""
     Grid = ReferenceGrid
@@ -430,6 +515,30 @@ class Reference:
         self.lib.pfr_step(g.h, pp.as_array(), arr)
         if take:
             g._take(ps)
+
+    # ---- particle adaptivity, the reference's own pa3d functions ----
+    def narrow_band_air(self, g: ReferenceGrid, ps: Particles, radius=2):
+        g._put(ps)
+        out = np.zeros(4, np.int32)
+        self.lib.pfr_narrow_band_air(g.h, int(radius), out)
+        g._take(ps)
+        return BandStats(*[int(v) for v in out])
+
+    def coarsen_particles(self, g: ReferenceGrid, ps: Particles, ptype, target, seed):
+        g._put(ps)
+        out = np.zeros(5, np.int32)
+        self.lib.pfr_coarsen_particles(g.h, int(ptype), int(target), int(seed) & 0xffffffff, out)
+        g._take(ps)
+        return CoarsenStats(*[int(v) for v in out])
+
+    def refill_liquid(self, g: ReferenceGrid, ps: Particles, target, seed, interface_only=False,
+                      interface_radius=1, max_added=0):
+        g._put(ps)
+        out = np.zeros(7, np.int32)
+        self.lib.pfr_refill_liquid(g.h, int(target), int(seed) & 0xffffffff, int(bool(interface_only)),
+                                   int(interface_radius), int(max_added), out)
+        g._take(ps)
+        return RefillStats(*[int(v) for v in out])
 
 
 def build(quiet=True):

@@ -726,3 +726,311 @@ int pfo_step(pfo_grid* g, pfo_grid* saved, size_t n, double* pos, double* vel,
   pfo_g2p(g, saved, n, pos, vel, type, cfg->alpha_l, cfg->alpha_g);
   return pfo_advect(g, n, pos, type, vel, vol, cfg->dt, cfg->advect_order, cst, NULL, NULL);
 }
+
+/* ------------------------------------------------------------------ */
+/* Particle adaptivity (src/driver/particle_adaptivity3d.h)            */
+/* ------------------------------------------------------------------ */
+
+/* ParticleCellDomain3D::particleCell (particle_adaptivity3d.h:36-47): finite
+ * position, truncating (int) casts of (x - o) / dx, inside the grid. */
+static int adapt_cell(const pfo_grid* g, const double* x, int* i, int* j, int* k) {
+  if (!isfinite(x[0]) || !isfinite(x[1]) || !isfinite(x[2])) return 0;
+  *i = (int)((x[0] - g->ox) / g->dx);
+  *j = (int)((x[1] - g->oy) / g->dx);
+  *k = (int)((x[2] - g->oz) / g->dx);
+  return in_cells(g, *i, *j, *k);
+}
+
+static size_t lin_cell(const pfo_grid* g, int i, int j, int k) {
+  return (size_t)i + (size_t)g->nx * ((size_t)j + (size_t)g->ny * (size_t)k);
+}
+
+/* mix32 (particle_adaptivity3d.h:75-82): the 32-bit integer finaliser */
+static unsigned mix32(unsigned x) {
+  x ^= x >> 16;
+  x *= 0x7feb352du;
+  x ^= x >> 15;
+  x *= 0x846ca68bu;
+  x ^= x >> 16;
+  return x;
+}
+
+/* particleScore (particle_adaptivity3d.h:84-102): cell and 1/1024-cell
+ * quantised in-cell position hashed with the seed */
+unsigned pfo_particle_score(const pfo_grid* g, const double* x, int i, int j, int k, unsigned seed) {
+  const int qx = (int)((x[0] - (g->ox + i * g->dx)) / g->dx * 1024.0);
+  const int qy = (int)((x[1] - (g->oy + j * g->dx)) / g->dx * 1024.0);
+  const int qz = (int)((x[2] - (g->oz + k * g->dx)) / g->dx * 1024.0);
+  unsigned h = seed;
+  h ^= mix32((unsigned)i + 0x9e3779b9u);
+  h ^= mix32((unsigned)j + 0x85ebca6bu);
+  h ^= mix32((unsigned)k + 0xc2b2ae35u);
+  h ^= mix32((unsigned)(qx & 2047) + 0x27d4eb2fu);
+  h ^= mix32((unsigned)(qy & 2047) + 0x165667b1u);
+  h ^= mix32((unsigned)(qz & 2047) + 0xd3a2646cu);
+  return mix32(h);
+}
+
+/* slotScore (particle_adaptivity3d.h:104-109) */
+unsigned pfo_slot_score(size_t cell, int slot, unsigned seed) {
+  unsigned h = seed;
+  h ^= mix32((unsigned)cell + 0x68bc21ebu);
+  h ^= mix32((unsigned)slot + 0x02e5be93u);
+  return mix32(h);
+}
+
+/* Particles3DTP::eraseIf (src/particles/particles3d_tp.h:13-35): survivors
+ * keep their order */
+static size_t keep_only(size_t n, double* pos, double* vel, unsigned char* type, double* vol,
+                        const unsigned char* keep) {
+  size_t w = 0;
+  for (size_t r = 0; r < n; ++r) {
+    if (!keep[r]) continue;
+    if (w != r) {
+      memcpy(pos + 3 * w, pos + 3 * r, 3 * sizeof(double));
+      memcpy(vel + 3 * w, vel + 3 * r, 3 * sizeof(double));
+      type[w] = type[r];
+      vol[w] = vol[r];
+    }
+    ++w;
+  }
+  return w;
+}
+
+/* any flag set in the (2r+1)^3 box around (i, j, k), clipped to the grid */
+static int any_in_box(const pfo_grid* g, const unsigned char* flag, int i, int j, int k, int r) {
+  for (int kk = k - r; kk <= k + r; ++kk) {
+    if (kk < 0 || kk >= g->nz) continue;
+    for (int jj = j - r; jj <= j + r; ++jj) {
+      if (jj < 0 || jj >= g->ny) continue;
+      for (int ii = i - r; ii <= i + r; ++ii) {
+        if (ii < 0 || ii >= g->nx) continue;
+        if (flag[lin_cell(g, ii, jj, kk)]) return 1;
+      }
+    }
+  }
+  return 0;
+}
+
+/* applyNarrowBandAir (particle_adaptivity3d.h:111-166): gas particles (type 1)
+ * survive only in a valid cell within `radius` cells (Chebyshev) of a cell
+ * holding a liquid particle; nothing happens when no cell holds liquid. */
+int pfo_narrow_band_air(const pfo_grid* g, size_t* n, double* pos, double* vel, unsigned char* type, double* vol,
+                        int radius, pfo_band_stats* st) {
+  memset(st, 0, sizeof(*st));
+  const size_t nc = (size_t)g->nx * g->ny * g->nz;
+  unsigned char* liquid = (unsigned char*)calloc(nc ? nc : 1, 1);
+  unsigned char* keep = (unsigned char*)malloc(*n ? *n : 1);
+  if (!liquid || !keep) { free(liquid); free(keep); return -1; }
+  for (size_t p = 0; p < *n; ++p) {
+    int i, j, k;
+    if (type[p] != 0 || !adapt_cell(g, pos + 3 * p, &i, &j, &k)) continue;
+    unsigned char* f = &liquid[lin_cell(g, i, j, k)];
+    if (!*f) { *f = 1; ++st->liquid_cells; }
+  }
+  if (st->liquid_cells > 0) {
+    const int r = radius > 0 ? radius : 0;
+    for (size_t p = 0; p < *n; ++p) {
+      keep[p] = 1;
+      if (type[p] != 1) continue;
+      ++st->gas_before;
+      int i, j, k;
+      keep[p] = adapt_cell(g, pos + 3 * p, &i, &j, &k) && any_in_box(g, liquid, i, j, k, r);
+      if (keep[p]) ++st->gas_after;
+    }
+    const size_t m = keep_only(*n, pos, vel, type, vol, keep);
+    st->removed = (int)(*n - m);
+    *n = m;
+  }
+  free(liquid);
+  free(keep);
+  return 0;
+}
+
+typedef struct { size_t index, cell; unsigned score; double volume; } coarse_entry;
+
+static int coarse_less(const void* a, const void* b) {
+  const coarse_entry* x = (const coarse_entry*)a;
+  const coarse_entry* y = (const coarse_entry*)b;
+  if (x->cell != y->cell) return x->cell < y->cell ? -1 : 1;
+  if (x->score != y->score) return x->score < y->score ? -1 : 1;
+  return x->index < y->index ? -1 : (x->index > y->index);
+}
+
+/* applyTypedParticleCoarsening (particle_adaptivity3d.h:168-248): per cell
+ * the `target` particles of type ptype with the lowest (score, index) stay
+ * and share the cell's summed volume (summed in that order); the others of
+ * that type, and those of that type outside the grid, are erased. */
+int pfo_coarsen_particles(const pfo_grid* g, size_t* n, double* pos, double* vel, unsigned char* type, double* vol,
+                          int ptype, int target, unsigned seed, pfo_coarsen_stats* st) {
+  memset(st, 0, sizeof(*st));
+  const size_t tgt = (size_t)(target > 1 ? target : 1);
+  coarse_entry* e = (coarse_entry*)malloc((*n ? *n : 1) * sizeof(coarse_entry));
+  unsigned char* keep = (unsigned char*)calloc(*n ? *n : 1, 1);
+  if (!e || !keep) { free(e); free(keep); return -1; }
+  size_t ne = 0;
+  for (size_t p = 0; p < *n; ++p) {
+    if (type[p] != (unsigned char)ptype) continue;
+    ++st->before;
+    int i, j, k;
+    if (!adapt_cell(g, pos + 3 * p, &i, &j, &k)) continue;
+    e[ne].index = p;
+    e[ne].cell = lin_cell(g, i, j, k);
+    e[ne].score = pfo_particle_score(g, pos + 3 * p, i, j, k, seed);
+    e[ne].volume = vol[p];
+    ++ne;
+  }
+  qsort(e, ne, sizeof(coarse_entry), coarse_less);
+  for (size_t a = 0; a < ne;) {
+    size_t b = a + 1;
+    while (b < ne && e[b].cell == e[a].cell) ++b;
+    ++st->cells;
+    const size_t count = b - a;
+    if (count > tgt) ++st->overfull_cells;
+    const size_t keep_count = count < tgt ? count : tgt;
+    double sum = 0.0;
+    for (size_t t = a; t < b; ++t) sum += e[t].volume;
+    const double kept = keep_count > 0 ? sum / (double)keep_count : 0.0;
+    for (size_t t = 0; t < keep_count; ++t) {
+      keep[e[a + t].index] = 1;
+      vol[e[a + t].index] = kept;
+      ++st->after;
+    }
+    a = b;
+  }
+  for (size_t p = 0; p < *n; ++p)
+    if (type[p] != (unsigned char)ptype) keep[p] = 1;
+  const size_t m = keep_only(*n, pos, vel, type, vol, keep);
+  st->removed = (int)(*n - m);
+  *n = m;
+  free(e);
+  free(keep);
+  return 0;
+}
+
+/* applyLiquidParticleRefill (particle_adaptivity3d.h:250-374): every cell
+ * holding fewer than `target` liquid particles (near gas within
+ * interface_radius, when interface_only) gets target - count new liquid
+ * particles at sub-cell centres taken in slotScore order, with the cell's mean
+ * liquid velocity; the cell's liquid volume is split evenly over old and new.
+ * Cells are visited in linear order against an optional budget. */
+int pfo_refill_liquid(const pfo_grid* g, size_t* n, size_t cap, double* pos, double* vel, unsigned char* type,
+                      double* vol, int target, unsigned seed, int interface_only, int interface_radius, int max_added,
+                      pfo_refill_stats* st) {
+  memset(st, 0, sizeof(*st));
+  const int tgt = target > 1 ? target : 1;
+  const size_t nc = (size_t)g->nx * g->ny * g->nz;
+  const size_t n0 = *n;
+  int* count = (int*)calloc(nc + 1, sizeof(int));
+  size_t* start = (size_t*)calloc(nc + 1, sizeof(size_t));
+  size_t* list = (size_t*)malloc((n0 ? n0 : 1) * sizeof(size_t));
+  unsigned char* gas = (unsigned char*)calloc(nc ? nc : 1, 1);
+  long long* cell_of_p = (long long*)malloc((n0 ? n0 : 1) * sizeof(long long));
+  if (!count || !start || !list || !gas || !cell_of_p) {
+    free(count); free(start); free(list); free(gas); free(cell_of_p);
+    return -1;
+  }
+  /* liquid particles per cell, in particle order */
+  for (size_t p = 0; p < n0; ++p) {
+    int i, j, k;
+    cell_of_p[p] = -1;
+    if (!adapt_cell(g, pos + 3 * p, &i, &j, &k)) continue;
+    const size_t c = lin_cell(g, i, j, k);
+    if (type[p] == 0) {
+      cell_of_p[p] = (long long)c;
+      ++count[c];
+    } else if (type[p] == 1) {
+      gas[c] = 1;
+    }
+  }
+  for (size_t c = 0; c < nc; ++c) start[c + 1] = start[c] + (size_t)count[c];
+  {
+    size_t* fill = (size_t*)malloc((nc ? nc : 1) * sizeof(size_t));
+    if (!fill) { free(count); free(start); free(list); free(gas); free(cell_of_p); return -1; }
+    memcpy(fill, start, nc * sizeof(size_t));
+    for (size_t p = 0; p < n0; ++p)
+      if (cell_of_p[p] >= 0) list[fill[cell_of_p[p]]++] = p;
+    free(fill);
+  }
+  /* the total to add, for the capacity check before anything changes */
+  const int r = interface_radius > 0 ? interface_radius : 0;
+  long long budget = max_added > 0 ? max_added : 2147483647LL;
+  size_t to_add_total = 0;
+  {
+    long long b = budget;
+    for (size_t c = 0; c < nc; ++c) {
+      const int cnt = count[c];
+      if (cnt <= 0 || cnt >= tgt) continue;
+      const int i = (int)(c % (size_t)g->nx), j = (int)((c / (size_t)g->nx) % (size_t)g->ny),
+                k = (int)(c / ((size_t)g->nx * (size_t)g->ny));
+      if (interface_only && !any_in_box(g, gas, i, j, k, r)) continue;
+      if (b <= 0) continue;
+      const long long want = tgt - cnt, add = want < b ? want : b;
+      to_add_total += (size_t)add;
+      b -= add;
+    }
+  }
+  if (n0 + to_add_total > cap) {
+    free(count); free(start); free(list); free(gas); free(cell_of_p);
+    return -1;
+  }
+  for (size_t c = 0; c < nc; ++c) {
+    const int cnt = count[c];
+    if (cnt <= 0) continue;
+    ++st->cells;
+    st->before += cnt;
+    st->after += cnt;
+    const int i = (int)(c % (size_t)g->nx), j = (int)((c / (size_t)g->nx) % (size_t)g->ny),
+              k = (int)(c / ((size_t)g->nx * (size_t)g->ny));
+    const int near = any_in_box(g, gas, i, j, k, r);
+    if (near) ++st->interface_cells;
+    if (interface_only && !near) continue;
+    if (cnt >= tgt) continue;
+    ++st->underfull_cells;
+    if (budget <= 0) { st->budget_limited = 1; continue; }
+    double vsum = 0.0, u[3] = {0.0, 0.0, 0.0};
+    for (size_t t = start[c]; t < start[c + 1]; ++t) {
+      const size_t p = list[t];
+      vsum += vol[p];
+      for (int a = 0; a < 3; ++a) u[a] += vel[3 * p + a];
+    }
+    const double inv = 1.0 / (double)cnt;
+    const double avg[3] = {u[0] * inv, u[1] * inv, u[2] * inv};
+    int slots[8] = {0, 1, 2, 3, 4, 5, 6, 7};
+    for (int a = 1; a < 8; ++a) { /* insertion sort by (slotScore, slot) */
+      const int s = slots[a];
+      const unsigned ss = pfo_slot_score(c, s, seed);
+      int b = a - 1;
+      while (b >= 0) {
+        const unsigned sb = pfo_slot_score(c, slots[b], seed);
+        if (sb < ss || (sb == ss && slots[b] < s)) break;
+        slots[b + 1] = slots[b];
+        --b;
+      }
+      slots[b + 1] = s;
+    }
+    const int want = tgt - cnt;
+    const int add = (long long)want < budget ? want : (int)budget;
+    if (add < want) st->budget_limited = 1;
+    const double split = vsum / (double)(cnt + add);
+    for (size_t t = start[c]; t < start[c + 1]; ++t) vol[list[t]] = split;
+    for (int a = 0; a < add; ++a) {
+      const int s = slots[a & 7];
+      const double sx = 0.25 + 0.5 * (double)(s & 1);
+      const double sy = 0.25 + 0.5 * (double)((s >> 1) & 1);
+      const double sz = 0.25 + 0.5 * (double)((s >> 2) & 1);
+      const size_t q = (*n)++;
+      pos[3 * q + 0] = g->ox + ((double)i + sx) * g->dx;
+      pos[3 * q + 1] = g->oy + ((double)j + sy) * g->dx;
+      pos[3 * q + 2] = g->oz + ((double)k + sz) * g->dx;
+      for (int d = 0; d < 3; ++d) vel[3 * q + d] = avg[d];
+      type[q] = 0;
+      vol[q] = split;
+      ++st->added;
+      ++st->after;
+    }
+    budget -= add;
+  }
+  free(count); free(start); free(list); free(gas); free(cell_of_p);
+  return 0;
+}

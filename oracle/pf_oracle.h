@@ -98,6 +98,25 @@ int pfo_step(pfo_grid* g, pfo_grid* saved, size_t n, double* pos, double* vel,
              const unsigned char* type, const double* vol, const pfo_phase* pp,
              const pfo_step_cfg* cfg, pfo_solve_stats* sst, pfo_clamp_stats* cst);
 
+/* ---- particle adaptivity (src/driver/particle_adaptivity3d.h) ---------- */
+/* Particles are the caller's arrays (pos, vel: 3 doubles each, type, vol);
+ * every function updates them in place and *n with the new count.  Erasures
+ * keep the survivors' order (Particles3DTP::eraseIf); refill appends at the
+ * end and fails (-1, nothing changed) if *n would exceed cap. */
+typedef struct { int removed, liquid_cells, gas_before, gas_after; } pfo_band_stats;
+typedef struct { int removed, cells, overfull_cells, before, after; } pfo_coarsen_stats;
+typedef struct { int added, cells, interface_cells, underfull_cells, budget_limited, before, after; } pfo_refill_stats;
+
+unsigned pfo_particle_score(const pfo_grid* g, const double* x, int i, int j, int k, unsigned seed);
+unsigned pfo_slot_score(size_t cell, int slot, unsigned seed);
+int pfo_narrow_band_air(const pfo_grid* g, size_t* n, double* pos, double* vel, unsigned char* type, double* vol,
+                        int radius, pfo_band_stats* st);
+int pfo_coarsen_particles(const pfo_grid* g, size_t* n, double* pos, double* vel, unsigned char* type, double* vol,
+                          int ptype, int target, unsigned seed, pfo_coarsen_stats* st);
+int pfo_refill_liquid(const pfo_grid* g, size_t* n, size_t cap, double* pos, double* vel, unsigned char* type,
+                      double* vol, int target, unsigned seed, int interface_only, int interface_radius, int max_added,
+                      pfo_refill_stats* st);
+
 #ifdef __cplusplus
 }
 #endif

@@ -10,8 +10,11 @@
 //   SparseSim3DTP::step()   (src/driver/sparse_sim3d_tp.cpp:854-884)
 //   calibrateRhoTilde0      (src/transfer/transfer3d_tp.cpp:29-36)
 //   phiFromRawDensity / betaFromPhi (src/physics/phasefield.h:10-18)
+//   pa3d::applyNarrowBandAir / applyTypedParticleCoarsening /
+//   applyLiquidParticleRefill (src/driver/particle_adaptivity3d.h:111-374)
 // and converts between its SparseMacGrid3D<4> block pool and dense arrays
 // plus one activity byte per 4^3 block.
+#include "driver/particle_adaptivity3d.h"
 #include "driver/sparse_ops3d_tp.h"
 #include "driver/sparse_sim3d_tp.h"
 #include "grid/sparse_mac_grid3d.h"
@@ -205,6 +208,43 @@ double pfr_phi_from_raw(double raw, const double* phase) {
 double pfr_beta_from_raw(double raw, const double* phase) {
   PhaseParams pp = phaseOf(phase);
   return betaFromPhi(phiFromRawDensity(raw, pp), pp);
+}
+
+// ---- particle adaptivity on the handle's particles and grid domain ----
+static pa3d::ParticleCellDomain3D domainOf(const Handle* h) {
+  const auto& g = h->sim.grid;
+  return pa3d::ParticleCellDomain3D{g.nx, g.ny, g.nz, g.dx, g.ox, g.oy, g.oz};
+}
+
+// out4: removed, liquidCells, gasBefore, gasAfter
+int pfr_narrow_band_air(void* hp, int radius, int* out4) {
+  Handle* h = static_cast<Handle*>(hp);
+  const auto r = pa3d::applyNarrowBandAir(h->sim.particles, domainOf(h), true, radius);
+  const int v[4] = {r.removed, r.liquidCells, r.gasBefore, r.gasAfter};
+  std::memcpy(out4, v, sizeof(v));
+  return 0;
+}
+
+// out5: removed, cells, overfullCells, particlesBefore, particlesAfter
+int pfr_coarsen_particles(void* hp, int ptype, int target, unsigned seed, int* out5) {
+  Handle* h = static_cast<Handle*>(hp);
+  const auto r = pa3d::applyTypedParticleCoarsening(h->sim.particles, domainOf(h), true,
+                                                    static_cast<unsigned char>(ptype), target, seed);
+  const int v[5] = {r.removed, r.cells, r.overfullCells, r.particlesBefore, r.particlesAfter};
+  std::memcpy(out5, v, sizeof(v));
+  return 0;
+}
+
+// out7: added, cells, interfaceCells, underfullCells, budgetLimited, particlesBefore, particlesAfter
+int pfr_refill_liquid(void* hp, int target, unsigned seed, int interface_only, int interface_radius,
+                      int max_added, int* out7) {
+  Handle* h = static_cast<Handle*>(hp);
+  const auto r = pa3d::applyLiquidParticleRefill(h->sim.particles, domainOf(h), true, target, seed,
+                                                 interface_only != 0, interface_radius, max_added);
+  const int v[7] = {r.added, r.cells, r.interfaceCells, r.underfullCells, r.budgetLimited, r.particlesBefore,
+                    r.particlesAfter};
+  std::memcpy(out7, v, sizeof(v));
+  return 0;
 }
 
 }  // extern "C"
