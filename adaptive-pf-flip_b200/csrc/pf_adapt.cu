@@ -539,8 +539,10 @@ int refill_liquid(pf_ctx* ctx, int target, unsigned seed, int interface_only, in
   const long long budget = max_added > 0 ? (long long)max_added : (long long)INT_MAX;
   const long long total = s->h_stats[4];
   const long long added = min(total, budget);
-  if ((size_t)n + (size_t)added > ctx->cap)
+  if ((size_t)n + (size_t)added > ctx->cap) {
+    if (st) *st = pf_refill_stats{(int)added, 0, 0, 0, 0, 0, 0};  // what it would add
     return set_error(ctx, PF_ERR_CAPACITY, "refill would exceed max_particles");
+  }
   if (added > 0)
     (++ctx->launches), k_refill_apply<<<8 * ctx->num_sms, kNT, 0, ctx->stream>>>(
         ctx->g, P, (size_t)n, s->cnt, s->start, s->sorted, s->wanted, s->woff, budget, seed);

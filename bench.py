@@ -475,6 +475,72 @@ def run_full_step(pf, n=48, steps=20, seed=0, solvers=("plain",), warmup=3):
     return out
 
 
+def run_adapt(pf, n=128, seed=0, reps=5, cpu=True):
+    """Particle adaptivity (src/driver/particle_adaptivity3d.h) on the
+    Rayleigh-Taylor scene: each operation on the full particle set, device time
+    (CUDA events on the library stream) per call over `reps` calls, each call on
+    a freshly uploaded copy (upload untimed).  The reference's own pa3d
+    functions (oracle/_ref, single-threaded) run once on the same particles.
+    Operations: narrow band r = 2, gas coarsening to 4, liquid coarsening to 4,
+    liquid refill to 10 per cell (every liquid cell gains two)."""
+    import torch
+    sc = pf.scenes.rayleigh_taylor(n, seed=seed)
+    npart = len(sc["pos"])
+    L = pf._lib
+    ops = [
+        ("narrow_band_air", L.BandStats, lambda lib, h, st: lib.pf_narrow_band_air(h, 2, C.byref(st)),
+         lambda lib, h, out: lib.pfr_narrow_band_air(h, 2, out), 4),
+        ("gas_coarsening", L.CoarsenStats,
+         lambda lib, h, st: lib.pf_coarsen_particles(h, 1, 4, 0x9e3779b9, C.byref(st)),
+         lambda lib, h, out: lib.pfr_coarsen_particles(h, 1, 4, 0x9e3779b9, out), 5),
+        ("liquid_coarsening", L.CoarsenStats,
+         lambda lib, h, st: lib.pf_coarsen_particles(h, 0, 4, 0x7f4a7c15, C.byref(st)),
+         lambda lib, h, out: lib.pfr_coarsen_particles(h, 0, 4, 0x7f4a7c15, out), 5),
+        ("liquid_refill", L.RefillStats,
+         lambda lib, h, st: lib.pf_refill_liquid(h, 10, 0x6a09e667, 0, 1, 0, C.byref(st)),
+         lambda lib, h, out: lib.pfr_refill_liquid(h, 10, 0x6a09e667, 0, 1, 0, out), 7),
+    ]
+    g = pf.SparseMacGrid3D(n, n, n, sc["dx"], max_particles=int(npart * 1.3))
+    lib = g.lib
+    stream = torch.cuda.ExternalStream(lib.pf_stream(g.ctx))
+    arrays = [np.ascontiguousarray(sc[k], dt) for k, dt in (("pos", np.float32), ("vel", np.float32),
+                                                             ("type", np.uint8), ("volume", np.float32))]
+    out = {"workload": f"rayleigh_taylor_{n}: {npart} particles, each operation on the full set, "
+                       f"{reps} device-timed calls", "unit": "particles/s", "ops": {}}
+    for name, Stats, call, _, _ in ops:
+        ms = []
+        st = Stats()
+        for _ in range(reps + 1):  # the first call allocates the scratch: untimed
+            L.check(lib.pf_upload_particles(g.ctx, npart, *[a.ctypes.data for a in arrays]), g.ctx, "upload")
+            lib.pf_sync(g.ctx)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            L.check(call(lib, g.ctx, st), g.ctx, name)
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        t = statistics.median(ms[1:])
+        out["ops"][name] = {"gpu_ms": t, "particles_per_s": npart / (t / 1000.0), "stats": list(st.as_tuple())}
+    g.close()
+    if cpu:
+        import oracle as O
+        ps = O.Particles(sc["pos"].astype(np.float64), sc["vel"].astype(np.float64), sc["type"],
+                         sc["volume"].astype(np.float64))
+        rg = O.ReferenceGrid(n, n, n, sc["dx"])
+        for name, _, _, rcall, nst in ops:
+            rg._put(ps)
+            res = np.zeros(nst, np.int32)
+            t0 = time.perf_counter()
+            rcall(rg.lib, rg.h, res)
+            t1 = time.perf_counter()
+            rec = out["ops"][name]
+            rec["cpu_reference_ms"] = 1000.0 * (t1 - t0)
+            rec["speedup_vs_reference"] = rec["cpu_reference_ms"] / rec["gpu_ms"]
+            rec["reference_stats_equal"] = [int(v) for v in res] == rec["stats"]
+        out["cpu_cores"] = 1
+    return out
+
+
 def run_ours(args, rank, world, local, dist):
     import torch
     pf = load_pkg()
@@ -543,6 +609,7 @@ def run_ours(args, rank, world, local, dist):
         line["pcg"] = run_pcg(pf, args.pcg_n, pcg_modes(pf, args.pcg_modes.split(",")))
         line["full_step"] = run_full_step(pf, n=args.full_step_n, steps=args.full_step_steps,
                                           solvers=("plain", "learned"))
+        line["adaptivity"] = run_adapt(pf, n=args.adapt_n, cpu=not args.no_cpu_baseline)
     if rank == 0 and not args.no_cpu_baseline:
         cores = 8
         np_s, times = cpu_reference_sample(sc, slab_cells=args.cpu_slab, steps=1)
@@ -585,7 +652,7 @@ def main():
     ap.add_argument("--n", type=int, default=128, help="grid cells per axis (128 is the benchmarked workload)")
     ap.add_argument("--cpu-slab", type=int, default=4, help="x-columns of the scene in the CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-extras", action="store_true", help="skip the PCG and full-step blocks")
+    ap.add_argument("--no-extras", action="store_true", help="skip the PCG, full-step and adaptivity blocks")
     ap.add_argument("--pcg-n", type=int, default=256, help="grid of the pressure-only block")
     ap.add_argument("--pcg-only", action="store_true", help="run only the pressure-only block")
     ap.add_argument("--pcg-max-iter", type=int, default=20000, help="iteration cap of the pressure-only block")
@@ -599,6 +666,8 @@ def main():
     ap.add_argument("--full-step-n", type=int, default=128, help="grid of the full-step block (Rayleigh-Taylor)")
     ap.add_argument("--full-step-steps", type=int, default=5, help="timed steps of the full-step block")
     ap.add_argument("--full-step-only", action="store_true", help="run only the full-step block")
+    ap.add_argument("--adapt-n", type=int, default=128, help="grid of the particle-adaptivity block")
+    ap.add_argument("--adapt-only", action="store_true", help="run only the particle-adaptivity block")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
@@ -606,6 +675,10 @@ def main():
         rank = int(os.environ.get("RANK", "0"))
         world = int(os.environ.get("WORLD_SIZE", "1"))
         run_reference(args, rank, world)
+        return
+    if args.adapt_only:  # the particle-adaptivity block alone
+        pf = load_pkg()
+        print(json.dumps(run_adapt(pf, n=args.adapt_n, cpu=not args.no_cpu_baseline)), flush=True)
         return
     if args.full_step_only:  # the full-step block alone
         pf = load_pkg()

@@ -247,7 +247,8 @@ PFGPU_API int pf_coarsen_particles(pf_ctx* ctx, int type, int per_cell_target, u
                                    pf_coarsen_stats* stats);
 /* pa3d::applyLiquidParticleRefill (:250-374): underfull liquid cells get new
  * particles at sub-cell centres.  PF_ERR_CAPACITY, with nothing changed, when
- * the result would exceed max_particles. */
+ * the result would exceed max_particles; stats->added then holds the number
+ * of particles the call would have added. */
 PFGPU_API int pf_refill_liquid(pf_ctx* ctx, int per_cell_target, unsigned seed, int interface_only,
                                int interface_radius, int max_added, pf_refill_stats* stats);
 /* Adaptivity run by pf_step (NULL: none, the default); the results of the

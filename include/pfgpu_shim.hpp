@@ -50,11 +50,40 @@ class ContextCache {
     ++clock_;
     for (Entry& e : entries_) {
       if (e.key == (const void*)&g && e.nx == g.nx && e.ny == g.ny && e.nz == g.nz && e.dx == g.dx &&
-          e.cap >= particles) {
+          e.ox == g.ox && e.oy == g.oy && e.oz == g.oz && e.cap >= particles) {
         e.used = clock_;
         return e.ctx;
       }
     }
+    return create((const void*)&g, g.nx, g.ny, g.nz, g.dx, g.ox, g.oy, g.oz, particles);
+  }
+
+  // A context for a particle cell domain (nx, ny, nz, dx, ox, oy, oz), which
+  // has no lasting address: matched by shape and origin.
+  template <class Domain>
+  pf_ctx* get_domain(const Domain& d, size_t particles) {
+    ++clock_;
+    for (Entry& e : entries_) {
+      if (!e.key && e.nx == d.nx && e.ny == d.ny && e.nz == d.nz && e.dx == d.dx && e.ox == d.ox &&
+          e.oy == d.oy && e.oz == d.oz && e.cap >= particles) {
+        e.used = clock_;
+        return e.ctx;
+      }
+    }
+    return create(nullptr, d.nx, d.ny, d.nz, d.dx, d.ox, d.oy, d.oz, particles);
+  }
+
+ private:
+  struct Entry {
+    const void* key;
+    int nx, ny, nz;
+    double dx, ox, oy, oz;
+    size_t cap;
+    pf_ctx* ctx;
+    unsigned long long used;
+  };
+  pf_ctx* create(const void* key, int nx, int ny, int nz, double dx, double ox, double oy, double oz,
+                 size_t particles) {
     if (entries_.size() >= kMax) {
       size_t lru = 0;
       for (size_t i = 1; i < entries_.size(); ++i)
@@ -62,22 +91,12 @@ class ContextCache {
       pf_destroy(entries_[lru].ctx);
       entries_.erase(entries_.begin() + (long)lru);
     }
-    pf_grid_desc d{g.nx, g.ny, g.nz, g.dx, g.ox, g.oy, g.oz, particles > 0 ? particles : 1, 0};
+    pf_grid_desc d{nx, ny, nz, dx, ox, oy, oz, particles > 0 ? particles : 1, 0};
     pf_ctx* ctx = nullptr;
     check(pf_create(&d, &ctx), nullptr, "pf_create");
-    entries_.push_back(Entry{(const void*)&g, g.nx, g.ny, g.nz, g.dx, d.max_particles, ctx, clock_});
+    entries_.push_back(Entry{key, nx, ny, nz, dx, ox, oy, oz, d.max_particles, ctx, clock_});
     return ctx;
   }
-
- private:
-  struct Entry {
-    const void* key;
-    int nx, ny, nz;
-    double dx;
-    size_t cap;
-    pf_ctx* ctx;
-    unsigned long long used;
-  };
   static constexpr size_t kMax = 4;
   std::vector<Entry> entries_;
   unsigned long long clock_ = 0;
@@ -238,6 +257,66 @@ void advect(Particles& ps, const Grid& g, double dt, Stats* stats, int order, Bu
       buffer->record((unsigned char)e[0], V{e[1], e[2], e[3]}, V{e[4], e[5], e[6]}, e[7]);
     }
   }
+}
+
+// ---- particle adaptivity (src/driver/particle_adaptivity3d.h:111-374) ----
+// Domain has the members of pa3d::ParticleCellDomain3D (nx, ny, nz, dx, ox,
+// oy, oz).  The particle set is rewritten: erasures keep the survivors' order,
+// refill appends.
+
+// the device particle set -> the caller's, resized to the device count
+template <class Particles>
+void download_all_particles(pf_ctx* ctx, Particles& ps) {
+  const size_t n = pf_num_particles(ctx);
+  ps.pos.resize(n);
+  ps.vel.resize(n);
+  ps.type.resize(n);
+  ps.volume.resize(n);
+  if (n)
+    check(pf_download_particles_f64(ctx, &ps.pos[0].x, &ps.vel[0].x, (uint8_t*)ps.type.data(), ps.volume.data()),
+          ctx, "pf_download_particles_f64");
+}
+
+template <class Particles, class Domain>
+pf_band_stats narrow_band_air(Particles& ps, const Domain& d, int radius) {
+  pf_ctx* ctx = cache().get_domain(d, ps.size());
+  upload_particles(ctx, ps);
+  pf_band_stats st{};
+  check(pf_narrow_band_air(ctx, radius, &st), ctx, "pf_narrow_band_air");
+  download_all_particles(ctx, ps);
+  return st;
+}
+
+template <class Particles, class Domain>
+pf_coarsen_stats coarsen_particles(Particles& ps, const Domain& d, int type, int target, unsigned seed) {
+  pf_ctx* ctx = cache().get_domain(d, ps.size());
+  upload_particles(ctx, ps);
+  pf_coarsen_stats st{};
+  check(pf_coarsen_particles(ctx, type, target, seed, &st), ctx, "pf_coarsen_particles");
+  download_all_particles(ctx, ps);
+  return st;
+}
+
+// A context too small for the result is replaced by one that holds it: the
+// failed call reports in `added` how many particles it would add.
+template <class Particles, class Domain>
+pf_refill_stats refill_liquid(Particles& ps, const Domain& d, int target, unsigned seed, bool interface_only,
+                              int interface_radius, int max_added) {
+  size_t cap = ps.size();
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    pf_ctx* ctx = cache().get_domain(d, cap);
+    upload_particles(ctx, ps);
+    pf_refill_stats st{};
+    const int rc = pf_refill_liquid(ctx, target, seed, interface_only ? 1 : 0, interface_radius, max_added, &st);
+    if (rc == PF_ERR_CAPACITY && attempt == 0) {
+      cap = ps.size() + (size_t)st.added;
+      continue;
+    }
+    check(rc, ctx, "pf_refill_liquid");
+    download_all_particles(ctx, ps);
+    return st;
+  }
+  return pf_refill_stats{};
 }
 
 }  // namespace pfgpu
