@@ -17,6 +17,7 @@ same names, argument meanings and order:
     applyLiquidParticleRefill(particles, grid, enabled, target, seed, interfaceOnly,
                               interfaceRadius, maxAddedPerStep)
                                                             src/driver/particle_adaptivity3d.h:264
+    diagnoseSparseInterface3D(grid, phase)                  src/driver/interface_diagnostics3d.cpp:363
     SparseMacGrid3D, Particles3DTP, PhaseParams             src/grid/sparse_mac_grid3d.h,
                                                             src/particles/particles3d_tp.h,
                                                             src/physics/phasefield.h
@@ -31,7 +32,7 @@ from .learned import LearnedCoarseSolver
 from .sparse import (ParticleEscapeBuffer3D, ParticleEscapeStats3D, Particles3DTP, PhaseParams, SolverConfig,
                      SparseMacGrid3D, SparseSim3DTP, applyGasParticleCoarsening, applyLiquidParticleRefill,
                      applyNarrowBandAir, applyTypedParticleCoarsening, betaFromPhi, calibrateRhoTilde0,
-                     densityFromPhi, etaPhi, phiFromRawDensity, spAdvect3D_tp, spG2P3D_tp, spP2G3D_tp,
+                     densityFromPhi, diagnoseSparseInterface3D, etaPhi, phiFromRawDensity, spAdvect3D_tp, spG2P3D_tp, spP2G3D_tp,
                      spProjectStepVC3D)
 from . import scenes
 
@@ -44,4 +45,5 @@ __all__ = [
     "spP2G3D_tp", "spProjectStepVC3D", "spG2P3D_tp", "spAdvect3D_tp", "calibrateRhoTilde0",
     "etaPhi", "phiFromRawDensity", "densityFromPhi", "betaFromPhi", "scenes",
     "applyNarrowBandAir", "applyTypedParticleCoarsening", "applyGasParticleCoarsening", "applyLiquidParticleRefill",
+    "diagnoseSparseInterface3D",
 ]

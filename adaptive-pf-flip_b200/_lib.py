@@ -38,10 +38,11 @@ EXPORTS = (
     "pf_learned_train",
     "pf_learned_eval", "pf_learned_adam",
     "pf_narrow_band_air", "pf_coarsen_particles", "pf_refill_liquid", "pf_set_adaptivity", "pf_get_adaptivity_stats",
+    "pf_interface_diagnostics", "pf_get_interface_stats",
 )
 
 STAGES = ("bin", "sort", "splat", "normalize", "mark", "boundary", "project", "pcg", "g2p", "precond_setup",
-          "adapt")
+          "adapt", "diag")
 
 
 class GridDesc(C.Structure):
@@ -125,6 +126,14 @@ class AdaptCfg(C.Structure):
                  refill_interface_radius=1)
         d.update(kw)
         super().__init__(**d)
+
+
+class InterfaceStats(_Stats):
+    """pf_interface_stats: InterfaceDiagnostics3D (src/driver/interface_diagnostics3d.h:7-19)"""
+    _fields_ = [("sample_cells", C.c_int), ("interface_cells", C.c_int), ("finite", C.c_int),
+                ("surface_tension_candidate", C.c_int), ("phi_min", C.c_double), ("phi_max", C.c_double),
+                ("phi_mean", C.c_double), ("grad_mean", C.c_double), ("grad_max", C.c_double),
+                ("curvature_abs_mean", C.c_double), ("curvature_abs_max", C.c_double)]
 
 
 class AdaptStats(C.Structure):
@@ -212,6 +221,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "pf_refill_liquid": (i, [vp, i, C.c_uint, i, i, i, P(RefillStats)]),
         "pf_set_adaptivity": (i, [vp, P(AdaptCfg)]),
         "pf_get_adaptivity_stats": (i, [vp, P(AdaptStats)]),
+        "pf_interface_diagnostics": (i, [vp, P(Phase), P(InterfaceStats)]),
+        "pf_get_interface_stats": (i, [vp, P(InterfaceStats)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

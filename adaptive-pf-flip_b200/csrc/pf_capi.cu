@@ -48,6 +48,7 @@ void free_all(pf_ctx* c) {
   auto F = [](void* p) { if (p) cudaFree(p); };
   pf::coarse_release(c);
   pf::adapt_free(c);
+  pf::diag_free(c);
   F(c->tile_slot); F(c->slot_tile); F(c->d_nslots); F(c->tile_need); F(c->tile_new); F(c->tile_rank);
   for (int f = 0; f < PF_NFIELDS; ++f) { F(c->fld[f]); F(c->act4[f]); }
   for (int a = 0; a < PF_NSAVED; ++a) F(c->saved[a]);
@@ -641,6 +642,8 @@ int pf_step(pf_ctx* ctx, const pf_step_cfg* cfg, pf_step_stats* stats) {
   if (rc) return rc;
   rc = pf::p2g(ctx, &cfg->phase, cfg->Vp);  // normalisation without the fused extras
   if (rc) return rc;
+  rc = pf::interface_diagnostics(ctx, &cfg->phase, nullptr);  // diagnoseSparseInterface3D after P2G
+  if (rc) return rc;
   rc = pf::save_velocity(ctx);
   if (rc) return rc;
   rc = pf::apply_gravity(ctx, cfg->dt, cfg->gravity);
@@ -692,6 +695,18 @@ int pf_refill_liquid(pf_ctx* ctx, int per_cell_target, unsigned seed, int interf
   const int rc = take_upload(ctx);
   if (rc) return rc;
   return pf::refill_liquid(ctx, per_cell_target, seed, interface_only, interface_radius, max_added, stats);
+}
+
+int pf_interface_diagnostics(pf_ctx* ctx, const pf_phase* phase, pf_interface_stats* stats) {
+  if (!ctx || !phase) return PF_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  return pf::interface_diagnostics(ctx, phase, stats);
+}
+
+int pf_get_interface_stats(const pf_ctx* ctx, pf_interface_stats* out) {
+  if (!ctx || !out) return PF_ERR_INVALID;
+  *out = ctx->diag_last;
+  return PF_OK;
 }
 
 int pf_set_adaptivity(pf_ctx* ctx, const pf_adapt_cfg* cfg) {

@@ -91,6 +91,9 @@ struct pf_ctx {
   bool adapt_on = false;
   pf_adapt_cfg adapt_cfg{};
   pf_adapt_stats adapt_last{};
+  // interface diagnostics: scratch (its own module) and the last result
+  void* idiag = nullptr;
+  pf_interface_stats diag_last{};
 
   // ---- misc ----
   int* d_clamp = nullptr;      // 8 counters
@@ -159,6 +162,10 @@ int refill_liquid(pf_ctx* ctx, int target, unsigned seed, int interface_only, in
                   pf_refill_stats* st);
 int apply_adaptivity(pf_ctx* ctx, const pf_adapt_cfg& cfg, pf_adapt_stats* st);
 void adapt_free(pf_ctx* ctx);
+
+// diag.cu
+int interface_diagnostics(pf_ctx* ctx, const pf_phase* ph, pf_interface_stats* st);
+void diag_free(pf_ctx* ctx);
 
 // capi.cu: the second particle set (asynchronous uploads, compaction target)
 int ensure_back_set(pf_ctx* ctx);

@@ -371,6 +371,13 @@ def spAdvect3D_tp(ps, g: SparseMacGrid3D, dt, stats: ParticleEscapeStats3D | Non
 # device-resident step (SparseSim3DTP)
 # ---------------------------------------------------------------------------
 
+def diagnoseSparseInterface3D(g: SparseMacGrid3D, pp: PhaseParams) -> L.InterfaceStats:
+    """diagnoseSparseInterface3D (src/driver/interface_diagnostics3d.cpp:363-379) on the device."""
+    st = L.InterfaceStats()
+    L.check(g.lib.pf_interface_diagnostics(g.ctx, C.byref(pp._c()), C.byref(st)), g.ctx, "pf_interface_diagnostics")
+    return st
+
+
 # ---------------------------------------------------------------------------
 # particle adaptivity (src/driver/particle_adaptivity3d.h), on the device; the
 # grid supplies the cell domain (ParticleCellDomain3D) and holds the particles
@@ -454,6 +461,7 @@ class SparseSim3DTP:
         self.liquid_particle_refill_interface_radius = 1
         self.liquid_particle_refill_max_added_per_step = 0
         self.adaptivity_last = L.AdaptStats()
+        self.interface_diagnostics_last = L.InterfaceStats()
 
     def set_particles(self, pos, vel, type, volume):
         """Upload FP32 (n,3) pos/vel, uint8 type, FP32 volume (host or device pointers via numpy)."""
@@ -538,6 +546,8 @@ class SparseSim3DTP:
         L.check(lib.pf_step(ctx, C.byref(cfg), C.byref(st)), ctx, "pf_step")
         if self._adaptivity_on():
             L.check(lib.pf_get_adaptivity_stats(ctx, C.byref(self.adaptivity_last)), ctx, "pf_get_adaptivity_stats")
+        L.check(lib.pf_get_interface_stats(ctx, C.byref(self.interface_diagnostics_last)), ctx,
+                "pf_get_interface_stats")
         self.n = int(lib.pf_num_particles(ctx))
         self.last_stats = st
         return st

@@ -132,6 +132,12 @@ typedef struct {
   int active_tiles;      /* pooled 8^3 tiles */
 } pf_step_stats;
 
+/* InterfaceDiagnostics3D (src/driver/interface_diagnostics3d.h:7-19) */
+typedef struct {
+  int sample_cells, interface_cells, finite, surface_tension_candidate;
+  double phi_min, phi_max, phi_mean, grad_mean, grad_max, curvature_abs_mean, curvature_abs_max;
+} pf_interface_stats;
+
 /* Particle adaptivity results (src/driver/particle_adaptivity3d.h:49-72:
  * NarrowBandAirResult3D, GasParticleCoarseningResult3D,
  * LiquidParticleRefillResult3D). */
@@ -232,6 +238,15 @@ PFGPU_API int pf_advect(pf_ctx* ctx, double dt, int order, pf_clamp_stats* stats
 /* One full step in the reference's step() order, device-resident. */
 PFGPU_API int pf_step(pf_ctx* ctx, const pf_step_cfg* cfg, pf_step_stats* stats);
 
+/* diagnoseSparseInterface3D (src/driver/interface_diagnostics3d.cpp:363-379)
+ * on the context's grid: phase field, gradient and curvature statistics over
+ * the fluid cells.  Counts, minima and maxima equal the reference's; the
+ * means agree to rounding (summed in another order).  pf_step computes them
+ * after P2G, as SparseSim3DTP::step() does; pf_get_interface_stats returns
+ * the last step's. */
+PFGPU_API int pf_interface_diagnostics(pf_ctx* ctx, const pf_phase* phase, pf_interface_stats* stats);
+PFGPU_API int pf_get_interface_stats(const pf_ctx* ctx, pf_interface_stats* out);
+
 /* ---- particle adaptivity (src/driver/particle_adaptivity3d.h) ----------
  * Each call rewrites the context's particle set on the device; erasures keep
  * the survivors' order, refill appends after the last particle.  Particle
@@ -272,6 +287,7 @@ enum pf_stage {
   PF_STAGE_G2P,          /* G2P and/or advection */
   PF_STAGE_PRECOND_SETUP, /* LEARNED solves: coarse operator, gate network, neighbour table */
   PF_STAGE_ADAPT,        /* particle adaptivity: narrow band, coarsening, refill */
+  PF_STAGE_DIAG,         /* interface diagnostics */
   PF_NSTAGES
 };
 typedef struct {

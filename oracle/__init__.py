@@ -81,6 +81,17 @@ class RefillStats(C.Structure):
         return tuple(getattr(self, n) for n, _ in self._fields_)
 
 
+class InterfaceStats(C.Structure):
+    """InterfaceDiagnostics3D (src/driver/interface_diagnostics3d.h:7-19)"""
+    _fields_ = [("sample_cells", C.c_int), ("interface_cells", C.c_int), ("finite", C.c_int),
+                ("surface_tension_candidate", C.c_int), ("phi_min", C.c_double), ("phi_max", C.c_double),
+                ("phi_mean", C.c_double), ("grad_mean", C.c_double), ("grad_max", C.c_double),
+                ("curvature_abs_mean", C.c_double), ("curvature_abs_max", C.c_double)]
+
+    def as_tuple(self):
+        return tuple(getattr(self, n) for n, _ in self._fields_)
+
+
 class ClampStats(C.Structure):
     _fields_ = [("clamped_liquid", C.c_int), ("clamped_gas", C.c_int),
                 ("x_lo", C.c_int), ("x_hi", C.c_int), ("y_lo", C.c_int),
@@ -200,6 +211,7 @@ def oracle_lib():
                                           C.POINTER(CoarsenStats)]
     lib.pfo_refill_liquid.argtypes = [vp, sp, C.c_size_t, _dp, _dp, _up, _dp, C.c_int, C.c_uint, C.c_int, C.c_int,
                                       C.c_int, C.POINTER(RefillStats)]
+    lib.pfo_interface_diagnostics.argtypes = [vp, C.POINTER(_Phase), C.POINTER(InterfaceStats)]
     lib._typed = True
     return lib
 
@@ -234,6 +246,7 @@ def ref_lib():
     lib.pfr_narrow_band_air.argtypes = [vp, C.c_int, _ip]
     lib.pfr_coarsen_particles.argtypes = [vp, C.c_int, C.c_int, C.c_uint, _ip]
     lib.pfr_refill_liquid.argtypes = [vp, C.c_int, C.c_uint, C.c_int, C.c_int, C.c_int, _ip]
+    lib.pfr_interface_diagnostics.argtypes = [vp, _dp, _ip, _dp]
     lib._typed = True
     return lib
 
@@ -460,6 +473,13 @@ class Oracle:
         return st
 
 
+    def interface_diagnostics(self, g, pp: PhaseParams):
+        """diagnoseSparseInterface3D (src/driver/interface_diagnostics3d.cpp:363-379)"""
+        st = InterfaceStats()
+        self.lib.pfo_interface_diagnostics(g.h, C.byref(pp.as_struct()), C.byref(st))
+        return st
+
+
 def _truncate(ps: Particles, n):
     ps.pos, ps.vel = ps.pos[:n].copy(), ps.vel[:n].copy()
     ps.type, ps.volume = ps.type[:n].copy(), ps.volume[:n].copy()
@@ -515,6 +535,11 @@ class Reference:
         self.lib.pfr_step(g.h, pp.as_array(), arr)
         if take:
             g._take(ps)
+
+    def interface_diagnostics(self, g: ReferenceGrid, pp: PhaseParams):
+        iv, dv = np.zeros(4, np.int32), np.zeros(7, np.float64)
+        self.lib.pfr_interface_diagnostics(g.h, pp.as_array(), iv, dv)
+        return InterfaceStats(*[int(v) for v in iv], *[float(v) for v in dv])
 
     # ---- particle adaptivity, the reference's own pa3d functions ----
     def narrow_band_air(self, g: ReferenceGrid, ps: Particles, radius=2):

@@ -150,7 +150,7 @@ double pfo_phi_from_raw(double raw, const pfo_phase* pp) {
   double excess = raw - rmin;
   if (excess < 0.0) excess = 0.0;
   const double v = sqrt(excess / (pp->alpha_phi * pp->rho_tilde_0 * pp->rho_l));
-  return v < 1.0 ? v : 1.0;
+  return 1.0 < v ? 1.0 : v; /* std::min(v, 1.0), NaN included */
 }
 
 double pfo_beta_from_raw(double raw, const pfo_phase* pp) {
@@ -1032,5 +1032,121 @@ int pfo_refill_liquid(const pfo_grid* g, size_t* n, size_t cap, double* pos, dou
     budget -= add;
   }
   free(count); free(start); free(list); free(gas); free(cell_of_p);
+  return 0;
+}
+
+/* ------------------------------------------------------------------ */
+/* Interface diagnostics (src/driver/interface_diagnostics3d.cpp)      */
+/* ------------------------------------------------------------------ */
+
+static int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+/* sparseCellPhi (interface_diagnostics3d.cpp:138-148): the mean phase field of
+ * the cell's six face raw masses; 0 outside the grid */
+static double cell_phi(const pfo_grid* g, const pfo_phase* pp, int i, int j, int k) {
+  if (!in_cells(g, i, j, k)) return 0.0;
+  double sum = 0.0;
+  sum += pfo_phi_from_raw(get(g, PFO_MU, i, j, k), pp);
+  sum += pfo_phi_from_raw(get(g, PFO_MU, i + 1, j, k), pp);
+  sum += pfo_phi_from_raw(get(g, PFO_MV, i, j, k), pp);
+  sum += pfo_phi_from_raw(get(g, PFO_MV, i, j + 1, k), pp);
+  sum += pfo_phi_from_raw(get(g, PFO_MW, i, j, k), pp);
+  sum += pfo_phi_from_raw(get(g, PFO_MW, i, j, k + 1), pp);
+  return sum / 6.0;
+}
+
+/* sparsePhiClamped (:150-156) */
+static double phi_clamped(const pfo_grid* g, const pfo_phase* pp, int i, int j, int k) {
+  return cell_phi(g, pp, clampi(i, 0, g->nx - 1), clampi(j, 0, g->ny - 1), clampi(k, 0, g->nz - 1));
+}
+
+/* sparseGradient (:158-175): central differences of the clamped phi, one-sided
+ * at the walls */
+static void phi_gradient(const pfo_grid* g, const pfo_phase* pp, int i, int j, int k, double out[3]) {
+  const int im = clampi(i - 1, 0, g->nx - 1), ip = clampi(i + 1, 0, g->nx - 1);
+  const int jm = clampi(j - 1, 0, g->ny - 1), jp = clampi(j + 1, 0, g->ny - 1);
+  const int km = clampi(k - 1, 0, g->nz - 1), kp = clampi(k + 1, 0, g->nz - 1);
+  const double dx = g->dx;
+  out[0] = (phi_clamped(g, pp, ip, j, k) - phi_clamped(g, pp, im, j, k)) / ((ip - im > 1 ? ip - im : 1) * dx);
+  out[1] = (phi_clamped(g, pp, i, jp, k) - phi_clamped(g, pp, i, jm, k)) / ((jp - jm > 1 ? jp - jm : 1) * dx);
+  out[2] = (phi_clamped(g, pp, i, j, kp) - phi_clamped(g, pp, i, j, km)) / ((kp - km > 1 ? kp - km : 1) * dx);
+}
+
+static double vlen(const double v[3]) { return sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]); }
+
+/* sparseNormal / normalizeGradient (:177-186): zero below |grad| = 1e-12 */
+static void phi_normal(const pfo_grid* g, const pfo_phase* pp, int i, int j, int k, double out[3]) {
+  double gr[3];
+  phi_gradient(g, pp, i, j, k, gr);
+  const double mag = vlen(gr);
+  if (mag <= 1e-12 || !isfinite(mag)) {
+    out[0] = out[1] = out[2] = 0.0;
+    return;
+  }
+  const double s = 1.0 / mag;
+  out[0] = gr[0] * s;
+  out[1] = gr[1] * s;
+  out[2] = gr[2] * s;
+}
+
+/* sparseCurvature (:188-208): divergence of the normal */
+static double phi_curvature(const pfo_grid* g, const pfo_phase* pp, int i, int j, int k) {
+  const int im = clampi(i - 1, 0, g->nx - 1), ip = clampi(i + 1, 0, g->nx - 1);
+  const int jm = clampi(j - 1, 0, g->ny - 1), jp = clampi(j + 1, 0, g->ny - 1);
+  const int km = clampi(k - 1, 0, g->nz - 1), kp = clampi(k + 1, 0, g->nz - 1);
+  const double dx = g->dx;
+  double nxm[3], nxp[3], nym[3], nyp[3], nzm[3], nzp[3];
+  phi_normal(g, pp, im, j, k, nxm);
+  phi_normal(g, pp, ip, j, k, nxp);
+  phi_normal(g, pp, i, jm, k, nym);
+  phi_normal(g, pp, i, jp, k, nyp);
+  phi_normal(g, pp, i, j, km, nzm);
+  phi_normal(g, pp, i, j, kp, nzp);
+  return (nxp[0] - nxm[0]) / ((ip - im > 1 ? ip - im : 1) * dx) +
+         (nyp[1] - nym[1]) / ((jp - jm > 1 ? jp - jm : 1) * dx) +
+         (nzp[2] - nzm[2]) / ((kp - km > 1 ? kp - km : 1) * dx);
+}
+
+/* diagnoseSparseInterface3D (:363-379) with accumulate / finishStats
+ * (:26-66): over the fluid cells in ascending linear order */
+int pfo_interface_diagnostics(const pfo_grid* g, const pfo_phase* pp, pfo_interface_stats* st) {
+  memset(st, 0, sizeof(*st));
+  st->finite = 1;
+  for (int k = 0; k < g->nz; ++k)
+    for (int j = 0; j < g->ny; ++j)
+      for (int i = 0; i < g->nx; ++i) {
+        if (cell_of(g, i, j, k) != 1) continue;
+        const double phi = cell_phi(g, pp, i, j, k);
+        double gr[3];
+        phi_gradient(g, pp, i, j, k, gr);
+        const double gm = vlen(gr);
+        const double curv = phi_curvature(g, pp, i, j, k);
+        if (!isfinite(phi) || !isfinite(gm) || !isfinite(curv)) {
+          st->finite = 0;
+          continue;
+        }
+        if (st->sample_cells == 0) {
+          st->phi_min = phi;
+          st->phi_max = phi;
+        } else {
+          st->phi_min = phi < st->phi_min ? phi : st->phi_min;
+          st->phi_max = phi > st->phi_max ? phi : st->phi_max;
+        }
+        ++st->sample_cells;
+        st->phi_mean += phi;
+        if (!(phi > 0.05 && phi < 0.95)) continue;
+        ++st->interface_cells;
+        st->grad_mean += gm;
+        st->grad_max = gm > st->grad_max ? gm : st->grad_max;
+        const double ac = fabs(curv);
+        st->curvature_abs_mean += ac;
+        st->curvature_abs_max = ac > st->curvature_abs_max ? ac : st->curvature_abs_max;
+      }
+  if (st->sample_cells > 0) st->phi_mean /= (double)st->sample_cells;
+  if (st->interface_cells > 0) {
+    st->grad_mean /= (double)st->interface_cells;
+    st->curvature_abs_mean /= (double)st->interface_cells;
+  }
+  st->surface_tension_candidate = st->finite && st->interface_cells > 0 && st->grad_max > 1e-5;
   return 0;
 }

@@ -117,6 +117,13 @@ int pfo_refill_liquid(const pfo_grid* g, size_t* n, size_t cap, double* pos, dou
                       double* vol, int target, unsigned seed, int interface_only, int interface_radius, int max_added,
                       pfo_refill_stats* st);
 
+/* ---- interface diagnostics (src/driver/interface_diagnostics3d.cpp:363-379) ---- */
+typedef struct {
+  int sample_cells, interface_cells, finite, surface_tension_candidate;
+  double phi_min, phi_max, phi_mean, grad_mean, grad_max, curvature_abs_mean, curvature_abs_max;
+} pfo_interface_stats;
+int pfo_interface_diagnostics(const pfo_grid* g, const pfo_phase* pp, pfo_interface_stats* st);
+
 #ifdef __cplusplus
 }
 #endif

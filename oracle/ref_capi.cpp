@@ -12,8 +12,10 @@
 //   phiFromRawDensity / betaFromPhi (src/physics/phasefield.h:10-18)
 //   pa3d::applyNarrowBandAir / applyTypedParticleCoarsening /
 //   applyLiquidParticleRefill (src/driver/particle_adaptivity3d.h:111-374)
+//   diagnoseSparseInterface3D (src/driver/interface_diagnostics3d.cpp:363-379)
 // and converts between its SparseMacGrid3D<4> block pool and dense arrays
 // plus one activity byte per 4^3 block.
+#include "driver/interface_diagnostics3d.h"
 #include "driver/particle_adaptivity3d.h"
 #include "driver/sparse_ops3d_tp.h"
 #include "driver/sparse_sim3d_tp.h"
@@ -244,6 +246,19 @@ int pfr_refill_liquid(void* hp, int target, unsigned seed, int interface_only, i
   const int v[7] = {r.added, r.cells, r.interfaceCells, r.underfullCells, r.budgetLimited, r.particlesBefore,
                     r.particlesAfter};
   std::memcpy(out7, v, sizeof(v));
+  return 0;
+}
+
+// ints4: sample_cells, interface_cells, finite, surface_tension_candidate;
+// dbl7: phi_min, phi_max, phi_mean, grad_mean, grad_max, curvature_abs_mean, curvature_abs_max
+int pfr_interface_diagnostics(void* hp, const double* phase, int* ints4, double* dbl7) {
+  Handle* h = static_cast<Handle*>(hp);
+  const InterfaceDiagnostics3D d = diagnoseSparseInterface3D(h->sim.grid, phaseOf(phase));
+  const int iv[4] = {d.sample_cells, d.interface_cells, d.finite, d.surface_tension_candidate};
+  const double dv[7] = {d.phi_min, d.phi_max, d.phi_mean, d.grad_mean, d.grad_max, d.curvature_abs_mean,
+                        d.curvature_abs_max};
+  std::memcpy(ints4, iv, sizeof(iv));
+  std::memcpy(dbl7, dv, sizeof(dv));
   return 0;
 }
 
