@@ -38,7 +38,7 @@ EXPORTS = (
     "pf_learned_train",
     "pf_learned_eval", "pf_learned_adam",
     "pf_narrow_band_air", "pf_coarsen_particles", "pf_refill_liquid", "pf_set_adaptivity", "pf_get_adaptivity_stats",
-    "pf_interface_diagnostics", "pf_get_interface_stats",
+    "pf_interface_diagnostics", "pf_get_interface_stats", "pf_set_step_controls", "pf_get_step_control_stats",
 )
 
 STAGES = ("bin", "sort", "splat", "normalize", "mark", "boundary", "project", "pcg", "g2p", "precond_setup",
@@ -136,6 +136,20 @@ class InterfaceStats(_Stats):
                 ("curvature_abs_mean", C.c_double), ("curvature_abs_max", C.c_double)]
 
 
+class StepControls(C.Structure):
+    """pf_step_controls: SparseSim3DTP's adaptive timestep and volume correction (src/driver/sparse_sim3d_tp.h:13-26)"""
+    _fields_ = [("adaptive_timestep", C.c_int), ("adaptive_cfl", C.c_double), ("adaptive_min_dt", C.c_double),
+                ("c_div_volume_correction", C.c_int), ("c_div_strength", C.c_double),
+                ("liquid_volume_target", C.c_double)]
+
+
+class StepControlStats(_Stats):
+    """pf_step_control_stats: TimestepStats3D (src/driver/timestep3d.h:8-14) and the volume statistics"""
+    _fields_ = [("requested_dt", C.c_double), ("effective_dt", C.c_double), ("max_particle_speed", C.c_double),
+                ("cfl_limit_dt", C.c_double), ("limited", C.c_int), ("liquid_volume_current", C.c_double),
+                ("liquid_volume_error", C.c_double), ("c_div", C.c_double)]
+
+
 class AdaptStats(C.Structure):
     _fields_ = [("band", BandStats), ("gas", CoarsenStats), ("liquid", CoarsenStats), ("refill", RefillStats)]
 
@@ -223,6 +237,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "pf_get_adaptivity_stats": (i, [vp, P(AdaptStats)]),
         "pf_interface_diagnostics": (i, [vp, P(Phase), P(InterfaceStats)]),
         "pf_get_interface_stats": (i, [vp, P(InterfaceStats)]),
+        "pf_set_step_controls": (i, [vp, P(StepControls)]),
+        "pf_get_step_control_stats": (i, [vp, P(StepControlStats)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

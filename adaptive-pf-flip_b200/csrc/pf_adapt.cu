@@ -20,6 +20,7 @@
 //     the per-cell requests: cell c gets clamp(budget - before(c), 0, wanted).
 // FP64 expressions are written with explicit _rn intrinsics so that no FMA
 // contraction changes a rounding against the reference.
+#include <algorithm>
 #include <climits>
 
 #include "pf_ctx.h"
@@ -560,6 +561,50 @@ int refill_liquid(pf_ctx* ctx, int target, unsigned seed, int interface_only, in
   return PF_OK;
 }
 
+// ---- the step's particle reductions: max speed and liquid volume -------------
+
+constexpr int kRedBlocks = 8 * 148;
+
+// per CTA: the largest finite |v| (sqrt(vx^2 + vy^2 + vz^2) in FP64, the
+// reference's order) and the liquid volume sum * Vp; part[2b], part[2b + 1]
+__global__ void __launch_bounds__(kNT) k_particle_reduce(PSet P, int n, double Vp, double* part) {
+  __shared__ double smax[kNT], ssum[kNT];
+  double vmax = 0.0, vol = 0.0;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    const double x = P.vx[p], y = P.vy[p], z = P.vz[p];
+    if (isfinite(x) && isfinite(y) && isfinite(z)) {
+      const double s = sqrt(__dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z)));
+      vmax = fmax(vmax, s);
+    }
+    if (P.type[p] == 0) vol = __dadd_rn(vol, __dmul_rn((double)P.vol[p], Vp));
+  }
+  smax[threadIdx.x] = vmax;
+  ssum[threadIdx.x] = vol;
+  __syncthreads();
+  for (int s = kNT / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      smax[threadIdx.x] = fmax(smax[threadIdx.x], smax[threadIdx.x + s]);
+      ssum[threadIdx.x] = __dadd_rn(ssum[threadIdx.x], ssum[threadIdx.x + s]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = smax[0];
+    part[2 * blockIdx.x + 1] = ssum[0];
+  }
+}
+
+// the partials in a fixed order (one thread: kRedBlocks values)
+__global__ void k_particle_reduce_total(const double* part, int nb, double* out) {
+  double vmax = 0.0, vol = 0.0;
+  for (int b = 0; b < nb; ++b) {
+    vmax = fmax(vmax, part[2 * b]);
+    vol = __dadd_rn(vol, part[2 * b + 1]);
+  }
+  out[0] = vmax;
+  out[1] = vol;
+}
+
 // SparseSim3DTP::applyParticleAdaptivity (src/driver/sparse_sim3d_tp.cpp:843-848)
 int apply_adaptivity(pf_ctx* ctx, const pf_adapt_cfg& a, pf_adapt_stats* st) {
   pf_adapt_stats out{};
@@ -573,6 +618,45 @@ int apply_adaptivity(pf_ctx* ctx, const pf_adapt_cfg& a, pf_adapt_stats* st) {
                        a.refill_interface_radius, a.refill_max_added, &out.refill);
   if (st) *st = out;
   return rc;
+}
+
+// computeAdaptiveParticleTimestep3D (src/driver/timestep3d.h:16-50) and
+// updateVolumeCorrectionStats (src/driver/sparse_sim3d_tp.cpp:368-379): the
+// step's dt and divergence correction from two device reductions.  The max
+// speed is exact; the liquid volume is an FP64 sum in another order than the
+// reference's particle order.
+int step_controls(pf_ctx* ctx, double dt, double Vp, const pf_step_controls& c, pf_step_control_stats* st) {
+  AdaptScratch* s = nullptr;
+  int rc = scratch(ctx, &s);
+  if (rc) return rc;
+  const int n = (int)ctx->np;
+  double* part = reinterpret_cast<double*>(ctx->partials);  // kRedBlocks * 2 doubles fit the PCG partials
+  static_assert(2 * kRedBlocks <= kMaxRedBlocks * kRedSlots, "partials buffer too small");
+  double* out = reinterpret_cast<double*>(s->d_stats + 8);  // two doubles in the 16-int statistics buffer
+  const int nb = kRedBlocks;
+  (++ctx->launches), k_particle_reduce<<<nb, kNT, 0, ctx->stream>>>(particles_of(ctx), n, Vp, part);
+  (++ctx->launches), k_particle_reduce_total<<<1, 1, 0, ctx->stream>>>(part, nb, out);
+  PF_CUDA_TRY(cudaGetLastError());
+  double h[2];
+  PF_CUDA_TRY(cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+  PF_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  pf_step_control_stats o{};
+  o.requested_dt = o.effective_dt = o.cfl_limit_dt = dt;
+  o.max_particle_speed = h[0];
+  if (c.adaptive_timestep && dt > 0.0 && ctx->g.dx > 0.0 && c.adaptive_cfl > 0.0 && h[0] > 0.0) {
+    o.cfl_limit_dt = c.adaptive_cfl * ctx->g.dx / h[0];
+    double lim = std::min(dt, o.cfl_limit_dt);
+    if (c.adaptive_min_dt > 0.0) lim = std::max(c.adaptive_min_dt, lim);
+    o.effective_dt = std::min(dt, lim);
+    o.limited = o.effective_dt < dt ? 1 : 0;
+  }
+  o.liquid_volume_current = h[1];
+  o.liquid_volume_error = c.liquid_volume_target - h[1];
+  o.c_div = 0.0;
+  if (c.c_div_volume_correction && c.c_div_strength > 0.0 && c.liquid_volume_target > 0.0 && o.effective_dt > 0.0)
+    o.c_div = c.c_div_strength * o.liquid_volume_error / (o.effective_dt * c.liquid_volume_target);
+  if (st) *st = o;
+  return PF_OK;
 }
 
 void adapt_free(pf_ctx* ctx) {

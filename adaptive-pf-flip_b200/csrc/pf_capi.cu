@@ -636,6 +636,12 @@ int pf_step(pf_ctx* ctx, const pf_step_cfg* cfg, pf_step_stats* stats) {
     rc = pf::apply_adaptivity(ctx, ctx->adapt_cfg, &ctx->adapt_last);
     if (rc) return rc;
   }
+  // then computeAdaptiveParticleTimestep3D and updateVolumeCorrectionStats
+  rc = pf::step_controls(ctx, cfg->dt, cfg->Vp, ctx->controls, &ctx->controls_last);
+  if (rc) return rc;
+  const double dt = ctx->controls_last.effective_dt;
+  pf_solve_cfg solve = cfg->solve;
+  if (ctx->controls.c_div_volume_correction) solve.c_div = ctx->controls_last.c_div;
   rc = pool_reset(ctx);
   if (rc) return rc;
   rc = pf::mark_cells(ctx);
@@ -646,15 +652,15 @@ int pf_step(pf_ctx* ctx, const pf_step_cfg* cfg, pf_step_stats* stats) {
   if (rc) return rc;
   rc = pf::save_velocity(ctx);
   if (rc) return rc;
-  rc = pf::apply_gravity(ctx, cfg->dt, cfg->gravity);
+  rc = pf::apply_gravity(ctx, dt, cfg->gravity);
   if (rc) return rc;
   rc = pf::apply_walls(ctx);
   if (rc) return rc;
   pf_solve_stats sst{};
-  rc = pf::project(ctx, &cfg->phase, cfg->dt, &cfg->solve, &sst);
+  rc = pf::project(ctx, &cfg->phase, dt, &solve, &sst);
   if (rc) return rc;
   pf_clamp_stats cst{};
-  rc = pf::g2p_advect(ctx, cfg->alpha_l, cfg->alpha_g, cfg->dt, cfg->advect_order, &cst);
+  rc = pf::g2p_advect(ctx, cfg->alpha_l, cfg->alpha_g, dt, cfg->advect_order, &cst);
   if (rc) return rc;
   if (stats) {
     stats->solve = sst;
@@ -706,6 +712,18 @@ int pf_interface_diagnostics(pf_ctx* ctx, const pf_phase* phase, pf_interface_st
 int pf_get_interface_stats(const pf_ctx* ctx, pf_interface_stats* out) {
   if (!ctx || !out) return PF_ERR_INVALID;
   *out = ctx->diag_last;
+  return PF_OK;
+}
+
+int pf_set_step_controls(pf_ctx* ctx, const pf_step_controls* controls) {
+  if (!ctx) return PF_ERR_INVALID;
+  ctx->controls = controls ? *controls : pf_step_controls{0, 0.5, 1e-5, 0, 1.0, 0.0};
+  return PF_OK;
+}
+
+int pf_get_step_control_stats(const pf_ctx* ctx, pf_step_control_stats* out) {
+  if (!ctx || !out) return PF_ERR_INVALID;
+  *out = ctx->controls_last;
   return PF_OK;
 }
 

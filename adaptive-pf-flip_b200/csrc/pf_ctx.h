@@ -94,6 +94,9 @@ struct pf_ctx {
   // interface diagnostics: scratch (its own module) and the last result
   void* idiag = nullptr;
   pf_interface_stats diag_last{};
+  // the step's adaptive timestep and volume correction
+  pf_step_controls controls{0, 0.5, 1e-5, 0, 1.0, 0.0};
+  pf_step_control_stats controls_last{};
 
   // ---- misc ----
   int* d_clamp = nullptr;      // 8 counters
@@ -161,6 +164,7 @@ int coarsen_particles(pf_ctx* ctx, int ptype, int target, unsigned seed, pf_coar
 int refill_liquid(pf_ctx* ctx, int target, unsigned seed, int interface_only, int interface_radius, int max_added,
                   pf_refill_stats* st);
 int apply_adaptivity(pf_ctx* ctx, const pf_adapt_cfg& cfg, pf_adapt_stats* st);
+int step_controls(pf_ctx* ctx, double dt, double Vp, const pf_step_controls& c, pf_step_control_stats* st);
 void adapt_free(pf_ctx* ctx);
 
 // diag.cu

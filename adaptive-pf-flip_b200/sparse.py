@@ -462,6 +462,12 @@ class SparseSim3DTP:
         self.liquid_particle_refill_max_added_per_step = 0
         self.adaptivity_last = L.AdaptStats()
         self.interface_diagnostics_last = L.InterfaceStats()
+        # adaptive timestep and volume correction (src/driver/sparse_sim3d_tp.h:13-26), off by default
+        self.adaptive_timestep, self.adaptive_cfl, self.adaptive_min_dt = False, 0.5, 1e-5
+        self.c_div_volume_correction, self.c_div_strength, self.liquid_volume_target = False, 1.0, 0.0
+        self.effective_dt_last, self.max_particle_speed_last, self.cfl_limit_dt_last = self.dt, 0.0, self.dt
+        self.adaptive_timestep_limited_last = 0
+        self.liquid_volume_current_last = self.liquid_volume_error_last = 0.0
 
     def set_particles(self, pos, vel, type, volume):
         """Upload FP32 (n,3) pos/vel, uint8 type, FP32 volume (host or device pointers via numpy)."""
@@ -543,7 +549,18 @@ class SparseSim3DTP:
             L.check(lib.pf_set_adaptivity(ctx, C.byref(ac)), ctx, "pf_set_adaptivity")
         else:
             L.check(lib.pf_set_adaptivity(ctx, None), ctx, "pf_set_adaptivity")
+        ctl = L.StepControls(int(self.adaptive_timestep), float(self.adaptive_cfl), float(self.adaptive_min_dt),
+                             int(self.c_div_volume_correction), float(self.c_div_strength),
+                             float(self.liquid_volume_target))
+        L.check(lib.pf_set_step_controls(ctx, C.byref(ctl)), ctx, "pf_set_step_controls")
         L.check(lib.pf_step(ctx, C.byref(cfg), C.byref(st)), ctx, "pf_step")
+        cs = L.StepControlStats()
+        L.check(lib.pf_get_step_control_stats(ctx, C.byref(cs)), ctx, "pf_get_step_control_stats")
+        self.effective_dt_last, self.max_particle_speed_last = cs.effective_dt, cs.max_particle_speed
+        self.cfl_limit_dt_last, self.adaptive_timestep_limited_last = cs.cfl_limit_dt, cs.limited
+        self.liquid_volume_current_last, self.liquid_volume_error_last = cs.liquid_volume_current, cs.liquid_volume_error
+        if self.c_div_volume_correction:
+            self.c_div_last = cs.c_div
         if self._adaptivity_on():
             L.check(lib.pf_get_adaptivity_stats(ctx, C.byref(self.adaptivity_last)), ctx, "pf_get_adaptivity_stats")
         L.check(lib.pf_get_interface_stats(ctx, C.byref(self.interface_diagnostics_last)), ctx,

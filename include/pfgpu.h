@@ -132,6 +132,24 @@ typedef struct {
   int active_tiles;      /* pooled 8^3 tiles */
 } pf_step_stats;
 
+/* The step's own controls (src/driver/sparse_sim3d_tp.h:13-26): the adaptive
+ * timestep (computeAdaptiveParticleTimestep3D, src/driver/timestep3d.h:16-50)
+ * and the volume-correcting divergence target (updateVolumeCorrectionStats,
+ * src/driver/sparse_sim3d_tp.cpp:368-379).  The reference's defaults: both
+ * off, cfl 0.5, min_dt 1e-5, strength 1, target 0. */
+typedef struct {
+  int adaptive_timestep;
+  double adaptive_cfl, adaptive_min_dt;
+  int c_div_volume_correction;
+  double c_div_strength, liquid_volume_target;
+} pf_step_controls;
+/* TimestepStats3D (src/driver/timestep3d.h:8-14) and the volume statistics */
+typedef struct {
+  double requested_dt, effective_dt, max_particle_speed, cfl_limit_dt;
+  int limited;
+  double liquid_volume_current, liquid_volume_error, c_div;
+} pf_step_control_stats;
+
 /* InterfaceDiagnostics3D (src/driver/interface_diagnostics3d.h:7-19) */
 typedef struct {
   int sample_cells, interface_cells, finite, surface_tension_candidate;
@@ -245,6 +263,13 @@ PFGPU_API int pf_step(pf_ctx* ctx, const pf_step_cfg* cfg, pf_step_stats* stats)
  * after P2G, as SparseSim3DTP::step() does; pf_get_interface_stats returns
  * the last step's. */
 PFGPU_API int pf_interface_diagnostics(pf_ctx* ctx, const pf_phase* phase, pf_interface_stats* stats);
+/* Controls pf_step applies after the adaptivity (NULL: both off).  Every step
+ * computes the statistics (max particle speed, liquid volume), as the
+ * reference's does; with the adaptive timestep on, the step runs with
+ * effective_dt instead of cfg->dt, and with the volume correction on, the
+ * projection uses c_div instead of cfg->solve.c_div. */
+PFGPU_API int pf_set_step_controls(pf_ctx* ctx, const pf_step_controls* controls);
+PFGPU_API int pf_get_step_control_stats(const pf_ctx* ctx, pf_step_control_stats* out);
 PFGPU_API int pf_get_interface_stats(const pf_ctx* ctx, pf_interface_stats* out);
 
 /* ---- particle adaptivity (src/driver/particle_adaptivity3d.h) ----------
