@@ -31,7 +31,7 @@ from ._lib import (PF_MK, PF_MU, PF_MV, PF_MW, PF_P, PF_PRECOND_EXACT_COARSE, PF
 from .learned import LearnedCoarseSolver
 from .sparse import (ParticleEscapeBuffer3D, ParticleEscapeStats3D, Particles3DTP, PhaseParams, SolverConfig,
                      SparseMacGrid3D, SparseSim3DTP, applyGasParticleCoarsening, applyLiquidParticleRefill,
-                     applyNarrowBandAir, applyTypedParticleCoarsening, betaFromPhi, calibrateRhoTilde0,
+                     applyNarrowBandAir, applySparseSurfaceTension3D, applyTypedParticleCoarsening, betaFromPhi, calibrateRhoTilde0,
                      densityFromPhi, diagnoseSparseInterface3D, etaPhi, phiFromRawDensity, spAdvect3D_tp, spG2P3D_tp, spP2G3D_tp,
                      spProjectStepVC3D)
 from . import scenes
@@ -45,5 +45,5 @@ __all__ = [
     "spP2G3D_tp", "spProjectStepVC3D", "spG2P3D_tp", "spAdvect3D_tp", "calibrateRhoTilde0",
     "etaPhi", "phiFromRawDensity", "densityFromPhi", "betaFromPhi", "scenes",
     "applyNarrowBandAir", "applyTypedParticleCoarsening", "applyGasParticleCoarsening", "applyLiquidParticleRefill",
-    "diagnoseSparseInterface3D",
+    "diagnoseSparseInterface3D", "applySparseSurfaceTension3D",
 ]

@@ -39,6 +39,7 @@ EXPORTS = (
     "pf_learned_eval", "pf_learned_adam",
     "pf_narrow_band_air", "pf_coarsen_particles", "pf_refill_liquid", "pf_set_adaptivity", "pf_get_adaptivity_stats",
     "pf_interface_diagnostics", "pf_get_interface_stats", "pf_set_step_controls", "pf_get_step_control_stats",
+    "pf_surface_tension", "pf_set_surface_tension", "pf_get_surface_stats",
 )
 
 STAGES = ("bin", "sort", "splat", "normalize", "mark", "boundary", "project", "pcg", "g2p", "precond_setup",
@@ -134,6 +135,16 @@ class InterfaceStats(_Stats):
                 ("surface_tension_candidate", C.c_int), ("phi_min", C.c_double), ("phi_max", C.c_double),
                 ("phi_mean", C.c_double), ("grad_mean", C.c_double), ("grad_max", C.c_double),
                 ("curvature_abs_mean", C.c_double), ("curvature_abs_max", C.c_double)]
+
+
+class SurfaceStats(_Stats):
+    """pf_surface_stats: SurfaceTensionStats3D (src/driver/interface_diagnostics3d.h:21-36)"""
+    _fields_ = [("enabled", C.c_int), ("applied_cells", C.c_int), ("finite", C.c_int),
+                ("curvature_smoothing_radius", C.c_int), ("capillary_stable", C.c_int), ("strength", C.c_double),
+                ("max_delta_speed_limit", C.c_double), ("mean_delta_speed", C.c_double),
+                ("max_delta_speed", C.c_double), ("raw_curvature_abs_mean", C.c_double),
+                ("raw_curvature_abs_max", C.c_double), ("smoothed_curvature_abs_mean", C.c_double),
+                ("smoothed_curvature_abs_max", C.c_double), ("capillary_dt_limit", C.c_double)]
 
 
 class StepControls(C.Structure):
@@ -238,6 +249,9 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "pf_interface_diagnostics": (i, [vp, P(Phase), P(InterfaceStats)]),
         "pf_get_interface_stats": (i, [vp, P(InterfaceStats)]),
         "pf_set_step_controls": (i, [vp, P(StepControls)]),
+        "pf_surface_tension": (i, [vp, P(Phase), d, d, d, i, P(SurfaceStats)]),
+        "pf_set_surface_tension": (i, [vp, d, d, i]),
+        "pf_get_surface_stats": (i, [vp, P(SurfaceStats)]),
         "pf_get_step_control_stats": (i, [vp, P(StepControlStats)]),
     }
     for name, (res, args) in sig.items():

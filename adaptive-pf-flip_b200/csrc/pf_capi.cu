@@ -654,6 +654,12 @@ int pf_step(pf_ctx* ctx, const pf_step_cfg* cfg, pf_step_stats* stats) {
   if (rc) return rc;
   rc = pf::apply_gravity(ctx, dt, cfg->gravity);
   if (rc) return rc;
+  if (ctx->st_strength > 0.0) {  // applySparseSurfaceTension3D between gravity and the walls
+    rc = pf::surface_tension(ctx, &cfg->phase, dt, ctx->st_strength, ctx->st_max_dv, ctx->st_radius, nullptr);
+    if (rc) return rc;
+  } else {
+    ctx->surface_last = pf_surface_stats{};
+  }
   rc = pf::apply_walls(ctx);
   if (rc) return rc;
   pf_solve_stats sst{};
@@ -712,6 +718,27 @@ int pf_interface_diagnostics(pf_ctx* ctx, const pf_phase* phase, pf_interface_st
 int pf_get_interface_stats(const pf_ctx* ctx, pf_interface_stats* out) {
   if (!ctx || !out) return PF_ERR_INVALID;
   *out = ctx->diag_last;
+  return PF_OK;
+}
+
+int pf_surface_tension(pf_ctx* ctx, const pf_phase* phase, double dt, double strength, double max_delta_speed,
+                       int smoothing_radius, pf_surface_stats* stats) {
+  if (!ctx || !phase) return PF_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  return pf::surface_tension(ctx, phase, dt, strength, max_delta_speed, smoothing_radius, stats);
+}
+
+int pf_set_surface_tension(pf_ctx* ctx, double strength, double max_delta_speed, int smoothing_radius) {
+  if (!ctx) return PF_ERR_INVALID;
+  ctx->st_strength = strength;
+  ctx->st_max_dv = max_delta_speed;
+  ctx->st_radius = smoothing_radius;
+  return PF_OK;
+}
+
+int pf_get_surface_stats(const pf_ctx* ctx, pf_surface_stats* out) {
+  if (!ctx || !out) return PF_ERR_INVALID;
+  *out = ctx->surface_last;
   return PF_OK;
 }
 

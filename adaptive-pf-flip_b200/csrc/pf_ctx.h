@@ -97,6 +97,10 @@ struct pf_ctx {
   // the step's adaptive timestep and volume correction
   pf_step_controls controls{0, 0.5, 1e-5, 0, 1.0, 0.0};
   pf_step_control_stats controls_last{};
+  // surface tension in the step (strength 0: off) and its last statistics
+  double st_strength = 0.0, st_max_dv = 0.0;
+  int st_radius = 0;
+  pf_surface_stats surface_last{};
 
   // ---- misc ----
   int* d_clamp = nullptr;      // 8 counters
@@ -169,6 +173,8 @@ void adapt_free(pf_ctx* ctx);
 
 // diag.cu
 int interface_diagnostics(pf_ctx* ctx, const pf_phase* ph, pf_interface_stats* st);
+int surface_tension(pf_ctx* ctx, const pf_phase* ph, double dt, double strength, double max_dv, int radius,
+                    pf_surface_stats* st);
 void diag_free(pf_ctx* ctx);
 
 // capi.cu: the second particle set (asynchronous uploads, compaction target)

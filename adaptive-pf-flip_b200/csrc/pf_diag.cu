@@ -13,7 +13,9 @@
 // reference's (FP64, _rn intrinsics, no FMA contraction), so counts, minima
 // and maxima are exact; the three means are sums in a different order than
 // the reference's ascending cell order and agree to rounding.
+#include <algorithm>
 #include <cfloat>
+#include <cmath>
 
 #include "pf_ctx.h"
 
@@ -32,12 +34,22 @@ struct DiagPartial {
   double phi_min, phi_max, phi_sum, grad_sum, grad_max, curv_sum, curv_max;
 };
 
+struct SurfPartial {
+  int applied, finite;
+  double dv_sum, dv_max, raw_sum, raw_max, sm_sum, sm_max;
+};
+
 struct DiagScratch {
   size_t ncell = 0;
   double* phi = nullptr;         // [ncell]
   DiagPartial* part = nullptr;   // [kDiagBlocks]
   DiagPartial* total = nullptr;  // [1]
   DiagPartial* h_total = nullptr;
+  // surface tension (allocated on first use)
+  float* h = nullptr;        // [ncell][3] FP32 half velocity changes
+  uint8_t* ok = nullptr;     // [ncell] cell applies its change
+  SurfPartial* spart = nullptr;  // [kDiagBlocks + 1] partial statistics
+  int* bad = nullptr;        // first cell with a non-finite change
 };
 
 // phiFromRawDensity (src/physics/phasefield.h:11-16)
@@ -187,6 +199,141 @@ __global__ void __launch_bounds__(kDiagNT) k_diag_total(const DiagPartial* part,
   block_combine(acc, total);
 }
 
+// ---- surface tension (interface_diagnostics3d.cpp:405-447) ----------------
+
+__device__ __forceinline__ bool interface_phi(double phi) { return phi > 0.05 && phi < 0.95; }
+
+// sparseSmoothedCurvature (:209-233)
+__device__ double smoothed_curvature(const Lattice& L, int i, int j, int k, double raw, int r) {
+  if (r <= 0 || !isfinite(raw)) return raw;
+  double sum = 0.0;
+  int count = 0;
+  for (int dz = -r; dz <= r; ++dz)
+    for (int dy = -r; dy <= r; ++dy)
+      for (int dx = -r; dx <= r; ++dx) {
+        const int ni = clampi(i + dx, 0, L.nx - 1), nj = clampi(j + dy, 0, L.ny - 1), nk = clampi(k + dz, 0, L.nz - 1);
+        if (!interface_phi(L.at(ni, nj, nk))) continue;
+        const double c = curvature(L, ni, nj, nk);
+        if (!isfinite(c)) continue;
+        sum = __dadd_rn(sum, c);
+        ++count;
+      }
+  return count > 0 ? __ddiv_rn(sum, (double)count) : raw;
+}
+
+
+__device__ void surf_combine(SurfPartial& a, const SurfPartial& b) {
+  a.applied += b.applied;
+  a.finite &= b.finite;
+  a.dv_sum = __dadd_rn(a.dv_sum, b.dv_sum);
+  a.raw_sum = __dadd_rn(a.raw_sum, b.raw_sum);
+  a.sm_sum = __dadd_rn(a.sm_sum, b.sm_sum);
+  a.dv_max = fmax(a.dv_max, b.dv_max);
+  a.raw_max = fmax(a.raw_max, b.raw_max);
+  a.sm_max = fmax(a.sm_max, b.sm_max);
+}
+
+__device__ void surf_block_combine(SurfPartial mine, SurfPartial* out) {
+  __shared__ SurfPartial sp[kDiagNT];
+  sp[threadIdx.x] = mine;
+  __syncthreads();
+  for (int s = kDiagNT / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) surf_combine(sp[threadIdx.x], sp[threadIdx.x + s]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = sp[0];
+}
+
+// Per fluid interface cell with |grad phi| > 1e-5: the limited capillary
+// velocity change (limitedDelta, :68-76), its half as the FP32 face
+// increments h, and the statistics (accumulateSurfaceStats, :107-126).  A
+// cell whose change is not finite lowers `first_bad`: the reference stops
+// updating the grid from the first such cell in ascending order on.
+__global__ void __launch_bounds__(kDiagNT) k_surface_cells(DevGrid G, Lattice L, double strength, double dt,
+                                                         double max_dv, int r, float* h, uint8_t* ok,
+                                                         int* first_bad, SurfPartial* part) {
+  SurfPartial acc{0, 1, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  const size_t nc = (size_t)L.nx * L.ny * L.nz;
+  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += (size_t)gridDim.x * blockDim.x) {
+    ok[c] = 0;
+    const int i = (int)(c % L.nx), j = (int)((c / L.nx) % L.ny), k = (int)(c / ((size_t)L.nx * L.ny));
+    if (cell_marker(G, i, j, k) != 1 || !interface_phi(L.phi[c])) continue;
+    double g[3];
+    gradient(L, i, j, k, g);
+    if (length3(g) <= 1e-5) continue;
+    const double raw = curvature(L, i, j, k);
+    const double sm = smoothed_curvature(L, i, j, k, raw, r);
+    const double s = __dmul_rn(__dmul_rn(-strength, sm), dt);
+    double d[3] = {__dmul_rn(g[0], s), __dmul_rn(g[1], s), __dmul_rn(g[2], s)};
+    const double m0 = length3(d);
+    if (!isfinite(m0)) {
+      d[0] = d[1] = d[2] = 0.0;
+    } else if (max_dv > 0.0 && m0 > max_dv) {
+      const double f = __ddiv_rn(max_dv, m0);
+      d[0] = __dmul_rn(d[0], f);
+      d[1] = __dmul_rn(d[1], f);
+      d[2] = __dmul_rn(d[2], f);
+    }
+    const double mag = length3(d);
+    if (!isfinite(mag) || !isfinite(raw) || !isfinite(sm)) {
+      acc.finite = 0;
+      atomicMin(first_bad, (int)c);
+      continue;
+    }
+    ++acc.applied;
+    acc.dv_sum = __dadd_rn(acc.dv_sum, mag);
+    acc.dv_max = fmax(acc.dv_max, mag);
+    acc.raw_sum = __dadd_rn(acc.raw_sum, fabs(raw));
+    acc.raw_max = fmax(acc.raw_max, fabs(raw));
+    acc.sm_sum = __dadd_rn(acc.sm_sum, fabs(sm));
+    acc.sm_max = fmax(acc.sm_max, fabs(sm));
+    h[3 * c + 0] = (float)__dmul_rn(0.5, d[0]);
+    h[3 * c + 1] = (float)__dmul_rn(0.5, d[1]);
+    h[3 * c + 2] = (float)__dmul_rn(0.5, d[2]);
+    ok[c] = 1;
+  }
+  surf_block_combine(acc, &part[blockIdx.x]);
+}
+
+__global__ void __launch_bounds__(kDiagNT) k_surface_total(const SurfPartial* part, int n, SurfPartial* total) {
+  SurfPartial acc{0, 1, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  for (int b = threadIdx.x; b < n; b += blockDim.x) surf_combine(acc, part[b]);
+  surf_block_combine(acc, total);
+}
+
+// Every face node of u, v, w with mass: the increments of its two cells, the
+// lower cell's first (the reference visits cells in ascending order), from the
+// cells before the first non-finite one.
+__global__ void k_surface_faces(DevGrid G, int nslots, const float* __restrict__ h, const uint8_t* __restrict__ ok,
+                                const int* __restrict__ first_bad) {
+  const int bad = *first_bad;
+  const Geom& g = G.g;
+  for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
+    const int t = G.slot_tile[s];
+    const int tx = t % g.TX, tq = t / g.TX, ty = tq % g.TY, tz = tq / g.TY;
+    const int i = tx * 8 + (threadIdx.x & 7), j = ty * 8 + ((threadIdx.x >> 3) & 7), k = tz * 8 + (threadIdx.x >> 6);
+    const size_t o = (size_t)s * PF_TV + threadIdx.x;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const int f = PF_U + a;
+      if (!in_field(g, f, i, j, k) || !(G.fld[PF_MU + a][o] > 0.0f)) continue;
+      const int p[3] = {i, j, k};
+      float u = G.fld[f][o];
+      bool changed = false;
+      for (int side = 0; side < 2; ++side) {  // the cell below the face, then the cell above
+        int q[3] = {p[0], p[1], p[2]};
+        q[a] -= 1 - side;
+        if (q[0] < 0 || q[1] < 0 || q[2] < 0 || q[0] >= g.nx || q[1] >= g.ny || q[2] >= g.nz) continue;
+        const size_t c = (size_t)q[0] + (size_t)g.nx * ((size_t)q[1] + (size_t)g.ny * (size_t)q[2]);
+        if (!ok[c] || (long long)c >= (long long)bad) continue;
+        u = __fadd_rn(u, h[3 * c + a]);
+        changed = true;
+      }
+      if (changed) G.fld[f][o] = u;
+    }
+  }
+}
+
 int scratch(pf_ctx* ctx, DiagScratch** out) {
   DiagScratch* s = static_cast<DiagScratch*>(ctx->idiag);
   if (!s) {
@@ -241,10 +388,78 @@ int interface_diagnostics(pf_ctx* ctx, const pf_phase* ph, pf_interface_stats* s
   return PF_OK;
 }
 
+// applySparseSurfaceTension3D (src/driver/interface_diagnostics3d.cpp:405-447)
+int surface_tension(pf_ctx* ctx, const pf_phase* ph, double dt, double strength, double max_dv, int radius,
+                    pf_surface_stats* st) {
+  StageScope stage(ctx, PF_STAGE_DIAG);
+  pf_surface_stats out{};
+  out.finite = 1;
+  out.enabled = strength > 0.0 && dt > 0.0;
+  out.strength = strength;
+  out.max_delta_speed_limit = max_dv;
+  out.curvature_smoothing_radius = std::min(3, std::max(0, radius));
+  {  // capillaryDtLimit (:78-83), initSurfaceStats (:85-99)
+    const double rho_min = std::min(ph->rho_l, ph->rho_g);
+    const double kpi = 3.14159265358979323846;
+    out.capillary_dt_limit = (ctx->g.dx <= 0.0 || strength <= 0.0 || rho_min <= 0.0 || !std::isfinite(rho_min))
+                                 ? 0.0
+                                 : std::sqrt((rho_min * ctx->g.dx * ctx->g.dx * ctx->g.dx) / (2.0 * kpi * strength));
+    out.capillary_stable = !out.enabled || out.capillary_dt_limit <= 0.0 || dt <= out.capillary_dt_limit + 1e-12;
+  }
+  if (out.enabled) {
+    DiagScratch* s = nullptr;
+    int rc = scratch(ctx, &s);
+    if (rc) return rc;
+    if (!s->h) {
+      PF_CUDA_TRY(cudaMalloc(&s->h, 3 * s->ncell * sizeof(float)));
+      PF_CUDA_TRY(cudaMalloc(&s->ok, s->ncell));
+      PF_CUDA_TRY(cudaMalloc(&s->spart, (kDiagBlocks + 1) * sizeof(SurfPartial)));
+      PF_CUDA_TRY(cudaMalloc(&s->bad, sizeof(int)));
+    }
+    PhiK P;
+    P.rmin = std::log(ph->rho_l / ph->rho_g) * ph->rho_g * ph->rho_tilde_0;
+    P.den = ph->alpha_phi * ph->rho_tilde_0 * ph->rho_l;
+    const DevGrid G = dev_grid(ctx);
+    const int nb = kDiagBlocks;
+    const int big = 0x7fffffff;
+    PF_CUDA_TRY(cudaMemcpyAsync(s->bad, &big, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    (++ctx->launches), k_cell_phi<<<nb, kDiagNT, 0, ctx->stream>>>(G, P, s->phi);
+    const Lattice L{s->phi, ctx->g.nx, ctx->g.ny, ctx->g.nz, ctx->g.dx};
+    (++ctx->launches), k_surface_cells<<<nb, kDiagNT, 0, ctx->stream>>>(G, L, strength, dt, max_dv,
+                                                                         out.curvature_smoothing_radius, s->h, s->ok,
+                                                                         s->bad, s->spart);
+    (++ctx->launches), k_surface_total<<<1, kDiagNT, 0, ctx->stream>>>(s->spart, nb, s->spart + nb);
+    if (ctx->nslots > 0)
+      (++ctx->launches), k_surface_faces<<<std::min(ctx->nslots, 64 * ctx->num_sms), PF_TV, 0, ctx->stream>>>(
+          G, ctx->nslots, s->h, s->ok, s->bad);
+    PF_CUDA_TRY(cudaGetLastError());
+    SurfPartial t;
+    PF_CUDA_TRY(cudaMemcpyAsync(&t, s->spart + nb, sizeof(t), cudaMemcpyDeviceToHost, ctx->stream));
+    PF_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    out.applied_cells = t.applied;
+    out.finite = t.finite;
+    out.max_delta_speed = t.dv_max;
+    out.raw_curvature_abs_max = t.raw_max;
+    out.smoothed_curvature_abs_max = t.sm_max;
+    if (t.applied > 0) {  // finishSurfaceStats (:128-135)
+      out.mean_delta_speed = t.dv_sum / (double)t.applied;
+      out.raw_curvature_abs_mean = t.raw_sum / (double)t.applied;
+      out.smoothed_curvature_abs_mean = t.sm_sum / (double)t.applied;
+    }
+  }
+  ctx->surface_last = out;
+  if (st) *st = out;
+  return PF_OK;
+}
+
 void diag_free(pf_ctx* ctx) {
   DiagScratch* s = static_cast<DiagScratch*>(ctx->idiag);
   if (!s) return;
   cudaFree(s->phi);
+  cudaFree(s->h);
+  cudaFree(s->ok);
+  cudaFree(s->spart);
+  cudaFree(s->bad);
   cudaFree(s->part);
   cudaFree(s->total);
   cudaFreeHost(s->h_total);

@@ -378,6 +378,15 @@ def diagnoseSparseInterface3D(g: SparseMacGrid3D, pp: PhaseParams) -> L.Interfac
     return st
 
 
+def applySparseSurfaceTension3D(g: SparseMacGrid3D, pp: PhaseParams, dt, strength, maxDeltaSpeed,
+                                curvatureSmoothingRadius) -> L.SurfaceStats:
+    """applySparseSurfaceTension3D (src/driver/interface_diagnostics3d.cpp:405-447) on the device."""
+    st = L.SurfaceStats()
+    L.check(g.lib.pf_surface_tension(g.ctx, C.byref(pp._c()), float(dt), float(strength), float(maxDeltaSpeed),
+                                     int(curvatureSmoothingRadius), C.byref(st)), g.ctx, "pf_surface_tension")
+    return st
+
+
 # ---------------------------------------------------------------------------
 # particle adaptivity (src/driver/particle_adaptivity3d.h), on the device; the
 # grid supplies the cell domain (ParticleCellDomain3D) and holds the particles
@@ -462,6 +471,10 @@ class SparseSim3DTP:
         self.liquid_particle_refill_max_added_per_step = 0
         self.adaptivity_last = L.AdaptStats()
         self.interface_diagnostics_last = L.InterfaceStats()
+        # surface tension (src/driver/sparse_sim3d_tp.h:156-159), off by default
+        self.surface_tension, self.surface_tension_strength = False, 0.02
+        self.surface_tension_max_delta_speed, self.surface_tension_curvature_smoothing_radius = 0.25, 0
+        self.surface_tension_stats_last = L.SurfaceStats()
         # adaptive timestep and volume correction (src/driver/sparse_sim3d_tp.h:13-26), off by default
         self.adaptive_timestep, self.adaptive_cfl, self.adaptive_min_dt = False, 0.5, 1e-5
         self.c_div_volume_correction, self.c_div_strength, self.liquid_volume_target = False, 1.0, 0.0
@@ -553,7 +566,12 @@ class SparseSim3DTP:
                              int(self.c_div_volume_correction), float(self.c_div_strength),
                              float(self.liquid_volume_target))
         L.check(lib.pf_set_step_controls(ctx, C.byref(ctl)), ctx, "pf_set_step_controls")
+        L.check(lib.pf_set_surface_tension(ctx, float(self.surface_tension_strength) if self.surface_tension else 0.0,
+                                           float(self.surface_tension_max_delta_speed),
+                                           int(self.surface_tension_curvature_smoothing_radius)), ctx,
+                "pf_set_surface_tension")
         L.check(lib.pf_step(ctx, C.byref(cfg), C.byref(st)), ctx, "pf_step")
+        L.check(lib.pf_get_surface_stats(ctx, C.byref(self.surface_tension_stats_last)), ctx, "pf_get_surface_stats")
         cs = L.StepControlStats()
         L.check(lib.pf_get_step_control_stats(ctx, C.byref(cs)), ctx, "pf_get_step_control_stats")
         self.effective_dt_last, self.max_particle_speed_last = cs.effective_dt, cs.max_particle_speed

@@ -132,6 +132,13 @@ typedef struct {
   int active_tiles;      /* pooled 8^3 tiles */
 } pf_step_stats;
 
+/* SurfaceTensionStats3D (src/driver/interface_diagnostics3d.h:21-36) */
+typedef struct {
+  int enabled, applied_cells, finite, curvature_smoothing_radius, capillary_stable;
+  double strength, max_delta_speed_limit, mean_delta_speed, max_delta_speed, raw_curvature_abs_mean,
+      raw_curvature_abs_max, smoothed_curvature_abs_mean, smoothed_curvature_abs_max, capillary_dt_limit;
+} pf_surface_stats;
+
 /* The step's own controls (src/driver/sparse_sim3d_tp.h:13-26): the adaptive
  * timestep (computeAdaptiveParticleTimestep3D, src/driver/timestep3d.h:16-50)
  * and the volume-correcting divergence target (updateVolumeCorrectionStats,
@@ -269,6 +276,18 @@ PFGPU_API int pf_interface_diagnostics(pf_ctx* ctx, const pf_phase* phase, pf_in
  * effective_dt instead of cfg->dt, and with the volume correction on, the
  * projection uses c_div instead of cfg->solve.c_div. */
 PFGPU_API int pf_set_step_controls(pf_ctx* ctx, const pf_step_controls* controls);
+/* applySparseSurfaceTension3D (src/driver/interface_diagnostics3d.cpp:405-447)
+ * on the context's grid: every fluid interface cell adds half its capillary
+ * velocity change -strength*curvature*grad(phi)*dt (limited to max_delta_speed
+ * when that is > 0; curvature averaged over a radius of 0..3 cells) to its
+ * six faces that hold mass.  Face velocities equal the reference's exactly;
+ * the statistics' means agree to rounding. */
+PFGPU_API int pf_surface_tension(pf_ctx* ctx, const pf_phase* phase, double dt, double strength,
+                                 double max_delta_speed, int smoothing_radius, pf_surface_stats* stats);
+/* pf_step applies it between gravity and the walls when strength > 0
+ * (the reference's surface_tension switch; 0 = off, the default). */
+PFGPU_API int pf_set_surface_tension(pf_ctx* ctx, double strength, double max_delta_speed, int smoothing_radius);
+PFGPU_API int pf_get_surface_stats(const pf_ctx* ctx, pf_surface_stats* out);
 PFGPU_API int pf_get_step_control_stats(const pf_ctx* ctx, pf_step_control_stats* out);
 PFGPU_API int pf_get_interface_stats(const pf_ctx* ctx, pf_interface_stats* out);
 

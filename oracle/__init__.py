@@ -92,6 +92,19 @@ class InterfaceStats(C.Structure):
         return tuple(getattr(self, n) for n, _ in self._fields_)
 
 
+class SurfaceStats(C.Structure):
+    """SurfaceTensionStats3D (src/driver/interface_diagnostics3d.h:21-36)"""
+    _fields_ = [("enabled", C.c_int), ("applied_cells", C.c_int), ("finite", C.c_int),
+                ("curvature_smoothing_radius", C.c_int), ("capillary_stable", C.c_int), ("strength", C.c_double),
+                ("max_delta_speed_limit", C.c_double), ("mean_delta_speed", C.c_double),
+                ("max_delta_speed", C.c_double), ("raw_curvature_abs_mean", C.c_double),
+                ("raw_curvature_abs_max", C.c_double), ("smoothed_curvature_abs_mean", C.c_double),
+                ("smoothed_curvature_abs_max", C.c_double), ("capillary_dt_limit", C.c_double)]
+
+    def as_tuple(self):
+        return tuple(getattr(self, n) for n, _ in self._fields_)
+
+
 class ClampStats(C.Structure):
     _fields_ = [("clamped_liquid", C.c_int), ("clamped_gas", C.c_int),
                 ("x_lo", C.c_int), ("x_hi", C.c_int), ("y_lo", C.c_int),
@@ -212,6 +225,8 @@ def oracle_lib():
     lib.pfo_refill_liquid.argtypes = [vp, sp, C.c_size_t, _dp, _dp, _up, _dp, C.c_int, C.c_uint, C.c_int, C.c_int,
                                       C.c_int, C.POINTER(RefillStats)]
     lib.pfo_interface_diagnostics.argtypes = [vp, C.POINTER(_Phase), C.POINTER(InterfaceStats)]
+    lib.pfo_surface_tension.argtypes = [vp, C.POINTER(_Phase), C.c_double, C.c_double, C.c_double, C.c_int,
+                                        C.POINTER(SurfaceStats)]
     lib._typed = True
     return lib
 
@@ -247,6 +262,7 @@ def ref_lib():
     lib.pfr_coarsen_particles.argtypes = [vp, C.c_int, C.c_int, C.c_uint, _ip]
     lib.pfr_refill_liquid.argtypes = [vp, C.c_int, C.c_uint, C.c_int, C.c_int, C.c_int, _ip]
     lib.pfr_interface_diagnostics.argtypes = [vp, _dp, _ip, _dp]
+    lib.pfr_surface_tension.argtypes = [vp, _dp, C.c_double, C.c_double, C.c_double, C.c_int, _ip, _dp]
     lib._typed = True
     return lib
 
@@ -480,6 +496,14 @@ class Oracle:
         return st
 
 
+    def surface_tension(self, g, pp: PhaseParams, dt, strength, max_delta_speed, smoothing_radius):
+        """applySparseSurfaceTension3D (src/driver/interface_diagnostics3d.cpp:405-447)"""
+        st = SurfaceStats()
+        self.lib.pfo_surface_tension(g.h, C.byref(pp.as_struct()), float(dt), float(strength),
+                                     float(max_delta_speed), int(smoothing_radius), C.byref(st))
+        return st
+
+
 def _truncate(ps: Particles, n):
     ps.pos, ps.vel = ps.pos[:n].copy(), ps.vel[:n].copy()
     ps.type, ps.volume = ps.type[:n].copy(), ps.volume[:n].copy()
@@ -540,6 +564,12 @@ class Reference:
         iv, dv = np.zeros(4, np.int32), np.zeros(7, np.float64)
         self.lib.pfr_interface_diagnostics(g.h, pp.as_array(), iv, dv)
         return InterfaceStats(*[int(v) for v in iv], *[float(v) for v in dv])
+
+    def surface_tension(self, g: ReferenceGrid, pp: PhaseParams, dt, strength, max_delta_speed, smoothing_radius):
+        iv, dv = np.zeros(5, np.int32), np.zeros(9, np.float64)
+        self.lib.pfr_surface_tension(g.h, pp.as_array(), float(dt), float(strength), float(max_delta_speed),
+                                     int(smoothing_radius), iv, dv)
+        return SurfaceStats(*[int(v) for v in iv], *[float(v) for v in dv])
 
     # ---- particle adaptivity, the reference's own pa3d functions ----
     def narrow_band_air(self, g: ReferenceGrid, ps: Particles, radius=2):

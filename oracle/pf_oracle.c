@@ -1150,3 +1150,104 @@ int pfo_interface_diagnostics(const pfo_grid* g, const pfo_phase* pp, pfo_interf
   st->surface_tension_candidate = st->finite && st->interface_cells > 0 && st->grad_max > 1e-5;
   return 0;
 }
+
+/* ------------------------------------------------------------------ */
+/* Surface tension (src/driver/interface_diagnostics3d.cpp:405-447)    */
+/* ------------------------------------------------------------------ */
+
+static int interface_phi(double phi) { return phi > 0.05 && phi < 0.95; }
+
+/* sparseSmoothedCurvature (:209-233): mean raw curvature of the interface
+ * cells in the (2r+1)^3 clamped neighbourhood */
+static double smoothed_curvature(const pfo_grid* g, const pfo_phase* pp, int i, int j, int k, double raw, int r) {
+  if (r <= 0 || !isfinite(raw)) return raw;
+  double sum = 0.0;
+  int count = 0;
+  for (int dz = -r; dz <= r; ++dz)
+    for (int dy = -r; dy <= r; ++dy)
+      for (int dx = -r; dx <= r; ++dx) {
+        const int ni = clampi(i + dx, 0, g->nx - 1), nj = clampi(j + dy, 0, g->ny - 1),
+                  nk = clampi(k + dz, 0, g->nz - 1);
+        if (!interface_phi(cell_phi(g, pp, ni, nj, nk))) continue;
+        const double c = phi_curvature(g, pp, ni, nj, nk);
+        if (!isfinite(c)) continue;
+        sum += c;
+        ++count;
+      }
+  return count > 0 ? sum / (double)count : raw;
+}
+
+/* applySparseSurfaceTension3D (:405-447) with initSurfaceStats,
+ * limitedDelta, accumulateSurfaceStats, finishSurfaceStats (:68-135): cells
+ * in ascending order, each adding half its capillary velocity change to its
+ * six faces where the face holds mass; the finite flag, once cleared, stops
+ * every later update. */
+int pfo_surface_tension(pfo_grid* g, const pfo_phase* pp, double dt, double strength, double max_delta_speed,
+                        int smoothing_radius, pfo_surface_stats* st) {
+  memset(st, 0, sizeof(*st));
+  st->finite = 1;
+  st->enabled = strength > 0.0 && dt > 0.0;
+  st->strength = strength;
+  st->max_delta_speed_limit = max_delta_speed;
+  st->curvature_smoothing_radius = clampi(smoothing_radius, 0, 3);
+  {
+    const double rho_min = pp->rho_l < pp->rho_g ? pp->rho_l : pp->rho_g;
+    const double kpi = 3.14159265358979323846;
+    st->capillary_dt_limit = (g->dx <= 0.0 || strength <= 0.0 || rho_min <= 0.0 || !isfinite(rho_min))
+                                 ? 0.0
+                                 : sqrt((rho_min * g->dx * g->dx * g->dx) / (2.0 * kpi * strength));
+  }
+  st->capillary_stable = !st->enabled || st->capillary_dt_limit <= 0.0 || dt <= st->capillary_dt_limit + 1e-12;
+  if (!st->enabled) return 0;
+  const int r = st->curvature_smoothing_radius;
+  for (int k = 0; k < g->nz; ++k)
+    for (int j = 0; j < g->ny; ++j)
+      for (int i = 0; i < g->nx; ++i) {
+        if (cell_of(g, i, j, k) != 1) continue;
+        const double phi = cell_phi(g, pp, i, j, k);
+        if (!interface_phi(phi)) continue;
+        double gr[3];
+        phi_gradient(g, pp, i, j, k, gr);
+        if (vlen(gr) <= 1e-5) continue;
+        const double raw = phi_curvature(g, pp, i, j, k);
+        const double sm = smoothed_curvature(g, pp, i, j, k, raw, r);
+        const double s = -strength * sm * dt;
+        double d[3] = {gr[0] * s, gr[1] * s, gr[2] * s};
+        const double mag0 = vlen(d);
+        if (!isfinite(mag0)) {
+          d[0] = d[1] = d[2] = 0.0;
+        } else if (max_delta_speed > 0.0 && mag0 > max_delta_speed) {
+          const double f = max_delta_speed / mag0;
+          d[0] *= f;
+          d[1] *= f;
+          d[2] *= f;
+        }
+        const double mag = vlen(d);
+        if (!isfinite(mag) || !isfinite(raw) || !isfinite(sm)) {
+          st->finite = 0;
+          continue;
+        }
+        ++st->applied_cells;
+        st->mean_delta_speed += mag;
+        st->max_delta_speed = mag > st->max_delta_speed ? mag : st->max_delta_speed;
+        st->raw_curvature_abs_mean += fabs(raw);
+        st->raw_curvature_abs_max = fabs(raw) > st->raw_curvature_abs_max ? fabs(raw) : st->raw_curvature_abs_max;
+        st->smoothed_curvature_abs_mean += fabs(sm);
+        st->smoothed_curvature_abs_max =
+            fabs(sm) > st->smoothed_curvature_abs_max ? fabs(sm) : st->smoothed_curvature_abs_max;
+        if (!st->finite) continue;
+        if (get(g, PFO_MU, i, j, k) > 0.0f) *ref(g, PFO_U, i, j, k) += (float)(0.5 * d[0]);
+        if (get(g, PFO_MU, i + 1, j, k) > 0.0f) *ref(g, PFO_U, i + 1, j, k) += (float)(0.5 * d[0]);
+        if (get(g, PFO_MV, i, j, k) > 0.0f) *ref(g, PFO_V, i, j, k) += (float)(0.5 * d[1]);
+        if (get(g, PFO_MV, i, j + 1, k) > 0.0f) *ref(g, PFO_V, i, j + 1, k) += (float)(0.5 * d[1]);
+        if (get(g, PFO_MW, i, j, k) > 0.0f) *ref(g, PFO_W, i, j, k) += (float)(0.5 * d[2]);
+        if (get(g, PFO_MW, i, j, k + 1) > 0.0f) *ref(g, PFO_W, i, j, k + 1) += (float)(0.5 * d[2]);
+      }
+  if (st->applied_cells > 0) {
+    const double den = (double)st->applied_cells;
+    st->mean_delta_speed /= den;
+    st->raw_curvature_abs_mean /= den;
+    st->smoothed_curvature_abs_mean /= den;
+  }
+  return 0;
+}

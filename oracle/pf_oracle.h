@@ -124,6 +124,15 @@ typedef struct {
 } pfo_interface_stats;
 int pfo_interface_diagnostics(const pfo_grid* g, const pfo_phase* pp, pfo_interface_stats* st);
 
+/* ---- surface tension (src/driver/interface_diagnostics3d.cpp:405-447) ---- */
+typedef struct {
+  int enabled, applied_cells, finite, curvature_smoothing_radius, capillary_stable;
+  double strength, max_delta_speed_limit, mean_delta_speed, max_delta_speed, raw_curvature_abs_mean,
+      raw_curvature_abs_max, smoothed_curvature_abs_mean, smoothed_curvature_abs_max, capillary_dt_limit;
+} pfo_surface_stats;
+int pfo_surface_tension(pfo_grid* g, const pfo_phase* pp, double dt, double strength, double max_delta_speed,
+                        int smoothing_radius, pfo_surface_stats* st);
+
 #ifdef __cplusplus
 }
 #endif

@@ -13,6 +13,7 @@
 //   pa3d::applyNarrowBandAir / applyTypedParticleCoarsening /
 //   applyLiquidParticleRefill (src/driver/particle_adaptivity3d.h:111-374)
 //   diagnoseSparseInterface3D (src/driver/interface_diagnostics3d.cpp:363-379)
+//   applySparseSurfaceTension3D (src/driver/interface_diagnostics3d.cpp:405-447)
 // and converts between its SparseMacGrid3D<4> block pool and dense arrays
 // plus one activity byte per 4^3 block.
 #include "driver/interface_diagnostics3d.h"
@@ -259,6 +260,23 @@ int pfr_interface_diagnostics(void* hp, const double* phase, int* ints4, double*
                         d.curvature_abs_max};
   std::memcpy(ints4, iv, sizeof(iv));
   std::memcpy(dbl7, dv, sizeof(dv));
+  return 0;
+}
+
+// ints5: enabled, applied_cells, finite, curvature_smoothing_radius, capillary_stable;
+// dbl9: strength, max_delta_speed_limit, mean_delta_speed, max_delta_speed, raw_curvature_abs_mean,
+//       raw_curvature_abs_max, smoothed_curvature_abs_mean, smoothed_curvature_abs_max, capillary_dt_limit
+int pfr_surface_tension(void* hp, const double* phase, double dt, double strength, double max_dv, int radius,
+                        int* ints5, double* dbl9) {
+  Handle* h = static_cast<Handle*>(hp);
+  const SurfaceTensionStats3D s =
+      applySparseSurfaceTension3D(h->sim.grid, phaseOf(phase), dt, strength, max_dv, radius);
+  const int iv[5] = {s.enabled, s.applied_cells, s.finite, s.curvature_smoothing_radius, s.capillary_stable};
+  const double dv[9] = {s.strength, s.max_delta_speed_limit, s.mean_delta_speed, s.max_delta_speed,
+                        s.raw_curvature_abs_mean, s.raw_curvature_abs_max, s.smoothed_curvature_abs_mean,
+                        s.smoothed_curvature_abs_max, s.capillary_dt_limit};
+  std::memcpy(ints5, iv, sizeof(iv));
+  std::memcpy(dbl9, dv, sizeof(dv));
   return 0;
 }
 

@@ -39,7 +39,8 @@ def test_struct_layouts_match_c(pf, tmp_path):
                "pf_step_stats": L.StepStats, "pf_timing": L.Timing, "pf_band_stats": L.BandStats,
                "pf_coarsen_stats": L.CoarsenStats, "pf_refill_stats": L.RefillStats, "pf_adapt_cfg": L.AdaptCfg,
                "pf_adapt_stats": L.AdaptStats, "pf_interface_stats": L.InterfaceStats,
-               "pf_step_controls": L.StepControls, "pf_step_control_stats": L.StepControlStats}
+               "pf_step_controls": L.StepControls, "pf_step_control_stats": L.StepControlStats,
+               "pf_surface_stats": L.SurfaceStats}
     src = ['#include <stdio.h>', '#include <stddef.h>', '#include "pfgpu.h"', "int main(void){"]
     for cname, py in structs.items():
         src.append(f'printf("{cname} %zu\\n", sizeof({cname}));')

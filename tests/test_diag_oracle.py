@@ -55,3 +55,23 @@ def test_interface_diagnostics_without_fluid_or_interface():
     go3, gr3, pp3 = stepped_pair(8, 6, rho=(1.0, 1.0))
     so = O.Oracle().interface_diagnostics(go3, pp3)
     assert so.as_tuple() == O.Reference().interface_diagnostics(gr3, pp3).as_tuple()
+
+
+@needs_ref
+@pytest.mark.parametrize("n,seed,air,strength,maxdv,radius", [
+    (12, 2, 0.3, 0.07, 0.0, 0), (12, 3, 0.3, 0.07, 0.0, 1), (16, 4, 0.5, 0.2, 0.05, 2), (10, 5, 0.0, 1.0, 0.0, 3),
+    (10, 6, 0.2, 0.0, 0.0, 1),  # disabled: strength 0
+])
+def test_surface_tension_matches_reference(n, seed, air, strength, maxdv, radius):
+    """applySparseSurfaceTension3D (src/driver/interface_diagnostics3d.cpp:405-447):
+    the oracle's statistics and updated face velocities equal the reference's."""
+    go, gr, pp = stepped_pair(n, seed, air)
+    dt = 1 / 120
+    so = O.Oracle().surface_tension(go, pp, dt, strength, maxdv, radius)
+    sr = O.Reference().surface_tension(gr, pp, dt, strength, maxdv, radius)
+    assert so.as_tuple() == sr.as_tuple()
+    if strength > 0:
+        assert so.applied_cells > 0
+    for f in range(8):
+        a, b = go.get_field(f), gr.get_field(f)
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]), O.FIELD_NAMES[f]

@@ -65,3 +65,34 @@ def test_step_records_diagnostics_after_p2g(pf):
     # P2G's FP32 accumulation order differs from the reference's: phi agrees to rounding
     for f in ("phi_min", "phi_max", "phi_mean", "grad_mean", "grad_max"):
         assert abs(getattr(got, f) - getattr(os_, f)) <= 1e-4 * max(abs(getattr(os_, f)), 1.0), f
+
+
+@pytest.mark.parametrize("n,seed,air,strength,maxdv,radius", [
+    (12, 2, 0.3, 0.07, 0.0, 0), (12, 3, 0.3, 0.07, 0.0, 1), (16, 4, 0.5, 0.2, 0.05, 2), (24, 5, 0.0, 1.0, 0.0, 3),
+    (10, 6, 0.2, 0.0, 0.0, 1),
+])
+def test_surface_tension_matches_oracle(pf, n, seed, air, strength, maxdv, radius):
+    """applySparseSurfaceTension3D: face velocities equal the oracle's bit for
+    bit; counts, flags and maxima exact, means within 1e-12."""
+    go, _, pp = stepped_pair(n, seed, air)
+    g = pf.SparseMacGrid3D(n, n, n, 1.0 / n)
+    for f in range(8):
+        g.set_field(f, *go.get_field(f))
+    dt = 1 / 120
+    gs = pf.applySparseSurfaceTension3D(g, pf.PhaseParams(pp.rho_l, pp.rho_g, pp.alpha_phi, pp.rho_tilde_0), dt,
+                                        strength, maxdv, radius)
+    os_ = O.Oracle().surface_tension(go, pp, dt, strength, maxdv, radius)
+    for f in ("enabled", "applied_cells", "finite", "curvature_smoothing_radius", "capillary_stable", "strength",
+              "max_delta_speed_limit", "max_delta_speed", "raw_curvature_abs_max", "smoothed_curvature_abs_max",
+              "capillary_dt_limit"):
+        assert getattr(gs, f) == getattr(os_, f), f
+    for f in ("mean_delta_speed", "raw_curvature_abs_mean", "smoothed_curvature_abs_mean"):
+        a, b = getattr(gs, f), getattr(os_, f)
+        assert abs(a - b) <= 1e-12 * max(abs(b), 1e-300), f
+    for f in range(8):
+        a, b = g.get_field(f), go.get_field(f)
+        assert np.array_equal(a[1], b[1]), f"field {f}: activity"
+        assert np.array_equal(a[0], b[0]), f"field {f}: values"
+    if strength > 0:
+        assert os_.applied_cells > 0
+    g.close()
