@@ -35,6 +35,11 @@ constexpr int kRow = 2 * kBox;
 constexpr int kFieldBox = kRow * kBox * kBox;  // floats per face field
 __device__ __forceinline__ int box_mom(int X, int Y, int Z) { return X + kRow * (Y + kBox * Z); }
 
+// shared-memory float add whose old value nobody waits for
+__device__ __forceinline__ void red_shared_add(float* p, float v) {
+  asm volatile("red.shared.add.f32 [%0], %1;" ::"r"((unsigned)__cvta_generic_to_shared(p)), "f"(v));
+}
+
 // grid coordinate (pos - o)/dx in the reference's double arithmetic
 __device__ __forceinline__ double grid_coord(float p, double o, double dx) {
   return __ddiv_rn(__dsub_rn((double)p, o), dx);
@@ -523,8 +528,8 @@ __device__ __forceinline__ unsigned long long splat_cell(const DevGrid& G, float
         idx[W::S1] = (q >> 1) % 3;
         idx[W::S2] = (q >> 1) / 3;
         const int si = box_mom(win.b[0] + idx[0], win.b[1] + idx[1], win.b[2] + idx[2]);
-        atomicAdd(&sbox[si], p2[e]);
-        atomicAdd(&sbox[si + kBox], m2[e]);
+        red_shared_add(&sbox[si], p2[e]);
+        red_shared_add(&sbox[si + kBox], m2[e]);
       }
     }
   }
