@@ -5,7 +5,10 @@ tests/test_sparse_vc3d.cpp and tests/test_sparse_sim3d_tp.cpp compiled unmodifie
 with adaptive-pf-flip_b200/shim/sparse_ops3d_tp_gpu.cpp in place of the
 reference's src/driver/sparse_ops3d_tp.cpp, so spP2G3D_tp, spProjectStepVC3D,
 spG2P3D_tp and spAdvect3D_tp (also inside SparseSim3DTP::step()) run on the GPU
-through the C ABI.  The binary is built by `make -C oracle ref_tests` where the
+through the C ABI.  adaptive-pf-flip_b200/shim/driver/particle_adaptivity3d.h
+shadows the reference's header of that name, so the step's particle
+adaptivity (the narrow-band, coarsening and refill cases of
+test_sparse_sim3d_tp.cpp) runs on the GPU too.  The binary is built by `make -C oracle ref_tests` where the
 reference tree exists and travels prebuilt.
 """
 import os
