@@ -839,13 +839,23 @@ __global__ void __launch_bounds__(256) k_g2p_tiles(DevGrid G, const int* __restr
   if (beg >= end) return;
   const int tx = t % G.g.TX, tq = t / G.g.TX, ty = tq % G.g.TY, tz = tq / G.g.TY;
   const int b0 = tx * 8 - 1, b1 = ty * 8 - 1, b2 = tz * 8 - 1;
+  // the pool slots of the 27 tiles around this one: the box's nodes (clamped
+  // to the lattice) lie in them, so each node needs no tile-map load of its own
+  __shared__ int nslot[27];
+  if (threadIdx.x < 27) {
+    const int x = tx + (int)threadIdx.x % 3 - 1, y = ty + ((int)threadIdx.x / 3) % 3 - 1, z = tz + (int)threadIdx.x / 9 - 1;
+    nslot[threadIdx.x] = (x >= 0 && y >= 0 && z >= 0 && x < G.g.TX && y < G.g.TY && z < G.g.TZ)
+                             ? G.tile_slot[tile_id(G.g, x, y, z)]
+                             : -1;
+  }
+  __syncthreads();
   for (int e = threadIdx.x; e < 3 * kG2PBox3; e += blockDim.x) {
     const int a = e / kG2PBox3, s = e - a * kG2PBox3;
     const int fv = PF_U + a;
     const int i = min(max(b0 + s % kG2PBox, 0), G.g.fdim[fv][0] - 1);
     const int j = min(max(b1 + (s / kG2PBox) % kG2PBox, 0), G.g.fdim[fv][1] - 1);
     const int k = min(max(b2 + s / (kG2PBox * kG2PBox), 0), G.g.fdim[fv][2] - 1);
-    const int sl = slot_of(G, i, j, k);
+    const int sl = nslot[((i >> 3) - tx + 1) + 3 * (((j >> 3) - ty + 1) + 3 * ((k >> 3) - tz + 1))];
     float2 v = make_float2(0.0f, 0.0f);
     if (sl >= 0) {
       const size_t o = (size_t)sl * PF_TV + local_id(i, j, k);
