@@ -146,12 +146,19 @@ def dist_setup(n_gpus):
 
 
 def reduce_max(dist, value, local):
+    """The largest of every rank's value (the job's time is its slowest replica's)."""
     if dist is None:
         return value
     import torch
-    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}")
+    device = "cpu" if dist.get_backend() == "gloo" else f"cuda:{local}"
+    t = torch.tensor([value], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def whole_job_rate(units_per_rank, steps, world, ms_max):
+    """Units per second of the whole job: every rank's units over the slowest rank's time."""
+    return units_per_rank * steps * world / (ms_max / 1000.0)
 
 
 def barrier(dist):
@@ -564,8 +571,8 @@ def run_ours(args, rank, world, local, dist):
         ms_e2e, _ = time_steps(ts, args.steps, max(1, args.warmup // 2), dist, local, e2e=True)
     n_faces = ts.active_faces()
 
-    value = n * args.steps * world / (ms / 1000.0)
-    e2e_value = n * args.steps * world / (ms_e2e / 1000.0)
+    value = whole_job_rate(n, args.steps, world, ms)
+    e2e_value = whole_job_rate(n, args.steps, world, ms_e2e)
     peak, peak_kind = measured_hbm()
     # dominant kernel of the step by device time
     splat_ms = stages["splat"][0] / max(stages["splat"][1], 1)
