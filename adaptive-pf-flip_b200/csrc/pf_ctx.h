@@ -76,6 +76,7 @@ struct pf_ctx {
   double *x = nullptr, *r = nullptr, *p = nullptr, *Ap = nullptr;
   double *diag = nullptr, *cx = nullptr, *cy = nullptr, *cz = nullptr;
   double* partials = nullptr;  // [kMaxRedBlocks * 4]
+  int* nbr_plain = nullptr;    // [cells_cap / 512 * 6] neighbour slots of each pooled tile (PLAIN PCG)
   uint8_t* kind = nullptr;     // per cell: 0 not an unknown, 1 fluid, 2 pinned
   pf::SolveCtl* ctl = nullptr;
   pf::SolveCtl* h_ctl = nullptr;  // pinned mirror

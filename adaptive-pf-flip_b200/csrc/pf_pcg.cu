@@ -59,6 +59,58 @@ __global__ void __launch_bounds__(PF_TV) k_spmv_plain(DevGrid G, int nslots, Sol
   block_reduce_2(acc, 0.0, partials, ctl, kStagePAp);
 }
 
+// Every pooled tile's six neighbour slots, nbr[6 s + d] in neighbor_slots'
+// order (+x -x +y -y +z -z; -1 outside the lattice or unpooled).
+__global__ void k_plain_nbr(DevGrid G, int nslots, int* nbr) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= 6 * nslots) return;
+  const int s = q / 6, d = q - 6 * s;
+  const int t = G.slot_tile[s];
+  int tx = t % G.g.TX, r = t / G.g.TX, ty = r % G.g.TY, tz = r / G.g.TY;
+  tx += d == 0 ? 1 : d == 1 ? -1 : 0;
+  ty += d == 2 ? 1 : d == 3 ? -1 : 0;
+  tz += d == 4 ? 1 : d == 5 ? -1 : 0;
+  nbr[q] = (tx >= 0 && ty >= 0 && tz >= 0 && tx < G.g.TX && ty < G.g.TY && tz < G.g.TZ)
+               ? G.tile_slot[tile_id(G.g, tx, ty, tz)]
+               : -1;
+}
+
+// k_spmv_plain with the cross-tile neighbours read from the table: no shared
+// memory or barriers per tile, so a CTA's loads of one tile do not wait on a
+// neighbour-slot round trip.  Same arithmetic and order as k_spmv_plain.
+__global__ void __launch_bounds__(PF_TV) k_spmv_plain_tab(int nslots, SolveCtl* ctl, const uint8_t* kind,
+                                                          const int* __restrict__ nbr, PcgVec<double> v,
+                                                          double scale, double* partials) {
+  if (ctl->done) return;
+  double acc = 0.0;
+  for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
+    const int l = threadIdx.x;
+    const size_t o = (size_t)s * PF_TV + l;
+    const uint8_t kd = kind[o];
+    if (!kd) continue;
+    const double p0 = v.p[o];
+    double ap;
+    if (kd == 2) {
+      ap = p0;
+    } else {
+      long long no[6];
+      neighbor_offsets_tab(nbr, s, l, no);
+      // +x -x +y -y +z -z, the reference's face order
+      const double c[6] = {no[0] >= 0 ? v.cx[no[0]] : 0.0, v.cx[o], no[2] >= 0 ? v.cy[no[2]] : 0.0, v.cy[o],
+                           no[4] >= 0 ? v.cz[no[4]] : 0.0, v.cz[o]};
+      double off = 0.0;
+#pragma unroll
+      for (int d = 0; d < 6; ++d) {
+        if (c[d] != 0.0 && no[d] >= 0) off = __dadd_rn(off, __dmul_rn(c[d], v.p[no[d]]));
+      }
+      ap = __dmul_rn(scale, __dsub_rn(__dmul_rn(v.diag[o], p0), off));
+    }
+    v.Ap[o] = ap;
+    acc = __dadd_rn(acc, __dmul_rn(p0, ap));
+  }
+  block_reduce_2(acc, 0.0, partials, ctl, kStagePAp);
+}
+
 __global__ void __launch_bounds__(PF_TV) k_update_plain(int nslots, SolveCtl* ctl, const uint8_t* kind,
                                                         PcgVec<double> v, double scale, double* partials) {
   if (ctl->done) return;
@@ -327,10 +379,13 @@ int pcg_plain(pf_ctx* ctx, int nslots, int nred, const uint8_t* kind, PcgVec<dou
   res->tol = c.tol;
   int launched = 0;
   int batch = cfg->check_every > 0 ? cfg->check_every : 4;
+  if (nslots > 0)
+    (++ctx->launches), k_plain_nbr<<<nblocks((size_t)6 * nslots, 256), 256, 0, ctx->stream>>>(G, nslots, ctx->nbr_plain);
   while (!c.done && launched < cfg->max_iter) {
     const int nb = std::min(batch, cfg->max_iter - launched);
     for (int q = 0; q < nb; ++q) {
-      (++ctx->launches), k_spmv_plain<<<nred, PF_TV, 0, ctx->stream>>>(G, nslots, ctx->ctl, kind, vec, scale, ctx->partials);
+      (++ctx->launches), k_spmv_plain_tab<<<nred, PF_TV, 0, ctx->stream>>>(nslots, ctx->ctl, kind, ctx->nbr_plain, vec,
+                                                                          scale, ctx->partials);
       (++ctx->launches), k_update_plain<<<nred, PF_TV, 0, ctx->stream>>>(nslots, ctx->ctl, kind, vec, scale, ctx->partials);
       (++ctx->launches), k_direction_plain<<<nred, PF_TV, 0, ctx->stream>>>(nslots, ctx->ctl, kind, vec, scale);
     }
