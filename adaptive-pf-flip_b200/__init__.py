@@ -32,7 +32,7 @@ from .learned import LearnedCoarseSolver
 from .sparse import (ParticleEscapeBuffer3D, ParticleEscapeStats3D, Particles3DTP, PhaseParams, SolverConfig,
                      SparseMacGrid3D, SparseSim3DTP, applyGasParticleCoarsening, applyLiquidParticleRefill,
                      applyNarrowBandAir, applySparseSurfaceTension3D, applyTypedParticleCoarsening, betaFromPhi, calibrateRhoTilde0,
-                     densityFromPhi, diagnoseSparseInterface3D, etaPhi, phiFromRawDensity, spAdvect3D_tp, spG2P3D_tp, spP2G3D_tp,
+                     defaultRenderCacheCamera3D, densityFromPhi, diagnoseSparseInterface3D, etaPhi, phiFromRawDensity, spAdvect3D_tp, spG2P3D_tp, spP2G3D_tp, writeSparseRenderCache3D,
                      spProjectStepVC3D)
 from . import scenes
 
@@ -46,4 +46,5 @@ __all__ = [
     "etaPhi", "phiFromRawDensity", "densityFromPhi", "betaFromPhi", "scenes",
     "applyNarrowBandAir", "applyTypedParticleCoarsening", "applyGasParticleCoarsening", "applyLiquidParticleRefill",
     "diagnoseSparseInterface3D", "applySparseSurfaceTension3D",
+    "writeSparseRenderCache3D", "defaultRenderCacheCamera3D",
 ]

@@ -40,6 +40,7 @@ EXPORTS = (
     "pf_narrow_band_air", "pf_coarsen_particles", "pf_refill_liquid", "pf_set_adaptivity", "pf_get_adaptivity_stats",
     "pf_interface_diagnostics", "pf_get_interface_stats", "pf_set_step_controls", "pf_get_step_control_stats",
     "pf_surface_tension", "pf_set_surface_tension", "pf_get_surface_stats",
+    "pf_default_render_camera", "pf_write_render_cache",
 )
 
 STAGES = ("bin", "sort", "splat", "normalize", "mark", "boundary", "project", "pcg", "g2p", "precond_setup",
@@ -154,6 +155,13 @@ class StepControls(C.Structure):
                 ("liquid_volume_target", C.c_double)]
 
 
+class RenderCamera(C.Structure):
+    """pf_render_camera: RenderCacheCamera3D (src/driver/render_cache3d.h:19-27)."""
+    _fields_ = [("position", C.c_double * 3), ("target", C.c_double * 3), ("up", C.c_double * 3),
+                ("fov_degrees", C.c_double), ("near_clip", C.c_double), ("far_clip", C.c_double),
+                ("focal_length_mm", C.c_double)]
+
+
 class StepControlStats(_Stats):
     """pf_step_control_stats: TimestepStats3D (src/driver/timestep3d.h:8-14) and the volume statistics"""
     _fields_ = [("requested_dt", C.c_double), ("effective_dt", C.c_double), ("max_particle_speed", C.c_double),
@@ -253,6 +261,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "pf_set_surface_tension": (i, [vp, d, d, i]),
         "pf_get_surface_stats": (i, [vp, P(SurfaceStats)]),
         "pf_get_step_control_stats": (i, [vp, P(StepControlStats)]),
+        "pf_default_render_camera": (i, [i, i, i, d, P(RenderCamera)]),
+        "pf_write_render_cache": (i, [vp, C.c_char_p, i, d, d, P(Phase), d, P(RenderCamera), P(C.c_longlong)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -1,0 +1,359 @@
+// Render-cache export: writeSparseRenderCache3D (src/driver/render_cache3d.h:551-600)
+// from the device pool.
+//
+// The phase-field section is the expensive part: every cell of every active
+// 4^3 marker block (or pressure block, when no marker block is active) with
+// marker != 0 or phi > 1e-8, phi being the mean of the cell's six faces'
+// phi(raw mass) (sparseCellPhi, :327-340).  Two kernels over the 4^3 blocks
+// (count, then an order-preserving write after an exclusive scan of the
+// counts) produce the compacted cell records on the device; only the kept
+// cells cross PCIe.  The JSONL text is formatted on the host with the same
+// std::ostream settings (setprecision(17)) as the reference, so every line it
+// writes is byte-identical for the same state.
+//
+// Block order: the reference lists cells block by block in the order its
+// marker blocks were first activated (a history of markCells' wall loops
+// and particle order); the pool keeps no activation history, so blocks are
+// listed in ascending block id, cells within a block in the reference's
+// lz, ly, lx order.  The set of cell lines is identical; the liquid volume
+// sum over them is accumulated in this order.
+#include <cub/device/device_scan.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <fstream>
+#include <iomanip>
+#include <limits>
+#include <string>
+#include <vector>
+
+#include "pf_ctx.h"
+
+namespace pf {
+namespace {
+
+struct RcPhiK {
+  double rmin, den;
+};
+
+struct RcCell {
+  int i, j, k, marker;
+  double phi;
+};
+
+// phiFromRawDensity (src/physics/phasefield.h:11-16)
+__device__ __forceinline__ double rc_phi_of_raw(double raw, const RcPhiK& P) {
+  if (raw < P.rmin) return 0.0;
+  double e = __dsub_rn(raw, P.rmin);
+  if (e < 0.0) e = 0.0;
+  const double v = sqrt(__ddiv_rn(e, P.den));
+  return 1.0 < v ? 1.0 : v;
+}
+
+// Cell t (lx fastest) of 4^3 block b: kept when the block is active in field
+// fsel, the cell is inside the grid and marker != 0 or phi > 1e-8
+// (sparsePhaseCells, render_cache3d.h:497-526).
+__device__ __forceinline__ bool rc_cell(const DevGrid& G, const RcPhiK& P, int fsel, int b, int t, RcCell* c) {
+  const Geom& g = G.g;
+  const int nbx = g.bdim[PF_MK][0], nby = g.bdim[PF_MK][1];
+  if (!G.act4[fsel][b]) return false;
+  const int bx = b % nbx, by = (b / nbx) % nby, bz = b / (nbx * nby);
+  const int i = bx * 4 + (t & 3), j = by * 4 + ((t >> 2) & 3), k = bz * 4 + (t >> 4);
+  if (!in_cells(g, i, j, k)) return false;
+  const int marker = cell_marker(G, i, j, k);
+  double s = 0.0;
+  s = __dadd_rn(s, rc_phi_of_raw((double)fget(G, PF_MU, i, j, k), P));
+  s = __dadd_rn(s, rc_phi_of_raw((double)fget(G, PF_MU, i + 1, j, k), P));
+  s = __dadd_rn(s, rc_phi_of_raw((double)fget(G, PF_MV, i, j, k), P));
+  s = __dadd_rn(s, rc_phi_of_raw((double)fget(G, PF_MV, i, j + 1, k), P));
+  s = __dadd_rn(s, rc_phi_of_raw((double)fget(G, PF_MW, i, j, k), P));
+  s = __dadd_rn(s, rc_phi_of_raw((double)fget(G, PF_MW, i, j, k + 1), P));
+  const double phi = __ddiv_rn(s, 6.0);
+  if (marker == 0 && phi <= 1e-8) return false;
+  *c = RcCell{i, j, k, marker, phi};
+  return true;
+}
+
+// One 64-thread CTA per 4^3 block (grid-stride): kept-cell count per block
+// and the number of active blocks of field fsel.
+__global__ void __launch_bounds__(64) k_rc_count(DevGrid G, RcPhiK P, int fsel, int nb4, int* cnt, int* nactive) {
+  for (int b = blockIdx.x; b < nb4; b += gridDim.x) {
+    RcCell c;
+    const int keep = rc_cell(G, P, fsel, b, threadIdx.x, &c) ? 1 : 0;
+    const int n = __syncthreads_count(keep);
+    if (threadIdx.x == 0) {
+      cnt[b] = n;
+      if (G.act4[fsel][b]) atomicAdd(nactive, 1);
+    }
+  }
+}
+
+// Same walk; each kept cell goes to off[b] + its rank among the block's kept
+// cells in lz, ly, lx order.
+__global__ void __launch_bounds__(64) k_rc_write(DevGrid G, RcPhiK P, int fsel, int nb4, const int* off, RcCell* out) {
+  __shared__ unsigned w0;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int b = blockIdx.x; b < nb4; b += gridDim.x) {
+    RcCell c;
+    const bool keep = rc_cell(G, P, fsel, b, threadIdx.x, &c);
+    const unsigned m = __ballot_sync(0xffffffffu, keep);
+    if (threadIdx.x == 0) w0 = m;
+    __syncthreads();
+    const int base = warp ? __popc(w0) : 0;
+    if (keep) out[off[b] + base + __popc(m & ((1u << lane) - 1u))] = c;
+    __syncthreads();
+  }
+}
+
+struct Bounds {
+  double mn[3], mx[3];
+  bool valid = false;
+};
+
+void include_point(Bounds& b, const double p[3]) {
+  if (!std::isfinite(p[0]) || !std::isfinite(p[1]) || !std::isfinite(p[2])) return;
+  if (!b.valid) {
+    for (int a = 0; a < 3; ++a) b.mn[a] = b.mx[a] = p[a];
+    b.valid = true;
+    return;
+  }
+  for (int a = 0; a < 3; ++a) {
+    b.mn[a] = std::min(b.mn[a], p[a]);
+    b.mx[a] = std::max(b.mx[a], p[a]);
+  }
+}
+
+void write_vec(std::ostream& out, const char* key, const double v[3]) {
+  out << "\"" << key << "\":[" << v[0] << "," << v[1] << "," << v[2] << "]";
+}
+
+void write_bounds(std::ostream& out, const char* kmin, const char* kmax, const Bounds& b, const Bounds& fb) {
+  const Bounds& u = b.valid ? b : fb;
+  write_vec(out, kmin, u.mn);
+  out << ",";
+  write_vec(out, kmax, u.mx);
+}
+
+bool finite3(const double v[3]) { return std::isfinite(v[0]) && std::isfinite(v[1]) && std::isfinite(v[2]); }
+
+}  // namespace
+
+// Kept phase cells of the current grid, compacted on the device.
+int render_cells(pf_ctx* ctx, const pf_phase* ph, std::vector<RcCell>* cells) {
+  const Geom& g = ctx->g;
+  const int nb4 = g.bdim[PF_MK][0] * g.bdim[PF_MK][1] * g.bdim[PF_MK][2];
+  RcPhiK P;
+  P.rmin = std::log(ph->rho_l / ph->rho_g) * ph->rho_g * ph->rho_tilde_0;
+  P.den = ph->alpha_phi * ph->rho_tilde_0 * ph->rho_l;
+  const DevGrid G = dev_grid(ctx);
+  int* d = nullptr;  // [nb4 + 1] counts, [nb4 + 1] offsets, [1] active blocks
+  void* tmp = nullptr;
+  RcCell* dc = nullptr;
+  size_t tmp_bytes = 0;
+  int rc = PF_OK;
+  cudaError_t e = cudaMalloc(&d, (2 * (size_t)(nb4 + 1) + 1) * sizeof(int));
+  if (e != cudaSuccess) return PF_ERR_CUDA;
+  int* cnt = d;
+  int* off = d + nb4 + 1;
+  int* nact = off + nb4 + 1;
+  const int grid = std::max(1, std::min(nb4, 148 * 32));
+  int h_act = 0, total = 0, fsel = PF_MK;
+  for (int pass = 0; pass < 2 && rc == PF_OK; ++pass) {
+    // activeBlockIds of mkf, or of pf when no marker block is active
+    if ((e = cudaMemsetAsync(d, 0, (2 * (size_t)(nb4 + 1) + 1) * sizeof(int), ctx->stream)) != cudaSuccess) break;
+    (++ctx->launches), k_rc_count<<<grid, 64, 0, ctx->stream>>>(G, P, fsel, nb4, cnt, nact);
+    if ((e = cudaMemcpyAsync(&h_act, nact, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream)) != cudaSuccess) break;
+    if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) break;
+    if (h_act > 0 || fsel == PF_P) break;
+    fsel = PF_P;
+  }
+  if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, cnt, off, nb4 + 1, ctx->stream);
+  if (e == cudaSuccess) e = cudaMalloc(&tmp, std::max<size_t>(tmp_bytes, 16));
+  if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, cnt, off, nb4 + 1, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&total, off + nb4, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e == cudaSuccess) {
+    cells->resize((size_t)total);
+    if (total > 0) {
+      e = cudaMalloc(&dc, (size_t)total * sizeof(RcCell));
+      if (e == cudaSuccess) {
+        (++ctx->launches), k_rc_write<<<grid, 64, 0, ctx->stream>>>(G, P, fsel, nb4, off, dc);
+        e = cudaGetLastError();
+      }
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(cells->data(), dc, (size_t)total * sizeof(RcCell), cudaMemcpyDeviceToHost, ctx->stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    }
+  }
+  if (e != cudaSuccess) rc = PF_ERR_CUDA;
+  cudaFree(dc);
+  cudaFree(tmp);
+  cudaFree(d);
+  return rc;
+}
+
+}  // namespace pf
+
+extern "C" {
+
+// writeSparseRenderCache3D (src/driver/render_cache3d.h:551-600) with empty
+// secondary droplet and bubble sets: this framework keeps no secondary
+// particle containers, so their sections carry zero counts, as the reference
+// writes them for a simulation that emitted none.
+int pf_write_render_cache(pf_ctx* ctx, const char* path, int frame, double time, double dt, const pf_phase* ph,
+                          double Vp, const pf_render_camera* cam, long long* bytes_written) {
+  if (!ctx || !path || !path[0] || !ph) return PF_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  const pf::Geom& g = ctx->g;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const double dx = g.dx;
+  pf_render_camera c{};
+  if (cam) {
+    c = *cam;
+  } else {
+    pf_default_render_camera(nx, ny, nz, dx, &c);
+  }
+  // writeHeader's argument check (:386-394)
+  if (nx <= 0 || ny <= 0 || nz <= 0 || dx <= 0.0 || !std::isfinite(dx) || !std::isfinite(dt) ||
+      !std::isfinite(time) || !pf::finite3(c.position) || !pf::finite3(c.target) || !pf::finite3(c.up) ||
+      c.fov_degrees <= 0.0 || !std::isfinite(c.fov_degrees) || c.near_clip <= 0.0 || c.far_clip <= c.near_clip ||
+      !std::isfinite(c.near_clip) || !std::isfinite(c.far_clip) || c.focal_length_mm <= 0.0 ||
+      !std::isfinite(c.focal_length_mm))
+    return PF_ERR_INVALID;
+
+  std::vector<pf::RcCell> cells;
+  int rc = pf::render_cells(ctx, ph, &cells);
+  if (rc) return rc;
+  const size_t n = ctx->np;
+  std::vector<float> pos(3 * n), vel(3 * n), vol(n);
+  std::vector<uint8_t> typ(n);
+  if (n) {
+    rc = pf_download_particles(ctx, pos.data(), vel.data(), typ.data(), vol.data());
+    if (rc) return rc;
+  }
+
+  double liquid = 0.0;
+  const double cell_volume = dx * dx * dx;
+  for (const pf::RcCell& x : cells) liquid += x.phi * cell_volume;
+  size_t n_liq = 0, n_gas = 0;
+  double v_liq = 0.0, v_gas = 0.0;
+  pf::Bounds water;
+  for (size_t p = 0; p < n; ++p) {
+    const double v = (double)vol[p] * Vp;
+    if (typ[p] == 0) {
+      ++n_liq;
+      v_liq += v;
+      const double q[3] = {pos[3 * p], pos[3 * p + 1], pos[3 * p + 2]};
+      pf::include_point(water, q);
+    } else if (typ[p] == 1) {
+      ++n_gas;
+      v_gas += v;
+    }
+  }
+  for (const pf::RcCell& x : cells) {  // waterBounds (:302-314), level 0
+    if (x.phi <= 0.0 && x.phi * cell_volume <= 0.0) continue;
+    const double lo[3] = {x.i * dx, x.j * dx, x.k * dx};
+    const double hi[3] = {(x.i + 1) * dx, (x.j + 1) * dx, (x.k + 1) * dx};
+    pf::include_point(water, lo);
+    pf::include_point(water, hi);
+  }
+  pf::Bounds domain;
+  domain.valid = true;
+  domain.mn[0] = domain.mn[1] = domain.mn[2] = 0.0;
+  domain.mx[0] = nx * dx;
+  domain.mx[1] = ny * dx;
+  domain.mx[2] = nz * dx;
+  pf::Bounds secondary{};  // no secondary particles
+  const double shutter_close = time + std::max(0.0, dt);
+
+  std::ofstream out(path);
+  if (!out) return PF_ERR_INVALID;
+  out << std::setprecision(17);
+  // writeHeader (:375-427)
+  out << "{\"section\":\"header\",\"lsfs_cache3d_version\":1"
+      << ",\"cache_schema_version\":2"
+      << ",\"sim_kind\":\"sparse3d_tp\""
+      << ",\"frame\":" << frame << ",\"time\":" << time << ",\"dt\":" << dt << ",\"dims\":[" << nx << "," << ny
+      << "," << nz << "]"
+      << ",\"dx\":" << dx << ",\"world_units\":\"cell\""
+      << ",\"shutter_open\":" << time << ",\"shutter_close\":" << shutter_close << ",\"frame_bounds_min\":["
+      << domain.mn[0] << "," << domain.mn[1] << "," << domain.mn[2] << "]"
+      << ",\"frame_bounds_max\":[" << domain.mx[0] << "," << domain.mx[1] << "," << domain.mx[2] << "]"
+      << ",\"phase\":{\"rho_l\":" << ph->rho_l << ",\"rho_g\":" << ph->rho_g << ",\"alpha_phi\":" << ph->alpha_phi
+      << ",\"rho_tilde_0\":" << ph->rho_tilde_0 << "}}\n";
+  out << "{\"section\":\"camera\",";
+  pf::write_vec(out, "position", c.position);
+  out << ",";
+  pf::write_vec(out, "target", c.target);
+  out << ",";
+  pf::write_vec(out, "up", c.up);
+  out << ",\"fov_degrees\":" << c.fov_degrees << ",\"vertical_fov_degrees\":" << c.fov_degrees
+      << ",\"near_clip\":" << c.near_clip << ",\"far_clip\":" << c.far_clip
+      << ",\"focal_length_mm\":" << c.focal_length_mm << "}\n";
+  // writeWaterSummary (:429-458)
+  out << "{\"section\":\"water_volume\""
+      << ",\"primary_liquid_volume\":" << v_liq << ",\"primary_gas_volume\":" << v_gas
+      << ",\"secondary_droplet_volume\":" << 0.0 << ",\"secondary_bubble_volume\":" << 0.0
+      << ",\"phase_field_liquid_volume\":" << liquid << ",\"phase_field_cells\":" << cells.size()
+      << ",\"primary_liquid_count\":" << n_liq << ",\"primary_gas_count\":" << n_gas
+      << ",\"secondary_droplet_count\":0,\"secondary_bubble_count\":0,\"secondary_particle_count\":0"
+      << ",\"secondary_droplet_age_min\":0,\"secondary_droplet_age_max\":0"
+      << ",\"secondary_bubble_age_min\":0,\"secondary_bubble_age_max\":0}\n";
+  // writeSecondaryChannels (:460-476)
+  out << "{\"section\":\"secondary_channels\",\"encoding\":\"render_channel_counts\""
+      << ",\"channel_names\":[\"droplet\",\"spray\",\"foam\",\"bubble\"]"
+      << ",\"droplet_count\":0,\"spray_count\":0,\"foam_count\":0,\"bubble_count\":0,\"total_count\":0}\n";
+  // writeCinematicMetadata (:478-523)
+  out << "{\"section\":\"cinematic_metadata\",\"cache_schema_version\":2,\"world_units\":\"cell\""
+      << ",\"shutter_open\":" << time << ",\"shutter_close\":" << shutter_close << ",\"frame_time\":" << time
+      << ",\"phase_field_sampling_stride\":1"
+      << ",\"water_bounds_valid\":" << (water.valid ? "true" : "false")
+      << ",\"secondary_bounds_valid\":" << (secondary.valid ? "true" : "false")
+      << ",\"primary_particle_count\":" << n << ",\"primary_liquid_count\":" << n_liq
+      << ",\"primary_gas_count\":" << n_gas
+      << ",\"secondary_droplet_count\":0,\"secondary_bubble_count\":0"
+      << ",\"secondary_spray_count\":0,\"secondary_foam_count\":0";
+  out << ",";
+  pf::write_bounds(out, "frame_bounds_min", "frame_bounds_max", domain, domain);
+  out << ",";
+  pf::write_bounds(out, "water_bounds_min", "water_bounds_max", water, domain);
+  out << ",";
+  pf::write_bounds(out, "secondary_bounds_min", "secondary_bounds_max", secondary, domain);
+  out << "}\n";
+  // writePhaseField (:525-539)
+  out << "{\"section\":\"phase_field\",\"encoding\":\"jsonl_cells\",\"count\":" << cells.size() << "}\n";
+  for (const pf::RcCell& x : cells)
+    out << "{\"section\":\"phase_cell\",\"i\":" << x.i << ",\"j\":" << x.j << ",\"k\":" << x.k
+        << ",\"level\":0,\"marker\":" << x.marker << ",\"phi\":" << x.phi
+        << ",\"liquid_volume\":" << x.phi * cell_volume << "}\n";
+  // writeParticleSection (:541-560), primary then the two empty secondary sets
+  out << "{\"section\":\"particles\",\"kind\":\"primary\",\"count\":" << n << "}\n";
+  for (size_t p = 0; p < n; ++p) {
+    const bool liq = typ[p] == 0;
+    out << "{\"section\":\"particle\",\"kind\":\"primary\",\"render_channel\":\"" << (liq ? "water" : "air")
+        << "\",\"index\":" << p << ",\"phase\":\"" << (liq ? "liquid" : "gas") << "\""
+        << ",\"position\":[" << (double)pos[3 * p] << "," << (double)pos[3 * p + 1] << "," << (double)pos[3 * p + 2]
+        << "]"
+        << ",\"velocity\":[" << (double)vel[3 * p] << "," << (double)vel[3 * p + 1] << "," << (double)vel[3 * p + 2]
+        << "]"
+        << ",\"volume\":" << (double)vol[p] * Vp << "}\n";
+  }
+  out << "{\"section\":\"particles\",\"kind\":\"secondary_droplet\",\"count\":0}\n";
+  out << "{\"section\":\"particles\",\"kind\":\"secondary_bubble\",\"count\":0}\n";
+  out.flush();
+  if (!out) return PF_ERR_INVALID;
+  if (bytes_written) *bytes_written = (long long)out.tellp();
+  return PF_OK;
+}
+
+// defaultRenderCacheCamera3D (src/driver/render_cache3d.h:47-61)
+int pf_default_render_camera(int nx, int ny, int nz, double dx, pf_render_camera* cam) {
+  if (!cam) return PF_ERR_INVALID;
+  const double cx = 0.5 * nx * dx, cy = 0.5 * ny * dx, cz = 0.5 * nz * dx;
+  const double span = std::max({nx * dx, ny * dx, nz * dx, dx});
+  *cam = pf_render_camera{{cx, cy + 0.2 * span, cz + 2.0 * span}, {cx, cy, cz}, {0.0, 1.0, 0.0}, 45.0,
+                          0.05 * dx, 5.0 * span, 50.0};
+  return PF_OK;
+}
+
+}  // extern "C"

@@ -378,6 +378,30 @@ def diagnoseSparseInterface3D(g: SparseMacGrid3D, pp: PhaseParams) -> L.Interfac
     return st
 
 
+def defaultRenderCacheCamera3D(nx, ny, nz, dx) -> L.RenderCamera:
+    """defaultRenderCacheCamera3D (src/driver/render_cache3d.h:47-61)."""
+    cam = L.RenderCamera()
+    L.check(L.load().pf_default_render_camera(int(nx), int(ny), int(nz), float(dx), C.byref(cam)), None,
+            "pf_default_render_camera")
+    return cam
+
+
+def writeSparseRenderCache3D(sim, path, frame, time, camera=None) -> int:
+    """writeSparseRenderCache3D (src/driver/render_cache3d.h:551-600): one JSONL
+    frame of the simulation's grid and particles, phase cells compacted on the
+    device.  Returns the bytes written; raises on an empty path or invalid
+    metadata, as the reference does."""
+    if not str(path):
+        raise RuntimeError("render cache path is empty")
+    g = sim.grid
+    nbytes = C.c_longlong(0)
+    cam = C.byref(camera) if camera is not None else None
+    L.check(g.lib.pf_write_render_cache(g.ctx, str(path).encode(), int(frame), float(time),
+                                        float(sim.effective_dt_last), C.byref(sim.phase._c()), float(sim.Vp), cam,
+                                        C.byref(nbytes)), g.ctx, "pf_write_render_cache")
+    return int(nbytes.value)
+
+
 def applySparseSurfaceTension3D(g: SparseMacGrid3D, pp: PhaseParams, dt, strength, maxDeltaSpeed,
                                 curvatureSmoothingRadius) -> L.SurfaceStats:
     """applySparseSurfaceTension3D (src/driver/interface_diagnostics3d.cpp:405-447) on the device."""

@@ -411,6 +411,30 @@ PFGPU_API int pf_learned_eval(pf_ctx* ctx, int X, int Y, int Z, const float* cop
 /* One Adam step (beta 0.9 / 0.999, eps 1e-8) with a caller-given gradient. */
 PFGPU_API int pf_learned_adam(pf_ctx* ctx, const float* grad, size_t n, double lr);
 
+/* ---- render-cache export (src/driver/render_cache3d.h) ---- */
+
+/* RenderCacheCamera3D (src/driver/render_cache3d.h:19-27) */
+typedef struct pf_render_camera {
+  double position[3], target[3], up[3];
+  double fov_degrees, near_clip, far_clip, focal_length_mm;
+} pf_render_camera;
+
+/* defaultRenderCacheCamera3D (src/driver/render_cache3d.h:47-61). */
+PFGPU_API int pf_default_render_camera(int nx, int ny, int nz, double dx, pf_render_camera* cam);
+
+/* writeSparseRenderCache3D (src/driver/render_cache3d.h:551-600): the JSONL
+ * frame (header, camera, water_volume, secondary_channels,
+ * cinematic_metadata, phase_field cells, particles) of the context's current
+ * grid and particles.  The phase cells are selected and compacted on the
+ * device; the text uses the reference's number format (17 significant
+ * digits).  dt is the step's effective dt, Vp the particle volume scale, cam
+ * NULL for the default camera.  Cells are listed by ascending 4^3 block id
+ * (the reference: marker-block activation order).  No secondary particles
+ * exist here, so their sections are empty.  PF_ERR_INVALID for an empty path,
+ * a file that cannot be written or the reference's invalid metadata. */
+PFGPU_API int pf_write_render_cache(pf_ctx* ctx, const char* path, int frame, double time, double dt, const pf_phase* ph,
+                          double Vp, const pf_render_camera* cam, long long* bytes_written);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,136 @@
+"""Render-cache export (src/driver/render_cache3d.h:551-600) on the GPU
+against a restatement of the reference writer's selection and number format.
+
+The drop-in compacts the phase cells on the device and formats the JSONL on
+the host with std::ostream at 17 significant digits, which prints a double as
+printf's %.17g does.  The expected lines are built here from the oracle grid
+the GPU grid was loaded from: sparsePhaseCells (:497-526; cells of active
+4^3 marker blocks with marker != 0 or phi > 1e-8, phi the sequential mean of
+the six faces' phiFromRawDensity) and writeParticleSection (:541-560).  The
+reference lists marker blocks in activation order and the drop-in in
+ascending block id, so the cell lines are compared as sorted lists.
+"""
+import json
+
+import numpy as np
+import pytest
+
+import oracle as O
+from gpu_helpers import phase_for, scene_particles, to_oracle_phase
+
+pytestmark = pytest.mark.gpu
+
+
+def _state(pf, n, seed):
+    sc = pf.scenes.rayleigh_taylor(n, seed=seed)
+    pp = phase_for(sc, pf)
+    ps = scene_particles(sc)
+    go = O.OracleGrid(n, n, n, 1.0 / n)
+    o = O.Oracle()
+    o.mark_cells(go, ps)
+    o.p2g(go, ps, to_oracle_phase(pp), 1.0)
+    sim = pf.SparseSim3DTP(n, n, n, 1.0 / n, max_particles=len(ps))
+    sim.phase, sim.Vp, sim.effective_dt_last = pp, 1.0, 1 / 240
+    sim.set_particles(sc["pos"], sc["vel"], sc["type"], sc["volume"])
+    for f in range(8):
+        sim.grid.set_field(f, *go.get_field(f))
+    return sim, go, ps, pp
+
+
+def _split(path):
+    lines = open(path).read().splitlines()
+    cells = [ln for ln in lines if ln.startswith('{"section":"phase_cell"')]
+    rest = [ln for ln in lines if not ln.startswith('{"section":"phase_cell"')]
+    return rest, cells
+
+
+def _g(x):
+    return "%.17g" % x
+
+
+def _expected_cells(go, pp):
+    o = O.Oracle()
+    opp = to_oracle_phase(pp)
+    nx, ny, nz = go.nx, go.ny, go.nz
+    mk, act = go.get_field(O.FIELD_NAMES.index("mk"))
+    mu, mv, mw = (go.get_field(O.FIELD_NAMES.index(f))[0] for f in ("mu", "mv", "mw"))
+    phi = lambda raw: o.phi_from_raw(float(raw), opp)
+    dv = go.dx * go.dx * go.dx  # cellVolume (render_cache3d.h:520)
+    out = []
+    for k in range(nz):
+        for j in range(ny):
+            for i in range(nx):
+                if not act[k // 4, j // 4, i // 4]:
+                    continue
+                m = int(mk[k, j, i] + np.float32(0.5))
+                s = 0.0
+                for raw in (mu[k, j, i], mu[k, j, i + 1], mv[k, j, i], mv[k, j + 1, i], mw[k, j, i], mw[k + 1, j, i]):
+                    s += phi(raw)
+                p = s / 6.0
+                if m == 0 and p <= 1e-8:
+                    continue
+                out.append('{"section":"phase_cell","i":%d,"j":%d,"k":%d,"level":0,"marker":%d,"phi":%s,'
+                           '"liquid_volume":%s}' % (i, j, k, m, _g(p), _g(p * dv)))
+    return out
+
+
+def _expected_particles(ps, Vp):
+    out = []
+    for p in range(len(ps)):
+        liq = ps.type[p] == 0
+        x, v = ps.pos[p], ps.vel[p]
+        out.append('{"section":"particle","kind":"primary","render_channel":"%s","index":%d,"phase":"%s",'
+                   '"position":[%s,%s,%s],"velocity":[%s,%s,%s],"volume":%s}'
+                   % ("water" if liq else "air", p, "liquid" if liq else "gas", _g(x[0]), _g(x[1]), _g(x[2]),
+                      _g(v[0]), _g(v[1]), _g(v[2]), _g(ps.volume[p] * Vp)))
+    return out
+
+
+@pytest.mark.parametrize("n,seed", [(16, 3), (12, 5)])
+def test_render_cache_matches_restated_writer(pf, tmp_path, n, seed):
+    sim, go, ps, pp = _state(pf, n, seed)
+    a = tmp_path / "gpu.jsonl"
+    nbytes = pf.writeSparseRenderCache3D(sim, a, 7, 0.125)
+    assert nbytes == a.stat().st_size
+    rest, cells = _split(a)
+    exp = _expected_cells(go, pp)
+    assert len(cells) == len(exp) > 0
+    assert sorted(cells) == sorted(exp)
+    parts = [ln for ln in rest if ln.startswith('{"section":"particle",')]
+    assert parts == _expected_particles(ps, 1.0)
+    sec = {json.loads(ln)["section"]: json.loads(ln) for ln in rest if not ln.startswith('{"section":"particle"')}
+    head = sec["header"]
+    assert head["sim_kind"] == "sparse3d_tp" and head["dims"] == [n, n, n] and head["frame"] == 7
+    assert head["dt"] == 1 / 240 and head["shutter_close"] == 0.125 + 1 / 240
+    wv = sec["water_volume"]
+    assert wv["phase_field_cells"] == len(exp)
+    assert wv["primary_liquid_count"] == int(np.sum(ps.type == 0))
+    assert wv["primary_gas_count"] == int(np.sum(ps.type == 1))
+    vol = sum(json.loads(c)["liquid_volume"] for c in exp)
+    assert wv["phase_field_liquid_volume"] == pytest.approx(vol, rel=1e-12)
+    cm = sec["cinematic_metadata"]
+    assert cm["water_bounds_valid"] is True and cm["secondary_bounds_valid"] is False
+    assert cm["secondary_bounds_min"] == [0.0, 0.0, 0.0]
+    assert sec["phase_field"]["count"] == len(exp)
+    cam = sec["camera"]
+    assert cam["target"] == [0.5, 0.5, 0.5] and cam["up"] == [0.0, 1.0, 0.0]
+
+
+def test_render_cache_rejects_bad_metadata(pf, tmp_path):
+    sim = pf.SparseSim3DTP(8, 8, 8, 0.125, max_particles=16)
+    with pytest.raises(Exception):
+        pf.writeSparseRenderCache3D(sim, "", 0, 0.0)
+    cam = pf.defaultRenderCacheCamera3D(8, 8, 8, 0.125)
+    assert list(cam.target) == [0.5, 0.5, 0.5] and cam.near_clip == 0.05 * 0.125
+    cam.far_clip = cam.near_clip / 2
+    with pytest.raises(Exception):
+        pf.writeSparseRenderCache3D(sim, tmp_path / "x.jsonl", 0, 0.0, cam)
+    sim.effective_dt_last = float("nan")
+    with pytest.raises(Exception):
+        pf.writeSparseRenderCache3D(sim, tmp_path / "y.jsonl", 0, 0.0)
+    # an empty grid writes the header sections and empty particle sets
+    sim.effective_dt_last = 0.01
+    pf.writeSparseRenderCache3D(sim, tmp_path / "z.jsonl", 1, 0.0)
+    sections = [json.loads(ln)["section"] for ln in open(tmp_path / "z.jsonl")]
+    assert sections[:6] == ["header", "camera", "water_volume", "secondary_channels", "cinematic_metadata",
+                            "phase_field"]
