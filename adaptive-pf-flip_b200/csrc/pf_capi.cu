@@ -54,7 +54,7 @@ void free_all(pf_ctx* c) {
   for (int a = 0; a < PF_NSAVED; ++a) F(c->saved[a]);
   F(c->d_wall_tiles);
   F(c->px); F(c->py); F(c->pz); F(c->vx); F(c->vy); F(c->vz); F(c->vol); F(c->type); F(c->staging);
-  F(c->tile_count); F(c->tile_start); F(c->pkey); F(c->prank); F(c->perm);
+  F(c->tile_count); F(c->tile_start); F(c->pkey); F(c->prank); F(c->perm); F(c->splat_stage);
   for (int* p : c->scan_levels) F(p);
   F(c->d_scalar);
   F(c->x); F(c->r); F(c->p); F(c->Ap); F(c->diag); F(c->cx); F(c->cy); F(c->cz); F(c->kind);
@@ -181,6 +181,7 @@ int create_impl(pf_ctx* ctx, const pf_grid_desc* d) {
   PF_CUDA_TRY(cudaMalloc(&ctx->pkey, cap * sizeof(int)));
   PF_CUDA_TRY(cudaMalloc(&ctx->prank, cap * sizeof(int)));
   PF_CUDA_TRY(cudaMalloc(&ctx->perm, cap * sizeof(int)));
+  PF_CUDA_TRY(cudaMalloc(&ctx->splat_stage, nt * (size_t)pf::kSplatStageTile * sizeof(float2)));
   size_t scan_max = cells + 1;
   if ((size_t)ncell > scan_max) scan_max = (size_t)ncell;
   if (cap > scan_max) scan_max = cap;

@@ -66,6 +66,8 @@ struct pf_ctx {
   int* pkey = nullptr;        // [cap]
   int* prank = nullptr;       // [cap]
   int* perm = nullptr;        // [cap]
+  float2* splat_stage = nullptr;  // [ntiles * kSplatStageTile] per-tile P2G staging boxes (momentum, raw mass)
+  bool splat_fresh = false;       // splat_stage holds the last P2G's boxes, not yet normalised
 
   // ---- scan scratch ----
   std::vector<int*> scan_levels;
@@ -180,6 +182,10 @@ void diag_free(pf_ctx* ctx);
 
 // capi.cu: the second particle set (asynchronous uploads, compaction target)
 int ensure_back_set(pf_ctx* ctx);
+
+// P2G staging box of one tile: per face field the nodes its cells reach,
+// 11 along the normal axis and 10 along each transverse axis (float2 each).
+constexpr int kSplatStageTile = 3 * 11 * 10 * 10;
 
 constexpr int kMaxRedBlocks = 1184;  // 8 CTAs per SM on 148 SMs
 constexpr int kRedSlots = 4;         // partial values one reduction CTA may write

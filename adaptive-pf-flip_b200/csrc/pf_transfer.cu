@@ -10,12 +10,14 @@
 //   calibrateRhoTilde0 src/transfer/transfer3d_tp.cpp:29-36
 //
 // P2G design (replaces the reference's 8 colour threads that each rescan every
-// particle): particles are binned by the 8^3 tile of their cell with
-// warp-aggregated atomics; one CTA per tile splats its particles into a
-// shared-memory box of 12^3 nodes per face field (the tile plus the kernel's
-// -2..+3 halo), then adds the box into the pooled field once.  Block
-// activation is decided in FP64 with the reference's exact operation order,
-// so the active 4^3 set is bit-identical; weights and accumulation are FP32.
+// particle): particles are binned by cell (tile-major) with warp-aggregated
+// atomics; one CTA per tile splats its particles, one thread per cell holding
+// a register window per face field, into warp-private shared boxes, combines
+// them into a staging box per tile, and the normalisation pass sums the
+// staging boxes that reach each node.  Every sum runs in a fixed order, so
+// P2G is reproducible bit for bit.  Block activation is decided with the
+// reference's FP64 operation order wherever FP32 could differ, so the active
+// 4^3 set is bit-identical; weights and accumulation are FP32.
 #include <cmath>
 
 #include "pf_ctx.h"
@@ -24,22 +26,6 @@ namespace pf {
 namespace {
 
 constexpr double kR2 = 2.25;  // KR*KR with KR = 1.5 (sparse_ops3d_tp.cpp:21)
-constexpr int kBox = 12;      // shared box edge: tile (8) + halo 2 below, 2 above
-constexpr int kBox3 = kBox * kBox * kBox;
-// Shared box of one face field: each x row holds the 12 momentum nodes and
-// then the 12 mass nodes, so a row is 24 floats.  The splat's flush adds, per
-// instruction, one window offset for a warp's 32 cells (8 along x, 4 rows
-// along y): with a row pitch of 24 words those land in 32 distinct banks, for
-// momentum (x + 24y) and for mass (x + 12 + 24y) alike.
-constexpr int kRow = 2 * kBox;
-constexpr int kFieldBox = kRow * kBox * kBox;  // floats per face field
-__device__ __forceinline__ int box_mom(int X, int Y, int Z) { return X + kRow * (Y + kBox * Z); }
-
-// shared-memory float add whose old value nobody waits for
-__device__ __forceinline__ void red_shared_add(float* p, float v) {
-  asm volatile("red.shared.add.f32 [%0], %1;" ::"r"((unsigned)__cvta_generic_to_shared(p)), "f"(v));
-}
-
 // grid coordinate (pos - o)/dx in the reference's double arithmetic
 __device__ __forceinline__ double grid_coord(float p, double o, double dx) {
   return __ddiv_rn(__dsub_rn((double)p, o), dx);
@@ -239,27 +225,53 @@ __global__ void k_mark_particles(DevGrid G, const float* __restrict__ px, const 
 // ---------------------------------------------------------------------------
 // P2G splat: one CTA per tile holding particles
 // ---------------------------------------------------------------------------
-// P2G splat, one thread per cell.  For face field a every particle of cell
-// (ci,cj,ck) touches nodes ci-1..ci+2 along the field's normal axis and
-// c-1..c+1 along the two transverse axes (the -1/2 shift puts the transverse
-// window base at c-1 whatever the particle's position).  A thread therefore
-// accumulates all particles of its cell into a 4x3x3 register window -- the
-// three or four window nodes a particle does not reach have |d| >= 1.5 and
-// receive weight 0 -- and adds the window into the tile's shared box once:
-// 72 shared atomics per cell and field instead of 54 per particle, and in each
-// atomic instruction the lanes (neighbouring cells) address distinct nodes.
+// One thread per cell, passes over the tile's 512 cells.  For face field A
+// every particle of cell c touches window nodes c-1..c+2 along the field's
+// normal axis L = A and c-1..c+1 along the two transverse axes S1 < S2 (the
+// -1/2 shift puts the transverse window base at c-1 whatever the particle's
+// position).  A thread accumulates all particles of its cell into a 4x3x3
+// register window; the nodes a particle does not reach have |d| >= 1.5 and
+// receive weight 0.
 //
-// The same pass decides the 4^3 activation (preactivateKernel,
-// sparse_ops3d_tp.cpp:23-40: the block of every node with w > 0, i.e.
-// fl(fl(dx^2 + dy^2) + dz^2) < 2.25 in FP64).  A window spans at most two
-// blocks per axis; a block is reached iff the sum of the per-axis minima of
-// d^2 over its window nodes is below 2.25.  The FP32 minima (the weights'
-// d^2/r^2, absolute error below 1e-5) decide every block clear of the
-// threshold by kReachEps; a particle with a block inside the band redoes the
-// field's blocks in the reference's FP64 arithmetic.  Reached blocks are
-// OR-ed per cell, then per tile, and each tile CTA writes its blocks' bytes.
-constexpr int kSplatThreads = 256;
+// Determinism.  Every node's sum is formed in one fixed order, so two runs on
+// the same particles give bit-identical fields:
+//   * a cell's particles are taken in ascending index (sorted at the start of
+//     the kernel; binning ranks particles in arrival order);
+//   * each warp adds its 32 cells' windows into a shared box of its own, one
+//     window offset at a time (the lanes address distinct nodes);
+//   * the 16 warp boxes of the tile are combined node by node in warp order
+//     into the tile's staging box in global memory;
+//   * k_normalize adds the staging boxes of the (up to 8) tiles covering a
+//     node in ascending tile offset.
+// No floating-point atomics are used.
+//
+// Activation (preactivateKernel, sparse_ops3d_tp.cpp:23-40: the 4^3 block of
+// every node with w > 0, i.e. fl(fl(dx^2 + dy^2) + dz^2) < 2.25 in FP64).  A
+// window spans at most two blocks per axis; a block is reached iff the sum of
+// the per-axis minima of d^2/r^2 over its window nodes is below 1.  The
+// thread keeps, per window block, the minimum of that FP32 sum over its
+// cell's particles: a minimum clear of 1 by kReachEps decides the block for
+// the whole cell (the FP32 sums are within 1e-5 of the FP64 ones); a minimum
+// inside the band sends every particle of the cell through the reference's
+// FP64 arithmetic (exact_reach).  Reached blocks are OR-ed per tile and each
+// tile CTA writes its blocks' bytes.
 constexpr float kReachEps = 2e-5f;
+constexpr int kSplatThreads = 128;                 // threads per tile CTA
+constexpr int kSplatPasses = PF_TV / kSplatThreads;
+constexpr int kSplatGroups = PF_TV / 32;           // warp boxes per tile (one per warp and pass)
+// Warp box of one field: the window nodes of a warp's 8 x 4 x 1 cells.  The x
+// pitch is 12 float2 (mom, mass) and a warp's lanes cover the rows y = 0, 2
+// (lanes 0-15) and 1, 3 (lanes 16-31), so each half-warp's 64-bit accesses
+// fall on 16 distinct bank pairs.
+constexpr int kWarpPitch = 12;
+constexpr int kWarpBox = kWarpPitch * 6 * 4;       // x pitch * max(GY * GZ) over the fields
+// Staging box of one tile and field: nodes -1..9 along the normal axis and
+// -1..8 along the transverse axes relative to the tile's first cell.
+constexpr int kStageField = 11 * 10 * 10;
+constexpr int kStageTile = 3 * kStageField;
+constexpr int kBigSortStage = kSplatGroups * kWarpBox * 2;  // ints of the warp boxes reused by the big-cell sort
+
+static_assert(kStageTile == kSplatStageTile, "staging size mismatch");
 
 // Two FP32 values in one 64-bit register, for the packed .f32x2 arithmetic
 // of sm_100 (one instruction for both lanes of add, sub, mul and fma).
@@ -272,6 +284,11 @@ __device__ __forceinline__ f32x2 f2_pack(float lo, float hi) {
 }
 __device__ __forceinline__ void f2_unpack(f32x2 v, float& lo, float& hi) {
   asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f32x2 f2_add(f32x2 a, f32x2 b) {
+  f32x2 d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
 }
 __device__ __forceinline__ f32x2 f2_sub(f32x2 a, f32x2 b) {
   f32x2 d;
@@ -295,6 +312,7 @@ __device__ __forceinline__ float sub_sat(float a, float b) {
   asm("sub.rn.sat.f32 %0, %1, %2;" : "=f"(d) : "f"(a), "f"(b));
   return d;
 }
+
 // The FP64 decision for one particle and field: bit x + 2y + 4z for window
 // block (x, y, z), where window block 0 along an axis holds the window nodes
 // before the split s of that axis.  n[] are the global first window nodes.
@@ -330,27 +348,61 @@ __device__ unsigned exact_reach(const DevGrid& G, float ppx, float ppy, float pp
   return r;
 }
 
-// Window geometry of one cell for face field A.  The window is 4 nodes along
-// the field's normal axis L = A and 3 along the transverse axes S1 < S2.
+// Batcher's odd-even merge sort of N register values (all indices resolve at
+// compile time).
+template <int N>
+__device__ __forceinline__ void sort_net(int (&a)[N]) {
+#pragma unroll
+  for (int p = 1; p < N; p <<= 1)
+#pragma unroll
+    for (int k = p; k >= 1; k >>= 1)
+#pragma unroll
+      for (int j = k % p; j + k < N; j += 2 * k)
+#pragma unroll
+        for (int i = 0; i < k; ++i)
+          if (i + j + k < N && (i + j) / (2 * p) == (i + j + k) / (2 * p)) {
+            const int x = a[i + j], y = a[i + j + k];
+            a[i + j] = min(x, y);
+            a[i + j + k] = max(x, y);
+          }
+}
+
+template <int N>
+__device__ __forceinline__ void sort_segment(int* __restrict__ perm, int beg, int n) {
+  int a[N];
+#pragma unroll
+  for (int i = 0; i < N; ++i) a[i] = i < n ? perm[beg + i] : 0x7fffffff;
+  sort_net<N>(a);
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+    if (i < n) perm[beg + i] = a[i];
+}
+
+// Cell of thread `tid` in pass `pass`: lane bits 0-2 give x, lane bits 3-4 the
+// row (0, 2, 1, 3 in that order, for the warp box's bank pattern), the warp's
+// flat index g = warps * pass + warp gives the y half (g & 1) and z (g >> 1).
+__device__ __forceinline__ int splat_cell_of(int tid, int pass) {
+  const int lane = tid & 31, g = (kSplatThreads / 32) * pass + (tid >> 5);
+  const int q = lane >> 3;
+  const int y = 4 * (g & 1) + (((q & 1) << 1) | (q >> 1));
+  return (lane & 7) + 8 * y + 64 * (g >> 1);
+}
+
+// Window geometry of one cell for face field A: 4 nodes along the normal axis
+// L = A, 3 along the transverse axes S1 < S2.
 template <int A>
 struct SplatWindow {
   static constexpr int S1 = A == 0 ? 1 : 0, S2 = A == 2 ? 1 : 2;
-  int b[3];      // box-local first window node (the cell minus one) per axis
-  int n[3];      // global first window node per axis
+  int n[3];      // global first window node per axis (the cell minus one)
   int sp[3];     // window nodes before the 4^3 block boundary per axis
   unsigned off;  // bit 4*axis + i: node i off the field's lattice
 
-  __device__ __forceinline__ SplatWindow(const DevGrid& G, int cl, int o0, int o1, int o2, bool edge) {
-    const int o[3] = {o0, o1, o2};
-    b[0] = (cl & 7) + 1;
-    b[1] = ((cl >> 3) & 7) + 1;
-    b[2] = (cl >> 6) + 1;
+  __device__ __forceinline__ SplatWindow(const DevGrid& G, const int (&c)[3], bool edge) {
     off = 0u;
 #pragma unroll
     for (int ax = 0; ax < 3; ++ax) {
-      n[ax] = o[ax] + b[ax];
+      n[ax] = c[ax] - 1;
       sp[ax] = min(4 - (n[ax] & 3), ax == A ? 4 : 3);
-      // only tiles at the domain's faces have window nodes off the lattice
       if (edge)
 #pragma unroll
         for (int i = 0; i < (ax == A ? 4 : 3); ++i)
@@ -358,13 +410,15 @@ struct SplatWindow {
     }
   }
 
-  // Coordinates g relative to the first window node (transverse ones shifted
-  // by -1/2 onto the node lattice) and a = d^2/r^2 for window node i, d = g - i.
-  // With a power-of-two dx and a zero origin the product with 1/dx is exact
-  // and the FMA rounds X/dx - n once: the FP64 value rounded to float.  Nodes
-  // off the lattice get a = 2 (weight 0, never reached).
+  // a[ax][i] = d^2/r^2 for window node i along axis ax, d = g - i with g the
+  // particle's coordinate relative to the first window node (transverse axes
+  // shifted by -1/2 onto the node lattice).  With a power-of-two dx and a
+  // zero origin the product with 1/dx is exact and the FMA rounds X/dx - n
+  // once: the FP64 value rounded to float.  Nodes off the lattice get a = 2
+  // (weight 0, never reached).  Pairs (a0, a1), (a2, a3) per axis.
   __device__ __forceinline__ void coords(const DevGrid& G, float X, float Y, float Z, bool fast, float inv_dx_f,
-                                         double inv_dx, bool edge, float (&g)[3], float (&a)[3][4]) const {
+                                         double inv_dx, bool edge, f32x2 (&a)[3][2]) const {
+    float g[3];
     if (fast) {
       g[0] = fmaf(X, inv_dx_f, (float)-n[0]);
       g[1] = fmaf(Y, inv_dx_f, (float)-n[1]);
@@ -382,74 +436,74 @@ struct SplatWindow {
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const f32x2 d = f2_sub(gg, f2_pack((float)(2 * h), (float)(2 * h + 1)));
-        f2_unpack(f2_mul(f2_mul(d, d), k2), a[ax][2 * h], a[ax][2 * h + 1]);
+        a[ax][h] = f2_mul(f2_mul(d, d), k2);
       }
     }
     if (edge) {
 #pragma unroll
       for (int ax = 0; ax < 3; ++ax)
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
-          if ((off >> (4 * ax + i)) & 1u) a[ax][i] = 2.0f;
+        for (int h = 0; h < 2; ++h) {
+          float lo, hi;
+          f2_unpack(a[ax][h], lo, hi);
+          if ((off >> (4 * ax + 2 * h)) & 1u) lo = 2.0f;
+          if ((off >> (4 * ax + 2 * h + 1)) & 1u) hi = 2.0f;
+          a[ax][h] = f2_pack(lo, hi);
+        }
     }
   }
 
-  // FP32 activation from the per-axis minima of a over each window block: sets
-  // the bits of the blocks reached clear of the threshold, returns whether a
-  // block lies within kReachEps of it (decided in FP64 afterwards).
-  __device__ __forceinline__ bool reach32(const float (&a)[3][4], unsigned& reach) const {
-    float mn[3][2];
+  // Per-axis minima of a over the window nodes on each side of the block
+  // split.  kNearest: the particle lies in its cell (coordinate in [1, 2) from
+  // the first window node along L, [0.5, 1.5) along the transverse axes after
+  // the shift), so the nearest node on each side is known without a search.
+  template <bool kNearest>
+  __device__ __forceinline__ void side_minima(const f32x2 (&a)[3][2], float (&m)[3][2]) const {
 #pragma unroll
     for (int ax = 0; ax < 3; ++ax) {
-      mn[ax][0] = mn[ax][1] = 4.0f;
+      float v[4];
+      f2_unpack(a[ax][0], v[0], v[1]);
+      f2_unpack(a[ax][1], v[2], v[3]);
+      const int s = sp[ax];
+      if (kNearest) {
+        if (ax == A) {
+          const float m12 = fminf(v[1], v[2]);
+          m[ax][0] = s == 1 ? v[0] : s == 2 ? v[1] : m12;
+          m[ax][1] = s == 1 ? m12 : s == 2 ? v[2] : s == 3 ? v[3] : 4.0f;
+        } else {
+          m[ax][0] = s == 1 ? v[0] : v[1];
+          m[ax][1] = s == 1 ? v[1] : s == 2 ? v[2] : 4.0f;
+        }
+      } else {
+        m[ax][0] = m[ax][1] = 4.0f;
 #pragma unroll
-      for (int i = 0; i < (ax == A ? 4 : 3); ++i) {
-        if (i < sp[ax]) mn[ax][0] = fminf(mn[ax][0], a[ax][i]);
-        else mn[ax][1] = fminf(mn[ax][1], a[ax][i]);
+        for (int i = 0; i < (ax == A ? 4 : 3); ++i) {
+          if (i < s) m[ax][0] = fminf(m[ax][0], v[i]);
+          else m[ax][1] = fminf(m[ax][1], v[i]);
+        }
       }
     }
-    bool band = false;
-#pragma unroll
-    for (int z = 0; z < 2; ++z)
-#pragma unroll
-      for (int y = 0; y < 2; ++y)
-#pragma unroll
-        for (int x = 0; x < 2; ++x) {
-          const float sa = (mn[0][x] + mn[1][y]) + mn[2][z];
-          if (sa < 1.0f - kReachEps) reach |= 1u << (x + 2 * y + 4 * z);
-          band = band || fabsf(sa - 1.0f) <= kReachEps;
-        }
-    return band;
   }
 };
 
-// Splat of one cell's particles into face field A; returns the cell's reached
-// blocks as bits of the tile's 4x4x4 block box.
+// Splat of one cell's particles (perm[beg, end), ascending index) into the
+// window accumulators of face field A, and the cell's per-block minima of the
+// FP32 reach sums (bmin, block x + 2y + 4z).
 //
-// Nodes are held in pairs along L, so one packed f32x2 instruction serves two
-// nodes: node pair h of transverse node (s1, s2) is accumulator
-// q = 2*(3*s2 + s1) + h, L nodes 2h and 2h + 1.  Per node and particle the
+// Node pair h of transverse row r = s1 + 3*s2 holds L nodes 2h and 2h + 1, so
+// one packed f32x2 instruction serves two nodes.  Per node and particle the
 // weight is w = t^3 with t = sat((1 - a_L) - (a_S1 + a_S2)), i.e.
-// 1 - d^2/r^2 clamped at 0 (t <= 1 holds by itself).  The weight sum is one
-// pass over the window, the accumulation a second one that recomputes the
-// weights, which is cheaper than holding 36 of them in registers.  Particles
-// near a block's threshold are decided in FP64 after the cell's window has
-// been added to the shared box, outside the register-heavy loop.
-template <int A>
-__device__ __forceinline__ unsigned long long splat_cell(const DevGrid& G, float* sm, int cl, int beg, int end,
-                                           const int* __restrict__ perm, const float* __restrict__ px,
-                                           const float* __restrict__ py, const float* __restrict__ pz,
-                                           const float* __restrict__ vA, const uint8_t* __restrict__ type,
-                                           const float* __restrict__ vol, float m_l, float m_g, int o0, int o1,
-                                           int o2, double inv_dx, float inv_dx_f, bool fast, bool edge) {
+// 1 - d^2/r^2 clamped at 0 (t <= 1 holds by itself).  The 36 weights are kept
+// in registers between the weight sum and the accumulation.
+template <int A, bool kNearest>
+__device__ __forceinline__ void splat_particles(const DevGrid& G, const SplatWindow<A>& win, int beg, int end,
+                                                const int* __restrict__ perm, const float* __restrict__ px,
+                                                const float* __restrict__ py, const float* __restrict__ pz,
+                                                const float* __restrict__ vA, const uint8_t* __restrict__ type,
+                                                const float* __restrict__ vol, float m_l, float m_g, double inv_dx,
+                                                float inv_dx_f, bool fast, bool edge, f32x2 (&am)[9][2],
+                                                f32x2 (&ap)[9][2], float (&bmin)[8]) {
   using W = SplatWindow<A>;
-  constexpr int NP = 18;  // node pairs: 9 transverse nodes x 2 pairs along L
-  const W win(G, cl, o0, o1, o2, edge);
-  f32x2 am[NP], ap[NP];
-#pragma unroll
-  for (int q = 0; q < NP; ++q) { am[q] = 0ull; ap[q] = 0ull; }
-  unsigned reach = 0u;
-  bool banded = false;
   const f32x2 one2 = f2_pack(1.0f, 1.0f);
   // the next particle's attributes are loaded while this one is splatted
   int pn = perm[beg];
@@ -467,187 +521,353 @@ __device__ __forceinline__ unsigned long long splat_cell(const DevGrid& G, float
       voln = vol[pn];
       tn = type[pn];
     }
-    float g[3], a[3][4];
-    win.coords(G, X, Y, Z, fast, inv_dx_f, inv_dx, edge, g, a);
-    banded |= win.reach32(a, reach);
-    // 1 - a along L, and a_S1 + a_S2 per transverse node
-    f32x2 om2[2];
+    f32x2 a[3][2];
+    win.coords(G, X, Y, Z, fast, inv_dx_f, inv_dx, edge, a);
+    {
+      float m[3][2];
+      win.template side_minima<kNearest>(a, m);
 #pragma unroll
-    for (int h = 0; h < 2; ++h) om2[h] = f2_sub(one2, f2_pack(a[A][2 * h], a[A][2 * h + 1]));
+      for (int y = 0; y < 2; ++y)
+#pragma unroll
+        for (int x = 0; x < 2; ++x) {
+          const float sxy = m[0][x] + m[1][y];
+#pragma unroll
+          for (int z = 0; z < 2; ++z) bmin[x + 2 * y + 4 * z] = fminf(bmin[x + 2 * y + 4 * z], sxy + m[2][z]);
+        }
+    }
+    // 1 - a along L, and a_S1 + a_S2 per transverse row
+    const f32x2 om2[2] = {f2_sub(one2, a[A][0]), f2_sub(one2, a[A][1])};
     float om[4];
     f2_unpack(om2[0], om[0], om[1]);
     f2_unpack(om2[1], om[2], om[3]);
-    float at[9];
+    float aS1[4], aS2[4];
+    f2_unpack(a[W::S1][0], aS1[0], aS1[1]);
+    f2_unpack(a[W::S1][1], aS1[2], aS1[3]);
+    f2_unpack(a[W::S2][0], aS2[0], aS2[1]);
+    f2_unpack(a[W::S2][1], aS2[2], aS2[3]);
+    f32x2 w[9][2];
+    f32x2 ws = 0ull;
 #pragma unroll
     for (int s2 = 0; s2 < 3; ++s2)
 #pragma unroll
-      for (int s1 = 0; s1 < 3; ++s1) at[3 * s2 + s1] = a[W::S1][s1] + a[W::S2][s2];
-    // pass 1: the weight sum.  Along L the particle sits in [1, 2) from the
-    // first window node, so node 0 (d = g) and node 3 (d = 3 - g) are never
-    // both inside r = 1.5: three L nodes per row carry all the weight.
-    const float oe = g[A] < 1.5f ? om[0] : om[3];
-    float ws0 = 0.0f, ws1 = 0.0f, ws2 = 0.0f;
+      for (int s1 = 0; s1 < 3; ++s1) {
+        const int r = s1 + 3 * s2;
+        const float at = aS1[s1] + aS2[s2];
 #pragma unroll
-    for (int r = 0; r < 9; ++r) {
-      const float t0 = sub_sat(oe, at[r]), t1 = sub_sat(om[1], at[r]), t2 = sub_sat(om[2], at[r]);
-      ws0 = fmaf(t0 * t0, t0, ws0);
-      ws1 = fmaf(t1 * t1, t1, ws1);
-      ws2 = fmaf(t2 * t2, t2, ws2);
-    }
-    const float wsum = (ws0 + ws1) + ws2;
+        for (int h = 0; h < 2; ++h) {
+          const f32x2 t = f2_pack(sub_sat(om[2 * h], at), sub_sat(om[2 * h + 1], at));
+          w[r][h] = f2_mul(f2_mul(t, t), t);
+          ws = f2_add(ws, w[r][h]);
+        }
+      }
+    float wlo, whi;
+    f2_unpack(ws, wlo, whi);
+    const float wsum = wlo + whi;
     if (!(wsum > 0.0f)) continue;
     const float mp = (TY == 0 ? m_l : m_g) * VOL;
     const float s_m = __fdividef(mp, wsum);
     const float s_p = s_m * VA;
     const f32x2 sm2 = f2_pack(s_m, s_m), sp2 = f2_pack(s_p, s_p);
-    // pass 2: the accumulation over the whole window, two L nodes per packed
-    // instruction (t clamped at 0 lane by lane; t <= 1 already)
 #pragma unroll
     for (int r = 0; r < 9; ++r)
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
-        float s0, s1;
-        f2_unpack(f2_sub(om2[h], f2_pack(at[r], at[r])), s0, s1);
-        const f32x2 t = f2_pack(fmaxf(s0, 0.0f), fmaxf(s1, 0.0f));
-        const f32x2 w = f2_mul(f2_mul(t, t), t);
-        am[2 * r + h] = f2_fma(w, sm2, am[2 * r + h]);
-        ap[2 * r + h] = f2_fma(w, sp2, ap[2 * r + h]);
+        am[r][h] = f2_fma(w[r][h], sm2, am[r][h]);
+        ap[r][h] = f2_fma(w[r][h], sp2, ap[r][h]);
       }
   }
-  float* sbox = sm + A * kFieldBox;
+}
+
+// Add a warp's window accumulators into its warp box, one (x, y) column of
+// window offsets at a time.  The lanes of a warp hold cells of one z layer, so
+// within a column the lanes and the z offsets address distinct nodes; between
+// columns a lane's node may be another lane's, hence the __syncwarp, which
+// also keeps the compiler from reordering the shared accesses across columns.
+template <int A>
+__device__ __forceinline__ void flush_window(float2* wb, int x, int yl, const f32x2 (&am)[9][2],
+                                             const f32x2 (&ap)[9][2]) {
+  constexpr int S1 = A == 0 ? 1 : 0, S2 = A == 2 ? 1 : 2;
+  constexpr int GY = A == 1 ? 7 : 6;
+  constexpr int NX = A == 0 ? 4 : 3, NY = A == 1 ? 4 : 3, NZ = A == 2 ? 4 : 3;
+  float2* base = wb + x + kWarpPitch * yl;
 #pragma unroll
-  for (int q = 0; q < NP; ++q) {
-    float m2[2], p2[2];
-    f2_unpack(am[q], m2[0], m2[1]);
-    f2_unpack(ap[q], p2[0], p2[1]);
+  for (int ix = 0; ix < NX; ++ix)
 #pragma unroll
-    for (int e = 0; e < 2; ++e) {
-      if (m2[e] != 0.0f || p2[e] != 0.0f) {
-        int idx[3];
-        idx[A] = 2 * (q & 1) + e;
-        idx[W::S1] = (q >> 1) % 3;
-        idx[W::S2] = (q >> 1) / 3;
-        const int si = box_mom(win.b[0] + idx[0], win.b[1] + idx[1], win.b[2] + idx[2]);
-        red_shared_add(&sbox[si], p2[e]);
-        red_shared_add(&sbox[si + kBox], m2[e]);
+    for (int iy = 0; iy < NY; ++iy) {
+#pragma unroll
+      for (int iz = 0; iz < NZ; ++iz) {
+        const int idx[3] = {ix, iy, iz};
+        const int l = idx[A], r = idx[S1] + 3 * idx[S2];
+        float2* p = base + ix + kWarpPitch * (iy + GY * iz);
+        float mlo, mhi, plo, phi;
+        f2_unpack(am[r][l >> 1], mlo, mhi);
+        f2_unpack(ap[r][l >> 1], plo, phi);
+        float2 v = *p;
+        v.x += (l & 1) ? phi : plo;
+        v.y += (l & 1) ? mhi : mlo;
+        *p = v;
       }
+      __syncwarp();
     }
-  }
-  // particles with a block inside the FP32 band: the reference's FP64 decision
-  if (banded) {
-    for (int q = beg; q < end; ++q) {
-      const int p = perm[q];
-      float g[3], a[3][4];
-      unsigned dummy = 0u;
-      win.coords(G, px[p], py[p], pz[p], fast, inv_dx_f, inv_dx, edge, g, a);
-      if (win.reach32(a, dummy)) reach |= exact_reach<A>(G, px[p], py[p], pz[p], win.n, win.sp);
-    }
-  }
-  // reached window blocks -> the tile's 4x4x4 block box (block of node o -> (o >> 2) - (o0 >> 2))
-  const int w0 = (win.n[0] >> 2) - (o0 >> 2), w1 = (win.n[1] >> 2) - (o1 >> 2), w2 = (win.n[2] >> 2) - (o2 >> 2);
+}
+
+// One field of the splat: every pass's cells into the warp boxes, then the
+// warp boxes into the tile's staging box.  Returns this thread's reached
+// blocks (bits of the tile's 4x4x4 block box).
+template <int A>
+__device__ __forceinline__ unsigned long long splat_field(const DevGrid& G, float2* wbox, float2* __restrict__ stage,
+                                                          const int* __restrict__ cs, const int* __restrict__ perm,
+                                                          const float* __restrict__ px, const float* __restrict__ py,
+                                                          const float* __restrict__ pz, const float* __restrict__ vA,
+                                                          const uint8_t* __restrict__ type,
+                                                          const float* __restrict__ vol, float m_l, float m_g,
+                                                          const int (&t0)[3], double inv_dx, float inv_dx_f, bool fast,
+                                                          bool edge) {
+  constexpr int GY = A == 1 ? 7 : 6, GZ = A == 2 ? 4 : 3;
+  constexpr int FX = A == 0 ? 11 : 10, FY = A == 1 ? 11 : 10, FZ = A == 2 ? 11 : 10;
+  const int tid = threadIdx.x, lane = tid & 31;
+  for (int e = tid; e < kSplatGroups * kWarpBox; e += kSplatThreads) wbox[e] = make_float2(0.0f, 0.0f);
+  __syncthreads();
   unsigned long long box = 0ull;
+#pragma unroll 1
+  for (int pass = 0; pass < kSplatPasses; ++pass) {
+    const int cl = splat_cell_of(tid, pass);
+    const int beg = cs[cl], end = cs[cl + 1];
+    const int c[3] = {t0[0] + (cl & 7), t0[1] + ((cl >> 3) & 7), t0[2] + (cl >> 6)};
+    const SplatWindow<A> win(G, c, edge);
+    f32x2 am[9][2], ap[9][2];
 #pragma unroll
-  for (int bb = 0; bb < 8; ++bb)
-    if ((reach >> bb) & 1u) box |= 1ull << ((w0 + (bb & 1)) + 4 * ((w1 + ((bb >> 1) & 1)) + 4 * (w2 + (bb >> 2))));
+    for (int r = 0; r < 9; ++r)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) am[r][h] = ap[r][h] = 0ull;
+    float bmin[8];
+#pragma unroll
+    for (int b = 0; b < 8; ++b) bmin[b] = 4.0f;
+    if (beg < end) {
+      if (fast && !edge)
+        splat_particles<A, true>(G, win, beg, end, perm, px, py, pz, vA, type, vol, m_l, m_g, inv_dx, inv_dx_f, fast,
+                                 edge, am, ap, bmin);
+      else
+        splat_particles<A, false>(G, win, beg, end, perm, px, py, pz, vA, type, vol, m_l, m_g, inv_dx, inv_dx_f,
+                                  fast, edge, am, ap, bmin);
+    }
+    // this warp's cells into its box (a warp whose cells are all empty adds nothing)
+    if (__any_sync(0xffffffffu, beg < end)) {
+      const int g = (kSplatThreads / 32) * pass + (tid >> 5);
+      const int q = lane >> 3;
+      flush_window<A>(wbox + g * kWarpBox, lane & 7, ((q & 1) << 1) | (q >> 1), am, ap);
+    }
+    // the cell's reached blocks; the FP64 test for a cell with a block in the band
+    unsigned reach = 0u;
+    bool band = false;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      if (bmin[b] < 1.0f - kReachEps) reach |= 1u << b;
+      band = band || fabsf(bmin[b] - 1.0f) <= kReachEps;
+    }
+    if (band)
+      for (int q2 = beg; q2 < end; ++q2) {
+        const int p = perm[q2];
+        reach |= exact_reach<A>(G, px[p], py[p], pz[p], win.n, win.sp);
+      }
+    // window blocks -> the tile's 4x4x4 block box (block of node o -> (o >> 2) - 2*tile - ... )
+    const int w0 = (win.n[0] >> 2) - (t0[0] >> 2) + 1, w1 = (win.n[1] >> 2) - (t0[1] >> 2) + 1,
+              w2 = (win.n[2] >> 2) - (t0[2] >> 2) + 1;
+#pragma unroll
+    for (int bb = 0; bb < 8; ++bb)
+      if ((reach >> bb) & 1u) box |= 1ull << ((w0 + (bb & 1)) + 4 * ((w1 + ((bb >> 1) & 1)) + 4 * (w2 + (bb >> 2))));
+  }
+  __syncthreads();
+  // warp boxes -> staging box, node by node in warp order (z ascending, then y half)
+  float2* st = stage + A * kStageField;
+  for (int e = tid; e < FX * FY * FZ; e += kSplatThreads) {
+    const int X = e % FX, Y = (e / FX) % FY, Z = e / (FX * FY);
+    float2 s = make_float2(0.0f, 0.0f);
+    const int zlo = max(0, Z - GZ + 1), zhi = min(7, Z);
+    for (int z = zlo; z <= zhi; ++z)
+#pragma unroll
+      for (int yh = 0; yh < 2; ++yh) {
+        const int Yl = Y - 4 * yh;
+        if (Yl < 0 || Yl >= GY) continue;
+        const float2 v = wbox[(2 * z + yh) * kWarpBox + X + kWarpPitch * (Yl + GY * (Z - z))];
+        s.x += v.x;
+        s.y += v.y;
+      }
+    st[e] = s;
+  }
+  __syncthreads();
   return box;
 }
 
-__global__ void __launch_bounds__(kSplatThreads, 2) k_splat(DevGrid G, const int* __restrict__ cell_start,
-                                                         const int* __restrict__ perm,
-                                                         const float* __restrict__ px,
-                                                         const float* __restrict__ py,
-                                                         const float* __restrict__ pz,
-                                                         const float* __restrict__ vx,
-                                                         const float* __restrict__ vy,
-                                                         const float* __restrict__ vz,
-                                                         const uint8_t* __restrict__ type,
-                                                         const float* __restrict__ vol, float m_l, float m_g) {
-  extern __shared__ float sm[];  // [3 axes][kFieldBox]: rows of 12 momentum, 12 mass nodes
-  __shared__ unsigned sblk[6];   // [3 axes][64 reached blocks of the box]
+// The tile's 4x4x4 block box: node-block (o >> 2) relative to the tile's first
+// 4^3 block minus one, i.e. box index 0 is the block below the tile.
+__global__ void __launch_bounds__(kSplatThreads, 3) k_splat(DevGrid G, const int* __restrict__ cell_start,
+                                                           int* __restrict__ perm, int* __restrict__ sort_tmp,
+                                                           float2* __restrict__ stage,
+                                                           const float* __restrict__ px,
+                                                           const float* __restrict__ py,
+                                                           const float* __restrict__ pz,
+                                                           const float* __restrict__ vx,
+                                                           const float* __restrict__ vy,
+                                                           const float* __restrict__ vz,
+                                                           const uint8_t* __restrict__ type,
+                                                           const float* __restrict__ vol, float m_l, float m_g) {
+  extern __shared__ float2 wbox[];  // [kSplatGroups][kWarpBox]
+  __shared__ unsigned sblk[6];      // [3 axes][64 reached blocks of the box]
+  __shared__ int nbig;
+  __shared__ int big[PF_TV];
   const int t = blockIdx.x;
   const int* cs = cell_start + (size_t)t * PF_TV;
   if (cs[0] >= cs[PF_TV]) return;
-  for (int e = threadIdx.x; e < 3 * kFieldBox; e += kSplatThreads) sm[e] = 0.0f;
-  if (threadIdx.x < 6) sblk[threadIdx.x] = 0u;
+  const int tid = threadIdx.x;
+  if (tid < 6) sblk[tid] = 0u;
+  if (tid == 0) nbig = 0;
   __syncthreads();
+  // cells in ascending particle index: small cells in registers, larger ones
+  // by ranks counted by the whole CTA
+  for (int pass = 0; pass < kSplatPasses; ++pass) {
+    const int cl = splat_cell_of(tid, pass);
+    const int beg = cs[cl], n = cs[cl + 1] - beg;
+    if (n <= 1) continue;
+    if (n <= 8) sort_segment<8>(perm, beg, n);
+    else if (n <= 16) sort_segment<16>(perm, beg, n);
+    else big[atomicAdd(&nbig, 1)] = cl;
+  }
+  __syncthreads();
+  for (int b = 0; b < nbig; ++b) {
+    const int cl = big[b];
+    const int beg = cs[cl], n = cs[cl + 1] - beg;
+    int* sv = reinterpret_cast<int*>(wbox);
+    const bool staged = n <= kBigSortStage;
+    if (staged)
+      for (int i = tid; i < n; i += kSplatThreads) sv[i] = perm[beg + i];
+    __syncthreads();
+    for (int i = tid; i < n; i += kSplatThreads) {
+      const int v = staged ? sv[i] : perm[beg + i];
+      int r = 0;
+      if (staged)
+        for (int j = 0; j < n; ++j) r += sv[j] < v;
+      else
+        for (int j = 0; j < n; ++j) r += perm[beg + j] < v;
+      sort_tmp[beg + r] = v;
+    }
+    __syncthreads();
+    for (int i = tid; i < n; i += kSplatThreads) perm[beg + i] = sort_tmp[beg + i];
+    __syncthreads();
+  }
   const int tx = t % G.g.TX, tq = t / G.g.TX, ty = tq % G.g.TY, tz = tq / G.g.TY;
-  const int o0 = tx * 8 - 2, o1 = ty * 8 - 2, o2 = tz * 8 - 2;
+  const int t0[3] = {tx * 8, ty * 8, tz * 8};
   const double inv_dx = G.g.inv_dx;
   const float inv_dx_f = (float)inv_dx;
   const bool fast = G.g.dx_pow2 && G.g.ox == 0.0 && G.g.oy == 0.0 && G.g.oz == 0.0;
   // window nodes of this tile's cells span global nodes 8t - 1 .. 8t + 9 per axis
   const bool edge = tx == 0 || ty == 0 || tz == 0 || tx * 8 + 10 > G.g.nx || ty * 8 + 10 > G.g.ny ||
                     tz * 8 + 10 > G.g.nz;
-  unsigned long long box[3] = {0ull, 0ull, 0ull};  // reached blocks of this thread's cells
-  for (int cl = threadIdx.x; cl < PF_TV; cl += kSplatThreads) {
-    const int beg = cs[cl], end = cs[cl + 1];
-    if (beg >= end) continue;
-    box[0] |= splat_cell<0>(G, sm, cl, beg, end, perm, px, py, pz, vx, type, vol, m_l, m_g, o0, o1, o2, inv_dx,
-                             inv_dx_f, fast, edge);
-    box[1] |= splat_cell<1>(G, sm, cl, beg, end, perm, px, py, pz, vy, type, vol, m_l, m_g, o0, o1, o2, inv_dx,
-                             inv_dx_f, fast, edge);
-    box[2] |= splat_cell<2>(G, sm, cl, beg, end, perm, px, py, pz, vz, type, vol, m_l, m_g, o0, o1, o2, inv_dx,
-                             inv_dx_f, fast, edge);
-  }
+  float2* st = stage + (size_t)t * kStageTile;
+  unsigned long long box[3];
+  box[0] = splat_field<0>(G, wbox, st, cs, perm, px, py, pz, vx, type, vol, m_l, m_g, t0, inv_dx, inv_dx_f, fast,
+                          edge);
+  box[1] = splat_field<1>(G, wbox, st, cs, perm, px, py, pz, vy, type, vol, m_l, m_g, t0, inv_dx, inv_dx_f, fast,
+                          edge);
+  box[2] = splat_field<2>(G, wbox, st, cs, perm, px, py, pz, vz, type, vol, m_l, m_g, t0, inv_dx, inv_dx_f, fast,
+                          edge);
   // one shared OR per warp and word
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     const unsigned lo = __reduce_or_sync(0xffffffffu, (unsigned)box[a]);
     const unsigned hi = __reduce_or_sync(0xffffffffu, (unsigned)(box[a] >> 32));
-    if ((threadIdx.x & 31) == 0) {
+    if ((tid & 31) == 0) {
       if (lo) atomicOr(&sblk[2 * a], lo);
       if (hi) atomicOr(&sblk[2 * a + 1], hi);
     }
   }
   __syncthreads();
   // activity bytes of the reached blocks (a byte is stored only when it reads 0)
-  if (threadIdx.x < 3 * 64) {
-    const int a = threadIdx.x >> 6, idx = threadIdx.x & 63;
+  for (int e = tid; e < 3 * 64; e += kSplatThreads) {
+    const int a = e >> 6, idx = e & 63;
     if ((sblk[2 * a + (idx >> 5)] >> (idx & 31)) & 1u) {
       const int fv = PF_U + a;
-      const int gbx = (o0 >> 2) + (idx & 3), gby = (o1 >> 2) + ((idx >> 2) & 3), gbz = (o2 >> 2) + (idx >> 4);
+      const int gbx = 2 * tx - 1 + (idx & 3), gby = 2 * ty - 1 + ((idx >> 2) & 3), gbz = 2 * tz - 1 + (idx >> 4);
       const int bi = gbx + G.g.bdim[fv][0] * (gby + G.g.bdim[fv][1] * gbz);
       if (!G.act4[fv][bi]) G.act4[fv][bi] = 1;
       if (!G.act4[fv + 3][bi]) G.act4[fv + 3][bi] = 1;
     }
   }
-  // add the box into the pooled fields (neighbouring tiles overlap in halos);
-  // contributions in blocks that end up inactive are cleared by k_normalize
-  for (int e = threadIdx.x; e < 3 * kBox3; e += kSplatThreads) {
-    const int a = e / kBox3, si = e - a * kBox3;
-    const int X = si % kBox, Y = (si / kBox) % kBox, Z = si / (kBox * kBox);
-    const float* sb = sm + a * kFieldBox + box_mom(X, Y, Z);
-    const float mom = sb[0], mas = sb[kBox];
-    if (mom == 0.0f && mas == 0.0f) continue;
-    const int i = o0 + X, j = o1 + Y, k = o2 + Z;
-    if (!in_field(G.g, PF_U + a, i, j, k)) continue;
-    const int sl = slot_of(G, i, j, k);
-    if (sl < 0) continue;
-    const size_t o = (size_t)sl * PF_TV + local_id(i, j, k);
-    atomicAdd(&G.fld[PF_U + a][o], mom);
-    atomicAdd(&G.fld[PF_MU + a][o], mas);
-  }
+}
+
+// Footprint index of local node l (0..7) of a tile along one axis in the
+// staging box of the tile at offset o (-1, 0, +1) along that axis, or -1 when
+// that tile's cells do not reach the node: along the normal axis a node takes
+// cells l-2..l+1, along a transverse axis l-1..l+1.
+__device__ __forceinline__ int stage_index(int l, int o, bool normal) {
+  if (o == 0) return l + 1;
+  if (o < 0) return (normal ? l <= 1 : l == 0) ? l + 9 : -1;
+  return l == 7 ? 0 : -1;
 }
 
 // normalisation u = P/m where m > 0 (sparse_ops3d_tp.cpp:126-152), with the
 // optional saved copy (step(): `saved = grid`) and gravity on v where mv > 0
-// (applyGravity) fused in.
-// Nodes of blocks the exact activation left inactive are cleared first: the
-// splat's FP32 weights may put a negligible contribution where the reference's
-// FP64 weight is zero, and inactive blocks stay zero.
-__global__ void k_normalize(DevGrid G, int nslots, int save, int gravity, float dv) {
+// (applyGravity) fused in.  With `gather` the momentum and raw mass of every
+// node are first summed from the staging boxes of the splatted tiles that
+// reach it, in ascending tile offset (z, then y, then x).
+// Nodes of blocks the exact activation left inactive are cleared: the splat's
+// FP32 weights may put a negligible contribution where the reference's FP64
+// weight is zero, and inactive blocks stay zero.
+__global__ void k_normalize(DevGrid G, const float2* __restrict__ stage, const int* __restrict__ cell_start,
+                            int gather, int nslots, int save, int gravity, float dv) {
+  __shared__ int splatted[27];
   for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
     const size_t o = (size_t)s * PF_TV + threadIdx.x;
     const int t = G.slot_tile[s];
     const int tx = t % G.g.TX, tq = t / G.g.TX, ty = tq % G.g.TY, tz = tq / G.g.TY;
-    const int i = tx * 8 + (threadIdx.x & 7), j = ty * 8 + ((threadIdx.x >> 3) & 7), k = tz * 8 + (threadIdx.x >> 6);
+    if (gather) {
+      __syncthreads();
+      if (threadIdx.x < 27) {
+        const int x = tx + (int)threadIdx.x % 3 - 1, y = ty + ((int)threadIdx.x / 3) % 3 - 1,
+                  z = tz + (int)threadIdx.x / 9 - 1;
+        int ok = 0;
+        if (x >= 0 && y >= 0 && z >= 0 && x < G.g.TX && y < G.g.TY && z < G.g.TZ) {
+          const size_t nt = (size_t)tile_id(G.g, x, y, z) * PF_TV;
+          ok = cell_start[nt] < cell_start[nt + PF_TV];
+        }
+        splatted[threadIdx.x] = ok;
+      }
+      __syncthreads();
+    }
+    const int li = threadIdx.x & 7, lj = (threadIdx.x >> 3) & 7, lk = threadIdx.x >> 6;
+    const int i = tx * 8 + li, j = ty * 8 + lj, k = tz * 8 + lk;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       const int f = PF_MU + a;
+      float m = 0.0f, u = 0.0f;
+      if (gather) {
+        const int FX = a == 0 ? 11 : 10, FY = a == 1 ? 11 : 10;
+#pragma unroll
+        for (int oz = -1; oz <= 1; ++oz) {
+          const int iz = stage_index(lk, oz, a == 2);
+          if (iz < 0) continue;
+#pragma unroll
+          for (int oy = -1; oy <= 1; ++oy) {
+            const int iy = stage_index(lj, oy, a == 1);
+            if (iy < 0) continue;
+#pragma unroll
+            for (int ox = -1; ox <= 1; ++ox) {
+              const int ix = stage_index(li, ox, a == 0);
+              if (ix < 0 || !splatted[(ox + 1) + 3 * ((oy + 1) + 3 * (oz + 1))]) continue;
+              const int tn = tile_id(G.g, tx + ox, ty + oy, tz + oz);
+              const float2 v = stage[(size_t)tn * kStageTile + a * kStageField + ix + FX * (iy + FY * iz)];
+              u += v.x;
+              m += v.y;
+            }
+          }
+        }
+      } else {
+        m = G.fld[f][o];
+        u = G.fld[PF_U + a][o];
+      }
       const bool act = in_field(G.g, f, i, j, k) && G.act4[f][act4_index(G.g, f, i, j, k)];
-      float m = act ? G.fld[f][o] : 0.0f;
-      float u = act ? G.fld[PF_U + a][o] : 0.0f;
-      if (!act) G.fld[f][o] = 0.0f;
+      if (!act) m = u = 0.0f;
+      G.fld[f][o] = m;
       if (m > 0.0f) u = u / m;
       if (save) G.saved[a][o] = u;
       if (a == 1 && gravity && m > 0.0f) u = u + dv;
@@ -1125,6 +1345,7 @@ static int p2g_core(pf_ctx* ctx, const pf_phase* ph, double Vp) {
   const int n = (int)ctx->np;
   const int nt = ctx->g.ntiles;
   ctx->bins_valid = false;
+  ctx->splat_fresh = false;
   for (int f = PF_U; f <= PF_MW; ++f) {
     int rc = field_clear(ctx, f);
     if (rc) return rc;
@@ -1160,10 +1381,11 @@ static int p2g_core(pf_ctx* ctx, const pf_phase* ph, double Vp) {
   }
   {
     StageScope sc(ctx, PF_STAGE_SPLAT);
-    const size_t smem = 3 * kFieldBox * sizeof(float);
+    const size_t smem = (size_t)kSplatGroups * kWarpBox * sizeof(float2);
     (++ctx->launches), k_splat<<<nt, kSplatThreads, smem, ctx->stream>>>(
-        dev_grid(ctx), ctx->tile_start, ctx->perm, ctx->px, ctx->py, ctx->pz, ctx->vx, ctx->vy, ctx->vz, ctx->type,
-        ctx->vol, (float)(ph->rho_l * Vp), (float)(ph->rho_g * Vp));
+        dev_grid(ctx), ctx->tile_start, ctx->perm, ctx->prank, ctx->splat_stage, ctx->px, ctx->py, ctx->pz, ctx->vx,
+        ctx->vy, ctx->vz, ctx->type, ctx->vol, (float)(ph->rho_l * Vp), (float)(ph->rho_g * Vp));
+    ctx->splat_fresh = true;
     PF_CUDA_TRY(cudaGetLastError());
   }
   return PF_OK;
@@ -1178,8 +1400,10 @@ int p2g(pf_ctx* ctx, const pf_phase* ph, double Vp) {
 int normalize_save_gravity(pf_ctx* ctx, bool save, bool gravity, double dt, double gval) {
   StageScope stage(ctx, PF_STAGE_NORMALIZE);
   if (ctx->nslots > 0)
-    (++ctx->launches), k_normalize<<<slot_grid(ctx), PF_TV, 0, ctx->stream>>>(dev_grid(ctx), ctx->nslots, save ? 1 : 0,
-                                                           gravity ? 1 : 0, (float)(dt * gval));
+    (++ctx->launches), k_normalize<<<slot_grid(ctx), PF_TV, 0, ctx->stream>>>(
+        dev_grid(ctx), ctx->splat_stage, ctx->tile_start, ctx->splat_fresh ? 1 : 0, ctx->nslots, save ? 1 : 0,
+        gravity ? 1 : 0, (float)(dt * gval));
+  ctx->splat_fresh = false;
   PF_CUDA_TRY(cudaGetLastError());
   if (save) ctx->saved_valid = true;
   return PF_OK;

@@ -243,6 +243,7 @@ def ref_lib():
     lib.pfr_get_field.argtypes = [vp, C.c_int, _fp, _up]
     lib.pfr_set_field.argtypes = [vp, C.c_int, _fp, _up]
     lib.pfr_active_block_ids.argtypes = [vp, C.c_int, C.c_void_p, C.POINTER(C.c_size_t)]
+    lib.pfr_collect_cells.argtypes = [vp, C.c_int, C.c_void_p, C.POINTER(C.c_size_t)]
     lib.pfr_set_particles.argtypes = [vp, C.c_size_t, _dp, _dp, _up, _dp]
     lib.pfr_num_particles.restype = C.c_size_t
     lib.pfr_num_particles.argtypes = [vp]
@@ -379,6 +380,16 @@ class ReferenceGrid(_GridBase):
         out = np.zeros(n.value, np.int32)
         self.lib.pfr_active_block_ids(self.h, f, out.ctypes.data, C.byref(n))
         return out
+
+    def collect_cells(self, marker=1):
+        """sparse3d::collectCellsWithMarker (src/driver/sparse_ops3d_common.h:65-85): the cells
+        with `marker`, ascending linear index, from the reference's own code."""
+        n = C.c_size_t()
+        self.lib.pfr_collect_cells(self.h, int(marker), None, C.byref(n))
+        out = np.zeros(max(n.value, 1), np.int32)
+        if self.lib.pfr_collect_cells(self.h, int(marker), out.ctypes.data, C.byref(n)) != 0:
+            raise RuntimeError("pfr_collect_cells failed")
+        return out[: n.value].astype(np.int64)
 
     def _put(self, ps: Particles):
         self.lib.pfr_set_particles(self.h, len(ps), ps.pos, ps.vel, ps.type, ps.volume)

@@ -9,8 +9,10 @@
 #include "pf_oracle.h"
 
 #include <math.h>
+#include <pthread.h>
 #include <stdlib.h>
 #include <string.h>
+#include <unistd.h>
 
 struct pfo_grid {
   int nx, ny, nz;
@@ -220,8 +222,9 @@ double pfo_calibrate_rho_tilde0(const pfo_phase* pp, double Vp) {
 /* ------------------------------------------------------------------ */
 
 /* preactivateKernel (:23-40): activate the block of every window node with
- * nonzero weight. */
-static void preactivate(pfo_grid* g, int f, double gx, double gy, double gz) {
+ * nonzero weight.  Only nodes with k in [klo, khi) are visited (the slab of
+ * the thread that owns those blocks; see pfo_p2g). */
+static void preactivate(pfo_grid* g, int f, double gx, double gy, double gz, int klo, int khi) {
   const int X = g->dim[f][0], Y = g->dim[f][1], Z = g->dim[f][2];
   const int i0 = (int)floor(gx), j0 = (int)floor(gy), k0 = (int)floor(gz);
   for (int dk = -2; dk <= 3; ++dk)
@@ -229,6 +232,7 @@ static void preactivate(pfo_grid* g, int f, double gx, double gy, double gz) {
       for (int di = -2; di <= 3; ++di) {
         const int a = i0 + di, b = j0 + dj, c = k0 + dk;
         if (a < 0 || a >= X || b < 0 || b >= Y || c < 0 || c >= Z) continue;
+        if (c < klo || c >= khi) continue;
         const double ex = gx - a, ey = gy - b, ez = gz - c;
         if (cubic_weight(ex * ex + ey * ey + ez * ez) <= 0.0) continue;
         activate(g, f, a, b, c);
@@ -237,11 +241,13 @@ static void preactivate(pfo_grid* g, int f, double gx, double gy, double gz) {
 
 /* splatKernelColor (:42-75) without the colour filter: each node still
  * receives its contributions in particle-index order, which is the order the
- * reference's owning colour thread adds them in. */
+ * reference's owning colour thread adds them in.  The weight sum runs over the
+ * whole window; only nodes with k in [klo, khi) are written. */
 static void splat(pfo_grid* g, int fmom, int fmass, double gx, double gy, double gz,
-                  double mom, double mass) {
+                  double mom, double mass, int klo, int khi) {
   const int X = g->dim[fmom][0], Y = g->dim[fmom][1], Z = g->dim[fmom][2];
   const int i0 = (int)floor(gx), j0 = (int)floor(gy), k0 = (int)floor(gz);
+  if (k0 + 3 < klo || k0 - 2 >= khi) return;
   double wsum = 0.0;
   for (int dk = -2; dk <= 3; ++dk)
     for (int dj = -2; dj <= 3; ++dj)
@@ -257,6 +263,7 @@ static void splat(pfo_grid* g, int fmom, int fmass, double gx, double gy, double
       for (int di = -2; di <= 3; ++di) {
         const int a = i0 + di, b = j0 + dj, c = k0 + dk;
         if (a < 0 || a >= X || b < 0 || b >= Y || c < 0 || c >= Z) continue;
+        if (c < klo || c >= khi) continue;
         const double ex = gx - a, ey = gy - b, ez = gz - c;
         const double w = cubic_weight(ex * ex + ey * ey + ez * ez) / wsum;
         if (w <= 0.0) continue;
@@ -267,31 +274,83 @@ static void splat(pfo_grid* g, int fmom, int fmass, double gx, double gy, double
       }
 }
 
+/* One thread's share of P2G: every node with k in [klo, khi), i.e. whole
+ * 4^3 block layers, so no block byte or node is written by two threads.  The
+ * thread visits all particles in index order, so each node receives its
+ * contributions in the sequential order and the result does not depend on
+ * the number of threads. */
+typedef struct {
+  pfo_grid* g;
+  size_t n;
+  const double *pos, *vel, *vol;
+  const unsigned char* type;
+  const pfo_phase* pp;
+  double Vp;
+  int klo, khi;
+} p2g_slab;
+
+static void* p2g_slab_run(void* arg) {
+  const p2g_slab* s = (const p2g_slab*)arg;
+  pfo_grid* g = s->g;
+  const double* pos = s->pos;
+  for (size_t p = 0; p < s->n; ++p) {
+    const double px = (pos[3 * p + 0] - g->ox) / g->dx;
+    const double py = (pos[3 * p + 1] - g->oy) / g->dx;
+    const double pz = (pos[3 * p + 2] - g->oz) / g->dx;
+    preactivate(g, PFO_U, px, py - 0.5, pz - 0.5, s->klo, s->khi);
+    preactivate(g, PFO_MU, px, py - 0.5, pz - 0.5, s->klo, s->khi);
+    preactivate(g, PFO_V, px - 0.5, py, pz - 0.5, s->klo, s->khi);
+    preactivate(g, PFO_MV, px - 0.5, py, pz - 0.5, s->klo, s->khi);
+    preactivate(g, PFO_W, px - 0.5, py - 0.5, pz, s->klo, s->khi);
+    preactivate(g, PFO_MW, px - 0.5, py - 0.5, pz, s->klo, s->khi);
+  }
+  for (size_t p = 0; p < s->n; ++p) {
+    const double rho = s->type[p] == 0 ? s->pp->rho_l : s->pp->rho_g;
+    const double mp = rho * s->Vp * s->vol[p];
+    const double px = (pos[3 * p + 0] - g->ox) / g->dx;
+    const double py = (pos[3 * p + 1] - g->oy) / g->dx;
+    const double pz = (pos[3 * p + 2] - g->oz) / g->dx;
+    splat(g, PFO_U, PFO_MU, px, py - 0.5, pz - 0.5, mp * s->vel[3 * p + 0], mp, s->klo, s->khi);
+    splat(g, PFO_V, PFO_MV, px - 0.5, py, pz - 0.5, mp * s->vel[3 * p + 1], mp, s->klo, s->khi);
+    splat(g, PFO_W, PFO_MW, px - 0.5, py - 0.5, pz, mp * s->vel[3 * p + 2], mp, s->klo, s->khi);
+  }
+  return NULL;
+}
+
+/* Threads for P2G: PFO_THREADS if set, else the online CPUs, at most 64. */
+static int p2g_threads(void) {
+  const char* e = getenv("PFO_THREADS");
+  long t = e ? strtol(e, NULL, 10) : sysconf(_SC_NPROCESSORS_ONLN);
+  if (t < 1) t = 1;
+  if (t > 64) t = 64;
+  return (int)t;
+}
+
 int pfo_p2g(pfo_grid* g, size_t n, const double* pos, const double* vel,
             const unsigned char* type, const double* vol, const pfo_phase* pp, double Vp) {
   if (!g || !pp || (n && (!pos || !vel || !type || !vol))) return -1;
   for (int f = PFO_U; f <= PFO_MW; ++f) pfo_clear_field(g, f);
-  for (size_t p = 0; p < n; ++p) {
-    const double px = (pos[3 * p + 0] - g->ox) / g->dx;
-    const double py = (pos[3 * p + 1] - g->oy) / g->dx;
-    const double pz = (pos[3 * p + 2] - g->oz) / g->dx;
-    preactivate(g, PFO_U, px, py - 0.5, pz - 0.5);
-    preactivate(g, PFO_MU, px, py - 0.5, pz - 0.5);
-    preactivate(g, PFO_V, px - 0.5, py, pz - 0.5);
-    preactivate(g, PFO_MV, px - 0.5, py, pz - 0.5);
-    preactivate(g, PFO_W, px - 0.5, py - 0.5, pz);
-    preactivate(g, PFO_MW, px - 0.5, py - 0.5, pz);
+  /* block layers along z (the w lattice has the most) shared out in order */
+  const int layers = g->bdim[PFO_W][2];
+  int nt = p2g_threads();
+  if (nt > layers) nt = layers;
+  p2g_slab slabs[64];
+  pthread_t tid[64];
+  for (int t = 0; t < nt; ++t) {
+    p2g_slab* s = &slabs[t];
+    s->g = g; s->n = n; s->pos = pos; s->vel = vel; s->vol = vol; s->type = type; s->pp = pp; s->Vp = Vp;
+    s->klo = 4 * (int)((long)layers * t / nt);
+    s->khi = 4 * (int)((long)layers * (t + 1) / nt);
   }
-  for (size_t p = 0; p < n; ++p) {
-    const double rho = type[p] == 0 ? pp->rho_l : pp->rho_g;
-    const double mp = rho * Vp * vol[p];
-    const double px = (pos[3 * p + 0] - g->ox) / g->dx;
-    const double py = (pos[3 * p + 1] - g->oy) / g->dx;
-    const double pz = (pos[3 * p + 2] - g->oz) / g->dx;
-    splat(g, PFO_U, PFO_MU, px, py - 0.5, pz - 0.5, mp * vel[3 * p + 0], mp);
-    splat(g, PFO_V, PFO_MV, px - 0.5, py, pz - 0.5, mp * vel[3 * p + 1], mp);
-    splat(g, PFO_W, PFO_MW, px - 0.5, py - 0.5, pz, mp * vel[3 * p + 2], mp);
+  int started = 0;
+  for (int t = 1; t < nt; ++t) {
+    if (pthread_create(&tid[t], NULL, p2g_slab_run, &slabs[t]) != 0) break;
+    started = t;
   }
+  /* slabs whose thread did not start run here, after slab 0 */
+  p2g_slab_run(&slabs[0]);
+  for (int t = started + 1; t < nt; ++t) p2g_slab_run(&slabs[t]);
+  for (int t = 1; t <= started; ++t) pthread_join(tid[t], NULL);
   /* normalisation (:126-152): u = momentum / raw mass where the mass is > 0 */
   for (int a = 0; a < 3; ++a) {
     const int fv = PFO_U + a, fm = PFO_MU + a;

@@ -14,10 +14,12 @@
 //   applyLiquidParticleRefill (src/driver/particle_adaptivity3d.h:111-374)
 //   diagnoseSparseInterface3D (src/driver/interface_diagnostics3d.cpp:363-379)
 //   applySparseSurfaceTension3D (src/driver/interface_diagnostics3d.cpp:405-447)
+//   sparse3d::collectCellsWithMarker (src/driver/sparse_ops3d_common.h:65-85)
 // and converts between its SparseMacGrid3D<4> block pool and dense arrays
 // plus one activity byte per 4^3 block.
 #include "driver/interface_diagnostics3d.h"
 #include "driver/particle_adaptivity3d.h"
+#include "driver/sparse_ops3d_common.h"
 #include "driver/sparse_ops3d_tp.h"
 #include "driver/sparse_sim3d_tp.h"
 #include "grid/sparse_mac_grid3d.h"
@@ -114,6 +116,18 @@ int pfr_active_block_ids(void* hp, int f, int* out, size_t* n) {
   const auto& ids = fld->activeBlockIds();
   if (out) std::memcpy(out, ids.data(), ids.size() * sizeof(int));
   *n = ids.size();
+  return 0;
+}
+
+// Cells with the given marker, ascending linear index, as the projection
+// enumerates them.
+int pfr_collect_cells(void* hp, int marker, int* out, size_t* n) {
+  const std::vector<int> cells = sparse3d::collectCellsWithMarker(static_cast<Handle*>(hp)->sim.grid, marker);
+  if (out) {
+    if (cells.size() > *n) return -1;
+    std::memcpy(out, cells.data(), cells.size() * sizeof(int));
+  }
+  *n = cells.size();
   return 0;
 }
 

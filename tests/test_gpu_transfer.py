@@ -334,5 +334,5 @@ def test_async_upload_swaps_in_before_use(pf):
         return out
 
     a, b = run(True, 3), run(False, 3)
-    # the splat's atomics may add in another order: equal to FP32 rounding
-    assert rel_err(a, b) < 1e-6
+    # P2G sums in a fixed order: the two transfer steps agree bit for bit
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))

@@ -170,6 +170,26 @@ def test_reference_allocation_order_is_a_permutation_of_the_sorted_set():
     assert sorted(order.tolist()) == g.active_blocks(O.U).tolist()
 
 
+@needs_ref
+@pytest.mark.parametrize("seed", [0, 1])
+def test_oracle_cell_list_equals_reference_collect(seed):
+    """The oracle's fluid-cell list (pfo_collect_cells, the projection's
+    enumeration) is the reference's collectCellsWithMarker, bit for bit, on
+    markCells output and on a random marker field with holes."""
+    n = 14
+    o = O.Oracle()
+    go = O.OracleGrid(n, n, n, 1.0 / n)
+    o.mark_cells(go, _random_scene(n, seed, 3000, 0.3))
+    rng = np.random.default_rng(seed)
+    for mk in (go.cell_markers(), rng.choice([0, 1, 2], size=(n, n, n), p=[0.4, 0.5, 0.1])):
+        a, b = O.OracleGrid(n, n, n, 1.0 / n), O.ReferenceGrid(n, n, n, 1.0 / n)
+        a.set_cells(mk)
+        b.set_cells(mk)
+        ref = b.collect_cells(1)
+        assert len(ref) > 0
+        assert np.array_equal(a.fluid_cells(), ref)
+
+
 # ------------------------------------------- reference tests, restated
 
 def test_phase_field_curve():
