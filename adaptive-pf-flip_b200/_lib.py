@@ -61,7 +61,7 @@ class SolveCfg(C.Structure):
     _fields_ = [("mode", C.c_int), ("max_iter", C.c_int), ("abs_tol", C.c_double), ("rel_tol", C.c_double),
                 ("c_div", C.c_double), ("bf16_storage", C.c_int), ("check_every", C.c_int),
                 ("max_refine", C.c_int), ("inner_rel_tol", C.c_double), ("precond", C.c_int),
-                ("accept_min_gain", C.c_double), ("inner_fp32", C.c_int)]
+                ("accept_min_gain", C.c_double), ("inner_fp32", C.c_int), ("inner_max_iter", C.c_int)]
 
 
 class SolveStats(C.Structure):

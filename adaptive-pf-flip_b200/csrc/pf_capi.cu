@@ -58,7 +58,7 @@ void free_all(pf_ctx* c) {
   for (int* p : c->scan_levels) F(p);
   F(c->d_scalar);
   F(c->x); F(c->r); F(c->p); F(c->Ap); F(c->diag); F(c->cx); F(c->cy); F(c->cz); F(c->kind);
-  F(c->partials); F(c->ctl); F(c->nbr_plain);
+  F(c->partials); F(c->ctl); F(c->ctl_outer); F(c->nbr_plain);
   F(c->xf); F(c->rf); F(c->pf32); F(c->Apf); F(c->diagf); F(c->cxf); F(c->cyf); F(c->czf); F(c->pbf); F(c->cbf);
   F(c->b64);
   F(c->d_clamp); F(c->d_flags); F(c->cell_flags); F(c->esc_buf);
@@ -202,6 +202,8 @@ int create_impl(pf_ctx* ctx, const pf_grid_desc* d) {
   PF_CUDA_TRY(cudaMalloc(&ctx->ctl, sizeof(SolveCtl)));
   PF_CUDA_TRY(cudaMemset(ctx->ctl, 0, sizeof(SolveCtl)));
   PF_CUDA_TRY(cudaMallocHost(&ctx->h_ctl, sizeof(SolveCtl)));
+  PF_CUDA_TRY(cudaMalloc(&ctx->ctl_outer, sizeof(SolveCtl)));
+  PF_CUDA_TRY(cudaMemset(ctx->ctl_outer, 0, sizeof(SolveCtl)));
   PF_CUDA_TRY(cudaMallocHost(&ctx->h_pinned_ints, 64 * sizeof(int)));
   PF_CUDA_TRY(cudaMalloc(&ctx->d_clamp, 8 * sizeof(int)));
   PF_CUDA_TRY(cudaMalloc(&ctx->d_flags, 2 * cap * sizeof(int)));

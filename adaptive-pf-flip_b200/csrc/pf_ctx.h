@@ -82,6 +82,7 @@ struct pf_ctx {
   uint8_t* kind = nullptr;     // per cell: 0 not an unknown, 1 fluid, 2 pinned
   pf::SolveCtl* ctl = nullptr;
   pf::SolveCtl* h_ctl = nullptr;  // pinned mirror
+  pf::SolveCtl* ctl_outer = nullptr;  // outer iteration of the inner-outer solves
   // mixed precision
   float *xf = nullptr, *rf = nullptr, *pf32 = nullptr, *Apf = nullptr;
   float *diagf = nullptr, *cxf = nullptr, *cyf = nullptr, *czf = nullptr;

@@ -297,47 +297,6 @@ __global__ void __launch_bounds__(PF_TV) k_fx_dir(const int* slot_tile, int nslo
   }
 }
 
-// x += sign * e
-__global__ void k_fx_add(int nslots, const uint8_t* kind, double* x, const float* e, double sign) {
-  for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
-    const size_t o = (size_t)s * PF_TV + threadIdx.x;
-    if (kind[o]) x[o] += sign * (double)e[o];
-  }
-}
-
-// r = b - A x with the exact FP64 operator; max|r| -> ctl->res
-__global__ void __launch_bounds__(PF_TV) k_fx_residual(const int* __restrict__ nbr, int nslots, SolveCtl* ctl,
-                                                       const uint8_t* kind, const double* x, const double* diag,
-                                                       const double* cx, const double* cy, const double* cz,
-                                                       const double* b, double scale, double* r, double* partials) {
-  double rmax = 0.0;
-  for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
-    const int l = threadIdx.x;
-    const size_t o = (size_t)s * PF_TV + l;
-    const uint8_t kd = kind[o];
-    if (!kd) continue;
-    double ax;
-    if (kd == 2) {
-      ax = x[o];
-    } else {
-      long long no[6];
-      neighbor_offsets_tab(nbr, s, l, no);
-      double off = 0.0;
-      if (no[0] >= 0) off += cx[no[0]] * x[no[0]];
-      if (no[1] >= 0) off += cx[o] * x[no[1]];
-      if (no[2] >= 0) off += cy[no[2]] * x[no[2]];
-      if (no[3] >= 0) off += cy[o] * x[no[3]];
-      if (no[4] >= 0) off += cz[no[4]] * x[no[4]];
-      if (no[5] >= 0) off += cz[o] * x[no[5]];
-      ax = scale * (diag[o] * x[o] - off);
-    }
-    const double rr = b[o] - ax;
-    r[o] = rr;
-    rmax = fmax(rmax, fabs(rr));
-  }
-  block_reduce_2(0.0, rmax, partials, ctl, kStageResid);
-}
-
 int poll_ctl(pf_ctx* ctx, SolveCtl* out) {
   PF_CUDA_TRY(cudaMemcpyAsync(ctx->h_ctl, ctx->ctl, sizeof(SolveCtl), cudaMemcpyDeviceToHost, ctx->stream));
   PF_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
@@ -444,10 +403,12 @@ int capture_iteration(pf_ctx* ctx, int nslots, int nred, const uint8_t* kind, co
 }
 
 // Flexible PCG from x = 0 on r_init until max|r| < max(tol_abs, tol_rel max|r0|).
+// `keep`, when given, holds the captured iteration body across calls with
+// the same vectors (the inner solves of one inner-outer solve).
 template <typename V>
 int flex_solve(pf_ctx* ctx, int nslots, int nred, const uint8_t* kind, FlexVec<V> m, const double* r_init,
                double tol_abs, double tol_rel, int max_iter, int check_every, int precond, double min_gain,
-               int reset_guard, SolveCtl* out) {
+               int reset_guard, SolveCtl* out, IterGraph* keep = nullptr) {
   CoarseOp& A = ((CoarseCtx*)ctx->learned)->op;
   const bool coarse = precond != PF_PRECOND_JACOBI;
   (++ctx->launches), k_fx_set<<<1, 1, 0, ctx->stream>>>(ctx->ctl, tol_abs, tol_rel, max_iter, coarse ? 1.0 : 0.0,
@@ -464,8 +425,9 @@ int flex_solve(pf_ctx* ctx, int nslots, int nred, const uint8_t* kind, FlexVec<V
   PF_CUDA_TRY(cudaGetLastError());
   // the exact coarse solve records training pairs on the host side, so it is
   // launched directly; the other bodies are replayed from a graph
-  IterGraph graph;
-  if (precond != PF_PRECOND_EXACT_COARSE) {
+  IterGraph local;
+  IterGraph& graph = keep ? *keep : local;
+  if (precond != PF_PRECOND_EXACT_COARSE && !graph.exec) {
     rc = capture_iteration<V>(ctx, nslots, nred, kind, m, precond, min_gain, &graph);
     if (rc) return rc;
   }
@@ -493,6 +455,29 @@ int flex_solve(pf_ctx* ctx, int nslots, int nred, const uint8_t* kind, FlexVec<V
   *out = c;
   return PF_OK;
 }
+
+// The inner solver of LEARNED with FP32 vectors: the flexible PCG with the
+// two-level preconditioner on the FP32 copy of the operator, from e = 0.
+struct LearnedInner final : InnerSolver {
+  int nslots = 0, nred = 0, check_every = 0, precond = 0;
+  const uint8_t* kind = nullptr;
+  double min_gain = 0.0;
+  FlexVec<float> m{};
+  IterGraph graph;
+  int accepted = 0, rejected = 0;
+  int solve(pf_ctx* ctx, double eta, int max_iter, bool first, const float** z, int* iters) override {
+    SolveCtl ic{};
+    const int poll_at = check_every > 0 ? check_every : std::max(1, max_iter / 2);
+    const int rc = flex_solve<float>(ctx, nslots, nred, kind, m, ctx->r, 0.0, eta, max_iter, poll_at, precond,
+                                     min_gain, first ? 1 : 0, &ic, &graph);
+    if (rc) return rc;
+    *iters = ic.it;
+    *z = m.e;
+    accepted = ic.accepted;
+    rejected = ic.rejected;
+    return ic.done == 4 ? set_error(ctx, PF_ERR_NONFINITE, "non-finite value in the inner solve") : PF_OK;
+  }
+};
 
 }  // namespace
 
@@ -549,67 +534,27 @@ int solve_learned(pf_ctx* ctx, int nslots, int nred, const uint8_t* kind, double
     return PF_OK;
   }
 
-  // FP32 flexible PCG inside FP64 iterative refinement
+  // FP64 flexible CG preconditioned by the learned flexible PCG in FP32
   rc = ensure_solver_buffers(ctx, PF_SOLVER_MIXED);
   if (rc) return rc;
   (++ctx->launches), k_fx_setup32<<<nred, PF_TV, 0, ctx->stream>>>(nslots, kind, ctx->diag, ctx->cx, ctx->cy, ctx->cz,
                                                                     ctx->r, scale, ctx->diagf, ctx->cxf, ctx->cyf,
                                                                     ctx->czf, ctx->b64);
   PF_CUDA_TRY(cudaGetLastError());
-  FlexVec<float> m{ctx->xf, ctx->rf, ctx->Apf, ctx->pf32, ctx->diagf, ctx->cxf, ctx->cyf, ctx->czf, cls, 1.0f};
-  const double tol = c.tol;
-  double resid = c.res0;
-  int iters = 0, sweeps = 0;
-  // Short sweeps: FP32 recurrences stagnate (and can overflow) long before a
-  // deep inner reduction at 1000:1, so each sweep stops after a modest
-  // reduction or kSweepIters iterations and the FP64 residual restarts it.
-  constexpr int kSweepIters = 1000;
-  const int max_sweeps = cfg->max_refine > 0 ? cfg->max_refine : 64;
-  const double inner_rel = cfg->inner_rel_tol > 0.0 ? cfg->inner_rel_tol : 1e-3;
-  bool converged = false, nonfinite = false;
-  while (!converged && sweeps < max_sweeps && iters < cfg->max_iter) {
-    SolveCtl ic{};
-    rc = flex_solve<float>(ctx, nslots, nred, kind, m, ctx->r, 0.0, inner_rel,
-                           std::min(kSweepIters, cfg->max_iter - iters), cfg->check_every, precond,
-                           cfg->accept_min_gain, sweeps == 0, &ic);
-    if (rc) return rc;
-    ++sweeps;
-    iters += ic.it;
-    res->precond_applied = ic.accepted;
-    res->precond_rejected = ic.rejected;
-    (++ctx->launches), k_fx_add<<<nred, PF_TV, 0, ctx->stream>>>(nslots, kind, ctx->x, m.e, 1.0);
-    (++ctx->launches), k_fx_residual<<<nred, PF_TV, 0, ctx->stream>>>(nbr, nslots, ctx->ctl, kind, ctx->x, ctx->diag,
-                                                                      ctx->cx, ctx->cy, ctx->cz, ctx->b64, scale,
-                                                                      ctx->r, ctx->partials);
-    PF_CUDA_TRY(cudaGetLastError());
-    rc = poll_ctl(ctx, &c);
-    if (rc) return rc;
-    if (!(c.res < resid) && ic.done != 4) {
-      // the sweep made the FP64 residual worse: take it back and stop with the best solution so far
-      (++ctx->launches), k_fx_add<<<nred, PF_TV, 0, ctx->stream>>>(nslots, kind, ctx->x, m.e, -1.0);
-      (++ctx->launches), k_fx_residual<<<nred, PF_TV, 0, ctx->stream>>>(nbr, nslots, ctx->ctl, kind, ctx->x,
-                                                                        ctx->diag, ctx->cx, ctx->cy, ctx->cz,
-                                                                        ctx->b64, scale, ctx->r, ctx->partials);
-      PF_CUDA_TRY(cudaGetLastError());
-      rc = poll_ctl(ctx, &c);
-      if (rc) return rc;
-      resid = c.res;
-      break;
-    }
-    resid = c.res;
-    if (!std::isfinite(resid) || ic.done == 4) {
-      nonfinite = true;
-      break;
-    }
-    converged = resid < tol;
-    if (ic.it == 0) break;
-  }
-  res->iterations = iters;
-  res->refinements = sweeps;
-  res->res_final = resid;
-  res->converged = converged ? 1 : 0;
-  res->nonfinite = nonfinite ? 1 : 0;
-  return PF_OK;
+  LearnedInner inner;
+  inner.nslots = nslots;
+  inner.nred = nred;
+  inner.kind = kind;
+  inner.check_every = cfg->check_every;
+  inner.precond = precond;
+  inner.min_gain = cfg->accept_min_gain;
+  inner.m = FlexVec<float>{ctx->xf, ctx->rf, ctx->Apf, ctx->pf32, ctx->diagf, ctx->cxf, ctx->cyf, ctx->czf, cls, 1.0f};
+  const double eta = cfg->inner_rel_tol > 0.0 ? cfg->inner_rel_tol : 1e-3;
+  const int inner_max = cfg->inner_max_iter > 0 ? cfg->inner_max_iter : 200;
+  rc = solve_inner_outer(ctx, nslots, nred, kind, nbr, scale, cfg, inner, eta, inner_max, res);
+  res->precond_applied = inner.accepted;
+  res->precond_rejected = inner.rejected;
+  return rc;
 }
 
 }  // namespace pf

@@ -11,11 +11,14 @@
 // reduction scratch) in one file-scope __device__ array of fixed size, so it
 // calls no allocator at all.
 //
-// It runs the same kernels as pf_project in PLAIN mode (the launchers in
-// pf_project.cu and pf_pcg.cu), on a pool in which every tile is active.
+// It runs pf_project's PLAIN set-up, Jacobi-PCG recurrences and velocity
+// update (the launchers in pf_project.cu and pf_pcg.cu) on a pool in which
+// every tile is active.  Its SpMV finds cross-tile neighbours through the tile
+// map in shared memory (k_spmv_plain); pf_project's PLAIN solve reads them
+// from a per-solve neighbour-slot table (k_spmv_plain_tab), which would need
+// memory this entry point does not have.  Both give the same rows.
 #include <cmath>
 #include <cstring>
-#include <mutex>
 
 #include "pf_ctx.h"
 #include "pf_solver.cuh"
@@ -56,22 +59,17 @@ constexpr size_t kScratchBytes = align256(kOffCtl + sizeof(SolveCtl));
 // The scratch array: every GPU that loads the library holds it until exit.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
-// Device address of g_noalloc_scratch, looked up once per device with that
-// device current (the host-side name is not a device address).
-constexpr int kMaxDevices = 64;
-unsigned char* g_base[kMaxDevices] = {};
-std::mutex g_base_mutex;
-
-int scratch_base(int device, unsigned char** out) {
-  if (device < 0 || device >= kMaxDevices) return PF_ERR_INVALID;
-  std::lock_guard<std::mutex> lock(g_base_mutex);
-  if (!g_base[device]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p) return PF_ERR_CUDA;
-    g_base[device] = (unsigned char*)p;
-  }
-  *out = g_base[device];
+// Device address of g_noalloc_scratch in the context current on the calling
+// thread (the host-side name is not a device address).  It is looked up on
+// every call, not cached: the address belongs to a context, and between two
+// calls the caller may have reset the device or made another context of its
+// own current.  Once the library's module is loaded in that context the
+// lookup allocates nothing.
+int scratch_base(unsigned char** out) {
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p) return PF_ERR_CUDA;
+  *out = (unsigned char*)p;
   return PF_OK;
 }
 
@@ -145,10 +143,8 @@ extern "C" int pf_project_noalloc(int nx, int ny, int nz, double dx, const float
     return PF_ERR_INVALID;
   const Geom g = make_geom(nx, ny, nz, dx);
   if (g.ntiles > kMaxTiles) return PF_ERR_INVALID;  // beyond the fixed scratch capacity
-  int device = 0;
-  if (cudaGetDevice(&device) != cudaSuccess) return PF_ERR_CUDA;
   unsigned char* base = nullptr;
-  int rc = scratch_base(device, &base);
+  int rc = scratch_base(&base);
   if (rc) return rc;
   cudaStream_t s = (cudaStream_t)stream;
 

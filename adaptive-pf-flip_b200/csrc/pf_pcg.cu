@@ -155,19 +155,19 @@ __device__ __forceinline__ void stc(__nv_bfloat16* a, long long i, float v) { a[
 __device__ __forceinline__ float rnd(float v, const float*) { return v; }
 __device__ __forceinline__ float rnd(float v, const __nv_bfloat16*) { return __bfloat162float(__float2bfloat16_rn(v)); }
 
-template <typename C>
+template <typename CC, typename CP>
 struct MixVec {
   float *e, *r, *Ap, *d;  // correction, inner residual, A'p, diagonal of A'
-  C* p;                   // search direction (FP32 or BF16)
-  C *cx, *cy, *cz;        // scaled low-face couplings (FP32 or BF16)
+  CP* p;                  // search direction (FP32 or BF16)
+  CC *cx, *cy, *cz;       // scaled low-face couplings (FP32 or BF16)
 };
 
 // Inner operator A': couplings w = round(scale*beta), diagonal = sum of the
 // rounded weights of all non-solid faces (air faces keep their exact-scaled
 // weight rounded the same way).
-template <typename C>
+template <typename CC, typename CP>
 __global__ void __launch_bounds__(PF_TV) k_mixed_setup(DevGrid G, int nslots, const uint8_t* kind, PcgVec<double> v,
-                                                       MixVec<C> m, double scale) {
+                                                       MixVec<CC, CP> m, double scale) {
   __shared__ int nbs[6];
   for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
     __syncthreads();
@@ -203,9 +203,9 @@ __global__ void __launch_bounds__(PF_TV) k_mixed_setup(DevGrid G, int nslots, co
 }
 
 // start an inner solve: r' = r64 (FP32), e = 0, p = z = r'/d'; r.z, max|r'|
-template <typename C>
+template <typename CC, typename CP>
 __global__ void __launch_bounds__(PF_TV) k_mixed_start(int nslots, SolveCtl* ctl, const uint8_t* kind,
-                                                       const double* r64, MixVec<C> m, double* partials) {
+                                                       const double* r64, MixVec<CC, CP> m, double* partials) {
   double rz = 0.0, rmax = 0.0;
   for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
     const size_t o = (size_t)s * PF_TV + threadIdx.x;
@@ -225,9 +225,9 @@ __global__ void __launch_bounds__(PF_TV) k_mixed_start(int nslots, SolveCtl* ctl
   block_reduce_2(rz, rmax, partials, ctl, kStageInit);
 }
 
-template <typename C>
+template <typename CC, typename CP>
 __global__ void __launch_bounds__(PF_TV) k_mixed_spmv(DevGrid G, int nslots, SolveCtl* ctl, const uint8_t* kind,
-                                                      MixVec<C> m, double* partials) {
+                                                      MixVec<CC, CP> m, double* partials) {
   if (ctl->done) return;
   __shared__ int nbs[6];
   double acc = 0.0;
@@ -261,8 +261,8 @@ __global__ void __launch_bounds__(PF_TV) k_mixed_spmv(DevGrid G, int nslots, Sol
   block_reduce_2(acc, 0.0, partials, ctl, kStagePAp);
 }
 
-template <typename C>
-__global__ void __launch_bounds__(PF_TV) k_mixed_update(int nslots, SolveCtl* ctl, const uint8_t* kind, MixVec<C> m,
+template <typename CC, typename CP>
+__global__ void __launch_bounds__(PF_TV) k_mixed_update(int nslots, SolveCtl* ctl, const uint8_t* kind, MixVec<CC, CP> m,
                                                         double* partials) {
   if (ctl->done) return;
   const float alpha = (float)ctl->alpha;
@@ -282,9 +282,9 @@ __global__ void __launch_bounds__(PF_TV) k_mixed_update(int nslots, SolveCtl* ct
   block_reduce_2(rz, rmax, partials, ctl, kStageUpdate);
 }
 
-template <typename C>
+template <typename CC, typename CP>
 __global__ void __launch_bounds__(PF_TV) k_mixed_direction(int nslots, const SolveCtl* ctl, const uint8_t* kind,
-                                                           MixVec<C> m) {
+                                                           MixVec<CC, CP> m) {
   if (ctl->done) return;
   const float beta = (float)ctl->beta;
   for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
@@ -293,59 +293,6 @@ __global__ void __launch_bounds__(PF_TV) k_mixed_direction(int nslots, const Sol
     const float d = m.d[o];
     const float z = d > 0.0f ? m.r[o] / d : 0.0f;
     stc(m.p, o, z + beta * ldc(m.p, o));
-  }
-}
-
-// r64 = b - A x with the exact FP64 operator; max|r64|.  x already holds
-// the sweep's correction (k_add_correction, a separate launch: folding it in
-// here would race with the neighbour reads of x).
-__global__ void __launch_bounds__(PF_TV) k_refine_residual(DevGrid G, int nslots, SolveCtl* ctl, const uint8_t* kind,
-                                                           PcgVec<double> v, const double* b, double scale,
-                                                           double* partials) {
-  __shared__ int nbs[6];
-  double rmax = 0.0;
-  for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
-    __syncthreads();
-    neighbor_slots(G, s, nbs);
-    __syncthreads();
-    const int l = threadIdx.x;
-    const size_t o = (size_t)s * PF_TV + l;
-    const uint8_t kd = kind[o];
-    if (!kd) continue;
-    const double x0 = v.x[o];
-    double ax;
-    if (kd == 2) {
-      ax = x0;
-    } else {
-      long long no[6];
-      neighbor_offsets(s, l, nbs, no);
-      const double c[6] = {no[0] >= 0 ? v.cx[no[0]] : 0.0, v.cx[o], no[2] >= 0 ? v.cy[no[2]] : 0.0, v.cy[o],
-                           no[4] >= 0 ? v.cz[no[4]] : 0.0, v.cz[o]};
-      double off = 0.0;
-#pragma unroll
-      for (int d = 0; d < 6; ++d)
-        if (c[d] != 0.0 && no[d] >= 0) off += c[d] * v.x[no[d]];
-      ax = scale * (v.diag[o] * x0 - off);
-    }
-    const double r = b[o] - ax;
-    v.r[o] = r;
-    rmax = fmax(rmax, fabs(r));
-  }
-  block_reduce_2(0.0, rmax, partials, ctl, kStageResid);
-}
-
-// x += sign * e
-__global__ void k_add_correction(int nslots, const uint8_t* kind, double* x, const float* e, double sign) {
-  for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
-    const size_t o = (size_t)s * PF_TV + threadIdx.x;
-    if (kind[o]) x[o] += sign * (double)e[o];
-  }
-}
-
-__global__ void k_copy_rhs(int nslots, const double* r, double* b) {
-  for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
-    const size_t o = (size_t)s * PF_TV + threadIdx.x;
-    b[o] = r[o];
   }
 }
 
@@ -420,12 +367,12 @@ int ensure_solver_buffers(pf_ctx* ctx, int mode) {
   return PF_OK;
 }
 
-template <typename C>
-static int mixed_inner(pf_ctx* ctx, int nslots, int nred, const uint8_t* kind, MixVec<C> m, double tol_abs,
+template <typename CC, typename CP>
+static int mixed_inner(pf_ctx* ctx, int nslots, int nred, const uint8_t* kind, MixVec<CC, CP> m, double tol_abs,
                        double tol_rel, int max_iter, int check_every, int* iters, SolveCtl* out) {
   DevGrid G = dev_grid(ctx);
   (++ctx->launches), k_set_inner<<<1, 1, 0, ctx->stream>>>(ctx->ctl, tol_abs, tol_rel, max_iter);
-  (++ctx->launches), k_mixed_start<C><<<nred, PF_TV, 0, ctx->stream>>>(nslots, ctx->ctl, kind, ctx->r, m, ctx->partials);
+  (++ctx->launches), k_mixed_start<CC, CP><<<nred, PF_TV, 0, ctx->stream>>>(nslots, ctx->ctl, kind, ctx->r, m, ctx->partials);
   PF_CUDA_TRY(cudaGetLastError());
   SolveCtl c{};
   int rc = poll(ctx, &c);
@@ -435,9 +382,9 @@ static int mixed_inner(pf_ctx* ctx, int nslots, int nred, const uint8_t* kind, M
   while (!c.done && launched < max_iter) {
     const int nb = std::min(batch, max_iter - launched);
     for (int q = 0; q < nb; ++q) {
-      (++ctx->launches), k_mixed_spmv<C><<<nred, PF_TV, 0, ctx->stream>>>(G, nslots, ctx->ctl, kind, m, ctx->partials);
-      (++ctx->launches), k_mixed_update<C><<<nred, PF_TV, 0, ctx->stream>>>(nslots, ctx->ctl, kind, m, ctx->partials);
-      (++ctx->launches), k_mixed_direction<C><<<nred, PF_TV, 0, ctx->stream>>>(nslots, ctx->ctl, kind, m);
+      (++ctx->launches), k_mixed_spmv<CC, CP><<<nred, PF_TV, 0, ctx->stream>>>(G, nslots, ctx->ctl, kind, m, ctx->partials);
+      (++ctx->launches), k_mixed_update<CC, CP><<<nred, PF_TV, 0, ctx->stream>>>(nslots, ctx->ctl, kind, m, ctx->partials);
+      (++ctx->launches), k_mixed_direction<CC, CP><<<nred, PF_TV, 0, ctx->stream>>>(nslots, ctx->ctl, kind, m);
     }
     PF_CUDA_TRY(cudaGetLastError());
     launched += nb;
@@ -450,62 +397,46 @@ static int mixed_inner(pf_ctx* ctx, int nslots, int nred, const uint8_t* kind, M
   return PF_OK;
 }
 
-template <typename C>
+// The inner solver of MIXED: Jacobi-PCG on A' with FP32 vectors (and FP32 or
+// BF16 couplings and direction), FP64 inner products, from e = 0.
+template <typename CC, typename CP>
+struct MixedInner final : InnerSolver {
+  int nslots = 0, nred = 0, check_every = 0;
+  const uint8_t* kind = nullptr;
+  MixVec<CC, CP> m{};
+  int solve(pf_ctx* ctx, double eta, int max_iter, bool, const float** z, int* iters) override {
+    SolveCtl ic{};
+    // one poll in the middle of the budget, one at its end
+    const int poll_at = check_every > 0 ? check_every : std::max(1, max_iter / 2);
+    int before = 0;
+    const int rc = mixed_inner<CC, CP>(ctx, nslots, nred, kind, m, 0.0, eta, max_iter, poll_at, &before, &ic);
+    if (rc) return rc;
+    *iters = ic.it;
+    *z = m.e;
+    return ic.done == 4 ? set_error(ctx, PF_ERR_NONFINITE, "non-finite value in the inner solve") : PF_OK;
+  }
+};
+
+// MIXED: FP64 flexible CG on the exact operator (pf_outer.cu), preconditioned
+// by the inner Jacobi-PCG on A' in reduced precision.
+template <typename CC, typename CP>
 static int solve_mixed_t(pf_ctx* ctx, int nslots, int nred, const uint8_t* kind, double scale,
-                         const pf_solve_cfg* cfg, MixVec<C> m, SolveResult* res) {
+                         const pf_solve_cfg* cfg, MixVec<CC, CP> m, SolveResult* res) {
   DevGrid G = dev_grid(ctx);
   PcgVec<double> v{ctx->x, ctx->r, ctx->p, ctx->Ap, ctx->diag, ctx->cx, ctx->cy, ctx->cz};
-  (++ctx->launches), k_mixed_setup<C><<<nred, PF_TV, 0, ctx->stream>>>(G, nslots, kind, v, m, scale);
-  (++ctx->launches), k_copy_rhs<<<nred, PF_TV, 0, ctx->stream>>>(nslots, ctx->r, ctx->b64);
+  (++ctx->launches), k_mixed_setup<CC, CP><<<nred, PF_TV, 0, ctx->stream>>>(G, nslots, kind, v, m, scale);
+  if (nslots > 0)
+    (++ctx->launches), k_plain_nbr<<<nblocks((size_t)6 * nslots, 256), 256, 0, ctx->stream>>>(G, nslots, ctx->nbr_plain);
   PF_CUDA_TRY(cudaGetLastError());
-  SolveCtl c{};
-  int rc = poll(ctx, &c);  // assembly finished: res0 / tol / done from the init stage
-  if (rc) return rc;
-  const double res0 = c.res0;
-  const double tol = c.tol;
-  res->res0 = res0;
-  res->tol = tol;
-  double resid = res0;
-  int iters = 0, sweeps = 0;
-  const int max_sweeps = cfg->max_refine > 0 ? cfg->max_refine : 8;
-  const double inner_rel = cfg->inner_rel_tol > 0.0 ? cfg->inner_rel_tol : 1e-4;
-  bool converged = !(res0 >= tol);
-  bool nonfinite = c.done == 4;
-  while (!converged && !nonfinite && sweeps < max_sweeps && iters < cfg->max_iter) {
-    SolveCtl ic{};
-    rc = mixed_inner<C>(ctx, nslots, nred, kind, m, 0.0, inner_rel, cfg->max_iter - iters, cfg->check_every,
-                        &iters, &ic);
-    if (rc) return rc;
-    ++sweeps;
-    (++ctx->launches), k_add_correction<<<nred, PF_TV, 0, ctx->stream>>>(nslots, kind, ctx->x, m.e, 1.0);
-    (++ctx->launches), k_refine_residual<<<nred, PF_TV, 0, ctx->stream>>>(G, nslots, ctx->ctl, kind, v, ctx->b64, scale,
-                                                                          ctx->partials);
-    PF_CUDA_TRY(cudaGetLastError());
-    rc = poll(ctx, &c);
-    if (rc) return rc;
-    if (!(c.res < resid) && ic.done != 4) {
-      // the sweep made the FP64 residual worse (FP32 recurrences past their
-      // accuracy): take it back and stop with the best solution so far
-      (++ctx->launches), k_add_correction<<<nred, PF_TV, 0, ctx->stream>>>(nslots, kind, ctx->x, m.e, -1.0);
-      (++ctx->launches), k_refine_residual<<<nred, PF_TV, 0, ctx->stream>>>(G, nslots, ctx->ctl, kind, v, ctx->b64,
-                                                                            scale, ctx->partials);
-      PF_CUDA_TRY(cudaGetLastError());
-      rc = poll(ctx, &c);
-      if (rc) return rc;
-      resid = c.res;
-      break;
-    }
-    resid = c.res;
-    if (!std::isfinite(resid) || ic.done == 4) { nonfinite = true; break; }
-    converged = resid < tol;
-    if (ic.done == 2 && !converged && ic.it == 0) break;  // inner breakdown without progress
-  }
-  res->iterations = iters;
-  res->refinements = sweeps;
-  res->res_final = resid;
-  res->converged = converged ? 1 : 0;
-  res->nonfinite = nonfinite ? 1 : 0;
-  return PF_OK;
+  MixedInner<CC, CP> inner;
+  inner.nslots = nslots;
+  inner.nred = nred;
+  inner.kind = kind;
+  inner.m = m;
+  inner.check_every = cfg->check_every;
+  const double eta = cfg->inner_rel_tol > 0.0 ? cfg->inner_rel_tol : 1e-3;
+  const int inner_max = cfg->inner_max_iter > 0 ? cfg->inner_max_iter : 200;
+  return solve_inner_outer(ctx, nslots, nred, kind, ctx->nbr_plain, scale, cfg, inner, eta, inner_max, res);
 }
 
 int solve_mixed(pf_ctx* ctx, int nslots, int nred, const uint8_t* kind, double scale, const pf_solve_cfg* cfg,
@@ -514,13 +445,19 @@ int solve_mixed(pf_ctx* ctx, int nslots, int nred, const uint8_t* kind, double s
   int rc = ensure_solver_buffers(ctx, cfg->mode);
   if (rc) return rc;
   // FP64 assembly first: exact operator, rhs, tolerance (shared with PLAIN)
-  if (cfg->bf16_storage) {
-    MixVec<__nv_bfloat16> m{ctx->xf, ctx->rf, ctx->Apf, ctx->diagf, (__nv_bfloat16*)ctx->pbf,
-                            (__nv_bfloat16*)ctx->cbf, (__nv_bfloat16*)ctx->cbf + ctx->cells_cap,
-                            (__nv_bfloat16*)ctx->cbf + 2 * ctx->cells_cap};
+  typedef __nv_bfloat16 bf16;
+  bf16* cb = (bf16*)ctx->cbf;
+  if (cfg->bf16_storage >= 2) {  // BF16 couplings and search direction
+    MixVec<bf16, bf16> m{ctx->xf, ctx->rf, ctx->Apf, ctx->diagf, (bf16*)ctx->pbf, cb, cb + ctx->cells_cap,
+                         cb + 2 * ctx->cells_cap};
     return solve_mixed_t(ctx, nslots, nred, kind, scale, cfg, m, res);
   }
-  MixVec<float> m{ctx->xf, ctx->rf, ctx->Apf, ctx->diagf, ctx->pf32, ctx->cxf, ctx->cyf, ctx->czf};
+  if (cfg->bf16_storage == 1) {  // BF16 couplings, FP32 search direction
+    MixVec<bf16, float> m{ctx->xf, ctx->rf, ctx->Apf, ctx->diagf, ctx->pf32, cb, cb + ctx->cells_cap,
+                          cb + 2 * ctx->cells_cap};
+    return solve_mixed_t(ctx, nslots, nred, kind, scale, cfg, m, res);
+  }
+  MixVec<float, float> m{ctx->xf, ctx->rf, ctx->Apf, ctx->diagf, ctx->pf32, ctx->cxf, ctx->cyf, ctx->czf};
   return solve_mixed_t(ctx, nslots, nred, kind, scale, cfg, m, res);
 }
 

@@ -29,6 +29,9 @@ enum RedStage {
   kStageUpdate = 2,  // after x/r update: r.z, max|r| -> convergence, beta
   kStageResid = 3,   // outer refinement: max|b - A x| (FP64)
   kStageFlex = 4,    // flexible PCG x/r update: max|r| -> convergence; r.D^-1 r, r.z_prev kept for the guard
+  kStageOuterBeta = 5,    // inner-outer FCG(1): z.q_prev -> beta (0 on the first outer iteration)
+  kStageOuterPAp = 6,     // inner-outer FCG(1): p.q, r.p -> alpha (breakdown check)
+  kStageOuterUpdate = 7,  // inner-outer FCG(1): max|r| -> convergence
 };
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -98,6 +101,27 @@ __device__ __forceinline__ void finalize_stage(SolveCtl* ctl, int stage, double 
     case kStageResid: {
       ctl->res = M;
       if (!isfinite(M)) ctl->done = 4;
+      break;
+    }
+    case kStageOuterBeta: {
+      double b = ctl->it > 0 && ctl->pAp != 0.0 ? S / ctl->pAp : 0.0;
+      if (!isfinite(b)) b = 0.0;
+      ctl->beta = b;
+      break;
+    }
+    case kStageOuterPAp: {
+      ctl->pAp = S;
+      if (!isfinite(S) || !isfinite(S2)) ctl->done = 4;
+      else if (!(S > 0.0) || !isfinite(S2 / S)) ctl->done = 2;
+      else ctl->alpha = S2 / S;
+      break;
+    }
+    case kStageOuterUpdate: {
+      ctl->it += 1;
+      ctl->res = M;
+      if (!isfinite(M)) ctl->done = 4;
+      else if (M < ctl->tol) ctl->done = 1;
+      else if (ctl->it >= ctl->max_iter) ctl->done = 3;
       break;
     }
     case kStageFlex: {
@@ -200,6 +224,22 @@ __device__ __forceinline__ void neighbor_offsets_tab(const int* __restrict__ nbr
 
 // nbr[6 s + d] for every pooled slot (pf_flex.cu)
 int build_neighbor_table(pf_ctx* ctx, int nslots, int** nbr);
+
+// A truncated inner solve in reduced precision, the preconditioner of the
+// inner-outer solver: from z = 0 it reduces the FP64 residual ctx->r by the
+// factor eta (max-norm) or stops after max_iter iterations, and returns z in
+// FP32 pool layout (zero off the unknowns) and its iteration count.  `first`
+// marks the first inner solve of an outer solve.
+struct InnerSolver {
+  virtual int solve(pf_ctx* ctx, double eta, int max_iter, bool first, const float** z, int* iters) = 0;
+  virtual ~InnerSolver() = default;
+};
+
+// FP64 flexible CG with one stored direction on the exact operator, each
+// outer iteration preconditioned by inner.solve (pf_outer.cu).  Reports the
+// inner iterations in res->iterations and the outer ones in res->refinements.
+int solve_inner_outer(pf_ctx* ctx, int nslots, int nred, const uint8_t* kind, const int* nbr, double scale,
+                      const pf_solve_cfg* cfg, InnerSolver& inner, double eta, int inner_max, SolveResult* res);
 
 // solver drivers (pf_pcg.cu)
 int pcg_plain(pf_ctx* ctx, int nslots, int nred, const uint8_t* kind, PcgVec<double> vec, double scale,

@@ -132,19 +132,20 @@ class SolverConfig:
     """Pressure solver selection beyond the reference's (cg_iters, cg_tol)."""
     mode: int = L.PF_SOLVER_PLAIN
     rel_tol: float = 0.0
-    bf16_storage: bool = False
+    bf16_storage: int = 0  # 1: BF16 couplings in the mixed inner solve; 2: also its search direction
     check_every: int = 0
     max_refine: int = 0
     inner_rel_tol: float = 0.0
     precond: int = L.PF_PRECOND_NETWORK
     accept_min_gain: float = 0.0
     inner_fp32: bool = False
+    inner_max_iter: int = 0
 
     def _c(self, cg_iters, cg_tol, c_div) -> L.SolveCfg:
         return L.SolveCfg(int(self.mode), int(cg_iters), float(cg_tol), float(self.rel_tol), float(c_div),
-                          int(bool(self.bf16_storage)), int(self.check_every), int(self.max_refine),
+                          int(self.bf16_storage), int(self.check_every), int(self.max_refine),
                           float(self.inner_rel_tol), int(self.precond), float(self.accept_min_gain),
-                          int(bool(self.inner_fp32)))
+                          int(bool(self.inner_fp32)), int(self.inner_max_iter))
 
 
 # ---------------------------------------------------------------------------

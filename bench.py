@@ -27,6 +27,7 @@ from __future__ import annotations
 
 import argparse
 import ctypes as C
+import dataclasses
 import importlib.util
 import json
 import os
@@ -297,17 +298,28 @@ def pcg_modes(pf, names):
     table = {
         "plain_fp64": pf.SolverConfig(mode=pf.PF_SOLVER_PLAIN, rel_tol=1e-6),
         "mixed_fp32": pf.SolverConfig(mode=pf.PF_SOLVER_MIXED, rel_tol=1e-6),
-        "mixed_bf16": pf.SolverConfig(mode=pf.PF_SOLVER_MIXED, rel_tol=1e-6, bf16_storage=True),
+        "mixed_bf16": pf.SolverConfig(mode=pf.PF_SOLVER_MIXED, rel_tol=1e-6, bf16_storage=1),
+        "mixed_bf16_dir": pf.SolverConfig(mode=pf.PF_SOLVER_MIXED, rel_tol=1e-6, bf16_storage=2),
         # the learned two-level preconditioner and its net-free ablation
         "learned": pf.SolverConfig(mode=L, rel_tol=1e-6, precond=pf.PF_PRECOND_NETWORK),
         "flex_jacobi": pf.SolverConfig(mode=L, rel_tol=1e-6, precond=pf.PF_PRECOND_JACOBI),
-        # the learned solver with FP32 inner flexible PCG inside FP64 refinement
-        "learned_fp32": pf.SolverConfig(mode=L, rel_tol=1e-6, precond=pf.PF_PRECOND_NETWORK, inner_fp32=True),
+        # FP64 flexible CG preconditioned by the learned flexible PCG in FP32
+        "learned_mixed": pf.SolverConfig(mode=L, rel_tol=1e-6, precond=pf.PF_PRECOND_NETWORK, inner_fp32=True),
         # the same two-level solver with an exact coarse solve: the bound a perfect network reaches
         "exact_coarse": pf.SolverConfig(mode=L, rel_tol=1e-6, precond=pf.PF_PRECOND_EXACT_COARSE),
     }
-    # "name#k" repeats a mode (a second solve on the same context: allocations done)
-    return [(name, table[name.split("#")[0]]) for name in names]
+    table["learned_fp32"] = table["learned_mixed"]
+    # "name#k" repeats a mode (a second solve on the same context: allocations done);
+    # "name@M:ETA" sets an inner-outer mode's inner cap and relative reduction
+    out = []
+    for name in names:
+        base = name.split("#")[0]
+        cfg = dataclasses.replace(table[base.split("@")[0]])
+        if "@" in base:
+            m, eta = base.split("@")[1].split(":")
+            cfg.inner_max_iter, cfg.inner_rel_tol = int(m), float(eta)
+        out.append((name, cfg))
+    return out
 
 
 def load_weights(pf, grid, path=None):

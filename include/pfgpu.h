@@ -75,7 +75,7 @@ typedef struct {
 
 /* pressure solver modes */
 #define PF_SOLVER_PLAIN 0   /* FP64 Jacobi-PCG, the reference-equivalent drop-in */
-#define PF_SOLVER_MIXED 1   /* FP32 SpMV/preconditioner, FP64 dots, iterative refinement */
+#define PF_SOLVER_MIXED 1   /* FP64 flexible CG preconditioned by FP32/BF16-storage Jacobi-PCG (FP64 dots) */
 #define PF_SOLVER_LEARNED 2 /* flexible PCG, Jacobi + learned two-level coarse correction */
 
 typedef struct {
@@ -84,13 +84,17 @@ typedef struct {
   double abs_tol;       /* reference cg_tol: stop when max|r| < tol */
   double rel_tol;       /* 0: reference rule; else tol = max(abs_tol, rel_tol*max|r0|) */
   double c_div;         /* divergenceCorrection */
-  int bf16_storage;     /* mixed/learned: store beta and search direction in BF16 */
+  int bf16_storage;     /* mixed: 1 store the inner solve's couplings (beta) in BF16; 2 also its search
+                           direction */
   int check_every;      /* host convergence poll interval in iterations (0 = default) */
-  int max_refine;       /* mixed/learned: outer refinement sweeps (0 = default) */
-  double inner_rel_tol; /* mixed/learned: inner solve relative reduction (0 = default) */
+  int max_refine;       /* unused (kept for the struct layout) */
+  double inner_rel_tol; /* mixed / learned FP32: an inner solve stops at max|r| <= inner_rel_tol max|r_0|
+                           (0 = default: 1e-3) */
   int precond;          /* learned: PF_PRECOND_* */
   double accept_min_gain; /* learned: keep the coarse term only if r.z >= (1+gain) r.D^-1 r */
-  int inner_fp32;       /* learned: 0 FP64 vectors; 1 FP32 vectors inside FP64 iterative refinement */
+  int inner_fp32;       /* learned: 0 FP64 flexible PCG; 1 FP64 flexible CG preconditioned by the learned
+                           flexible PCG in FP32 */
+  int inner_max_iter;   /* mixed / learned FP32: iteration cap of one inner solve (0 = default: 200) */
 } pf_solve_cfg;
 
 /* preconditioner of the LEARNED mode's flexible PCG */
@@ -100,7 +104,7 @@ typedef struct {
 
 typedef struct {
   int iterations;        /* total inner PCG iterations */
-  int refinements;       /* outer refinement sweeps (mixed/learned) */
+  int refinements;       /* mixed / learned FP32: outer FP64 iterations (iterations counts the inner ones) */
   int n_cells;           /* fluid cells (unknowns incl. the pin) */
   int converged;
   int breakdown;         /* |p.Ap| < 1e-30 or non-finite */
@@ -348,7 +352,9 @@ PFGPU_API int pf_get_timing(pf_ctx* ctx, pf_timing* out, int reset);
  * memory: hosts that reserve the whole device budget themselves and hand out
  * buffers from their own allocator (and plug-ins running inside such hosts),
  * or fixed-rate loops that must never wait on the driver's allocator.  It
- * does what pf_project does in PLAIN mode (same kernels, same results to
+ * does what pf_project does in PLAIN mode (the same set-up, Jacobi-PCG
+ * recurrences and velocity update; its SpMV looks cross-tile neighbours up
+ * through the tile map instead of a per-solve table; results agree to
  * rounding of the inner products) on dense device arrays the caller owns:
  * mk (nx,ny,nz) markers 0/1/2, face raw masses mu/mv/mw and face velocities
  * u/v/w on the field lattices of pf_grid_set_field (index i + X*(j + Y*k)),
@@ -357,11 +363,15 @@ PFGPU_API int pf_get_timing(pf_ctx* ctx, pf_timing* out, int reset);
  *
  * All working memory sits in one fixed __device__ array inside the library
  * (about 6.3 MB on every GPU that loads it, held until the process exits);
- * the call makes no cudaMalloc/cudaFree or other allocating call.  Limit:
+ * the call makes no cudaMalloc/cudaFree or other allocating call.  With CUDA's
+ * lazy module loading (the default) the first call in a context loads the
+ * library's module, which is when that array is allocated; later calls
+ * allocate nothing.  Limit:
  * ceil((nx+1)/8)*ceil((ny+1)/8)*ceil((nz+1)/8) <= PF_NOALLOC_MAX_TILES, e.g.
  * grids up to 39^3 cells; larger grids return PF_ERR_INVALID without running.
- * The first call on a device looks the array's device address up
- * (cudaGetSymbolAddress, with that device current); make that first call
+ * Every call looks the array's device address up in the current context
+ * (cudaGetSymbolAddress), so it stays valid after a device reset or when the
+ * caller makes a context of its own current; make the first call in a context
  * before any stream capture.  Every call uses the same array and leaves its
  * contents behind (each call re-initialises what it reads), so calls whose
  * work overlaps on the GPU -- on different streams, or from different host

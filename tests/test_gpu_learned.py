@@ -296,3 +296,30 @@ def test_shipped_weights_ablation_128(pf):
         assert st_n.iterations < 0.6 * st_j.iterations, (st_n.iterations, st_j.iterations)
     finally:
         g.close()
+
+
+@pytest.mark.parametrize("name", ["mixed_fp32", "mixed_bf16", "mixed_bf16_dir", "learned_mixed"])
+def test_inner_outer_solvers_reach_the_fp64_tolerance(pf, name):
+    """The reduced-precision solvers at 1000:1: FP64 flexible CG on the exact
+    operator, preconditioned by an inner solve in FP32 (Jacobi-PCG with FP32
+    or BF16 couplings and directions, or the learned flexible PCG).  Each
+    reaches the 1e-6 relative FP64 residual and the plain solution, where
+    FP32 iterative refinement stalls at this condition number."""
+    g, solve = _pressure_system(pf, 64, seed=0)
+    try:
+        cfg = {
+            "mixed_fp32": pf.SolverConfig(mode=pf.PF_SOLVER_MIXED, rel_tol=1e-6),
+            "mixed_bf16": pf.SolverConfig(mode=pf.PF_SOLVER_MIXED, rel_tol=1e-6, bf16_storage=1),
+            "mixed_bf16_dir": pf.SolverConfig(mode=pf.PF_SOLVER_MIXED, rel_tol=1e-6, bf16_storage=2),
+            "learned_mixed": pf.SolverConfig(mode=pf.PF_SOLVER_LEARNED, rel_tol=1e-6,
+                                             precond=pf.PF_PRECOND_NETWORK, inner_fp32=True),
+        }[name]
+        if name == "learned_mixed":
+            pf.LearnedCoarseSolver(g).load_default()
+        st_p, p_plain = solve(pf.SolverConfig(mode=pf.PF_SOLVER_PLAIN, rel_tol=1e-6))
+        st, p = solve(cfg, max_iter=60000)
+        assert st.converged and st.res_final <= 1e-6 * st.res0, (st.iterations, st.res_final / st.res0)
+        assert st.refinements > 0  # outer FP64 iterations
+        assert np.abs(p - p_plain).max() < 2e-4 * np.abs(p_plain).max()
+    finally:
+        g.close()
