@@ -26,7 +26,7 @@ Every compute call goes through libpfgpu.so (include/pfgpu.h); nothing here
 computes on the CPU except scalar phase-field helpers used on results.
 """
 from ._lib import (PF_MK, PF_MU, PF_MV, PF_MW, PF_P, PF_PRECOND_EXACT_COARSE, PF_PRECOND_JACOBI,
-                   PF_PRECOND_NETWORK, PF_SOLVER_LEARNED, PF_SOLVER_MIXED, PF_SOLVER_PLAIN, PF_U, PF_V, PF_W, PfError,
+                   PF_PRECOND_NETWORK, PF_SCENE_BUBBLE_TANK, PF_SCENE_RAYLEIGH_TAYLOR, PF_SOLVER_LEARNED, PF_SOLVER_MIXED, PF_SOLVER_PLAIN, PF_U, PF_V, PF_W, PfError,
                    load)
 from .learned import LearnedCoarseSolver
 from .sparse import (ParticleEscapeBuffer3D, ParticleEscapeStats3D, Particles3DTP, PhaseParams, SolverConfig,
@@ -39,7 +39,8 @@ from . import scenes
 __all__ = [
     "PF_U", "PF_V", "PF_W", "PF_MU", "PF_MV", "PF_MW", "PF_P", "PF_MK",
     "PF_SOLVER_PLAIN", "PF_SOLVER_MIXED", "PF_SOLVER_LEARNED", "PfError", "load",
-    "PF_PRECOND_NETWORK", "PF_PRECOND_EXACT_COARSE", "PF_PRECOND_JACOBI", "LearnedCoarseSolver",
+    "PF_PRECOND_NETWORK", "PF_PRECOND_EXACT_COARSE", "PF_PRECOND_JACOBI", "PF_SCENE_RAYLEIGH_TAYLOR",
+    "PF_SCENE_BUBBLE_TANK", "LearnedCoarseSolver",
     "PhaseParams", "Particles3DTP", "SparseMacGrid3D", "SparseSim3DTP", "SolverConfig",
     "ParticleEscapeStats3D", "ParticleEscapeBuffer3D",
     "spP2G3D_tp", "spProjectStepVC3D", "spG2P3D_tp", "spAdvect3D_tp", "calibrateRhoTilde0",

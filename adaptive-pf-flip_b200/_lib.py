@@ -23,6 +23,7 @@ ERR_NAMES = {PF_ERR_INVALID: "PF_ERR_INVALID", PF_ERR_CUDA: "PF_ERR_CUDA", PF_ER
 PF_U, PF_V, PF_W, PF_MU, PF_MV, PF_MW, PF_P, PF_MK = range(8)
 PF_SOLVER_PLAIN, PF_SOLVER_MIXED, PF_SOLVER_LEARNED = 0, 1, 2
 PF_PRECOND_NETWORK, PF_PRECOND_EXACT_COARSE, PF_PRECOND_JACOBI = 0, 1, 2
+PF_SCENE_RAYLEIGH_TAYLOR, PF_SCENE_BUBBLE_TANK = 0, 1
 
 # every entry point include/pfgpu.h declares
 EXPORTS = (
@@ -40,7 +41,7 @@ EXPORTS = (
     "pf_narrow_band_air", "pf_coarsen_particles", "pf_refill_liquid", "pf_set_adaptivity", "pf_get_adaptivity_stats",
     "pf_interface_diagnostics", "pf_get_interface_stats", "pf_set_step_controls", "pf_get_step_control_stats",
     "pf_surface_tension", "pf_set_surface_tension", "pf_get_surface_stats",
-    "pf_default_render_camera", "pf_write_render_cache",
+    "pf_default_render_camera", "pf_write_render_cache", "pf_seed_scene",
 )
 
 STAGES = ("bin", "sort", "splat", "normalize", "mark", "boundary", "project", "pcg", "g2p", "precond_setup",
@@ -233,6 +234,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "pf_advect": (i, [vp, d, i, P(ClampStats), vp, P(sz)]),
         "pf_step": (i, [vp, P(StepCfg), P(StepStats)]),
         "pf_calibrate_rho_tilde0": (i, [vp, P(Phase), d, P(d)]),
+        "pf_seed_scene": (i, [vp, i, C.c_ulonglong, P(sz)]),
         "pf_set_timing": (i, [vp, i]),
         "pf_get_timing": (i, [vp, P(Timing), i]),
         "pf_launch_count": (C.c_longlong, [vp]),

@@ -773,3 +773,9 @@ int pf_get_adaptivity_stats(const pf_ctx* ctx, pf_adapt_stats* out) {
 }
 
 }  // extern "C"
+
+namespace pf {
+// the pending asynchronous upload, swapped in before another producer of the
+// particle set (pf_seed_scene) overwrites it
+int take_upload_for(pf_ctx* ctx) { return take_upload(ctx); }
+}  // namespace pf

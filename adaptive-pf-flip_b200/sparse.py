@@ -520,6 +520,17 @@ class SparseSim3DTP:
         L.check(rc, self.grid.ctx, "pf_upload_particles")
         self.n = n
 
+    def seed_scene(self, scene, seed=0):
+        """Seed the resident particle set on the device with a benchmark scene
+        ("rayleigh_taylor" or "bubble_tank", pf_seed_scene): the particles
+        scenes.rayleigh_taylor / scenes.bubble_tank give for this grid and seed.
+        Returns the particle count."""
+        kind = {"rayleigh_taylor": L.PF_SCENE_RAYLEIGH_TAYLOR, "bubble_tank": L.PF_SCENE_BUBBLE_TANK}[scene]
+        n = C.c_size_t()
+        L.check(self.grid.lib.pf_seed_scene(self.grid.ctx, kind, int(seed), C.byref(n)), self.grid.ctx, "pf_seed_scene")
+        self.n = int(n.value)
+        return self.n
+
     def get_particles(self):
         n = self.n
         pos = np.empty((n, 3), np.float32)

@@ -64,6 +64,57 @@ P2G_BYTES_PER_PARTICLE = 29
 P2G_BYTES_PER_FACE = 8       # momentum->velocity + raw mass written once per active face node
 G2P_BYTES_PER_PARTICLE = 37  # read pos+vel+type, write vel
 G2P_BYTES_PER_FACE = 8       # current + saved face velocity read once
+# Algorithmic bytes per unknown and iteration of the pressure solvers: the
+# arrays each pass reads or writes once (FP64 8 B, FP32 4 B, BF16 2 B, the
+# kind / coarse-class bytes 1 B); a neighbour's value is an L1/L2 hit and is
+# not counted again.
+PCG_BYTES = {
+    "plain": 139,            # k_spmv_plain_tab 49 (p, 3 couplings, diagonal, kind, Ap), k_update_plain 57, k_direction_plain 33
+    "flex64": 141,           # k_fx_spmv 49, k_fx_update 58, k_fx_dir 34 (the learned coarse path is not HBM-bound)
+    "inner_fp32": 71,        # k_mixed_spmv 25, k_mixed_update 29, k_mixed_direction 17
+    "inner_bf16": 65,        # the same with BF16 couplings
+    "inner_bf16_dir": 57,    # BF16 couplings and search direction
+    "inner_learned32": 73,   # FP32 k_fx_spmv 25, k_fx_update 30, k_fx_dir 18
+    "outer": 165,            # per outer FCG(1) iteration: k_oc_beta 13, k_oc_dir 21, k_oc_spmv 57, k_oc_update 49, inner start 25
+}
+
+
+def pcg_bytes(pf, cfg, st):
+    """Algorithmic bytes per unknown of one solve (PCG_BYTES x iterations)."""
+    if cfg.mode == pf.PF_SOLVER_PLAIN:
+        return PCG_BYTES["plain"] * st.iterations
+    if cfg.mode == pf.PF_SOLVER_LEARNED and not cfg.inner_fp32:
+        return PCG_BYTES["flex64"] * st.iterations
+    if cfg.mode == pf.PF_SOLVER_LEARNED:
+        inner = PCG_BYTES["inner_learned32"]
+    else:
+        inner = PCG_BYTES[{0: "inner_fp32", 1: "inner_bf16"}.get(int(cfg.bf16_storage), "inner_bf16_dir")]
+    return inner * st.iterations + PCG_BYTES["outer"] * st.refinements
+
+
+def pcg_roofline(pf, cfg, st, peak):
+    """Achieved bytes/s of a solve's fine-level passes against the HBM peak."""
+    b = pcg_bytes(pf, cfg, st) * st.n_cells
+    gbs = b / max(st.solve_ms / 1000.0, 1e-12) / 1e9
+    return {"bytes_per_unknown": pcg_bytes(pf, cfg, st), "achieved_gbs": gbs, "frac": gbs / peak}
+
+
+def host_info():
+    """The host's CPUs as this process sees them."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    model = ln.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    try:
+        affinity = len(os.sched_getaffinity(0))
+    except AttributeError:
+        affinity = os.cpu_count()
+    return {"cpu_model": model, "online_cpus": os.cpu_count(), "affinity_cpus": affinity}
 
 
 def measured_hbm():
@@ -331,16 +382,39 @@ def load_weights(pf, grid, path=None):
     return net.load_default()
 
 
-def run_pcg(pf, n, modes, max_iter=20000, seed=0, weights_path=None):
+def oracle_pressure(sc, f, pp, n, dt, rel_tol=1e-10):
+    """The CPU FP64 oracle's pressure of the same system (oracle/pf_oracle.c,
+    Jacobi-PCG to rel_tol), and its wall time."""
+    import oracle as O
+    names = ("u", "v", "w", "mu", "mv", "mw", "p", "mk")
+    go = O.OracleGrid(n, n, n, sc["dx"])
+    for k in ("u", "v", "w", "mu", "mv", "mw", "mk"):
+        i = names.index(k)
+        go.set_field(i, f[k], np.ones(go.bdims(i)[::-1], np.uint8))
+    t0 = time.perf_counter()
+    st = O.Oracle().project(go, O.PhaseParams(pp.rho_l, pp.rho_g, pp.alpha_phi, pp.rho_tilde_0), dt, 200000, 0.0,
+                            rel_tol=rel_tol)
+    wall = time.perf_counter() - t0
+    p, _ = go.get_field(O.P)
+    return p.astype(np.float64), {"rel_tol": rel_tol, "iterations": st.iterations, "converged": bool(st.converged),
+                                  "cpu_s": wall, "cores": 1}
+
+
+def run_pcg(pf, n, modes, max_iter=20000, seed=0, weights_path=None, fp64_oracle=False):
     """Pressure-only system (n^3, every interior cell fluid, 64 air ellipsoids
     in water at 1000:1, band-limited RHS): device time to a 1e-6 relative
     FP64 residual per solver mode, and each mode's pressure against the
-    PLAIN FP64 solve (the first mode)."""
+    PLAIN FP64 solve (the first mode) and, with fp64_oracle, against the CPU
+    FP64 oracle solved to 1e-10."""
     sc = pf.scenes.ellipsoid_pressure(n, seed=seed)
     pp = pf.PhaseParams(sc["rho_l"], sc["rho_g"])
     g = pf.SparseMacGrid3D(n, n, n, sc["dx"], max_particles=1)
     pp.rho_tilde_0 = pf.calibrateRhoTilde0(pp, 1.0, grid=g)
     f = pf.scenes.pressure_grid_fields(sc, pp.rho_tilde_0)
+    peak, _ = measured_hbm()
+    p_oracle, oracle_note = None, None
+    if fp64_oracle:
+        p_oracle, oracle_note = oracle_pressure(sc, f, pp, n, 1.0 / 240.0)
     full = {k: np.ones(g.bdims(i)[::-1], np.uint8) for i, k in enumerate(("u", "v", "w", "mu", "mv", "mw", "p", "mk"))}
     for k in ("mu", "mv", "mw", "mk"):
         g.set_field(("u", "v", "w", "mu", "mv", "mw", "p", "mk").index(k), f[k], full[k])
@@ -360,7 +434,7 @@ def run_pcg(pf, n, modes, max_iter=20000, seed=0, weights_path=None):
         p, _ = g.get_field(pf.PF_P)
         rec = {"ms_to_1e-6": st.solve_ms, "iterations": st.iterations, "refinements": st.refinements,
                "converged": bool(st.converged), "rel_residual": st.res_final / max(st.res0, 1e-300),
-               "setup_ms": tm.as_dict()["precond_setup"][0]}
+               "setup_ms": tm.as_dict()["precond_setup"][0], "roofline": pcg_roofline(pf, cfg, st, peak)}
         if cfg.mode == pf.PF_SOLVER_LEARNED:
             rec["coarse_accepted"] = st.precond_applied
             rec["coarse_rejected"] = st.precond_rejected
@@ -370,23 +444,40 @@ def run_pcg(pf, n, modes, max_iter=20000, seed=0, weights_path=None):
             p_plain = p.astype(np.float64)
         else:
             rec["p_rel_diff_vs_plain"] = float(np.abs(p - p_plain).max() / max(np.abs(p_plain).max(), 1e-300))
+        if p_oracle is not None:
+            rec["err_vs_fp64_oracle"] = float(np.abs(p - p_oracle).max() / max(np.abs(p_oracle).max(), 1e-300))
         out[name] = rec
     base = out[modes[0][0]]["ms_to_1e-6"]
     for name in out:
         out[name]["speedup_vs_plain"] = base / max(out[name]["ms_to_1e-6"], 1e-9)
-    return {"workload": f"ellipsoid_pressure_{n}: {(n - 2) ** 3} unknowns, 64 air ellipsoids, 1000:1, "
-                        "band-limited RHS |k|<=8", "modes": out}
+    res = {"workload": f"ellipsoid_pressure_{n}: {(n - 2) ** 3} unknowns, 64 air ellipsoids, 1000:1, "
+                       "band-limited RHS |k|<=8", "peak_gbs": peak, "modes": out}
+    if oracle_note:
+        res["fp64_oracle"] = oracle_note
+    return res
 
 
-def step_scene(pf, name, n, seed=0):
-    """Scene of a whole-step pressure system: Rayleigh-Taylor (heavy over
-    light, 1000:1, walls only) or the bubble tank (air bubble in water, open
-    headspace)."""
-    if name == "rt":
-        return pf.scenes.rayleigh_taylor(n, seed=seed)
+STEP_SCENES = {"rt": "rayleigh_taylor", "bubble": "bubble_tank"}
+
+
+def seeded_sim(pf, name, n, seed=0, max_iter=20000):
+    """A solver on the scene of a whole-step system, seeded on the device
+    (pf_seed_scene: the particles scenes.py gives, without the host-side
+    generation): Rayleigh-Taylor (heavy over light, 1000:1, walls only) or
+    the bubble tank (air bubble in water, open headspace)."""
+    if name not in STEP_SCENES:
+        raise ValueError(f"unknown step scene {name!r} (rt, bubble)")
+    dx = 1.0 / n
+    sim = pf.SparseSim3DTP(n, n, n, dx, max_particles=8 * (n - 2) ** 3)
+    sim.phase = pf.PhaseParams(1000.0, 1.0)
+    sim.phase.rho_tilde_0 = pf.calibrateRhoTilde0(sim.phase, 1.0, grid=sim.grid)
+    sim.dt = 1.0 / 240.0
     if name == "bubble":
-        return pf.scenes.bubble_tank(n, seed=seed)
-    raise ValueError(f"unknown step scene {name!r} (rt, bubble)")
+        sim.alpha_liquid = sim.alpha_gas = 0.97
+    sim.cg_iters, sim.cg_tol = max_iter, 0.0
+    sim.solver = pf.SolverConfig(rel_tol=1e-6)
+    sim.seed_scene(STEP_SCENES[name], seed)
+    return sim
 
 
 def run_step_pcg(pf, name, n, modes, pre_steps=1, max_iter=20000, seed=0, weights_path=None):
@@ -395,18 +486,9 @@ def run_step_pcg(pf, name, n, modes, pre_steps=1, max_iter=20000, seed=0, weight
     from that same particle snapshot.  Reports each solve's device time to a
     1e-6 relative FP64 residual, iterations, the coarse-correction fallback
     rate and the pressure against the PLAIN solve (the first mode)."""
-    sc = step_scene(pf, name, n, seed)
-    np_ = len(sc["pos"])
-    sim = pf.SparseSim3DTP(n, n, n, sc["dx"], max_particles=np_)
-    sim.phase = pf.PhaseParams(sc["rho_l"], sc["rho_g"])
-    sim.phase.rho_tilde_0 = pf.calibrateRhoTilde0(sim.phase, 1.0, grid=sim.grid)
-    sim.dt = 1.0 / 240.0
-    if name == "bubble":
-        sim.alpha_liquid = sim.alpha_gas = 0.97
-    sim.cg_iters, sim.cg_tol = max_iter, 0.0
-    sim.solver = pf.SolverConfig(rel_tol=1e-6)
-    sim.set_particles(sc["pos"], sc["vel"], sc["type"], sc["volume"])
-    del sc
+    sim = seeded_sim(pf, name, n, seed, max_iter)
+    np_ = sim.n
+    peak, _ = measured_hbm()
     for _ in range(pre_steps):
         sim.step()
     snap = sim.get_particles()
@@ -427,7 +509,7 @@ def run_step_pcg(pf, name, n, modes, pre_steps=1, max_iter=20000, seed=0, weight
         stages = tm.as_dict()
         rec = {"ms_to_1e-6": st.solve_ms, "iterations": st.iterations, "refinements": st.refinements,
                "converged": bool(st.converged), "rel_residual": st.res_final / max(st.res0, 1e-300),
-               "setup_ms": stages["precond_setup"][0]}
+               "setup_ms": stages["precond_setup"][0], "roofline": pcg_roofline(pf, cfg, st, peak)}
         if cfg.mode == pf.PF_SOLVER_LEARNED:
             tot = st.precond_applied + st.precond_rejected
             rec["coarse_accepted"] = st.precond_applied
@@ -443,6 +525,7 @@ def run_step_pcg(pf, name, n, modes, pre_steps=1, max_iter=20000, seed=0, weight
     base = out[modes[0][0]]["ms_to_1e-6"]
     for mname in out:
         out[mname]["speedup_vs_plain"] = base / max(out[mname]["ms_to_1e-6"], 1e-9)
+    sim.grid.close()
     return {"workload": f"{name}_{n} step pressure system after {pre_steps} plain step(s): {np_} particles, "
                         f"1000:1, dt 1/240", "unknowns": int(st.n_cells), "modes": out}
 
@@ -454,21 +537,15 @@ def run_full_step(pf, n=48, steps=20, seed=0, solvers=("plain",), warmup=3):
     preconditioner with the shipped weights), every solver from the same
     initial particles."""
     import torch
-    sc = pf.scenes.rayleigh_taylor(n, seed=seed)
-    out = {"workload": f"rayleigh_taylor_{n}: {len(sc['pos'])} particles, 1000:1, dt 1/240, "
-                       f"pressure to 1e-6, {warmup} warm-up + {steps} timed steps"}
+    out = {}
     for solver in solvers:
-        sim = pf.SparseSim3DTP(n, n, n, sc["dx"], max_particles=len(sc["pos"]))
-        sim.phase = pf.PhaseParams(sc["rho_l"], sc["rho_g"])
-        sim.phase.rho_tilde_0 = pf.calibrateRhoTilde0(sim.phase, 1.0, grid=sim.grid)
-        sim.dt = 1.0 / 240.0
-        sim.cg_iters, sim.cg_tol = 20000, 0.0
+        sim = seeded_sim(pf, "rt", n, seed)
         if solver == "learned":
             pf.LearnedCoarseSolver(sim.grid).load_default()
             sim.solver = pf.SolverConfig(mode=pf.PF_SOLVER_LEARNED, rel_tol=1e-6, precond=pf.PF_PRECOND_NETWORK)
-        else:
-            sim.solver = pf.SolverConfig(rel_tol=1e-6)
-        sim.set_particles(sc["pos"], sc["vel"], sc["type"], sc["volume"])
+        out["workload"] = (f"rayleigh_taylor_{n}: {sim.n} particles, 1000:1, dt 1/240, pressure to 1e-6, "
+                           f"{warmup} warm-up + {steps} timed steps")
+        npart = sim.n
         stream = torch.cuda.ExternalStream(pf.load().pf_stream(sim.grid.ctx))
         for _ in range(warmup):
             sim.step()
@@ -483,7 +560,7 @@ def run_full_step(pf, n=48, steps=20, seed=0, solvers=("plain",), warmup=3):
         e1.record(stream)
         e1.synchronize()
         ms = e0.elapsed_time(e1)
-        rec = {"particles_per_s": len(sc["pos"]) * steps / (ms / 1000.0), "ms_per_step": ms / steps,
+        rec = {"particles_per_s": npart * steps / (ms / 1000.0), "ms_per_step": ms / steps,
                "pcg_iterations_per_step": iters / steps}
         if solver == "learned":
             rec["coarse_rejected"] = rejected
@@ -491,6 +568,58 @@ def run_full_step(pf, n=48, steps=20, seed=0, solvers=("plain",), warmup=3):
         sim.grid.close()
     if "plain" in out and "learned" in out:
         out["learned_speedup"] = out["plain"]["ms_per_step"] / out["learned"]["ms_per_step"]
+    return out
+
+
+def run_pressure_cpu(pf, n=48, seed=0):
+    """The reference's own projection (spProjectStepVC3D from oracle/_ref, the
+    unmodified sources; single-threaded) on the pressure system of the first
+    Rayleigh-Taylor step at n^3 (1000:1, dt 1/240: markCells, P2G, gravity
+    and walls by the oracle), timed on the host beside the GPU's PLAIN and
+    learned solves of the same system.  The reference stops on an absolute
+    max-norm tolerance, set to 1e-6 max|r0| of this system: the relative rule
+    the GPU solves use."""
+    import oracle as O
+    sc = pf.scenes.rayleigh_taylor(n, seed=seed)
+    pp = pf.PhaseParams(sc["rho_l"], sc["rho_g"])
+    opp = O.PhaseParams(sc["rho_l"], sc["rho_g"])
+    opp.rho_tilde_0 = pp.rho_tilde_0 = O.Oracle().calibrate_rho_tilde0(opp, 1.0)
+    ps = O.Particles(sc["pos"].astype(np.float64), sc["vel"].astype(np.float64), sc["type"],
+                     sc["volume"].astype(np.float64))
+    o = O.Oracle()
+    go = O.OracleGrid(n, n, n, sc["dx"])
+    o.mark_cells(go, ps)
+    o.p2g(go, ps, opp, 1.0)
+    o.apply_gravity(go, 1.0 / 240.0, -9.81)
+    o.apply_wall_boundary(go)
+    fields = [go.get_field(f) for f in range(8)]
+    out = {"workload": f"rayleigh_taylor_{n} first-step pressure system: 1000:1, dt 1/240, to 1e-6 relative"}
+    g = pf.SparseMacGrid3D(n, n, n, sc["dx"], max_particles=1)
+    gpu_p = {}
+    for name, cfg in (("plain", pf.SolverConfig(rel_tol=1e-6)),
+                      ("learned", pf.SolverConfig(mode=pf.PF_SOLVER_LEARNED, rel_tol=1e-6,
+                                                  precond=pf.PF_PRECOND_NETWORK))):
+        if name == "learned":
+            load_weights(pf, g)
+        for f in range(8):
+            g.set_field(f, *fields[f])
+        st = pf.spProjectStepVC3D(g, pp, 1.0 / 240.0, 20000, 0.0, solver=cfg)
+        gpu_p[name] = g.get_field(pf.PF_P)[0].astype(np.float64)
+        out[f"gpu_{name}"] = {"ms": st.solve_ms, "iterations": st.iterations, "converged": bool(st.converged)}
+        res0 = st.res0
+    g.close()
+    rg = O.ReferenceGrid(n, n, n, sc["dx"])
+    for f in range(8):
+        rg.set_field(f, *fields[f])
+    t0 = time.perf_counter()
+    O.Reference().project(rg, opp, 1.0 / 240.0, 20000, 1e-6 * res0)
+    ref_ms = 1000.0 * (time.perf_counter() - t0)
+    p_ref = rg.get_field(O.P)[0].astype(np.float64)
+    scale = max(np.abs(p_ref).max(), 1e-300)
+    out["reference"] = {"ms": ref_ms, "cores": 1, "abs_tol": 1e-6 * res0, "kind": "reference"}
+    for name in gpu_p:
+        out[f"gpu_{name}"]["speedup_vs_reference"] = ref_ms / max(out[f"gpu_{name}"]["ms"], 1e-9)
+        out[f"gpu_{name}"]["p_rel_diff_vs_reference"] = float(np.abs(gpu_p[name] - p_ref).max() / scale)
     return out
 
 
@@ -557,7 +686,14 @@ def run_adapt(pf, n=128, seed=0, reps=5, cpu=True):
             rec["speedup_vs_reference"] = rec["cpu_reference_ms"] / rec["gpu_ms"]
             rec["reference_stats_equal"] = [int(v) for v in res] == rec["stats"]
         out["cpu_cores"] = 1
+        out["host"] = host_info()
     return out
+
+
+# solvers of the whole-step pressure systems: PLAIN, the learned two-level
+# preconditioner, and the same with an exact coarse solve (the bound a perfect
+# network reaches)
+STEP_MODES = ["plain_fp64", "learned", "exact_coarse"]
 
 
 def run_ours(args, rank, world, local, dist):
@@ -625,17 +761,28 @@ def run_ours(args, rank, world, local, dist):
         "clocks": clk.summary(),
     }
     if rank == 0 and not args.no_extras:
-        line["pcg"] = run_pcg(pf, args.pcg_n, pcg_modes(pf, args.pcg_modes.split(",")))
+        line["pcg"] = run_pcg(pf, args.pcg_n, pcg_modes(pf, args.pcg_modes.split(",")), max_iter=args.pcg_max_iter)
+        line["pcg_fp64_oracle"] = run_pcg(pf, 64, pcg_modes(pf, args.pcg_modes.split(",")),
+                                          max_iter=args.pcg_max_iter, fp64_oracle=True)
+        line["step_pcg"] = [run_step_pcg(pf, name, int(sz), pcg_modes(pf, STEP_MODES), max_iter=args.pcg_max_iter)
+                            for name, sz in (item.split(":") for item in args.step_pcg_default.split(","))]
         line["full_step"] = run_full_step(pf, n=args.full_step_n, steps=args.full_step_steps,
                                           solvers=("plain", "learned"))
         line["adaptivity"] = run_adapt(pf, n=args.adapt_n, cpu=not args.no_cpu_baseline)
+        if not args.no_cpu_baseline:
+            line["pressure_cpu_baseline"] = run_pressure_cpu(pf)
     if rank == 0 and not args.no_cpu_baseline:
-        cores = 8
-        np_s, times = cpu_reference_sample(sc, slab_cells=args.cpu_slab, steps=1)
-        line["cpu_baseline"] = {"value": np_s / times[0], "unit": UNIT, "cores": cores, "kind": "reference",
+        host = host_info()
+        # the reference's P2G runs its 8 colour threads (runColor8), G2P one
+        cores = min(8, host["affinity_cpus"] or 1)
+        np_s, times = cpu_reference_sample(sc, slab_cells=args.cpu_slab, steps=args.cpu_steps, warmup=1)
+        mean = sum(times) / len(times)
+        line["cpu_baseline"] = {"value": np_s / mean, "unit": UNIT, "cores": cores, "kind": "reference",
+                                "host": host,
                                 "sample": f"reference spP2G3D_tp + saved copy + spG2P3D_tp on the {np_s} particles "
-                                          f"of the first {args.cpu_slab} x-columns of the 128^3 scene, 1 step "
-                                          f"({times[0]:.1f} s); P2G uses the reference's 8 colour threads, G2P 1"}
+                                          f"of the first {args.cpu_slab} x-columns of the 128^3 scene, 1 warm-up "
+                                          f"+ {len(times)} timed steps ({mean:.2f} s each); P2G on up to 8 colour "
+                                          f"threads, G2P on one"}
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -654,8 +801,10 @@ def run_reference(args, rank, world):
         "dtype": "f64", "data": "synthetic (seeded bubble tank scene)", "impl": "reference",
         "config": {"workload": f"bubble_tank_{args.n} transfer stress: P2G(u,v,w,raw mass)+G2P, FLIP 0.97",
                    "grid": [args.n] * 3, "sample_particles": np_s},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 8, "kind": "reference",
-                         "sample": f"{np_s} particles (first {args.cpu_slab} x-columns) per step"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": min(8, host_info()["affinity_cpus"] or 1),
+                         "kind": "reference", "host": host_info(),
+                         "sample": f"{np_s} particles (first {args.cpu_slab} x-columns) per step; P2G on up to 8 "
+                                   f"colour threads, G2P on one"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -674,15 +823,19 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip the PCG, full-step and adaptivity blocks")
     ap.add_argument("--pcg-n", type=int, default=256, help="grid of the pressure-only block")
     ap.add_argument("--pcg-only", action="store_true", help="run only the pressure-only block")
-    ap.add_argument("--pcg-max-iter", type=int, default=20000, help="iteration cap of the pressure-only block")
-    ap.add_argument("--pcg-modes", default="plain_fp64,learned,flex_jacobi",
+    ap.add_argument("--pcg-max-iter", type=int, default=60000, help="iteration cap of the pressure blocks")
+    ap.add_argument("--pcg-modes", default="plain_fp64,learned,flex_jacobi,mixed_fp32,mixed_bf16,learned_mixed",
                     help="solvers of the pressure-only block (plain_fp64 first): plain_fp64, learned, "
-                         "flex_jacobi, mixed_fp32, mixed_bf16")
+                         "flex_jacobi, exact_coarse, mixed_fp32, mixed_bf16, mixed_bf16_dir, learned_mixed "
+                         "(name@M:ETA sets an inner-outer mode's inner cap and reduction)")
+    ap.add_argument("--step-pcg-default", default="rt:256,bubble:128",
+                    help="whole-step pressure systems of the default run (plain, learned, exact coarse)")
+    ap.add_argument("--cpu-steps", type=int, default=2, help="timed steps of the CPU reference sample")
     ap.add_argument("--step-pcg", default="",
                     help="run only whole-step pressure systems, e.g. rt:256,bubble:128 (modes from --pcg-modes)")
     ap.add_argument("--step-pcg-pre", type=int, default=1, help="plain steps before the step-pressure snapshot")
     ap.add_argument("--weights", default="", help="network weights for the learned mode (default: shipped)")
-    ap.add_argument("--full-step-n", type=int, default=128, help="grid of the full-step block (Rayleigh-Taylor)")
+    ap.add_argument("--full-step-n", type=int, default=256, help="grid of the full-step block (Rayleigh-Taylor)")
     ap.add_argument("--full-step-steps", type=int, default=5, help="timed steps of the full-step block")
     ap.add_argument("--full-step-only", action="store_true", help="run only the full-step block")
     ap.add_argument("--adapt-n", type=int, default=128, help="grid of the particle-adaptivity block")

@@ -384,6 +384,23 @@ PFGPU_API int pf_project_noalloc(int nx, int ny, int nz, double dx, const float*
                                  const pf_phase* phase, double dt, int max_iter, double abs_tol,
                                  double rel_tol, double c_div, pf_solve_stats* stats, void* stream);
 
+/* ---- synthetic scenes of the benchmark configurations -------------------
+ * Seeds the context's particle set on the device (replacing it) with 8
+ * jittered particles per seeded cell, in the layouts of the reference's
+ * SparseSim3DTP::initRayleighTaylor / initBubbleTank
+ * (src/driver/sparse_sim3d_tp.cpp:739-776) at the benchmark densities:
+ *   PF_SCENE_RAYLEIGH_TAYLOR: every interior cell; type 0 (heavy) above
+ *     y = 0.5 + 0.05 cos(2 pi x) cos(2 pi z), type 1 below; zero velocity;
+ *   PF_SCENE_BUBBLE_TANK: interior cells whose centre lies below y = 0.7;
+ *     type 1 inside the sphere of radius 0.15 at (0.5, 0.3, 0.5), type 0
+ *     elsewhere; velocities N(0, 0.1^2) per component.
+ * Volumes are 1.  Positions are bit-identical to the host generator of the
+ * same seed (adaptive-pf-flip_b200/scenes.py).  *n_out receives the count;
+ * PF_ERR_CAPACITY if it exceeds max_particles. */
+#define PF_SCENE_RAYLEIGH_TAYLOR 0
+#define PF_SCENE_BUBBLE_TANK 1
+PFGPU_API int pf_seed_scene(pf_ctx* ctx, int scene, unsigned long long seed, size_t* n_out);
+
 /* calibrateRhoTilde0 (src/transfer/transfer3d_tp.cpp:29-36), on the device. */
 PFGPU_API int pf_calibrate_rho_tilde0(pf_ctx* ctx, const pf_phase* phase, double Vp, double* out);
 

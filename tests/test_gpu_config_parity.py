@@ -216,3 +216,21 @@ def test_active_cells_match_reference_collect(pf, case):
     assert len(ref) > 0
     assert np.array_equal(g.fluid_cells(), ref)
     g.close()
+
+
+@pytest.mark.parametrize("scene,n,seed", [("rayleigh_taylor", 24, 0), ("rayleigh_taylor", 40, 3),
+                                          ("bubble_tank", 32, 0), ("bubble_tank", 48, 5)])
+def test_device_scene_equals_host_generator(pf, scene, n, seed):
+    """pf_seed_scene against scenes.py: positions and types identical, volumes
+    1, bubble-tank velocities within one FP32 ulp (Box-Muller on the device's
+    libm)."""
+    sc = getattr(pf.scenes, scene)(n, seed=seed)
+    sim = pf.SparseSim3DTP(n, n, n, 1.0 / n, max_particles=len(sc["pos"]))
+    assert sim.seed_scene(scene, seed) == len(sc["pos"])
+    pos, vel, typ, vol = sim.get_particles()
+    assert np.array_equal(_bits(pos), _bits(sc["pos"]))
+    assert np.array_equal(typ, sc["type"])
+    assert np.all(vol == 1.0)
+    ulp = np.spacing(np.abs(sc["vel"]).astype(np.float32))
+    assert np.all(np.abs(vel - sc["vel"]) <= ulp)
+    sim.grid.close()
