@@ -61,7 +61,7 @@ void free_all(pf_ctx* c) {
   F(c->partials); F(c->ctl); F(c->ctl_outer); F(c->nbr_plain);
   F(c->xf); F(c->rf); F(c->pf32); F(c->Apf); F(c->diagf); F(c->cxf); F(c->cyf); F(c->czf); F(c->pbf); F(c->cbf);
   F(c->b64);
-  F(c->d_clamp); F(c->d_flags); F(c->cell_flags); F(c->esc_buf);
+  F(c->d_clamp); F(c->d_flags); F(c->cell_flags); F(c->esc_buf); F(c->mk_first); F(c->rc_buf);
   if (c->up_stream) cudaStreamSynchronize(c->up_stream);
   F(c->bpx); F(c->bpy); F(c->bpz); F(c->bvx); F(c->bvy); F(c->bvz); F(c->bvol); F(c->btype); F(c->up_staging);
   if (c->up_done) cudaEventDestroy(c->up_done);
@@ -211,6 +211,8 @@ int create_impl(pf_ctx* ctx, const pf_grid_desc* d) {
   for (int f = 0; f < PF_NFIELDS; ++f)
     if (2 * ctx->act4_n[f] + 2 > cf) cf = 2 * ctx->act4_n[f] + 2;
   PF_CUDA_TRY(cudaMalloc(&ctx->cell_flags, cf * sizeof(int32_t)));
+  PF_CUDA_TRY(cudaMalloc(&ctx->mk_first, ctx->act4_n[PF_MK] * sizeof(uint32_t)));
+  PF_CUDA_TRY(cudaMemset(ctx->mk_first, 0xff, ctx->act4_n[PF_MK] * sizeof(uint32_t)));
   PF_CUDA_TRY(cudaDeviceSynchronize());
   return PF_OK;
 }

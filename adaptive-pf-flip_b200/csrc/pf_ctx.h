@@ -28,6 +28,11 @@ struct pf_ctx {
   float* saved[PF_NSAVED] = {};
   uint8_t* act4[PF_NFIELDS] = {};
   size_t act4_n[PF_NFIELDS] = {};
+  // first-touch key of each 4^3 marker block: the position, in the reference's
+  // markCells order (wall loops, then particles), of the write that activated it
+  uint32_t* mk_first = nullptr;
+  void* rc_buf = nullptr;  // render-cache export scratch, grown on demand
+  size_t rc_bytes = 0;
   std::vector<int> wall_tiles;  // tiles written by markCells walls / applyWallBoundary
   int* d_wall_tiles = nullptr;
   bool saved_valid = false;

@@ -231,6 +231,8 @@ int field_clear(pf_ctx* ctx, int f) {
   if (ctx->nslots > 0)
     PF_CUDA_TRY(cudaMemsetAsync(ctx->fld[f], 0, (size_t)ctx->nslots * PF_TV * sizeof(float), ctx->stream));
   PF_CUDA_TRY(cudaMemsetAsync(ctx->act4[f], 0, ctx->act4_n[f], ctx->stream));
+  if (f == PF_MK && ctx->mk_first)
+    PF_CUDA_TRY(cudaMemsetAsync(ctx->mk_first, 0xff, ctx->act4_n[PF_MK] * sizeof(uint32_t), ctx->stream));
   return PF_OK;  // the saved copy is separate storage and stays valid
 }
 
@@ -253,6 +255,13 @@ __global__ void k_request_from_act4(Geom g, int f, const uint8_t* act, uint8_t* 
   const int by = q % g.bdim[f][1];
   const int bz = q / g.bdim[f][1];
   need[tile_id(g, bx >> 1, by >> 1, bz >> 1)] = 1;
+}
+
+// An imported marker field's blocks count as activated in ascending block id,
+// the order in which the reference's setCell loop over (k, j, i) touches them.
+__global__ void k_first_from_act(const uint8_t* act, int n, uint32_t* first) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b < n) first[b] = act[b] ? (uint32_t)b : 0xffffffffu;
 }
 
 __global__ void k_import_field(DevGrid G, int f, const float* dense, int nslots) {
@@ -326,6 +335,7 @@ int grid_set_field(pf_ctx* ctx, int f, const float* dense, const uint8_t* act4) 
   PF_CUDA_TRY(cudaMemcpyAsync(ctx->act4[f], d_act, ctx->act4_n[f], cudaMemcpyDeviceToDevice, ctx->stream));
   const int nb = (int)ctx->act4_n[f];
   (++ctx->launches), k_request_from_act4<<<nblocks(nb, 256), 256, 0, ctx->stream>>>(g, f, ctx->act4[f], ctx->tile_need);
+  if (f == PF_MK) (++ctx->launches), k_first_from_act<<<nblocks(nb, 256), 256, 0, ctx->stream>>>(ctx->act4[f], nb, ctx->mk_first);
   PF_CUDA_TRY(cudaGetLastError());
   int rc = pool_commit(ctx);
   if (rc) return rc;

@@ -12,11 +12,15 @@
 // writes is byte-identical for the same state.
 //
 // Block order: the reference lists cells block by block in the order its
-// marker blocks were first activated (a history of markCells' wall loops
-// and particle order); the pool keeps no activation history, so blocks are
-// listed in ascending block id, cells within a block in the reference's
-// lz, ly, lx order.  The set of cell lines is identical; the liquid volume
-// sum over them is accumulated in this order.
+// marker blocks were first activated (activeBlockIds: markCells' wall loops,
+// then the particles in index order), cells within a block in lz, ly, lx
+// order.  markCells here keeps each marker block's first-touch key (its
+// position in that sequence; ascending block id for an imported marker
+// field), and the blocks are listed sorted by it, so the file lists the cells
+// in the reference's order and sums the liquid volume in that order too.
+// With no marker block active the pressure blocks are listed in ascending
+// block id.
+#include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
 #include <algorithm>
@@ -74,33 +78,41 @@ __device__ __forceinline__ bool rc_cell(const DevGrid& G, const RcPhiK& P, int f
   return true;
 }
 
-// One 64-thread CTA per 4^3 block (grid-stride): kept-cell count per block
-// and the number of active blocks of field fsel.
-__global__ void __launch_bounds__(64) k_rc_count(DevGrid G, RcPhiK P, int fsel, int nb4, int* cnt, int* nactive) {
-  for (int b = blockIdx.x; b < nb4; b += gridDim.x) {
+// The active blocks of field fsel, each with its listing key (the marker
+// field's first-touch key, or the block id), compacted in any order: the sort
+// that follows fixes it.
+__global__ void k_rc_list(const uint8_t* act, const uint32_t* first, int nb4, int* nlist, uint32_t* key, int* list) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb4 || !act[b]) return;
+  const int q = atomicAdd(nlist, 1);
+  key[q] = first ? first[b] : (uint32_t)b;
+  list[q] = b;
+}
+
+// One 64-thread CTA per listed block (grid-stride): its kept-cell count.
+__global__ void __launch_bounds__(64) k_rc_count(DevGrid G, RcPhiK P, int fsel, const int* list, int n, int* cnt) {
+  for (int q = blockIdx.x; q < n; q += gridDim.x) {
     RcCell c;
-    const int keep = rc_cell(G, P, fsel, b, threadIdx.x, &c) ? 1 : 0;
-    const int n = __syncthreads_count(keep);
-    if (threadIdx.x == 0) {
-      cnt[b] = n;
-      if (G.act4[fsel][b]) atomicAdd(nactive, 1);
-    }
+    const int keep = rc_cell(G, P, fsel, list[q], threadIdx.x, &c) ? 1 : 0;
+    const int k = __syncthreads_count(keep);
+    if (threadIdx.x == 0) cnt[q] = k;
   }
 }
 
-// Same walk; each kept cell goes to off[b] + its rank among the block's kept
+// Same walk; each kept cell goes to off[q] + its rank among the block's kept
 // cells in lz, ly, lx order.
-__global__ void __launch_bounds__(64) k_rc_write(DevGrid G, RcPhiK P, int fsel, int nb4, const int* off, RcCell* out) {
+__global__ void __launch_bounds__(64) k_rc_write(DevGrid G, RcPhiK P, int fsel, const int* list, int n,
+                                                 const int* off, RcCell* out) {
   __shared__ unsigned w0;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int b = blockIdx.x; b < nb4; b += gridDim.x) {
+  for (int q = blockIdx.x; q < n; q += gridDim.x) {
     RcCell c;
-    const bool keep = rc_cell(G, P, fsel, b, threadIdx.x, &c);
+    const bool keep = rc_cell(G, P, fsel, list[q], threadIdx.x, &c);
     const unsigned m = __ballot_sync(0xffffffffu, keep);
     if (threadIdx.x == 0) w0 = m;
     __syncthreads();
     const int base = warp ? __popc(w0) : 0;
-    if (keep) out[off[b] + base + __popc(m & ((1u << lane) - 1u))] = c;
+    if (keep) out[off[q] + base + __popc(m & ((1u << lane) - 1u))] = c;
     __syncthreads();
   }
 }
@@ -138,7 +150,23 @@ bool finite3(const double v[3]) { return std::isfinite(v[0]) && std::isfinite(v[
 
 }  // namespace
 
-// Kept phase cells of the current grid, compacted on the device.
+// The export's device scratch, kept by the context and grown on demand.
+static int rc_scratch(pf_ctx* ctx, size_t bytes, char** out) {
+  if (bytes > ctx->rc_bytes) {
+    if (ctx->rc_buf) PF_CUDA_TRY(cudaFree(ctx->rc_buf));
+    ctx->rc_buf = nullptr;
+    ctx->rc_bytes = 0;
+    PF_CUDA_TRY(cudaMalloc(&ctx->rc_buf, bytes));
+    ctx->rc_bytes = bytes;
+  }
+  *out = (char*)ctx->rc_buf;
+  return PF_OK;
+}
+
+static size_t align_up(size_t v) { return (v + 255) & ~(size_t)255; }
+
+// Kept phase cells of the current grid, compacted on the device in the
+// reference's block order.
 int render_cells(pf_ctx* ctx, const pf_phase* ph, std::vector<RcCell>* cells) {
   const Geom& g = ctx->g;
   const int nb4 = g.bdim[PF_MK][0] * g.bdim[PF_MK][1] * g.bdim[PF_MK][2];
@@ -146,50 +174,75 @@ int render_cells(pf_ctx* ctx, const pf_phase* ph, std::vector<RcCell>* cells) {
   P.rmin = std::log(ph->rho_l / ph->rho_g) * ph->rho_g * ph->rho_tilde_0;
   P.den = ph->alpha_phi * ph->rho_tilde_0 * ph->rho_l;
   const DevGrid G = dev_grid(ctx);
-  int* d = nullptr;  // [nb4 + 1] counts, [nb4 + 1] offsets, [1] active blocks
-  void* tmp = nullptr;
-  RcCell* dc = nullptr;
-  size_t tmp_bytes = 0;
-  int rc = PF_OK;
-  cudaError_t e = cudaMalloc(&d, (2 * (size_t)(nb4 + 1) + 1) * sizeof(int));
-  if (e != cudaSuccess) return PF_ERR_CUDA;
-  int* cnt = d;
-  int* off = d + nb4 + 1;
-  int* nact = off + nb4 + 1;
-  const int grid = std::max(1, std::min(nb4, 148 * 32));
-  int h_act = 0, total = 0, fsel = PF_MK;
-  for (int pass = 0; pass < 2 && rc == PF_OK; ++pass) {
-    // activeBlockIds of mkf, or of pf when no marker block is active
-    if ((e = cudaMemsetAsync(d, 0, (2 * (size_t)(nb4 + 1) + 1) * sizeof(int), ctx->stream)) != cudaSuccess) break;
-    (++ctx->launches), k_rc_count<<<grid, 64, 0, ctx->stream>>>(G, P, fsel, nb4, cnt, nact);
-    if ((e = cudaMemcpyAsync(&h_act, nact, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream)) != cudaSuccess) break;
-    if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) break;
-    if (h_act > 0 || fsel == PF_P) break;
+  // scratch: keys and lists (unsorted, sorted), counts, offsets, list size,
+  // then the cub temporary storage of the sort and the scan
+  size_t sort_tmp = 0, scan_tmp = 0;
+  PF_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, sort_tmp, (uint32_t*)nullptr, (uint32_t*)nullptr,
+                                              (int*)nullptr, (int*)nullptr, nb4, 0, 32, ctx->stream));
+  PF_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, scan_tmp, (int*)nullptr, (int*)nullptr, nb4 + 1, ctx->stream));
+  const size_t n4 = align_up((size_t)(nb4 + 1) * 4);
+  const size_t tmp_bytes = align_up(std::max(sort_tmp, scan_tmp));
+  const size_t fixed = 6 * n4 + 256 + tmp_bytes;
+  char* buf = nullptr;
+  int rc = rc_scratch(ctx, fixed, &buf);
+  if (rc) return rc;
+  uint32_t* key_in = (uint32_t*)buf;
+  uint32_t* key = (uint32_t*)(buf + n4);
+  int* list_in = (int*)(buf + 2 * n4);
+  int* list = (int*)(buf + 3 * n4);
+  int* cnt = (int*)(buf + 4 * n4);
+  int* off = (int*)(buf + 5 * n4);
+  int* nlist = (int*)(buf + 6 * n4);
+  void* tmp = buf + 6 * n4 + 256;
+  // activeBlockIds of mkf, or of pf when no marker block is active
+  int n = 0, fsel = PF_MK;
+  for (int pass = 0; pass < 2; ++pass) {
+    PF_CUDA_TRY(cudaMemsetAsync(nlist, 0, sizeof(int), ctx->stream));
+    (++ctx->launches), k_rc_list<<<nblocks(nb4, 256), 256, 0, ctx->stream>>>(
+        ctx->act4[fsel], fsel == PF_MK ? ctx->mk_first : nullptr, nb4, nlist, key_in, list_in);
+    PF_CUDA_TRY(cudaGetLastError());
+    PF_CUDA_TRY(cudaMemcpyAsync(ctx->h_pinned_ints, nlist, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    PF_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    n = ctx->h_pinned_ints[0];
+    if (n > 0 || fsel == PF_P) break;
     fsel = PF_P;
   }
-  if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, cnt, off, nb4 + 1, ctx->stream);
-  if (e == cudaSuccess) e = cudaMalloc(&tmp, std::max<size_t>(tmp_bytes, 16));
-  if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, cnt, off, nb4 + 1, ctx->stream);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(&total, off + nb4, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-  if (e == cudaSuccess) {
-    cells->resize((size_t)total);
-    if (total > 0) {
-      e = cudaMalloc(&dc, (size_t)total * sizeof(RcCell));
-      if (e == cudaSuccess) {
-        (++ctx->launches), k_rc_write<<<grid, 64, 0, ctx->stream>>>(G, P, fsel, nb4, off, dc);
-        e = cudaGetLastError();
-      }
-      if (e == cudaSuccess)
-        e = cudaMemcpyAsync(cells->data(), dc, (size_t)total * sizeof(RcCell), cudaMemcpyDeviceToHost, ctx->stream);
-      if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-    }
+  cells->clear();
+  if (n == 0) return PF_OK;
+  size_t tb = tmp_bytes;
+  PF_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, tb, key_in, key, list_in, list, n, 0, 32, ctx->stream));
+  const int grid = std::max(1, std::min(n, 148 * 32));
+  (++ctx->launches), k_rc_count<<<grid, 64, 0, ctx->stream>>>(G, P, fsel, list, n, cnt);
+  PF_CUDA_TRY(cudaMemsetAsync(cnt + n, 0, sizeof(int), ctx->stream));
+  tb = tmp_bytes;
+  PF_CUDA_TRY(cub::DeviceScan::ExclusiveSum(tmp, tb, cnt, off, n + 1, ctx->stream));
+  PF_CUDA_TRY(cudaMemcpyAsync(ctx->h_pinned_ints, off + n, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  PF_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  const int total = ctx->h_pinned_ints[0];
+  if (total == 0) return PF_OK;
+  // the cell records after the fixed part (the scratch grows, keeping nothing of the fixed part's contents
+  // that is still needed: list and offsets are copied into the grown buffer first when it moves)
+  const size_t need = fixed + (size_t)total * sizeof(RcCell);
+  if (need > ctx->rc_bytes) {
+    char* old = buf;
+    void* grown = nullptr;
+    PF_CUDA_TRY(cudaMalloc(&grown, need));
+    PF_CUDA_TRY(cudaMemcpyAsync(grown, old, fixed, cudaMemcpyDeviceToDevice, ctx->stream));
+    PF_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    PF_CUDA_TRY(cudaFree(ctx->rc_buf));
+    ctx->rc_buf = grown;
+    ctx->rc_bytes = need;
+    buf = (char*)grown;
+    list = (int*)(buf + 3 * n4);
+    off = (int*)(buf + 5 * n4);
   }
-  if (e != cudaSuccess) rc = PF_ERR_CUDA;
-  cudaFree(dc);
-  cudaFree(tmp);
-  cudaFree(d);
-  return rc;
+  RcCell* dc = (RcCell*)(buf + fixed);
+  (++ctx->launches), k_rc_write<<<grid, 64, 0, ctx->stream>>>(G, P, fsel, list, n, off, dc);
+  PF_CUDA_TRY(cudaGetLastError());
+  cells->resize((size_t)total);
+  PF_CUDA_TRY(cudaMemcpyAsync(cells->data(), dc, (size_t)total * sizeof(RcCell), cudaMemcpyDeviceToHost, ctx->stream));
+  PF_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return PF_OK;
 }
 
 }  // namespace pf

@@ -180,7 +180,12 @@ __global__ void k_bin_scatter(const int* __restrict__ pkey, const int* __restric
 // ---------------------------------------------------------------------------
 // markCells (sparse_sim3d_tp.cpp:22-50)
 // ---------------------------------------------------------------------------
-__global__ void k_mark_walls(DevGrid G) {
+// Every marker write also lowers the first-touch key of its 4^3 block to the
+// write's position in the reference's markCells sequence: the three wall
+// loops (x, y, z walls; position q as enumerated here), then the particles
+// (position walls + particle index).  Sorting the active blocks by the key
+// gives the reference's activeBlockIds() order of the marker field.
+__global__ void k_mark_walls(DevGrid G, uint32_t* first) {
   const int nx = G.g.nx, ny = G.g.ny, nz = G.g.nz;
   const long long nxf = 2LL * ny * nz, nyf = 2LL * nx * nz, nzf = 2LL * nx * ny;
   const long long total = nxf + nyf + nzf;
@@ -201,11 +206,12 @@ __global__ void k_mark_walls(DevGrid G) {
     if (sl < 0) continue;  // unreachable: wall tiles are pooled first
     G.fld[PF_MK][(size_t)sl * PF_TV + local_id(i, j, k)] = 2.0f;
     activate4(G, PF_MK, i, j, k);
+    atomicMin(&first[act4_index(G.g, PF_MK, i, j, k)], (uint32_t)q);
   }
 }
 
 __global__ void k_mark_particles(DevGrid G, const float* __restrict__ px, const float* __restrict__ py,
-                                 const float* __restrict__ pz, int n) {
+                                 const float* __restrict__ pz, int n, uint32_t* first, uint32_t walls) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
   // (int) truncation, as the reference's cast
@@ -219,6 +225,7 @@ __global__ void k_mark_particles(DevGrid G, const float* __restrict__ px, const 
   if ((int)(*m + 0.5f) != 2) {
     *m = 1.0f;
     activate4(G, PF_MK, i, j, k);
+    atomicMin(&first[act4_index(G.g, PF_MK, i, j, k)], walls + (uint32_t)p);
   }
 }
 
@@ -505,22 +512,21 @@ __device__ __forceinline__ void splat_particles(const DevGrid& G, const SplatWin
                                                 f32x2 (&ap)[9][2], float (&bmin)[8]) {
   using W = SplatWindow<A>;
   const f32x2 one2 = f2_pack(1.0f, 1.0f);
-  // the next particle's attributes are loaded while this one is splatted
+  // the next particle's attributes are loaded while this one is splatted (the
+  // last particle reloads itself, so the loads need no branch)
   int pn = perm[beg];
   float xn = px[pn], yn = py[pn], zn = pz[pn], vn = vA[pn], voln = vol[pn];
   uint8_t tn = type[pn];
   for (int q = beg; q < end; ++q) {
     const float X = xn, Y = yn, Z = zn, VA = vn, VOL = voln;
     const uint8_t TY = tn;
-    if (q + 1 < end) {
-      pn = perm[q + 1];
-      xn = px[pn];
-      yn = py[pn];
-      zn = pz[pn];
-      vn = vA[pn];
-      voln = vol[pn];
-      tn = type[pn];
-    }
+    pn = perm[min(q + 1, end - 1)];
+    xn = px[pn];
+    yn = py[pn];
+    zn = pz[pn];
+    vn = vA[pn];
+    voln = vol[pn];
+    tn = type[pn];
     f32x2 a[3][2];
     win.coords(G, X, Y, Z, fast, inv_dx_f, inv_dx, edge, a);
     {
@@ -546,7 +552,6 @@ __device__ __forceinline__ void splat_particles(const DevGrid& G, const SplatWin
     f2_unpack(a[W::S2][0], aS2[0], aS2[1]);
     f2_unpack(a[W::S2][1], aS2[2], aS2[3]);
     f32x2 w[9][2];
-    f32x2 ws = 0ull;
 #pragma unroll
     for (int s2 = 0; s2 < 3; ++s2)
 #pragma unroll
@@ -557,9 +562,14 @@ __device__ __forceinline__ void splat_particles(const DevGrid& G, const SplatWin
         for (int h = 0; h < 2; ++h) {
           const f32x2 t = f2_pack(sub_sat(om[2 * h], at), sub_sat(om[2 * h + 1], at));
           w[r][h] = f2_mul(f2_mul(t, t), t);
-          ws = f2_add(ws, w[r][h]);
         }
       }
+    // the weight sum as a fixed tree (short dependency chains)
+    f32x2 q9[9];
+#pragma unroll
+    for (int r = 0; r < 9; ++r) q9[r] = f2_add(w[r][0], w[r][1]);
+    const f32x2 ws = f2_add(f2_add(f2_add(q9[0], q9[1]), f2_add(q9[2], q9[3])),
+                            f2_add(f2_add(q9[4], q9[5]), f2_add(f2_add(q9[6], q9[7]), q9[8])));
     float wlo, whi;
     f2_unpack(ws, wlo, whi);
     const float wsum = wlo + whi;
@@ -795,14 +805,18 @@ __global__ void __launch_bounds__(kSplatThreads, 3) k_splat(DevGrid G, const int
   }
 }
 
-// Footprint index of local node l (0..7) of a tile along one axis in the
-// staging box of the tile at offset o (-1, 0, +1) along that axis, or -1 when
-// that tile's cells do not reach the node: along the normal axis a node takes
-// cells l-2..l+1, along a transverse axis l-1..l+1.
-__device__ __forceinline__ int stage_index(int l, int o, bool normal) {
-  if (o == 0) return l + 1;
-  if (o < 0) return (normal ? l <= 1 : l == 0) ? l + 9 : -1;
-  return l == 7 ? 0 : -1;
+// The tiles whose cells reach local node l (0..7) of a tile along one axis,
+// in ascending offset, with the node's index in each one's staging box: along
+// the normal axis a node takes cells l-2..l+1, along a transverse axis
+// l-1..l+1, so it has one or two such tiles.  Returns their number.
+__device__ __forceinline__ int stage_axis(int l, bool normal, int (&off)[2], int (&idx)[2]) {
+  const bool lo = normal ? l <= 1 : l == 0;  // the tile below reaches it
+  const bool hi = l == 7;                     // the tile above reaches it
+  off[0] = lo ? -1 : 0;
+  idx[0] = lo ? l + 9 : l + 1;
+  off[1] = lo ? 0 : 1;
+  idx[1] = lo ? l + 1 : 0;
+  return lo || hi ? 2 : 1;
 }
 
 // normalisation u = P/m where m > 0 (sparse_ops3d_tp.cpp:126-152), with the
@@ -813,7 +827,7 @@ __device__ __forceinline__ int stage_index(int l, int o, bool normal) {
 // Nodes of blocks the exact activation left inactive are cleared: the splat's
 // FP32 weights may put a negligible contribution where the reference's FP64
 // weight is zero, and inactive blocks stay zero.
-__global__ void k_normalize(DevGrid G, const float2* __restrict__ stage, const int* __restrict__ cell_start,
+__global__ void __launch_bounds__(PF_TV, 2) k_normalize(DevGrid G, const float2* __restrict__ stage, const int* __restrict__ cell_start,
                             int gather, int nslots, int save, int gravity, float dv) {
   __shared__ int splatted[27];
   for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
@@ -836,42 +850,46 @@ __global__ void k_normalize(DevGrid G, const float2* __restrict__ stage, const i
     }
     const int li = threadIdx.x & 7, lj = (threadIdx.x >> 3) & 7, lk = threadIdx.x >> 6;
     const int i = tx * 8 + li, j = ty * 8 + lj, k = tz * 8 + lk;
+    // every load of the three fields first, then the stores (the stores may
+    // alias the field arrays, so interleaving them would serialise the loads)
+    float m[3], u[3];
+    bool act[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       const int f = PF_MU + a;
-      float m = 0.0f, u = 0.0f;
+      act[a] = in_field(G.g, f, i, j, k) && G.act4[f][act4_index(G.g, f, i, j, k)];
+      m[a] = u[a] = 0.0f;
       if (gather) {
         const int FX = a == 0 ? 11 : 10, FY = a == 1 ? 11 : 10;
+        int ox[2], oy[2], oz[2], ix[2], iy[2], iz[2];
+        const int nx = stage_axis(li, a == 0, ox, ix), ny = stage_axis(lj, a == 1, oy, iy),
+                  nz = stage_axis(lk, a == 2, oz, iz);
 #pragma unroll
-        for (int oz = -1; oz <= 1; ++oz) {
-          const int iz = stage_index(lk, oz, a == 2);
-          if (iz < 0) continue;
+        for (int c = 0; c < 2; ++c)
 #pragma unroll
-          for (int oy = -1; oy <= 1; ++oy) {
-            const int iy = stage_index(lj, oy, a == 1);
-            if (iy < 0) continue;
+          for (int b = 0; b < 2; ++b)
 #pragma unroll
-            for (int ox = -1; ox <= 1; ++ox) {
-              const int ix = stage_index(li, ox, a == 0);
-              if (ix < 0 || !splatted[(ox + 1) + 3 * ((oy + 1) + 3 * (oz + 1))]) continue;
-              const int tn = tile_id(G.g, tx + ox, ty + oy, tz + oz);
-              const float2 v = stage[(size_t)tn * kStageTile + a * kStageField + ix + FX * (iy + FY * iz)];
-              u += v.x;
-              m += v.y;
+            for (int d = 0; d < 2; ++d) {
+              if (c >= nz || b >= ny || d >= nx) continue;
+              if (!splatted[(ox[d] + 1) + 3 * ((oy[b] + 1) + 3 * (oz[c] + 1))]) continue;
+              const int tn = tile_id(G.g, tx + ox[d], ty + oy[b], tz + oz[c]);
+              const float2 v = stage[(size_t)tn * kStageTile + a * kStageField + ix[d] + FX * (iy[b] + FY * iz[c])];
+              u[a] += v.x;
+              m[a] += v.y;
             }
-          }
-        }
       } else {
-        m = G.fld[f][o];
-        u = G.fld[PF_U + a][o];
+        m[a] = G.fld[f][o];
+        u[a] = G.fld[PF_U + a][o];
       }
-      const bool act = in_field(G.g, f, i, j, k) && G.act4[f][act4_index(G.g, f, i, j, k)];
-      if (!act) m = u = 0.0f;
-      G.fld[f][o] = m;
-      if (m > 0.0f) u = u / m;
-      if (save) G.saved[a][o] = u;
-      if (a == 1 && gravity && m > 0.0f) u = u + dv;
-      G.fld[PF_U + a][o] = u;
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      float mm = act[a] ? m[a] : 0.0f, uu = act[a] ? u[a] : 0.0f;
+      G.fld[PF_MU + a][o] = mm;
+      if (mm > 0.0f) uu = uu / mm;
+      if (save) G.saved[a][o] = uu;
+      if (a == 1 && gravity && mm > 0.0f) uu = uu + dv;
+      G.fld[PF_U + a][o] = uu;
     }
   }
 }
@@ -1335,8 +1353,11 @@ int mark_cells(pf_ctx* ctx) {
   rc = pool_commit(ctx);
   if (rc) return rc;
   G = dev_grid(ctx);
-  (++ctx->launches), k_mark_walls<<<4 * ctx->num_sms, 256, 0, ctx->stream>>>(G);
-  if (n > 0) (++ctx->launches), k_mark_particles<<<nblocks(n, 256), 256, 0, ctx->stream>>>(G, ctx->px, ctx->py, ctx->pz, n);
+  const uint32_t walls = (uint32_t)(2LL * ctx->g.ny * ctx->g.nz + 2LL * ctx->g.nx * ctx->g.nz + 2LL * ctx->g.nx * ctx->g.ny);
+  (++ctx->launches), k_mark_walls<<<4 * ctx->num_sms, 256, 0, ctx->stream>>>(G, ctx->mk_first);
+  if (n > 0)
+    (++ctx->launches), k_mark_particles<<<nblocks(n, 256), 256, 0, ctx->stream>>>(G, ctx->px, ctx->py, ctx->pz, n,
+                                                                                   ctx->mk_first, walls);
   PF_CUDA_TRY(cudaGetLastError());
   return PF_OK;
 }

@@ -64,6 +64,9 @@ P2G_BYTES_PER_PARTICLE = 29
 P2G_BYTES_PER_FACE = 8       # momentum->velocity + raw mass written once per active face node
 G2P_BYTES_PER_PARTICLE = 37  # read pos+vel+type, write vel
 G2P_BYTES_PER_FACE = 8       # current + saved face velocity read once
+# warp instructions k_splat issues per particle (ncu, profiles/k_splat_bubble128.md): the
+# splat's issue roofline is this count over 148 SMs x 4 schedulers at the SM clock
+SPLAT_WARP_INST_PER_PARTICLE = 42.1
 # Algorithmic bytes per unknown and iteration of the pressure solvers: the
 # arrays each pass reads or writes once (FP64 8 B, FP32 4 B, BF16 2 B, the
 # kind / coarse-class bytes 1 B); a neighbour's value is an L1/L2 hit and is
@@ -97,6 +100,15 @@ def pcg_roofline(pf, cfg, st, peak):
     b = pcg_bytes(pf, cfg, st) * st.n_cells
     gbs = b / max(st.solve_ms / 1000.0, 1e-12) / 1e9
     return {"bytes_per_unknown": pcg_bytes(pf, cfg, st), "achieved_gbs": gbs, "frac": gbs / peak}
+
+
+def issue_roofline(n_particles, splat_ms, sm_mhz, sms=148, schedulers=4):
+    """k_splat against its warp-instruction issue rate at the sampled SM clock."""
+    inst = SPLAT_WARP_INST_PER_PARTICLE * n_particles
+    bound_ms = inst / (sms * schedulers * sm_mhz * 1e6) * 1000.0
+    return {"kernel": "k_splat (P2G)", "warp_inst_per_launch": inst, "issue_bound_ms": bound_ms,
+            "mean_launch_ms": splat_ms, "frac": bound_ms / max(splat_ms, 1e-12), "sm_mhz": sm_mhz,
+            "source": "warp instructions per particle from ncu (profiles/k_splat_bubble128.md)"}
 
 
 def host_info():
@@ -700,7 +712,7 @@ def run_ours(args, rank, world, local, dist):
     import torch
     pf = load_pkg()
     torch.cuda.set_device(local)
-    sc = pf.scenes.bubble_tank(args.n, seed=args.seed + rank)
+    sc = pf.scenes.bubble_tank(args.n, seed=args.seed + rank, level=args.bubble_level)
     ts = TransferStep(pf, sc, local)
     n = ts.n
     # device-resident timing with per-stage events
@@ -718,6 +730,7 @@ def run_ours(args, rank, world, local, dist):
         # end-to-end from pinned host buffers
         ms_e2e, _ = time_steps(ts, args.steps, max(1, args.warmup // 2), dist, local, e2e=True)
     n_faces = ts.active_faces()
+    clk_mhz = clk.summary()["sm_mhz"] or 1965.0
 
     value = whole_job_rate(n, args.steps, world, ms)
     e2e_value = whole_job_rate(n, args.steps, world, ms_e2e)
@@ -748,7 +761,8 @@ def run_ours(args, rank, world, local, dist):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded bubble tank scene)",
-        "config": {"workload": f"bubble_tank_{args.n} transfer stress: P2G(u,v,w,raw mass)+G2P, FLIP 0.97",
+        "config": {"workload": f"bubble_tank_{args.n} transfer stress: P2G(u,v,w,raw mass)+G2P, FLIP 0.97"
+                               + ("" if args.bubble_level == 0.7 else f", water level {args.bubble_level}"),
                    "grid": [args.n] * 3, "tile": 8, "particles_per_gpu": n, "global_particles": n * world,
                    "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (particle SoA %.0f MB per GPU)" % (n * 29 / 1e6)},
@@ -756,6 +770,8 @@ def run_ours(args, rank, world, local, dist):
         "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                      "algorithmic_bytes_per_launch": kbytes, "mean_launch_ms": kms},
+        # the splat's true bound: warp-instruction issue (HBM bytes are a few percent of the peak)
+        "issue_roofline": issue_roofline(n, splat_ms, clk_mhz),
         "stages_ms_per_step": {k: v[0] / max(args.steps, 1) for k, v in stages.items() if v[1]},
         "gpu_launches": int(launches) * world,
         "clocks": clk.summary(),
@@ -799,7 +815,8 @@ def run_reference(args, rank, world):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000.0 * total / len(times), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded bubble tank scene)", "impl": "reference",
-        "config": {"workload": f"bubble_tank_{args.n} transfer stress: P2G(u,v,w,raw mass)+G2P, FLIP 0.97",
+        "config": {"workload": f"bubble_tank_{args.n} transfer stress: P2G(u,v,w,raw mass)+G2P, FLIP 0.97"
+                               + ("" if args.bubble_level == 0.7 else f", water level {args.bubble_level}"),
                    "grid": [args.n] * 3, "sample_particles": np_s},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": min(8, host_info()["affinity_cpus"] or 1),
                          "kind": "reference", "host": host_info(),
@@ -818,6 +835,9 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--n", type=int, default=128, help="grid cells per axis (128 is the benchmarked workload)")
+    ap.add_argument("--bubble-level", type=float, default=0.7,
+                    help="water level of the transfer scene (0.7 is the benchmarked workload; lower levels give "
+                         "smaller cases of the same kernels for profiling)")
     ap.add_argument("--cpu-slab", type=int, default=4, help="x-columns of the scene in the CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the PCG, full-step and adaptivity blocks")

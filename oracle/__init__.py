@@ -244,6 +244,7 @@ def ref_lib():
     lib.pfr_set_field.argtypes = [vp, C.c_int, _fp, _up]
     lib.pfr_active_block_ids.argtypes = [vp, C.c_int, C.c_void_p, C.POINTER(C.c_size_t)]
     lib.pfr_collect_cells.argtypes = [vp, C.c_int, C.c_void_p, C.POINTER(C.c_size_t)]
+    lib.pfr_write_render_cache.argtypes = [vp, C.c_char_p, C.c_int, C.c_double, C.c_double, _dp, C.c_double, _dp]
     lib.pfr_set_particles.argtypes = [vp, C.c_size_t, _dp, _dp, _up, _dp]
     lib.pfr_num_particles.restype = C.c_size_t
     lib.pfr_num_particles.argtypes = [vp]
@@ -390,6 +391,15 @@ class ReferenceGrid(_GridBase):
         if self.lib.pfr_collect_cells(self.h, int(marker), out.ctypes.data, C.byref(n)) != 0:
             raise RuntimeError("pfr_collect_cells failed")
         return out[: n.value].astype(np.int64)
+
+    def write_render_cache(self, path, frame, time, dt, pp: PhaseParams, Vp, camera):
+        """writeSparseRenderCache3D (src/driver/render_cache3d.h:617-663) of this grid and its particles;
+        camera: 13 doubles (position, target, up, fov, near, far, focal length)."""
+        cam = np.ascontiguousarray(camera, np.float64)
+        rc = self.lib.pfr_write_render_cache(self.h, str(path).encode(), int(frame), float(time), float(dt),
+                                             pp.as_array(), float(Vp), cam)
+        if rc != 0:
+            raise RuntimeError("writeSparseRenderCache3D failed")
 
     def _put(self, ps: Particles):
         self.lib.pfr_set_particles(self.h, len(ps), ps.pos, ps.vel, ps.type, ps.volume)

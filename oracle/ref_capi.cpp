@@ -15,10 +15,12 @@
 //   diagnoseSparseInterface3D (src/driver/interface_diagnostics3d.cpp:363-379)
 //   applySparseSurfaceTension3D (src/driver/interface_diagnostics3d.cpp:405-447)
 //   sparse3d::collectCellsWithMarker (src/driver/sparse_ops3d_common.h:65-85)
+//   writeSparseRenderCache3D (src/driver/render_cache3d.h:617-663)
 // and converts between its SparseMacGrid3D<4> block pool and dense arrays
 // plus one activity byte per 4^3 block.
 #include "driver/interface_diagnostics3d.h"
 #include "driver/particle_adaptivity3d.h"
+#include "driver/render_cache3d.h"
 #include "driver/sparse_ops3d_common.h"
 #include "driver/sparse_ops3d_tp.h"
 #include "driver/sparse_sim3d_tp.h"
@@ -128,6 +130,32 @@ int pfr_collect_cells(void* hp, int marker, int* out, size_t* n) {
     std::memcpy(out, cells.data(), cells.size() * sizeof(int));
   }
   *n = cells.size();
+  return 0;
+}
+
+// writeSparseRenderCache3D on this handle's simulation state, with phase, Vp
+// and the last effective dt as given.  cam: position, target, up (3 doubles
+// each), fov_degrees, near_clip, far_clip, focal_length_mm.  Returns -1 if
+// the writer throws (an invalid path or metadata), 0 otherwise.
+int pfr_write_render_cache(void* hp, const char* path, int frame, double time, double dt, const double* phase,
+                           double Vp, const double* cam) {
+  SparseSim3DTP& s = static_cast<Handle*>(hp)->sim;
+  s.phase = phaseOf(phase);
+  s.Vp = Vp;
+  s.effective_dt_last = dt;
+  RenderCacheCamera3D c;
+  c.position = Vec3{cam[0], cam[1], cam[2]};
+  c.target = Vec3{cam[3], cam[4], cam[5]};
+  c.up = Vec3{cam[6], cam[7], cam[8]};
+  c.fov_degrees = cam[9];
+  c.near_clip = cam[10];
+  c.far_clip = cam[11];
+  c.focal_length_mm = cam[12];
+  try {
+    writeSparseRenderCache3D(s, path, frame, time, c);
+  } catch (...) {
+    return -1;
+  }
   return 0;
 }
 

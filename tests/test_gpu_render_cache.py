@@ -1,15 +1,16 @@
-"""Render-cache export (src/driver/render_cache3d.h:551-600) on the GPU
-against a restatement of the reference writer's selection and number format.
+"""Render-cache export (src/driver/render_cache3d.h:551-600) on the GPU.
 
-The drop-in compacts the phase cells on the device and formats the JSONL on
-the host with std::ostream at 17 significant digits, which prints a double as
-printf's %.17g does.  The expected lines are built here from the oracle grid
-the GPU grid was loaded from: sparsePhaseCells (:497-526; cells of active
-4^3 marker blocks with marker != 0 or phi > 1e-8, phi the sequential mean of
-the six faces' phiFromRawDensity) and writeParticleSection (:541-560).  The
-reference lists marker blocks in activation order and the drop-in in
-ascending block id, so the cell lines are compared as sorted lists.
+1. Byte for byte against the reference's own writer (writeSparseRenderCache3D,
+   compiled into oracle/_ref): the reference runs its own markCells on the
+   same particles -- its marker blocks then sit in their first-touch order,
+   the order it lists phase cells in -- and is given the GPU's face fields and
+   particles; both files must be identical, the liquid-volume sum included.
+2. Against a restatement of the writer's selection and number format
+   (sparsePhaseCells, :497-526, and writeParticleSection, :541-560), on a grid
+   imported from the oracle.
+3. The metadata checks and the empty-grid sections.
 """
+import ctypes as C
 import json
 
 import numpy as np
@@ -86,6 +87,48 @@ def _expected_particles(ps, Vp):
     return out
 
 
+@pytest.mark.skipif(not O.reference_available(), reason="compiled reference (oracle/_ref) not built")
+@pytest.mark.parametrize("scene,n,seed", [("rayleigh_taylor", 16, 3), ("bubble_tank", 20, 5)])
+def test_render_cache_equals_reference_writer(pf, tmp_path, scene, n, seed):
+    sc = getattr(pf.scenes, scene)(n, seed=seed)
+    pp = phase_for(sc, pf)
+    ps = scene_particles(sc)
+    opp = to_oracle_phase(pp)
+    dt, frame, time = 1 / 240, 4, 0.5
+    # GPU: markCells and P2G of the scene
+    sim = pf.SparseSim3DTP(n, n, n, 1.0 / n, max_particles=len(ps))
+    sim.phase, sim.Vp, sim.effective_dt_last = pp, 1.0, dt
+    sim.set_particles(sc["pos"], sc["vel"], sc["type"], sc["volume"])
+    lib = pf.load()
+    pf._lib.check(lib.pf_mark_cells(sim.grid.ctx), sim.grid.ctx, "pf_mark_cells")
+    pf._lib.check(lib.pf_p2g(sim.grid.ctx, C.byref(pp._c()), 1.0), sim.grid.ctx, "pf_p2g")
+    # reference: its own step marks the cells of the same particles (marker
+    # blocks in first-touch order); then the GPU's fields and particles
+    rg = O.ReferenceGrid(n, n, n, 1.0 / n)
+    O.Reference().step(rg, ps.copy(), opp, dict(dt=dt, gravity=-9.81, Vp=1.0, alpha_l=0.95, alpha_g=0.95,
+                                                cg_iters=50, cg_tol=1e-7))
+    dg, ag = sim.grid.get_field(pf.PF_MK)
+    dr, ar = rg.get_field(O.MK)
+    assert np.array_equal(dg, dr) and np.array_equal(ag, ar)
+    for f in range(7):
+        rg.set_field(f, *sim.grid.get_field(f))
+    pos, vel, typ, vol = sim.get_particles()
+    rg._put(O.Particles(pos.astype(np.float64), vel.astype(np.float64), typ, vol.astype(np.float64)))
+    cam = pf.defaultRenderCacheCamera3D(n, n, n, 1.0 / n)
+    a, b = tmp_path / "gpu.jsonl", tmp_path / "ref.jsonl"
+    pf.writeSparseRenderCache3D(sim, a, frame, time, cam)
+    rg.write_render_cache(b, frame, time, dt, opp, 1.0,
+                          list(cam.position) + list(cam.target) + list(cam.up) +
+                          [cam.fov_degrees, cam.near_clip, cam.far_clip, cam.focal_length_mm])
+    ta, tb = a.read_text(), b.read_text()
+    la, lb = ta.splitlines(), tb.splitlines()
+    assert len(la) == len(lb)
+    bad = [(i, x, y) for i, (x, y) in enumerate(zip(la, lb)) if x != y]
+    assert not bad, bad[:3]
+    assert ta == tb
+    sim.grid.close()
+
+
 @pytest.mark.parametrize("n,seed", [(16, 3), (12, 5)])
 def test_render_cache_matches_restated_writer(pf, tmp_path, n, seed):
     sim, go, ps, pp = _state(pf, n, seed)
@@ -95,6 +138,8 @@ def test_render_cache_matches_restated_writer(pf, tmp_path, n, seed):
     rest, cells = _split(a)
     exp = _expected_cells(go, pp)
     assert len(cells) == len(exp) > 0
+    # the set and the number format (the order is checked against the
+    # reference's writer above)
     assert sorted(cells) == sorted(exp)
     parts = [ln for ln in rest if ln.startswith('{"section":"particle",')]
     assert parts == _expected_particles(ps, 1.0)
