@@ -48,6 +48,13 @@ struct AdaptScratch {
   int* sorted = nullptr;     // [cap] per-cell lists in the reference's order
   int* d_stats = nullptr;    // [16]
   int* h_stats = nullptr;    // [16] pinned
+  // the step controls' two reductions (max speed, liquid volume), copied back
+  // behind ctl_ev; a deferred read keeps the dt and settings it is for
+  double* h_ctl = nullptr;   // [2] pinned
+  cudaEvent_t ctl_ev = nullptr;
+  bool ctl_pending = false;
+  double ctl_dt = 0.0;
+  pf_step_controls ctl_cfg{};
 };
 
 int scratch(pf_ctx* ctx, AdaptScratch** out) {
@@ -66,6 +73,8 @@ int scratch(pf_ctx* ctx, AdaptScratch** out) {
     PF_CUDA_TRY(cudaMalloc(&s->sorted, (s->cap + 1) * sizeof(int)));
     PF_CUDA_TRY(cudaMalloc(&s->d_stats, 16 * sizeof(int)));
     PF_CUDA_TRY(cudaMallocHost(&s->h_stats, 16 * sizeof(int)));
+    PF_CUDA_TRY(cudaMallocHost(&s->h_ctl, 2 * sizeof(double)));
+    PF_CUDA_TRY(cudaEventCreateWithFlags(&s->ctl_ev, cudaEventDisableTiming));
   }
   *out = s;
   return PF_OK;
@@ -624,8 +633,11 @@ int apply_adaptivity(pf_ctx* ctx, const pf_adapt_cfg& a, pf_adapt_stats* st) {
 // updateVolumeCorrectionStats (src/driver/sparse_sim3d_tp.cpp:368-379): the
 // step's dt and divergence correction from two device reductions.  The max
 // speed is exact; the liquid volume is an FP64 sum in another order than the
-// reference's particle order.
-int step_controls(pf_ctx* ctx, double dt, double Vp, const pf_step_controls& c, pf_step_control_stats* st) {
+// reference's particle order.  With wait == false (neither control changes
+// the step) the reductions are read back behind an event and turned into
+// statistics by step_controls_finish.
+int step_controls(pf_ctx* ctx, double dt, double Vp, const pf_step_controls& c, pf_step_control_stats* st,
+                  bool wait) {
   AdaptScratch* s = nullptr;
   int rc = scratch(ctx, &s);
   if (rc) return rc;
@@ -637,9 +649,30 @@ int step_controls(pf_ctx* ctx, double dt, double Vp, const pf_step_controls& c, 
   (++ctx->launches), k_particle_reduce<<<nb, kNT, 0, ctx->stream>>>(particles_of(ctx), n, Vp, part);
   (++ctx->launches), k_particle_reduce_total<<<1, 1, 0, ctx->stream>>>(part, nb, out);
   PF_CUDA_TRY(cudaGetLastError());
-  double h[2];
-  PF_CUDA_TRY(cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
-  PF_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  PF_CUDA_TRY(cudaMemcpyAsync(s->h_ctl, out, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  PF_CUDA_TRY(cudaEventRecord(s->ctl_ev, ctx->stream));
+  s->ctl_pending = true;
+  s->ctl_dt = dt;
+  s->ctl_cfg = c;
+  if (!wait) {
+    // the step goes on with the requested dt, which is what the statistics will say
+    pf_step_control_stats o{};
+    o.requested_dt = o.effective_dt = o.cfl_limit_dt = dt;
+    if (st) *st = o;
+    return PF_OK;
+  }
+  rc = step_controls_finish(ctx, st);
+  return rc;
+}
+
+int step_controls_finish(pf_ctx* ctx, pf_step_control_stats* st) {
+  AdaptScratch* s = static_cast<AdaptScratch*>(ctx->adapt);
+  if (!s || !s->ctl_pending) return PF_OK;
+  PF_CUDA_TRY(cudaEventSynchronize(s->ctl_ev));
+  s->ctl_pending = false;
+  const double* h = s->h_ctl;
+  const double dt = s->ctl_dt;
+  const pf_step_controls& c = s->ctl_cfg;
   pf_step_control_stats o{};
   o.requested_dt = o.effective_dt = o.cfl_limit_dt = dt;
   o.max_particle_speed = h[0];
@@ -672,6 +705,8 @@ void adapt_free(pf_ctx* ctx) {
   cudaFree(s->sorted);
   cudaFree(s->d_stats);
   cudaFreeHost(s->h_stats);
+  cudaFreeHost(s->h_ctl);
+  if (s->ctl_ev) cudaEventDestroy(s->ctl_ev);
   delete s;
   ctx->adapt = nullptr;
 }

@@ -80,6 +80,7 @@ void free_all(pf_ctx* c) {
   if (c->h_pinned_ints) cudaFreeHost(c->h_pinned_ints);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->pool_ev) cudaEventDestroy(c->pool_ev);
   if (c->stream) cudaStreamDestroy(c->stream);
 }
 
@@ -205,6 +206,8 @@ int create_impl(pf_ctx* ctx, const pf_grid_desc* d) {
   PF_CUDA_TRY(cudaMalloc(&ctx->ctl_outer, sizeof(SolveCtl)));
   PF_CUDA_TRY(cudaMemset(ctx->ctl_outer, 0, sizeof(SolveCtl)));
   PF_CUDA_TRY(cudaMallocHost(&ctx->h_pinned_ints, 64 * sizeof(int)));
+  ctx->h_nslots = ctx->h_pinned_ints + 32;  // the deferred pool-size read-back; no other use of that entry
+  PF_CUDA_TRY(cudaEventCreateWithFlags(&ctx->pool_ev, cudaEventDisableTiming));
   PF_CUDA_TRY(cudaMalloc(&ctx->d_clamp, 8 * sizeof(int)));
   PF_CUDA_TRY(cudaMalloc(&ctx->d_flags, 2 * cap * sizeof(int)));
   size_t cf = 2 * (size_t)ncell + 2;
@@ -282,7 +285,15 @@ void* pf_stream(pf_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 
 size_t pf_num_particles(const pf_ctx* ctx) { return ctx ? (ctx->up_pending ? ctx->np_next : ctx->np) : 0; }
 
-int pf_active_tiles(const pf_ctx* ctx) { return ctx ? ctx->nslots : -1; }
+// the pool size lives on the device until read back; reading it here waits
+// for that copy (the only state this changes)
+int pf_active_tiles(const pf_ctx* ctx) {
+  if (!ctx) return -1;
+  pf_ctx* c = const_cast<pf_ctx*>(ctx);
+  cudaSetDevice(c->device);
+  if (pool_sync(c)) return -1;
+  return c->nslots;
+}
 
 // Swap in the particle set of a pending asynchronous upload: the context
 // stream waits for it, and the set it replaces becomes free for the next
@@ -521,7 +532,8 @@ int pf_grid_copy(pf_ctx* dst, const pf_ctx* src) {
   pf_ctx* ctx = dst;
   cudaSetDevice(ctx->device);
   PF_CUDA_TRY(cudaStreamSynchronize(src->stream));
-  int rc = pool_reset(dst);
+  int rc = pool_sync(const_cast<pf_ctx*>(src));  // the source's pool size, read back
+  if (!rc) rc = pool_reset(dst);
   if (rc) return rc;
   const size_t nt = (size_t)a.ntiles;
   const size_t cells = (size_t)src->nslots * PF_TV;
@@ -631,10 +643,11 @@ int pf_advect(pf_ctx* ctx, double dt, int order, pf_clamp_stats* stats, double* 
 // SparseSim3DTP::step() order (src/driver/sparse_sim3d_tp.cpp:854-884):
 // markCells, P2G, saved copy, gravity, walls, projection, G2P, advection.
 // The grid holds nothing across steps, so the pool is rebuilt from scratch.
-int pf_step(pf_ctx* ctx, const pf_step_cfg* cfg, pf_step_stats* stats) {
-  if (!ctx || !cfg || check_solve_cfg(&cfg->solve)) return PF_ERR_INVALID;
-  if (cfg->advect_order != 2 && cfg->advect_order != 3) return PF_ERR_INVALID;
-  cudaSetDevice(ctx->device);
+// Up to the projection nothing waits for the device: the pool grows on the
+// device, and the step-control and interface statistics are read back behind
+// events once the solve has synchronised anyway (unless the adaptive timestep
+// or the volume correction needs them first, or adaptivity is on).
+static int step_impl(pf_ctx* ctx, const pf_step_cfg* cfg, pf_step_stats* stats) {
   int rc = take_upload(ctx);
   if (rc) return rc;
   // applyParticleAdaptivity comes first in SparseSim3DTP::step()
@@ -643,7 +656,8 @@ int pf_step(pf_ctx* ctx, const pf_step_cfg* cfg, pf_step_stats* stats) {
     if (rc) return rc;
   }
   // then computeAdaptiveParticleTimestep3D and updateVolumeCorrectionStats
-  rc = pf::step_controls(ctx, cfg->dt, cfg->Vp, ctx->controls, &ctx->controls_last);
+  const bool controls_now = ctx->controls.adaptive_timestep || ctx->controls.c_div_volume_correction;
+  rc = pf::step_controls(ctx, cfg->dt, cfg->Vp, ctx->controls, &ctx->controls_last, controls_now);
   if (rc) return rc;
   const double dt = ctx->controls_last.effective_dt;
   pf_solve_cfg solve = cfg->solve;
@@ -654,7 +668,7 @@ int pf_step(pf_ctx* ctx, const pf_step_cfg* cfg, pf_step_stats* stats) {
   if (rc) return rc;
   rc = pf::p2g(ctx, &cfg->phase, cfg->Vp);  // normalisation without the fused extras
   if (rc) return rc;
-  rc = pf::interface_diagnostics(ctx, &cfg->phase, nullptr);  // diagnoseSparseInterface3D after P2G
+  rc = pf::interface_diagnostics(ctx, &cfg->phase, nullptr, false);  // diagnoseSparseInterface3D after P2G
   if (rc) return rc;
   rc = pf::save_velocity(ctx);
   if (rc) return rc;
@@ -674,12 +688,27 @@ int pf_step(pf_ctx* ctx, const pf_step_cfg* cfg, pf_step_stats* stats) {
   pf_clamp_stats cst{};
   rc = pf::g2p_advect(ctx, cfg->alpha_l, cfg->alpha_g, dt, cfg->advect_order, &cst);
   if (rc) return rc;
+  rc = pool_sync(ctx);
+  if (rc) return rc;
   if (stats) {
     stats->solve = sst;
     stats->clamp = cst;
     stats->active_tiles = ctx->nslots;
   }
   return PF_OK;
+}
+
+int pf_step(pf_ctx* ctx, const pf_step_cfg* cfg, pf_step_stats* stats) {
+  if (!ctx || !cfg || check_solve_cfg(&cfg->solve)) return PF_ERR_INVALID;
+  if (cfg->advect_order != 2 && cfg->advect_order != 3) return PF_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  int rc = step_impl(ctx, cfg, stats);
+  // the deferred read-backs complete on every path
+  const int r1 = pf::step_controls_finish(ctx, &ctx->controls_last);
+  const int r2 = pf::interface_diagnostics_finish(ctx);
+  const int r3 = pool_sync(ctx);
+  if (!rc) rc = r1 ? r1 : r2 ? r2 : r3;
+  return rc;
 }
 
 int pf_calibrate_rho_tilde0(pf_ctx* ctx, const pf_phase* phase, double Vp, double* out) {

@@ -21,6 +21,13 @@ struct pf_ctx {
   int* slot_tile = nullptr;   // [ntiles] slot -> tile
   int nslots = 0;             // host copy of the pool size
   int* d_nslots = nullptr;    // device copy
+  // The pool grows without a host round trip: pool_commit leaves the new size
+  // on the device (slot loops read d_nslots, their grids are sized to
+  // capacity) and copies it to h_nslots behind pool_ev; pool_sync waits for
+  // that copy before the host uses nslots again.
+  bool pool_pending = false;
+  int* h_nslots = nullptr;    // pinned
+  cudaEvent_t pool_ev = nullptr;
   uint8_t* tile_need = nullptr;  // [ntiles] activation requests
   int* tile_new = nullptr;       // [ntiles] scratch for slot assignment
   int* tile_rank = nullptr;      // [ntiles] scratch for slot assignment
@@ -146,8 +153,10 @@ int scan_alloc(pf_ctx* ctx, size_t max_n);
 
 // pool.cu
 int pool_reset(pf_ctx* ctx);
-int pool_commit(pf_ctx* ctx);  // give slots to requested tiles, read back nslots
-int field_clear(pf_ctx* ctx, int f);
+int pool_commit(pf_ctx* ctx);  // give slots to requested tiles; the new size stays on the device
+int pool_sync(pf_ctx* ctx);    // wait for a deferred nslots read-back
+int slot_blocks(const pf_ctx* ctx, int cap);  // grid for a slot loop reading d_nslots
+int field_clear(pf_ctx* ctx, int f, bool data = true);
 int request_wall_tiles(pf_ctx* ctx);
 DevGrid dev_grid(const pf_ctx* ctx);
 int grid_set_field(pf_ctx* ctx, int f, const float* dense, const uint8_t* act4);
@@ -177,11 +186,14 @@ int coarsen_particles(pf_ctx* ctx, int ptype, int target, unsigned seed, pf_coar
 int refill_liquid(pf_ctx* ctx, int target, unsigned seed, int interface_only, int interface_radius, int max_added,
                   pf_refill_stats* st);
 int apply_adaptivity(pf_ctx* ctx, const pf_adapt_cfg& cfg, pf_adapt_stats* st);
-int step_controls(pf_ctx* ctx, double dt, double Vp, const pf_step_controls& c, pf_step_control_stats* st);
+int step_controls(pf_ctx* ctx, double dt, double Vp, const pf_step_controls& c, pf_step_control_stats* st,
+                  bool wait = true);
+int step_controls_finish(pf_ctx* ctx, pf_step_control_stats* st);  // statistics of a wait == false launch
 void adapt_free(pf_ctx* ctx);
 
 // diag.cu
-int interface_diagnostics(pf_ctx* ctx, const pf_phase* ph, pf_interface_stats* st);
+int interface_diagnostics(pf_ctx* ctx, const pf_phase* ph, pf_interface_stats* st, bool wait = true);
+int interface_diagnostics_finish(pf_ctx* ctx);  // statistics of a launch made with wait == false
 int surface_tension(pf_ctx* ctx, const pf_phase* ph, double dt, double strength, double max_dv, int radius,
                     pf_surface_stats* st);
 void diag_free(pf_ctx* ctx);

@@ -45,6 +45,8 @@ struct DiagScratch {
   DiagPartial* part = nullptr;   // [kDiagBlocks]
   DiagPartial* total = nullptr;  // [1]
   DiagPartial* h_total = nullptr;
+  cudaEvent_t copied = nullptr;  // h_total holds the last launch's totals
+  bool pending = false;          // ... not yet turned into ctx->diag_last
   // surface tension (allocated on first use)
   float* h = nullptr;        // [ncell][3] FP32 half velocity changes
   uint8_t* ok = nullptr;     // [ncell] cell applies its change
@@ -344,6 +346,7 @@ int scratch(pf_ctx* ctx, DiagScratch** out) {
     PF_CUDA_TRY(cudaMalloc(&s->part, kDiagBlocks * sizeof(DiagPartial)));
     PF_CUDA_TRY(cudaMalloc(&s->total, sizeof(DiagPartial)));
     PF_CUDA_TRY(cudaMallocHost(&s->h_total, sizeof(DiagPartial)));
+    PF_CUDA_TRY(cudaEventCreateWithFlags(&s->copied, cudaEventDisableTiming));
   }
   *out = s;
   return PF_OK;
@@ -351,7 +354,10 @@ int scratch(pf_ctx* ctx, DiagScratch** out) {
 
 }  // namespace
 
-int interface_diagnostics(pf_ctx* ctx, const pf_phase* ph, pf_interface_stats* st) {
+// With wait == false the totals are copied back behind an event and turned
+// into statistics by interface_diagnostics_finish, so that the caller's
+// stream keeps going.
+int interface_diagnostics(pf_ctx* ctx, const pf_phase* ph, pf_interface_stats* st, bool wait) {
   StageScope stage(ctx, PF_STAGE_DIAG);
   DiagScratch* s = nullptr;
   int rc = scratch(ctx, &s);
@@ -368,7 +374,19 @@ int interface_diagnostics(pf_ctx* ctx, const pf_phase* ph, pf_interface_stats* s
   (++ctx->launches), k_diag_total<<<1, kDiagNT, 0, ctx->stream>>>(s->part, nb, s->total);
   PF_CUDA_TRY(cudaGetLastError());
   PF_CUDA_TRY(cudaMemcpyAsync(s->h_total, s->total, sizeof(DiagPartial), cudaMemcpyDeviceToHost, ctx->stream));
-  PF_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  PF_CUDA_TRY(cudaEventRecord(s->copied, ctx->stream));
+  s->pending = true;
+  if (!wait) return PF_OK;
+  rc = interface_diagnostics_finish(ctx);
+  if (!rc && st) *st = ctx->diag_last;
+  return rc;
+}
+
+int interface_diagnostics_finish(pf_ctx* ctx) {
+  DiagScratch* s = static_cast<DiagScratch*>(ctx->idiag);
+  if (!s || !s->pending) return PF_OK;
+  PF_CUDA_TRY(cudaEventSynchronize(s->copied));
+  s->pending = false;
   const DiagPartial& t = *s->h_total;
   // finishStats (:55-66)
   pf_interface_stats out{};
@@ -384,7 +402,6 @@ int interface_diagnostics(pf_ctx* ctx, const pf_phase* ph, pf_interface_stats* s
   out.curvature_abs_max = t.curv_max;
   out.surface_tension_candidate = (t.finite && t.interface > 0 && t.grad_max > 1e-5) ? 1 : 0;
   ctx->diag_last = out;
-  if (st) *st = out;
   return PF_OK;
 }
 
@@ -429,6 +446,8 @@ int surface_tension(pf_ctx* ctx, const pf_phase* ph, double dt, double strength,
                                                                          out.curvature_smoothing_radius, s->h, s->ok,
                                                                          s->bad, s->spart);
     (++ctx->launches), k_surface_total<<<1, kDiagNT, 0, ctx->stream>>>(s->spart, nb, s->spart + nb);
+    rc = pool_sync(ctx);
+    if (rc) return rc;
     if (ctx->nslots > 0)
       (++ctx->launches), k_surface_faces<<<std::min(ctx->nslots, 64 * ctx->num_sms), PF_TV, 0, ctx->stream>>>(
           G, ctx->nslots, s->h, s->ok, s->bad);
@@ -463,6 +482,7 @@ void diag_free(pf_ctx* ctx) {
   cudaFree(s->part);
   cudaFree(s->total);
   cudaFreeHost(s->h_total);
+  if (s->copied) cudaEventDestroy(s->copied);
   delete s;
   ctx->idiag = nullptr;
 }

@@ -154,6 +154,8 @@ __global__ void k_pool_reset(DevGrid G, int* tile_slot, int nslots) {
 }
 
 int pool_reset(pf_ctx* ctx) {
+  int rc = pool_sync(ctx);
+  if (rc) return rc;
   if (ctx->nslots > 0) {
     const int nb = ctx->nslots < 4 * ctx->num_sms ? ctx->nslots : 4 * ctx->num_sms;
     (++ctx->launches), k_pool_reset<<<nb, PF_TV, 0, ctx->stream>>>(dev_grid(ctx), ctx->tile_slot, ctx->nslots);
@@ -199,12 +201,26 @@ int pool_commit(pf_ctx* ctx) {
                                                           ctx->slot_tile, ctx->d_nslots, n);
   (++ctx->launches), k_bump_nslots<<<1, 1, 0, ctx->stream>>>(ctx->d_nslots, ctx->d_scalar);
   PF_CUDA_TRY(cudaGetLastError());
-  PF_CUDA_TRY(cudaMemcpyAsync(ctx->h_pinned_ints, ctx->d_nslots, sizeof(int), cudaMemcpyDeviceToHost,
-                              ctx->stream));
-  PF_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-  ctx->nslots = ctx->h_pinned_ints[0];
-  if (ctx->nslots < 0 || ctx->nslots > n) return set_error(ctx, PF_ERR_INVALID, "pool size out of range");
+  PF_CUDA_TRY(cudaMemcpyAsync(ctx->h_nslots, ctx->d_nslots, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  PF_CUDA_TRY(cudaEventRecord(ctx->pool_ev, ctx->stream));
+  ctx->pool_pending = true;
   return PF_OK;
+}
+
+int pool_sync(pf_ctx* ctx) {
+  if (!ctx->pool_pending) return PF_OK;
+  PF_CUDA_TRY(cudaEventSynchronize(ctx->pool_ev));
+  ctx->pool_pending = false;
+  ctx->nslots = *ctx->h_nslots;
+  if (ctx->nslots < 0 || ctx->nslots > ctx->g.ntiles) return set_error(ctx, PF_ERR_INVALID, "pool size out of range");
+  return PF_OK;
+}
+
+// A grid-stride slot loop that reads the pool size from d_nslots: the host's
+// nslots when it is current, else `cap` CTAs (the pool may have grown).
+int slot_blocks(const pf_ctx* ctx, int cap) {
+  if (ctx->pool_pending) return cap;
+  return ctx->nslots < cap ? ctx->nslots : cap;
 }
 
 __global__ void k_request_list(uint8_t* need, const int* tiles, int n) {
@@ -227,8 +243,14 @@ __global__ void k_zero_field(float* f, int nslots) {
 
 // SparseBlockGrid3D::clear (src/grid/sparse_block_grid3d.h:64-67) with the
 // zero-fill that reactivation performs.
-int field_clear(pf_ctx* ctx, int f) {
-  if (ctx->nslots > 0)
+// With data == false only the activity is reset: the caller overwrites every
+// pooled node of the field afterwards.
+int field_clear(pf_ctx* ctx, int f, bool data) {
+  if (data) {
+    int rc = pool_sync(ctx);
+    if (rc) return rc;
+  }
+  if (data && ctx->nslots > 0)
     PF_CUDA_TRY(cudaMemsetAsync(ctx->fld[f], 0, (size_t)ctx->nslots * PF_TV * sizeof(float), ctx->stream));
   PF_CUDA_TRY(cudaMemsetAsync(ctx->act4[f], 0, ctx->act4_n[f], ctx->stream));
   if (f == PF_MK && ctx->mk_first)
@@ -338,6 +360,7 @@ int grid_set_field(pf_ctx* ctx, int f, const float* dense, const uint8_t* act4) 
   if (f == PF_MK) (++ctx->launches), k_first_from_act<<<nblocks(nb, 256), 256, 0, ctx->stream>>>(ctx->act4[f], nb, ctx->mk_first);
   PF_CUDA_TRY(cudaGetLastError());
   int rc = pool_commit(ctx);
+  if (!rc) rc = pool_sync(ctx);
   if (rc) return rc;
   if (ctx->nslots > 0)
     (++ctx->launches), k_import_field<<<ctx->nslots, PF_TV, 0, ctx->stream>>>(dev_grid(ctx), f, d_dense, ctx->nslots);
@@ -352,6 +375,8 @@ int grid_get_field(pf_ctx* ctx, int f, float* dense, uint8_t* act4) {
   if (nn * sizeof(float) > ctx->staging_bytes) return set_error(ctx, PF_ERR_INVALID, "field larger than staging");
   float* d_dense = (float*)ctx->staging;
   if (dense) {
+    int rc = pool_sync(ctx);
+    if (rc) return rc;
     PF_CUDA_TRY(cudaMemsetAsync(d_dense, 0, nn * sizeof(float), ctx->stream));
     if (ctx->nslots > 0)
       (++ctx->launches), k_export_field<<<ctx->nslots, PF_TV, 0, ctx->stream>>>(dev_grid(ctx), f, d_dense, ctx->nslots);

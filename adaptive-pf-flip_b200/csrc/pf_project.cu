@@ -229,7 +229,7 @@ int project(pf_ctx* ctx, const pf_phase* ph, double dt, const pf_solve_cfg* cfg,
   StageScope stage(ctx, PF_STAGE_PROJECT);
   pf_solve_stats local{};
   local.pin_cell = -1;
-  int rc = field_clear(ctx, PF_P);
+  int rc = field_clear(ctx, PF_P);  // waits for any pending pool growth
   if (rc) return rc;
   // pool the tiles of every fluid-cell face (no-op inside a step)
   if (ctx->nslots > 0) {
@@ -237,6 +237,7 @@ int project(pf_ctx* ctx, const pf_phase* ph, double dt, const pf_solve_cfg* cfg,
     PF_CUDA_TRY(cudaGetLastError());
   }
   rc = pool_commit(ctx);
+  if (!rc) rc = pool_sync(ctx);
   if (rc) return rc;
   const int nslots = ctx->nslots;
   if (nslots == 0) { if (st) *st = local; return PF_OK; }

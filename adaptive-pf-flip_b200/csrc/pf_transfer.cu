@@ -828,8 +828,9 @@ __device__ __forceinline__ int stage_axis(int l, bool normal, int (&off)[2], int
 // FP32 weights may put a negligible contribution where the reference's FP64
 // weight is zero, and inactive blocks stay zero.
 __global__ void __launch_bounds__(PF_TV, 2) k_normalize(DevGrid G, const float2* __restrict__ stage, const int* __restrict__ cell_start,
-                            int gather, int nslots, int save, int gravity, float dv) {
+                            int gather, const int* __restrict__ d_nslots, int save, int gravity, float dv) {
   __shared__ int splatted[27];
+  const int nslots = *d_nslots;
   for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
     const size_t o = (size_t)s * PF_TV + threadIdx.x;
     const int t = G.slot_tile[s];
@@ -894,7 +895,8 @@ __global__ void __launch_bounds__(PF_TV, 2) k_normalize(DevGrid G, const float2*
   }
 }
 
-__global__ void k_save(DevGrid G, int nslots) {
+__global__ void k_save(DevGrid G, const int* __restrict__ d_nslots) {
+  const int nslots = *d_nslots;
   for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
     const size_t o = (size_t)s * PF_TV + threadIdx.x;
 #pragma unroll
@@ -902,7 +904,8 @@ __global__ void k_save(DevGrid G, int nslots) {
   }
 }
 
-__global__ void k_gravity(DevGrid G, int nslots, float dv) {
+__global__ void k_gravity(DevGrid G, const int* __restrict__ d_nslots, float dv) {
+  const int nslots = *d_nslots;
   for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
     const size_t o = (size_t)s * PF_TV + threadIdx.x;
     if (G.fld[PF_MV][o] > 0.0f) {
@@ -1268,6 +1271,219 @@ __global__ void __launch_bounds__(256) k_advect(DevGrid G, ParticlePtrs P, int n
   warp_count(counters, 7, high[2]);
 }
 
+// The last pass of the step over the P2G bins (the particles have not moved
+// since the binning): one CTA per tile with particles stages the current and
+// saved u, v, w on the tile's nodes with a two-node halo -- 12^3 nodes per
+// field, node indices clamped to the field lattice exactly as sample2 clamps
+// them -- then, per particle, blends the FLIP/PIC velocity from the first
+// stage's samples and takes the RK2 (or RK3) stages from the same box.  A
+// sample whose stencil leaves the box (a midpoint more than a cell outside the
+// tile, or a position outside the domain) takes the global path.  Every value
+// equals k_advect's: the same clamped nodes, weights and summation order.
+constexpr int kAdvBox = 12;
+constexpr int kAdvBox3 = kAdvBox * kAdvBox * kAdvBox;
+
+// trilinear sample of box field `a` whose stencil origin is (li, lj, lk) in
+// box coordinates, with FP32 fractions
+template <bool kOld>
+__device__ __forceinline__ void box_tri(const float2 (*box)[kAdvBox3], int a, int li, int lj, int lk, float fx,
+                                        float fy, float fz, float& cur, float& old) {
+  const float wx[2] = {1.0f - fx, fx}, wy[2] = {1.0f - fy, fy}, wz[2] = {1.0f - fz, fz};
+  const float2* bp = &box[a][li + kAdvBox * (lj + kAdvBox * lk)];
+  float s = 0.0f, so = 0.0f;
+#pragma unroll
+  for (int dk = 0; dk < 2; ++dk)
+#pragma unroll
+    for (int dj = 0; dj < 2; ++dj)
+#pragma unroll
+      for (int di = 0; di < 2; ++di) {
+        const float w = wx[di] * wy[dj] * wz[dk];
+        const float2 v = bp[di + kAdvBox * (dj + kAdvBox * dk)];
+        s += w * v.x;
+        if (kOld) so += w * v.y;
+      }
+  cur = s;
+  old = so;
+}
+
+// velocity_at from the box where the stencils fit
+__device__ __forceinline__ void box_velocity(const DevGrid& G, const float2 (*box)[kAdvBox3], int b0, int b1, int b2,
+                                             double x, double y, double z, double out[3]) {
+  const double g[3] = {to_grid(x, G.g.ox, G.g.inv_dx), to_grid(y, G.g.oy, G.g.inv_dx),
+                       to_grid(z, G.g.oz, G.g.inv_dx)};
+#pragma unroll
+  for (int ax = 0; ax < 3; ++ax) {
+    double c[3];
+    int n0[3];
+    float fr[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      c[d] = d == ax ? g[d] : g[d] - 0.5;
+      n0[d] = (int)floor(c[d]);
+      fr[d] = (float)(c[d] - n0[d]);
+    }
+    const int li = n0[0] - b0, lj = n0[1] - b1, lk = n0[2] - b2;
+    float cur, old;
+    if ((unsigned)li < kAdvBox - 1 && (unsigned)lj < kAdvBox - 1 && (unsigned)lk < kAdvBox - 1)
+      box_tri<false>(box, ax, li, lj, lk, fr[0], fr[1], fr[2], cur, old);
+    else
+      sample2<false>(G, ax, c[0], c[1], c[2], cur, old);
+    out[ax] = cur;
+  }
+}
+
+__global__ void __launch_bounds__(256, 3) k_g2p_advect_tiles(DevGrid G, const int* __restrict__ cell_start,
+                                                          const int* __restrict__ perm, ParticlePtrs P, double dt,
+                                                          int order, double aL, double aG, int* counters) {
+  __shared__ float2 box[3][kAdvBox3];  // (current, saved)
+  __shared__ int nslot[27];
+  __shared__ int tally[8];
+  const int t = blockIdx.x;
+  const int beg = cell_start[(size_t)t * PF_TV], end = cell_start[(size_t)(t + 1) * PF_TV];
+  if (beg >= end) return;
+  const int tx = t % G.g.TX, tq = t / G.g.TX, ty = tq % G.g.TY, tz = tq / G.g.TY;
+  const int b0 = tx * 8 - 2, b1 = ty * 8 - 2, b2 = tz * 8 - 2;
+  if (threadIdx.x < 27) {
+    const int x = tx + (int)threadIdx.x % 3 - 1, y = ty + ((int)threadIdx.x / 3) % 3 - 1, z = tz + (int)threadIdx.x / 9 - 1;
+    nslot[threadIdx.x] = (x >= 0 && y >= 0 && z >= 0 && x < G.g.TX && y < G.g.TY && z < G.g.TZ)
+                             ? G.tile_slot[tile_id(G.g, x, y, z)]
+                             : -1;
+  }
+  if (threadIdx.x < 8) tally[threadIdx.x] = 0;
+  __syncthreads();
+  // the box spans nodes [8t - 2, 8t + 10) per axis; clamped into the lattice
+  // they lie in tiles t-1 .. t+1
+  for (int e = threadIdx.x; e < 3 * kAdvBox3; e += blockDim.x) {
+    const int a = e / kAdvBox3, s = e - a * kAdvBox3;
+    const int fv = PF_U + a;
+    const int i = min(max(b0 + s % kAdvBox, 0), G.g.fdim[fv][0] - 1);
+    const int j = min(max(b1 + (s / kAdvBox) % kAdvBox, 0), G.g.fdim[fv][1] - 1);
+    const int k = min(max(b2 + s / (kAdvBox * kAdvBox), 0), G.g.fdim[fv][2] - 1);
+    const int sl = nslot[((i >> 3) - tx + 1) + 3 * (((j >> 3) - ty + 1) + 3 * ((k >> 3) - tz + 1))];
+    float2 v = make_float2(0.0f, 0.0f);
+    if (sl >= 0) {
+      const size_t o = (size_t)sl * PF_TV + local_id(i, j, k);
+      v = make_float2(G.fld[fv][o], G.saved[a][o]);
+    }
+    box[a][s] = v;
+  }
+  __syncthreads();
+  float* vp[3] = {P.vx, P.vy, P.vz};
+  float* pp[3] = {P.px, P.py, P.pz};
+  const bool fast = G.g.dx_pow2 && G.g.ox == 0.0 && G.g.oy == 0.0 && G.g.oz == 0.0;
+  const float inv_dx_f = (float)G.g.inv_dx;
+  const double lo[3] = {G.g.ox + 0.5 * G.g.dx, G.g.oy + 0.5 * G.g.dx, G.g.oz + 0.5 * G.g.dx};
+  const double hi[3] = {G.g.ox + (G.g.nx - 0.5) * G.g.dx, G.g.oy + (G.g.ny - 0.5) * G.g.dx,
+                        G.g.oz + (G.g.nz - 0.5) * G.g.dx};
+  unsigned cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int q = beg + threadIdx.x;
+  int pn = 0;
+  float xn = 0.0f, yn = 0.0f, zn = 0.0f, vn[3] = {0.0f, 0.0f, 0.0f};
+  uint8_t tn = 0;
+  if (q < end) {
+    pn = perm[q];
+    xn = P.px[pn]; yn = P.py[pn]; zn = P.pz[pn]; tn = P.type[pn];
+    vn[0] = P.vx[pn]; vn[1] = P.vy[pn]; vn[2] = P.vz[pn];
+  }
+  for (; q < end; q += blockDim.x) {
+    const int p = pn;
+    const float X = xn, Y = yn, Z = zn, v0[3] = {vn[0], vn[1], vn[2]};
+    const uint8_t ptype = tn;
+    if (q + (int)blockDim.x < end) {
+      pn = perm[q + blockDim.x];
+      xn = P.px[pn]; yn = P.py[pn]; zn = P.pz[pn]; tn = P.type[pn];
+      vn[0] = P.vx[pn]; vn[1] = P.vy[pn]; vn[2] = P.vz[pn];
+    }
+    // stage 1: current and saved samples at the particle (see k_g2p_tiles for
+    // the exact FP32 coordinates)
+    float gf[3];
+    double gd[3];
+    if (fast) {
+      gf[0] = X * inv_dx_f;
+      gf[1] = Y * inv_dx_f;
+      gf[2] = Z * inv_dx_f;
+    } else {
+      gd[0] = to_grid((double)X, G.g.ox, G.g.inv_dx);
+      gd[1] = to_grid((double)Y, G.g.oy, G.g.inv_dx);
+      gd[2] = to_grid((double)Z, G.g.oz, G.g.inv_dx);
+    }
+    const float al = ptype == 0 ? (float)aL : (float)aG;
+    double k1[3];
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+      int n0[3];
+      float fr[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        if (fast) {
+          const float c = d == ax ? gf[d] : gf[d] - 0.5f;
+          n0[d] = (int)floorf(c);
+          fr[d] = c - (float)n0[d];
+        } else {
+          const double c = d == ax ? gd[d] : gd[d] - 0.5;
+          n0[d] = (int)floor(c);
+          fr[d] = (float)(c - n0[d]);
+        }
+      }
+      const int li = n0[0] - b0, lj = n0[1] - b1, lk = n0[2] - b2;
+      float cur, old;
+      if ((unsigned)li < kAdvBox - 1 && (unsigned)lj < kAdvBox - 1 && (unsigned)lk < kAdvBox - 1) {
+        box_tri<true>(box, ax, li, lj, lk, fr[0], fr[1], fr[2], cur, old);
+      } else {
+        double c[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          const double g = fast ? (double)gf[d] : gd[d];
+          c[d] = d == ax ? g : g - 0.5;
+        }
+        sample2<true>(G, ax, c[0], c[1], c[2], cur, old);
+      }
+      k1[ax] = cur;
+      vp[ax][p] = (v0[ax] + (cur - old)) * al + cur * (1.0f - al);
+    }
+    // the remaining stages, in k_advect's arithmetic
+    const double x0[3] = {(double)X, (double)Y, (double)Z};
+    double k2[3], nx[3];
+    if (order == 3) {
+      double m1[3], m2[3], k3[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) m1[c] = x0[c] + k1[c] * (0.5 * dt);
+      box_velocity(G, box, b0, b1, b2, m1[0], m1[1], m1[2], k2);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) m2[c] = (x0[c] - k1[c] * dt) + k2[c] * (2.0 * dt);
+      box_velocity(G, box, b0, b1, b2, m2[0], m2[1], m2[2], k3);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) nx[c] = x0[c] + ((k1[c] + k2[c] * 4.0) + k3[c]) * (dt / 6.0);
+    } else {
+      double mid[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) mid[c] = x0[c] + k1[c] * (0.5 * dt);
+      box_velocity(G, box, b0, b1, b2, mid[0], mid[1], mid[2], k2);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) nx[c] = x0[c] + k2[c] * dt;
+    }
+    bool any = false;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const bool l = nx[c] < lo[c], h = nx[c] > hi[c];
+      cnt[2 + 2 * c] += l;
+      cnt[3 + 2 * c] += h;
+      any = any || l || h;
+      pp[c][p] = (float)fmax(lo[c], fmin(hi[c], nx[c]));
+    }
+    cnt[0] += any && ptype == 0;
+    cnt[1] += any && ptype == 1;
+  }
+  // clamp statistics: one atomic per counter and CTA
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    const unsigned w = __reduce_add_sync(0xffffffffu, cnt[c]);
+    if ((threadIdx.x & 31) == 0 && w) atomicAdd(&tally[c], (int)w);
+  }
+  __syncthreads();
+  if (threadIdx.x < 8 && tally[threadIdx.x]) atomicAdd(&counters[threadIdx.x], tally[threadIdx.x]);
+}
+
 __global__ void k_escape_records(ParticlePtrs P, const int* flags, const int* pos, int n, double* out) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n || !flags[p]) return;
@@ -1326,10 +1542,10 @@ ParticlePtrs particle_ptrs(pf_ctx* ctx) {
   return ParticlePtrs{ctx->px, ctx->py, ctx->pz, ctx->vx, ctx->vy, ctx->vz, ctx->vol, ctx->type};
 }
 
-int slot_grid(const pf_ctx* ctx) {
-  const int cap = 16 * ctx->num_sms;
-  return ctx->nslots < cap ? ctx->nslots : cap;
-}
+int slot_grid(const pf_ctx* ctx) { return slot_blocks(ctx, 16 * ctx->num_sms); }
+
+// the pool may hold slots (its size is then on the device only)
+bool pool_nonempty(const pf_ctx* ctx) { return ctx->pool_pending || ctx->nslots > 0; }
 
 }  // namespace
 
@@ -1367,8 +1583,10 @@ static int p2g_core(pf_ctx* ctx, const pf_phase* ph, double Vp) {
   const int nt = ctx->g.ntiles;
   ctx->bins_valid = false;
   ctx->splat_fresh = false;
+  // with particles the normalisation overwrites every pooled node of these
+  // fields from the splat's staging, so only their activity is reset
   for (int f = PF_U; f <= PF_MW; ++f) {
-    int rc = field_clear(ctx, f);
+    int rc = field_clear(ctx, f, n == 0);
     if (rc) return rc;
   }
   int rc;
@@ -1420,9 +1638,9 @@ int p2g(pf_ctx* ctx, const pf_phase* ph, double Vp) {
 
 int normalize_save_gravity(pf_ctx* ctx, bool save, bool gravity, double dt, double gval) {
   StageScope stage(ctx, PF_STAGE_NORMALIZE);
-  if (ctx->nslots > 0)
+  if (pool_nonempty(ctx))
     (++ctx->launches), k_normalize<<<slot_grid(ctx), PF_TV, 0, ctx->stream>>>(
-        dev_grid(ctx), ctx->splat_stage, ctx->tile_start, ctx->splat_fresh ? 1 : 0, ctx->nslots, save ? 1 : 0,
+        dev_grid(ctx), ctx->splat_stage, ctx->tile_start, ctx->splat_fresh ? 1 : 0, ctx->d_nslots, save ? 1 : 0,
         gravity ? 1 : 0, (float)(dt * gval));
   ctx->splat_fresh = false;
   PF_CUDA_TRY(cudaGetLastError());
@@ -1432,7 +1650,8 @@ int normalize_save_gravity(pf_ctx* ctx, bool save, bool gravity, double dt, doub
 
 int save_velocity(pf_ctx* ctx) {
   StageScope stage(ctx, PF_STAGE_BOUNDARY);
-  if (ctx->nslots > 0) (++ctx->launches), k_save<<<slot_grid(ctx), PF_TV, 0, ctx->stream>>>(dev_grid(ctx), ctx->nslots);
+  if (pool_nonempty(ctx))
+    (++ctx->launches), k_save<<<slot_grid(ctx), PF_TV, 0, ctx->stream>>>(dev_grid(ctx), ctx->d_nslots);
   PF_CUDA_TRY(cudaGetLastError());
   ctx->saved_valid = true;
   return PF_OK;
@@ -1440,8 +1659,9 @@ int save_velocity(pf_ctx* ctx) {
 
 int apply_gravity(pf_ctx* ctx, double dt, double gval) {
   StageScope stage(ctx, PF_STAGE_BOUNDARY);
-  if (ctx->nslots > 0)
-    (++ctx->launches), k_gravity<<<slot_grid(ctx), PF_TV, 0, ctx->stream>>>(dev_grid(ctx), ctx->nslots, (float)(dt * gval));
+  if (pool_nonempty(ctx))
+    (++ctx->launches), k_gravity<<<slot_grid(ctx), PF_TV, 0, ctx->stream>>>(dev_grid(ctx), ctx->d_nslots,
+                                                                            (float)(dt * gval));
   PF_CUDA_TRY(cudaGetLastError());
   return PF_OK;
 }
@@ -1530,13 +1750,17 @@ int advect(pf_ctx* ctx, double dt, int order, pf_clamp_stats* st, double* esc, s
 int g2p_advect(pf_ctx* ctx, double aL, double aG, double dt, int order, pf_clamp_stats* st) {
   StageScope stage(ctx, PF_STAGE_G2P);
   const int n = (int)ctx->np;
-  ctx->bins_valid = false;  // particles move
   PF_CUDA_TRY(cudaMemsetAsync(ctx->d_clamp, 0, 8 * sizeof(int), ctx->stream));
   if (n > 0) {
-    (++ctx->launches), k_advect<<<nblocks(n, 256), 256, 0, ctx->stream>>>(dev_grid(ctx), particle_ptrs(ctx), n, dt, order,
-                                                        ctx->d_clamp, nullptr, 1, aL, aG);
+    if (ctx->bins_valid)
+      (++ctx->launches), k_g2p_advect_tiles<<<ctx->g.ntiles, 256, 0, ctx->stream>>>(
+          dev_grid(ctx), ctx->tile_start, ctx->perm, particle_ptrs(ctx), dt, order, aL, aG, ctx->d_clamp);
+    else
+      (++ctx->launches), k_advect<<<nblocks(n, 256), 256, 0, ctx->stream>>>(dev_grid(ctx), particle_ptrs(ctx), n, dt,
+                                                                             order, ctx->d_clamp, nullptr, 1, aL, aG);
     PF_CUDA_TRY(cudaGetLastError());
   }
+  ctx->bins_valid = false;  // particles moved
   if (st) return read_clamp(ctx, st);
   return PF_OK;
 }

@@ -576,6 +576,24 @@ def run_full_step(pf, n=48, steps=20, seed=0, solvers=("plain",), warmup=3):
                "pcg_iterations_per_step": iters / steps}
         if solver == "learned":
             rec["coarse_rejected"] = rejected
+        # where a step's time goes: per-stage device times (CUDA events on the
+        # context stream) over two more steps, outside the timed region
+        lib = pf.load()
+        lib.pf_set_timing(sim.grid.ctx, 1)
+        tm = pf._lib.Timing()
+        lib.pf_get_timing(sim.grid.ctx, C.byref(tm), 1)
+        e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e2.record(stream)
+        for _ in range(2):
+            sim.step()
+        e3.record(stream)
+        e3.synchronize()
+        lib.pf_get_timing(sim.grid.ctx, C.byref(tm), 1)
+        lib.pf_set_timing(sim.grid.ctx, 0)
+        step_ms = e2.elapsed_time(e3) / 2
+        stages = {k: v[0] / 2 for k, v in tm.as_dict().items() if v[1]}
+        rec["stages_ms_per_step"] = stages
+        rec["g2p_advect_share"] = stages.get("g2p", 0.0) / step_ms
         out[solver] = rec
         sim.grid.close()
     if "plain" in out and "learned" in out:
