@@ -133,6 +133,63 @@ typedef struct {
 int pfo_surface_tension(pfo_grid* g, const pfo_phase* pp, double dt, double strength, double max_delta_speed,
                         int smoothing_radius, pfo_surface_stats* st);
 
+/* ---- 2-level multires step (pf_oracle_mr.c) ------------------------------
+ * src/grid/multires_layout3d.h, src/driver/multires_ops3d_tp.cpp,
+ * src/driver/multires_sim3d_tp.cpp:23-227, 577-733,
+ * src/pressure/multires_pressure3d.cpp.  The layout is one flag per level-1
+ * block of 8^3 fine cells (1: split into level-0 blocks), x fastest.  Face
+ * fields are dense over the fine face lattice; 0..5 = u v w mu mv mw, 6..8 =
+ * the step's saved u v w.  Markers and pressure are per fine cell (the value
+ * of the leaf cell holding it). */
+enum { PFO_MR_NFACE = 9 };
+typedef struct pfo_mr pfo_mr;
+typedef struct {
+  int enabled, particle_padding, gas_padding, hysteresis_cells, max_fine_leaves;
+} pfo_mr_dynamic;
+typedef struct {
+  int max_iter;
+  double abs_tol, rel_tol;
+  int jacobi, flexible_beta, adaptive_restart;
+  double restart_growth, c_div;
+} pfo_mr_solve_cfg;
+typedef struct {
+  int active_cells, pinned_cell, max_iterations, iterations, restarts, beta_resets, converged, breakdown;
+  double initial_residual, final_residual, effective_tolerance, min_positive_diag, max_diag;
+} pfo_mr_solve_stats;
+typedef struct {
+  double dt, gravity, Vp, alpha_l, alpha_g;
+  int advect_order;
+  pfo_mr_solve_cfg solve;
+} pfo_mr_step_cfg;
+
+pfo_mr* pfo_mr_create(int nx, int ny, int nz, double dx);
+void pfo_mr_destroy(pfo_mr* m);
+void pfo_mr_dims(const pfo_mr* m, int* blocks3);
+int pfo_mr_set_layout(pfo_mr* m, const int* boxes, int nbox); /* coarse everywhere, then refine each box */
+int pfo_mr_set_levels(pfo_mr* m, const unsigned char* refined);
+int pfo_mr_get_levels(const pfo_mr* m, unsigned char* refined);
+int pfo_mr_count_fine_leaves(const pfo_mr* m);
+int pfo_mr_update_refinement(pfo_mr* m, const pfo_mr_dynamic* dyn, size_t n, const double* pos,
+                             const unsigned char* type);
+void pfo_mr_refinement_state(const pfo_mr* m, int* out8);
+int pfo_mr_face_valid(const pfo_mr* m, int axis, unsigned char* out);
+int pfo_mr_get_face(const pfo_mr* m, int field, float* out);
+int pfo_mr_set_face(pfo_mr* m, int field, const float* in);
+int pfo_mr_get_cells(const pfo_mr* m, float* marker, float* pressure);
+int pfo_mr_mark_cells(pfo_mr* m, size_t n, const double* pos);
+int pfo_mr_p2g(pfo_mr* m, size_t n, const double* pos, const double* vel, const unsigned char* type,
+               const double* vol, const pfo_phase* pp, double Vp);
+int pfo_mr_apply_gravity(pfo_mr* m, double dt, double gravity);
+int pfo_mr_apply_walls(pfo_mr* m);
+int pfo_mr_project(pfo_mr* m, const pfo_phase* pp, double dt, const pfo_mr_solve_cfg* cfg, pfo_mr_solve_stats* st);
+int pfo_mr_g2p(const pfo_mr* m, size_t n, const double* pos, double* vel, const unsigned char* type, double aL,
+               double aG);
+int pfo_mr_advect(const pfo_mr* m, size_t n, double* pos, const unsigned char* type, double dt, int order,
+                  pfo_clamp_stats* st);
+int pfo_mr_step(pfo_mr* m, const pfo_mr_dynamic* dyn, size_t n, double* pos, double* vel,
+                const unsigned char* type, const double* vol, const pfo_phase* pp, const pfo_mr_step_cfg* cfg,
+                pfo_mr_solve_stats* sst, pfo_clamp_stats* cst);
+
 #ifdef __cplusplus
 }
 #endif

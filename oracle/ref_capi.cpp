@@ -16,9 +16,15 @@
 //   applySparseSurfaceTension3D (src/driver/interface_diagnostics3d.cpp:405-447)
 //   sparse3d::collectCellsWithMarker (src/driver/sparse_ops3d_common.h:65-85)
 //   writeSparseRenderCache3D (src/driver/render_cache3d.h:617-663)
+//   MRSim3DTP (src/driver/multires_sim3d_tp.h:10-191): step(),
+//     initBubbleTankInterfaceBand(), updateDynamicRefinement(), and
+//     mrP2G3D_tp (src/driver/multires_ops3d_tp.cpp:209-274)
 // and converts between its SparseMacGrid3D<4> block pool and dense arrays
-// plus one activity byte per 4^3 block.
+// plus one activity byte per 4^3 block, and between MRMacGrid3D<4>'s maps and
+// dense fine lattices (absent face keys and cells read 0).
 #include "driver/interface_diagnostics3d.h"
+#include "driver/multires_ops3d_tp.h"
+#include "driver/multires_sim3d_tp.h"
 #include "driver/particle_adaptivity3d.h"
 #include "driver/render_cache3d.h"
 #include "driver/sparse_ops3d_common.h"
@@ -29,8 +35,10 @@
 #include "physics/phasefield.h"
 #include "transfer/transfer3d_tp.h"
 
+#include <algorithm>
 #include <cstddef>
 #include <cstring>
+#include <map>
 #include <new>
 
 namespace {
@@ -319,6 +327,184 @@ int pfr_surface_tension(void* hp, const double* phase, double dt, double strengt
                         s.smoothed_curvature_abs_max, s.capillary_dt_limit};
   std::memcpy(ints5, iv, sizeof(iv));
   std::memcpy(dbl9, dv, sizeof(dv));
+  return 0;
+}
+
+
+// ---- multires (MRSim3DTP) -------------------------------------------------
+
+struct MRHandle {
+  MRSim3DTP sim;
+  MRHandle(int nx, int ny, int nz, double dx) : sim(nx, ny, nz, dx) {}
+};
+
+void* pfr_mr_create(int nx, int ny, int nz, double dx) { return new (std::nothrow) MRHandle(nx, ny, nz, dx); }
+
+void pfr_mr_destroy(void* hp) { delete static_cast<MRHandle*>(hp); }
+
+// d: dt, gravity, Vp, alpha_liquid, alpha_gas, cg_tol, cg_rel_tol, cg_restart_growth
+// i: advection_order, cg_iters, cg_jacobi_preconditioner, cg_flexible_beta,
+//    cg_adaptive_restart, dynamic_refinement, dynamic_particle_padding,
+//    dynamic_gas_padding, dynamic_hysteresis_cells, dynamic_max_fine_leaves
+int pfr_mr_configure(void* hp, const double* phase, const double* d, const int* i) {
+  MRSim3DTP& s = static_cast<MRHandle*>(hp)->sim;
+  s.phase = phaseOf(phase);
+  s.dt = d[0];
+  s.gravity = d[1];
+  s.Vp = d[2];
+  s.alpha_liquid = d[3];
+  s.alpha_gas = d[4];
+  s.cg_tol = d[5];
+  s.cg_rel_tol = d[6];
+  s.cg_restart_growth = d[7];
+  s.advection_order = i[0];
+  s.cg_iters = i[1];
+  s.cg_jacobi_preconditioner = i[2] != 0;
+  s.cg_flexible_beta = i[3] != 0;
+  s.cg_adaptive_restart = i[4] != 0;
+  s.dynamic_refinement = i[5] != 0;
+  s.dynamic_particle_padding = i[6];
+  s.dynamic_gas_padding = i[7];
+  s.dynamic_hysteresis_cells = i[8];
+  s.dynamic_max_fine_leaves = i[9];
+  return 0;
+}
+
+// The layout setCoarseEverywhere(1) + refineFineCellBox of each clamped box
+// (as the static layouts of multires_sim3d_tp.cpp:158-170 are made), and a
+// fresh grid on it.
+int pfr_mr_set_layout(void* hp, const int* boxes, int nbox) {
+  MRSim3DTP& s = static_cast<MRHandle*>(hp)->sim;
+  s.layout.setCoarseEverywhere(1);
+  for (int b = 0; b < nbox; ++b) {
+    const int* q = boxes + 6 * b;
+    const int x0 = std::max(0, std::min(s.layout.nx, q[0])), y0 = std::max(0, std::min(s.layout.ny, q[1]));
+    const int z0 = std::max(0, std::min(s.layout.nz, q[2])), x1 = std::max(0, std::min(s.layout.nx, q[3]));
+    const int y1 = std::max(0, std::min(s.layout.ny, q[4])), z1 = std::max(0, std::min(s.layout.nz, q[5]));
+    if (x0 < x1 && y0 < y1 && z0 < z1) s.layout.refineFineCellBox(x0, y0, z0, x1, y1, z1);
+  }
+  s.layout.enforceTwoToOneBalance();
+  s.grid = MRMacGrid3D<4>(s.layout);
+  return 0;
+}
+
+// One byte per level-1 block (x fastest): 1 where the layout holds its
+// level-0 children.
+int pfr_mr_get_levels(void* hp, unsigned char* refined) {
+  const MRLayout3D<4>& L = static_cast<MRHandle*>(hp)->sim.layout;
+  const int MX = L.levelBlockCountX(1), MY = L.levelBlockCountY(1), MZ = L.levelBlockCountZ(1);
+  std::memset(refined, 0, (size_t)MX * MY * MZ);
+  for (const MRBlockKey3D& b : L.leaves())
+    if (b.level == 0) refined[(b.bx >> 1) + MX * ((b.by >> 1) + MY * (b.bz >> 1))] = 1;
+  return 0;
+}
+
+int pfr_mr_count_level(void* hp, int level) {
+  return (int)static_cast<MRHandle*>(hp)->sim.layout.countLevel(level);
+}
+
+int pfr_mr_set_particles(void* hp, size_t n, const double* pos, const double* vel, const unsigned char* type,
+                         const double* vol) {
+  Particles3DTP& ps = static_cast<MRHandle*>(hp)->sim.particles;
+  ps = Particles3DTP();
+  for (size_t p = 0; p < n; ++p)
+    ps.add({pos[3 * p], pos[3 * p + 1], pos[3 * p + 2]}, {vel[3 * p], vel[3 * p + 1], vel[3 * p + 2]}, type[p],
+           vol[p]);
+  return 0;
+}
+
+size_t pfr_mr_num_particles(void* hp) { return static_cast<MRHandle*>(hp)->sim.particles.size(); }
+
+int pfr_mr_get_particles(void* hp, double* pos, double* vel, unsigned char* type, double* vol) {
+  const Particles3DTP& ps = static_cast<MRHandle*>(hp)->sim.particles;
+  for (size_t p = 0; p < ps.size(); ++p) {
+    if (pos) { pos[3 * p] = ps.pos[p].x; pos[3 * p + 1] = ps.pos[p].y; pos[3 * p + 2] = ps.pos[p].z; }
+    if (vel) { vel[3 * p] = ps.vel[p].x; vel[3 * p + 1] = ps.vel[p].y; vel[3 * p + 2] = ps.vel[p].z; }
+    if (type) type[p] = ps.type[p];
+    if (vol) vol[p] = ps.volume[p];
+  }
+  return 0;
+}
+
+int pfr_mr_init_bubble_tank(void* hp) {
+  static_cast<MRHandle*>(hp)->sim.initBubbleTankInterfaceBand();
+  return 0;
+}
+
+// updateDynamicRefinement; out7: retained box (valid, x0, y0, z0, x1, y1, z1)
+int pfr_mr_update_refinement(void* hp, int* out8) {
+  MRSim3DTP& s = static_cast<MRHandle*>(hp)->sim;
+  s.updateDynamicRefinement();
+  const int v[8] = {s.dynamic_retained_box_valid, s.dynamic_retained_x0, s.dynamic_retained_y0,
+                    s.dynamic_retained_z0, s.dynamic_retained_x1, s.dynamic_retained_y1, s.dynamic_retained_z1,
+                    s.dynamic_budget_limited};
+  std::memcpy(out8, v, sizeof(v));
+  return 0;
+}
+
+int pfr_mr_p2g(void* hp) {
+  MRSim3DTP& s = static_cast<MRHandle*>(hp)->sim;
+  mrP2G3D_tp(s.grid, s.particles, s.phase, s.Vp);
+  return 0;
+}
+
+// step(); ints10: active cells, pinned cell, iterations, restarts, beta resets,
+// converged, breakdown, fine leaves, clamped liquid, clamped gas;
+// dbl3: initial, final residual, effective tolerance
+int pfr_mr_step(void* hp, int* ints10, double* dbl3) {
+  MRSim3DTP& s = static_cast<MRHandle*>(hp)->sim;
+  s.step();
+  const MRPressureSolveStats3D& st = s.last_pressure_stats;
+  const int iv[10] = {st.active_cells, st.pinned_cell, st.iterations, st.restarts, st.beta_resets,
+                      st.converged ? 1 : 0, st.breakdown ? 1 : 0, (int)s.layout.countLevel(0),
+                      s.particle_boundary_clamped_liquid_last, s.particle_boundary_clamped_gas_last};
+  const double dv[3] = {st.initial_residual, st.final_residual, st.effective_tolerance};
+  std::memcpy(ints10, iv, sizeof(iv));
+  std::memcpy(dbl3, dv, sizeof(dv));
+  return 0;
+}
+
+// a face field on the dense fine face lattice: 0..5 = u v w mu mv mw
+int pfr_mr_get_face(void* hp, int field, float* dense) {
+  const MRMacGrid3D<4>& g = static_cast<MRHandle*>(hp)->sim.grid;
+  const std::map<MRFaceKey3D, float>* maps[6] = {&g.ufield, &g.vfield, &g.wfield, &g.mu, &g.mv, &g.mw};
+  if (field < 0 || field > 5) return -1;
+  const int axis = field % 3;
+  const size_t X = (size_t)g.layout.nx + (axis == 0), Y = (size_t)g.layout.ny + (axis == 1);
+  const size_t Z = (size_t)g.layout.nz + (axis == 2);
+  std::memset(dense, 0, X * Y * Z * sizeof(float));
+  for (const auto& kv : *maps[field]) {
+    const MRFaceKey3D& f = kv.first;
+    if (f.fineX < 0 || f.fineY < 0 || f.fineZ < 0 || (size_t)f.fineX >= X || (size_t)f.fineY >= Y ||
+        (size_t)f.fineZ >= Z)
+      return -2;
+    dense[(size_t)f.fineX + X * ((size_t)f.fineY + Y * (size_t)f.fineZ)] = kv.second;
+  }
+  return 0;
+}
+
+// the valid faces of one axis (the face list of the current layout)
+int pfr_mr_face_valid(void* hp, int axis, unsigned char* dense) {
+  const MRMacGrid3D<4>& g = static_cast<MRHandle*>(hp)->sim.grid;
+  const std::vector<MRFaceKey3D>& faces = axis == 0 ? g.uFaceRefs() : axis == 1 ? g.vFaceRefs() : g.wFaceRefs();
+  const size_t X = (size_t)g.layout.nx + (axis == 0), Y = (size_t)g.layout.ny + (axis == 1);
+  const size_t Z = (size_t)g.layout.nz + (axis == 2);
+  std::memset(dense, 0, X * Y * Z);
+  for (const MRFaceKey3D& f : faces) dense[(size_t)f.fineX + X * ((size_t)f.fineY + Y * (size_t)f.fineZ)] = 1;
+  return 0;
+}
+
+// marker and pressure per fine cell (the value of its leaf cell)
+int pfr_mr_get_cells(void* hp, float* marker, float* pressure) {
+  const MRMacGrid3D<4>& g = static_cast<MRHandle*>(hp)->sim.grid;
+  const int nx = g.layout.nx, ny = g.layout.ny, nz = g.layout.nz;
+  for (int k = 0; k < nz; ++k)
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) {
+        const size_t o = (size_t)i + (size_t)nx * ((size_t)j + (size_t)ny * k);
+        if (marker) marker[o] = g.marker.get(g.marker.cellAtFineCell(i, j, k));
+        if (pressure) pressure[o] = g.p.get(g.p.cellAtFineCell(i, j, k));
+      }
   return 0;
 }
 
