@@ -18,6 +18,7 @@ same names, argument meanings and order:
                               interfaceRadius, maxAddedPerStep)
                                                             src/driver/particle_adaptivity3d.h:264
     diagnoseSparseInterface3D(grid, phase)                  src/driver/interface_diagnostics3d.cpp:363
+    MRSim3DTP (2-level multires step)                       src/driver/multires_sim3d_tp.cpp:671-733
     SparseMacGrid3D, Particles3DTP, PhaseParams             src/grid/sparse_mac_grid3d.h,
                                                             src/particles/particles3d_tp.h,
                                                             src/physics/phasefield.h
@@ -29,6 +30,7 @@ from ._lib import (PF_MK, PF_MU, PF_MV, PF_MW, PF_P, PF_PRECOND_EXACT_COARSE, PF
                    PF_PRECOND_NETWORK, PF_SCENE_BUBBLE_TANK, PF_SCENE_RAYLEIGH_TAYLOR, PF_SOLVER_LEARNED, PF_SOLVER_MIXED, PF_SOLVER_PLAIN, PF_U, PF_V, PF_W, PfError,
                    load)
 from .learned import LearnedCoarseSolver
+from .multires import MRSim3DTP
 from .sparse import (ParticleEscapeBuffer3D, ParticleEscapeStats3D, Particles3DTP, PhaseParams, SolverConfig,
                      SparseMacGrid3D, SparseSim3DTP, applyGasParticleCoarsening, applyLiquidParticleRefill,
                      applyNarrowBandAir, applySparseSurfaceTension3D, applyTypedParticleCoarsening, betaFromPhi, calibrateRhoTilde0,
@@ -40,7 +42,7 @@ __all__ = [
     "PF_U", "PF_V", "PF_W", "PF_MU", "PF_MV", "PF_MW", "PF_P", "PF_MK",
     "PF_SOLVER_PLAIN", "PF_SOLVER_MIXED", "PF_SOLVER_LEARNED", "PfError", "load",
     "PF_PRECOND_NETWORK", "PF_PRECOND_EXACT_COARSE", "PF_PRECOND_JACOBI", "PF_SCENE_RAYLEIGH_TAYLOR",
-    "PF_SCENE_BUBBLE_TANK", "LearnedCoarseSolver",
+    "PF_SCENE_BUBBLE_TANK", "LearnedCoarseSolver", "MRSim3DTP",
     "PhaseParams", "Particles3DTP", "SparseMacGrid3D", "SparseSim3DTP", "SolverConfig",
     "ParticleEscapeStats3D", "ParticleEscapeBuffer3D",
     "spP2G3D_tp", "spProjectStepVC3D", "spG2P3D_tp", "spAdvect3D_tp", "calibrateRhoTilde0",

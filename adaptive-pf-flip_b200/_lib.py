@@ -42,6 +42,8 @@ EXPORTS = (
     "pf_interface_diagnostics", "pf_get_interface_stats", "pf_set_step_controls", "pf_get_step_control_stats",
     "pf_surface_tension", "pf_set_surface_tension", "pf_get_surface_stats",
     "pf_default_render_camera", "pf_write_render_cache", "pf_seed_scene",
+    "pf_mr_set_layout", "pf_mr_set_levels", "pf_mr_get_levels", "pf_mr_set_dynamic", "pf_mr_reset_refinement",
+    "pf_mr_update_refinement", "pf_mr_step", "pf_mr_p2g", "pf_mr_get_face", "pf_mr_get_cells",
 )
 
 STAGES = ("bin", "sort", "splat", "normalize", "mark", "boundary", "project", "pcg", "g2p", "precond_setup",
@@ -86,6 +88,30 @@ class ClampStats(C.Structure):
 class StepCfg(C.Structure):
     _fields_ = [("dt", C.c_double), ("gravity", C.c_double), ("Vp", C.c_double), ("alpha_l", C.c_double),
                 ("alpha_g", C.c_double), ("phase", Phase), ("solve", SolveCfg), ("advect_order", C.c_int)]
+
+
+class MRBox(C.Structure):
+    _fields_ = [("x0", C.c_int), ("y0", C.c_int), ("z0", C.c_int), ("x1", C.c_int), ("y1", C.c_int), ("z1", C.c_int)]
+
+
+class MRDynamic(C.Structure):
+    _fields_ = [("enabled", C.c_int), ("particle_padding", C.c_int), ("gas_padding", C.c_int),
+                ("hysteresis_cells", C.c_int), ("max_fine_leaves", C.c_int)]
+
+
+class MRStepCfg(C.Structure):
+    _fields_ = [("dt", C.c_double), ("gravity", C.c_double), ("Vp", C.c_double), ("alpha_l", C.c_double),
+                ("alpha_g", C.c_double), ("phase", Phase), ("advect_order", C.c_int), ("cg_iters", C.c_int),
+                ("cg_tol", C.c_double), ("cg_rel_tol", C.c_double), ("jacobi", C.c_int), ("flexible_beta", C.c_int),
+                ("adaptive_restart", C.c_int), ("restart_growth", C.c_double), ("c_div", C.c_double)]
+
+
+class MRStepStats(C.Structure):
+    _fields_ = [("active_cells", C.c_int), ("pinned_cell", C.c_int), ("iterations", C.c_int), ("restarts", C.c_int),
+                ("beta_resets", C.c_int), ("converged", C.c_int), ("breakdown", C.c_int),
+                ("initial_residual", C.c_double), ("final_residual", C.c_double),
+                ("effective_tolerance", C.c_double), ("fine_leaves", C.c_int), ("clamp", ClampStats),
+                ("solve_ms", C.c_double)]
 
 
 class StepStats(C.Structure):
@@ -235,6 +261,16 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "pf_step": (i, [vp, P(StepCfg), P(StepStats)]),
         "pf_calibrate_rho_tilde0": (i, [vp, P(Phase), d, P(d)]),
         "pf_seed_scene": (i, [vp, i, C.c_ulonglong, P(sz)]),
+        "pf_mr_set_layout": (i, [vp, vp, i]),
+        "pf_mr_set_levels": (i, [vp, vp]),
+        "pf_mr_get_levels": (i, [vp, vp, vp]),
+        "pf_mr_set_dynamic": (i, [vp, P(MRDynamic)]),
+        "pf_mr_reset_refinement": (i, [vp]),
+        "pf_mr_update_refinement": (i, [vp, vp]),
+        "pf_mr_step": (i, [vp, P(MRStepCfg), P(MRStepStats)]),
+        "pf_mr_p2g": (i, [vp, P(Phase), d]),
+        "pf_mr_get_face": (i, [vp, i, vp]),
+        "pf_mr_get_cells": (i, [vp, vp, vp]),
         "pf_set_timing": (i, [vp, i]),
         "pf_get_timing": (i, [vp, P(Timing), i]),
         "pf_launch_count": (C.c_longlong, [vp]),

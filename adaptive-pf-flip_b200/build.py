@@ -27,7 +27,7 @@ FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcomp
                 "--expt-relaxed-constexpr", "-I", INCLUDE, "-I", CSRC]
 
 SOURCES = ["pf_pool.cu", "pf_transfer.cu", "pf_project.cu", "pf_pcg.cu", "pf_timing.cu", "pf_noalloc.cu",
-           "pf_coarse.cu", "pf_flex.cu", "pf_outer.cu", "pf_learned.cu", "pf_adapt.cu", "pf_diag.cu", "pf_render.cu", "pf_scene.cu", "pf_capi.cu"]
+           "pf_coarse.cu", "pf_flex.cu", "pf_outer.cu", "pf_learned.cu", "pf_adapt.cu", "pf_diag.cu", "pf_render.cu", "pf_scene.cu", "pf_mr.cu", "pf_capi.cu"]
 
 
 def _deps():

@@ -49,6 +49,7 @@ void free_all(pf_ctx* c) {
   pf::coarse_release(c);
   pf::adapt_free(c);
   pf::diag_free(c);
+  pf::mr_free(c);
   F(c->tile_slot); F(c->slot_tile); F(c->d_nslots); F(c->tile_need); F(c->tile_new); F(c->tile_rank);
   for (int f = 0; f < PF_NFIELDS; ++f) { F(c->fld[f]); F(c->act4[f]); }
   for (int a = 0; a < PF_NSAVED; ++a) F(c->saved[a]);

@@ -102,6 +102,8 @@ struct pf_ctx {
   double* b64 = nullptr;  // right-hand side kept in FP64
   // learned preconditioner state lives in its own module
   void* learned = nullptr;
+  // the 2-level multires grid (pf_mr.cu), made on first use
+  void* mr = nullptr;
   // particle adaptivity: scratch (its own module) and the step's settings
   void* adapt = nullptr;
   bool adapt_on = false;
@@ -197,6 +199,9 @@ int interface_diagnostics_finish(pf_ctx* ctx);  // statistics of a launch made w
 int surface_tension(pf_ctx* ctx, const pf_phase* ph, double dt, double strength, double max_dv, int radius,
                     pf_surface_stats* st);
 void diag_free(pf_ctx* ctx);
+
+// mr.cu
+void mr_free(pf_ctx* ctx);
 
 // capi.cu: the second particle set (asynchronous uploads, compaction target)
 int ensure_back_set(pf_ctx* ctx);

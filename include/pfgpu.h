@@ -404,6 +404,69 @@ PFGPU_API int pf_seed_scene(pf_ctx* ctx, int scene, unsigned long long seed, siz
 /* calibrateRhoTilde0 (src/transfer/transfer3d_tp.cpp:29-36), on the device. */
 PFGPU_API int pf_calibrate_rho_tilde0(pf_ctx* ctx, const pf_phase* phase, double Vp, double* out);
 
+/* ---- 2-level multires step (MRSim3DTP) ------------------------------------
+ * The reference's multires solver step (src/driver/multires_sim3d_tp.cpp:
+ * 671-733) on the context's particle set, with its own grid on the same
+ * nx, ny, nz and dx (the origin must be 0).  The layout holds level-1 blocks
+ * of 8^3 fine cells (x fastest), each coarse (4^3 cells of 2 dx) or refined
+ * into fine cells (src/grid/multires_layout3d.h:25-162).
+ *
+ * pf_mr_set_layout: setCoarseEverywhere(1), then refineFineCellBox of each
+ *   box clamped to the domain (the static layouts of
+ *   src/driver/multires_sim3d_tp.cpp:158-180).  Before any layout is set every
+ *   block is coarse.
+ * pf_mr_set_levels / pf_mr_get_levels: one byte per level-1 block, 1 where it
+ *   is refined; blocks3 receives the block counts ceil(n / 8).
+ * pf_mr_set_dynamic: updateDynamicRefinement's settings (enabled, particle and
+ *   gas padding, hysteresis, fine-leaf budget; MRSim3DTP's defaults are
+ *   {1, 1, 2, 1, 0}).  pf_mr_update_refinement runs it alone (state8: the
+ *   retained box's valid flag and x0 y0 z0 x1 y1 z1, the budget flag);
+ *   pf_mr_reset_refinement forgets the retained box.
+ * pf_mr_step: updateDynamicRefinement (when enabled), markCells, mrP2G3D_tp,
+ *   the saved copy, gravity, walls, projectMR3D with the Jacobi PCG (adaptive
+ *   restart, optional flexible beta; the coarse-correction and coarse
+ *   preconditioner options are not available), mrG2P3D_tp, mrAdvect3D_tp.
+ * pf_mr_p2g: mrP2G3D_tp (src/driver/multires_ops3d_tp.cpp:209-274) alone.
+ * pf_mr_get_face: a face field on the dense fine face lattice (0..5 = u v w mu
+ *   mv mw, 6..8 = the last step's saved u v w); patches off the leaf-cell
+ *   boundaries read 0.  pf_mr_get_cells: marker (0 empty, 1 fluid, 2 solid)
+ *   and pressure per fine cell, the value of the leaf cell holding it. */
+typedef struct {
+  int x0, y0, z0, x1, y1, z1; /* fine cells [x0, x1) x [y0, y1) x [z0, z1) */
+} pf_mr_box;
+typedef struct {
+  int enabled, particle_padding, gas_padding, hysteresis_cells, max_fine_leaves;
+} pf_mr_dynamic;
+typedef struct {
+  double dt, gravity, Vp, alpha_l, alpha_g;
+  pf_phase phase;
+  int advect_order;     /* 2 or 3 */
+  int cg_iters;         /* max_iterations */
+  double cg_tol;        /* absolute_tolerance */
+  double cg_rel_tol;    /* relative_tolerance */
+  int jacobi, flexible_beta, adaptive_restart;
+  double restart_growth;
+  double c_div;         /* divergence_correction */
+} pf_mr_step_cfg;
+typedef struct {
+  /* MRPressureSolveStats3D (src/pressure/multires_pressure3d.h:60-133) */
+  int active_cells, pinned_cell, iterations, restarts, beta_resets, converged, breakdown;
+  double initial_residual, final_residual, effective_tolerance;
+  int fine_leaves;     /* level-0 blocks of the step's layout */
+  pf_clamp_stats clamp;
+  double solve_ms;     /* device time of assembly and PCG */
+} pf_mr_step_stats;
+PFGPU_API int pf_mr_set_layout(pf_ctx* ctx, const pf_mr_box* boxes, int n);
+PFGPU_API int pf_mr_set_levels(pf_ctx* ctx, const uint8_t* refined);
+PFGPU_API int pf_mr_get_levels(pf_ctx* ctx, uint8_t* refined, int* blocks3);
+PFGPU_API int pf_mr_set_dynamic(pf_ctx* ctx, const pf_mr_dynamic* dyn);
+PFGPU_API int pf_mr_reset_refinement(pf_ctx* ctx);
+PFGPU_API int pf_mr_update_refinement(pf_ctx* ctx, int* state8);
+PFGPU_API int pf_mr_step(pf_ctx* ctx, const pf_mr_step_cfg* cfg, pf_mr_step_stats* stats);
+PFGPU_API int pf_mr_p2g(pf_ctx* ctx, const pf_phase* phase, double Vp);
+PFGPU_API int pf_mr_get_face(pf_ctx* ctx, int field, float* dense);
+PFGPU_API int pf_mr_get_cells(pf_ctx* ctx, uint8_t* marker, float* pressure);
+
 /* ---- learned coarse solve (PF_SOLVER_LEARNED with PF_PRECOND_NETWORK) ----
  * New in this library (the reference's sparse path has no learned solver; its
  * flexible-PCG / guarded-preconditioner pattern is

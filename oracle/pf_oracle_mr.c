@@ -1042,7 +1042,7 @@ int pfo_mr_advect(const pfo_mr* m, size_t n, double* pos, const unsigned char* t
     /* ParticleEscapeStats3D::recordClamp */
     if (any) {
       if (type[q] == 0) s.clamped_liquid++;
-      else s.clamped_gas++;
+      else if (type[q] == 1) s.clamped_gas++;
     }
     s.x_lo += l[0];
     s.x_hi += h[0];

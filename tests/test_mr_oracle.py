@@ -136,3 +136,14 @@ def test_dynamic_refinement_box_equals_reference(budget):
         assert np.array_equal(o.levels(), r.levels())
         assert o.fine_leaves() == r.fine_leaves()
         centre = centre + np.array([1.5, 0.5, 1.0]) * (move % 2 * 2 - 1) + np.array([0.7, 0.4, 0.6])
+
+
+@pytest.mark.parametrize("n,boxes", [((20, 13, 18), [(3, 2, 5, 11, 7, 12)]), ((16, 24, 16), [(0, 0, 0, 16, 14, 16)]),
+                                     ((9, 17, 7), [(8, 0, 0, 9, 9, 7), (0, 16, 0, 2, 17, 2)])])
+def test_closed_form_face_list_equals_oracle(pf, n, boxes):
+    """The GPU's face-patch rule (even position, far side, or beside a refined
+    block) written in numpy in the package, against the restated face list."""
+    o = OracleMR(*n, 1.0)
+    o.set_layout(boxes)
+    for ax in range(3):
+        assert np.array_equal(pf.multires.valid_faces(o.levels(), *n, ax), o.face_valid(ax).astype(bool))
