@@ -23,7 +23,7 @@ ERR_NAMES = {PF_ERR_INVALID: "PF_ERR_INVALID", PF_ERR_CUDA: "PF_ERR_CUDA", PF_ER
 PF_U, PF_V, PF_W, PF_MU, PF_MV, PF_MW, PF_P, PF_MK = range(8)
 PF_SOLVER_PLAIN, PF_SOLVER_MIXED, PF_SOLVER_LEARNED = 0, 1, 2
 PF_PRECOND_NETWORK, PF_PRECOND_EXACT_COARSE, PF_PRECOND_JACOBI = 0, 1, 2
-PF_SCENE_RAYLEIGH_TAYLOR, PF_SCENE_BUBBLE_TANK = 0, 1
+PF_SCENE_RAYLEIGH_TAYLOR, PF_SCENE_BUBBLE_TANK, PF_SCENE_DAM_BREAK = 0, 1, 2
 
 # every entry point include/pfgpu.h declares
 EXPORTS = (

@@ -960,6 +960,7 @@ int fine_leaves_for(const MrGeom& g, const Box& b) {
 }
 
 int update_refinement(pf_ctx* ctx, MrState* s) {
+  StageScope stage(ctx, PF_STAGE_ADAPT);
   const MrGeom& g = s->g;
   const size_t n = ctx->np;
   (++ctx->launches), k_mr_minmax_init<<<1, 32, 0, ctx->stream>>>(s->minmax, g.nx, g.ny, g.nz);
@@ -1065,6 +1066,7 @@ MrFaces faces_of(MrState* s) {
 }
 
 int mark_cells_mr(pf_ctx* ctx, MrState* s) {
+  StageScope stage(ctx, PF_STAGE_MARK);
   const size_t n = ctx->np;
   (++ctx->launches), k_mr_mark_walls<<<grid_for(s->ncell, 8 * ctx->num_sms), kMrNT, 0, ctx->stream>>>(s->g, s->mk);
   if (n > 0)
@@ -1075,6 +1077,7 @@ int mark_cells_mr(pf_ctx* ctx, MrState* s) {
 }
 
 int p2g_mr(pf_ctx* ctx, MrState* s, const pf_phase* ph, double Vp) {
+  StageScope stage(ctx, PF_STAGE_SPLAT);
   for (int q = 0; q < 6; ++q)
     PF_CUDA_TRY(cudaMemsetAsync(s->f[q], 0, s->nface[q % 3] * sizeof(float), ctx->stream));
   const size_t n = ctx->np;
@@ -1090,6 +1093,7 @@ int p2g_mr(pf_ctx* ctx, MrState* s, const pf_phase* ph, double Vp) {
 }
 
 int project_mr(pf_ctx* ctx, MrState* s, const pf_mr_step_cfg* cfg, pf_mr_step_stats* st) {
+  StageScope stage(ctx, PF_STAGE_PROJECT);
   const MrGeom& g = s->g;
   const int big = 8 * ctx->num_sms;
   PF_CUDA_TRY(cudaMemsetAsync(s->pcell, 0, s->ncell * sizeof(float), ctx->stream));
@@ -1152,6 +1156,7 @@ int project_mr(pf_ctx* ctx, MrState* s, const pf_mr_step_cfg* cfg, pf_mr_step_st
   PF_CUDA_TRY(cudaGetLastError());
   MrCtl c{};
   int launched = 0;
+  stage_begin(ctx, PF_STAGE_PCG);
   while (true) {
     PF_CUDA_TRY(cudaMemcpyAsync(s->h_ctl, s->ctl, sizeof(MrCtl), cudaMemcpyDeviceToHost, ctx->stream));
     PF_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
@@ -1168,6 +1173,7 @@ int project_mr(pf_ctx* ctx, MrState* s, const pf_mr_step_cfg* cfg, pf_mr_step_st
     launched += batch;
   }
   PF_CUDA_TRY(cudaEventRecord(s->e1, ctx->stream));
+  stage_end(ctx, PF_STAGE_PCG);
   st->iterations = c.it;
   st->restarts = c.restarts;
   st->beta_resets = c.beta_resets;
@@ -1316,24 +1322,29 @@ int pf_mr_step(pf_ctx* ctx, const pf_mr_step_cfg* cfg, pf_mr_step_stats* stats) 
   rc = mark_cells_mr(ctx, s);
   if (!rc) rc = p2g_mr(ctx, s, &cfg->phase, cfg->Vp);
   if (rc) return rc;
-  for (int a = 0; a < 3; ++a)
-    PF_CUDA_TRY(cudaMemcpyAsync(s->f[6 + a], s->f[a], s->nface[a] * sizeof(float), cudaMemcpyDeviceToDevice,
-                                ctx->stream));
-  const int big = 8 * ctx->num_sms;
-  const float dv = (float)(cfg->dt * cfg->gravity);
-  for (int a = 0; a < 3; ++a)
-    (++ctx->launches), k_mr_forces<<<grid_for(s->nface[a], big), kMrNT, 0, ctx->stream>>>(s->g, a, s->f[a],
-                                                                                          s->f[3 + a], dv);
-  PF_CUDA_TRY(cudaGetLastError());
+  {
+    StageScope stage(ctx, PF_STAGE_BOUNDARY);
+    for (int a = 0; a < 3; ++a)
+      PF_CUDA_TRY(cudaMemcpyAsync(s->f[6 + a], s->f[a], s->nface[a] * sizeof(float), cudaMemcpyDeviceToDevice,
+                                  ctx->stream));
+    const int big = 8 * ctx->num_sms;
+    const float dv = (float)(cfg->dt * cfg->gravity);
+    for (int a = 0; a < 3; ++a)
+      (++ctx->launches), k_mr_forces<<<grid_for(s->nface[a], big), kMrNT, 0, ctx->stream>>>(s->g, a, s->f[a],
+                                                                                            s->f[3 + a], dv);
+    PF_CUDA_TRY(cudaGetLastError());
+  }
   rc = project_mr(ctx, s, cfg, &st);
   if (rc) return rc;
   const size_t n = ctx->np;
+  stage_begin(ctx, PF_STAGE_G2P);
   PF_CUDA_TRY(cudaMemsetAsync(s->counters, 0, 8 * sizeof(int), ctx->stream));
   if (n > 0)
     (++ctx->launches), k_mr_g2p_advect<<<grid_for(n, INT_MAX), kMrNT, 0, ctx->stream>>>(
         s->g, faces_of(s), ctx->px, ctx->py, ctx->pz, ctx->vx, ctx->vy, ctx->vz, ctx->type, n, cfg->alpha_l,
         cfg->alpha_g, cfg->dt, cfg->advect_order, s->counters);
   PF_CUDA_TRY(cudaGetLastError());
+  stage_end(ctx, PF_STAGE_G2P);
   ctx->bins_valid = false;
   PF_CUDA_TRY(cudaMemcpyAsync(s->h_ints + 8, s->counters, 8 * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   PF_CUDA_TRY(cudaStreamSynchronize(ctx->stream));

@@ -15,7 +15,9 @@
 // The scene layouts follow the reference's initRayleighTaylor / initBubbleTank
 // (src/driver/sparse_sim3d_tp.cpp:739-776: interior cells, heavy phase above
 // a cos.cos-perturbed interface; water with an air bubble and an empty
-// headspace) at the sizes and densities of the benchmark configurations.
+// headspace) at the sizes and densities of the benchmark configurations, and
+// the dam break of the multires configuration (a water column beside a
+// shallow pool, air empty).
 #include <cmath>
 
 #include "pf_ctx.h"
@@ -43,6 +45,8 @@ struct SceneArgs {
   int kind;
   int nx, ny, nz;
   int ci, cj;  // seeded cells along x and y (x-fastest, then y, then z)
+  int pi, pj;  // dam break: the pool's cells along x and y, seeded after the column's
+  size_t ncol; // dam break: cells of the column
   double dx;
   unsigned long long seed;
   size_t n;
@@ -54,11 +58,19 @@ __global__ void k_seed(SceneArgs a, float* px, float* py, float* pz, float* vx, 
                        uint8_t* type) {
   const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= a.n) return;
-  const size_t c = p >> 3;
+  size_t c = p >> 3;
   const int s = (int)(p & 7);
-  const int i = 1 + (int)(c % a.ci);
-  const int j = 1 + (int)((c / a.ci) % a.cj);
-  const int k = 1 + (int)(c / ((size_t)a.ci * a.cj));
+  int i, j, k;
+  if (a.kind == PF_SCENE_DAM_BREAK && c >= a.ncol) {
+    c -= a.ncol;
+    i = 1 + a.ci + (int)(c % a.pi);
+    j = 1 + (int)((c / a.pi) % a.pj);
+    k = 1 + (int)(c / ((size_t)a.pi * a.pj));
+  } else {
+    i = 1 + (int)(c % a.ci);
+    j = 1 + (int)((c / a.ci) % a.cj);
+    k = 1 + (int)(c / ((size_t)a.ci * a.cj));
+  }
   const unsigned long long cell = (unsigned long long)i + (unsigned long long)a.nx * (j + (unsigned long long)a.ny * k);
   const unsigned long long key = cell * 8ull + s;
   const double ux = uniform01(a.seed, key, 0), uy = uniform01(a.seed, key, 1), uz = uniform01(a.seed, key, 2);
@@ -71,7 +83,10 @@ __global__ void k_seed(SceneArgs a, float* px, float* py, float* pz, float* vx, 
   pz[p] = fz;
   vol[p] = 1.0f;
   const double X = fx, Y = fy, Z = fz;
-  if (a.kind == PF_SCENE_RAYLEIGH_TAYLOR) {
+  if (a.kind == PF_SCENE_DAM_BREAK) {
+    type[p] = 0;
+    vx[p] = vy[p] = vz[p] = 0.0f;
+  } else if (a.kind == PF_SCENE_RAYLEIGH_TAYLOR) {
     const double pi2 = 2.0 * 3.14159265358979323846;
     const double iface = __dadd_rn(0.5, __dmul_rn(__dmul_rn(a.amp, cos(__dmul_rn(pi2, X))), cos(__dmul_rn(pi2, Z))));
     type[p] = Y > iface ? 0 : 1;
@@ -94,7 +109,8 @@ int take_upload_for(pf_ctx* ctx);
 
 extern "C" int pf_seed_scene(pf_ctx* ctx, int scene, unsigned long long seed, size_t* n_out) {
   using namespace pf;
-  if (!ctx || (scene != PF_SCENE_RAYLEIGH_TAYLOR && scene != PF_SCENE_BUBBLE_TANK)) return PF_ERR_INVALID;
+  if (!ctx || (scene != PF_SCENE_RAYLEIGH_TAYLOR && scene != PF_SCENE_BUBBLE_TANK && scene != PF_SCENE_DAM_BREAK))
+    return PF_ERR_INVALID;
   const Geom& g = ctx->g;
   if (g.nx < 3 || g.ny < 3 || g.nz < 3) return set_error(ctx, PF_ERR_INVALID, "pf_seed_scene: grid too small");
   cudaSetDevice(ctx->device);
@@ -108,7 +124,20 @@ extern "C" int pf_seed_scene(pf_ctx* ctx, int scene, unsigned long long seed, si
   a.dx = g.dx;
   a.seed = seed;
   a.ci = g.nx - 2;
-  if (scene == PF_SCENE_RAYLEIGH_TAYLOR) {
+  // the last index whose cell centre lies below frac * n (at most n - 2)
+  auto last_below = [](double frac, int n) {
+    return std::min((int)std::floor(frac * n - 0.5 - 1e-12), n - 2);
+  };
+  if (scene == PF_SCENE_DAM_BREAK) {
+    // water column x < 0.4, y < 0.6, then the pool y < 0.15 beside it
+    a.ci = last_below(0.4, g.nx);
+    a.cj = last_below(0.6, g.ny);
+    a.pi = g.nx - 2 - a.ci;
+    a.pj = last_below(0.15, g.ny);
+    if (a.ci < 1 || a.cj < 1 || a.pi < 1 || a.pj < 1)
+      return set_error(ctx, PF_ERR_INVALID, "pf_seed_scene: grid too small for the dam break");
+    a.ncol = (size_t)a.ci * a.cj * (size_t)(g.nz - 2);
+  } else if (scene == PF_SCENE_RAYLEIGH_TAYLOR) {
     // heavy (type 0, rho_l) above y = 0.5 + 0.05 cos(2 pi x) cos(2 pi z), light below
     a.cj = g.ny - 2;
     a.amp = 0.05;
@@ -126,6 +155,7 @@ extern "C" int pf_seed_scene(pf_ctx* ctx, int scene, unsigned long long seed, si
     a.sigma = 0.1;
   }
   a.n = (size_t)8 * a.ci * a.cj * (size_t)(g.nz - 2);
+  if (scene == PF_SCENE_DAM_BREAK) a.n = 8 * (a.ncol + (size_t)a.pi * a.pj * (size_t)(g.nz - 2));
   if (a.n > ctx->cap) return set_error(ctx, PF_ERR_CAPACITY, "pf_seed_scene: more particles than max_particles");
   ctx->np = a.n;
   ctx->bins_valid = false;

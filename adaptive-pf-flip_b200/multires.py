@@ -48,6 +48,31 @@ def valid_faces(levels, nx, ny, nz, axis):
     return ok | before | after
 
 
+def interface_levels(liquid, radius=3):
+    """A layout refined around a free surface: one byte per level-1 block
+    (8^3 fine cells), 1 when both liquid cells and empty interior cells lie
+    within the block widened by `radius` cells.  `liquid` is a (nz, ny, nx)
+    bool array of liquid cells; the domain's boundary layer counts as
+    neither.  The layout goes to MRSim3DTP.set_levels."""
+    liquid = np.asarray(liquid, bool)
+    nz, ny, nx = liquid.shape
+    interior = np.zeros_like(liquid)
+    interior[1:-1, 1:-1, 1:-1] = True
+    out = []
+    for mask in (liquid & interior, ~liquid & interior):
+        s = np.zeros((nz + 1, ny + 1, nx + 1), np.int64)
+        s[1:, 1:, 1:] = mask.cumsum(0).cumsum(1).cumsum(2)
+        MX, MY, MZ = (nx + 7) // 8, (ny + 7) // 8, (nz + 7) // 8
+        lo = [np.clip(np.arange(m) * 8 - radius, 0, n) for m, n in ((MZ, nz), (MY, ny), (MX, nx))]
+        hi = [np.clip(np.arange(m) * 8 + 8 + radius, 0, n) for m, n in ((MZ, nz), (MY, ny), (MX, nx))]
+        z0, y0, x0 = np.ix_(*lo)
+        z1, y1, x1 = np.ix_(*hi)
+        tot = (s[z1, y1, x1] - s[z0, y1, x1] - s[z1, y0, x1] - s[z1, y1, x0] + s[z0, y0, x1] + s[z0, y1, x0]
+               + s[z1, y0, x0] - s[z0, y0, x0])
+        out.append(tot > 0)
+    return (out[0] & out[1]).astype(np.uint8)
+
+
 class MRSim3DTP:
     def __init__(self, nx, ny, nz, dx, max_particles=1 << 20, device=0):
         self.grid = SparseMacGrid3D(nx, ny, nz, dx, max_particles=max_particles, device=device)
@@ -94,6 +119,17 @@ class MRSim3DTP:
         L.check(self.lib.pf_upload_particles(self.ctx, n, pos.ctypes.data, vel.ctypes.data, typ.ctypes.data,
                                              vol.ctypes.data), self.ctx, "pf_upload_particles")
         self.n = n
+
+    def seed_scene(self, scene, seed=0):
+        """Seed the particle set on the device (pf_seed_scene): "dam_break",
+        "bubble_tank" or "rayleigh_taylor", the particles of the scenes
+        module's generator of that name.  Returns the count."""
+        kind = {"rayleigh_taylor": L.PF_SCENE_RAYLEIGH_TAYLOR, "bubble_tank": L.PF_SCENE_BUBBLE_TANK,
+                "dam_break": L.PF_SCENE_DAM_BREAK}[scene]
+        n = C.c_size_t()
+        L.check(self.lib.pf_seed_scene(self.ctx, kind, int(seed), C.byref(n)), self.ctx, "pf_seed_scene")
+        self.n = int(n.value)
+        return self.n
 
     def get_particles(self):
         n = self.n

@@ -113,6 +113,38 @@ def bubble_tank(n=128, seed=0, level=0.7, center=(0.5, 0.3, 0.5), radius=0.15, s
                 volume=vol, rho_l=rho_water, rho_g=rho_air)
 
 
+def _last_centre_below(frac, n):
+    """Largest index whose cell centre (c + 0.5) / n lies below frac."""
+    return min(int(math.floor(frac * n - 0.5 - 1e-12)), n - 2)
+
+
+def dam_break_cells(n, column=(0.4, 0.6), pool=0.15):
+    """The liquid cells of the dam break, in seeding order: the column
+    (interior cells whose centre has x < column[0] and y < column[1]), then the
+    pool beside it (x beyond the column, y < pool), each x fastest, then y,
+    then z.  Returns (i, j, k) index arrays."""
+    ic, cj, pj = _last_centre_below(column[0], n), _last_centre_below(column[1], n), _last_centre_below(pool, n)
+    k, j, i = np.meshgrid(np.arange(1, n - 1), np.arange(1, cj + 1), np.arange(1, ic + 1), indexing="ij")
+    k2, j2, i2 = np.meshgrid(np.arange(1, n - 1), np.arange(1, pj + 1), np.arange(ic + 1, n - 1), indexing="ij")
+    return (np.concatenate([i.reshape(-1), i2.reshape(-1)]), np.concatenate([j.reshape(-1), j2.reshape(-1)]),
+            np.concatenate([k.reshape(-1), k2.reshape(-1)]))
+
+
+def dam_break(n=128, seed=0, column=(0.4, 0.6), pool=0.15, rho_water=1000.0, rho_air=1.0):
+    """Dam break: a water column (x < 0.4, y < 0.6) beside a pool 0.15 deep,
+    eight particles per water cell (type 0) at rest, the air above empty."""
+    dims = (n, n, n)
+    dx = 1.0 / n
+    i, j, k = dam_break_cells(n, column, pool)
+    pos, _ = _seed_cells(i, j, k, dims, dx, seed)
+    pos = pos.astype(np.float32)
+    typ = np.zeros(len(pos), np.uint8)
+    vel = np.zeros_like(pos)
+    vol = np.ones(len(pos), np.float32)
+    return dict(name=f"dam_break_{n}", nx=n, ny=n, nz=n, dx=dx, pos=pos, vel=vel, type=typ, volume=vol,
+                rho_l=rho_water, rho_g=rho_air)
+
+
 def ellipsoid_pressure(n=256, seed=0, n_ellipsoids=64, semi=(0.02, 0.08), kmax=8, rho_background=1000.0,
                        rho_bubble=1.0):
     """Pressure-only system on an n^3 grid: every interior cell fluid, solid

@@ -522,10 +522,12 @@ class SparseSim3DTP:
 
     def seed_scene(self, scene, seed=0):
         """Seed the resident particle set on the device with a benchmark scene
-        ("rayleigh_taylor" or "bubble_tank", pf_seed_scene): the particles
-        scenes.rayleigh_taylor / scenes.bubble_tank give for this grid and seed.
+        ("rayleigh_taylor", "bubble_tank" or "dam_break", pf_seed_scene): the
+        particles the scenes module's generator of that name gives for this
+        grid and seed.
         Returns the particle count."""
-        kind = {"rayleigh_taylor": L.PF_SCENE_RAYLEIGH_TAYLOR, "bubble_tank": L.PF_SCENE_BUBBLE_TANK}[scene]
+        kind = {"rayleigh_taylor": L.PF_SCENE_RAYLEIGH_TAYLOR, "bubble_tank": L.PF_SCENE_BUBBLE_TANK,
+                "dam_break": L.PF_SCENE_DAM_BREAK}[scene]
         n = C.c_size_t()
         L.check(self.grid.lib.pf_seed_scene(self.grid.ctx, kind, int(seed), C.byref(n)), self.grid.ctx, "pf_seed_scene")
         self.n = int(n.value)

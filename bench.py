@@ -601,6 +601,94 @@ def run_full_step(pf, n=48, steps=20, seed=0, solvers=("plain",), warmup=3):
     return out
 
 
+def mr_dam_break_layout(pf, n):
+    """The multires dam break's layout at n^3 fine cells: level-1 blocks
+    refined where water and empty cells lie within 3 cells of each other."""
+    i, j, k = pf.scenes.dam_break_cells(n)
+    liquid = np.zeros((n, n, n), bool)
+    liquid[k, j, i] = True
+    return pf.multires.interface_levels(liquid, 3)
+
+
+def run_multires_step(pf, n=256, steps=5, warmup=2, cpu_n=48, cpu=True, seed=0):
+    """The 2-level multires step (pf_mr_step, the reference's MRSim3DTP::step)
+    on the dam break at n^3 fine cells: a water column beside a pool, eight
+    particles per water cell, 1000:1, dt 1/480, a static layout refined where
+    water and empty cells lie within 3 cells of each other, the reference's
+    default pressure solve (Jacobi PCG with adaptive restart, 160 iterations,
+    tolerance max(1e-7, 1e-6 max|r0|)).  Device-timed particles/s and the
+    stage times; beside it the reference's own MRSim3DTP::step on the same
+    scene and layout rule at cpu_n^3 on one host core."""
+    import torch
+    sim = pf.MRSim3DTP(n, n, n, 1.0 / n, max_particles=8 * n ** 3 // 2)
+    sim.phase = pf.PhaseParams(1000.0, 1.0)
+    sim.phase.rho_tilde_0 = pf.calibrateRhoTilde0(sim.phase, 1.0, sim.grid)
+    sim.dt = 1.0 / 480.0
+    sim.dynamic_refinement = False
+    npart = sim.seed_scene("dam_break", seed)
+    levels = mr_dam_break_layout(pf, n)
+    sim.set_levels(levels)
+    lib = pf.load()
+    stream = torch.cuda.ExternalStream(lib.pf_stream(sim.ctx))
+    for _ in range(warmup):
+        sim.step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    iters, conv, cells = 0, 0, 0
+    e0.record(stream)
+    for _ in range(steps):
+        st = sim.step()
+        iters += st.iterations
+        conv += st.converged
+        cells = st.active_cells
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    # stage times over two more steps, outside the timed region
+    lib.pf_set_timing(sim.ctx, 1)
+    tm = pf._lib.Timing()
+    lib.pf_get_timing(sim.ctx, C.byref(tm), 1)
+    for _ in range(2):
+        last = sim.step()
+    lib.pf_get_timing(sim.ctx, C.byref(tm), 1)
+    lib.pf_set_timing(sim.ctx, 0)
+    stages = {k: v[0] / 2 for k, v in tm.as_dict().items() if v[1]}
+    fine_blocks = int(levels.sum())
+    out = {"workload": f"dam_break_{n} multires: {npart} particles, 2 levels ({fine_blocks} of {levels.size} "
+                       f"8^3 blocks fine), 1000:1, dt 1/480, MRSim3DTP default PCG, {warmup} warm-up + {steps} "
+                       f"timed steps",
+           "particles_per_s": npart / (ms / 1000.0), "ms_per_step": ms, "unknowns": cells,
+           "pcg_iterations_per_step": iters / steps, "converged_steps": conv,
+           "final_relative_residual": last.final_residual / max(last.initial_residual, 1e-300),
+           "stages_ms_per_step": stages}
+    sim.close()
+    if cpu:
+        from oracle.multires import MRSettings, ReferenceMR
+        import oracle as O
+        sc = pf.scenes.dam_break(cpu_n, seed=seed)
+        ph = O.PhaseParams(1000.0, 1.0)
+        ph.rho_tilde_0 = O.Oracle().calibrate_rho_tilde0(ph, 1.0)
+        r = ReferenceMR(cpu_n, cpu_n, cpu_n, 1.0 / cpu_n,
+                        MRSettings(dt=1.0 / 480.0, phase=ph, dynamic_refinement=False))
+        lv = mr_dam_break_layout(pf, cpu_n)
+        r.set_layout([(8 * bx, 8 * by, 8 * bz, 8 * bx + 8, 8 * by + 8, 8 * bz + 8)
+                      for bz, by, bx in zip(*np.nonzero(lv))])
+        r.set_particles(sc["pos"].astype(np.float64), sc["vel"].astype(np.float64), sc["type"])
+        r.step()  # warm-up
+        times = []
+        for _ in range(2):
+            t0 = time.perf_counter()
+            r.step()
+            times.append(time.perf_counter() - t0)
+        mean = sum(times) / len(times)
+        out["cpu_reference"] = {"particles_per_s": len(sc["pos"]) / mean, "s_per_step": mean, "cores": 1,
+                                "sample": f"the reference's MRSim3DTP::step on the dam break at {cpu_n}^3 "
+                                          f"({len(sc['pos'])} particles, same layout rule), 1 warm-up + 2 timed "
+                                          f"steps"}
+        out["speedup_vs_cpu_reference"] = out["particles_per_s"] / out["cpu_reference"]["particles_per_s"]
+    return out
+
+
 def run_pressure_cpu(pf, n=48, seed=0):
     """The reference's own projection (spProjectStepVC3D from oracle/_ref, the
     unmodified sources; single-threaded) on the pressure system of the first
@@ -803,6 +891,7 @@ def run_ours(args, rank, world, local, dist):
         line["full_step"] = run_full_step(pf, n=args.full_step_n, steps=args.full_step_steps,
                                           solvers=("plain", "learned"))
         line["adaptivity"] = run_adapt(pf, n=args.adapt_n, cpu=not args.no_cpu_baseline)
+        line["multires_step"] = run_multires_step(pf, n=args.mr_n, steps=args.mr_steps, cpu=not args.no_cpu_baseline)
         if not args.no_cpu_baseline:
             line["pressure_cpu_baseline"] = run_pressure_cpu(pf)
     if rank == 0 and not args.no_cpu_baseline:
@@ -878,6 +967,9 @@ def main():
     ap.add_argument("--full-step-only", action="store_true", help="run only the full-step block")
     ap.add_argument("--adapt-n", type=int, default=128, help="grid of the particle-adaptivity block")
     ap.add_argument("--adapt-only", action="store_true", help="run only the particle-adaptivity block")
+    ap.add_argument("--mr-n", type=int, default=256, help="fine grid of the multires block (dam break)")
+    ap.add_argument("--mr-steps", type=int, default=5, help="timed steps of the multires block")
+    ap.add_argument("--mr-only", action="store_true", help="run only the multires block")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
@@ -889,6 +981,11 @@ def main():
     if args.adapt_only:  # the particle-adaptivity block alone
         pf = load_pkg()
         print(json.dumps(run_adapt(pf, n=args.adapt_n, cpu=not args.no_cpu_baseline)), flush=True)
+        return
+    if args.mr_only:  # the multires block alone
+        pf = load_pkg()
+        print(json.dumps(run_multires_step(pf, n=args.mr_n, steps=args.mr_steps, cpu=not args.no_cpu_baseline)),
+              flush=True)
         return
     if args.full_step_only:  # the full-step block alone
         pf = load_pkg()

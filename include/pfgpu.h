@@ -19,6 +19,9 @@
  *     call order of src/driver/sparse_sim3d_tp.cpp:22-97, 854-884)
  *                                                       -> pf_mark_cells,
  *        pf_apply_gravity, pf_apply_wall_boundary, pf_save_velocity, pf_step
+ *   MRSim3DTP::step, 2-level multires (src/driver/multires_sim3d_tp.cpp:671-733),
+ *     mrP2G3D_tp (src/driver/multires_ops3d_tp.h:8)   -> pf_mr_step, pf_mr_p2g,
+ *        pf_mr_set_layout, pf_mr_set_dynamic, pf_mr_update_refinement
  *   SparseMacGrid3D<4> / SparseBlockGrid3D<4> storage
  *     (src/grid/sparse_mac_grid3d.h:6-47, src/grid/sparse_block_grid3d.h:10-68)
  *                                                       -> pf_grid_set_field,
@@ -322,7 +325,10 @@ PFGPU_API int pf_get_adaptivity_stats(const pf_ctx* ctx, pf_adapt_stats* out);
 /* ---- per-stage device timing (CUDA events on the context stream) -------
  * Off by default.  When on, every solver-step entry point brackets its
  * stages with events; pf_get_timing synchronises and returns the summed
- * device milliseconds and launch counts per stage since the last reset. */
+ * device milliseconds and launch counts per stage since the last reset.
+ * pf_mr_step reports its refinement as ADAPT, markCells as MARK, P2G as
+ * SPLAT, the saved copy, gravity and walls as BOUNDARY, the projection as
+ * PROJECT (its PCG iterations as PCG) and G2P with advection as G2P. */
 enum pf_stage {
   PF_STAGE_BIN = 0,      /* particle binning + exact 4^3 activation + pool growth */
   PF_STAGE_SORT,         /* tile offsets scan + particle permutation */
@@ -393,12 +399,16 @@ PFGPU_API int pf_project_noalloc(int nx, int ny, int nz, double dx, const float*
  *     y = 0.5 + 0.05 cos(2 pi x) cos(2 pi z), type 1 below; zero velocity;
  *   PF_SCENE_BUBBLE_TANK: interior cells whose centre lies below y = 0.7;
  *     type 1 inside the sphere of radius 0.15 at (0.5, 0.3, 0.5), type 0
- *     elsewhere; velocities N(0, 0.1^2) per component.
+ *     elsewhere; velocities N(0, 0.1^2) per component;
+ *   PF_SCENE_DAM_BREAK: a water column (interior cells whose centre has
+ *     x < 0.4 and y < 0.6), then a pool beside it (y < 0.15); type 0, zero
+ *     velocity, the air empty (the multires configuration's scene).
  * Volumes are 1.  Positions are bit-identical to the host generator of the
  * same seed (adaptive-pf-flip_b200/scenes.py).  *n_out receives the count;
  * PF_ERR_CAPACITY if it exceeds max_particles. */
 #define PF_SCENE_RAYLEIGH_TAYLOR 0
 #define PF_SCENE_BUBBLE_TANK 1
+#define PF_SCENE_DAM_BREAK 2
 PFGPU_API int pf_seed_scene(pf_ctx* ctx, int scene, unsigned long long seed, size_t* n_out);
 
 /* calibrateRhoTilde0 (src/transfer/transfer3d_tp.cpp:29-36), on the device. */

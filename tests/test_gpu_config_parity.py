@@ -273,7 +273,8 @@ def test_active_cells_match_reference_collect(pf, case):
 
 
 @pytest.mark.parametrize("scene,n,seed", [("rayleigh_taylor", 24, 0), ("rayleigh_taylor", 40, 3),
-                                          ("bubble_tank", 32, 0), ("bubble_tank", 48, 5)])
+                                          ("bubble_tank", 32, 0), ("bubble_tank", 48, 5), ("dam_break", 32, 2),
+                                          ("dam_break", 45, 7)])
 def test_device_scene_equals_host_generator(pf, scene, n, seed):
     """pf_seed_scene against scenes.py: positions and types identical, volumes
     1, bubble-tank velocities within one FP32 ulp (Box-Muller on the device's
