@@ -40,7 +40,6 @@ namespace pf {
 namespace {
 
 constexpr int kMrNT = 256;
-constexpr int kMrRedBlocks = 592;  // 4 CTAs per SM
 constexpr int kMrPoll = 16;        // PCG iterations launched between polls
 
 struct MrGeom {
@@ -68,13 +67,15 @@ struct MrState {
   uint8_t* refined = nullptr;
   std::vector<uint8_t> h_refined;
   float* f[9] = {};      // u v w mu mv mw, the saved u v w
+  float2* acc[3] = {};   // P2G scratch: (momentum, raw mass) per face
   uint8_t* mk = nullptr; // per fine cell
   float* pcell = nullptr;
   int* cell_idx = nullptr;
   int *flag0 = nullptr, *pos0 = nullptr, *flag1 = nullptr, *pos1 = nullptr;
   int4* cells = nullptr;  // fluid leaf cells: fine origin and level
-  int* row_len = nullptr;
-  int* row_ptr = nullptr;
+  int* row_len = nullptr;    // off-diagonal terms per row
+  int* slice_len = nullptr;  // entries per 32-row slice (32 x its longest row)
+  int* slice_ptr = nullptr;  // exclusive scan of slice_len
   int* col = nullptr;
   double* coef = nullptr;
   size_t nnz_cap = 0;
@@ -337,56 +338,88 @@ __global__ void k_mr_mark_particles(MrGeom g, const float* px, const float* py, 
 
 // ---- P2G (src/driver/multires_ops3d_tp.cpp:20-130, 209-274) --------------
 
-__device__ __forceinline__ double mr_kernel(double d2) {
-  const double r = 1.5;
-  const double q = d2 / (r * r);
-  const double t = 1.0 - q;
-  return t > 0.0 ? t * t * t : 0.0;
-}
 
 // One axis of one particle: the weights of the leaf-boundary patches within
 // the kernel radius (collectWeightedFaces: (k, j, i) order, clamped ranges),
 // normalised by their sum, splatted into momentum and raw mass.  The two
 // passes evaluate each weight with the same operations, so the sum is the
 // reference's.
-__device__ __forceinline__ void mr_splat_axis(const MrGeom& g, int axis, double px, double py, double pz, double mp,
-                                              double v, float* mom, float* mass) {
+// One axis of one particle: the weights of the leaf-boundary patches within
+// the kernel radius (collectWeightedFaces: every lattice patch with
+// |d| < 1.5 per axis, at most 3 per axis), normalised by their sum and handed
+// to sink(i, j, k, momentum, mass).  The squared distance splits per axis, so
+// the 3 + 3 + 3 squared offsets are formed once and each of the 27 weights
+// costs two adds and the cubic; the arithmetic is FP32 (the reference's
+// FP64 weights to within FP32 rounding).  Patch validity is tested per patch
+// only where the candidates straddle both levels.
+template <class Sink>
+__device__ __forceinline__ void mr_splat_axis(const MrGeom& g, int axis, double px, double py, double pz, float mp,
+                                              float v, Sink&& sink) {
   const double c[3] = {px, py, pz};
   const int n[3] = {g.nx, g.ny, g.nz};
-  int lo[3], hi[3];
+  int p0[3], cnt[3];
+  float e[3];  // offset of the particle from the first candidate, per axis
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     const double s = d == axis ? c[d] : c[d] - 0.5;
     const int top = d == axis ? n[d] : n[d] - 1;
-    lo[d] = max(0, min(top, (int)floor(s - 1.5)));
-    hi[d] = max(0, min(top, (int)ceil(s + 1.5)));
+    const int first = (int)floor(s - 1.5) + 1;  // the first integer above s - 1.5
+    const int lo = max(first, 0), hi = min(first + 2, top);
+    p0[d] = lo;
+    cnt[d] = max(0, hi - lo + 1);
+    e[d] = (float)(s - (double)lo);
   }
-  double wsum = 0.0;
+  if (cnt[0] == 0 || cnt[1] == 0 || cnt[2] == 0) return;
+  // the levels of the blocks the candidates' cells can lie in (along the
+  // axis the cells on both sides of each patch)
+  int mode;  // 0 all refined, 1 all coarse, 2 mixed
+  {
+    int cl[3], ch[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      cl[d] = max(0, p0[d] - (d == axis ? 1 : 0));
+      ch[d] = min(n[d] - 1, p0[d] + cnt[d] - 1);
+    }
+    int nref = 0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) nref += mr_refined(g, q & 1 ? ch[0] : cl[0], q & 2 ? ch[1] : cl[1], q & 4 ? ch[2] : cl[2]);
+    mode = nref == 8 ? 0 : nref == 0 ? 1 : 2;
+  }
+  const int na = n[axis];
+  float wsum = 0.0f;
+#pragma unroll 1
   for (int pass = 0; pass < 2; ++pass) {
-    for (int k = lo[2]; k <= hi[2]; ++k) {
-      const double dz = pz - (axis == 2 ? (double)k : (double)k + 0.5);
-      if (dz * dz >= 2.25) continue;  // weight 0 for every (i, j)
-      for (int j = lo[1]; j <= hi[1]; ++j) {
-        const double dy = py - (axis == 1 ? (double)j : (double)j + 0.5);
-        if (dy * dy >= 2.25) continue;
-        for (int i = lo[0]; i <= hi[0]; ++i) {
-          const double dx = px - (axis == 0 ? (double)i : (double)i + 0.5);
-          const double w = mr_kernel(dx * dx + dy * dy + dz * dz);
-          if (w <= 0.0) continue;
-          if (!mr_face_valid(g, axis, i, j, k)) continue;
+    const float inv = pass ? 1.0f / wsum : 0.0f;
+#pragma unroll 1
+    for (int k = 0; k < cnt[2]; ++k) {
+      const float dz = e[2] - (float)k;
+#pragma unroll 1
+      for (int j = 0; j < cnt[1]; ++j) {
+        const float dy = e[1] - (float)j;
+        const float dyz = dy * dy + dz * dz;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+          if (i >= cnt[0]) continue;
+          const float dx = e[0] - (float)i;
+          const float t = 1.0f - (dx * dx + dyz) * (1.0f / 2.25f);
+          if (!(t > 0.0f)) continue;
+          const int fi = p0[0] + i, fj = p0[1] + j, fk = p0[2] + k;
+          if (mode != 0) {
+            const int pos = axis == 0 ? fi : axis == 1 ? fj : fk;
+            const bool edge = (pos & 1) == 0 || pos == na;
+            if (!edge && (mode == 1 || !mr_face_valid(g, axis, fi, fj, fk))) continue;
+          }
+          const float w = t * t * t;
           if (pass == 0) {
             wsum += w;
           } else {
-            const double wn = w / wsum;
-            if (wn <= 0.0) continue;
-            const size_t f = mr_face(g, axis, i, j, k);
-            atomicAdd(&mom[f], (float)(wn * mp * v));
-            atomicAdd(&mass[f], (float)(wn * mp));
+            const float wn = w * inv;
+            sink(fi, fj, fk, wn * mp * v, wn * mp);
           }
         }
       }
     }
-    if (!(wsum > 0.0)) return;
+    if (!(wsum > 0.0f)) return;
   }
 }
 
@@ -394,23 +427,35 @@ struct MrFaces {
   float* f[9];
 };
 
+// P2G: one thread per particle (memory order), the momentum and raw mass of
+// a patch added together by one vector atomic into an interleaved scratch
+// lattice; k_mr_split then writes u = momentum / mass (where mass > 0) and
+// the mass.  Accumulation order is the atomics' (not the reference's
+// particle order).
 __global__ void __launch_bounds__(kMrNT) k_mr_p2g(MrGeom g, const float* px, const float* py, const float* pz,
                                                 const float* vx, const float* vy, const float* vz, const float* vol,
-                                                const uint8_t* type, size_t n, double mpl, double mpg, MrFaces F) {
+                                                const uint8_t* type, size_t n, double mpl, double mpg, float2* acc0,
+                                                float2* acc1, float2* acc2) {
   const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n) return;
-  const double mp = (type[q] == 0 ? mpl : mpg) * (double)vol[q];
+  const float mp = (float)((type[q] == 0 ? mpl : mpg) * (double)vol[q]);
   const double x = (double)px[q] / g.dx, y = (double)py[q] / g.dx, z = (double)pz[q] / g.dx;
-  mr_splat_axis(g, 0, x, y, z, mp, (double)vx[q], F.f[0], F.f[3]);
-  mr_splat_axis(g, 1, x, y, z, mp, (double)vy[q], F.f[1], F.f[4]);
-  mr_splat_axis(g, 2, x, y, z, mp, (double)vz[q], F.f[2], F.f[5]);
+  const float v0 = vx[q], v1 = vy[q], v2 = vz[q];
+#pragma unroll 1
+  for (int a = 0; a < 3; ++a) {
+    float2* acc = a == 0 ? acc0 : a == 1 ? acc1 : acc2;
+    mr_splat_axis(g, a, x, y, z, mp, a == 0 ? v0 : a == 1 ? v1 : v2, [&](int i, int j, int k, float m, float w) {
+      atomicAdd(&acc[mr_face(g, a, i, j, k)], make_float2(m, w));
+    });
+  }
 }
 
-// momentum / mass where the mass is positive
-__global__ void k_mr_normalize(float* mom, const float* mass, size_t n) {
+// u = momentum / mass where the mass is positive (else the momentum, 0), mass
+__global__ void k_mr_split(const float2* __restrict__ acc, float* u, float* mass, size_t n) {
   for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
-    const float m = mass[e];
-    if (m > 0.0f) mom[e] = mom[e] / m;
+    const float2 a = acc[e];
+    mass[e] = a.y;
+    u[e] = a.y > 0.0f ? a.x / a.y : a.x;
   }
 }
 
@@ -539,16 +584,32 @@ __global__ void k_mr_row_count(MrGeom g, const uint8_t* mk, const int4* cells, c
   }
 }
 
+// The rows are stored as 32-row slices (sliced ELLPACK): term t of row r is
+// entry slice_ptr[r / 32] + 32 t + r % 32, so a warp's 32 rows load each term
+// position together; a slice is as wide as its longest row and shorter rows
+// end in (col = r, coef = 0) terms, which add an exact zero.  Each row keeps
+// its terms in the reference's visit order.
+__global__ void k_mr_slices(int N, const int* row_len, int* slice_len) {
+  const int nslice = (N + 31) / 32;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s <= nslice; s += gridDim.x * blockDim.x) {
+    int w = 0;
+    if (s < nslice)
+      for (int r = 32 * s; r < min(N, 32 * s + 32); ++r) w = max(w, row_len[r]);
+    slice_len[s] = 32 * w;
+  }
+}
+
 struct MrVecs {
   double *x, *r, *z, *p, *Ap, *diag;
 };
 
 // rows (:788-822): diagonal, off-diagonal terms and right-hand side; then
-// x = 0, r = b, z = M^-1 r, p = z, and r.z, max|r| -> tolerance
+// x = 0, r = b, z = M^-1 r, p = 0 (the first direction is z), and r.z,
+// max|r| -> tolerance
 __global__ void __launch_bounds__(kMrNT) k_mr_rows(MrGeom g, const uint8_t* mk, const int4* cells,
                                                  const int* cell_idx, int N, const int* air, MrFaces F, MrPhase P,
-                                                 double dt, double c_div, const int* row_ptr, int* col, double* coef,
-                                                 MrVecs V, MrCtl* ctl, double* partials) {
+                                                 double dt, double c_div, const int* slice_ptr, int* col,
+                                                 double* coef, MrVecs V, MrCtl* ctl, double* partials) {
   const int pin = mr_pin(air, N);
   const double area = g.dx * g.dx * 1.0 * 1.0;
   const int jacobi = ctl->jacobi;
@@ -558,10 +619,12 @@ __global__ void __launch_bounds__(kMrNT) k_mr_rows(MrGeom g, const uint8_t* mk, 
     const double h = g.dx * (double)(1 << c.w);
     const double vol = h * h * h;
     double diag = 0.0, div = 0.0;
+    const int base = slice_ptr[r >> 5] + (r & 31);
+    const int width = (slice_ptr[(r >> 5) + 1] - slice_ptr[r >> 5]) >> 5;
+    int t = 0;
     if (r == pin) {
       diag = 1.0;
     } else {
-      int at = row_ptr[r];
       mr_visit(g, c, [&](int axis, int fi, int fj, int fk, int ni, int nj, int nk, double sign) {
         const int m = mr_marker(g, mk, ni, nj, nk);
         if (m == 2) return;
@@ -578,12 +641,16 @@ __global__ void __launch_bounds__(kMrNT) k_mr_rows(MrGeom g, const uint8_t* mk, 
         diag += coeff;
         const int o = mr_in(g, ni, nj, nk) ? cell_idx[mr_cell(g, ni, nj, nk)] : -1;
         if (o >= 0 && o != pin) {
-          col[at] = o;
-          coef[at] = coeff;
-          ++at;
+          col[base + 32 * t] = o;
+          coef[base + 32 * t] = coeff;
+          ++t;
         }
         div += sign * (double)F.f[axis][f] * area / vol;
       });
+    }
+    for (; t < width; ++t) {
+      col[base + 32 * t] = r;
+      coef[base + 32 * t] = 0.0;
     }
     const double b = r == pin ? 0.0 : -div + c_div;
     V.diag[r] = diag;
@@ -591,30 +658,53 @@ __global__ void __launch_bounds__(kMrNT) k_mr_rows(MrGeom g, const uint8_t* mk, 
     V.r[r] = b;
     const double z = (jacobi && diag > 0.0) ? b / diag : b;
     V.z[r] = z;
-    V.p[r] = z;
+    V.p[r] = 0.0;
     rz += b * z;
     rmax = fmax(rmax, fabs(b));
   }
   mr_reduce(rz, 0.0, 0.0, rmax, partials, ctl, kMrInit);
 }
 
-// Ap (applyA, :824-838) and p.Ap -> alpha
-__global__ void __launch_bounds__(kMrNT) k_mr_spmv(int N, const int* row_ptr, const int* col, const double* coef,
-                                                 MrVecs V, MrCtl* ctl, double* partials, const int* air) {
+// The direction p = z + beta p_prev (the previous iteration's update, or a
+// restart's beta = 0) formed where it is used, Ap (applyA, :824-838) and
+// p.Ap -> alpha.  p_prev and p are separate buffers, alternated by the host.
+__global__ void __launch_bounds__(kMrNT) k_mr_spmv(int N, const int* __restrict__ slice_ptr,
+                                                 const int* __restrict__ col, const double* __restrict__ coef,
+                                                 const double* __restrict__ z, const double* __restrict__ p_prev,
+                                                 double* p, double* Ap, const double* __restrict__ diag, MrCtl* ctl,
+                                                 double* partials, const int* air) {
   if (ctl->done) return;
   const int pin = mr_pin(air, N);
+  const double beta = ctl->beta;
   double pap = 0.0;
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < N; r += gridDim.x * blockDim.x) {
-    const double pr = V.p[r];
+    const double pr = z[r] + beta * p_prev[r];
     double ap;
     if (r == pin) {
       ap = pr;
     } else {
+      const int s = r >> 5;
+      const int b0 = slice_ptr[s] + (r & 31), width = (slice_ptr[s + 1] - slice_ptr[s]) >> 5;
+      // the loads of four terms go out together; the sum keeps the term order
       double off = 0.0;
-      for (int t = row_ptr[r]; t < row_ptr[r + 1]; ++t) off += coef[t] * V.p[col[t]];
-      ap = V.diag[r] * pr - off;
+      for (int t = 0; t < width; t += 4) {
+        int cc[4];
+        double cf[4], pv[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          cc[u] = t + u < width ? col[b0 + 32 * (t + u)] : r;
+          cf[u] = t + u < width ? coef[b0 + 32 * (t + u)] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) pv[u] = z[cc[u]] + beta * p_prev[cc[u]];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          if (t + u < width) off += cf[u] * pv[u];
+      }
+      ap = diag[r] * pr - off;
     }
-    V.Ap[r] = ap;
+    p[r] = pr;
+    Ap[r] = ap;
     pap += pr * ap;
   }
   mr_reduce(pap, 0.0, 0.0, 0.0, partials, ctl, kMrPAp);
@@ -641,14 +731,6 @@ __global__ void __launch_bounds__(kMrNT) k_mr_update(int N, MrVecs V, MrCtl* ctl
     if (flexible) num += rr * (z - zp);
   }
   mr_reduce(rz, num, bad, rmax, partials, ctl, kMrUpdate);
-}
-
-// p = z + beta p
-__global__ void k_mr_dir(int N, MrVecs V, const MrCtl* ctl) {
-  if (ctl->done) return;
-  const double beta = ctl->beta;
-  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < N; r += gridDim.x * blockDim.x)
-    V.p[r] = V.z[r] + beta * V.p[r];
 }
 
 __global__ void k_mr_ctl_init(MrCtl* ctl, int max_iter, double abs_tol, double rel_tol, int jacobi, int flexible,
@@ -867,6 +949,7 @@ int mr_state(pf_ctx* ctx, MrState** out) {
     PF_CUDA_TRY(cudaMalloc(&s->f[q], s->nface[q % 3] * sizeof(float)));
     PF_CUDA_TRY(cudaMemset(s->f[q], 0, s->nface[q % 3] * sizeof(float)));
   }
+  for (int a = 0; a < 3; ++a) PF_CUDA_TRY(cudaMalloc(&s->acc[a], s->nface[a] * sizeof(float2)));
   PF_CUDA_TRY(cudaMalloc(&s->mk, s->ncell));
   PF_CUDA_TRY(cudaMemset(s->mk, 0, s->ncell));
   PF_CUDA_TRY(cudaMalloc(&s->pcell, s->ncell * sizeof(float)));
@@ -878,13 +961,14 @@ int mr_state(pf_ctx* ctx, MrState** out) {
   PF_CUDA_TRY(cudaMalloc(&s->pos1, (s->nkey1 + 1) * sizeof(int)));
   PF_CUDA_TRY(cudaMalloc(&s->cells, s->ncell * sizeof(int4)));
   PF_CUDA_TRY(cudaMalloc(&s->row_len, (s->ncell + 1) * sizeof(int)));
-  PF_CUDA_TRY(cudaMalloc(&s->row_ptr, (s->ncell + 2) * sizeof(int)));
+  PF_CUDA_TRY(cudaMalloc(&s->slice_len, (s->ncell / 32 + 3) * sizeof(int)));
+  PF_CUDA_TRY(cudaMalloc(&s->slice_ptr, (s->ncell / 32 + 3) * sizeof(int)));
   PF_CUDA_TRY(cudaMalloc(&s->minmax, 16 * sizeof(int)));
   PF_CUDA_TRY(cudaMalloc(&s->counters, 16 * sizeof(int)));
   PF_CUDA_TRY(cudaMalloc(&s->ctl, sizeof(MrCtl)));
   PF_CUDA_TRY(cudaMallocHost(&s->h_ctl, sizeof(MrCtl)));
   PF_CUDA_TRY(cudaMallocHost(&s->h_ints, 32 * sizeof(int)));
-  PF_CUDA_TRY(cudaMalloc(&s->partials, 4 * kMrRedBlocks * sizeof(double)));
+  PF_CUDA_TRY(cudaMalloc(&s->partials, 4 * (s->ncell / kMrNT + 2) * sizeof(double)));
   PF_CUDA_TRY(cudaEventCreate(&s->e0));
   PF_CUDA_TRY(cudaEventCreate(&s->e1));
   *out = s;
@@ -1078,16 +1162,16 @@ int mark_cells_mr(pf_ctx* ctx, MrState* s) {
 
 int p2g_mr(pf_ctx* ctx, MrState* s, const pf_phase* ph, double Vp) {
   StageScope stage(ctx, PF_STAGE_SPLAT);
-  for (int q = 0; q < 6; ++q)
-    PF_CUDA_TRY(cudaMemsetAsync(s->f[q], 0, s->nface[q % 3] * sizeof(float), ctx->stream));
+  for (int a = 0; a < 3; ++a)
+    PF_CUDA_TRY(cudaMemsetAsync(s->acc[a], 0, s->nface[a] * sizeof(float2), ctx->stream));
   const size_t n = ctx->np;
   if (n > 0)
     (++ctx->launches), k_mr_p2g<<<grid_for(n, INT_MAX), kMrNT, 0, ctx->stream>>>(
         s->g, ctx->px, ctx->py, ctx->pz, ctx->vx, ctx->vy, ctx->vz, ctx->vol, ctx->type, n, ph->rho_l * Vp,
-        ph->rho_g * Vp, faces_of(s));
+        ph->rho_g * Vp, s->acc[0], s->acc[1], s->acc[2]);
   for (int a = 0; a < 3; ++a)
-    (++ctx->launches), k_mr_normalize<<<grid_for(s->nface[a], 8 * ctx->num_sms), kMrNT, 0, ctx->stream>>>(
-        s->f[a], s->f[3 + a], s->nface[a]);
+    (++ctx->launches), k_mr_split<<<grid_for(s->nface[a], 8 * ctx->num_sms), kMrNT, 0, ctx->stream>>>(
+        s->acc[a], s->f[a], s->f[3 + a], s->nface[a]);
   PF_CUDA_TRY(cudaGetLastError());
   return PF_OK;
 }
@@ -1123,8 +1207,10 @@ int project_mr(pf_ctx* ctx, MrState* s, const pf_mr_step_cfg* cfg, pf_mr_step_st
   (++ctx->launches), k_mr_row_count<<<grid_for(N, big), kMrNT, 0, ctx->stream>>>(g, s->mk, s->cells, s->cell_idx, N,
                                                                                  tot + 3, s->row_len);
   PF_CUDA_TRY(cudaGetLastError());
-  PF_CUDA_TRY(cudaMemsetAsync(s->row_len + N, 0, sizeof(int), ctx->stream));
-  rc = scan_exclusive(ctx, s->row_len, s->row_ptr, N + 1, tot + 2);  // row_ptr[N] = total = nonzeros
+  const int nslice = (N + 31) / 32;
+  (++ctx->launches), k_mr_slices<<<grid_for(nslice + 1, big), kMrNT, 0, ctx->stream>>>(N, s->row_len, s->slice_len);
+  PF_CUDA_TRY(cudaGetLastError());
+  rc = scan_exclusive(ctx, s->slice_len, s->slice_ptr, nslice + 1, tot + 2);  // total = stored entries
   if (rc) return rc;
   PF_CUDA_TRY(cudaMemcpyAsync(s->h_ints + 2, tot + 2, 2 * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   PF_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
@@ -1143,15 +1229,19 @@ int project_mr(pf_ctx* ctx, MrState* s, const pf_mr_step_cfg* cfg, pf_mr_step_st
   }
   // the context's FP64 solver vectors (sized for every tile of the pool) hold
   // the multires unknowns: N <= nx ny nz <= their length
+  // the direction alternates between ctx->p and ctx->cy
   MrVecs V{ctx->x, ctx->r, ctx->cx, ctx->p, ctx->Ap, ctx->diag};
-  const int nred = grid_for(N, kMrRedBlocks);
+  double* pbuf[2] = {ctx->p, ctx->cy};
+  // 4 CTAs per SM: more CTAs spend more on the last-CTA reductions' atomics
+  // than they gain in load parallelism
+  const int nred = grid_for(N, 4 * ctx->num_sms);
   (++ctx->launches), k_mr_ctl_init<<<1, 1, 0, ctx->stream>>>(s->ctl, cfg->cg_iters, cfg->cg_tol, cfg->cg_rel_tol,
                                                              cfg->jacobi, cfg->flexible_beta, cfg->adaptive_restart,
                                                              cfg->restart_growth);
   PF_CUDA_TRY(cudaEventRecord(s->e0, ctx->stream));
   (++ctx->launches), k_mr_rows<<<nred, kMrNT, 0, ctx->stream>>>(g, s->mk, s->cells, s->cell_idx, N, tot + 3,
                                                                 faces_of(s), phase_of(&cfg->phase), cfg->dt,
-                                                                cfg->c_div, s->row_ptr, s->col, s->coef, V, s->ctl,
+                                                                cfg->c_div, s->slice_ptr, s->col, s->coef, V, s->ctl,
                                                                 s->partials);
   PF_CUDA_TRY(cudaGetLastError());
   MrCtl c{};
@@ -1164,10 +1254,14 @@ int project_mr(pf_ctx* ctx, MrState* s, const pf_mr_step_cfg* cfg, pf_mr_step_st
     if (c.done || launched >= cfg->cg_iters) break;
     const int batch = std::min(kMrPoll, cfg->cg_iters - launched);
     for (int b = 0; b < batch; ++b) {
-      (++ctx->launches), k_mr_spmv<<<nred, kMrNT, 0, ctx->stream>>>(N, s->row_ptr, s->col, s->coef, V, s->ctl,
-                                                                    s->partials, tot + 3);
-      (++ctx->launches), k_mr_update<<<nred, kMrNT, 0, ctx->stream>>>(N, V, s->ctl, s->partials);
-      (++ctx->launches), k_mr_dir<<<nred, kMrNT, 0, ctx->stream>>>(N, V, s->ctl);
+      const int q = (launched + b) & 1;
+      double* p_prev = pbuf[q];
+      double* p = pbuf[q ^ 1];
+      (++ctx->launches), k_mr_spmv<<<nred, kMrNT, 0, ctx->stream>>>(N, s->slice_ptr, s->col, s->coef, V.z, p_prev,
+                                                                    p, V.Ap, V.diag, s->ctl, s->partials, tot + 3);
+      MrVecs Vi = V;
+      Vi.p = p;
+      (++ctx->launches), k_mr_update<<<nred, kMrNT, 0, ctx->stream>>>(N, Vi, s->ctl, s->partials);
     }
     PF_CUDA_TRY(cudaGetLastError());
     launched += batch;
@@ -1199,8 +1293,9 @@ void mr_free(pf_ctx* ctx) {
   auto F = [](void* p) { if (p) cudaFree(p); };
   F(s->refined);
   for (int q = 0; q < 9; ++q) F(s->f[q]);
+  for (int a = 0; a < 3; ++a) F(s->acc[a]);
   F(s->mk); F(s->pcell); F(s->cell_idx); F(s->flag0); F(s->pos0); F(s->flag1); F(s->pos1); F(s->cells);
-  F(s->row_len); F(s->row_ptr); F(s->col); F(s->coef); F(s->minmax); F(s->counters); F(s->ctl); F(s->partials);
+  F(s->row_len); F(s->slice_len); F(s->slice_ptr); F(s->col); F(s->coef); F(s->minmax); F(s->counters); F(s->ctl); F(s->partials);
   if (s->h_ctl) cudaFreeHost(s->h_ctl);
   if (s->h_ints) cudaFreeHost(s->h_ints);
   if (s->e0) cudaEventDestroy(s->e0);

@@ -70,7 +70,10 @@ def test_mr_p2g_matches_oracle(pf):
     o.p2g()
     for f in range(6):
         g, c = sim.face(f), o.face(f)
-        assert np.array_equal(g != 0, c != 0), f"face field {f}: touched patches differ"
+        # FP32 weights: a patch at the kernel's edge may get a weight of order
+        # 1e-21 on one side only
+        tiny = 1e-9 * float(np.abs(c).max())
+        assert np.array_equal(np.abs(g) > tiny, np.abs(c) > tiny), f"face field {f}: touched patches differ"
         assert rel_err(g, c) < 1e-5, f"face field {f}: {rel_err(g, c)}"
     for ax in range(3):
         valid = o.face_valid(ax).astype(bool)
