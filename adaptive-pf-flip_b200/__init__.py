@@ -35,6 +35,7 @@ from .sparse import (ParticleEscapeBuffer3D, ParticleEscapeStats3D, Particles3DT
                      SparseMacGrid3D, SparseSim3DTP, applyGasParticleCoarsening, applyLiquidParticleRefill,
                      applyNarrowBandAir, applySparseSurfaceTension3D, applyTypedParticleCoarsening, betaFromPhi, calibrateRhoTilde0,
                      defaultRenderCacheCamera3D, densityFromPhi, diagnoseSparseInterface3D, etaPhi, phiFromRawDensity, spAdvect3D_tp, spG2P3D_tp, spP2G3D_tp, writeSparseRenderCache3D,
+                     RenderCacheManifestFrame3D, writeRenderCacheManifest3D,
                      spProjectStepVC3D)
 from . import scenes
 
@@ -49,5 +50,6 @@ __all__ = [
     "etaPhi", "phiFromRawDensity", "densityFromPhi", "betaFromPhi", "scenes",
     "applyNarrowBandAir", "applyTypedParticleCoarsening", "applyGasParticleCoarsening", "applyLiquidParticleRefill",
     "diagnoseSparseInterface3D", "applySparseSurfaceTension3D",
-    "writeSparseRenderCache3D", "defaultRenderCacheCamera3D",
+    "writeSparseRenderCache3D", "defaultRenderCacheCamera3D", "writeRenderCacheManifest3D",
+    "RenderCacheManifestFrame3D",
 ]

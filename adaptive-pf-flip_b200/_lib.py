@@ -44,6 +44,7 @@ EXPORTS = (
     "pf_default_render_camera", "pf_write_render_cache", "pf_seed_scene",
     "pf_mr_set_layout", "pf_mr_set_levels", "pf_mr_get_levels", "pf_mr_set_dynamic", "pf_mr_reset_refinement",
     "pf_mr_update_refinement", "pf_mr_step", "pf_mr_p2g", "pf_mr_get_face", "pf_mr_get_cells",
+    "pf_write_render_manifest",
 )
 
 STAGES = ("bin", "sort", "splat", "normalize", "mark", "boundary", "project", "pcg", "g2p", "precond_setup",
@@ -88,6 +89,11 @@ class ClampStats(C.Structure):
 class StepCfg(C.Structure):
     _fields_ = [("dt", C.c_double), ("gravity", C.c_double), ("Vp", C.c_double), ("alpha_l", C.c_double),
                 ("alpha_g", C.c_double), ("phase", Phase), ("solve", SolveCfg), ("advect_order", C.c_int)]
+
+
+class RenderManifestFrame(C.Structure):
+    _fields_ = [("frame", C.c_int), ("step", C.c_int), ("time", C.c_double), ("path", C.c_char_p),
+                ("bytes", C.c_longlong)]
 
 
 class MRBox(C.Structure):
@@ -271,6 +277,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "pf_mr_p2g": (i, [vp, P(Phase), d]),
         "pf_mr_get_face": (i, [vp, i, vp]),
         "pf_mr_get_cells": (i, [vp, vp, vp]),
+        "pf_write_render_manifest": (i, [C.c_char_p, C.c_char_p, i, i, i, d, P(RenderManifestFrame), i]),
         "pf_set_timing": (i, [vp, i]),
         "pf_get_timing": (i, [vp, P(Timing), i]),
         "pf_launch_count": (C.c_longlong, [vp]),

@@ -148,6 +148,28 @@ void write_bounds(std::ostream& out, const char* kmin, const char* kmax, const B
 
 bool finite3(const double v[3]) { return std::isfinite(v[0]) && std::isfinite(v[1]) && std::isfinite(v[2]); }
 
+// A JSON string literal with the escapes of writeJsonString
+// (src/driver/render_cache3d.h:121-146): quote, backslash and the named
+// control characters by their short escapes, other bytes below 0x20 as
+// \u00XX, everything else verbatim.
+void write_json_string(std::ostream& out, const char* s) {
+  static const char digits[] = "0123456789abcdef";
+  out << '"';
+  for (const unsigned char* p = (const unsigned char*)s; *p; ++p) {
+    const unsigned char c = *p;
+    if (c == '"') out << "\\\"";
+    else if (c == '\\') out << "\\\\";
+    else if (c == '\b') out << "\\b";
+    else if (c == '\f') out << "\\f";
+    else if (c == '\n') out << "\\n";
+    else if (c == '\r') out << "\\r";
+    else if (c == '\t') out << "\\t";
+    else if (c < 0x20) out << "\\u00" << digits[c >> 4] << digits[c & 15];
+    else out << (char)c;
+  }
+  out << '"';
+}
+
 }  // namespace
 
 // The export's device scratch, kept by the context and grown on demand.
@@ -407,6 +429,50 @@ int pf_default_render_camera(int nx, int ny, int nz, double dx, pf_render_camera
   *cam = pf_render_camera{{cx, cy + 0.2 * span, cz + 2.0 * span}, {cx, cy, cz}, {0.0, 1.0, 0.0}, 45.0,
                           0.05 * dx, 5.0 * span, 50.0};
   return PF_OK;
+}
+
+int pf_write_render_manifest(const char* path, const char* sim_kind, int nx, int ny, int nz, double dx,
+                             const pf_render_manifest_frame* frames, int n_frames) {
+  // requireValidPath and requireManifestArgs (:101-105, :149-164)
+  if (!path || !path[0] || !sim_kind || !sim_kind[0] || nx <= 0 || ny <= 0 || nz <= 0 || !(dx > 0.0) ||
+      !std::isfinite(dx) || n_frames < 0 || (n_frames > 0 && !frames))
+    return PF_ERR_INVALID;
+  for (int i = 0; i < n_frames; ++i) {
+    const pf_render_manifest_frame& f = frames[i];
+    if (f.frame < 0 || f.step < 0 || !f.path || !f.path[0] || f.bytes < 0 || !std::isfinite(f.time))
+      return PF_ERR_INVALID;
+  }
+  std::ofstream out(path);
+  if (!out) return PF_ERR_INVALID;
+  out << std::setprecision(17);
+  const double ex = nx * dx, ey = ny * dx, ez = nz * dx;
+  out << "{\n";
+  out << "  \"lsfs_cache3d_manifest_version\":1,\n";
+  out << "  \"cache_schema_version\":2,\n";
+  out << "  \"world_units\":\"cell\",\n";
+  out << "  \"sim_kind\":";
+  pf::write_json_string(out, sim_kind);
+  out << ",\n";
+  out << "  \"dims\":[" << nx << "," << ny << "," << nz << "],\n";
+  out << "  \"dx\":" << dx << ",\n";
+  out << "  \"frame_bounds_min\":[0,0,0],\n";
+  out << "  \"frame_bounds_max\":[" << ex << "," << ey << "," << ez << "],\n";
+  out << "  \"frame_count\":" << n_frames << ",\n";
+  out << "  \"frames\":[\n";
+  for (int i = 0; i < n_frames; ++i) {
+    const pf_render_manifest_frame& f = frames[i];
+    out << "    {\"frame\":" << f.frame << ",\"step\":" << f.step << ",\"time\":" << f.time
+        << ",\"shutter_open\":" << f.time << ",\"shutter_close\":" << f.time << ",\"frame_bounds_min\":[0,0,0]"
+        << ",\"frame_bounds_max\":[" << ex << "," << ey << "," << ez << "]"
+        << ",\"path\":";
+    pf::write_json_string(out, f.path);
+    out << ",\"bytes\":" << f.bytes << "}";
+    if (i + 1 < n_frames) out << ",";
+    out << "\n";
+  }
+  out << "  ]\n";
+  out << "}\n";
+  return out ? PF_OK : PF_ERR_INVALID;
 }
 
 }  // extern "C"

@@ -403,6 +403,31 @@ def writeSparseRenderCache3D(sim, path, frame, time, camera=None) -> int:
     return int(nbytes.value)
 
 
+@dataclass
+class RenderCacheManifestFrame3D:
+    """RenderCacheManifestFrame3D (src/driver/render_cache3d.h:39-45)."""
+    frame: int = 0
+    step: int = 0
+    time: float = 0.0
+    path: str = ""
+    bytes: int = 0
+
+
+def writeRenderCacheManifest3D(path, simKind, nx, ny, nz, dx, frames):
+    """writeRenderCacheManifest3D (src/driver/render_cache3d.h:711-755): the
+    JSON manifest of a frame sequence, written by the library's host code
+    (pf_write_render_manifest; no device needed).  Raises on the reference's
+    invalid arguments."""
+    lib = L.load()
+    keep = [str(f.path).encode() for f in frames]
+    arr = (L.RenderManifestFrame * max(1, len(frames)))(
+        *[L.RenderManifestFrame(int(f.frame), int(f.step), float(f.time), p, int(f.bytes)) for f, p in zip(frames, keep)])
+    rc = lib.pf_write_render_manifest(str(path).encode(), str(simKind).encode(), int(nx), int(ny), int(nz), float(dx),
+                                      arr, len(frames))
+    if rc:
+        raise ValueError("invalid render cache manifest metadata or unwritable path")
+
+
 def applySparseSurfaceTension3D(g: SparseMacGrid3D, pp: PhaseParams, dt, strength, maxDeltaSpeed,
                                 curvatureSmoothingRadius) -> L.SurfaceStats:
     """applySparseSurfaceTension3D (src/driver/interface_diagnostics3d.cpp:405-447) on the device."""

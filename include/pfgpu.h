@@ -528,12 +528,29 @@ PFGPU_API int pf_default_render_camera(int nx, int ny, int nz, double dx, pf_ren
  * grid and particles.  The phase cells are selected and compacted on the
  * device; the text uses the reference's number format (17 significant
  * digits).  dt is the step's effective dt, Vp the particle volume scale, cam
- * NULL for the default camera.  Cells are listed by ascending 4^3 block id
- * (the reference: marker-block activation order).  No secondary particles
- * exist here, so their sections are empty.  PF_ERR_INVALID for an empty path,
- * a file that cannot be written or the reference's invalid metadata. */
+ * NULL for the default camera.  Cells are listed as the reference lists
+ * them: marker blocks in the order markCells first activated them, cells in
+ * each block in lattice order.  No secondary particles exist here, so their
+ * sections are empty.  PF_ERR_INVALID for an empty path, a file that cannot
+ * be written or the reference's invalid metadata. */
 PFGPU_API int pf_write_render_cache(pf_ctx* ctx, const char* path, int frame, double time, double dt, const pf_phase* ph,
                           double Vp, const pf_render_camera* cam, long long* bytes_written);
+
+/* writeRenderCacheManifest3D (src/driver/render_cache3d.h:711-755): the JSON
+ * manifest of a sequence of render-cache frames, text identical to the
+ * reference's (17 significant digits, its string escaping).  Host only: no
+ * context or device is needed.  PF_ERR_INVALID for an empty path or sim_kind,
+ * non-positive dims or dx, a non-finite dx, a frame with a negative frame,
+ * step or byte count, an empty path or a non-finite time (the reference's
+ * checks), or a file that cannot be written. */
+typedef struct {
+  int frame, step;
+  double time;
+  const char* path;
+  long long bytes;
+} pf_render_manifest_frame;
+PFGPU_API int pf_write_render_manifest(const char* path, const char* sim_kind, int nx, int ny, int nz, double dx,
+                                       const pf_render_manifest_frame* frames, int n_frames);
 
 #ifdef __cplusplus
 }

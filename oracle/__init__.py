@@ -265,6 +265,9 @@ def ref_lib():
     lib.pfr_refill_liquid.argtypes = [vp, C.c_int, C.c_uint, C.c_int, C.c_int, C.c_int, _ip]
     lib.pfr_interface_diagnostics.argtypes = [vp, _dp, _ip, _dp]
     lib.pfr_surface_tension.argtypes = [vp, _dp, C.c_double, C.c_double, C.c_double, C.c_int, _ip, _dp]
+    lib.pfr_write_render_manifest.argtypes = [C.c_char_p, C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int,
+                                              _ip, _ip, _dp, C.POINTER(C.c_char_p),
+                                              np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")]
     lib._typed = True
     return lib
 

@@ -16,6 +16,7 @@
 //   applySparseSurfaceTension3D (src/driver/interface_diagnostics3d.cpp:405-447)
 //   sparse3d::collectCellsWithMarker (src/driver/sparse_ops3d_common.h:65-85)
 //   writeSparseRenderCache3D (src/driver/render_cache3d.h:617-663)
+//   writeRenderCacheManifest3D (src/driver/render_cache3d.h:711-755)
 //   MRSim3DTP (src/driver/multires_sim3d_tp.h:10-191): step(),
 //     initBubbleTankInterfaceBand(), updateDynamicRefinement(), and
 //     mrP2G3D_tp (src/driver/multires_ops3d_tp.cpp:209-274)
@@ -330,6 +331,21 @@ int pfr_surface_tension(void* hp, const double* phase, double dt, double strengt
   return 0;
 }
 
+
+// writeRenderCacheManifest3D (src/driver/render_cache3d.h:711-755) for frames
+// given as parallel arrays; -1 if the writer throws.
+int pfr_write_render_manifest(const char* path, const char* sim_kind, int nx, int ny, int nz, double dx, int n,
+                              const int* frame, const int* step, const double* time, const char* const* paths,
+                              const long long* bytes) {
+  std::vector<RenderCacheManifestFrame3D> frames;
+  for (int i = 0; i < n; ++i) frames.push_back(RenderCacheManifestFrame3D{frame[i], step[i], time[i], paths[i], bytes[i]});
+  try {
+    writeRenderCacheManifest3D(path, sim_kind, nx, ny, nz, dx, frames);
+  } catch (...) {
+    return -1;
+  }
+  return 0;
+}
 
 // ---- multires (MRSim3DTP) -------------------------------------------------
 
