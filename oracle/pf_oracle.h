@@ -162,6 +162,57 @@ typedef struct {
   pfo_mr_solve_cfg solve;
 } pfo_mr_step_cfg;
 
+/* ---- secondary particles (pf_oracle_sec.c) --------------------------------
+ * src/driver/secondary_particles3d.h:9-467.  A set is caller storage:
+ * positions and velocities (3 doubles each), volumes and ages, n of cap. */
+typedef struct {
+  size_t n, cap;
+  double *pos, *vel, *vol;
+  int* age;
+} pfo_sec_set;
+typedef struct {
+  int nx, ny, nz;
+  double dx, ox, oy, oz;
+} pfo_sec_domain;
+typedef struct { /* SecondaryParticleLifecycleConfig3D */
+  int enabled, droplet_lifetime_steps, bubble_lifetime_steps;
+  double velocity_damping, reabsorb_margin_cells, gravity, droplet_gravity_scale, bubble_buoyancy_scale,
+      droplet_drag, bubble_drag, particle_volume_scale;
+} pfo_sec_cfg;
+typedef struct { /* SecondaryParticleLifecycleStats3D */
+  int enabled, finite, advected_droplets, advected_bubbles, reabsorbed_droplets, reabsorbed_bubbles,
+      expired_droplets, expired_bubbles, dragged_droplets, dragged_bubbles, reabsorbed_droplets_to_primary,
+      reabsorbed_bubbles_to_primary;
+  double current_droplet_volume, current_bubble_volume, reabsorbed_droplet_volume, reabsorbed_bubble_volume,
+      expired_droplet_volume, expired_bubble_volume, reabsorbed_droplet_volume_to_primary,
+      reabsorbed_bubble_volume_to_primary;
+} pfo_sec_stats;
+typedef struct { /* SecondarySprayEmissionConfig3D */
+  int enabled, requested_particles;
+  double droplet_fraction, droplet_volume, bubble_volume, particle_volume_scale;
+  int interface_gate, interface_cells;
+  double interface_grad_max, interface_curvature_abs_max;
+  int min_interface_cells;
+  double min_interface_grad_max, min_interface_curvature_abs_max;
+  int impact_splash_candidates;
+  double impact_region_fraction, impact_downward_speed_min, impact_foam_fraction;
+} pfo_spray_cfg;
+typedef struct { /* SecondarySprayEmissionStats3D */
+  int enabled, finite, requested_particles, effective_requested_particles, interface_gate_enabled,
+      interface_gate_passed, interface_cells, candidate_liquid_particles, impact_candidate_liquid_particles,
+      foam_ready_droplets, emitted_droplets, emitted_bubbles;
+  double interface_grad_max, interface_curvature_abs_max, emitted_droplet_volume, emitted_bubble_volume;
+} pfo_spray_stats;
+double pfo_sec_volume_sum(const pfo_sec_set* s, double scale);
+/* advanceSecondaryParticles3D; reab_* NULL unless reabsorbed particles go back
+ * to the primary set.  -1 when a set's capacity is exceeded. */
+int pfo_sec_advance(const pfo_sec_domain* d, const pfo_sec_cfg* c, double dt, pfo_sec_set* droplets,
+                    pfo_sec_set* bubbles, pfo_sec_set* reab_droplets, pfo_sec_set* reab_bubbles, pfo_sec_stats* st);
+/* emitSecondarySpraySeeds3D on a primary particle set */
+int pfo_spray_emit(size_t n, const double* pos, const double* vel, const unsigned char* type, const double* vol,
+                   const pfo_spray_cfg* c, int frame_index, pfo_sec_set* droplets, pfo_sec_set* bubbles,
+                   pfo_spray_stats* st);
+
 pfo_mr* pfo_mr_create(int nx, int ny, int nz, double dx);
 void pfo_mr_destroy(pfo_mr* m);
 void pfo_mr_dims(const pfo_mr* m, int* blocks3);

@@ -332,6 +332,118 @@ int pfr_surface_tension(void* hp, const double* phase, double dt, double strengt
 }
 
 
+// ---- secondary particles (src/driver/secondary_particles3d.h, the escape
+// branching, lifecycle and spray emission of SparseSim3DTP::step,
+// src/driver/sparse_sim3d_tp.cpp:192-337) ------------------------------------
+
+// iv: escaped_particle_branching, secondary_particle_lifecycle,
+//     secondary_droplet_lifetime_steps, secondary_bubble_lifetime_steps,
+//     secondary_reabsorb_to_primary, secondary_spray_emission,
+//     secondary_spray_particles_per_step, secondary_spray_interface_gate,
+//     secondary_spray_min_interface_cells, secondary_spray_impact_candidates
+// dv: secondary_velocity_damping, secondary_reabsorb_margin_cells,
+//     secondary_droplet_gravity_scale, secondary_bubble_buoyancy_scale,
+//     secondary_droplet_drag, secondary_bubble_drag,
+//     secondary_spray_droplet_fraction, secondary_spray_droplet_volume,
+//     secondary_spray_bubble_volume, secondary_spray_min_interface_grad_max,
+//     secondary_spray_min_interface_curvature_abs_max,
+//     secondary_spray_impact_region_fraction,
+//     secondary_spray_impact_downward_speed_min, secondary_spray_impact_foam_fraction
+int pfr_set_secondary(void* hp, const int* iv, const double* dv) {
+  SparseSim3DTP& s = static_cast<Handle*>(hp)->sim;
+  s.escaped_particle_branching = iv[0] != 0;
+  s.secondary_particle_lifecycle = iv[1] != 0;
+  s.secondary_droplet_lifetime_steps = iv[2];
+  s.secondary_bubble_lifetime_steps = iv[3];
+  s.secondary_reabsorb_to_primary = iv[4] != 0;
+  s.secondary_spray_emission = iv[5] != 0;
+  s.secondary_spray_particles_per_step = iv[6];
+  s.secondary_spray_interface_gate = iv[7] != 0;
+  s.secondary_spray_min_interface_cells = iv[8];
+  s.secondary_spray_impact_candidates = iv[9] != 0;
+  s.secondary_velocity_damping = dv[0];
+  s.secondary_reabsorb_margin_cells = dv[1];
+  s.secondary_droplet_gravity_scale = dv[2];
+  s.secondary_bubble_buoyancy_scale = dv[3];
+  s.secondary_droplet_drag = dv[4];
+  s.secondary_bubble_drag = dv[5];
+  s.secondary_spray_droplet_fraction = dv[6];
+  s.secondary_spray_droplet_volume = dv[7];
+  s.secondary_spray_bubble_volume = dv[8];
+  s.secondary_spray_min_interface_grad_max = dv[9];
+  s.secondary_spray_min_interface_curvature_abs_max = dv[10];
+  s.secondary_spray_impact_region_fraction = dv[11];
+  s.secondary_spray_impact_downward_speed_min = dv[12];
+  s.secondary_spray_impact_foam_fraction = dv[13];
+  return 0;
+}
+
+static Particles3DTP& secondarySet(SparseSim3DTP& s, int which) {
+  return which == 0 ? s.escaped_droplets : s.escaped_bubbles;
+}
+static std::vector<int>& secondaryAges(SparseSim3DTP& s, int which) {
+  return which == 0 ? s.escaped_droplet_ages : s.escaped_bubble_ages;
+}
+
+size_t pfr_secondary_count(void* hp, int which) {
+  return secondarySet(static_cast<Handle*>(hp)->sim, which).size();
+}
+
+int pfr_get_secondary(void* hp, int which, double* pos, double* vel, double* vol, int* ages) {
+  SparseSim3DTP& s = static_cast<Handle*>(hp)->sim;
+  const Particles3DTP& ps = secondarySet(s, which);
+  const std::vector<int>& ag = secondaryAges(s, which);
+  for (size_t p = 0; p < ps.size(); ++p) {
+    pos[3 * p] = ps.pos[p].x; pos[3 * p + 1] = ps.pos[p].y; pos[3 * p + 2] = ps.pos[p].z;
+    vel[3 * p] = ps.vel[p].x; vel[3 * p + 1] = ps.vel[p].y; vel[3 * p + 2] = ps.vel[p].z;
+    vol[p] = ps.volume[p];
+    ages[p] = p < ag.size() ? ag[p] : 0;
+  }
+  return 0;
+}
+
+int pfr_set_secondary_set(void* hp, int which, size_t n, const double* pos, const double* vel, const double* vol,
+                          const int* ages) {
+  SparseSim3DTP& s = static_cast<Handle*>(hp)->sim;
+  Particles3DTP& ps = secondarySet(s, which);
+  std::vector<int>& ag = secondaryAges(s, which);
+  ps = Particles3DTP();
+  ag.clear();
+  for (size_t p = 0; p < n; ++p) {
+    ps.add({pos[3 * p], pos[3 * p + 1], pos[3 * p + 2]}, {vel[3 * p], vel[3 * p + 1], vel[3 * p + 2]},
+           (unsigned char)which, vol[p]);
+    ag.push_back(ages[p]);
+  }
+  return 0;
+}
+
+// the last step's statistics: iv (30 ints) and dv (20 doubles), in the
+// field order of SecondaryParticleLifecycleStats3D,
+// SecondarySprayEmissionStats3D and the added counts
+int pfr_secondary_stats(void* hp, int* iv, double* dv) {
+  SparseSim3DTP& s = static_cast<Handle*>(hp)->sim;
+  const SecondaryParticleLifecycleStats3D& l = s.secondary_lifecycle_stats_last;
+  const SecondarySprayEmissionStats3D& e = s.secondary_spray_emission_stats_last;
+  const int I[30] = {l.enabled, l.finite, l.advected_droplets, l.advected_bubbles, l.reabsorbed_droplets,
+                     l.reabsorbed_bubbles, l.expired_droplets, l.expired_bubbles, l.dragged_droplets,
+                     l.dragged_bubbles, l.reabsorbed_droplets_to_primary, l.reabsorbed_bubbles_to_primary,
+                     e.enabled, e.finite, e.requested_particles, e.effective_requested_particles,
+                     e.interface_gate_enabled, e.interface_gate_passed, e.interface_cells,
+                     e.candidate_liquid_particles, e.impact_candidate_liquid_particles, e.foam_ready_droplets,
+                     e.emitted_droplets, e.emitted_bubbles, s.escaped_droplets_added_last,
+                     s.escaped_bubbles_added_last, s.secondary_spray_emission_step_index, 0, 0, 0};
+  const double D[20] = {l.current_droplet_volume, l.current_bubble_volume, l.reabsorbed_droplet_volume,
+                        l.reabsorbed_bubble_volume, l.expired_droplet_volume, l.expired_bubble_volume,
+                        l.reabsorbed_droplet_volume_to_primary, l.reabsorbed_bubble_volume_to_primary,
+                        e.interface_grad_max, e.interface_curvature_abs_max, e.emitted_droplet_volume,
+                        e.emitted_bubble_volume, s.escaped_droplet_volume_added_last,
+                        s.escaped_bubble_volume_added_last, s.secondary_droplet_volume_current_last,
+                        s.secondary_bubble_volume_current_last, 0, 0, 0, 0};
+  std::memcpy(iv, I, sizeof(I));
+  std::memcpy(dv, D, sizeof(D));
+  return 0;
+}
+
 // writeRenderCacheManifest3D (src/driver/render_cache3d.h:711-755) for frames
 // given as parallel arrays; -1 if the writer throws.
 int pfr_write_render_manifest(const char* path, const char* sim_kind, int nx, int ny, int nz, double dx, int n,
