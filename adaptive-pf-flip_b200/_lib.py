@@ -45,6 +45,8 @@ EXPORTS = (
     "pf_mr_set_layout", "pf_mr_set_levels", "pf_mr_get_levels", "pf_mr_set_dynamic", "pf_mr_reset_refinement",
     "pf_mr_update_refinement", "pf_mr_step", "pf_mr_p2g", "pf_mr_get_face", "pf_mr_get_cells",
     "pf_write_render_manifest",
+    "pf_secondary_default_cfg", "pf_set_secondary", "pf_get_secondary_stats", "pf_secondary_count",
+    "pf_get_secondary", "pf_set_secondary_particles", "pf_secondary_advance", "pf_secondary_spray",
 )
 
 STAGES = ("bin", "sort", "splat", "normalize", "mark", "boundary", "project", "pcg", "g2p", "precond_setup",
@@ -202,6 +204,48 @@ class StepControlStats(_Stats):
                 ("liquid_volume_error", C.c_double), ("c_div", C.c_double)]
 
 
+class SecondaryCfg(C.Structure):
+    """pf_secondary_cfg: SparseSim3DTP's secondary-particle settings (src/driver/sparse_sim3d_tp.h:82-137)."""
+    _fields_ = [("escaped_particle_branching", C.c_int), ("lifecycle", C.c_int),
+                ("droplet_lifetime_steps", C.c_int), ("bubble_lifetime_steps", C.c_int),
+                ("velocity_damping", C.c_double), ("reabsorb_margin_cells", C.c_double),
+                ("droplet_gravity_scale", C.c_double), ("bubble_buoyancy_scale", C.c_double),
+                ("droplet_drag", C.c_double), ("bubble_drag", C.c_double), ("reabsorb_to_primary", C.c_int),
+                ("spray_emission", C.c_int), ("spray_particles_per_step", C.c_int),
+                ("spray_droplet_fraction", C.c_double), ("spray_droplet_volume", C.c_double),
+                ("spray_bubble_volume", C.c_double), ("spray_interface_gate", C.c_int),
+                ("spray_min_interface_cells", C.c_int), ("spray_min_interface_grad_max", C.c_double),
+                ("spray_min_interface_curvature_abs_max", C.c_double), ("spray_impact_candidates", C.c_int),
+                ("spray_impact_region_fraction", C.c_double), ("spray_impact_downward_speed_min", C.c_double),
+                ("spray_impact_foam_fraction", C.c_double)]
+
+
+class SecondaryStats(_Stats):
+    """pf_secondary_stats: SecondaryParticleLifecycleStats3D and SecondarySprayEmissionStats3D
+    (src/driver/secondary_particles3d.h:33-54, 76-93), the step's additions and the sets' volumes."""
+    _fields_ = [(n, C.c_int) for n in (
+        "lifecycle_enabled", "lifecycle_finite", "advected_droplets", "advected_bubbles", "reabsorbed_droplets",
+        "reabsorbed_bubbles", "expired_droplets", "expired_bubbles", "dragged_droplets", "dragged_bubbles",
+        "reabsorbed_droplets_to_primary", "reabsorbed_bubbles_to_primary")] + \
+        [(n, C.c_double) for n in (
+            "lifecycle_droplet_volume", "lifecycle_bubble_volume", "reabsorbed_droplet_volume",
+            "reabsorbed_bubble_volume", "expired_droplet_volume", "expired_bubble_volume",
+            "reabsorbed_droplet_volume_to_primary", "reabsorbed_bubble_volume_to_primary")] + \
+        [(n, C.c_int) for n in (
+            "spray_enabled", "spray_finite", "spray_requested_particles", "spray_effective_requested_particles",
+            "spray_interface_gate_enabled", "spray_interface_gate_passed", "spray_interface_cells",
+            "spray_candidate_liquid_particles", "spray_impact_candidate_liquid_particles",
+            "spray_foam_ready_droplets", "spray_emitted_droplets", "spray_emitted_bubbles")] + \
+        [(n, C.c_double) for n in (
+            "spray_interface_grad_max", "spray_interface_curvature_abs_max", "spray_emitted_droplet_volume",
+            "spray_emitted_bubble_volume")] + \
+        [("escaped_droplets_added", C.c_int), ("escaped_bubbles_added", C.c_int),
+         ("escaped_droplet_volume_added", C.c_double), ("escaped_bubble_volume_added", C.c_double),
+         ("escape_droplet_volume", C.c_double), ("escape_bubble_volume", C.c_double),
+         ("spray_step_index", C.c_int), ("droplet_volume_current", C.c_double),
+         ("bubble_volume_current", C.c_double)]
+
+
 class AdaptStats(C.Structure):
     _fields_ = [("band", BandStats), ("gas", CoarsenStats), ("liquid", CoarsenStats), ("refill", RefillStats)]
 
@@ -308,6 +352,14 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "pf_get_step_control_stats": (i, [vp, P(StepControlStats)]),
         "pf_default_render_camera": (i, [i, i, i, d, P(RenderCamera)]),
         "pf_write_render_cache": (i, [vp, C.c_char_p, i, d, d, P(Phase), d, P(RenderCamera), P(C.c_longlong)]),
+        "pf_secondary_default_cfg": (i, [P(SecondaryCfg)]),
+        "pf_set_secondary": (i, [vp, P(SecondaryCfg)]),
+        "pf_get_secondary_stats": (i, [vp, P(SecondaryStats)]),
+        "pf_secondary_count": (i, [vp, i, P(sz)]),
+        "pf_get_secondary": (i, [vp, i, vp, vp, vp, vp]),
+        "pf_set_secondary_particles": (i, [vp, i, sz, vp, vp, vp, vp]),
+        "pf_secondary_advance": (i, [vp, d, d, d]),
+        "pf_secondary_spray": (i, [vp, d, P(InterfaceStats)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

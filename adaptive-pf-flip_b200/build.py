@@ -24,10 +24,12 @@ INCLUDE = os.path.join(ROOT, "include")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
+                "-Xcompiler", "-ffp-contract=off",
                 "--expt-relaxed-constexpr", "-I", INCLUDE, "-I", CSRC]
 
 SOURCES = ["pf_pool.cu", "pf_transfer.cu", "pf_project.cu", "pf_pcg.cu", "pf_timing.cu", "pf_noalloc.cu",
-           "pf_coarse.cu", "pf_flex.cu", "pf_outer.cu", "pf_learned.cu", "pf_adapt.cu", "pf_diag.cu", "pf_render.cu", "pf_scene.cu", "pf_mr.cu", "pf_capi.cu"]
+           "pf_coarse.cu", "pf_flex.cu", "pf_outer.cu", "pf_learned.cu", "pf_adapt.cu", "pf_diag.cu", "pf_render.cu", "pf_scene.cu", "pf_mr.cu", "pf_secondary.cu",
+           "pf_capi.cu"]
 
 
 def _deps():

@@ -50,6 +50,7 @@ void free_all(pf_ctx* c) {
   pf::adapt_free(c);
   pf::diag_free(c);
   pf::mr_free(c);
+  pf::secondary_free(c);
   F(c->tile_slot); F(c->slot_tile); F(c->d_nslots); F(c->tile_need); F(c->tile_new); F(c->tile_rank);
   for (int f = 0; f < PF_NFIELDS; ++f) { F(c->fld[f]); F(c->act4[f]); }
   for (int a = 0; a < PF_NSAVED; ++a) F(c->saved[a]);
@@ -661,6 +662,26 @@ static int step_impl(pf_ctx* ctx, const pf_step_cfg* cfg, pf_step_stats* stats) 
   rc = pf::step_controls(ctx, cfg->dt, cfg->Vp, ctx->controls, &ctx->controls_last, controls_now);
   if (rc) return rc;
   const double dt = ctx->controls_last.effective_dt;
+  // advanceSecondaryLifecycle, before updateVolumeCorrectionStats: when it
+  // may move particles into the primary set the liquid volume is taken again
+  const bool secondary = pf::secondary_active(ctx);
+  if (secondary) {
+    const bool reabsorbs = pf::secondary_reabsorbs(ctx);
+    rc = pf::secondary_lifecycle(ctx, dt, cfg->gravity, cfg->Vp);
+    if (rc) return rc;
+    if (reabsorbs) {
+      rc = pf::step_controls_finish(ctx, &ctx->controls_last);  // the timestep, from before the lifecycle
+      if (rc) return rc;
+      pf_step_controls vc = ctx->controls;
+      vc.adaptive_timestep = 0;
+      pf_step_control_stats vs{};
+      rc = pf::step_controls(ctx, dt, cfg->Vp, vc, &vs, true);
+      if (rc) return rc;
+      ctx->controls_last.liquid_volume_current = vs.liquid_volume_current;
+      ctx->controls_last.liquid_volume_error = vs.liquid_volume_error;
+      ctx->controls_last.c_div = vs.c_div;
+    }
+  }
   pf_solve_cfg solve = cfg->solve;
   if (ctx->controls.c_div_volume_correction) solve.c_div = ctx->controls_last.c_div;
   rc = pool_reset(ctx);
@@ -687,8 +708,15 @@ static int step_impl(pf_ctx* ctx, const pf_step_cfg* cfg, pf_step_stats* stats) 
   rc = pf::project(ctx, &cfg->phase, dt, &solve, &sst);
   if (rc) return rc;
   pf_clamp_stats cst{};
-  rc = pf::g2p_advect(ctx, cfg->alpha_l, cfg->alpha_g, dt, cfg->advect_order, &cst);
+  int* esc = secondary ? pf::secondary_escape_flags(ctx) : nullptr;
+  rc = pf::g2p_advect(ctx, cfg->alpha_l, cfg->alpha_g, dt, cfg->advect_order, &cst, esc);
   if (rc) return rc;
+  if (secondary) {  // storeEscapedParticles and emitSecondarySpray
+    rc = pf::interface_diagnostics_finish(ctx);
+    if (rc) return rc;
+    rc = pf::secondary_after_advect(ctx, esc, cfg->Vp, ctx->diag_last);
+    if (rc) return rc;
+  }
   rc = pool_sync(ctx);
   if (rc) return rc;
   if (stats) {

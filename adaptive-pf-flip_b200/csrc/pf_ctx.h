@@ -104,6 +104,8 @@ struct pf_ctx {
   void* learned = nullptr;
   // the 2-level multires grid (pf_mr.cu), made on first use
   void* mr = nullptr;
+  // the secondary droplet and bubble sets (pf_secondary.cu), made on first use
+  void* secondary = nullptr;
   // particle adaptivity: scratch (its own module) and the step's settings
   void* adapt = nullptr;
   bool adapt_on = false;
@@ -175,7 +177,8 @@ int apply_walls(pf_ctx* ctx);
 int normalize_save_gravity(pf_ctx* ctx, bool save, bool gravity, double dt, double gval);
 int g2p(pf_ctx* ctx, const pf_ctx* saved, double aL, double aG);
 int advect(pf_ctx* ctx, double dt, int order, pf_clamp_stats* st, double* esc, size_t* nesc);
-int g2p_advect(pf_ctx* ctx, double aL, double aG, double dt, int order, pf_clamp_stats* st);
+int g2p_advect(pf_ctx* ctx, double aL, double aG, double dt, int order, pf_clamp_stats* st,
+               int* esc_flags = nullptr);
 int calibrate(pf_ctx* ctx, const pf_phase* ph, double Vp, double* out);
 
 // project.cu
@@ -202,6 +205,14 @@ void diag_free(pf_ctx* ctx);
 
 // mr.cu
 void mr_free(pf_ctx* ctx);
+
+// secondary.cu
+bool secondary_active(const pf_ctx* ctx);
+bool secondary_reabsorbs(const pf_ctx* ctx);
+int* secondary_escape_flags(pf_ctx* ctx);
+int secondary_lifecycle(pf_ctx* ctx, double dt, double gravity, double Vp);
+int secondary_after_advect(pf_ctx* ctx, const int* esc_flags, double Vp, const pf_interface_stats& iface);
+void secondary_free(pf_ctx* ctx);
 
 // capi.cu: the second particle set (asynchronous uploads, compaction target)
 int ensure_back_set(pf_ctx* ctx);

@@ -1747,17 +1747,19 @@ int advect(pf_ctx* ctx, double dt, int order, pf_clamp_stats* st, double* esc, s
   return read_clamp(ctx, st);
 }
 
-int g2p_advect(pf_ctx* ctx, double aL, double aG, double dt, int order, pf_clamp_stats* st) {
+// With esc_flags the per-particle kernel also flags the clamped particles
+// (the escape records' source); the tile kernel has no flags.
+int g2p_advect(pf_ctx* ctx, double aL, double aG, double dt, int order, pf_clamp_stats* st, int* esc_flags) {
   StageScope stage(ctx, PF_STAGE_G2P);
   const int n = (int)ctx->np;
   PF_CUDA_TRY(cudaMemsetAsync(ctx->d_clamp, 0, 8 * sizeof(int), ctx->stream));
   if (n > 0) {
-    if (ctx->bins_valid)
+    if (ctx->bins_valid && !esc_flags)
       (++ctx->launches), k_g2p_advect_tiles<<<ctx->g.ntiles, 256, 0, ctx->stream>>>(
           dev_grid(ctx), ctx->tile_start, ctx->perm, particle_ptrs(ctx), dt, order, aL, aG, ctx->d_clamp);
     else
       (++ctx->launches), k_advect<<<nblocks(n, 256), 256, 0, ctx->stream>>>(dev_grid(ctx), particle_ptrs(ctx), n, dt,
-                                                                             order, ctx->d_clamp, nullptr, 1, aL, aG);
+                                                                             order, ctx->d_clamp, esc_flags, 1, aL, aG);
     PF_CUDA_TRY(cudaGetLastError());
   }
   ctx->bins_valid = false;  // particles moved

@@ -491,6 +491,29 @@ def applyLiquidParticleRefill(particles, grid: SparseMacGrid3D, enabled=True, pa
     return st
 
 
+# SparseSim3DTP's secondary-particle totals and the per-step statistic each accumulates
+_SECONDARY_TOTALS = {
+    "secondary_droplets_advected": "advected_droplets", "secondary_bubbles_advected": "advected_bubbles",
+    "secondary_droplets_reabsorbed": "reabsorbed_droplets", "secondary_bubbles_reabsorbed": "reabsorbed_bubbles",
+    "secondary_droplets_expired": "expired_droplets", "secondary_bubbles_expired": "expired_bubbles",
+    "secondary_droplets_dragged": "dragged_droplets", "secondary_bubbles_dragged": "dragged_bubbles",
+    "secondary_droplets_reabsorbed_to_primary": "reabsorbed_droplets_to_primary",
+    "secondary_bubbles_reabsorbed_to_primary": "reabsorbed_bubbles_to_primary",
+    "secondary_droplet_volume_reabsorbed": "reabsorbed_droplet_volume",
+    "secondary_bubble_volume_reabsorbed": "reabsorbed_bubble_volume",
+    "secondary_droplet_volume_expired": "expired_droplet_volume",
+    "secondary_bubble_volume_expired": "expired_bubble_volume",
+    "secondary_droplet_volume_reabsorbed_to_primary": "reabsorbed_droplet_volume_to_primary",
+    "secondary_bubble_volume_reabsorbed_to_primary": "reabsorbed_bubble_volume_to_primary",
+    "secondary_spray_emitted_droplets": "spray_emitted_droplets",
+    "secondary_spray_emitted_bubbles": "spray_emitted_bubbles",
+    "secondary_spray_emitted_droplet_volume": "spray_emitted_droplet_volume",
+    "secondary_spray_emitted_bubble_volume": "spray_emitted_bubble_volume",
+    "escaped_droplets_added": None, "escaped_bubbles_added": None,
+    "escaped_droplet_volume_added": None, "escaped_bubble_volume_added": None,
+}
+
+
 class SparseSim3DTP:
     """SparseSim3DTP with particles resident on the GPU; step() runs
     markCells, P2G, saved copy, gravity, walls, projection, G2P and
@@ -531,6 +554,28 @@ class SparseSim3DTP:
         self.effective_dt_last, self.max_particle_speed_last, self.cfl_limit_dt_last = self.dt, 0.0, self.dt
         self.adaptive_timestep_limited_last = 0
         self.liquid_volume_current_last = self.liquid_volume_error_last = 0.0
+        # secondary particles (src/driver/sparse_sim3d_tp.h:82-137), off by default
+        self.escaped_particle_branching = False
+        self.secondary_particle_lifecycle = False
+        self.secondary_droplet_lifetime_steps = self.secondary_bubble_lifetime_steps = 48
+        self.secondary_velocity_damping, self.secondary_reabsorb_margin_cells = 0.98, 1.0
+        self.secondary_droplet_gravity_scale, self.secondary_bubble_buoyancy_scale = 1.0, 0.25
+        self.secondary_droplet_drag = self.secondary_bubble_drag = 0.0
+        self.secondary_reabsorb_to_primary = False
+        self.secondary_spray_emission, self.secondary_spray_particles_per_step = False, 0
+        self.secondary_spray_droplet_fraction = 0.9
+        self.secondary_spray_droplet_volume, self.secondary_spray_bubble_volume = 0.55, 0.45
+        self.secondary_spray_interface_gate, self.secondary_spray_min_interface_cells = False, 1
+        self.secondary_spray_min_interface_grad_max = 1e-5
+        self.secondary_spray_min_interface_curvature_abs_max = 0.0
+        self.secondary_spray_impact_candidates = False
+        self.secondary_spray_impact_region_fraction = 0.55
+        self.secondary_spray_impact_downward_speed_min = 1.0
+        self.secondary_spray_impact_foam_fraction = 0.3
+        self.secondary_stats_last = L.SecondaryStats()
+        self.secondary_spray_emission_step_index = 0
+        self.secondary_totals = {k: 0 for k in _SECONDARY_TOTALS}
+        self._secondary_configured = False
 
     def set_particles(self, pos, vel, type, volume):
         """Upload FP32 (n,3) pos/vel, uint8 type, FP32 volume (host or device pointers via numpy)."""
@@ -559,7 +604,7 @@ class SparseSim3DTP:
         return self.n
 
     def get_particles(self):
-        n = self.n
+        n = self.n = int(self.grid.lib.pf_num_particles(self.grid.ctx))
         pos = np.empty((n, 3), np.float32)
         vel = np.empty((n, 3), np.float32)
         typ = np.empty(n, np.uint8)
@@ -610,6 +655,82 @@ class SparseSim3DTP:
         self.n = int(lib.pf_num_particles(ctx))
         return out
 
+    def secondary_cfg(self) -> L.SecondaryCfg:
+        return L.SecondaryCfg(
+            int(self.escaped_particle_branching), int(self.secondary_particle_lifecycle),
+            int(self.secondary_droplet_lifetime_steps), int(self.secondary_bubble_lifetime_steps),
+            float(self.secondary_velocity_damping), float(self.secondary_reabsorb_margin_cells),
+            float(self.secondary_droplet_gravity_scale), float(self.secondary_bubble_buoyancy_scale),
+            float(self.secondary_droplet_drag), float(self.secondary_bubble_drag),
+            int(self.secondary_reabsorb_to_primary), int(self.secondary_spray_emission),
+            int(self.secondary_spray_particles_per_step), float(self.secondary_spray_droplet_fraction),
+            float(self.secondary_spray_droplet_volume), float(self.secondary_spray_bubble_volume),
+            int(self.secondary_spray_interface_gate), int(self.secondary_spray_min_interface_cells),
+            float(self.secondary_spray_min_interface_grad_max),
+            float(self.secondary_spray_min_interface_curvature_abs_max),
+            int(self.secondary_spray_impact_candidates), float(self.secondary_spray_impact_region_fraction),
+            float(self.secondary_spray_impact_downward_speed_min), float(self.secondary_spray_impact_foam_fraction))
+
+    def _secondary_on(self):
+        return self.escaped_particle_branching or self.secondary_particle_lifecycle or self.secondary_spray_emission
+
+    def secondary_set(self, which):
+        """The droplet (0) or bubble (1) set: FP64 positions and velocities (n, 3),
+        volumes and ages (escaped_droplets / escaped_droplet_ages of the reference)."""
+        ctx, lib = self.grid.ctx, self.grid.lib
+        n = C.c_size_t()
+        L.check(lib.pf_secondary_count(ctx, int(which), C.byref(n)), ctx, "pf_secondary_count")
+        n = int(n.value)
+        pos, vel = np.zeros((n, 3)), np.zeros((n, 3))
+        vol, age = np.zeros(n), np.zeros(n, np.int32)
+        if n:
+            L.check(lib.pf_get_secondary(ctx, int(which), pos.ctypes.data, vel.ctypes.data, vol.ctypes.data,
+                                         age.ctypes.data), ctx, "pf_get_secondary")
+        return pos, vel, vol, age
+
+    def set_secondary_set(self, which, pos, vel, vol, age):
+        ctx, lib = self.grid.ctx, self.grid.lib
+        pos = np.ascontiguousarray(pos, np.float64).reshape(-1, 3)
+        vel = np.ascontiguousarray(vel, np.float64).reshape(-1, 3)
+        vol = np.ascontiguousarray(vol, np.float64).reshape(-1)
+        age = np.ascontiguousarray(age, np.int32).reshape(-1)
+        if not (len(pos) == len(vel) == len(vol) == len(age)):
+            raise ValueError("secondary set arrays differ in length")
+        L.check(lib.pf_set_secondary_particles(ctx, int(which), len(pos), pos.ctypes.data, vel.ctypes.data,
+                                               vol.ctypes.data, age.ctypes.data), ctx, "pf_set_secondary_particles")
+
+    @property
+    def escaped_droplets(self):
+        return self.secondary_set(0)
+
+    @property
+    def escaped_bubbles(self):
+        return self.secondary_set(1)
+
+    def _secondary_after_step(self):
+        """The reference's *_last and *_total bookkeeping of the secondary
+        particles (src/driver/sparse_sim3d_tp.cpp:192-337), from the step's statistics."""
+        ctx, lib = self.grid.ctx, self.grid.lib
+        st = L.SecondaryStats()
+        L.check(lib.pf_get_secondary_stats(ctx, C.byref(st)), ctx, "pf_get_secondary_stats")
+        self.secondary_stats_last = st
+        self.secondary_spray_emission_step_index = st.spray_step_index
+        t = self.secondary_totals
+        for key, field in _SECONDARY_TOTALS.items():
+            if key.startswith("escaped_"):
+                continue
+            t[key] += getattr(st, field)
+        # storeEscapedParticles adds the escaped particles, emitSecondarySpray the seeds
+        t["escaped_droplets_added"] += st.escaped_droplets_added - st.spray_emitted_droplets
+        t["escaped_bubbles_added"] += st.escaped_bubbles_added - st.spray_emitted_bubbles
+        if self.escaped_particle_branching:
+            t["escaped_droplet_volume_added"] += st.escape_droplet_volume
+            t["escaped_bubble_volume_added"] += st.escape_bubble_volume
+        t["escaped_droplets_added"] += st.spray_emitted_droplets
+        t["escaped_bubbles_added"] += st.spray_emitted_bubbles
+        t["escaped_droplet_volume_added"] += st.spray_emitted_droplet_volume
+        t["escaped_bubble_volume_added"] += st.spray_emitted_bubble_volume
+
     def step_cfg(self):
         solve = self.solver._c(self.cg_iters, self.cg_tol, self.c_div_last)
         return L.StepCfg(self.dt, self.gravity, self.Vp, self.alpha_liquid, self.alpha_gas, self.phase._c(), solve,
@@ -633,7 +754,15 @@ class SparseSim3DTP:
                                            float(self.surface_tension_max_delta_speed),
                                            int(self.surface_tension_curvature_smoothing_radius)), ctx,
                 "pf_set_surface_tension")
+        if self._secondary_on():
+            sc = self.secondary_cfg()
+            L.check(lib.pf_set_secondary(ctx, C.byref(sc)), ctx, "pf_set_secondary")
+            self._secondary_configured = True
+        elif self._secondary_configured:
+            L.check(lib.pf_set_secondary(ctx, None), ctx, "pf_set_secondary")
         L.check(lib.pf_step(ctx, C.byref(cfg), C.byref(st)), ctx, "pf_step")
+        if self._secondary_configured:
+            self._secondary_after_step()
         L.check(lib.pf_get_surface_stats(ctx, C.byref(self.surface_tension_stats_last)), ctx, "pf_get_surface_stats")
         cs = L.StepControlStats()
         L.check(lib.pf_get_step_control_stats(ctx, C.byref(cs)), ctx, "pf_get_step_control_stats")

@@ -31,6 +31,11 @@
  *   Particles3DTP storage (src/particles/particles3d_tp.h:4-35)
  *                                                       -> pf_upload_particles*,
  *        pf_download_particles*
+ *   advanceSecondaryParticles3D, emitSecondarySpraySeeds3D
+ *     (src/driver/secondary_particles3d.h:136-467) and the step's escape
+ *     branching (src/driver/sparse_sim3d_tp.cpp:185-337)
+ *                                                       -> pf_set_secondary,
+ *        pf_secondary_advance, pf_secondary_spray, pf_get_secondary
  */
 #ifndef PFGPU_H
 #define PFGPU_H
@@ -321,6 +326,77 @@ PFGPU_API int pf_refill_liquid(pf_ctx* ctx, int per_cell_target, unsigned seed, 
  * last step's adaptivity. */
 PFGPU_API int pf_set_adaptivity(pf_ctx* ctx, const pf_adapt_cfg* cfg);
 PFGPU_API int pf_get_adaptivity_stats(const pf_ctx* ctx, pf_adapt_stats* out);
+
+/* ---- secondary particles (src/driver/secondary_particles3d.h) -----------
+ * Two FP64 sets beside the primary particles: droplets (set 0) and bubbles
+ * (set 1), each particle with an age in steps.  pf_step runs, at the places
+ * SparseSim3DTP::step does (src/driver/sparse_sim3d_tp.cpp:854-884): the
+ * lifecycle after the step controls, the escape branching (every particle the
+ * advection clamps to the domain is copied into the set of its type, age 0)
+ * and the spray seeds after the advection.  Sets and statistics equal the
+ * reference's arithmetic on the same inputs; spray candidates with equal
+ * scores are ranked in particle order. */
+/* SparseSim3DTP's settings (src/driver/sparse_sim3d_tp.h:82-137);
+ * pf_secondary_default_cfg gives the reference's defaults (all switches off,
+ * lifetimes 48 steps, damping 0.98, margin 1 cell, gravity scale 1, buoyancy
+ * scale 0.25, spray droplet fraction 0.9, volumes 0.55 / 0.45, gate minima
+ * 1 cell and 1e-5, impact region 0.55, impact speed 1, foam fraction 0.3). */
+typedef struct {
+  int escaped_particle_branching;
+  int lifecycle;                                       /* secondary_particle_lifecycle */
+  int droplet_lifetime_steps, bubble_lifetime_steps;   /* < 0: no expiry */
+  double velocity_damping, reabsorb_margin_cells;
+  double droplet_gravity_scale, bubble_buoyancy_scale;
+  double droplet_drag, bubble_drag;                    /* per second; 0: none */
+  int reabsorb_to_primary;                             /* reabsorbed particles rejoin the primary set */
+  int spray_emission, spray_particles_per_step;
+  double spray_droplet_fraction, spray_droplet_volume, spray_bubble_volume;
+  int spray_interface_gate, spray_min_interface_cells;
+  double spray_min_interface_grad_max, spray_min_interface_curvature_abs_max;
+  int spray_impact_candidates;
+  double spray_impact_region_fraction, spray_impact_downward_speed_min, spray_impact_foam_fraction;
+} pf_secondary_cfg;
+/* The last step's SecondaryParticleLifecycleStats3D (:33-54; volumes scaled
+ * by Vp; lifecycle_*_volume are the sets' volumes after the lifecycle),
+ * SecondarySprayEmissionStats3D (:76-93), the particles and volume added to
+ * each set by the escapes and the spray together, the spray step index after
+ * the step, and the sets' volumes at the end of the step. */
+typedef struct {
+  int lifecycle_enabled, lifecycle_finite;
+  int advected_droplets, advected_bubbles, reabsorbed_droplets, reabsorbed_bubbles;
+  int expired_droplets, expired_bubbles, dragged_droplets, dragged_bubbles;
+  int reabsorbed_droplets_to_primary, reabsorbed_bubbles_to_primary;
+  double lifecycle_droplet_volume, lifecycle_bubble_volume;
+  double reabsorbed_droplet_volume, reabsorbed_bubble_volume, expired_droplet_volume, expired_bubble_volume;
+  double reabsorbed_droplet_volume_to_primary, reabsorbed_bubble_volume_to_primary;
+  int spray_enabled, spray_finite, spray_requested_particles, spray_effective_requested_particles;
+  int spray_interface_gate_enabled, spray_interface_gate_passed, spray_interface_cells;
+  int spray_candidate_liquid_particles, spray_impact_candidate_liquid_particles, spray_foam_ready_droplets;
+  int spray_emitted_droplets, spray_emitted_bubbles;
+  double spray_interface_grad_max, spray_interface_curvature_abs_max;
+  double spray_emitted_droplet_volume, spray_emitted_bubble_volume;
+  int escaped_droplets_added, escaped_bubbles_added;
+  double escaped_droplet_volume_added, escaped_bubble_volume_added;
+  double escape_droplet_volume, escape_bubble_volume; /* the escaped particles' share of the two above */
+  int spray_step_index;
+  double droplet_volume_current, bubble_volume_current;
+} pf_secondary_stats;
+PFGPU_API int pf_secondary_default_cfg(pf_secondary_cfg* out);
+/* Settings pf_step uses (NULL: all switches off; the sets are kept). */
+PFGPU_API int pf_set_secondary(pf_ctx* ctx, const pf_secondary_cfg* cfg);
+PFGPU_API int pf_get_secondary_stats(const pf_ctx* ctx, pf_secondary_stats* out);
+/* Set `which` (0 droplets, 1 bubbles): its size, and its particles as host
+ * arrays (pos/vel n x 3 interleaved; any pointer may be NULL). */
+PFGPU_API int pf_secondary_count(const pf_ctx* ctx, int which, size_t* n);
+PFGPU_API int pf_get_secondary(pf_ctx* ctx, int which, double* pos, double* vel, double* vol, int* age);
+PFGPU_API int pf_set_secondary_particles(pf_ctx* ctx, int which, size_t n, const double* pos, const double* vel,
+                                         const double* vol, const int* age);
+/* The step's pieces on their own: advanceSecondaryLifecycle (reabsorbed
+ * particles appended to the primary set when reabsorb_to_primary is on;
+ * PF_ERR_CAPACITY when they would not fit) and emitSecondarySpray on the
+ * current particles with the given interface statistics. */
+PFGPU_API int pf_secondary_advance(pf_ctx* ctx, double dt, double gravity, double Vp);
+PFGPU_API int pf_secondary_spray(pf_ctx* ctx, double Vp, const pf_interface_stats* iface);
 
 /* ---- per-stage device timing (CUDA events on the context stream) -------
  * Off by default.  When on, every solver-step entry point brackets its

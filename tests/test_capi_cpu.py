@@ -40,7 +40,10 @@ def test_struct_layouts_match_c(pf, tmp_path):
                "pf_coarsen_stats": L.CoarsenStats, "pf_refill_stats": L.RefillStats, "pf_adapt_cfg": L.AdaptCfg,
                "pf_adapt_stats": L.AdaptStats, "pf_interface_stats": L.InterfaceStats,
                "pf_step_controls": L.StepControls, "pf_step_control_stats": L.StepControlStats,
-               "pf_surface_stats": L.SurfaceStats}
+               "pf_surface_stats": L.SurfaceStats, "pf_render_camera": L.RenderCamera,
+               "pf_render_manifest_frame": L.RenderManifestFrame, "pf_mr_box": L.MRBox,
+               "pf_mr_dynamic": L.MRDynamic, "pf_mr_step_cfg": L.MRStepCfg, "pf_mr_step_stats": L.MRStepStats,
+               "pf_secondary_cfg": L.SecondaryCfg, "pf_secondary_stats": L.SecondaryStats}
     src = ['#include <stdio.h>', '#include <stddef.h>', '#include "pfgpu.h"', "int main(void){"]
     for cname, py in structs.items():
         src.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
