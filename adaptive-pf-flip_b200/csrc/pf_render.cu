@@ -271,10 +271,9 @@ int render_cells(pf_ctx* ctx, const pf_phase* ph, std::vector<RcCell>* cells) {
 
 extern "C" {
 
-// writeSparseRenderCache3D (src/driver/render_cache3d.h:551-600) with empty
-// secondary droplet and bubble sets: this framework keeps no secondary
-// particle containers, so their sections carry zero counts, as the reference
-// writes them for a simulation that emitted none.
+// writeSparseRenderCache3D (src/driver/render_cache3d.h:551-600): the
+// primary particles and the context's secondary droplet and bubble sets
+// (empty unless the step branches escaped particles or emits spray).
 int pf_write_render_cache(pf_ctx* ctx, const char* path, int frame, double time, double dt, const pf_phase* ph,
                           double Vp, const pf_render_camera* cam, long long* bytes_written) {
   if (!ctx || !path || !path[0] || !ph) return PF_ERR_INVALID;
@@ -338,7 +337,59 @@ int pf_write_render_cache(pf_ctx* ctx, const char* path, int frame, double time,
   domain.mx[0] = nx * dx;
   domain.mx[1] = ny * dx;
   domain.mx[2] = nz * dx;
-  pf::Bounds secondary{};  // no secondary particles
+  // the secondary sets (escaped_droplets, escaped_bubbles and their ages)
+  struct Set {
+    std::vector<double> pos, vel, vol;
+    std::vector<int> age;
+    size_t n = 0;
+  } sec[2];
+  for (int w = 0; w < 2; ++w) {
+    rc = pf_secondary_count(ctx, w, &sec[w].n);
+    if (rc) return rc;
+    Set& t = sec[w];
+    t.pos.resize(3 * t.n);
+    t.vel.resize(3 * t.n);
+    t.vol.resize(t.n);
+    t.age.resize(t.n);
+    if (t.n) {
+      rc = pf_get_secondary(ctx, w, t.pos.data(), t.vel.data(), t.vol.data(), t.age.data());
+      if (rc) return rc;
+    }
+  }
+  // secondaryVolume, secondaryAgeRange, secondaryBounds and the render
+  // channels of secondaryRenderChannelCounts (:190-300)
+  double sec_vol[2] = {0.0, 0.0};
+  int age_min[2] = {0, 0}, age_max[2] = {0, 0};
+  size_t ch_droplet = 0, ch_spray = 0, ch_foam = 0, ch_bubble = 0;
+  std::vector<const char*> channel[2];
+  pf::Bounds secondary{};
+  for (int w = 0; w < 2; ++w) {
+    const Set& t = sec[w];
+    int mn = std::numeric_limits<int>::max(), mx = 0;
+    channel[w].resize(t.n);
+    for (size_t p = 0; p < t.n; ++p) {
+      sec_vol[w] += t.vol[p] * Vp;
+      const int a = std::max(0, t.age[p]);
+      mn = std::min(mn, a);
+      mx = std::max(mx, a);
+      pf::include_point(secondary, &t.pos[3 * p]);
+      const char* ch = "bubble";
+      if (w == 0) {
+        const double* v = &t.vel[3 * p];
+        const double speed = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        ch = (a >= 4 && speed <= 0.5) ? "foam" : (a <= 1 || speed >= 1.0) ? "spray" : "droplet";
+      }
+      channel[w][p] = ch;
+      if (ch[0] == 'f') ++ch_foam;
+      else if (ch[0] == 's') ++ch_spray;
+      else if (ch[0] == 'd') ++ch_droplet;
+      else ++ch_bubble;
+    }
+    if (t.n) {
+      age_min[w] = mn == std::numeric_limits<int>::max() ? 0 : mn;
+      age_max[w] = mx;
+    }
+  }
   const double shutter_close = time + std::max(0.0, dt);
 
   std::ofstream out(path);
@@ -368,16 +419,20 @@ int pf_write_render_cache(pf_ctx* ctx, const char* path, int frame, double time,
   // writeWaterSummary (:429-458)
   out << "{\"section\":\"water_volume\""
       << ",\"primary_liquid_volume\":" << v_liq << ",\"primary_gas_volume\":" << v_gas
-      << ",\"secondary_droplet_volume\":" << 0.0 << ",\"secondary_bubble_volume\":" << 0.0
+      << ",\"secondary_droplet_volume\":" << sec_vol[0] << ",\"secondary_bubble_volume\":" << sec_vol[1]
       << ",\"phase_field_liquid_volume\":" << liquid << ",\"phase_field_cells\":" << cells.size()
       << ",\"primary_liquid_count\":" << n_liq << ",\"primary_gas_count\":" << n_gas
-      << ",\"secondary_droplet_count\":0,\"secondary_bubble_count\":0,\"secondary_particle_count\":0"
-      << ",\"secondary_droplet_age_min\":0,\"secondary_droplet_age_max\":0"
-      << ",\"secondary_bubble_age_min\":0,\"secondary_bubble_age_max\":0}\n";
+      << ",\"secondary_droplet_count\":" << sec[0].n << ",\"secondary_bubble_count\":" << sec[1].n
+      << ",\"secondary_particle_count\":" << sec[0].n + sec[1].n
+      << ",\"secondary_droplet_age_min\":" << age_min[0] << ",\"secondary_droplet_age_max\":" << age_max[0]
+      << ",\"secondary_bubble_age_min\":" << age_min[1] << ",\"secondary_bubble_age_max\":" << age_max[1]
+      << "}\n";
   // writeSecondaryChannels (:460-476)
   out << "{\"section\":\"secondary_channels\",\"encoding\":\"render_channel_counts\""
       << ",\"channel_names\":[\"droplet\",\"spray\",\"foam\",\"bubble\"]"
-      << ",\"droplet_count\":0,\"spray_count\":0,\"foam_count\":0,\"bubble_count\":0,\"total_count\":0}\n";
+      << ",\"droplet_count\":" << ch_droplet << ",\"spray_count\":" << ch_spray << ",\"foam_count\":" << ch_foam
+      << ",\"bubble_count\":" << ch_bubble << ",\"total_count\":" << ch_droplet + ch_spray + ch_foam + ch_bubble
+      << "}\n";
   // writeCinematicMetadata (:478-523)
   out << "{\"section\":\"cinematic_metadata\",\"cache_schema_version\":2,\"world_units\":\"cell\""
       << ",\"shutter_open\":" << time << ",\"shutter_close\":" << shutter_close << ",\"frame_time\":" << time
@@ -386,8 +441,8 @@ int pf_write_render_cache(pf_ctx* ctx, const char* path, int frame, double time,
       << ",\"secondary_bounds_valid\":" << (secondary.valid ? "true" : "false")
       << ",\"primary_particle_count\":" << n << ",\"primary_liquid_count\":" << n_liq
       << ",\"primary_gas_count\":" << n_gas
-      << ",\"secondary_droplet_count\":0,\"secondary_bubble_count\":0"
-      << ",\"secondary_spray_count\":0,\"secondary_foam_count\":0";
+      << ",\"secondary_droplet_count\":" << sec[0].n << ",\"secondary_bubble_count\":" << sec[1].n
+      << ",\"secondary_spray_count\":" << ch_spray << ",\"secondary_foam_count\":" << ch_foam;
   out << ",";
   pf::write_bounds(out, "frame_bounds_min", "frame_bounds_max", domain, domain);
   out << ",";
@@ -401,7 +456,7 @@ int pf_write_render_cache(pf_ctx* ctx, const char* path, int frame, double time,
     out << "{\"section\":\"phase_cell\",\"i\":" << x.i << ",\"j\":" << x.j << ",\"k\":" << x.k
         << ",\"level\":0,\"marker\":" << x.marker << ",\"phi\":" << x.phi
         << ",\"liquid_volume\":" << x.phi * cell_volume << "}\n";
-  // writeParticleSection (:541-560), primary then the two empty secondary sets
+  // writeParticleSection (:541-560), primary then the two secondary sets
   out << "{\"section\":\"particles\",\"kind\":\"primary\",\"count\":" << n << "}\n";
   for (size_t p = 0; p < n; ++p) {
     const bool liq = typ[p] == 0;
@@ -413,8 +468,20 @@ int pf_write_render_cache(pf_ctx* ctx, const char* path, int frame, double time,
         << "]"
         << ",\"volume\":" << (double)vol[p] * Vp << "}\n";
   }
-  out << "{\"section\":\"particles\",\"kind\":\"secondary_droplet\",\"count\":0}\n";
-  out << "{\"section\":\"particles\",\"kind\":\"secondary_bubble\",\"count\":0}\n";
+  for (int w = 0; w < 2; ++w) {
+    const Set& t = sec[w];
+    const char* kind = w == 0 ? "secondary_droplet" : "secondary_bubble";
+    out << "{\"section\":\"particles\",\"kind\":\"" << kind << "\",\"count\":" << t.n << "}\n";
+    for (size_t p = 0; p < t.n; ++p) {
+      const double* q = &t.pos[3 * p];
+      const double* v = &t.vel[3 * p];
+      out << "{\"section\":\"particle\",\"kind\":\"" << kind << "\",\"render_channel\":\"" << channel[w][p]
+          << "\",\"index\":" << p << ",\"phase\":\"" << (w == 0 ? "liquid" : "gas") << "\""
+          << ",\"position\":[" << q[0] << "," << q[1] << "," << q[2] << "]"
+          << ",\"velocity\":[" << v[0] << "," << v[1] << "," << v[2] << "]"
+          << ",\"volume\":" << t.vol[p] * Vp << ",\"age\":" << t.age[p] << "}\n";
+    }
+  }
   out.flush();
   if (!out) return PF_ERR_INVALID;
   if (bytes_written) *bytes_written = (long long)out.tellp();

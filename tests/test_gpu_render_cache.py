@@ -4,7 +4,9 @@
    compiled into oracle/_ref): the reference runs its own markCells on the
    same particles -- its marker blocks then sit in their first-touch order,
    the order it lists phase cells in -- and is given the GPU's face fields and
-   particles; both files must be identical, the liquid-volume sum included.
+   particles (and, in one case, the same secondary droplet and bubble sets,
+   with ages and speeds across every render channel); both files must be
+   identical, the liquid-volume sum included.
 2. Against a restatement of the writer's selection and number format
    (sparsePhaseCells, :497-526, and writeParticleSection, :541-560), on a grid
    imported from the oracle.
@@ -12,6 +14,7 @@
 """
 import ctypes as C
 import json
+import re
 
 import numpy as np
 import pytest
@@ -88,8 +91,21 @@ def _expected_particles(ps, Vp):
 
 
 @pytest.mark.skipif(not O.reference_available(), reason="compiled reference (oracle/_ref) not built")
-@pytest.mark.parametrize("scene,n,seed", [("rayleigh_taylor", 16, 3), ("bubble_tank", 20, 5)])
-def test_render_cache_equals_reference_writer(pf, tmp_path, scene, n, seed):
+def _secondary_sets(rng, n):
+    out = []
+    for m in (140, 60):
+        pos = rng.uniform(0.5 / n, 1.0 - 0.5 / n, (m, 3))
+        vel = rng.normal(0.0, 0.6, (m, 3))
+        vol = rng.uniform(0.3, 1.2, m)
+        age = rng.integers(-1, 8, m).astype(np.int32)  # ages <= 1 and >= 4, and a negative one
+        pos[5] = [np.nan, 0.5, 0.5]  # left out of the secondary bounds
+        out.append((pos, vel, vol, age))
+    return out
+
+
+@pytest.mark.parametrize("scene,n,seed,secondary", [("rayleigh_taylor", 16, 3, False), ("bubble_tank", 20, 5, False),
+                                                    ("bubble_tank", 20, 7, True)])
+def test_render_cache_equals_reference_writer(pf, tmp_path, scene, n, seed, secondary):
     sc = getattr(pf.scenes, scene)(n, seed=seed)
     pp = phase_for(sc, pf)
     ps = scene_particles(sc)
@@ -114,6 +130,12 @@ def test_render_cache_equals_reference_writer(pf, tmp_path, scene, n, seed):
         rg.set_field(f, *sim.grid.get_field(f))
     pos, vel, typ, vol = sim.get_particles()
     rg._put(O.Particles(pos.astype(np.float64), vel.astype(np.float64), typ, vol.astype(np.float64)))
+    if secondary:
+        from oracle.secondary import _typed_ref
+        _typed_ref(rg.lib)
+        for w, (sp, sv, svol, sage) in enumerate(_secondary_sets(np.random.default_rng(seed), n)):
+            sim.set_secondary_set(w, sp, sv, svol, sage)
+            rg.lib.pfr_set_secondary_set(rg.h, w, len(sp), sp, sv, svol, sage)
     cam = pf.defaultRenderCacheCamera3D(n, n, n, 1.0 / n)
     a, b = tmp_path / "gpu.jsonl", tmp_path / "ref.jsonl"
     pf.writeSparseRenderCache3D(sim, a, frame, time, cam)
@@ -126,6 +148,11 @@ def test_render_cache_equals_reference_writer(pf, tmp_path, scene, n, seed):
     bad = [(i, x, y) for i, (x, y) in enumerate(zip(la, lb)) if x != y]
     assert not bad, bad[:3]
     assert ta == tb
+    if secondary:
+        # (the planted NaN position makes its line non-JSON, as the reference writes it)
+        channels = {re.search(r'"render_channel":"(\w+)"', ln).group(1) for ln in la
+                    if '"kind":"secondary_droplet","render' in ln}
+        assert channels == {"droplet", "spray", "foam"}
     sim.grid.close()
 
 
