@@ -111,6 +111,8 @@ __device__ __forceinline__ void restrict_warp(const uint8_t* cls, size_t o, doub
 
 // rc[2 tile + c] = sum of the 16 warp partials of the tile's slot, in order
 __global__ void k_rc_reduce(const float* part, const int* slot_tile, int nslots, float* rc, const SolveCtl* skip) {
+  pdl_wait();
+  pdl_launch_dependents();
   if (skip && skip->done) return;
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < 2 * nslots; q += gridDim.x * blockDim.x) {
     const int s = q >> 1, c = q & 1;
@@ -158,6 +160,8 @@ __global__ void k_build_nbr(DevGrid G, int nslots, int* nbr) {
 template <typename V>
 __global__ void __launch_bounds__(PF_TV) k_fx_spmv(const int* __restrict__ nbr, int nslots, SolveCtl* ctl,
                                                    const uint8_t* kind, FlexVec<V> m, double* partials) {
+  pdl_wait();
+  pdl_launch_dependents();
   if (ctl->done) return;
   double acc = 0.0;
   for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
@@ -194,6 +198,8 @@ template <typename V>
 __global__ void __launch_bounds__(PF_TV) k_fx_update(int nslots, SolveCtl* ctl, const uint8_t* kind, FlexVec<V> m,
                                                      const int* slot_tile, const float* ec, float* rc_part,
                                                      double* partials) {
+  pdl_wait();
+  pdl_launch_dependents();
   if (ctl->done) return;
   const V alpha = (V)ctl->alpha;
   const bool used_c = ctl->aux[0] != 0.0;
@@ -227,6 +233,8 @@ constexpr int kGuardThreads = 256;
 
 __global__ void __launch_bounds__(kGuardThreads) k_fx_guard(SolveCtl* ctl, const float* rc, const float* ec, int nu,
                                                             int first, double min_gain, double* partials) {
+  pdl_wait();
+  pdl_launch_dependents();
   if (ctl->done) return;
   const bool offered = ctl->aux[2] != 0.0 && ctl->aux[1] == 0.0;
   double d = 0.0;
@@ -284,6 +292,8 @@ __global__ void __launch_bounds__(kGuardThreads) k_fx_guard(SolveCtl* ctl, const
 template <typename V>
 __global__ void __launch_bounds__(PF_TV) k_fx_dir(const int* slot_tile, int nslots, const SolveCtl* ctl,
                                                   const uint8_t* kind, FlexVec<V> m, const float* ec) {
+  pdl_wait();
+  pdl_launch_dependents();
   if (ctl->done) return;
   const V beta = (V)ctl->beta;
   const bool use_c = ctl->aux[0] != 0.0;
@@ -333,9 +343,9 @@ namespace {
 int coarse_solve(pf_ctx* ctx, int nslots, int precond) {
   CoarseCtx* c = (CoarseCtx*)ctx->learned;
   const int blocks = std::max(1, std::min((2 * nslots + 255) / 256, 148 * 8));
-  (++ctx->launches), k_rc_reduce<<<blocks, 256, 0, ctx->stream>>>(c->rc_part, ctx->slot_tile, nslots, c->op.rc,
-                                                                  ctx->ctl);
-  PF_CUDA_TRY(cudaGetLastError());
+  ++ctx->launches;
+  PF_CUDA_TRY(launch_pdl(k_rc_reduce, dim3(blocks), dim3(256), ctx->stream, (const float*)c->rc_part,
+                         (const int*)ctx->slot_tile, nslots, c->op.rc, (const SolveCtl*)ctx->ctl));
   if (precond == PF_PRECOND_EXACT_COARSE) return coarse_solve_exact(ctx, 400, 1e-6, ctx->ctl);
   return coarse_solve_net(ctx, ctx->ctl);
 }
@@ -344,9 +354,9 @@ int launch_guard(pf_ctx* ctx, bool coarse, int first, double min_gain) {
   CoarseOp& A = ((CoarseCtx*)ctx->learned)->op;
   const int nu = coarse ? 2 * A.nt : 0;
   const int blocks = std::max(1, std::min((nu + kGuardThreads - 1) / kGuardThreads, 64));
-  (++ctx->launches), k_fx_guard<<<blocks, kGuardThreads, 0, ctx->stream>>>(ctx->ctl, A.rc, A.ec, nu, first, min_gain,
-                                                                          ctx->partials);
-  PF_CUDA_TRY(cudaGetLastError());
+  ++ctx->launches;
+  PF_CUDA_TRY(launch_pdl(k_fx_guard, dim3(blocks), dim3(kGuardThreads), ctx->stream, ctx->ctl, (const float*)A.rc,
+                         (const float*)A.ec, nu, first, min_gain, ctx->partials));
   return PF_OK;
 }
 
@@ -357,18 +367,22 @@ int launch_iteration(pf_ctx* ctx, int nslots, int nred, const uint8_t* kind, con
   CoarseOp& A = ((CoarseCtx*)ctx->learned)->op;
   const bool coarse = precond != PF_PRECOND_JACOBI;
   const int* nbr = ((CoarseCtx*)ctx->learned)->nbr;
-  (++ctx->launches), k_fx_spmv<V><<<nred, PF_TV, 0, ctx->stream>>>(nbr, nslots, ctx->ctl, kind, m, ctx->partials);
+  ++ctx->launches;
+  PF_CUDA_TRY(launch_pdl(k_fx_spmv<V>, dim3(nred), dim3(PF_TV), ctx->stream, nbr, nslots, ctx->ctl, kind, m,
+                         ctx->partials));
   float* rc_part = coarse ? ((CoarseCtx*)ctx->learned)->rc_part : nullptr;
-  (++ctx->launches), k_fx_update<V><<<nred, PF_TV, 0, ctx->stream>>>(nslots, ctx->ctl, kind, m, ctx->slot_tile, A.ec,
-                                                                     rc_part, ctx->partials);
+  ++ctx->launches;
+  PF_CUDA_TRY(launch_pdl(k_fx_update<V>, dim3(nred), dim3(PF_TV), ctx->stream, nslots, ctx->ctl, kind, m,
+                         (const int*)ctx->slot_tile, (const float*)A.ec, rc_part, ctx->partials));
   if (coarse) {
     int rc = coarse_solve(ctx, nslots, precond);
     if (rc) return rc;
   }
   int rcg = launch_guard(ctx, coarse, 0, min_gain);
   if (rcg) return rcg;
-  (++ctx->launches), k_fx_dir<V><<<nred, PF_TV, 0, ctx->stream>>>(ctx->slot_tile, nslots, ctx->ctl, kind, m, A.ec);
-  PF_CUDA_TRY(cudaGetLastError());
+  ++ctx->launches;
+  PF_CUDA_TRY(launch_pdl(k_fx_dir<V>, dim3(nred), dim3(PF_TV), ctx->stream, (const int*)ctx->slot_tile, nslots,
+                         (const SolveCtl*)ctx->ctl, kind, m, (const float*)A.ec));
   return PF_OK;
 }
 

@@ -134,6 +134,30 @@ struct SolveCtl {
   double flex[2];          // flexible PCG: r.D^-1 r and r.z_prev of the current residual
 };
 
+// Programmatic dependent launch.  A kernel started by launch_pdl may begin
+// while its predecessor on the stream is still running: it calls pdl_wait()
+// before it touches memory the predecessor writes (the wait returns once the
+// predecessor grid has completed and its writes are visible), and
+// pdl_launch_dependents() to let its own successor be scheduled.  Work before
+// the wait may only read memory no earlier kernel of the chain writes.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;\n" ::); }
+
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t stream, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 }  // namespace pf
 
 #define PF_CUDA_TRY(expr)                                   \

@@ -457,7 +457,10 @@ int unet_backward(pf_ctx* ctx, LearnedState* L, Work& W) {
 // the G path (B samples): e = S G^T G S rc
 
 // Inference: 2 NL launches of the 16-channel G kernel (pool, gates, upsampling
-// and the diagonal scaling folded into its staging and epilogue).
+// and the diagonal scaling folded into its staging and epilogue).  The first
+// launch waits for every earlier kernel, the weights' packing included; the
+// others are programmatic dependent launches that copy their weights while
+// their predecessor drains.
 int gtg_apply(pf_ctx* ctx, LearnedState* L, Work& W, const float* cop, const float* rc_in, float* e_out,
               const SolveCtl* skip) {
   const int NL = W.NL;
@@ -488,7 +491,7 @@ int gtg_apply(pf_ctx* ctx, LearnedState* L, Work& W, const float* cop, const flo
       k_gconv<GIN_SCALE, GOUT_GATE, 2><<<grid(l), 128, 0, ctx->stream>>>(a);
     } else {
       a.x = W.q[l];
-      k_gconv<GIN_PLAIN, GOUT_GATE, 2><<<grid(l), 128, 0, ctx->stream>>>(a);
+      PF_CUDA_TRY(launch_pdl(k_gconv<GIN_PLAIN, GOUT_GATE, 2>, grid(l), dim3(128), ctx->stream, a));
     }
   }
   for (int l = NL - 1; l >= 0; --l) {
@@ -499,11 +502,11 @@ int gtg_apply(pf_ctx* ctx, LearnedState* L, Work& W, const float* cop, const flo
     if (l > 0) {
       a.wf = L->wt[g_layer(l)];
       a.y = W.v[l];
-      k_gconv<GIN_TGATE, GOUT_PLAIN, 2><<<grid(l), 128, 0, ctx->stream>>>(a);
+      PF_CUDA_TRY(launch_pdl(k_gconv<GIN_TGATE, GOUT_PLAIN, 2>, grid(l), dim3(128), ctx->stream, a));
     } else {
       a.wf = L->wt[L_G0];
       a.y = e_out;
-      k_gconv<GIN_TGATE, GOUT_SCALE, 1><<<grid(l), 128, 0, ctx->stream>>>(a);
+      PF_CUDA_TRY(launch_pdl(k_gconv<GIN_TGATE, GOUT_SCALE, 1>, grid(l), dim3(128), ctx->stream, a));
     }
   }
   PF_CUDA_TRY(cudaGetLastError());

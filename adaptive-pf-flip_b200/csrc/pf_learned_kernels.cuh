@@ -798,7 +798,6 @@ __device__ __forceinline__ void ldmatrix_x4(uint32_t* r, uint32_t addr) {
 
 template <int IN, int OUT, int NT>
 __global__ void __launch_bounds__(128) k_gconv(GConvArgs a) {
-  if (a.skip && a.skip->done) return;
   __shared__ __align__(16) __nv_bfloat16 S[kGHN * kGPitch];
   __shared__ __align__(16) uint2 SW[27 * NT * 32];
   __shared__ float2 zx[OUT == GOUT_GATE ? 2 * 32 * NT : 1];
@@ -815,6 +814,14 @@ __global__ void __launch_bounds__(128) k_gconv(GConvArgs a) {
     for (int e = tid; e < kChunks; e += 128)
       asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst + e * 16), "l"(src + (size_t)e * 16));
     asm volatile("cp.async.commit_group;\n" ::);
+  }
+  // the weights are fixed during a solve, so they are copied before the wait
+  // for the previous kernel of the chain (programmatic dependent launch)
+  pdl_wait();
+  pdl_launch_dependents();
+  if (a.skip && a.skip->done) {
+    asm volatile("cp.async.wait_all;\n" ::);
+    return;
   }
 
   // operand halo (10x6x4 positions), rounded to BF16
