@@ -569,26 +569,39 @@ __global__ void k_mr_pin_probe(MrGeom g, const uint8_t* mk, const int4* cells, i
 
 __device__ __forceinline__ int mr_pin(const int* air, int N) { return (*air || N == 0) ? -1 : 0; }
 
+// the most face patches a leaf visits: 6 faces of a 2x2-patch coarse leaf
+constexpr int kMrMaxPatches = 24;
+
+// off-diagonal terms of each row: one per distinct neighbour leaf
 __global__ void k_mr_row_count(MrGeom g, const uint8_t* mk, const int4* cells, const int* cell_idx, int N,
                                const int* air, int* row_len) {
   const int pin = mr_pin(air, N);
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < N; r += gridDim.x * blockDim.x) {
-    int cnt = 0;
+    int cols[kMrMaxPatches];
+    int n = 0;
     if (r != pin)
       mr_visit(g, cells[r], [&](int, int, int, int, int ni, int nj, int nk, double) {
         if (mr_marker(g, mk, ni, nj, nk) == 2) return;
         const int o = cell_idx[mr_cell(g, ni, nj, nk)];  // marker < 2: in the domain
-        if (o >= 0 && o != pin) ++cnt;
+        if (o < 0 || o == pin) return;
+        int q = 0;
+        while (q < n && cols[q] != o) ++q;
+        if (q == n && n < kMrMaxPatches) cols[n++] = o;
       });
-    row_len[r] = cnt;
+    row_len[r] = n;
   }
 }
 
 // The rows are stored as 32-row slices (sliced ELLPACK): term t of row r is
 // entry slice_ptr[r / 32] + 32 t + r % 32, so a warp's 32 rows load each term
 // position together; a slice is as wide as its longest row and shorter rows
-// end in (col = r, coef = 0) terms, which add an exact zero.  Each row keeps
-// its terms in the reference's visit order.
+// end in (col = r, coef = 0) terms, which add an exact zero.  A row holds one
+// term per neighbour leaf, in the order the reference's visit first meets it;
+// the patches a coarse face shares with one coarse neighbour (up to 4) are
+// summed into that term in visit order.  The reference keeps one term per
+// patch; merging them regroups the row's sum (the operator is the same up to
+// rounding, and stays symmetric: both rows of a pair visit their shared
+// patches in the same order) and cuts a coarse row from 24 stored terms to 6.
 __global__ void k_mr_slices(int N, const int* row_len, int* slice_len) {
   const int nslice = (N + 31) / 32;
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s <= nslice; s += gridDim.x * blockDim.x) {
@@ -622,6 +635,8 @@ __global__ void __launch_bounds__(kMrNT) k_mr_rows(MrGeom g, const uint8_t* mk, 
     const int base = slice_ptr[r >> 5] + (r & 31);
     const int width = (slice_ptr[(r >> 5) + 1] - slice_ptr[r >> 5]) >> 5;
     int t = 0;
+    int cols[kMrMaxPatches];
+    double cfs[kMrMaxPatches];
     if (r == pin) {
       diag = 1.0;
     } else {
@@ -641,12 +656,22 @@ __global__ void __launch_bounds__(kMrNT) k_mr_rows(MrGeom g, const uint8_t* mk, 
         diag += coeff;
         const int o = mr_in(g, ni, nj, nk) ? cell_idx[mr_cell(g, ni, nj, nk)] : -1;
         if (o >= 0 && o != pin) {
-          col[base + 32 * t] = o;
-          coef[base + 32 * t] = coeff;
-          ++t;
+          int q = 0;
+          while (q < t && cols[q] != o) ++q;
+          if (q < t) {
+            cfs[q] += coeff;
+          } else if (t < kMrMaxPatches) {
+            cols[t] = o;
+            cfs[t] = coeff;
+            ++t;
+          }
         }
         div += sign * (double)F.f[axis][f] * area / vol;
       });
+      for (int q = 0; q < t; ++q) {
+        col[base + 32 * q] = cols[q];
+        coef[base + 32 * q] = cfs[q];
+      }
     }
     for (; t < width; ++t) {
       col[base + 32 * t] = r;
@@ -710,25 +735,47 @@ __global__ void __launch_bounds__(kMrNT) k_mr_spmv(int N, const int* __restrict_
   mr_reduce(pap, 0.0, 0.0, 0.0, partials, ctl, kMrPAp);
 }
 
-// x += alpha p, r -= alpha Ap, z = M^-1 r; r.z, r.(z - z_prev), max|r|
+// x += alpha p, r -= alpha Ap, z = M^-1 r; r.z, r.(z - z_prev), max|r|.
+// A thread takes kMrRows rows per pass and issues all their loads before its
+// first store, so their memory latencies overlap (the vectors may alias as
+// far as the compiler knows, which would otherwise order every load of a row
+// after the previous row's stores).
+constexpr int kMrRows = 4;
 __global__ void __launch_bounds__(kMrNT) k_mr_update(int N, MrVecs V, MrCtl* ctl, double* partials) {
   if (ctl->done) return;
   const double alpha = ctl->alpha;
   const int jacobi = ctl->jacobi, flexible = ctl->flexible;
+  const int stride = gridDim.x * blockDim.x;
   double rz = 0.0, num = 0.0, bad = 0.0, rmax = 0.0;
-  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < N; r += gridDim.x * blockDim.x) {
-    const double x = V.x[r] + alpha * V.p[r];
-    const double rr = V.r[r] - alpha * V.Ap[r];
-    V.x[r] = x;
-    V.r[r] = rr;
-    if (!isfinite(x) || !isfinite(rr)) bad += 1.0;
-    if (isfinite(rr)) rmax = fmax(rmax, fabs(rr));
-    const double d = V.diag[r];
-    const double z = (jacobi && d > 0.0) ? rr / d : rr;
-    const double zp = V.z[r];
-    V.z[r] = z;
-    rz += rr * z;
-    if (flexible) num += rr * (z - zp);
+  for (int r0 = blockIdx.x * blockDim.x + threadIdx.x; r0 < N; r0 += kMrRows * stride) {
+    double x[kMrRows], p[kMrRows], rr[kMrRows], ap[kMrRows], d[kMrRows], zp[kMrRows];
+#pragma unroll
+    for (int k = 0; k < kMrRows; ++k) {
+      const int r = r0 + k * stride;
+      if (r < N) {
+        x[k] = V.x[r];
+        p[k] = V.p[r];
+        rr[k] = V.r[r];
+        ap[k] = V.Ap[r];
+        d[k] = V.diag[r];
+        zp[k] = V.z[r];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kMrRows; ++k) {
+      const int r = r0 + k * stride;
+      if (r >= N) continue;
+      const double xn = x[k] + alpha * p[k];
+      const double rn = rr[k] - alpha * ap[k];
+      V.x[r] = xn;
+      V.r[r] = rn;
+      if (!isfinite(xn) || !isfinite(rn)) bad += 1.0;
+      if (isfinite(rn)) rmax = fmax(rmax, fabs(rn));
+      const double z = (jacobi && d[k] > 0.0) ? rn / d[k] : rn;
+      V.z[r] = z;
+      rz += rn * z;
+      if (flexible) num += rn * (z - zp[k]);
+    }
   }
   mr_reduce(rz, num, bad, rmax, partials, ctl, kMrUpdate);
 }
@@ -1235,6 +1282,9 @@ int project_mr(pf_ctx* ctx, MrState* s, const pf_mr_step_cfg* cfg, pf_mr_step_st
   // 4 CTAs per SM: more CTAs spend more on the last-CTA reductions' atomics
   // than they gain in load parallelism
   const int nred = grid_for(N, 4 * ctx->num_sms);
+  // the update keeps kMrRows rows of loads in flight per thread (94
+  // registers): one wave of 2 CTAs per SM
+  const int nupd = grid_for(N, 2 * ctx->num_sms);
   (++ctx->launches), k_mr_ctl_init<<<1, 1, 0, ctx->stream>>>(s->ctl, cfg->cg_iters, cfg->cg_tol, cfg->cg_rel_tol,
                                                              cfg->jacobi, cfg->flexible_beta, cfg->adaptive_restart,
                                                              cfg->restart_growth);
@@ -1261,7 +1311,7 @@ int project_mr(pf_ctx* ctx, MrState* s, const pf_mr_step_cfg* cfg, pf_mr_step_st
                                                                     p, V.Ap, V.diag, s->ctl, s->partials, tot + 3);
       MrVecs Vi = V;
       Vi.p = p;
-      (++ctx->launches), k_mr_update<<<nred, kMrNT, 0, ctx->stream>>>(N, Vi, s->ctl, s->partials);
+      (++ctx->launches), k_mr_update<<<nupd, kMrNT, 0, ctx->stream>>>(N, Vi, s->ctl, s->partials);
     }
     PF_CUDA_TRY(cudaGetLastError());
     launched += batch;
