@@ -158,16 +158,18 @@ __global__ void k_build_nbr(DevGrid G, int nslots, int* nbr) {
 }
 
 template <typename V>
-__global__ void __launch_bounds__(PF_TV) k_fx_spmv(const int* __restrict__ nbr, int nslots, SolveCtl* ctl,
+__global__ void __launch_bounds__(PF_TV, 4) k_fx_spmv(const int* __restrict__ nbr, int nslots, SolveCtl* ctl,
                                                    const uint8_t* kind, FlexVec<V> m, double* partials) {
   pdl_wait();
   pdl_launch_dependents();
   if (ctl->done) return;
+  const int l = threadIdx.x;
   double acc = 0.0;
+  uint8_t kd_next = blockIdx.x < nslots ? kind[(size_t)blockIdx.x * PF_TV + l] : 0;
   for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
-    const int l = threadIdx.x;
     const size_t o = (size_t)s * PF_TV + l;
-    const uint8_t kd = kind[o];
+    const uint8_t kd = kd_next;
+    kd_next = next_kind(kind, s + gridDim.x, nslots, l);
     if (!kd) continue;
     const V p0 = m.p[o];
     V ap;
@@ -204,9 +206,11 @@ __global__ void __launch_bounds__(PF_TV) k_fx_update(int nslots, SolveCtl* ctl, 
   const V alpha = (V)ctl->alpha;
   const bool used_c = ctl->aux[0] != 0.0;
   double rmax = 0.0, rzj = 0.0, rzp = 0.0;
+  uint8_t kd_next = blockIdx.x < nslots ? kind[(size_t)blockIdx.x * PF_TV + threadIdx.x] : 0;
   for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
     const size_t o = (size_t)s * PF_TV + threadIdx.x;
-    const uint8_t kd = kind[o];
+    const uint8_t kd = kd_next;
+    kd_next = next_kind(kind, s + gridDim.x, nslots, threadIdx.x);
     double rn = 0.0;
     if (kd) {
       m.e[o] += alpha * m.p[o];
@@ -297,9 +301,11 @@ __global__ void __launch_bounds__(PF_TV) k_fx_dir(const int* slot_tile, int nslo
   if (ctl->done) return;
   const V beta = (V)ctl->beta;
   const bool use_c = ctl->aux[0] != 0.0;
+  uint8_t kd_next = blockIdx.x < nslots ? kind[(size_t)blockIdx.x * PF_TV + threadIdx.x] : 0;
   for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
     const size_t o = (size_t)s * PF_TV + threadIdx.x;
-    const uint8_t kd = kind[o];
+    const uint8_t kd = kd_next;
+    kd_next = next_kind(kind, s + gridDim.x, nslots, threadIdx.x);
     if (!kd) continue;
     double z = (double)m.r[o] * inv_diag(m, kd, o);
     if (use_c) z += coarse_term(m, slot_tile, s, o, ec);

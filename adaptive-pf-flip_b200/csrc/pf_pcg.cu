@@ -82,11 +82,13 @@ __global__ void __launch_bounds__(PF_TV) k_spmv_plain_tab(int nslots, SolveCtl* 
                                                           const int* __restrict__ nbr, PcgVec<double> v,
                                                           double scale, double* partials) {
   if (ctl->done) return;
+  const int l = threadIdx.x;
   double acc = 0.0;
+  uint8_t kd_next = next_kind(kind, blockIdx.x, nslots, l);
   for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
-    const int l = threadIdx.x;
     const size_t o = (size_t)s * PF_TV + l;
-    const uint8_t kd = kind[o];
+    const uint8_t kd = kd_next;
+    kd_next = next_kind(kind, s + gridDim.x, nslots, l);
     if (!kd) continue;
     const double p0 = v.p[o];
     double ap;
@@ -116,9 +118,11 @@ __global__ void __launch_bounds__(PF_TV) k_update_plain(int nslots, SolveCtl* ct
   if (ctl->done) return;
   const double alpha = ctl->alpha;
   double rz = 0.0, rmax = 0.0;
+  uint8_t kd_next = next_kind(kind, blockIdx.x, nslots, threadIdx.x);
   for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
     const size_t o = (size_t)s * PF_TV + threadIdx.x;
-    const uint8_t kd = kind[o];
+    const uint8_t kd = kd_next;
+    kd_next = next_kind(kind, s + gridDim.x, nslots, threadIdx.x);
     if (!kd) continue;
     const double pp = v.p[o];
     v.x[o] = __dadd_rn(v.x[o], __dmul_rn(alpha, pp));
@@ -136,9 +140,11 @@ __global__ void __launch_bounds__(PF_TV) k_direction_plain(int nslots, const Sol
                                                            PcgVec<double> v, double scale) {
   if (ctl->done) return;
   const double beta = ctl->beta;
+  uint8_t kd_next = next_kind(kind, blockIdx.x, nslots, threadIdx.x);
   for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
     const size_t o = (size_t)s * PF_TV + threadIdx.x;
-    const uint8_t kd = kind[o];
+    const uint8_t kd = kd_next;
+    kd_next = next_kind(kind, s + gridDim.x, nslots, threadIdx.x);
     if (!kd) continue;
     const double d = kd == 2 ? 1.0 : __dmul_rn(scale, v.diag[o]);
     const double z = d > 0.0 ? __ddiv_rn(v.r[o], d) : 0.0;
@@ -230,14 +236,16 @@ __global__ void __launch_bounds__(PF_TV) k_mixed_spmv(DevGrid G, int nslots, Sol
                                                       MixVec<CC, CP> m, double* partials) {
   if (ctl->done) return;
   __shared__ int nbs[6];
+  const int l = threadIdx.x;
   double acc = 0.0;
+  uint8_t kd_next = next_kind(kind, blockIdx.x, nslots, l);
   for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
     __syncthreads();
     neighbor_slots(G, s, nbs);
     __syncthreads();
-    const int l = threadIdx.x;
     const size_t o = (size_t)s * PF_TV + l;
-    const uint8_t kd = kind[o];
+    const uint8_t kd = kd_next;
+    kd_next = next_kind(kind, s + gridDim.x, nslots, l);
     if (!kd) continue;
     const float p0 = ldc(m.p, o);
     float ap;
@@ -267,9 +275,11 @@ __global__ void __launch_bounds__(PF_TV) k_mixed_update(int nslots, SolveCtl* ct
   if (ctl->done) return;
   const float alpha = (float)ctl->alpha;
   double rz = 0.0, rmax = 0.0;
+  uint8_t kd_next = next_kind(kind, blockIdx.x, nslots, threadIdx.x);
   for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
     const size_t o = (size_t)s * PF_TV + threadIdx.x;
-    const uint8_t kd = kind[o];
+    const uint8_t kd = kd_next;
+    kd_next = next_kind(kind, s + gridDim.x, nslots, threadIdx.x);
     if (!kd) continue;
     m.e[o] += alpha * ldc(m.p, o);
     const float r = m.r[o] - alpha * m.Ap[o];
@@ -287,9 +297,12 @@ __global__ void __launch_bounds__(PF_TV) k_mixed_direction(int nslots, const Sol
                                                            MixVec<CC, CP> m) {
   if (ctl->done) return;
   const float beta = (float)ctl->beta;
+  uint8_t kd_next = next_kind(kind, blockIdx.x, nslots, threadIdx.x);
   for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
     const size_t o = (size_t)s * PF_TV + threadIdx.x;
-    if (!kind[o]) continue;
+    const uint8_t kd = kd_next;
+    kd_next = next_kind(kind, s + gridDim.x, nslots, threadIdx.x);
+    if (!kd) continue;
     const float d = m.d[o];
     const float z = d > 0.0f ? m.r[o] / d : 0.0f;
     stc(m.p, o, z + beta * ldc(m.p, o));

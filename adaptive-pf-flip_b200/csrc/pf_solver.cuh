@@ -177,6 +177,14 @@ __device__ __forceinline__ void block_reduce_2(double a, double b, double* parti
   block_reduce_3(a, b, 0.0, partials, ctl, stage);
 }
 
+// The streaming passes of the solvers walk their slots with a grid stride
+// and read each cell's kind before its operands.  They load the kind of the
+// next slot one trip ahead, so a trip waits for one round of memory latency
+// (the operands) instead of two (kind, then operands).
+__device__ __forceinline__ uint8_t next_kind(const uint8_t* kind, int s, int nslots, int l) {
+  return s < nslots ? kind[(size_t)s * PF_TV + l] : (uint8_t)0;
+}
+
 // Neighbour slots of the tile of slot s, order +x -x +y -y +z -z (-1 if none).
 __device__ __forceinline__ void neighbor_slots(const DevGrid& G, int s, int* nbs) {
   if (threadIdx.x < 6) {
