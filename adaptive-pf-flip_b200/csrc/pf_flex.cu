@@ -81,11 +81,20 @@ __device__ __forceinline__ double inv_diag(const FlexVec<V>& m, uint8_t kd, size
   return d > 0.0 ? 1.0 / d : 0.0;
 }
 
+// The passes round exactly as written: every multiply-add is an explicit fused
+// fma (or an explicit product and sum), so the results do not depend on which
+// products the compiler would contract in a given code layout.
+__device__ __forceinline__ double fmav(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float fmav(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+
+// r d^-1 + c (Jacobi term plus the coarse term), a product then a sum
+__device__ __forceinline__ double coarse_add(double r, double di, double c) { return __dadd_rn(__dmul_rn(r, di), c); }
+
+// inv_diag from the diagonal entry already loaded
 template <typename V>
-__device__ __forceinline__ double coarse_term(const FlexVec<V>& m, const int* slot_tile, int s, size_t o,
-                                              const float* ec) {
-  const uint8_t c = m.cls[o];
-  return c != 255 ? (double)ec[coarse_index(slot_tile[s], c)] : 0.0;
+__device__ __forceinline__ double inv_diag_of(const FlexVec<V>& m, uint8_t kd, V dv) {
+  const double d = kd == 1 ? (double)m.scale * (double)dv : 0.0;
+  return d > 0.0 ? 1.0 / d : 0.0;
 }
 
 constexpr int kWarpsPerSlot = PF_TV / 32;
@@ -95,6 +104,22 @@ constexpr int kWarpsPerSlot = PF_TV / 32;
 __device__ __forceinline__ void restrict_warp(const uint8_t* cls, size_t o, double r, int s, float* part) {
   // FP32 suffices for the coarse residual (the preconditioner's input)
   const uint8_t c = cls[o];
+  const float rf = (float)r;
+  float a0 = c == 0 ? rf : 0.0f, a1 = c == 1 ? rf : 0.0f;
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) {
+    a0 += __shfl_down_sync(0xffffffffu, a0, d);
+    a1 += __shfl_down_sync(0xffffffffu, a1, d);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    float* q = part + ((size_t)s * kWarpsPerSlot + (threadIdx.x >> 5)) * 2;
+    q[0] = a0;
+    q[1] = a1;
+  }
+}
+
+// restrict_warp with the cell's class already loaded
+__device__ __forceinline__ void restrict_warp_c(uint8_t c, double r, int s, float* part) {
   const float rf = (float)r;
   float a0 = c == 0 ? rf : 0.0f, a1 = c == 1 ? rf : 0.0f;
 #pragma unroll
@@ -165,7 +190,7 @@ __global__ void __launch_bounds__(PF_TV, 4) k_fx_spmv(const int* __restrict__ nb
   if (ctl->done) return;
   const int l = threadIdx.x;
   double acc = 0.0;
-  uint8_t kd_next = blockIdx.x < nslots ? kind[(size_t)blockIdx.x * PF_TV + l] : 0;
+  uint8_t kd_next = next_kind(kind, blockIdx.x, nslots, l);
   for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
     const size_t o = (size_t)s * PF_TV + l;
     const uint8_t kd = kd_next;
@@ -179,16 +204,16 @@ __global__ void __launch_bounds__(PF_TV, 4) k_fx_spmv(const int* __restrict__ nb
       long long no[6];
       neighbor_offsets_tab(nbr, s, l, no);
       V off = (V)0;
-      if (no[0] >= 0) off += m.cx[no[0]] * m.p[no[0]];
-      if (no[1] >= 0) off += m.cx[o] * m.p[no[1]];
-      if (no[2] >= 0) off += m.cy[no[2]] * m.p[no[2]];
-      if (no[3] >= 0) off += m.cy[o] * m.p[no[3]];
-      if (no[4] >= 0) off += m.cz[no[4]] * m.p[no[4]];
-      if (no[5] >= 0) off += m.cz[o] * m.p[no[5]];
-      ap = m.scale * (m.d[o] * p0 - off);
+      if (no[0] >= 0) off = fmav(m.cx[no[0]], m.p[no[0]], off);
+      if (no[1] >= 0) off = fmav(m.cx[o], m.p[no[1]], off);
+      if (no[2] >= 0) off = fmav(m.cy[no[2]], m.p[no[2]], off);
+      if (no[3] >= 0) off = fmav(m.cy[o], m.p[no[3]], off);
+      if (no[4] >= 0) off = fmav(m.cz[no[4]], m.p[no[4]], off);
+      if (no[5] >= 0) off = fmav(m.cz[o], m.p[no[5]], off);
+      ap = m.scale * fmav(m.d[o], p0, -off);
     }
     m.Ap[o] = ap;
-    acc += (double)p0 * (double)ap;
+    acc = fmav((double)p0, (double)ap, acc);
   }
   block_reduce_2(acc, 0.0, partials, ctl, kStagePAp);
 }
@@ -206,26 +231,34 @@ __global__ void __launch_bounds__(PF_TV) k_fx_update(int nslots, SolveCtl* ctl, 
   const V alpha = (V)ctl->alpha;
   const bool used_c = ctl->aux[0] != 0.0;
   double rmax = 0.0, rzj = 0.0, rzp = 0.0;
-  uint8_t kd_next = blockIdx.x < nslots ? kind[(size_t)blockIdx.x * PF_TV + threadIdx.x] : 0;
+  const int l = threadIdx.x;
+  const bool want_cls = used_c || rc_part != nullptr;
+  uint8_t kd_next = next_kind(kind, blockIdx.x, nslots, l);
+  uint8_t cl_next = want_cls ? next_kind(m.cls, blockIdx.x, nslots, l) : (uint8_t)255;
+  int tile_next = used_c && blockIdx.x < nslots ? slot_tile[blockIdx.x] : 0;
   for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
-    const size_t o = (size_t)s * PF_TV + threadIdx.x;
-    const uint8_t kd = kd_next;
-    kd_next = next_kind(kind, s + gridDim.x, nslots, threadIdx.x);
+    const size_t o = (size_t)s * PF_TV + l;
+    const uint8_t kd = kd_next, cl = cl_next;
+    const int tile = tile_next;
+    const int sn = s + gridDim.x;
+    kd_next = next_kind(kind, sn, nslots, l);
+    if (want_cls) cl_next = next_kind(m.cls, sn, nslots, l);
+    if (used_c && sn < nslots) tile_next = slot_tile[sn];
     double rn = 0.0;
     if (kd) {
-      m.e[o] += alpha * m.p[o];
-      const V r_old = m.r[o];
-      const V r = r_old - alpha * m.Ap[o];
+      const float ev = used_c && cl != 255 ? ec[coarse_index(tile, cl)] : 0.0f;
+      const V e = m.e[o], p = m.p[o], r_old = m.r[o], ap = m.Ap[o], dv = m.d[o];
+      m.e[o] = fmav(alpha, p, e);
+      const V r = fmav(-alpha, ap, r_old);
       m.r[o] = r;
       rn = (double)r;
-      const double di = inv_diag(m, kd, o);
-      double zp = (double)r_old * di;
-      if (used_c) zp += coarse_term(m, slot_tile, s, o, ec);
+      const double di = inv_diag_of(m, kd, dv);
+      const double zp = used_c ? coarse_add((double)r_old, di, cl != 255 ? (double)ev : 0.0) : (double)r_old * di;
       rmax = fmax(rmax, fabs(rn));
-      rzj += rn * rn * di;
-      rzp += rn * zp;
+      rzj = fmav(rn * rn, di, rzj);
+      rzp = fmav(rn, zp, rzp);
     }
-    if (rc_part) restrict_warp(m.cls, o, rn, s, rc_part);
+    if (rc_part) restrict_warp_c(cl, rn, s, rc_part);
   }
   block_reduce_3(rzj, rmax, rzp, partials, ctl, kStageFlex);
 }
@@ -301,15 +334,29 @@ __global__ void __launch_bounds__(PF_TV) k_fx_dir(const int* slot_tile, int nslo
   if (ctl->done) return;
   const V beta = (V)ctl->beta;
   const bool use_c = ctl->aux[0] != 0.0;
-  uint8_t kd_next = blockIdx.x < nslots ? kind[(size_t)blockIdx.x * PF_TV + threadIdx.x] : 0;
+  const int l = threadIdx.x;
+  uint8_t kd_next = next_kind(kind, blockIdx.x, nslots, l);
+  uint8_t cl_next = use_c ? next_kind(m.cls, blockIdx.x, nslots, l) : (uint8_t)255;
+  int tile_next = use_c && blockIdx.x < nslots ? slot_tile[blockIdx.x] : 0;
   for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
-    const size_t o = (size_t)s * PF_TV + threadIdx.x;
-    const uint8_t kd = kd_next;
-    kd_next = next_kind(kind, s + gridDim.x, nslots, threadIdx.x);
+    const size_t o = (size_t)s * PF_TV + l;
+    const uint8_t kd = kd_next, cl = cl_next;
+    const int tile = tile_next;
+    const int sn = s + gridDim.x;
+    kd_next = next_kind(kind, sn, nslots, l);
+    if (use_c) {
+      cl_next = next_kind(m.cls, sn, nslots, l);
+      if (sn < nslots) tile_next = slot_tile[sn];
+    }
     if (!kd) continue;
-    double z = (double)m.r[o] * inv_diag(m, kd, o);
-    if (use_c) z += coarse_term(m, slot_tile, s, o, ec);
-    m.p[o] = (V)z + beta * m.p[o];
+    const float ev = use_c && cl != 255 ? ec[coarse_index(tile, cl)] : 0.0f;
+    const double di = inv_diag(m, kd, o);
+    if (use_c) {
+      const double z = coarse_add((double)m.r[o], di, cl != 255 ? (double)ev : 0.0);
+      m.p[o] = fmav(beta, m.p[o], (V)z);
+    } else {  // Jacobi only: one fma of r d^-1 over beta p
+      m.p[o] = (V)fmav((double)m.r[o], di, (double)(beta * m.p[o]));
+    }
   }
 }
 

@@ -78,17 +78,21 @@ __global__ void k_plain_nbr(DevGrid G, int nslots, int* nbr) {
 // k_spmv_plain with the cross-tile neighbours read from the table: no shared
 // memory or barriers per tile, so a CTA's loads of one tile do not wait on a
 // neighbour-slot round trip.  Same arithmetic and order as k_spmv_plain.
-__global__ void __launch_bounds__(PF_TV) k_spmv_plain_tab(int nslots, SolveCtl* ctl, const uint8_t* kind,
+__global__ void __launch_bounds__(PF_TV, 4) k_spmv_plain_tab(int nslots, SolveCtl* ctl, const uint8_t* kind,
                                                           const int* __restrict__ nbr, PcgVec<double> v,
                                                           double scale, double* partials) {
   if (ctl->done) return;
   const int l = threadIdx.x;
   double acc = 0.0;
   uint8_t kd_next = next_kind(kind, blockIdx.x, nslots, l);
+  int nb_next = nbr_lane(nbr, blockIdx.x, nslots);
   for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
     const size_t o = (size_t)s * PF_TV + l;
     const uint8_t kd = kd_next;
+    const int nb = nb_next;
     kd_next = next_kind(kind, s + gridDim.x, nslots, l);
+    nb_next = nbr_lane(nbr, s + gridDim.x, nslots);
+    const int3 nt = neighbor_lanes(nb, l);
     if (!kd) continue;
     const double p0 = v.p[o];
     double ap;
@@ -96,7 +100,7 @@ __global__ void __launch_bounds__(PF_TV) k_spmv_plain_tab(int nslots, SolveCtl* 
       ap = p0;
     } else {
       long long no[6];
-      neighbor_offsets_tab(nbr, s, l, no);
+      neighbor_offsets_sel(nt, s, l, no);
       // +x -x +y -y +z -z, the reference's face order
       const double c[6] = {no[0] >= 0 ? v.cx[no[0]] : 0.0, v.cx[o], no[2] >= 0 ? v.cy[no[2]] : 0.0, v.cy[o],
                            no[4] >= 0 ? v.cz[no[4]] : 0.0, v.cz[o]};
@@ -124,11 +128,11 @@ __global__ void __launch_bounds__(PF_TV) k_update_plain(int nslots, SolveCtl* ct
     const uint8_t kd = kd_next;
     kd_next = next_kind(kind, s + gridDim.x, nslots, threadIdx.x);
     if (!kd) continue;
-    const double pp = v.p[o];
-    v.x[o] = __dadd_rn(v.x[o], __dmul_rn(alpha, pp));
-    const double r = __dsub_rn(v.r[o], __dmul_rn(alpha, v.Ap[o]));
+    const double pp = v.p[o], x = v.x[o], r_old = v.r[o], ap = v.Ap[o], dg = v.diag[o];
+    v.x[o] = __dadd_rn(x, __dmul_rn(alpha, pp));
+    const double r = __dsub_rn(r_old, __dmul_rn(alpha, ap));
     v.r[o] = r;
-    const double d = kd == 2 ? 1.0 : __dmul_rn(scale, v.diag[o]);
+    const double d = kd == 2 ? 1.0 : __dmul_rn(scale, dg);
     const double z = d > 0.0 ? __ddiv_rn(r, d) : 0.0;
     rz = __dadd_rn(rz, __dmul_rn(r, z));
     rmax = fmax(rmax, fabs(r));

@@ -180,7 +180,11 @@ __device__ __forceinline__ void block_reduce_2(double a, double b, double* parti
 // The streaming passes of the solvers walk their slots with a grid stride
 // and read each cell's kind before its operands.  They load the kind of the
 // next slot one trip ahead, so a trip waits for one round of memory latency
-// (the operands) instead of two (kind, then operands).
+// (the operands) instead of two (kind, then operands).  The same holds for
+// every other value an operand's address depends on (a cell's coarse class,
+// the slot's tile, the neighbour table), and a pass issues all loads of a
+// cell before its first store: the vectors may alias as far as the compiler
+// knows, so a load after a store waits for the store's operands.
 __device__ __forceinline__ uint8_t next_kind(const uint8_t* kind, int s, int nslots, int l) {
   return s < nslots ? kind[(size_t)s * PF_TV + l] : (uint8_t)0;
 }
@@ -228,6 +232,37 @@ __device__ __forceinline__ void neighbor_offsets_tab(const int* __restrict__ nbr
   off[3] = ly > 0 ? base + l - 8 : ((t = __ldg(nb + 3)) >= 0 ? (long long)t * PF_TV + (l | 56) : -1);
   off[4] = lz < 7 ? base + l + 64 : ((t = __ldg(nb + 4)) >= 0 ? (long long)t * PF_TV + (l & ~448) : -1);
   off[5] = lz > 0 ? base + l - 64 : ((t = __ldg(nb + 5)) >= 0 ? (long long)t * PF_TV + (l | 448) : -1);
+}
+
+// The table entries of slot s held one per lane: lane d < 6 of every warp
+// holds nbr[6 s + d] (-1 past the last slot).  A pass loads them one trip of
+// its slot loop ahead, so the neighbour gathers of a trip need no table round
+// trip.
+__device__ __forceinline__ int nbr_lane(const int* __restrict__ nbr, int s, int nslots) {
+  const int lane = threadIdx.x & 31;
+  return s < nslots && lane < 6 ? __ldg(nbr + 6 * (size_t)s + lane) : -1;
+}
+
+// The neighbour slot a cell needs per axis, from the entries nbr_lane gave:
+// the +side slot for a cell on the tile's high face, the -side slot
+// otherwise (only a cell on the low face uses it).  Every lane of the warp
+// must call it (shuffles).
+__device__ __forceinline__ int3 neighbor_lanes(int nbl, int l) {
+  const int lx = l & 7, ly = (l >> 3) & 7, lz = l >> 6;
+  return make_int3(__shfl_sync(0xffffffffu, nbl, lx == 7 ? 0 : 1), __shfl_sync(0xffffffffu, nbl, ly == 7 ? 2 : 3),
+                   __shfl_sync(0xffffffffu, nbl, lz == 7 ? 4 : 5));
+}
+
+// neighbor_offsets_tab from the slots neighbor_lanes gave
+__device__ __forceinline__ void neighbor_offsets_sel(int3 t, int s, int l, long long* off) {
+  const int lx = l & 7, ly = (l >> 3) & 7, lz = l >> 6;
+  const long long base = (long long)s * PF_TV;
+  off[0] = lx < 7 ? base + l + 1 : (t.x >= 0 ? (long long)t.x * PF_TV + (l & ~7) : -1);
+  off[1] = lx > 0 ? base + l - 1 : (t.x >= 0 ? (long long)t.x * PF_TV + (l | 7) : -1);
+  off[2] = ly < 7 ? base + l + 8 : (t.y >= 0 ? (long long)t.y * PF_TV + (l & ~56) : -1);
+  off[3] = ly > 0 ? base + l - 8 : (t.y >= 0 ? (long long)t.y * PF_TV + (l | 56) : -1);
+  off[4] = lz < 7 ? base + l + 64 : (t.z >= 0 ? (long long)t.z * PF_TV + (l & ~448) : -1);
+  off[5] = lz > 0 ? base + l - 64 : (t.z >= 0 ? (long long)t.z * PF_TV + (l | 448) : -1);
 }
 
 // nbr[6 s + d] for every pooled slot (pf_flex.cu)
