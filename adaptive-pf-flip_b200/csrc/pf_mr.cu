@@ -693,6 +693,11 @@ __global__ void __launch_bounds__(kMrNT) k_mr_rows(MrGeom g, const uint8_t* mk, 
 // The direction p = z + beta p_prev (the previous iteration's update, or a
 // restart's beta = 0) formed where it is used, Ap (applyA, :824-838) and
 // p.Ap -> alpha.  p_prev and p are separate buffers, alternated by the host.
+// Two rows per thread and pass (rows r and r + stride, in that order, so the
+// p.Ap partial keeps the one-row order): the slice offsets, the column and
+// coefficient loads and the neighbour gathers of both rows go out together,
+// so a row's three dependent rounds of memory latency overlap the other's.
+constexpr int kMrSpmvRows = 2;
 __global__ void __launch_bounds__(kMrNT) k_mr_spmv(int N, const int* __restrict__ slice_ptr,
                                                  const int* __restrict__ col, const double* __restrict__ coef,
                                                  const double* __restrict__ z, const double* __restrict__ p_prev,
@@ -701,36 +706,61 @@ __global__ void __launch_bounds__(kMrNT) k_mr_spmv(int N, const int* __restrict_
   if (ctl->done) return;
   const int pin = mr_pin(air, N);
   const double beta = ctl->beta;
+  const int stride = gridDim.x * blockDim.x;
   double pap = 0.0;
-  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < N; r += gridDim.x * blockDim.x) {
-    const double pr = z[r] + beta * p_prev[r];
-    double ap;
-    if (r == pin) {
-      ap = pr;
-    } else {
-      const int s = r >> 5;
-      const int b0 = slice_ptr[s] + (r & 31), width = (slice_ptr[s + 1] - slice_ptr[s]) >> 5;
-      // the loads of four terms go out together; the sum keeps the term order
-      double off = 0.0;
-      for (int t = 0; t < width; t += 4) {
-        int cc[4];
-        double cf[4], pv[4];
+  for (int r0 = blockIdx.x * blockDim.x + threadIdx.x; r0 < N; r0 += kMrSpmvRows * stride) {
+    int rr[kMrSpmvRows], b0[kMrSpmvRows], w[kMrSpmvRows];
+    double zr[kMrSpmvRows], pq[kMrSpmvRows], dg[kMrSpmvRows], off[kMrSpmvRows];
+#pragma unroll
+    for (int k = 0; k < kMrSpmvRows; ++k) {
+      const int r = r0 + k * stride;
+      rr[k] = r;
+      w[k] = 0;
+      b0[k] = 0;
+      off[k] = 0.0;
+      if (r < N) {
+        zr[k] = z[r];
+        pq[k] = p_prev[r];
+        dg[k] = diag[r];
+        const int s = r >> 5;
+        const int a = slice_ptr[s];
+        b0[k] = a + (r & 31);
+        w[k] = r == pin ? 0 : (slice_ptr[s + 1] - a) >> 5;
+      }
+    }
+    const int wmax = max(w[0], w[1]);
+    // the loads of four terms per row go out together; each row's sum keeps its term order
+    for (int t = 0; t < wmax; t += 4) {
+      int cc[kMrSpmvRows][4];
+      double cf[kMrSpmvRows][4], pv[kMrSpmvRows][4];
+#pragma unroll
+      for (int k = 0; k < kMrSpmvRows; ++k)
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-          cc[u] = t + u < width ? col[b0 + 32 * (t + u)] : r;
-          cf[u] = t + u < width ? coef[b0 + 32 * (t + u)] : 0.0;
+          const bool in = t + u < w[k];
+          cc[k][u] = in ? col[b0[k] + 32 * (t + u)] : -1;
+          cf[k][u] = in ? coef[b0[k] + 32 * (t + u)] : 0.0;
         }
 #pragma unroll
-        for (int u = 0; u < 4; ++u) pv[u] = z[cc[u]] + beta * p_prev[cc[u]];
+      for (int k = 0; k < kMrSpmvRows; ++k)
+#pragma unroll
+        for (int u = 0; u < 4; ++u) pv[k][u] = cc[k][u] >= 0 ? z[cc[k][u]] + beta * p_prev[cc[k][u]] : 0.0;
+#pragma unroll
+      for (int k = 0; k < kMrSpmvRows; ++k)
 #pragma unroll
         for (int u = 0; u < 4; ++u)
-          if (t + u < width) off += cf[u] * pv[u];
-      }
-      ap = diag[r] * pr - off;
+          if (t + u < w[k]) off[k] += cf[k][u] * pv[k][u];
     }
-    p[r] = pr;
-    Ap[r] = ap;
-    pap += pr * ap;
+#pragma unroll
+    for (int k = 0; k < kMrSpmvRows; ++k) {
+      const int r = rr[k];
+      if (r >= N) continue;
+      const double pr = zr[k] + beta * pq[k];
+      const double ap = r == pin ? pr : dg[k] * pr - off[k];
+      p[r] = pr;
+      Ap[r] = ap;
+      pap += pr * ap;
+    }
   }
   mr_reduce(pap, 0.0, 0.0, 0.0, partials, ctl, kMrPAp);
 }
@@ -1285,6 +1315,9 @@ int project_mr(pf_ctx* ctx, MrState* s, const pf_mr_step_cfg* cfg, pf_mr_step_st
   // the update keeps kMrRows rows of loads in flight per thread (94
   // registers): one wave of 2 CTAs per SM
   const int nupd = grid_for(N, 2 * ctx->num_sms);
+  // the SpMV keeps two rows in flight per thread (80 registers): one wave of
+  // 3 CTAs per SM
+  const int nspmv = grid_for(N, 3 * ctx->num_sms);
   (++ctx->launches), k_mr_ctl_init<<<1, 1, 0, ctx->stream>>>(s->ctl, cfg->cg_iters, cfg->cg_tol, cfg->cg_rel_tol,
                                                              cfg->jacobi, cfg->flexible_beta, cfg->adaptive_restart,
                                                              cfg->restart_growth);
@@ -1307,7 +1340,7 @@ int project_mr(pf_ctx* ctx, MrState* s, const pf_mr_step_cfg* cfg, pf_mr_step_st
       const int q = (launched + b) & 1;
       double* p_prev = pbuf[q];
       double* p = pbuf[q ^ 1];
-      (++ctx->launches), k_mr_spmv<<<nred, kMrNT, 0, ctx->stream>>>(N, s->slice_ptr, s->col, s->coef, V.z, p_prev,
+      (++ctx->launches), k_mr_spmv<<<nspmv, kMrNT, 0, ctx->stream>>>(N, s->slice_ptr, s->col, s->coef, V.z, p_prev,
                                                                     p, V.Ap, V.diag, s->ctl, s->partials, tot + 3);
       MrVecs Vi = V;
       Vi.p = p;
