@@ -827,7 +827,7 @@ __device__ __forceinline__ int stage_axis(int l, bool normal, int (&off)[2], int
 // Nodes of blocks the exact activation left inactive are cleared: the splat's
 // FP32 weights may put a negligible contribution where the reference's FP64
 // weight is zero, and inactive blocks stay zero.
-__global__ void __launch_bounds__(PF_TV, 2) k_normalize(DevGrid G, const float2* __restrict__ stage, const int* __restrict__ cell_start,
+__global__ void __launch_bounds__(PF_TV, 4) k_normalize(DevGrid G, const float2* __restrict__ stage, const int* __restrict__ cell_start,
                             int gather, const int* __restrict__ d_nslots, int save, int gravity, float dv) {
   __shared__ int splatted[27];
   const int nslots = *d_nslots;
