@@ -339,90 +339,6 @@ __global__ void k_mr_mark_particles(MrGeom g, const float* px, const float* py, 
 // ---- P2G (src/driver/multires_ops3d_tp.cpp:20-130, 209-274) --------------
 
 
-// One axis of one particle: the weights of the leaf-boundary patches within
-// the kernel radius (collectWeightedFaces: (k, j, i) order, clamped ranges),
-// normalised by their sum, splatted into momentum and raw mass.  The two
-// passes evaluate each weight with the same operations, so the sum is the
-// reference's.
-// One axis of one particle: the weights of the leaf-boundary patches within
-// the kernel radius (collectWeightedFaces: every lattice patch with
-// |d| < 1.5 per axis, at most 3 per axis), normalised by their sum and handed
-// to sink(i, j, k, momentum, mass).  The squared distance splits per axis, so
-// the 3 + 3 + 3 squared offsets are formed once and each of the 27 weights
-// costs two adds and the cubic; the arithmetic is FP32 (the reference's
-// FP64 weights to within FP32 rounding).  Patch validity is tested per patch
-// only where the candidates straddle both levels.
-template <class Sink>
-__device__ __forceinline__ void mr_splat_axis(const MrGeom& g, int axis, double px, double py, double pz, float mp,
-                                              float v, Sink&& sink) {
-  const double c[3] = {px, py, pz};
-  const int n[3] = {g.nx, g.ny, g.nz};
-  int p0[3], cnt[3];
-  float e[3];  // offset of the particle from the first candidate, per axis
-#pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    const double s = d == axis ? c[d] : c[d] - 0.5;
-    const int top = d == axis ? n[d] : n[d] - 1;
-    const int first = (int)floor(s - 1.5) + 1;  // the first integer above s - 1.5
-    const int lo = max(first, 0), hi = min(first + 2, top);
-    p0[d] = lo;
-    cnt[d] = max(0, hi - lo + 1);
-    e[d] = (float)(s - (double)lo);
-  }
-  if (cnt[0] == 0 || cnt[1] == 0 || cnt[2] == 0) return;
-  // the levels of the blocks the candidates' cells can lie in (along the
-  // axis the cells on both sides of each patch)
-  int mode;  // 0 all refined, 1 all coarse, 2 mixed
-  {
-    int cl[3], ch[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      cl[d] = max(0, p0[d] - (d == axis ? 1 : 0));
-      ch[d] = min(n[d] - 1, p0[d] + cnt[d] - 1);
-    }
-    int nref = 0;
-#pragma unroll
-    for (int q = 0; q < 8; ++q) nref += mr_refined(g, q & 1 ? ch[0] : cl[0], q & 2 ? ch[1] : cl[1], q & 4 ? ch[2] : cl[2]);
-    mode = nref == 8 ? 0 : nref == 0 ? 1 : 2;
-  }
-  const int na = n[axis];
-  float wsum = 0.0f;
-#pragma unroll 1
-  for (int pass = 0; pass < 2; ++pass) {
-    const float inv = pass ? 1.0f / wsum : 0.0f;
-#pragma unroll 1
-    for (int k = 0; k < cnt[2]; ++k) {
-      const float dz = e[2] - (float)k;
-#pragma unroll 1
-      for (int j = 0; j < cnt[1]; ++j) {
-        const float dy = e[1] - (float)j;
-        const float dyz = dy * dy + dz * dz;
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-          if (i >= cnt[0]) continue;
-          const float dx = e[0] - (float)i;
-          const float t = 1.0f - (dx * dx + dyz) * (1.0f / 2.25f);
-          if (!(t > 0.0f)) continue;
-          const int fi = p0[0] + i, fj = p0[1] + j, fk = p0[2] + k;
-          if (mode != 0) {
-            const int pos = axis == 0 ? fi : axis == 1 ? fj : fk;
-            const bool edge = (pos & 1) == 0 || pos == na;
-            if (!edge && (mode == 1 || !mr_face_valid(g, axis, fi, fj, fk))) continue;
-          }
-          const float w = t * t * t;
-          if (pass == 0) {
-            wsum += w;
-          } else {
-            const float wn = w * inv;
-            sink(fi, fj, fk, wn * mp * v, wn * mp);
-          }
-        }
-      }
-    }
-    if (!(wsum > 0.0f)) return;
-  }
-}
-
 struct MrFaces {
   float* f[9];
 };
@@ -432,6 +348,97 @@ struct MrFaces {
 // lattice; k_mr_split then writes u = momentum / mass (where mass > 0) and
 // the mass.  Accumulation order is the atomics' (not the reference's
 // particle order).
+// One particle's splat onto the leaf-boundary patches of face axis AX within
+// the kernel radius (collectWeightedFaces: every lattice patch with |d| < 1.5
+// per axis, at most 3 per axis, in (k, j, i) order over clamped ranges),
+// normalised by their sum.  The squared distance splits per axis, so each of
+// the 27 weights costs two adds and the cubic in FP32 (the reference's FP64
+// weights to within FP32 rounding); they are held in registers between the
+// sum and the splat.  Patch validity is tested per patch only where the
+// candidates' cells straddle both levels.  Momentum and raw mass of a patch
+// go out in one vector atomic.
+template <int AX>
+__device__ __forceinline__ void mr_p2g_axis(const MrGeom& g, double px, double py, double pz, float mp, float v,
+                                            float2* acc) {
+  const double c[3] = {px, py, pz};
+  const int n[3] = {g.nx, g.ny, g.nz};
+  int p0[3], cnt[3];
+  float e[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double s = d == AX ? c[d] : c[d] - 0.5;
+    const int top = d == AX ? n[d] : n[d] - 1;
+    const int first = (int)floor(s - 1.5) + 1;
+    const int lo = max(first, 0), hi = min(first + 2, top);
+    p0[d] = lo;
+    cnt[d] = max(0, hi - lo + 1);
+    e[d] = (float)(s - (double)lo);
+  }
+  if (cnt[0] == 0 || cnt[1] == 0 || cnt[2] == 0) return;
+  int mode;  // 0 all refined, 1 all coarse, 2 mixed
+  {
+    int cl[3], ch[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      cl[d] = max(0, p0[d] - (d == AX ? 1 : 0));
+      ch[d] = min(n[d] - 1, p0[d] + cnt[d] - 1);
+    }
+    int nref = 0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) nref += mr_refined(g, q & 1 ? ch[0] : cl[0], q & 2 ? ch[1] : cl[1], q & 4 ? ch[2] : cl[2]);
+    mode = nref == 8 ? 0 : nref == 0 ? 1 : 2;
+  }
+  const int na = n[AX];
+  float w[27];
+  float wsum = 0.0f;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const float dz = e[2] - (float)k;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const float dy = e[1] - (float)j;
+      const float dyz = dy * dy + dz * dz;
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        float ww = 0.0f;
+        if (i < cnt[0] && j < cnt[1] && k < cnt[2]) {
+          const float dx = e[0] - (float)i;
+          const float t = 1.0f - (dx * dx + dyz) * (1.0f / 2.25f);
+          if (t > 0.0f) {
+            bool ok = true;
+            if (mode != 0) {
+              const int pos = AX == 0 ? p0[0] + i : AX == 1 ? p0[1] + j : p0[2] + k;
+              const bool edge = (pos & 1) == 0 || pos == na;
+              ok = edge || (mode == 2 && mr_face_valid(g, AX, p0[0] + i, p0[1] + j, p0[2] + k));
+            }
+            if (ok) {
+              ww = t * t * t;
+              wsum += ww;
+            }
+          }
+        }
+        w[i + 3 * j + 9 * k] = ww;
+      }
+    }
+  }
+  if (!(wsum > 0.0f)) return;
+  const float inv = 1.0f / wsum;
+  const size_t X = (size_t)g.nx + (AX == 0), Y = (size_t)g.ny + (AX == 1);
+  float2* base = acc + mr_face(g, AX, p0[0], p0[1], p0[2]);
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        const float ww = w[i + 3 * j + 9 * k];
+        if (ww > 0.0f) {
+          const float wn = ww * inv;
+          atomicAdd(base + (i + X * (j + Y * k)), make_float2(wn * mp * v, wn * mp));
+        }
+      }
+}
+
 __global__ void __launch_bounds__(kMrNT) k_mr_p2g(MrGeom g, const float* px, const float* py, const float* pz,
                                                 const float* vx, const float* vy, const float* vz, const float* vol,
                                                 const uint8_t* type, size_t n, double mpl, double mpg, float2* acc0,
@@ -440,14 +447,9 @@ __global__ void __launch_bounds__(kMrNT) k_mr_p2g(MrGeom g, const float* px, con
   if (q >= n) return;
   const float mp = (float)((type[q] == 0 ? mpl : mpg) * (double)vol[q]);
   const double x = (double)px[q] / g.dx, y = (double)py[q] / g.dx, z = (double)pz[q] / g.dx;
-  const float v0 = vx[q], v1 = vy[q], v2 = vz[q];
-#pragma unroll 1
-  for (int a = 0; a < 3; ++a) {
-    float2* acc = a == 0 ? acc0 : a == 1 ? acc1 : acc2;
-    mr_splat_axis(g, a, x, y, z, mp, a == 0 ? v0 : a == 1 ? v1 : v2, [&](int i, int j, int k, float m, float w) {
-      atomicAdd(&acc[mr_face(g, a, i, j, k)], make_float2(m, w));
-    });
-  }
+  mr_p2g_axis<0>(g, x, y, z, mp, vx[q], acc0);
+  mr_p2g_axis<1>(g, x, y, z, mp, vy[q], acc1);
+  mr_p2g_axis<2>(g, x, y, z, mp, vz[q], acc2);
 }
 
 // u = momentum / mass where the mass is positive (else the momentum, 0), mass
