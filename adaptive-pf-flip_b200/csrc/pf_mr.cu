@@ -705,6 +705,8 @@ __global__ void __launch_bounds__(kMrNT) k_mr_spmv(int N, const int* __restrict_
                                                  const double* __restrict__ z, const double* __restrict__ p_prev,
                                                  double* p, double* Ap, const double* __restrict__ diag, MrCtl* ctl,
                                                  double* partials, const int* air) {
+  pdl_wait();
+  pdl_launch_dependents();
   if (ctl->done) return;
   const int pin = mr_pin(air, N);
   const double beta = ctl->beta;
@@ -774,6 +776,8 @@ __global__ void __launch_bounds__(kMrNT) k_mr_spmv(int N, const int* __restrict_
 // after the previous row's stores).
 constexpr int kMrRows = 4;
 __global__ void __launch_bounds__(kMrNT) k_mr_update(int N, MrVecs V, MrCtl* ctl, double* partials) {
+  pdl_wait();
+  pdl_launch_dependents();
   if (ctl->done) return;
   const double alpha = ctl->alpha;
   const int jacobi = ctl->jacobi, flexible = ctl->flexible;
@@ -1342,11 +1346,16 @@ int project_mr(pf_ctx* ctx, MrState* s, const pf_mr_step_cfg* cfg, pf_mr_step_st
       const int q = (launched + b) & 1;
       double* p_prev = pbuf[q];
       double* p = pbuf[q ^ 1];
-      (++ctx->launches), k_mr_spmv<<<nspmv, kMrNT, 0, ctx->stream>>>(N, s->slice_ptr, s->col, s->coef, V.z, p_prev,
-                                                                    p, V.Ap, V.diag, s->ctl, s->partials, tot + 3);
+      // programmatic dependent launches: each kernel's CTAs are scheduled
+      // while its predecessor drains and wait for it before reading anything
+      ++ctx->launches;
+      PF_CUDA_TRY(launch_pdl(k_mr_spmv, dim3(nspmv), dim3(kMrNT), ctx->stream, N, (const int*)s->slice_ptr,
+                             (const int*)s->col, (const double*)s->coef, (const double*)V.z, (const double*)p_prev,
+                             p, V.Ap, (const double*)V.diag, s->ctl, s->partials, (const int*)(tot + 3)));
       MrVecs Vi = V;
       Vi.p = p;
-      (++ctx->launches), k_mr_update<<<nupd, kMrNT, 0, ctx->stream>>>(N, Vi, s->ctl, s->partials);
+      ++ctx->launches;
+      PF_CUDA_TRY(launch_pdl(k_mr_update, dim3(nupd), dim3(kMrNT), ctx->stream, N, Vi, s->ctl, s->partials));
     }
     PF_CUDA_TRY(cudaGetLastError());
     launched += batch;
