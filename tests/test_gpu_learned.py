@@ -323,3 +323,55 @@ def test_inner_outer_solvers_reach_the_fp64_tolerance(pf, name):
         assert np.abs(p - p_plain).max() < 2e-4 * np.abs(p_plain).max()
     finally:
         g.close()
+
+
+def test_solutions_against_the_fp64_oracle(pf):
+    """Every solver mode's pressure on a 48^3 ellipsoid system at 1000:1 (the
+    network with its shipped weights) against the CPU FP64 oracle's
+    (oracle/pf_oracle.c, Jacobi-PCG to a 1e-10 relative residual).  The
+    single-level FP64 Krylov solves on the exact operator (PLAIN, and the
+    flexible PCG with or without the network) land within 1e-6 of the
+    pressure scale.  The inner-outer solvers stop at the same 1e-6 relative
+    FP64 residual along another Krylov path, and at 1000:1 that residual
+    bounds the error only to about 1e-5."""
+    import oracle as O
+
+    n = 48
+    sc = pf.scenes.ellipsoid_pressure(n, seed=0)
+    pp = pf.PhaseParams(sc["rho_l"], sc["rho_g"])
+    names = ("u", "v", "w", "mu", "mv", "mw", "p", "mk")
+    g, solve = _pressure_system(pf, n, seed=0)
+    try:
+        pp.rho_tilde_0 = pf.calibrateRhoTilde0(pp, 1.0, grid=g)
+        f = pf.scenes.pressure_grid_fields(sc, pp.rho_tilde_0)
+        go = O.OracleGrid(n, n, n, sc["dx"])
+        for k in ("u", "v", "w", "mu", "mv", "mw", "mk"):
+            i = names.index(k)
+            go.set_field(i, f[k], np.ones(go.bdims(i)[::-1], np.uint8))
+        st_o = O.Oracle().project(go, O.PhaseParams(pp.rho_l, pp.rho_g, pp.alpha_phi, pp.rho_tilde_0), 1.0 / 240.0,
+                                  200000, 0.0, rel_tol=1e-10)
+        assert st_o.converged
+        p_o, _ = go.get_field(O.P)
+        p_o = p_o.astype(np.float64)
+        scale = np.abs(p_o).max()
+        pf.LearnedCoarseSolver(g).load_default()
+        L = pf.PF_SOLVER_LEARNED
+        modes = {
+            "plain": (pf.SolverConfig(mode=pf.PF_SOLVER_PLAIN, rel_tol=1e-6), 1e-6),
+            "learned": (pf.SolverConfig(mode=L, rel_tol=1e-6, precond=pf.PF_PRECOND_NETWORK), 1e-6),
+            "flex_jacobi": (pf.SolverConfig(mode=L, rel_tol=1e-6, precond=pf.PF_PRECOND_JACOBI), 1e-6),
+            "mixed_fp32": (pf.SolverConfig(mode=pf.PF_SOLVER_MIXED, rel_tol=1e-6), 1e-5),
+            "learned_mixed": (pf.SolverConfig(mode=L, rel_tol=1e-6, precond=pf.PF_PRECOND_NETWORK, inner_fp32=True),
+                              1e-5),
+            "mixed_bf16": (pf.SolverConfig(mode=pf.PF_SOLVER_MIXED, rel_tol=1e-6, bf16_storage=1), 1e-5),
+        }
+        errs = {}
+        for name, (cfg, tol) in modes.items():
+            st, p = solve(cfg, max_iter=60000)
+            assert st.converged and st.res_final <= 1e-6 * st.res0, name
+            errs[name] = float(np.abs(p - p_o).max() / scale)
+        print("error against the FP64 oracle:", errs)
+        for name, (_, tol) in modes.items():
+            assert errs[name] <= tol, (name, errs)
+    finally:
+        g.close()
