@@ -574,6 +574,11 @@ __device__ __forceinline__ int mr_pin(const int* air, int N) { return (*air || N
 // the most face patches a leaf visits: 6 faces of a 2x2-patch coarse leaf
 constexpr int kMrMaxPatches = 24;
 
+// The row builders keep a row's distinct columns in a local array and search
+// it below its running count, which the front end cannot tell apart from a
+// read of unset entries (diagnostic 549).
+#pragma nv_diag_suppress 549
+
 // off-diagonal terms of each row: one per distinct neighbour leaf
 __global__ void k_mr_row_count(MrGeom g, const uint8_t* mk, const int4* cells, const int* cell_idx, int N,
                                const int* air, int* row_len) {
@@ -695,6 +700,8 @@ __global__ void __launch_bounds__(kMrNT) k_mr_rows(MrGeom g, const uint8_t* mk, 
 // The direction p = z + beta p_prev (the previous iteration's update, or a
 // restart's beta = 0) formed where it is used, Ap (applyA, :824-838) and
 // p.Ap -> alpha.  p_prev and p are separate buffers, alternated by the host.
+#pragma nv_diag_default 549
+
 // Two rows per thread and pass (rows r and r + stride, in that order, so the
 // p.Ap partial keeps the one-row order): the slice offsets, the column and
 // coefficient loads and the neighbour gathers of both rows go out together,
@@ -732,7 +739,9 @@ __global__ void __launch_bounds__(kMrNT) k_mr_spmv(int N, const int* __restrict_
         w[k] = r == pin ? 0 : (slice_ptr[s + 1] - a) >> 5;
       }
     }
-    const int wmax = max(w[0], w[1]);
+    int wmax = 0;
+#pragma unroll
+    for (int k = 0; k < kMrSpmvRows; ++k) wmax = max(wmax, w[k]);
     // the loads of four terms per row go out together; each row's sum keeps its term order
     for (int t = 0; t < wmax; t += 4) {
       int cc[kMrSpmvRows][4];
