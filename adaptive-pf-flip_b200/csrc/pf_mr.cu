@@ -45,6 +45,8 @@ constexpr int kMrPoll = 16;        // PCG iterations launched between polls
 struct MrGeom {
   int nx, ny, nz;
   double dx;
+  double inv_dx;  // 1/dx
+  int dx_pow2;    // dx is a power of two: x / dx == x * inv_dx exactly
   int MX, MY, MZ;      // level-1 blocks, ceil(n / 8)
   int BX0, BY0, BZ0;   // level-0 blocks, ceil(n / 4)
   const uint8_t* refined;
@@ -92,6 +94,9 @@ struct MrState {
 };
 
 // ---- lattice helpers ----------------------------------------------------
+
+// x / dx, as a product where that is exact
+__device__ __forceinline__ double mr_grid(const MrGeom& g, double x) { return g.dx_pow2 ? x * g.inv_dx : x / g.dx; }
 
 __device__ __forceinline__ bool mr_in(const MrGeom& g, int i, int j, int k) {
   return i >= 0 && i < g.nx && j >= 0 && j < g.ny && k >= 0 && k < g.nz;
@@ -282,7 +287,7 @@ __global__ void __launch_bounds__(kMrNT) k_mr_bounds(MrGeom g, const float* px, 
   for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
     const double x = px[q], y = py[q], z = pz[q];
     if (!isfinite(x) || !isfinite(y) || !isfinite(z)) continue;
-    const int c[3] = {(int)(x / g.dx), (int)(y / g.dx), (int)(z / g.dx)};
+    const int c[3] = {(int)mr_grid(g, x), (int)mr_grid(g, y), (int)mr_grid(g, z)};
     if (!mr_in(g, c[0], c[1], c[2])) continue;
     const bool gas = type[q] == 1;
 #pragma unroll
@@ -327,7 +332,7 @@ __global__ void k_mr_mark_particles(MrGeom g, const float* px, const float* py, 
                                     uint8_t* mk) {
   const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n) return;
-  const int i = (int)((double)px[q] / g.dx), j = (int)((double)py[q] / g.dx), k = (int)((double)pz[q] / g.dx);
+  const int i = (int)mr_grid(g, (double)px[q]), j = (int)mr_grid(g, (double)py[q]), k = (int)mr_grid(g, (double)pz[q]);
   if (!mr_in(g, i, j, k) || mk[mr_cell(g, i, j, k)] == 2) return;
   int o[3];
   const int s = 1 << mr_leaf(g, i, j, k, o);
@@ -446,7 +451,7 @@ __global__ void __launch_bounds__(kMrNT) k_mr_p2g(MrGeom g, const float* px, con
   const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n) return;
   const float mp = (float)((type[q] == 0 ? mpl : mpg) * (double)vol[q]);
-  const double x = (double)px[q] / g.dx, y = (double)py[q] / g.dx, z = (double)pz[q] / g.dx;
+  const double x = mr_grid(g, (double)px[q]), y = mr_grid(g, (double)py[q]), z = mr_grid(g, (double)pz[q]);
   mr_p2g_axis<0>(g, x, y, z, mp, vx[q], acc0);
   mr_p2g_axis<1>(g, x, y, z, mp, vy[q], acc1);
   mr_p2g_axis<2>(g, x, y, z, mp, vz[q], acc2);
@@ -898,7 +903,7 @@ __global__ void k_mr_velocity(MrGeom g, int axis, const uint8_t* mk, const int* 
 // sampleU / sampleV / sampleW: clamped trilinear over the fine face lattice
 __device__ __forceinline__ double mr_sample(const MrGeom& g, const float* __restrict__ f, int axis, double x, double y,
                                             double z) {
-  const double p[3] = {x / g.dx, y / g.dx, z / g.dx};
+  const double p[3] = {mr_grid(g, x), mr_grid(g, y), mr_grid(g, z)};
   int b[3];
   double fr[3];
 #pragma unroll
@@ -1019,6 +1024,8 @@ int mr_state(pf_ctx* ctx, MrState** out) {
   g.ny = G.ny;
   g.nz = G.nz;
   g.dx = G.dx;
+  g.inv_dx = G.inv_dx;
+  g.dx_pow2 = G.dx_pow2;
   g.MX = (g.nx + 7) / 8;
   g.MY = (g.ny + 7) / 8;
   g.MZ = (g.nz + 7) / 8;
