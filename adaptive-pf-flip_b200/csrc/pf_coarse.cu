@@ -289,7 +289,7 @@ void coarse_release(pf_ctx* ctx) {
   if (!c) return;
   learned_release(c);
   CoarseOp& A = c->op;
-  void* ptrs[] = {A.cop, A.rc, A.ec, A.cls, A.drange, A.work, c->nbr, c->rc_part};
+  void* ptrs[] = {A.cop, A.rc, A.ec, A.cls, A.drange, A.work, c->nbr, c->rc_part, c->inv_d};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   delete c;

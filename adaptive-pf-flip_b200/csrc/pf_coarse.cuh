@@ -44,6 +44,7 @@ struct CoarseCtx {
   LearnedState* net = nullptr;
   size_t cls_cap = 0;
   int* nbr = nullptr;       // neighbour-slot table of the pool (6 per slot)
+  double* inv_d = nullptr;  // 1 / (scale diag) per cell of an FP64 flexible solve, 0 off the unknowns
   float* rc_part = nullptr; // per-warp restriction partials (16 warps x 2 classes per slot)
   size_t nbr_cap = 0;       // slots
 };

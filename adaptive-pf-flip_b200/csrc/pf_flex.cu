@@ -40,6 +40,9 @@ struct FlexVec {
   V *d, *cx, *cy, *cz;  // operator: diagonal and low-face couplings, times scale
   const uint8_t* cls;   // coarse class of each unknown (255: none)
   V scale;
+  // FP64 solves: inv_diag of every cell, formed once per solve (the passes
+  // then load it where they would load d, and divide nowhere)
+  const double* di;
 };
 
 __global__ void k_fx_set(SolveCtl* ctl, double tol_abs, double tol_rel, int max_iter, double offered, int reset) {
@@ -90,11 +93,12 @@ __device__ __forceinline__ float fmav(float a, float b, float c) { return __fmaf
 // r d^-1 + c (Jacobi term plus the coarse term), a product then a sum
 __device__ __forceinline__ double coarse_add(double r, double di, double c) { return __dadd_rn(__dmul_rn(r, di), c); }
 
-// inv_diag from the diagonal entry already loaded
+// 1 / (scale diag) of cell o: from the per-solve array in FP64 solves, else
+// formed here
 template <typename V>
-__device__ __forceinline__ double inv_diag_of(const FlexVec<V>& m, uint8_t kd, V dv) {
-  const double d = kd == 1 ? (double)m.scale * (double)dv : 0.0;
-  return d > 0.0 ? 1.0 / d : 0.0;
+__device__ __forceinline__ double inv_diag_at(const FlexVec<V>& m, uint8_t kd, size_t o) {
+  if constexpr (sizeof(V) == 8) return m.di[o];
+  else return inv_diag(m, kd, o);
 }
 
 constexpr int kWarpsPerSlot = PF_TV / 32;
@@ -165,6 +169,16 @@ __global__ void __launch_bounds__(PF_TV) k_fx_start(int nslots, SolveCtl* ctl, c
     if (rc_part) restrict_warp(m.cls, o, (double)r, s, rc_part);
   }
   block_reduce_3(rzj, rmax, 0.0, partials, ctl, kStageInit);  // res0, tol, done; flex = {r.D^-1 r, 0}
+}
+
+// inv_diag of every cell of the pooled slots (0 off the unknowns), once per
+// FP64 solve
+template <typename V>
+__global__ void __launch_bounds__(PF_TV) k_fx_inv_diag(int nslots, const uint8_t* kind, FlexVec<V> m, double* di) {
+  for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
+    const size_t o = (size_t)s * PF_TV + threadIdx.x;
+    di[o] = inv_diag(m, kind[o], o);
+  }
 }
 
 __global__ void k_build_nbr(DevGrid G, int nslots, int* nbr) {
@@ -247,12 +261,12 @@ __global__ void __launch_bounds__(PF_TV) k_fx_update(int nslots, SolveCtl* ctl, 
     double rn = 0.0;
     if (kd) {
       const float ev = used_c && cl != 255 ? ec[coarse_index(tile, cl)] : 0.0f;
-      const V e = m.e[o], p = m.p[o], r_old = m.r[o], ap = m.Ap[o], dv = m.d[o];
+      const V e = m.e[o], p = m.p[o], r_old = m.r[o], ap = m.Ap[o];
+      const double di = inv_diag_at(m, kd, o);
       m.e[o] = fmav(alpha, p, e);
       const V r = fmav(-alpha, ap, r_old);
       m.r[o] = r;
       rn = (double)r;
-      const double di = inv_diag_of(m, kd, dv);
       const double zp = used_c ? coarse_add((double)r_old, di, cl != 255 ? (double)ev : 0.0) : (double)r_old * di;
       rmax = fmax(rmax, fabs(rn));
       rzj = fmav(rn * rn, di, rzj);
@@ -350,7 +364,7 @@ __global__ void __launch_bounds__(PF_TV) k_fx_dir(const int* slot_tile, int nslo
     }
     if (!kd) continue;
     const float ev = use_c && cl != 255 ? ec[coarse_index(tile, cl)] : 0.0f;
-    const double di = inv_diag(m, kd, o);
+    const double di = inv_diag_at(m, kd, o);
     if (use_c) {
       const double z = coarse_add((double)m.r[o], di, cl != 255 ? (double)ev : 0.0);
       m.p[o] = fmav(beta, m.p[o], (V)z);
@@ -375,9 +389,12 @@ int build_neighbor_table(pf_ctx* ctx, int nslots, int** nbr) {
   if (c->nbr_cap < cap) {
     if (c->nbr) cudaFree(c->nbr);
     if (c->rc_part) cudaFree(c->rc_part);
+    if (c->inv_d) cudaFree(c->inv_d);
     c->nbr = nullptr;
     c->rc_part = nullptr;
+    c->inv_d = nullptr;
     PF_CUDA_TRY(cudaMalloc(&c->nbr, 6 * cap * sizeof(int)));
+    PF_CUDA_TRY(cudaMalloc(&c->inv_d, cap * PF_TV * sizeof(double)));
     PF_CUDA_TRY(cudaMalloc(&c->rc_part, cap * kWarpsPerSlot * 2 * sizeof(float)));
     c->nbr_cap = cap;
   }
@@ -586,6 +603,10 @@ int solve_learned(pf_ctx* ctx, int nslots, int nred, const uint8_t* kind, double
   if (!cfg->inner_fp32) {
     // FP64 flexible PCG on the exact operator
     FlexVec<double> m{ctx->x, ctx->r, ctx->Ap, ctx->p, ctx->diag, ctx->cx, ctx->cy, ctx->cz, cls, scale};
+    double* di = ((CoarseCtx*)ctx->learned)->inv_d;
+    (++ctx->launches), k_fx_inv_diag<double><<<nred, PF_TV, 0, ctx->stream>>>(nslots, kind, m, di);
+    PF_CUDA_TRY(cudaGetLastError());
+    m.di = di;
     SolveCtl o{};
     rc = flex_solve<double>(ctx, nslots, nred, kind, m, ctx->r, cfg->abs_tol, cfg->rel_tol, cfg->max_iter,
                             cfg->check_every, precond, cfg->accept_min_gain, 1, &o);
