@@ -215,9 +215,9 @@ __global__ void k_mark_particles(DevGrid G, const float* __restrict__ px, const 
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
   // (int) truncation, as the reference's cast
-  const int i = __double2int_rz(grid_coord(px[p], G.g.ox, G.g.dx));
-  const int j = __double2int_rz(grid_coord(py[p], G.g.oy, G.g.dx));
-  const int k = __double2int_rz(grid_coord(pz[p], G.g.oz, G.g.dx));
+  const int i = __double2int_rz(grid_coord_g(G.g, px[p], G.g.ox));
+  const int j = __double2int_rz(grid_coord_g(G.g, py[p], G.g.oy));
+  const int k = __double2int_rz(grid_coord_g(G.g, pz[p], G.g.oz));
   if (!in_cells(G.g, i, j, k)) return;
   const int sl = slot_of(G, i, j, k);
   if (sl < 0) return;  // unreachable: particle cell tiles are pooled first
@@ -225,7 +225,12 @@ __global__ void k_mark_particles(DevGrid G, const float* __restrict__ px, const 
   if ((int)(*m + 0.5f) != 2) {
     *m = 1.0f;
     activate4(G, PF_MK, i, j, k);
-    atomicMin(&first[act4_index(G.g, PF_MK, i, j, k)], walls + (uint32_t)p);
+    // the block's first-touch key is its smallest particle index: the lanes
+    // marking one block send one atomicMin, from the lowest lane (the
+    // smallest index of the group)
+    const int bid = act4_index(G.g, PF_MK, i, j, k);
+    const unsigned peers = __match_any_sync(__activemask(), bid);
+    if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicMin(&first[bid], walls + (uint32_t)p);
   }
 }
 
