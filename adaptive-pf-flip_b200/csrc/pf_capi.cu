@@ -59,7 +59,7 @@ void free_all(pf_ctx* c) {
   F(c->tile_count); F(c->tile_start); F(c->pkey); F(c->prank); F(c->perm); F(c->splat_stage);
   for (int* p : c->scan_levels) F(p);
   F(c->d_scalar);
-  F(c->x); F(c->r); F(c->p); F(c->Ap); F(c->diag); F(c->cx); F(c->cy); F(c->cz); F(c->kind);
+  F(c->x); F(c->r); F(c->p); F(c->Ap); F(c->diag); F(c->cx); F(c->cy); F(c->cz); F(c->kind); F(c->z_plain);
   F(c->partials); F(c->ctl); F(c->ctl_outer); F(c->nbr_plain);
   F(c->xf); F(c->rf); F(c->pf32); F(c->Apf); F(c->diagf); F(c->cxf); F(c->cyf); F(c->czf); F(c->pbf); F(c->cbf);
   F(c->b64);
@@ -192,7 +192,7 @@ int create_impl(pf_ctx* ctx, const pf_grid_desc* d) {
   if (rc) return rc;
   PF_CUDA_TRY(cudaMalloc(&ctx->d_scalar, 16 * sizeof(int)));
 
-  double** dv[8] = {&ctx->x, &ctx->r, &ctx->p, &ctx->Ap, &ctx->diag, &ctx->cx, &ctx->cy, &ctx->cz};
+  double** dv[9] = {&ctx->x, &ctx->r, &ctx->p, &ctx->Ap, &ctx->diag, &ctx->cx, &ctx->cy, &ctx->cz, &ctx->z_plain};
   for (double** q : dv) {
     PF_CUDA_TRY(cudaMalloc(q, cells * sizeof(double)));
     PF_CUDA_TRY(cudaMemset(*q, 0, cells * sizeof(double)));

@@ -91,6 +91,7 @@ struct pf_ctx {
   double *diag = nullptr, *cx = nullptr, *cy = nullptr, *cz = nullptr;
   double* partials = nullptr;  // [kMaxRedBlocks * 4]
   int* nbr_plain = nullptr;    // [cells_cap / 512 * 6] neighbour slots of each pooled tile (PLAIN PCG)
+  double* z_plain = nullptr;   // [cells_cap] PLAIN PCG's z (r / diag), from its update to its direction pass
   uint8_t* kind = nullptr;     // per cell: 0 not an unknown, 1 fluid, 2 pinned
   pf::SolveCtl* ctl = nullptr;
   pf::SolveCtl* h_ctl = nullptr;  // pinned mirror

@@ -13,6 +13,7 @@ namespace pf {
 template <typename V>
 struct PcgVec {
   V *x, *r, *p, *Ap, *diag, *cx, *cy, *cz;
+  V* z;  // PLAIN: z = r / diag from the update to the direction pass (null: formed in both)
   __device__ __forceinline__ void store_p(size_t o, double v) const { p[o] = (V)v; }
 };
 
